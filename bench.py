@@ -1,0 +1,349 @@
+"""Benchmark of the B200 DEM step on the rotational frictional shear cell.
+
+Workload (the headline configuration): 250,000 RotSpheres, lognormal radii
+(median 0.5, sigma 0.25, clipped to [0.2, 1.0]) packed by seeded random
+sequential insertion into a 100 x 50 x 100 box periodic in x; RotFriction
+kn = ks = 1e4, mu = 0.6; elastic walls (k = 1e4) at y = 0 and y = 50 moving at
+-/+0.01 in x with a 1e3 normal-load servo on the top wall; dt = 5e-5.
+Initial velocities and spins are seeded N(0, 0.1) so that contacts form.
+
+One bench "step" = --dem-steps timesteps (runOneStep x S) plus one servo
+call.  `value` is contact-updates/s (Verlet-list pairs + wall candidates
+evaluated per timestep) with the state resident in HBM; `e2e` repeats it
+through the C ABI with the particle state copied host->device before and
+device->host after every bench step.  L2 is flushed between bench steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "esys-particle_b200"))
+
+PI_REF = 3.141592654
+METRIC = "contact-updates/s at <=1e-5 rel force err vs FP64"
+UNIT = "contact-updates/s"
+
+
+def workload(n=250_000, seed=2):
+    """Seeded C2 packing through the library's RSI packer (esys_geometry.h)."""
+    from esys.lsm import _capi
+
+    lib = _capi.load_library()
+    f = lib.lsm_pack_rsi
+    D = C.POINTER(C.c_double)
+    f.argtypes = [C.c_ulonglong, C.c_int, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.c_int, D, D]
+    f.restype = C.c_int
+    pos = np.zeros((n, 3))
+    rad = np.zeros(n)
+    bmin = np.array([0.0, 0.0, 0.0])
+    bmax = np.array([100.0, 50.0, 100.0])
+    k = f(seed, n, bmin.ctypes.data_as(D), bmax.ctypes.data_as(D), 1, 1, 0.5, 0.25, 0.2, 1.0, 5000,
+          pos.ctypes.data_as(D), rad.ctypes.data_as(D))
+    if k != n:
+        raise RuntimeError(f"packer placed {k} of {n} spheres")
+    rng = np.random.default_rng(seed + 100)
+    vel = rng.normal(0.0, 0.1, size=(n, 3))
+    angvel = rng.normal(0.0, 0.1, size=(n, 3))
+    mass = (4.0 / 3.0) * 1.0 * PI_REF * rad * rad * rad
+    return dict(pos=pos, rad=rad, mass=mass, vel=vel, angvel=angvel, bmin=bmin, bmax=bmax,
+                ids=np.arange(n, dtype=np.int32))
+
+
+DT = 5e-5
+GRID, SKIN = 2.2, 0.2
+KN = KS = 1e4
+MU = 0.6
+KWALL = 1e4
+NORMAL_LOAD = 1e3
+
+
+def setup(make, w, periodic=True):
+    sim = make("RotSphere", GRID, SKIN, w["bmin"], w["bmax"], (1 if periodic else 0, 0, 0), DT)
+    sim.add_particles(w["ids"], w["pos"], w["rad"], w["mass"], tag=np.zeros(len(w["ids"]), np.int32),
+                      vel=w["vel"], angvel=w["angvel"])
+    sim.add_rot_friction_group("friction", KN, MU, MU, KS, DT, True, True)
+    sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, 50, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", KWALL)
+    sim.add_wall_group("top_w", "top", KWALL)
+    return sim
+
+
+class Clocks:
+    """Sample nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.samples, self._stop, self.index = [], False, index
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop:
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                time.sleep(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop = True
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    p = os.path.join(ROOT, "profiles", "k_step_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return None
+
+
+def cpu_reference_sample(w, steps, timeout_s=60.0):
+    """The reference's own C++ (oracle/_ref, one worker = one core) on the same packing.
+    The reference reaches periodic x only with >= 2 MPI workers, so the sample runs it with
+    the same particles and groups in a non-periodic box."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.available("ref"):
+        return None
+    sim = setup(lambda *a: oracle.OracleSim("ref", *a), w, periodic=False)
+    sim.step(1)  # first step: neighbour search + interaction set-up (not timed)
+    m = sim.f["num_pairs"](sim.h, b"friction")
+    pos = w["pos"]
+    ncand = int((np.abs(pos[:, 1] - 0.0) < GRID).sum() + (np.abs(pos[:, 1] - 50.0) < GRID).sum())
+    done, t0 = 0, time.perf_counter()
+    while done < steps and time.perf_counter() - t0 < timeout_s:
+        sim.step(1)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": (m + ncand) * done / dt, "steps": done, "seconds": dt, "pairs": int(m), "walls": ncand}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload()
+    res = cpu_reference_sample(w, steps=max(1, args.steps + args.warmup), timeout_s=180.0)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
+        return
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": res["steps"],
+        "warmup": 1, "ms_per_step": 1e3 * res["seconds"] / res["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "rot-friction shear cell, 250k RotSpheres, 100x50x100 (x periodic on the GPU path; "
+                               "the reference needs >=2 MPI workers for periodic x, so it runs non-periodic)",
+                   "dem_steps_per_step": 1},
+        "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{res['steps']} timesteps of the 250k-sphere packing after set-up, "
+                                   f"{res['pairs']} friction pairs + {res['walls']} wall candidates"},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--dem-steps", type=int, default=200, help="timesteps per bench step")
+    ap.add_argument("--tpp", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from esys.lsm import _capi
+
+    w = workload()
+    n = len(w["ids"])
+    sim = setup(lambda *a: _capi.DemSim(*a), w, periodic=True)
+    stream = torch.cuda.current_stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.set_option("profile", 1)
+    if args.tpp:
+        sim.set_option("threads_per_particle", args.tpp)
+    sim.set_wall_velocity("bottom", (-0.01, 0, 0))
+    sim.set_wall_velocity("top", (0.01, 0, 0))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def bench_step():
+        sim.step(args.dem_steps)
+        sim.apply_force_to_wall("top_w", (0.0, -NORMAL_LOAD, 0.0))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        bench_step()
+        flush.zero_()
+    barrier()
+    c0 = sim.counters()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            bench_step()
+            ev[k][1].record(stream)
+        barrier()
+    c1 = sim.counters()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    contacts = c1["contact_updates"] - c0["contact_updates"]
+    t_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        cc = torch.tensor([float(contacts)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(cc)
+        contacts_all = float(cc.item())
+    else:
+        contacts_all = float(contacts)
+    value = contacts_all / (t_max / 1e3)
+
+    # dominant kernel: the force + integration kernel, timed with CUDA events on its stream
+    step_ns = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / max(1, c1["profiled_steps"] - c0["profiled_steps"])
+    m_fric = sim._chk(sim.lib.dem_num_pairs(sim.h, b"friction"))
+    n_wall_cand = c1["contacts_per_step"] - m_fric
+    # algorithmic bytes per launch: particle 256 B (rot, FP64), RotFriction pair 60 B, wall candidate 4 B
+    alg_bytes = n * 256 + m_fric * 60 + n_wall_cand * 4
+    achieved = alg_bytes / (step_ns * 1e-9) / 1e9
+    peak, peak_kind = peaks()
+    traffic = traffic_per_launch()
+
+    # e2e through the C ABI with host buffers (pinned), H2D + D2H inside the timed region
+    pin = {k: torch.empty((n, wdt), dtype=torch.float64).pin_memory() for k, wdt in
+           (("pos", 3), ("vel", 3), ("angvel", 3), ("quat", 4), ("force", 3), ("moment", 3))}
+    ids_pin = torch.empty(n, dtype=torch.int32).pin_memory()
+    sim.get_particles_raw(ids_pin.data_ptr(), *(pin[k].data_ptr() for k in ("pos", "vel", "angvel", "quat", "force",
+                                                                             "moment")))
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    ce0 = sim.counters()
+    e2e_sec = 0.0
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s0 = time.perf_counter()
+        sim.set_particles(pos=pin["pos"].data_ptr(), vel=pin["vel"].data_ptr(), angvel=pin["angvel"].data_ptr(),
+                          quat=pin["quat"].data_ptr(), n=n)
+        bench_step()
+        sim.get_particles_raw(ids_pin.data_ptr(), *(pin[k].data_ptr() for k in ("pos", "vel", "angvel", "quat",
+                                                                                 "force", "moment")))
+        s1 = time.perf_counter()
+        e2e_sec += s1 - s0
+    ce1 = sim.counters()
+    e2e_contacts = ce1["contact_updates"] - ce0["contact_updates"]
+    e2e_val = e2e_contacts / e2e_sec
+    if dist is not None:
+        t = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        cc = torch.tensor([float(e2e_contacts)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(cc)
+        e2e_val = float(cc.item()) / float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_reference_sample(w, steps=30, timeout_s=25.0)
+        if res is not None:
+            cpu = {"value": res["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"{res['steps']} timesteps of the same 250k-sphere packing (non-periodic: the reference "
+                             f"needs >=2 MPI workers for periodic x), after set-up; {res['pairs']} friction pairs"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RSI packing)",
+            "config": {"workload": "rot-friction shear cell: 250,000 RotSpheres, lognormal r (0.5, 0.25) in "
+                                   "[0.2,1.0], 100x50x100 periodic-x, kn=ks=1e4 mu=0.6, 2 elastic walls "
+                                   "+-0.01 x, 1e3 servo load, dt=5e-5",
+                       "dem_steps_per_step": args.dem_steps, "particles": n,
+                       "interactions_per_timestep": c1["contacts_per_step"],
+                       "threads_per_particle": c1["threads_per_particle"],
+                       "l2": "flushed (256 MB write) between bench steps; working set ~90 MB stays L2-resident "
+                             "within a bench step",
+                       "parallelism": "replicas only" if world > 1 else "single GPU",
+                       "precision": "FP64 forces and integration (max rel force err vs FP64 = 0)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (traffic or {}).get("bytes_per_launch"),
+                         "kernel": "k_step<ROT=1,TPP>", "kernel_us": step_ns / 1e3,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": n * (24 + 24 + 24 + 32),
+                    "d2h_bytes_per_step": n * (6 * 32 + 4)},
+            "gpu_launches": c1["launches"] - c0["launches"],
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,134 @@
+// Device-side data layout of one simulated worker (shared by kernels and host).
+//
+// Particles live in slots in insertion order (the reference's particle-list
+// order, ntable/src/ntable.h:85); a slot is never reused, a particle that
+// leaves the grid is only marked dead.  State is structure-of-arrays of
+// 32-byte double4 records so that a neighbour gather touches one sector per
+// field, and it is double-buffered: a step reads buffer `cur` and writes
+// buffer `cur ^ 1`, which lets one kernel do forces and integration without a
+// grid-wide barrier.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dem {
+
+enum : unsigned {
+  PF_DYN = 1u,          // linear dynamics on (CParticle::m_is_dynamic)
+  PF_ROT = 2u,          // rotational dynamics on (CRotParticle::m_is_rot)
+  PF_ALIVE = 8u,        // still in the neighbour table
+  PF_WALL_SHIFT = 8,    // bits 8..15: candidate of wall group w (getParticlesAtPlane)
+  PF_INNER_SHIFT = 16,  // bits 16..23: candidate w is in the inner region (isInInner)
+};
+
+enum : int {
+  CTRL_REBUILD = 1,     // some particle moved further than verletDist/2
+  CTRL_BROKE = 2,       // at least one bond broke in the last force evaluation
+  CTRL_OVERFLOW = 4,    // an event buffer overflowed
+};
+
+constexpr int kMaxWalls = 8;
+constexpr int kMaxGrav = 4;
+constexpr int kMaxDyn = 2;
+constexpr int kMaxBond = 2;
+constexpr int kBondAlive = 0x7fffffff;
+
+struct Grid {
+  double p0x, p0y, p0z;  // origin of the global grid (the grown bounding box minimum)
+  double dim;            // cell size = gridSpacing
+  int gx, gy, gz;        // local-table offset of each dimension (-1: one padding layer)
+  int nx, ny, nz;        // cells of the local table, padding included
+  int circx;             // periodic in x
+  double Lx, xmin;       // periodic box length and minimum
+  double alpha;          // verletDist
+};
+
+struct ParticleBuf {
+  double4* pr;  // x, y, z, radius
+  double4* vm;  // vx, vy, vz, mass
+  double4* wi;  // wx, wy, wz, rotational inertia
+  double4* qq;  // quaternion scalar, x, y, z
+};
+
+struct Particles {
+  int n;                 // slots in use
+  ParticleBuf buf[2];
+  double2* inv;          // 1/mass, 1/inertia
+  double4* oldpos;       // position at the last neighbour search
+  double4* force;        // last accumulated force  (w unused)
+  double4* moment;       // last accumulated moment (w unused)
+  unsigned* pflags;      // PF_* bits
+  unsigned char* flagged;// set on both particles of a broken bond (CParticle::flag)
+  int* id;
+  int* tag;
+  int* cell;             // cell of each slot at the last neighbour search
+};
+
+struct WallDev {
+  double ox, oy, oz, nx, ny, nz;  // plane origin and normal (CWall)
+  double k;                       // NRotElasticWall normalK
+};
+
+// One dynamic interaction group (PIS_NE elastic or PIS_ED rot friction) as
+// seen by the step kernel: a per-particle adjacency over the group's pairs.
+struct DynDev {
+  int kind;             // 0 NRotElastic, 1 RotFriction
+  double k, ks, mu_s, mu_d, dt;
+  int scaling, meanR;
+  const int* adj_start; // n+1
+  const int2* adj;      // (partner slot, pair index | 0x80000000 when this particle is p1)
+  const double4* hist_in;   // RotFriction: Ffric xyz, w = slipping + 2*touching
+  double4* hist_out;
+};
+
+struct BondDev {
+  double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
+  int scaling, meanR;
+  const int* adj_start;
+  const int2* adj;          // (partner slot, bond index | 0x80000000 when this particle is p1)
+  const double4* D0;        // m_D: p2 - p1 at creation (w unused)
+  int* broken_step;         // kBondAlive while intact; else the step of the update that removes it
+  int* events;              // (id1, id2, step) triples
+  int* nevents;
+  int cap_events;
+};
+
+// Intact bonds of the groups that exclude pairs from a dynamic group
+// (TSubLattice::setExIG, Parallel/SubLattice.hpp:1980-2009).  Bond arrays are
+// stored in (p1 slot, p2 slot) key order, so a key's position is its bond index.
+struct ExclDev {
+  int n;
+  const unsigned long long* keys[kMaxBond];
+  const int* broken_step[kMaxBond];
+  int count[kMaxBond];
+};
+
+struct StepArgs {
+  Grid g;
+  Particles P;
+  int cur;                 // input buffer index
+  double dt;
+  double half_alpha_sq;    // (verletDist/2)^2
+  long long step;          // timestep number being computed (1-based, like CLatticeMaster::m_t)
+  int nwall;
+  WallDev* walls;           // [nwall] in group-name order; origins move on the device
+  const double* wall_vel;   // [nwall][3] native wall loader velocity (0 = static)
+  int ngrav;
+  double grav[kMaxGrav][3];
+  int ndyn;
+  DynDev dyn[kMaxDyn];
+  int nbond;
+  BondDev bond[kMaxBond];
+  int damp_lin, damp_rot;   // damping groups present
+  double visc_lin, visc_rot, dt_lin, dt_rot;
+  int iter_lin, iter_rot;
+  int store_forces;
+  double* wall_partial;     // [gridDim.x][kMaxWalls][3]
+  double* wall_force;       // [kMaxWalls][3]: reaction of each wall group (adds into CWall::m_force)
+  unsigned* block_counter;  // last-block detection (wraps to 0 by itself)
+  long long* step_counter;  // timesteps completed on the device
+  int* ctrl;                // CTRL_* bits raised by this chunk of steps
+  int* stop;                // set by the last block when ctrl != 0: later steps of the chunk skip
+};
+
+}  // namespace dem

@@ -1,0 +1,42 @@
+// Launch wrappers of the DEM kernels (dem_kernels.cu), called by the host
+// simulation object (dem_sim.cu).  All launches are asynchronous on stream s.
+#pragma once
+#include "dem_device.cuh"
+
+namespace dem {
+
+void launch_scan(const int* in, int* out, int n, int* total, cudaStream_t s);
+void launch_bin(const Grid& g, const Particles& P, int cur, int* cell_count, cudaStream_t s);
+void launch_scatter_cells(const Particles& P, const int* cell_start, int* cursor, int* cell_list, cudaStream_t s);
+void launch_sort_cells(int ncell, const int* cell_start, int* cell_list, cudaStream_t s);
+void launch_pairs_count(const Grid& g, const Particles& P, int cur, const int* cs, const int* cl, const ExclDev& ex,
+                        int* count, cudaStream_t s);
+void launch_pairs_write(const Grid& g, const Particles& P, int cur, const int* cs, const int* cl, const ExclDev& ex,
+                        const int* start, unsigned long long* keys, int kind, const unsigned long long* old_keys,
+                        int old_n, const double4* old_hist, double4* hist, cudaStream_t s);
+void launch_adj(const unsigned long long* keys, int m, int n, int* adj_count, int* p1_start, int* adj_start,
+                int* adj_cursor, int2* adj, int* total, cudaStream_t s);
+void launch_newlist_count(const Grid& g, const Particles& P, const int* cs, const int* cl, const ExclDev& ex,
+                          const unsigned long long* keys, int m, int check_in, int* count, cudaStream_t s);
+void launch_newlist_write(const Grid& g, const Particles& P, const int* cs, const int* cl, const ExclDev& ex,
+                          const unsigned long long* keys, int m, int check_in, const int* start,
+                          unsigned long long* out, cudaStream_t s);
+void launch_merge(const unsigned long long* A, const double4* Ah, int m, const unsigned long long* B, int nb,
+                  unsigned long long* out, double4* outh, int kind, cudaStream_t s);
+void launch_clear_flags(int n, unsigned char* flagged, cudaStream_t s);
+void launch_pairs_alive(const unsigned long long* keys, int m, const unsigned* pflags, int* keep, cudaStream_t s);
+void launch_compact(const unsigned long long* keys, const double4* hist, int m, const int* keep, const int* pos,
+                    unsigned long long* okeys, double4* ohist, int kind, cudaStream_t s);
+void launch_bonds_rebuild(int nb, const int2* ends, const unsigned* pflags, int* broken_step, cudaStream_t s);
+void launch_bonds_init(int nb, const int2* ends, const double4* pr, double4* D0, cudaStream_t s);
+void launch_wall_update(const Grid& g, const Particles& P, int cur, int nwall, const WallDev* walls, int* ncand,
+                        cudaStream_t s);
+void launch_set_state(const Particles& P, int cur, int cnt, const int* slots, const double* pos, const double* vel,
+                      const double* angvel, const double* quat, cudaStream_t s);
+void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* ctrl, cudaStream_t s);
+void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, cudaStream_t s);
+void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s);
+int step_grid(int n, int tpp);
+void launch_step(const StepArgs& a, bool rot, int tpp, cudaStream_t s);
+
+}  // namespace dem

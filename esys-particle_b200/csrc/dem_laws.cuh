@@ -1,0 +1,277 @@
+// Per-pair and per-particle force laws of the DEM step, FP64.
+//
+// Each law is evaluated in the canonical orientation (p1 = lower particle id,
+// p2 = higher), with p2's position already replaced by its periodic image
+// nearest p1.  A particle-centric kernel evaluates every pair from both
+// sides; both sides call the same function on the same inputs, so both get
+// bit-identical results and the pair's contributions cancel exactly.
+#pragma once
+#include "dem_math.cuh"
+
+namespace dem {
+
+using V = V3<double>;
+using Qd = Quat<double>;
+
+// CElasticInteraction ctor scaling (Model/ElasticInteraction.cpp:25-49).
+__device__ __forceinline__ double elastic_k(double k, int scaling, double r1, double r2) {
+  double effR = 1.0, effA = 1.0, effL = 1.0;
+  double r0 = r1 + r2;
+  if (scaling) { effR = 0.5 * r0; effL = r0; effA = effR * effR; }
+  return k * effA / effL;
+}
+
+// CElasticInteraction::calcForces (Model/ElasticInteraction.cpp:54-71).
+// Returns true when touching; F is the force applied to p2 (p1 gets -F).
+__device__ __forceinline__ bool law_elastic(double k_eff, const V& x1, double r1, const V& x2, double r2, V& F) {
+  V D = x1 - x2;
+  double dist = dot(D, D);
+  double eq_dist = r1 + r2;
+  if (dist < (eq_dist * eq_dist)) {
+    dist = sqrt(dist);
+    F = D * (k_eff * (dist - eq_dist) / dist);
+    return true;
+  }
+  return false;
+}
+
+// CRotFrictionInteraction ctor scaling (Model/RotFricInteraction.cpp:103-146).
+__device__ __forceinline__ void friction_k(double k, double ks, int scaling, int meanR, double r1, double r2,
+                                           double& k_eff, double& ks_eff) {
+  double effR = 1.0, effL = 1.0, effA = 1.0;
+  double r0 = r1 + r2;
+  if (scaling) {
+    if (meanR) effR = 0.5 * r0; else effR = fmin(r1, r2);
+    effL = r0;
+    effA = effR * effR;
+  }
+  k_eff = k * effA / effL;
+  ks_eff = ks * effA / effL;
+}
+
+struct FricOut {
+  V fn;        // normal force applied to p2 (p1 gets -fn)
+  V Ffric;     // tangential force after the update (p1 gets +Ffric, p2 gets -Ffric)
+  V M1, M2;    // moments on p1, p2
+  bool touching, slipping;
+};
+
+// CRotFrictionInteraction::calcSimpleForces (Model/RotFricInteraction.cpp:171-231).
+__device__ __forceinline__ void law_friction(double k_eff, double ks_eff, double mu_s, double mu_d, double dt,
+                                             const V& x1, double r1, const V& v1, const V& w1, const V& x2, double r2,
+                                             const V& v2, const V& w2, V Ffric, bool slipping, FricOut& o) {
+  double mu_current = slipping ? mu_d : mu_s;
+  const V D = x1 - x2;
+  double dist = dot(D, D);
+  const double eq_dist = r1 + r2;
+  if (dist < (eq_dist * eq_dist)) {
+    dist = sqrt(dist);
+    const V force = D * (k_eff * (dist - eq_dist) / dist);
+    const V pos = x2 + (r2 / eq_dist) * D;
+    const V vp1 = v1 + cross(w1, pos - x1);
+    const V vp2 = v2 + cross(w2, pos - x2);
+    V ds = (vp2 - vp1) * dt;
+    ds -= ((dot(ds, D)) / (norm2(D))) * D;
+    Ffric += ks_eff * ds;
+    const double FfricNorm = norm(Ffric);
+    const double forceNorm = norm(force);
+    if (FfricNorm > forceNorm * mu_current) {
+      Ffric = Ffric * ((mu_d * forceNorm) / FfricNorm);
+      o.slipping = true;
+    } else {
+      o.slipping = false;
+    }
+    o.M1 = cross(pos - x1, Ffric);
+    o.M2 = cross(pos - x2, -Ffric);
+    o.fn = force;
+    o.Ffric = Ffric;
+    o.touching = true;
+  } else {
+    o.Ffric = mk(0.0, 0.0, 0.0);
+    o.fn = mk(0.0, 0.0, 0.0);
+    o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+    o.slipping = false;
+    o.touching = false;
+  }
+}
+
+// CRotFrictionInteraction::isPersistent (Model/RotFricInteraction.cpp:345-351).
+__device__ __forceinline__ bool friction_persistent(const V& x1, double r1, const V& x2, double r2) {
+  V D = x1 - x2;
+  double dist = dot(D, D);
+  double eq_dist = r1 + r2;
+  return dist <= (eq_dist * eq_dist);
+}
+
+// Scaled RotBond constants (ARotBondedInteraction.cpp:141-180 overridden by
+// CRotBondedInteraction ctor, Model/RotBondedInteraction.cpp:122-161).  dist0 is
+// |m_D|, the particle distance when the bond was created.
+struct BondK {
+  double kr, ks, kb, kt, max_n, max_s, max_b, max_t;
+};
+__device__ __forceinline__ BondK bond_k(double kr, double ks, double kt, double kb, double mn, double ms, double mt,
+                                        double mb, int scaling, int meanR, double dist0, double r1, double r2) {
+  double effR = 1.0, effL = 1.0, effA = 1.0, J = 1.0, I = 1.0;
+  if (scaling) {
+    if (meanR) effR = 0.5 * dist0; else effR = fmin(r1, r2);
+    effL = dist0;
+    effA = effR * effR;
+    J = 0.5 * effR * effR * effR * effR;
+    I = 0.5 * J;
+  }
+  BondK b;
+  b.kr = kr * effA / effL;
+  b.ks = ks * effA / effL;
+  b.kb = kb * I / effL;
+  b.kt = kt * J / effL;
+  b.max_n = mn * effA;
+  b.max_s = ms * effA;
+  b.max_b = mb * I / effR;
+  b.max_t = mt * J / effR;
+  return b;
+}
+
+// calc_angle (Model/ARotBondedInteraction.cpp:22-51).
+__device__ __forceinline__ double calc_angle(double s_in, double c_os) {
+  if (s_in > 0.0) return (c_os >= 1.0 || c_os <= -1.0) ? 0.0 : acos(c_os);
+  if (s_in == 0.0) return 0.0;
+  return (c_os >= 1.0 || c_os <= -1.0) ? 0.0 : -acos(c_os);
+}
+
+struct BondOut {
+  V force;    // applied to p1 (p2 gets -force)
+  V moment1;  // applied to p1
+  V moment2;  // applied to p2
+  double nF, shF, tM, bM;
+};
+
+// ARotBondedInteraction::calcForces (Model/ARotBondedInteraction.cpp:307-448).
+__device__ __forceinline__ void law_bond(const BondK& K, const V& m_D, const V& x1, double r1, const Qd& q1,
+                                         const V& x2, double r2, const Qd& q2, BondOut& o) {
+  const double HALF_SQRT_2 = 0.5 * sqrt(2.0);
+  double s_fai = 0.0, c_fai = 0.0, c_pasi2 = 0.0, s_pasi2 = 0.0, sita = 0.0, pasi = 0.0;
+  const M3<double> mat0 = to_matrix(q1);
+  const V rbp = x2 - x1;
+  const double rbpNorm = norm(rbp);
+  const V rb = mul(mat0, x2 - x1);
+  const double rbNorm = norm(rb);
+  const double r_0Norm = r1 + r2;
+  const V delta_r = (rbNorm - r_0Norm) * rb / rbNorm;
+  const V Fr = K.kr * delta_r;
+  const double gama_cos = dot(rb, m_D) / (rbNorm * norm(m_D));
+  double gama = 0.0;
+  if (gama_cos < 1.0 && gama_cos > -1.0) gama = acos(gama_cos);
+  const V rb_0 = cross(rb, m_D);
+  const V rb_b0 = cross(rb, rb_0);
+  const double rb_b0Norm = norm(rb_b0);
+  V Fst = mk(0.0, 0.0, 0.0);
+  if (rb_b0Norm != 0) Fst = K.ks * r_0Norm * gama * rb_b0 / rb_b0Norm;
+  V Mst = mk(0.0, 0.0, 0.0);
+  const double rb_0Norm = norm(rb_0);
+  if (rb_0Norm != 0) Mst = -norm(Fst) * rb_0 / rb_0Norm;
+  const double m0 = HALF_SQRT_2 * sqrt((rbNorm + rb.z) / rbNorm);
+  double m1 = -HALF_SQRT_2 * sqrt((rbNorm - rb.z) / rbNorm);
+  double m2 = -m1;
+  const double m3 = 0.0;
+  const double rbX2PlusRbY2 = rb.x * rb.x + rb.y * rb.y;
+  if (rbX2PlusRbY2 != 0.0) {
+    const double denomSqrt = sqrt(rbX2PlusRbY2);
+    m1 = m1 * rb.y / denomSqrt;
+    m2 = m2 * rb.x / denomSqrt;
+  }
+  const Qd qm{m0, mk(m1, m2, m3)};
+  const M3<double> mat = to_matrix(qm);
+  const Qd rp = qmul(qinv(q1), q2);
+  const Qd r = qmul(qmul(qinv(qm), rp), qm);
+  const double temp0 = r.s * r.s + r.v.z * r.v.z;
+  if (temp0 == 0.0) {
+    pasi = 0.0;
+  } else {
+    const double sqrtTemp0 = sqrt(temp0);
+    c_pasi2 = r.s / sqrtTemp0;
+    s_pasi2 = r.v.z / sqrtTemp0;
+    pasi = 2.0 * calc_angle(s_pasi2, c_pasi2);
+  }
+  const V Mtp = mk(0.0, 0.0, K.kt * pasi);
+  const V Mtr = mulT(mat, Mtp);
+  const double temp2 = r.v.x * r.v.x + r.v.y * r.v.y;
+  const double temp3 = r.v.x * r.v.z + r.s * r.v.y;
+  const double temp4 = r.v.y * r.v.z - r.s * r.v.x;
+  V Mbr = mk(0.0, 0.0, 0.0), Fsr = mk(0.0, 0.0, 0.0), Msr = mk(0.0, 0.0, 0.0);
+  if (temp2 != 0.0) {
+    const double temp1 = temp0 - temp2;
+    if (temp1 >= 1.0 || temp1 <= -1.0) sita = 0.0; else sita = acos(temp1);
+    if (temp0 == 0.0) {
+      const double sqrtDenom = sqrt(temp2);
+      c_fai = r.v.y / sqrtDenom;
+      s_fai = -r.v.x / sqrtDenom;
+    } else {
+      const double sqrtDenom = sqrt(temp0 * temp2);
+      c_fai = temp3 / sqrtDenom;
+      s_fai = temp4 / sqrtDenom;
+    }
+    const V Mbp = mk(-0.5 * K.kb * sita * s_fai, 0.5 * K.kb * sita * c_fai, 0.0);
+    Mbr = mulT(mat, Mbp);
+    const V Fsp = mk(-0.5 * K.ks * c_fai * sita * r_0Norm, -0.5 * K.ks * s_fai * sita * r_0Norm, 0.0);
+    Fsr = mulT(mat, Fsp);
+    const V Msp = mk(0.5 * K.ks * s_fai * sita * r_0Norm, -0.5 * K.ks * c_fai * sita * r_0Norm, 0.0);
+    Msr = mulT(mat, Msp);
+  }
+  const double eq_rad1 = r1 / (r1 + r2);
+  const double eq_rad2 = r2 / (r1 + r2);
+  o.force = mulT(mat0, Fr + Fst + Fsr);
+  o.moment1 = mulT(mat0, Mbr + Mtr + Msr * eq_rad1 * rbpNorm + Mst * eq_rad1 * rbpNorm);
+  o.moment2 = mulT(mat0, Msr * eq_rad2 * rbpNorm + Mst * eq_rad2 * rbpNorm - Mbr - Mtr);
+  o.shF = norm(Fst + Fsr);
+  o.tM = norm(Mtr);
+  o.bM = norm(Mbr);
+  const double r0 = r1 + r2;
+  const V D = x1 - x2;
+  const double dist = sqrt(dot(D, D));
+  o.nF = ((dist < r0) ? -1.0 : 1.0) * norm(Fr);
+}
+
+// CRotBondedInteraction::broken (Model/RotBondedInteraction.cpp:175-219), beta1 = beta2 = 1.
+__device__ __forceinline__ bool bond_broken(const BondK& K, const BondOut& o, double truncated) {
+  const double beta1 = 1.0, beta2 = 1.0;
+  double shearStress = o.shF / K.max_s + beta2 * o.tM / K.max_t;
+  double normalStress = o.nF / K.max_n + beta1 * o.bM / K.max_b;
+  return (normalStress > truncated) || (shearStress > (1.0 - normalStress));
+}
+
+// CElasticWallInteraction: ctor scaling (Model/EWallInteraction.hpp:26-36) and
+// calcForces (:42-78).  Returns true when in contact; F is the force on the particle.
+__device__ __forceinline__ bool law_wall(double k, const V& o, const V& n, const V& x, double r, V& F) {
+  double f = 1.0;
+  f *= 3.141592654 * r;
+  const double m_k = f * k;
+  double dist = dot(x - o, n);
+  if (dist < r) {
+    F = m_k * (r - dist) * n;
+    return true;
+  }
+  return false;
+}
+
+// CDamping<T>::calcForces (Model/Damping.hpp:99-124) with v_ref = 0: returns the damping
+// force for velocity v, accumulated force frc, inverse mass s and mass m.  The
+// rotational form (Model/RotDamping.hpp:58-84) is the same iteration on (omega,
+// moment, 1/I, I).
+__device__ __forceinline__ V damping_force(const V& v, const V& frc, double s, double mass, double visc, double dt,
+                                           int maxiter) {
+  const double s_limit2 = 1e-12;
+  const V vref = mk(0.0, 0.0, 0.0);
+  V v_rel = mk(0.0, 0.0, 0.0);
+  double error = 1.0;
+  int count = 0;
+  while ((error * error > s_limit2) & (count < maxiter)) {
+    count++;
+    V v_old = v_rel;
+    v_rel = v - vref + s * dt * (frc - v_rel * visc * mass);
+    error = norm2(v_rel - v_old);
+  }
+  if (count >= maxiter) v_rel = mk(0.0, 0.0, 0.0);
+  return -1.0 * visc * v_rel * mass;
+}
+
+}  // namespace dem

@@ -1,0 +1,1108 @@
+// Host side of one simulated worker on one GPU, and the C ABI (include/esys_dem.h).
+//
+// DemSim plays the role of TSubLattice<T> / TRotSubLattice<T>
+// (Parallel/SubLattice.hpp, Parallel/RotSubLattice.hpp) for a single worker:
+// it owns every particle and interaction in device memory and replays the
+// per-step sequence of CLatticeMaster::runOneStep
+// (Parallel/LatticeMaster.cpp:2602-2725) -- neighbour check, rebuild,
+// interaction update, force + integration -- as stream-ordered kernels.  The
+// force/integration kernel of several consecutive steps is launched without a
+// host round trip; a step that needs host work (rebuild, bond-break update)
+// raises a control flag that makes the remaining launches of the chunk
+// return at once, and the host resumes from there.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/esys_dem.h"
+#include "dem_device.cuh"
+#include "dem_kernels.h"
+
+namespace dem {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define DEM_CUDA(x)                                                                                    \
+  do {                                                                                                 \
+    cudaError_t e_ = (x);                                                                              \
+    if (e_ != cudaSuccess) throw ::dem::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+// Growable device array.
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  void reserve(size_t n, bool keep = false, cudaStream_t s = 0) {
+    if (n <= cap) return;
+    size_t nc = std::max<size_t>(n, cap + cap / 2 + 64);
+    T* q = nullptr;
+    DEM_CUDA(cudaMalloc(&q, nc * sizeof(T)));
+    if (keep && p && cap) DEM_CUDA(cudaMemcpyAsync(q, p, cap * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (p) { DEM_CUDA(cudaStreamSynchronize(s)); cudaFree(p); }
+    p = q;
+    cap = nc;
+  }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+struct Wall {
+  double o[3], n[3];
+};
+
+struct WallGroup {
+  std::string wall;
+  double k;
+};
+
+struct DynGroup {
+  int kind;  // 0 elastic, 1 rot friction
+  double k = 0, ks = 0, mu_s = 0, mu_d = 0, dt = 0;
+  int scaling = 1, meanR = 1;
+  std::vector<std::string> excl;  // excluding bond groups
+  int m = 0;                      // pairs
+  int update_ts = 0;
+  DBuf<unsigned long long> keys, keys_spare, cand;
+  DBuf<double4> hist[2], hist_spare;  // hist[c]: read by the step whose particle input buffer is c
+  DBuf<int> adj_start, adj_count, adj_cursor, p1_start;
+  DBuf<int2> adj;
+  void release() {
+    keys.release(); keys_spare.release(); cand.release();
+    hist[0].release(); hist[1].release(); hist_spare.release();
+    adj_start.release(); adj_count.release(); adj_cursor.release(); p1_start.release(); adj.release();
+  }
+};
+
+struct BondGroup {
+  int tag;
+  double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
+  int scaling, meanR;
+  int nb = 0;
+  DBuf<unsigned long long> keys;
+  DBuf<int2> ends;
+  DBuf<double4> D0;
+  DBuf<int> broken_step, adj_start, adj_count, adj_cursor, p1_start, events, nevents;
+  DBuf<int2> adj;
+  int cap_events = 0;
+  void release() {
+    keys.release(); ends.release(); D0.release(); broken_step.release(); adj_start.release(); adj_count.release();
+    adj_cursor.release(); p1_start.release(); events.release(); nevents.release(); adj.release();
+  }
+};
+
+struct DemSim {
+  std::string err;
+  int rot;
+  double dt, nrange, alpha;
+  Grid g{};
+  cudaStream_t s = nullptr;
+  int tpp = 0;           // 0 = choose from the mean adjacency length
+  int chunk = 64;        // steps launched per host round trip
+  int store_forces = 1;
+  // particles
+  int n = 0, cap = 0;
+  Particles P{};
+  std::vector<int> h_id;                 // slot -> id
+  std::unordered_map<int, int> id2slot;  // id -> slot (of particles ever added)
+  int cur = 0;
+  // cells
+  int ncell = 0;
+  DBuf<int> cell_count, cell_start, cell_cursor, cell_list, scratch_i, scratch_j, scalars;
+  // groups (std::map keeps the reference's name order)
+  std::map<std::string, Wall> walls;
+  std::map<std::string, WallGroup> wig;
+  std::map<std::string, std::vector<double>> grav;
+  std::map<std::string, DynGroup> dyn;
+  std::map<std::string, BondGroup> bond;
+  std::map<int, std::vector<int>> temp_conn;
+  int damp_lin = 0, damp_rot = 0, iter_lin = 100, iter_rot = 100;
+  double visc_lin = 0, visc_rot = 0;
+  // device control
+  DBuf<WallDev> d_walls;
+  DBuf<double> d_wall_vel, d_wall_partial, d_wall_force;
+  std::vector<double> wall_vel;  // per wall name, keyed by wig order at upload
+  std::map<std::string, std::vector<double>> wall_loader;  // wall name -> velocity
+  DBuf<unsigned> d_block_counter;
+  DBuf<long long> d_step;
+  DBuf<int> d_ctrl, d_stop;
+  int* h_ctrl = nullptr;  // pinned
+  long long t = 0;
+  int timestamp = 0, last_ns = -1;
+  bool first = true;
+  int pending_ctrl = 0;   // flags raised on the device that the host has not handled yet
+  bool own_stream = true;
+  // counters (dem_get_counters)
+  long long c_steps = 0, c_contacts = 0, c_rebuilds = 0, c_launches = 0, prof_steps = 0;
+  double prof_ms = 0.0;
+  bool profile = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  long long wall_cand = 0;               // wall-candidate interactions at the last update
+  std::map<std::string, int> bond_alive; // intact bonds per group at the last update
+  DBuf<double> stage;                    // host-state staging (dem_set_particles)
+  DBuf<int> stage_slot;
+
+  DemSim() {
+    DEM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DEM_CUDA(cudaMallocHost(&h_ctrl, 4 * sizeof(long long)));
+    d_block_counter.reserve(1); d_step.reserve(1); d_ctrl.reserve(1); d_stop.reserve(1); scalars.reserve(8);
+    DEM_CUDA(cudaMemsetAsync(d_block_counter.p, 0, sizeof(unsigned), s));
+    DEM_CUDA(cudaMemsetAsync(d_step.p, 0, sizeof(long long), s));
+    DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+    DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
+    d_wall_force.reserve(kMaxWalls * 3);
+    DEM_CUDA(cudaMemsetAsync(d_wall_force.p, 0, sizeof(double) * kMaxWalls * 3, s));
+  }
+  ~DemSim() {
+    cudaStreamSynchronize(s);
+    for (auto& d : dyn) d.second.release();
+    for (auto& b : bond) b.second.release();
+    void* ps[] = {P.buf[0].pr, P.buf[0].vm, P.buf[0].wi, P.buf[0].qq, P.buf[1].pr, P.buf[1].vm, P.buf[1].wi,
+                  P.buf[1].qq, P.inv, P.oldpos, P.force, P.moment, P.pflags, P.flagged, P.id, P.tag, P.cell};
+    for (void* p : ps) if (p) cudaFree(p);
+    cell_count.release(); cell_start.release(); cell_cursor.release(); cell_list.release();
+    scratch_i.release(); scratch_j.release(); scalars.release();
+    d_walls.release(); d_wall_vel.release(); d_wall_partial.release(); d_wall_force.release();
+    d_block_counter.release(); d_step.release(); d_ctrl.release(); d_stop.release();
+    stage.release(); stage_slot.release();
+    if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_stream) cudaStreamDestroy(s);
+  }
+
+  void sync() { DEM_CUDA(cudaStreamSynchronize(s)); }
+  int read_int(const int* d) {
+    DEM_CUDA(cudaMemcpyAsync(h_ctrl, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+    sync();
+    return h_ctrl[0];
+  }
+
+  // TSubLattice::initNeighborTable (SubLattice.hpp:455-564) + ParallelParticleArray ctor (pp_array.hpp:55-100).
+  void init_grid(const double* mn, const double* mx, const int* circ) {
+    double size[3];
+    bool circx = circ && circ[0];
+    for (int i = 0; i < 3; ++i) {
+      double sz = mx[i] - mn[i];
+      if (i == 0 && circx) {
+        if (std::fabs(sz / nrange - std::lrint(sz / nrange)) > 1e-6) nrange = sz / std::floor(sz / nrange);
+        size[i] = sz;
+      } else {
+        size[i] = nrange * std::ceil(sz / nrange);
+      }
+    }
+    double grow[3], nmin[3], nmax[3];
+    for (int i = 0; i < 3; ++i) {
+      grow[i] = size[i] - (mx[i] - mn[i]);
+      nmin[i] = mn[i] - 0.5 * grow[i];
+      nmax[i] = mx[i] + 0.5 * grow[i];
+    }
+    g.p0x = nmin[0]; g.p0y = nmin[1]; g.p0z = nmin[2];
+    g.dim = nrange;
+    g.alpha = alpha;
+    int nxg = (int)std::lrint((nmax[0] - nmin[0]) / nrange);
+    int nyg = (int)std::lrint((nmax[1] - nmin[1]) / nrange);
+    int nzg = (int)std::lrint((nmax[2] - nmin[2]) / nrange);
+    g.circx = circx;
+    if (circx) {
+      if (nxg < 3) throw std::invalid_argument("periodic x needs at least 3 cells");
+      g.gx = 0; g.nx = nxg; g.Lx = nmax[0] - nmin[0]; g.xmin = nmin[0];
+    } else {
+      g.gx = -1; g.nx = nxg + 2;
+    }
+    g.gy = -1; g.ny = nyg + 2;
+    g.gz = -1; g.nz = nzg + 2;
+    ncell = g.nx * g.ny * g.nz;
+    cell_count.reserve(ncell + 1); cell_start.reserve(ncell + 1); cell_cursor.reserve(ncell + 1);
+  }
+
+  template <class T>
+  void grow_array(T*& p, int oldn, int newcap) {
+    T* q = nullptr;
+    DEM_CUDA(cudaMalloc(&q, sizeof(T) * (size_t)newcap));
+    if (p) {
+      if (oldn) DEM_CUDA(cudaMemcpyAsync(q, p, sizeof(T) * oldn, cudaMemcpyDeviceToDevice, s));
+      sync();
+      cudaFree(p);
+    }
+    p = q;
+  }
+  void ensure_capacity(int need) {
+    if (need <= cap) return;
+    int nc = std::max(need, cap + cap / 2 + 1024);
+    for (int b = 0; b < 2; ++b) {
+      grow_array(P.buf[b].pr, n, nc); grow_array(P.buf[b].vm, n, nc);
+      grow_array(P.buf[b].wi, n, nc); grow_array(P.buf[b].qq, n, nc);
+    }
+    grow_array(P.inv, n, nc); grow_array(P.oldpos, n, nc); grow_array(P.force, n, nc); grow_array(P.moment, n, nc);
+    grow_array(P.pflags, n, nc); grow_array(P.flagged, n, nc); grow_array(P.id, n, nc); grow_array(P.tag, n, nc);
+    grow_array(P.cell, n, nc);
+    cap = nc;
+  }
+
+  int add_particles(int cnt, const int* id, const int* tag, const double* pos, const double* rad, const double* mass,
+                    const double* vel, const double* angvel, const double* quat, const int* flags) {
+    std::vector<double4> pr, vm, wi, qq;
+    std::vector<double2> inv;
+    std::vector<unsigned> pf;
+    std::vector<int> ids, tags;
+    for (int i = 0; i < cnt; ++i) {
+      // NeighborTable::insert drops particles outside the table (ntable.hpp:243-258)
+      auto cc = [&](double x, double p0, int gg) { return int(std::floor((x - p0) / g.dim)) - gg; };
+      int ix = cc(pos[3 * i], g.p0x, g.gx), iy = cc(pos[3 * i + 1], g.p0y, g.gy), iz = cc(pos[3 * i + 2], g.p0z, g.gz);
+      if (g.circx) ix = ((ix % g.nx) + g.nx) % g.nx;
+      if (!(ix >= 0 && ix < g.nx && iy >= 0 && iy < g.ny && iz >= 0 && iz < g.nz)) continue;
+      if (id2slot.count(id[i])) throw std::invalid_argument("duplicate particle id " + std::to_string(id[i]));
+      if (!(rad[i] > 0) || !(mass[i] > 0)) throw std::invalid_argument("particle radius and mass must be positive");
+      pr.push_back(make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], rad[i]));
+      vm.push_back(make_double4(vel ? vel[3 * i] : 0.0, vel ? vel[3 * i + 1] : 0.0, vel ? vel[3 * i + 2] : 0.0, mass[i]));
+      const double inert = 0.4 * mass[i] * rad[i] * rad[i];  // RotParticle.cpp:34
+      bool r_on = rot && !(flags && (flags[i] & 2));
+      wi.push_back(make_double4(angvel && rot ? angvel[3 * i] : 0.0, angvel && rot ? angvel[3 * i + 1] : 0.0,
+                                angvel && rot ? angvel[3 * i + 2] : 0.0, inert));
+      qq.push_back(quat && rot ? make_double4(quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3])
+                               : make_double4(1.0, 0.0, 0.0, 0.0));
+      inv.push_back(make_double2(mass[i] != 0.0 ? 1.0 / mass[i] : 0.0, 1.0 / inert));
+      unsigned f = PF_ALIVE;
+      if (!(flags && (flags[i] & 1))) f |= PF_DYN;
+      if (r_on) f |= PF_ROT;
+      pf.push_back(f);
+      ids.push_back(id[i]);
+      tags.push_back(tag ? tag[i] : 0);
+    }
+    const int add = (int)pr.size();
+    ensure_capacity(n + add);
+    if (add) {
+      auto up = [&](void* dst, const void* src, size_t bytes) {
+        DEM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+      };
+      up(P.buf[cur].pr + n, pr.data(), sizeof(double4) * add);
+      up(P.buf[cur].vm + n, vm.data(), sizeof(double4) * add);
+      up(P.buf[cur].wi + n, wi.data(), sizeof(double4) * add);
+      up(P.buf[cur].qq + n, qq.data(), sizeof(double4) * add);
+      up(P.inv + n, inv.data(), sizeof(double2) * add);
+      up(P.pflags + n, pf.data(), sizeof(unsigned) * add);
+      up(P.id + n, ids.data(), sizeof(int) * add);
+      up(P.tag + n, tags.data(), sizeof(int) * add);
+      DEM_CUDA(cudaMemsetAsync(P.flagged + n, 0, add, s));
+      DEM_CUDA(cudaMemsetAsync(P.force + n, 0, sizeof(double4) * add, s));
+      DEM_CUDA(cudaMemsetAsync(P.moment + n, 0, sizeof(double4) * add, s));
+      for (int i = 0; i < add; ++i) { id2slot[ids[i]] = n + i; h_id.push_back(ids[i]); }
+      n += add;
+      P.n = n;
+      sync();
+    }
+    search_neighbors();  // CLatticeMaster::addParticles ends with searchNeighbors(true) (LatticeMaster.hpp:329)
+    resize_adjacency();
+    return 0;
+  }
+
+  // Per-particle adjacency arrays are sized by the particle count: re-derive them
+  // whenever particles are added or a group is created.
+  void resize_adjacency() {
+    for (auto& d : dyn) build_adjacency(d.second.keys, d.second.m, d.second.adj_start, d.second.adj_count,
+                                        d.second.adj_cursor, d.second.p1_start, d.second.adj);
+    for (auto& b : bond) build_adjacency(b.second.keys, b.second.nb, b.second.adj_start, b.second.adj_count,
+                                         b.second.adj_cursor, b.second.p1_start, b.second.adj);
+    sync();
+  }
+
+  // Bulk state update of existing particles (rows = slots when id is NULL).
+  int set_particles(int cnt, const int* id, const double* pos, const double* vel, const double* angvel,
+                    const double* quat) {
+    if (cnt < 0 || (!id && cnt != n)) throw std::invalid_argument("without ids, rows must cover every particle slot");
+    stage.reserve((size_t)cnt * 13 + 1);
+    stage_slot.reserve(cnt + 1);
+    double* d = stage.p;
+    const size_t c3 = (size_t)cnt * 3;
+    if (pos) DEM_CUDA(cudaMemcpyAsync(d, pos, sizeof(double) * c3, cudaMemcpyHostToDevice, s));
+    if (vel) DEM_CUDA(cudaMemcpyAsync(d + c3, vel, sizeof(double) * c3, cudaMemcpyHostToDevice, s));
+    if (angvel && rot) DEM_CUDA(cudaMemcpyAsync(d + 2 * c3, angvel, sizeof(double) * c3, cudaMemcpyHostToDevice, s));
+    if (quat && rot) DEM_CUDA(cudaMemcpyAsync(d + 3 * c3, quat, sizeof(double) * 4 * cnt, cudaMemcpyHostToDevice, s));
+    const int* slots = nullptr;
+    if (id) {
+      std::vector<int> sl(cnt);
+      for (int i = 0; i < cnt; ++i) {
+        auto it = id2slot.find(id[i]);
+        if (it == id2slot.end()) throw std::invalid_argument("unknown particle id " + std::to_string(id[i]));
+        sl[i] = it->second;
+      }
+      DEM_CUDA(cudaMemcpyAsync(stage_slot.p, sl.data(), sizeof(int) * cnt, cudaMemcpyHostToDevice, s));
+      sync();
+      slots = stage_slot.p;
+    }
+    launch_set_state(P, cur, cnt, slots, pos ? d : nullptr, vel ? d + c3 : nullptr,
+                     (angvel && rot) ? d + 2 * c3 : nullptr, (quat && rot) ? d + 3 * c3 : nullptr, s);
+    // moved particles are checked like any displacement before the next step
+    launch_check_disp(P, cur, (0.5 * alpha) * (0.5 * alpha), d_ctrl.p, s);
+    pending_ctrl |= read_int(d_ctrl.p);
+    DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+    c_launches += 2;
+    return 0;
+  }
+
+  // ---- neighbour search (TSubLattice::searchNeighbors, SubLattice.hpp:2395-2408) ----
+  void search_neighbors() {
+    DEM_CUDA(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * (ncell + 1), s));
+    launch_bin(g, P, cur, cell_count.p, s);
+    launch_scan(cell_count.p, cell_start.p, ncell + 1, scalars.p, s);
+    DEM_CUDA(cudaMemsetAsync(cell_cursor.p, 0, sizeof(int) * (ncell + 1), s));
+    cell_list.reserve(std::max(n, 1));
+    launch_scatter_cells(P, cell_start.p, cell_cursor.p, cell_list.p, s);
+    launch_sort_cells(ncell, cell_start.p, cell_list.p, s);
+    for (auto& b : bond) launch_bonds_rebuild(b.second.nb, b.second.ends.p, P.pflags, b.second.broken_step.p, s);
+    timestamp++;
+    c_rebuilds++;
+    c_launches += 4 + (long long)bond.size();
+  }
+
+  ExclDev excl_of(const DynGroup& G) {
+    ExclDev ex{};
+    for (auto& nm : G.excl) {
+      auto it = bond.find(nm);
+      if (it == bond.end() || ex.n >= kMaxBond) continue;
+      ex.keys[ex.n] = it->second.keys.p;
+      ex.broken_step[ex.n] = it->second.broken_step.p;
+      ex.count[ex.n] = it->second.nb;
+      ex.n++;
+    }
+    return ex;
+  }
+
+  void build_adjacency(DBuf<unsigned long long>& keys, int m, DBuf<int>& adj_start, DBuf<int>& adj_count,
+                       DBuf<int>& adj_cursor, DBuf<int>& p1_start, DBuf<int2>& adj) {
+    adj_start.reserve(n + 2); adj_count.reserve(n + 2); adj_cursor.reserve(n + 2); p1_start.reserve(n + 2);
+    adj.reserve(std::max(2 * m, 1));
+    launch_adj(keys.p, m, n, adj_count.p, p1_start.p, adj_start.p, adj_cursor.p, adj.p, scalars.p + 1, s);
+    c_launches += 5;
+  }
+
+  // PIS_NE::update / PIS_ED::update after a rebuild: the full pair list with history carried
+  // for persistent RotFriction interactions (pi_storage_ne.hpp:49-80, pi_storage_ed.hpp:84-129).
+  void dyn_full_update(DynGroup& G) {
+    ExclDev ex = excl_of(G);
+    scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
+    launch_pairs_count(g, P, cur, cell_start.p, cell_list.p, ex, scratch_i.p, s);
+    launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, s);
+    const int m = read_int(scalars.p);
+    c_launches += 3;
+    G.keys_spare.reserve(std::max(m, 1));
+    if (G.kind == 1) G.hist_spare.reserve(std::max(m, 1));
+    launch_pairs_write(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind, G.keys.p, G.m,
+                       G.hist[cur].p, G.hist_spare.p, s);
+    std::swap(G.keys, G.keys_spare);
+    if (G.kind == 1) {
+      std::swap(G.hist[cur], G.hist_spare);
+      G.hist[cur ^ 1].reserve(std::max(m, 1));
+    }
+    G.m = m;
+    build_adjacency(G.keys, m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
+  }
+
+  // PIS_NE / PIS_ED::update without a rebuild: append the "new list" of flagged pairs
+  // (ntable.hpp:628-664; pi_storage_ne.hpp:80-98, pi_storage_ed.hpp:130-155).
+  void dyn_new_update(DynGroup& G) {
+    ExclDev ex = excl_of(G);
+    const int check_in = G.kind == 1;  // PIS_NE appends without the isIn test
+    scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
+    launch_newlist_count(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_i.p, s);
+    launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, s);
+    const int nb = read_int(scalars.p);
+    c_launches += 3;
+    if (nb > 0) {
+      c_launches += 2;
+      G.cand.reserve(nb);
+      launch_newlist_write(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_j.p, G.cand.p, s);
+      const int m2 = G.m + nb;
+      G.keys_spare.reserve(m2);
+      if (G.kind == 1) G.hist_spare.reserve(m2);
+      launch_merge(G.keys.p, G.hist[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist_spare.p, G.kind, s);
+      std::swap(G.keys, G.keys_spare);
+      if (G.kind == 1) {
+        std::swap(G.hist[cur], G.hist_spare);
+        G.hist[cur ^ 1].reserve(m2);
+      }
+      G.m = m2;
+      build_adjacency(G.keys, G.m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
+    }
+    launch_clear_flags(n, P.flagged, s);  // getNewList clears every flag (ntable.hpp:658-662)
+  }
+
+  void upload_walls() {
+    std::vector<WallDev> w;
+    std::vector<double> v;
+    for (auto& it : wig) {
+      const Wall& W = walls.at(it.second.wall);
+      w.push_back(WallDev{W.o[0], W.o[1], W.o[2], W.n[0], W.n[1], W.n[2], it.second.k});
+      auto lv = wall_loader.find(it.second.wall);
+      for (int k = 0; k < 3; ++k) v.push_back(lv == wall_loader.end() ? 0.0 : lv->second[k]);
+    }
+    d_walls.reserve(kMaxWalls);
+    d_wall_vel.reserve(kMaxWalls * 3);
+    if (!w.empty()) {
+      DEM_CUDA(cudaMemcpyAsync(d_walls.p, w.data(), sizeof(WallDev) * w.size(), cudaMemcpyHostToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_wall_vel.p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, s));
+    }
+    sync();
+  }
+  // device wall origins are authoritative once groups exist: bring them back to the host
+  void download_walls() {
+    if (wig.empty()) return;
+    std::vector<WallDev> w(wig.size());
+    DEM_CUDA(cudaMemcpyAsync(w.data(), d_walls.p, sizeof(WallDev) * w.size(), cudaMemcpyDeviceToHost, s));
+    sync();
+    int k = 0;
+    for (auto& it : wig) {
+      Wall& W = walls.at(it.second.wall);
+      W.o[0] = w[k].ox; W.o[1] = w[k].oy; W.o[2] = w[k].oz;
+      ++k;
+    }
+  }
+
+  // TSubLattice::updateInteractions (SubLattice.hpp:2416-2466)
+  void update_interactions(bool need) {
+    if (timestamp > last_ns || need) {
+      bool flags_consumed = false;
+      for (auto& d : dyn) {
+        DynGroup& G = d.second;
+        if (G.update_ts != timestamp) dyn_full_update(G);
+        else if (!flags_consumed) { dyn_new_update(G); flags_consumed = true; }
+        G.update_ts = timestamp;
+      }
+      if (!wig.empty()) {
+        DEM_CUDA(cudaMemsetAsync(scalars.p + 2, 0, sizeof(int), s));
+        launch_wall_update(g, P, cur, (int)wig.size(), d_walls.p, scalars.p + 2, s);
+        wall_cand = read_int(scalars.p + 2);
+        c_launches += 1;
+      }
+      for (auto& b : bond) {
+        int ne = read_int(b.second.nevents.p);
+        bond_alive[b.first] = b.second.nb - ne;
+      }
+      last_ns = timestamp;
+    }
+  }
+
+  // interactions evaluated per step: Verlet pairs + intact bonds + wall candidates
+  long long contacts_per_step() const {
+    long long c = wall_cand;
+    for (auto& d : dyn) c += d.second.m;
+    for (auto& b : bond) {
+      auto it = bond_alive.find(b.first);
+      c += it == bond_alive.end() ? b.second.nb : it->second;
+    }
+    return c;
+  }
+
+  StepArgs make_args(int c) {
+    StepArgs a{};
+    a.g = g;
+    a.P = P;
+    a.cur = c;
+    a.dt = dt;
+    a.half_alpha_sq = (0.5 * alpha) * (0.5 * alpha);
+    a.nwall = (int)wig.size();
+    a.walls = d_walls.p;
+    a.wall_vel = d_wall_vel.p;
+    a.ngrav = 0;
+    for (auto& gr : grav) {
+      if (a.ngrav >= kMaxGrav) break;
+      for (int k = 0; k < 3; ++k) a.grav[a.ngrav][k] = gr.second[k];
+      a.ngrav++;
+    }
+    a.ndyn = 0;
+    for (auto& d : dyn) {
+      DynGroup& G = d.second;
+      DynDev& D = a.dyn[a.ndyn++];
+      D.kind = G.kind; D.k = G.k; D.ks = G.ks; D.mu_s = G.mu_s; D.mu_d = G.mu_d; D.dt = G.dt;
+      D.scaling = G.scaling; D.meanR = G.meanR;
+      D.adj_start = G.adj_start.p; D.adj = G.adj.p;
+      D.hist_in = G.hist[c].p; D.hist_out = G.hist[c ^ 1].p;
+    }
+    a.nbond = 0;
+    for (auto& b : bond) {
+      BondGroup& B = b.second;
+      BondDev& D = a.bond[a.nbond++];
+      D.kr = B.kr; D.ks = B.ks; D.kt = B.kt; D.kb = B.kb; D.mn = B.mn; D.ms = B.ms; D.mt = B.mt; D.mb = B.mb;
+      D.truncated = B.truncated; D.scaling = B.scaling; D.meanR = B.meanR;
+      D.adj_start = B.adj_start.p; D.adj = B.adj.p; D.D0 = B.D0.p; D.broken_step = B.broken_step.p;
+      D.events = B.events.p; D.nevents = B.nevents.p; D.cap_events = B.cap_events;
+    }
+    a.damp_lin = damp_lin; a.damp_rot = damp_rot;
+    a.visc_lin = visc_lin; a.visc_rot = visc_rot; a.dt_lin = dt; a.dt_rot = dt;
+    a.iter_lin = iter_lin; a.iter_rot = iter_rot;
+    a.store_forces = store_forces;
+    a.wall_partial = d_wall_partial.p;
+    a.wall_force = d_wall_force.p;
+    a.block_counter = d_block_counter.p;
+    a.step_counter = d_step.p;
+    a.ctrl = d_ctrl.p;
+    a.stop = d_stop.p;
+    return a;
+  }
+
+  int pick_tpp() {
+    if (tpp) return tpp;
+    long long e = 0;
+    for (auto& d : dyn) e += 2LL * d.second.m;
+    for (auto& b : bond) e += 2LL * b.second.nb;
+    double mean = n ? (double)e / n : 0.0;
+    if (mean >= 12) return 8;
+    if (mean >= 6) return 4;
+    if (mean >= 2.5) return 2;
+    return 1;
+  }
+
+  // CLatticeMaster::runOneStep x nsteps (LatticeMaster.cpp:2602-2740), without savers and runnables.
+  int step(int nsteps) {
+    int done = 0;
+    while (done < nsteps) {
+      if (first) { search_neighbors(); first = false; }
+      // checkNeighbors + searchNeighbors (LatticeMaster.cpp:1864-1908)
+      if (pending_ctrl & CTRL_REBUILD) search_neighbors();
+      update_interactions((pending_ctrl & CTRL_BROKE) != 0);
+      if (pending_ctrl & CTRL_OVERFLOW) { err = "bond-break event log overflowed"; return -2; }
+      pending_ctrl = 0;
+      // launch a chunk of force + integration steps
+      const int k = std::min(chunk, nsteps - done);
+      const int t_pp = pick_tpp();
+      const int grid = step_grid(n, t_pp);
+      d_wall_partial.reserve((size_t)grid * kMaxWalls * 3);
+      DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+      DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
+      const long long t0 = t;
+      const long long cps = contacts_per_step();
+      if (profile) {
+        if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
+        DEM_CUDA(cudaEventRecord(ev0, s));
+      }
+      for (int j = 0; j < k; ++j) {
+        StepArgs a = make_args((cur + j) & 1);
+        launch_step(a, rot != 0, t_pp, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+      if (profile) DEM_CUDA(cudaEventRecord(ev1, s));
+      c_launches += k;
+      DEM_CUDA(cudaMemcpyAsync(h_ctrl, d_step.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(h_ctrl + 2, d_ctrl.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      sync();
+      long long dev_t;
+      std::memcpy(&dev_t, h_ctrl, sizeof(long long));
+      const int ran = (int)(dev_t - t0);
+      pending_ctrl = h_ctrl[2];
+      if (ran < 1 || ran > k) { err = "device step counter out of sequence"; return -3; }
+      t = dev_t;
+      cur = (cur + ran) & 1;
+      done += ran;
+      c_steps += ran;
+      c_contacts += (long long)ran * cps;
+      if (profile) {
+        float ms = 0.f;
+        DEM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        prof_ms += ms;
+        prof_steps += ran;
+      }
+    }
+    return 0;
+  }
+};
+
+}  // namespace dem
+
+using dem::DemSim;
+
+namespace {
+template <class F>
+int guard(dem_sim* h, F&& f) {
+  DemSim* s = reinterpret_cast<DemSim*>(h);
+  try {
+    return f(*s);
+  } catch (const dem::CudaError& e) {
+    s->err = e.what();
+    return DEM_ERR_CUDA;
+  } catch (const std::invalid_argument& e) {
+    s->err = e.what();
+    return DEM_ERR_ARG;
+  } catch (const std::exception& e) {
+    s->err = e.what();
+    return DEM_ERR_INTERNAL;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int dem_create(dem_sim** out, int particle_type, double grid_spacing, double verlet_dist, const double* bbox_min,
+               const double* bbox_max, const int* circ, double dt) {
+  if (!out) return DEM_ERR_ARG;
+  *out = nullptr;
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return DEM_ERR_CUDA;
+  if (!(grid_spacing > 0) || !(verlet_dist >= 0) || !(dt > 0) || !bbox_min || !bbox_max) return DEM_ERR_ARG;
+  DemSim* s = nullptr;
+  try {
+    s = new DemSim();
+    s->rot = particle_type ? 1 : 0;
+    s->dt = dt; s->nrange = grid_spacing; s->alpha = verlet_dist;
+    s->init_grid(bbox_min, bbox_max, circ);
+  } catch (const std::exception&) {
+    delete s;
+    return DEM_ERR_ARG;
+  }
+  *out = reinterpret_cast<dem_sim*>(s);
+  return DEM_OK;
+}
+
+int dem_destroy(dem_sim* h) {
+  delete reinterpret_cast<DemSim*>(h);
+  return DEM_OK;
+}
+
+const char* dem_last_error(dem_sim* h) { return h ? reinterpret_cast<DemSim*>(h)->err.c_str() : "null handle"; }
+
+int dem_add_particles(dem_sim* h, int n, const int* id, const int* tag, const double* pos, const double* rad,
+                      const double* mass, const double* vel, const double* angvel, const double* quat,
+                      const int* flags) {
+  return guard(h, [&](DemSim& s) {
+    if (n < 0 || (n && (!id || !pos || !rad || !mass))) throw std::invalid_argument("bad particle arrays");
+    return s.add_particles(n, id, tag, pos, rad, mass, vel, angvel, quat, flags);
+  });
+}
+
+int dem_add_connections(dem_sim* h, int n, const int* tag, const int* id1, const int* id2) {
+  return guard(h, [&](DemSim& s) {
+    for (int i = 0; i < n; ++i) { s.temp_conn[tag[i]].push_back(id1[i]); s.temp_conn[tag[i]].push_back(id2[i]); }
+    s.search_neighbors();  // LatticeMaster.hpp:397
+    return DEM_OK;
+  });
+}
+
+int dem_add_wall(dem_sim* h, const char* name, const double* o, const double* nrm) {
+  return guard(h, [&](DemSim& s) {
+    s.download_walls();
+    dem::Wall w;
+    for (int k = 0; k < 3; ++k) { w.o[k] = o[k]; w.n[k] = nrm[k]; }
+    s.walls[name] = w;
+    s.upload_walls();
+    return DEM_OK;
+  });
+}
+
+int dem_add_elastic_group(dem_sim* h, const char* name, double k, int scaling) {
+  return guard(h, [&](DemSim& s) {
+    if ((int)s.dyn.size() >= dem::kMaxDyn) throw std::invalid_argument("too many dynamic interaction groups");
+    dem::DynGroup& G = s.dyn[name];
+    G.kind = 0; G.k = k; G.scaling = scaling != 0;
+    s.resize_adjacency();
+    return DEM_OK;
+  });
+}
+
+int dem_add_rot_friction_group(dem_sim* h, const char* name, double k, double mu_s, double mu_d, double ks, double dt,
+                               int scaling, int meanR) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.rot) throw std::invalid_argument("RotFriction needs RotSphere particles");
+    if ((int)s.dyn.size() >= dem::kMaxDyn) throw std::invalid_argument("too many dynamic interaction groups");
+    dem::DynGroup& G = s.dyn[name];
+    G.kind = 1; G.k = k; G.mu_s = mu_s; G.mu_d = mu_d; G.ks = ks; G.dt = dt; G.scaling = scaling != 0;
+    G.meanR = meanR != 0;
+    s.resize_adjacency();
+    return DEM_OK;
+  });
+}
+
+// TRotSubLattice::addRotBondedIG (RotSubLattice.hpp:116-186) with PIS_E::tryInsert (pi_storage_e.hpp:222-263).
+int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                           double mn, double ms, double mt, double mb, int scaling, int meanR, double truncated) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.rot) throw std::invalid_argument("RotBond needs RotSphere particles");
+    if ((int)s.bond.size() >= dem::kMaxBond) throw std::invalid_argument("too many bonded interaction groups");
+    std::vector<unsigned> pf(s.n);
+    if (s.n) {
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), s.P.pflags, sizeof(unsigned) * s.n, cudaMemcpyDeviceToHost, s.s));
+      s.sync();
+    }
+    std::set<std::pair<int, int>> seen;
+    std::vector<unsigned long long> keys;
+    const std::vector<int>& c = s.temp_conn[tag];
+    for (size_t i = 0; i + 1 < c.size(); i += 2) {
+      int a = std::min(c[i], c[i + 1]), b = std::max(c[i], c[i + 1]);
+      if (!seen.insert({a, b}).second) continue;
+      auto ia = s.id2slot.find(a), ib = s.id2slot.find(b);
+      if (ia == s.id2slot.end() || ib == s.id2slot.end()) continue;
+      if (!(pf[ia->second] & dem::PF_ALIVE) || !(pf[ib->second] & dem::PF_ALIVE)) continue;
+      keys.push_back(((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second);
+    }
+    std::sort(keys.begin(), keys.end());
+    dem::BondGroup& B = s.bond[name];
+    B.tag = tag; B.kr = kr; B.ks = ks; B.kt = kt; B.kb = kb; B.mn = mn; B.ms = ms; B.mt = mt; B.mb = mb;
+    B.scaling = scaling != 0; B.meanR = meanR != 0; B.truncated = truncated;
+    B.nb = (int)keys.size();
+    const int nb = std::max(B.nb, 1);
+    B.keys.reserve(nb); B.ends.reserve(nb); B.D0.reserve(nb); B.broken_step.reserve(nb);
+    B.cap_events = std::max(1024, B.nb);
+    B.events.reserve(3 * B.cap_events); B.nevents.reserve(1);
+    std::vector<int2> ends(B.nb);
+    for (int i = 0; i < B.nb; ++i) ends[i] = make_int2((int)(keys[i] >> 32), (int)(keys[i] & 0xffffffffu));
+    std::vector<int> alive(B.nb, dem::kBondAlive);
+    if (B.nb) {
+      DEM_CUDA(cudaMemcpyAsync(B.keys.p, keys.data(), sizeof(unsigned long long) * B.nb, cudaMemcpyHostToDevice, s.s));
+      DEM_CUDA(cudaMemcpyAsync(B.ends.p, ends.data(), sizeof(int2) * B.nb, cudaMemcpyHostToDevice, s.s));
+      DEM_CUDA(cudaMemcpyAsync(B.broken_step.p, alive.data(), sizeof(int) * B.nb, cudaMemcpyHostToDevice, s.s));
+    }
+    DEM_CUDA(cudaMemsetAsync(B.nevents.p, 0, sizeof(int), s.s));
+    dem::launch_bonds_init(B.nb, B.ends.p, s.P.buf[s.cur].pr, B.D0.p, s.s);
+    s.build_adjacency(B.keys, B.nb, B.adj_start, B.adj_count, B.adj_cursor, B.p1_start, B.adj);
+    s.sync();
+    return DEM_OK;
+  });
+}
+
+int dem_add_wall_group(dem_sim* h, const char* name, const char* wall, double k) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.walls.count(wall)) throw std::invalid_argument(std::string("wall name '") + wall + "' not found in map of walls");
+    if (!s.wig.count(name) && (int)s.wig.size() >= dem::kMaxWalls) throw std::invalid_argument("too many wall groups");
+    s.download_walls();
+    s.wig[name] = dem::WallGroup{wall, k};
+    s.upload_walls();
+    DEM_CUDA(cudaMemsetAsync(s.scalars.p + 2, 0, sizeof(int), s.s));
+    dem::launch_wall_update(s.g, s.P, s.cur, (int)s.wig.size(), s.d_walls.p, s.scalars.p + 2, s.s);  // CEWallInteractionGroup::Update
+    s.wall_cand = s.read_int(s.scalars.p + 2);
+    s.sync();
+    return DEM_OK;
+  });
+}
+
+int dem_add_gravity(dem_sim* h, const char* name, const double* gv) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.grav.count(name) && (int)s.grav.size() >= dem::kMaxGrav) throw std::invalid_argument("too many body forces");
+    s.grav[name] = {gv[0], gv[1], gv[2]};
+    return DEM_OK;
+  });
+}
+
+int dem_add_damping(dem_sim* h, int rot, double visc, int max_iter) {
+  return guard(h, [&](DemSim& s) {
+    if (rot) {
+      if (!s.rot) throw std::invalid_argument("RotDamping needs RotSphere particles");
+      s.damp_rot = 1; s.visc_rot = visc; s.iter_rot = max_iter;
+    } else {
+      s.damp_lin = 1; s.visc_lin = visc; s.iter_lin = max_iter;
+    }
+    return DEM_OK;
+  });
+}
+
+// TSubLattice::setExIG (SubLattice.hpp:1980-2009) + PIS_ED::addExIG (pi_storage_ed.hpp:20-40).
+int dem_add_exclusion(dem_sim* h, const char* bonded, const char* dynamic) {
+  return guard(h, [&](DemSim& s) {
+    auto dy = s.dyn.find(dynamic);
+    if (dy == s.dyn.end() || !s.bond.count(bonded))
+      throw std::invalid_argument("nonexisting interaction group");
+    dem::DynGroup& G = dy->second;
+    G.excl.push_back(bonded);
+    if (G.m > 0) {  // clean out pairs that are now excluded, keeping the others' history
+      dem::BondGroup& B = s.bond[bonded];
+      std::vector<unsigned long long> keys(G.m), bk(B.nb);
+      std::vector<double4> hist(G.kind == 1 ? G.m : 0);
+      std::vector<int> bs(B.nb);
+      DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
+      if (G.kind == 1) DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
+      if (B.nb) {
+        DEM_CUDA(cudaMemcpyAsync(bk.data(), B.keys.p, sizeof(unsigned long long) * B.nb, cudaMemcpyDeviceToHost, s.s));
+        DEM_CUDA(cudaMemcpyAsync(bs.data(), B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToHost, s.s));
+      }
+      s.sync();
+      std::vector<unsigned long long> k2;
+      std::vector<double4> h2;
+      for (int i = 0; i < G.m; ++i) {
+        auto p = std::lower_bound(bk.begin(), bk.end(), keys[i]);
+        bool ex = p != bk.end() && *p == keys[i] && bs[p - bk.begin()] == dem::kBondAlive;
+        if (!ex) { k2.push_back(keys[i]); if (G.kind == 1) h2.push_back(hist[i]); }
+      }
+      G.m = (int)k2.size();
+      if (G.m) {
+        DEM_CUDA(cudaMemcpyAsync(G.keys.p, k2.data(), sizeof(unsigned long long) * G.m, cudaMemcpyHostToDevice, s.s));
+        if (G.kind == 1) DEM_CUDA(cudaMemcpyAsync(G.hist[s.cur].p, h2.data(), sizeof(double4) * G.m, cudaMemcpyHostToDevice, s.s));
+      }
+      s.build_adjacency(G.keys, G.m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
+      s.sync();
+    }
+    return DEM_OK;
+  });
+}
+
+int dem_set_timestep(dem_sim* h, double dt) {
+  return guard(h, [&](DemSim& s) {
+    if (!(dt > 0)) throw std::invalid_argument("time step must be positive");
+    s.dt = dt;  // TSubLattice::setTimeStepSize (SubLattice.hpp:2163-2204) propagates to the groups
+    for (auto& d : s.dyn) d.second.dt = dt;
+    return DEM_OK;
+  });
+}
+
+int dem_step(dem_sim* h, int nsteps) {
+  return guard(h, [&](DemSim& s) {
+    if (nsteps < 0) throw std::invalid_argument("negative step count");
+    return s.step(nsteps);
+  });
+}
+
+int dem_move_wall(dem_sim* h, const char* name, const double* d) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.walls.count(name)) throw std::invalid_argument("no such wall");
+    s.download_walls();
+    dem::Wall& W = s.walls[name];
+    for (int k = 0; k < 3; ++k) W.o[k] += d[k];  // CWall::moveBy (Model/Wall.h:53-60)
+    s.upload_walls();
+    return DEM_OK;
+  });
+}
+
+int dem_set_wall_velocity(dem_sim* h, const char* name, const double* v) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.walls.count(name)) throw std::invalid_argument("no such wall");
+    s.download_walls();
+    s.wall_loader[name] = {v[0], v[1], v[2]};
+    s.upload_walls();
+    return DEM_OK;
+  });
+}
+
+int dem_apply_force_to_wall(dem_sim* h, const char* group, const double* f) {
+  return guard(h, [&](DemSim& s) {
+    auto it = s.wig.find(group);
+    if (it == s.wig.end()) throw std::invalid_argument("no such wall group");
+    int w = (int)std::distance(s.wig.begin(), it);
+    dem::launch_wall_servo(s.P, s.cur, w, s.d_walls.p, f, s.s);
+    s.sync();
+    // the servo moves the group's copy of the wall: propagate to groups sharing the wall
+    std::vector<dem::WallDev> wd(s.wig.size());
+    DEM_CUDA(cudaMemcpyAsync(wd.data(), s.d_walls.p, sizeof(dem::WallDev) * wd.size(), cudaMemcpyDeviceToHost, s.s));
+    s.sync();
+    dem::Wall& W = s.walls.at(it->second.wall);
+    W.o[0] = wd[w].ox; W.o[1] = wd[w].oy; W.o[2] = wd[w].oz;
+    s.upload_walls();
+    return DEM_OK;
+  });
+}
+
+int dem_get_wall(dem_sim* h, const char* name, double* pos, double* force) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.walls.count(name)) throw std::invalid_argument("no such wall");
+    s.download_walls();
+    double wf[dem::kMaxWalls * 3];
+    DEM_CUDA(cudaMemcpyAsync(wf, s.d_wall_force.p, sizeof(wf), cudaMemcpyDeviceToHost, s.s));
+    s.sync();
+    double F[3] = {0, 0, 0};
+    int k = 0;
+    for (auto& it : s.wig) {
+      if (it.second.wall == name) for (int c = 0; c < 3; ++c) F[c] += wf[3 * k + c];
+      ++k;
+    }
+    for (int c = 0; c < 3; ++c) { if (pos) pos[c] = s.walls[name].o[c]; if (force) force[c] = F[c]; }
+    return DEM_OK;
+  });
+}
+
+int dem_num_particles(dem_sim* h) {
+  return guard(h, [&](DemSim& s) {
+    std::vector<unsigned> pf(s.n);
+    if (s.n) DEM_CUDA(cudaMemcpyAsync(pf.data(), s.P.pflags, sizeof(unsigned) * s.n, cudaMemcpyDeviceToHost, s.s));
+    s.sync();
+    int c = 0;
+    for (unsigned f : pf) c += (f & dem::PF_ALIVE) ? 1 : 0;
+    return c;
+  });
+}
+
+int dem_get_particles(dem_sim* h, int* id, double* pos, double* vel, double* angvel, double* quat, double* force,
+                      double* moment) {
+  return guard(h, [&](DemSim& s) {
+    const int n = s.n;
+    std::vector<double4> pr(n), vm(n), wi(n), qq(n), f(n), m(n);
+    std::vector<unsigned> pf(n);
+    if (n) {
+      auto dn = [&](void* dst, const void* src, size_t b) { DEM_CUDA(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s.s)); };
+      dn(pr.data(), s.P.buf[s.cur].pr, sizeof(double4) * n);
+      dn(vm.data(), s.P.buf[s.cur].vm, sizeof(double4) * n);
+      dn(wi.data(), s.P.buf[s.cur].wi, sizeof(double4) * n);
+      dn(qq.data(), s.P.buf[s.cur].qq, sizeof(double4) * n);
+      dn(f.data(), s.P.force, sizeof(double4) * n);
+      dn(m.data(), s.P.moment, sizeof(double4) * n);
+      dn(pf.data(), s.P.pflags, sizeof(unsigned) * n);
+    }
+    s.sync();
+    int k = 0;
+    for (int i = 0; i < n; ++i) {
+      if (!(pf[i] & dem::PF_ALIVE)) continue;
+      if (id) id[k] = s.h_id[i];
+      const double4* src[5] = {&pr[i], &vm[i], &wi[i], &f[i], &m[i]};
+      double* dst[5] = {pos, vel, angvel, force, moment};
+      for (int a = 0; a < 5; ++a)
+        if (dst[a]) {
+          double v3[3] = {src[a]->x, src[a]->y, src[a]->z};
+          if ((a == 2 || a == 4) && !s.rot) v3[0] = v3[1] = v3[2] = 0.0;
+          for (int c = 0; c < 3; ++c) dst[a][3 * k + c] = v3[c];
+        }
+      if (quat) {
+        if (s.rot) { quat[4 * k] = qq[i].x; quat[4 * k + 1] = qq[i].y; quat[4 * k + 2] = qq[i].z; quat[4 * k + 3] = qq[i].w; }
+        else { quat[4 * k] = 1.0; quat[4 * k + 1] = quat[4 * k + 2] = quat[4 * k + 3] = 0.0; }
+      }
+      ++k;
+    }
+    return k;
+  });
+}
+
+int dem_num_pairs(dem_sim* h, const char* group) {
+  return guard(h, [&](DemSim& s) {
+    auto d = s.dyn.find(group);
+    if (d != s.dyn.end()) return d->second.m;
+    auto b = s.bond.find(group);
+    if (b == s.bond.end()) throw std::invalid_argument("no such group");
+    std::vector<int> bs(b->second.nb);
+    if (b->second.nb) DEM_CUDA(cudaMemcpyAsync(bs.data(), b->second.broken_step.p, sizeof(int) * bs.size(), cudaMemcpyDeviceToHost, s.s));
+    s.sync();
+    int c = 0;
+    for (int v : bs) c += v > s.t ? 1 : 0;
+    return c;
+  });
+}
+
+int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* state) {
+  return guard(h, [&](DemSim& s) {
+    auto d = s.dyn.find(group);
+    if (d != s.dyn.end()) {
+      dem::DynGroup& G = d->second;
+      std::vector<unsigned long long> keys(G.m);
+      std::vector<double4> hist(G.kind == 1 ? G.m : 0);
+      if (G.m) DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
+      if (G.kind == 1 && G.m) DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
+      s.sync();
+      for (int i = 0; i < G.m; ++i) {
+        id1[i] = s.h_id[(int)(keys[i] >> 32)];
+        id2[i] = s.h_id[(int)(keys[i] & 0xffffffffu)];
+        if (state) {
+          for (int c = 0; c < 5; ++c) state[5 * i + c] = 0.0;
+          if (G.kind == 1) {
+            const int fl = (int)hist[i].w;
+            const bool touching = (fl & 2) != 0;
+            if (touching) { state[5 * i] = hist[i].x; state[5 * i + 1] = hist[i].y; state[5 * i + 2] = hist[i].z; }
+            state[5 * i + 3] = (fl & 1) ? 1.0 : 0.0;
+            state[5 * i + 4] = touching ? 1.0 : 0.0;
+          }
+        }
+      }
+      return G.m;
+    }
+    auto b = s.bond.find(group);
+    if (b == s.bond.end()) throw std::invalid_argument("no such group");
+    dem::BondGroup& B = b->second;
+    std::vector<int2> ends(B.nb);
+    std::vector<int> bs(B.nb);
+    if (B.nb) {
+      DEM_CUDA(cudaMemcpyAsync(ends.data(), B.ends.p, sizeof(int2) * B.nb, cudaMemcpyDeviceToHost, s.s));
+      DEM_CUDA(cudaMemcpyAsync(bs.data(), B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToHost, s.s));
+    }
+    s.sync();
+    int k = 0;
+    for (int i = 0; i < B.nb; ++i) {
+      if (bs[i] <= s.t) continue;
+      id1[k] = s.h_id[ends[i].x];
+      id2[k] = s.h_id[ends[i].y];
+      if (state) for (int c = 0; c < 5; ++c) state[5 * k + c] = 0.0;
+      ++k;
+    }
+    return k;
+  });
+}
+
+int dem_num_breaks(dem_sim* h) {
+  return guard(h, [&](DemSim& s) {
+    int tot = 0;
+    for (auto& b : s.bond) tot += std::min(s.read_int(b.second.nevents.p), b.second.cap_events);
+    return tot;
+  });
+}
+
+int dem_get_breaks(dem_sim* h, int* id1, int* id2, int* step) {
+  return guard(h, [&](DemSim& s) {
+    int k = 0;
+    for (auto& b : s.bond) {
+      int ne = std::min(s.read_int(b.second.nevents.p), b.second.cap_events);
+      std::vector<int> ev(3 * (size_t)ne);
+      if (ne) DEM_CUDA(cudaMemcpyAsync(ev.data(), b.second.events.p, sizeof(int) * ev.size(), cudaMemcpyDeviceToHost, s.s));
+      s.sync();
+      for (int i = 0; i < ne; ++i) { id1[k] = ev[3 * i]; id2[k] = ev[3 * i + 1]; step[k] = ev[3 * i + 2]; ++k; }
+    }
+    return k;
+  });
+}
+
+int dem_move_tagged(dem_sim* h, int tag, int mask, const double* d) {
+  (void)mask;
+  return guard(h, [&](DemSim& s) {
+    dem::launch_move_tagged(s.P, s.cur, tag, d, s.s);
+    // a host-side move is checked like any displacement (checkNeighbors runs after pre-runnables)
+    dem::launch_check_disp(s.P, s.cur, (0.5 * s.alpha) * (0.5 * s.alpha), s.d_ctrl.p, s.s);
+    s.pending_ctrl |= s.read_int(s.d_ctrl.p);
+    return DEM_OK;
+  });
+}
+
+long long dem_timestep(dem_sim* h) { return h ? reinterpret_cast<DemSim*>(h)->t : -1; }
+
+int dem_set_stream(dem_sim* h, void* stream) {
+  return guard(h, [&](DemSim& s) {
+    s.sync();
+    if (s.own_stream) DEM_CUDA(cudaStreamDestroy(s.s));
+    s.s = reinterpret_cast<cudaStream_t>(stream);
+    s.own_stream = false;
+    return DEM_OK;
+  });
+}
+
+int dem_get_counters(dem_sim* h, long long* out, int n) {
+  return guard(h, [&](DemSim& s) {
+    long long v[8] = {s.c_steps, s.c_contacts, s.c_rebuilds, s.c_launches,
+                      (long long)(s.prof_ms * 1e6), s.prof_steps, s.contacts_per_step(), (long long)s.pick_tpp()};
+    for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
+    return std::min(n, 8);
+  });
+}
+
+int dem_set_particles(dem_sim* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
+                      const double* quat) {
+  return guard(h, [&](DemSim& s) { return s.set_particles(n, id, pos, vel, angvel, quat); });
+}
+
+int dem_set_option(dem_sim* h, const char* key, double value) {
+  return guard(h, [&](DemSim& s) {
+    std::string k = key ? key : "";
+    if (k == "threads_per_particle") {
+      int v = (int)value;
+      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8) throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8");
+      s.tpp = v;
+    } else if (k == "chunk") {
+      if (value < 1) throw std::invalid_argument("chunk must be >= 1");
+      s.chunk = (int)value;
+    } else if (k == "store_forces") {
+      s.store_forces = value != 0;
+    } else if (k == "profile") {
+      s.profile = value != 0;
+    } else {
+      throw std::invalid_argument("unknown option " + k);
+    }
+    return DEM_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,259 @@
+"""ctypes binding of the B200 DEM library's C ABI (include/esys_dem.h).
+
+``DemSim`` is a thin, one-to-one wrapper of the ``dem_*`` functions: one handle
+is one ESyS-Particle worker sub-lattice on one GPU.  The library must have been
+built (``python esys-particle_b200/build.py``); there is no CPU fallback and
+loading fails loudly when the shared object or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libesys_dem_b200.so"))
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_P = C.c_void_p
+_S = C.c_char_p
+
+# name -> (restype, argtypes); every symbol declared in include/esys_dem.h
+SIGNATURES = {
+    "dem_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_double, C.c_double, _D, _D, _I, C.c_double]),
+    "dem_destroy": (C.c_int, [_P]),
+    "dem_last_error": (_S, [_P]),
+    "dem_add_particles": (C.c_int, [_P, C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _I]),
+    "dem_add_connections": (C.c_int, [_P, C.c_int, _I, _I, _I]),
+    "dem_add_wall": (C.c_int, [_P, _S, _D, _D]),
+    "dem_add_elastic_group": (C.c_int, [_P, _S, C.c_double, C.c_int]),
+    "dem_add_rot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 5 + [C.c_int, C.c_int]),
+    "dem_add_rot_bond_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 8 + [C.c_int, C.c_int, C.c_double]),
+    "dem_add_wall_group": (C.c_int, [_P, _S, _S, C.c_double]),
+    "dem_add_gravity": (C.c_int, [_P, _S, _D]),
+    "dem_add_damping": (C.c_int, [_P, C.c_int, C.c_double, C.c_int]),
+    "dem_add_exclusion": (C.c_int, [_P, _S, _S]),
+    "dem_set_timestep": (C.c_int, [_P, C.c_double]),
+    "dem_step": (C.c_int, [_P, C.c_int]),
+    "dem_move_wall": (C.c_int, [_P, _S, _D]),
+    "dem_set_wall_velocity": (C.c_int, [_P, _S, _D]),
+    "dem_apply_force_to_wall": (C.c_int, [_P, _S, _D]),
+    "dem_get_wall": (C.c_int, [_P, _S, _D, _D]),
+    "dem_num_particles": (C.c_int, [_P]),
+    "dem_get_particles": (C.c_int, [_P, _I, _D, _D, _D, _D, _D, _D]),
+    "dem_num_pairs": (C.c_int, [_P, _S]),
+    "dem_get_pairs": (C.c_int, [_P, _S, _I, _I, _D]),
+    "dem_num_breaks": (C.c_int, [_P]),
+    "dem_get_breaks": (C.c_int, [_P, _I, _I, _I]),
+    "dem_move_tagged": (C.c_int, [_P, C.c_int, C.c_int, _D]),
+    "dem_timestep": (C.c_longlong, [_P]),
+    "dem_set_option": (C.c_int, [_P, _S, C.c_double]),
+    "dem_set_particles": (C.c_int, [_P, C.c_int, _I, _D, _D, _D, _D]),
+    "dem_set_stream": (C.c_int, [_P, C.c_void_p]),
+    "dem_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the DEM library and bind every C-ABI symbol; raise if anything is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"B200 DEM library not built: {path} (run esys-particle_b200/build.py)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)  # AttributeError if the symbol is missing
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_I)
+
+
+def _v3(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(3))
+
+
+class DemError(RuntimeError):
+    pass
+
+
+class DemSim:
+    """One worker sub-lattice on the GPU (a ``dem_sim`` handle)."""
+
+    def __init__(self, particle_type, grid_spacing, verlet_dist, bbox_min, bbox_max, circ=(0, 0, 0), dt=1e-4):
+        self.lib = load_library()
+        self.h = _P()
+        mn, mx = _v3(bbox_min), _v3(bbox_max)
+        cc = np.ascontiguousarray(np.asarray(circ, dtype=np.int32))
+        pt = {"NRotSphere": 0, "RotSphere": 1}[particle_type] if isinstance(particle_type, str) else int(particle_type)
+        rc = self.lib.dem_create(C.byref(self.h), pt, float(grid_spacing), float(verlet_dist), _dp(mn), _dp(mx),
+                                 _ip(cc), float(dt))
+        if rc != 0:
+            raise DemError(f"dem_create failed ({rc}): no usable GPU or invalid domain")
+        self.rot = pt == 1
+
+    def _chk(self, rc):
+        if rc < 0:
+            raise DemError(self.lib.dem_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dem_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_particles(self, id, pos, rad, mass, tag=None, vel=None, angvel=None, quat=None, flags=None):
+        a = lambda x, dt: None if x is None else np.ascontiguousarray(np.asarray(x, dtype=dt))
+        id, tag, flags = a(id, np.int32), a(tag, np.int32), a(flags, np.int32)
+        pos, rad, mass = a(pos, np.float64), a(rad, np.float64), a(mass, np.float64)
+        vel, angvel, quat = a(vel, np.float64), a(angvel, np.float64), a(quat, np.float64)
+        self._chk(self.lib.dem_add_particles(self.h, len(id), _ip(id), _ip(tag), _dp(pos), _dp(rad), _dp(mass),
+                                             _dp(vel), _dp(angvel), _dp(quat), _ip(flags)))
+
+    def add_connections(self, tag, id1, id2):
+        t = np.ascontiguousarray(tag, dtype=np.int32)
+        a = np.ascontiguousarray(id1, dtype=np.int32)
+        b = np.ascontiguousarray(id2, dtype=np.int32)
+        self._chk(self.lib.dem_add_connections(self.h, len(a), _ip(t), _ip(a), _ip(b)))
+
+    def add_wall(self, name, origin, normal):
+        self._chk(self.lib.dem_add_wall(self.h, name.encode(), _dp(_v3(origin)), _dp(_v3(normal))))
+
+    def add_elastic_group(self, name, k, scaling=True):
+        self._chk(self.lib.dem_add_elastic_group(self.h, name.encode(), float(k), int(scaling)))
+
+    def add_rot_friction_group(self, name, k, mu_s, mu_d, k_s, dt, scaling=True, meanR_scaling=True):
+        self._chk(self.lib.dem_add_rot_friction_group(self.h, name.encode(), float(k), float(mu_s), float(mu_d),
+                                                      float(k_s), float(dt), int(scaling), int(meanR_scaling)))
+
+    def add_rot_bond_group(self, name, tag, kr, ks, kt, kb, max_n, max_s, max_t, max_b, scaling=True,
+                           meanR_scaling=True, truncated=1.0):
+        self._chk(self.lib.dem_add_rot_bond_group(self.h, name.encode(), int(tag), float(kr), float(ks), float(kt),
+                                                  float(kb), float(max_n), float(max_s), float(max_t), float(max_b),
+                                                  int(scaling), int(meanR_scaling), float(truncated)))
+
+    def add_wall_group(self, name, wall, k):
+        self._chk(self.lib.dem_add_wall_group(self.h, name.encode(), wall.encode(), float(k)))
+
+    def add_gravity(self, name, g):
+        self._chk(self.lib.dem_add_gravity(self.h, name.encode(), _dp(_v3(g))))
+
+    def add_damping(self, rot, visc, max_iter=100):
+        self._chk(self.lib.dem_add_damping(self.h, int(rot), float(visc), int(max_iter)))
+
+    def add_exclusion(self, bonded, dynamic):
+        self._chk(self.lib.dem_add_exclusion(self.h, bonded.encode(), dynamic.encode()))
+
+    def set_timestep(self, dt):
+        self._chk(self.lib.dem_set_timestep(self.h, float(dt)))
+
+    def step(self, n=1):
+        self._chk(self.lib.dem_step(self.h, int(n)))
+
+    def move_wall(self, name, d):
+        self._chk(self.lib.dem_move_wall(self.h, name.encode(), _dp(_v3(d))))
+
+    def set_wall_velocity(self, name, v):
+        self._chk(self.lib.dem_set_wall_velocity(self.h, name.encode(), _dp(_v3(v))))
+
+    def apply_force_to_wall(self, group, force):
+        self._chk(self.lib.dem_apply_force_to_wall(self.h, group.encode(), _dp(_v3(force))))
+
+    def move_tagged(self, tag, d, mask=-1):
+        self._chk(self.lib.dem_move_tagged(self.h, int(tag), int(mask), _dp(_v3(d))))
+
+    def set_option(self, key, value):
+        self._chk(self.lib.dem_set_option(self.h, key.encode(), float(value)))
+
+    def set_particles(self, pos=None, vel=None, angvel=None, quat=None, id=None, n=None):
+        """Bulk state update.  Arrays may be numpy arrays or raw host pointers (int) of
+        n rows; with id=None row i is particle slot i."""
+        def ptr(x, t):
+            if x is None:
+                return None
+            if isinstance(x, int):
+                return C.cast(C.c_void_p(x), t)
+            return np.ascontiguousarray(x).ctypes.data_as(t)
+        keep = [np.ascontiguousarray(x) for x in (pos, vel, angvel, quat, id) if x is not None and not isinstance(x, int)]
+        if n is None:
+            n = len(keep[0]) if keep else 0
+        self._chk(self.lib.dem_set_particles(self.h, int(n), ptr(id, _I), ptr(pos, _D), ptr(vel, _D),
+                                             ptr(angvel, _D), ptr(quat, _D)))
+        del keep
+
+    def set_stream(self, stream_handle: int):
+        self._chk(self.lib.dem_set_stream(self.h, C.c_void_p(int(stream_handle))))
+
+    def counters(self):
+        out = (C.c_longlong * 8)()
+        self._chk(self.lib.dem_get_counters(self.h, out, 8))
+        keys = ("steps", "contact_updates", "rebuilds", "launches", "step_kernel_ns", "profiled_steps",
+                "contacts_per_step", "threads_per_particle")
+        return dict(zip(keys, list(out)))
+
+    def get_particles_raw(self, id_ptr, pos_ptr, vel_ptr, angvel_ptr, quat_ptr, force_ptr, moment_ptr):
+        """dem_get_particles into caller-owned host buffers given as raw pointers (0 = skip)."""
+        cv = lambda p, t: None if not p else C.cast(C.c_void_p(p), t)
+        return self._chk(self.lib.dem_get_particles(self.h, cv(id_ptr, _I), cv(pos_ptr, _D), cv(vel_ptr, _D),
+                                                    cv(angvel_ptr, _D), cv(quat_ptr, _D), cv(force_ptr, _D),
+                                                    cv(moment_ptr, _D)))
+
+    def wall(self, name):
+        p, f = np.zeros(3), np.zeros(3)
+        self._chk(self.lib.dem_get_wall(self.h, name.encode(), _dp(p), _dp(f)))
+        return p, f
+
+    def num_particles(self):
+        return self._chk(self.lib.dem_num_particles(self.h))
+
+    def particles(self, sort=True):
+        n = self.num_particles()
+        out = {"id": np.zeros(n, np.int32)}
+        for k, w in (("pos", 3), ("vel", 3), ("angvel", 3), ("quat", 4), ("force", 3), ("moment", 3)):
+            out[k] = np.zeros((n, w))
+        self._chk(self.lib.dem_get_particles(self.h, _ip(out["id"]), _dp(out["pos"]), _dp(out["vel"]),
+                                             _dp(out["angvel"]), _dp(out["quat"]), _dp(out["force"]),
+                                             _dp(out["moment"])))
+        if not sort:
+            return out
+        order = np.argsort(out["id"], kind="stable")
+        return {k: v[order] for k, v in out.items()}
+
+    def pairs(self, group):
+        n = self._chk(self.lib.dem_num_pairs(self.h, group.encode()))
+        a, b = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        st = np.zeros((n, 5))
+        m = self._chk(self.lib.dem_get_pairs(self.h, group.encode(), _ip(a), _ip(b), _dp(st)))
+        a, b, st = a[:m], b[:m], st[:m]
+        order = np.lexsort((b, a))
+        return a[order], b[order], st[order]
+
+    def breaks(self):
+        n = self._chk(self.lib.dem_num_breaks(self.h))
+        a, b, s = (np.zeros(n, np.int32) for _ in range(3))
+        self._chk(self.lib.dem_get_breaks(self.h, _ip(a), _ip(b), _ip(s)))
+        order = np.lexsort((b, a, s))
+        return a[order], b[order], s[order]
+
+    @property
+    def timestep(self):
+        return int(self.lib.dem_timestep(self.h))

@@ -1,0 +1,167 @@
+/*
+ * esys_dem.h -- C ABI of the B200 DEM step (libesys_dem_b200.so).
+ *
+ * One dem_sim handle is one ESyS-Particle worker sub-lattice living on one GPU:
+ * the state and operations of TSubLattice<T> / TRotSubLattice<T>
+ * (Parallel/SubLattice.h:77-302, Parallel/RotSubLattice.h), behind the
+ * ASubLattice operations the master drives over MPI
+ * (Parallel/ASubLattice.h:36-197, Parallel/SubLatticeControler.cpp:534-600).
+ * Plain pointers and sizes only; all arrays are host memory owned by the
+ * caller; the library owns all device memory.
+ *
+ * Every function returns a status (DEM_OK = 0, negative on failure) or a
+ * non-negative count; dem_last_error() gives the message of the last failure.
+ * The reference throws std::runtime_error for the same conditions
+ * (SubLattice.hpp:688-692, 1709-1714; pp_array.hpp:77-88).
+ * A handle is single-threaded: calls on one handle must not overlap.
+ */
+#ifndef ESYS_DEM_H
+#define ESYS_DEM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dem_sim dem_sim;
+
+enum {
+  DEM_OK = 0,
+  DEM_ERR_ARG = -1,      /* invalid argument (unknown group or wall, bad sizes, wrong particle type) */
+  DEM_ERR_OVERFLOW = -2, /* a device-side log ran out of room */
+  DEM_ERR_CUDA = -3,     /* CUDA error or no GPU */
+  DEM_ERR_INTERNAL = -4
+};
+
+/* Particle types: 0 = "NRotSphere" (CParticle), 1 = "RotSphere" (CRotParticle). */
+
+/* CLatticeMaster::makeLattice + setTimeStepSize + setSpatialDomain
+ * (Parallel/LatticeMaster.cpp:528-553, 574-583, 613-693) -> TSubLattice ctor and
+ * initNeighborTable(min, max[, circ]) (Parallel/SubLattice.hpp:455-564).
+ * grid_spacing / verlet_dist are initNeighbourSearch's gridSpacing and
+ * verletDist; circ[0] != 0 makes x periodic (circDimList). */
+int dem_create(dem_sim** out, int particle_type, double grid_spacing, double verlet_dist, const double* bbox_min,
+               const double* bbox_max, const int* circ, double dt);
+int dem_destroy(dem_sim* h);
+const char* dem_last_error(dem_sim* h);
+
+/* TSubLattice::receiveParticles + searchNeighbors(true) (Parallel/SubLattice.hpp:573-588,
+ * Parallel/LatticeMaster.hpp:260-330).  pos/vel/angvel are n x 3, quat n x 4 (scalar first),
+ * vel/angvel/quat/tag/flags may be NULL.  flags bit0: non-dynamic, bit1: non-rotational.
+ * Rotational inertia is 0.4 m r^2 (Model/RotParticle.cpp:34).  Particles outside the
+ * search grid are dropped (ntable/src/ntable.hpp:243-258). */
+int dem_add_particles(dem_sim* h, int n, const int* id, const int* tag, const double* pos, const double* rad,
+                      const double* mass, const double* vel, const double* angvel, const double* quat,
+                      const int* flags);
+
+/* TSubLattice::receiveConnections (Parallel/SubLattice.hpp:598-622): (tag, id1, id2) triples
+ * stored for a later bonded group with that tag. */
+int dem_add_connections(dem_sim* h, int n, const int* tag, const int* id1, const int* id2);
+
+/* TSubLattice::addWall (Parallel/SubLattice.hpp:629-642): plane through origin o with normal n. */
+int dem_add_wall(dem_sim* h, const char* name, const double* o, const double* n);
+
+/* addPairIG "Elastic" -> PIS_NE<T,CElasticInteraction> (Parallel/SubLattice.hpp:1038-1054);
+ * parameters of CElasticIGP (Model/ElasticInteraction.h:24-41). */
+int dem_add_elastic_group(dem_sim* h, const char* name, double k, int scaling);
+
+/* addPairIG "RotFriction" -> PIS_ED<CRotParticle,CRotFrictionInteraction>
+ * (Parallel/SubLattice.hpp:1202-1227), parameters in CRotFrictionIGP packing order
+ * k, mu_s, mu_d, k_s, dt, scaling, meanR_scaling (Parallel/LatticeMaster.cpp:3223-3235). */
+int dem_add_rot_friction_group(dem_sim* h, const char* name, double k, double mu_s, double mu_d, double ks,
+                               double dt, int scaling, int meanR_scaling);
+
+/* TRotSubLattice::addRotBondedIG (Parallel/RotSubLattice.hpp:116-186): bonds from the stored
+ * connections with this tag, CRotBondedIGP fields in packing order; beta1 = beta2 = 1. */
+int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                           double max_nForce, double max_shForce, double max_tMoment, double max_bMoment,
+                           int scaling, int meanR_scaling, double truncated);
+
+/* TSubLattice::addElasticWIG (Parallel/SubLattice.hpp:667-696): CEWallInteractionGroup<T>. */
+int dem_add_wall_group(dem_sim* h, const char* name, const char* wall, double k);
+
+/* TSubLattice::addSingleIG "Gravity" -> BodyForceGroup<T> (Parallel/SubLattice.hpp:1687-1697). */
+int dem_add_gravity(dem_sim* h, const char* name, const double* g);
+
+/* TSubLattice::doAddDamping "Damping" / TRotSubLattice::doAddDamping "RotDamping"
+ * (Parallel/SubLattice.hpp:1748-1784, Parallel/RotSubLattice.hpp:79-109); v_ref = 0. */
+int dem_add_damping(dem_sim* h, int rotational, double viscosity, int max_iterations);
+
+/* TSubLattice::setExIG (Parallel/SubLattice.hpp:1980-2009): pairs bonded in `bonded` are
+ * excluded from the dynamic group `dynamic` while the bond is intact. */
+int dem_add_exclusion(dem_sim* h, const char* bonded, const char* dynamic);
+
+/* TSubLattice::setTimeStepSize (Parallel/SubLattice.hpp:2163-2204). */
+int dem_set_timestep(dem_sim* h, double dt);
+
+/* nsteps x CLatticeMaster::runOneStep (Parallel/LatticeMaster.cpp:2602-2725) on this worker:
+ * checkNeighbors -> searchNeighbors -> updateInteractions -> oneStep (zeroForces, calcForces,
+ * integrate).  Field savers and Python runnables are the caller's. */
+int dem_step(dem_sim* h, int nsteps);
+
+/* TSubLattice::moveWallBy (Parallel/SubLattice.hpp:2878-2895) -> CWall::moveBy (Model/Wall.h:54-60). */
+int dem_move_wall(dem_sim* h, const char* name, const double* d);
+
+/* Device-side wall loader: moves the wall by v*dt after every step, the constant-speed phase of
+ * WallLoaderRunnable (Doc/Tutorial/examples/WallLoader.py.tex) without a host call per step. */
+int dem_set_wall_velocity(dem_sim* h, const char* name, const double* v);
+
+/* TSubLattice::applyForceToWall (Parallel/SubLattice.hpp:2935-2950) -> CEWallInteractionGroup::applyForce
+ * (Model/EWallInteractionGroup.hpp:93-164). */
+int dem_apply_force_to_wall(dem_sim* h, const char* group, const double* f);
+
+/* getWallPosition / getWallForce (Python/esys/lsm/LsmMpiPy.cpp:2767-2786); either output may be NULL. */
+int dem_get_wall(dem_sim* h, const char* name, double* pos, double* force);
+
+/* TSubLattice::getNumParticles (Parallel/SubLattice.hpp:486-490): particles in the table. */
+int dem_num_particles(dem_sim* h);
+
+/* Particle state (the fields CParticle / CRotParticle expose to savers), one row per particle
+ * in table order; any output may be NULL.  Returns the number of rows written. */
+int dem_get_particles(dem_sim* h, int* id, double* pos, double* vel, double* angvel, double* quat, double* force,
+                      double* moment);
+
+/* Interactions of a group as (id1 < id2) pairs (CLatticeMaster::getBondGroupIdPairs, Parallel/LatticeMaster.cpp:2742-2766);
+ * state is n x 5 or NULL: RotFriction -> tangential force (3), slipping, touching.
+ * Returns the number of pairs. */
+int dem_num_pairs(dem_sim* h, const char* group);
+int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* state);
+
+/* Bond failures so far (PIS_EB::update, pis/pi_storage_eb.hpp:23-49): (id1, id2, step) per
+ * broken bond, step = the time step whose interaction update removed it. */
+int dem_num_breaks(dem_sim* h);
+int dem_get_breaks(dem_sim* h, int* id1, int* id2, int* step);
+
+/* TSubLattice::moveTaggedParticlesBy (Parallel/SubLattice.hpp:2577-2587). */
+int dem_move_tagged(dem_sim* h, int tag, int mask, const double* d);
+
+/* Time steps completed (CLatticeMaster::m_t). */
+long long dem_timestep(dem_sim* h);
+
+/* Bulk update of existing particles' state (pos/vel n x 3, angvel n x 3, quat n x 4; any may be
+ * NULL), like setParticleVelocity / moveParticleTo over many particles
+ * (Python/esys/lsm/LsmMpiPy.cpp:3054-3136).  With id == NULL, row i is particle slot i (the
+ * order of dem_get_particles while no particle has left the grid).  A move is checked against
+ * verletDist/2 before the next step, as checkNeighbors would. */
+int dem_set_particles(dem_sim* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
+                      const double* quat);
+
+/* Run all device work of this handle on the caller's CUDA stream (a cudaStream_t); the caller
+ * keeps ownership.  No reference counterpart (the reference has no device). */
+int dem_set_stream(dem_sim* h, void* stream);
+
+/* Counters, no reference counterpart (the reference's MpiWTimers, Foundation/Timer.h:28-102, time
+ * phases instead): out[0] steps, [1] interactions evaluated (Verlet pairs + intact bonds + wall
+ * candidates, summed over steps), [2] neighbour searches, [3] kernel launches, [4] device time of
+ * the force/integration kernels in ns (with option "profile"), [5] steps timed by [4],
+ * [6] interactions evaluated per step now, [7] threads per particle in use.  Returns entries written. */
+int dem_get_counters(dem_sim* h, long long* out, int n);
+
+/* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic, 1, 2, 4, 8),
+ * "chunk" (steps launched per host round trip), "store_forces" (keep per-particle F/M),
+ * "profile" (time the force/integration kernels with CUDA events). */
+int dem_set_option(dem_sim* h, const char* key, double value);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

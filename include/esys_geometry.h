@@ -1,0 +1,24 @@
+/*
+ * esys_geometry.h -- seeded synthetic packings for the DEM benchmarks and tests.
+ * Stands in for the reference's set-up packers (Geometry/RandomBoxPacker.hpp,
+ * Python RandomBoxPacker) that generate particle inputs; not part of the
+ * per-step hot path.
+ */
+#ifndef ESYS_GEOMETRY_H
+#define ESYS_GEOMETRY_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Random sequential insertion of up to n spheres into [bmin, bmax] (x periodic when
+ * periodic_x != 0): radii uniform in [p0, p1] (dist = 0) or lognormal with median p0 and
+ * log-sigma p1 (dist = 1), clipped to [rmin, rmax], inserted largest first with up to
+ * max_attempts trials each.  Writes pos (3 per sphere) and rad; returns the number placed
+ * (<= n) or -1 on bad arguments. */
+int lsm_pack_rsi(unsigned long long seed, int n, const double* bmin, const double* bmax, int periodic_x, int dist,
+                 double p0, double p1, double rmin, double rmax, int max_attempts, double* pos, double* rad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -387,14 +387,15 @@ struct RefSim : public ASim {
     err = "no such group";
     return -1;
   }
-  /* state per pair: friction -> Ffric (3), slipping, touching; elastic/bond -> force on p1 (3) and 2 zeros */
+  /* state per pair (5 doubles): friction -> tangential force (3), slipping, touching;
+   * elastic -> last force on p2 (3), 0, touching; bond -> force on p1 (3), failure criterion, 0 */
   int get_pairs(const char* group, int* id1, int* id2, double* state) override {
     int i = 0;
     if (elastic.count(group)) {
       for (auto& in : elastic[group]->list()) {
         auto v = in.getAllID();
         id1[i] = v[0]; id2[i] = v[1];
-        if (state) { Vec3 f = in.getForce(); for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k]; state[5 * i + 3] = state[5 * i + 4] = 0; }
+        if (state) { Vec3 f = in.getForce(); for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k]; state[5 * i + 3] = 0; state[5 * i + 4] = in.Count(); }
         ++i;
       }
       return i;

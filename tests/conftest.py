@@ -1,0 +1,47 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (os.path.join(ROOT, "esys-particle_b200"), os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); run with -m gpu")
+
+
+def gpu_available() -> bool:
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def dem_lib():
+    """The built B200 DEM library (built on demand; never a CPU fallback)."""
+    import build  # esys-particle_b200/build.py
+
+    build.build()
+    from esys.lsm import _capi
+
+    return _capi.load_library()
+
+
+@pytest.fixture(scope="session")
+def oracle_libs():
+    """Build the CPU restatement (and the reference harness when the reference tree is present)."""
+    import subprocess
+
+    odir = os.path.join(ROOT, "oracle")
+    subprocess.run(["make", "-s", "-C", odir, "restate"], check=True)
+    if os.path.isdir("/root/reference"):
+        subprocess.run(["make", "-s", "-j8", "-C", odir, "ref"], check=True)
+    import oracle
+
+    return oracle

@@ -1,0 +1,112 @@
+"""Seeded synthetic scenarios shared by the parity tests.
+
+Each builder takes a ``make(particle_type, grid_spacing, verlet_dist, bbox_min,
+bbox_max, circ, dt)`` factory and returns the simulation it set up, so the same
+scenario drives the CUDA path and the CPU oracles through identical calls.
+Particle masses follow CParticle::setDensity with rho = 1 and pi = 3.141592654
+(Model/Particle.cpp:108-122).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PI_REF = 3.141592654
+
+
+def sphere_mass(r, rho=1.0):
+    r = np.asarray(r, dtype=np.float64)
+    return (4.0 / 3.0) * rho * PI_REF * r * r * r
+
+
+def gravity_box(make, n_side=6, seed=1, steps_dt=1e-4, layers=None, gap=1.0):
+    """Small form of the NRotSphere gravity packing: jittered cubic lattice,
+    NRotElastic k=1000, gravity -9.81 z, linear damping 0.01, six elastic walls."""
+    rng = np.random.default_rng(seed)
+    layers = layers or n_side
+    L = n_side * gap
+    H = 2 * layers * gap
+    g = np.stack(np.meshgrid(np.arange(n_side), np.arange(n_side), np.arange(layers), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) * gap + rng.uniform(-0.05, 0.05, size=g.shape)
+    rad = rng.uniform(0.4, 0.5, size=len(g))
+    n = len(g)
+    sim = make("NRotSphere", 1.2, 0.2, (0, 0, 0), (L, L, H), (0, 0, 0), steps_dt)
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32))
+    sim.add_elastic_group("elastic", 1000.0, True)
+    sim.add_gravity("gravity", (0, 0, -9.81))
+    sim.add_damping(0, 0.01, 100)
+    for name, o, nrm in (("xlo", (0, 0, 0), (1, 0, 0)), ("xhi", (L, 0, 0), (-1, 0, 0)),
+                         ("ylo", (0, 0, 0), (0, 1, 0)), ("yhi", (0, L, 0), (0, -1, 0)),
+                         ("zlo", (0, 0, 0), (0, 0, 1)), ("zhi", (0, 0, H), (0, 0, -1))):
+        sim.add_wall(name, o, nrm)
+        sim.add_wall_group(name + "_w", name, 1000.0)
+    return sim
+
+
+def friction_pack(make, nx=6, ny=5, nz=6, seed=2, periodic=False, dt=5e-5, vscale=0.5, squeeze=0.93):
+    """Small rotational frictional pack: slightly overlapping jittered lattice of
+    RotSpheres (lognormal radii), RotFriction kn=ks=1e4 mu=0.6, elastic floor and
+    roof, random initial linear and angular velocities, linear + rotational damping."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    spacing = 1.0 * squeeze
+    pos = (g + 0.5) * spacing + rng.uniform(-0.03, 0.03, size=g.shape)
+    rad = np.clip(np.exp(np.log(0.5) + 0.25 * rng.standard_normal(len(g))) * 0.5 + 0.25, 0.3, 0.5)
+    n = len(g)
+    Lx, Ly, Lz = nx * spacing, ny * spacing + 0.2, nz * spacing
+    sim = make("RotSphere", 1.2, 0.2, (0, -0.1, 0), (Lx, Ly - 0.1, Lz), (1 if periodic else 0, 0, 0), dt)
+    vel = rng.normal(0, vscale, size=(n, 3))
+    angvel = rng.normal(0, vscale, size=(n, 3))
+    sim.add_particles(np.arange(n)[::-1].copy(), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=vel,
+                      angvel=angvel)
+    sim.add_rot_friction_group("friction", 1e4, 0.6, 0.6, 1e4, dt, True, True)
+    sim.add_wall("floor", (0, -0.1, 0), (0, 1, 0))
+    sim.add_wall("roof", (0, Ly - 0.1, 0), (0, -1, 0))
+    sim.add_wall_group("floor_w", "floor", 1e4)
+    sim.add_wall_group("roof_w", "roof", 1e4)
+    sim.add_damping(0, 0.002, 50)
+    sim.add_damping(1, 0.002, 50)
+    return sim
+
+
+def bonded_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, strength=(0.5, 1.0, 1.0, 0.5), load_rate=0.02,
+                 with_friction=True):
+    """Small bonded block: jittered cubic RotSpheres, every pair within gap 1e-3
+    of touching bonded (cf. Geometry/DistConnections), RotBond with brittle
+    failure, RotFriction + exclusion for post-break contacts, platens at y."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) * 1.0 + rng.uniform(-0.02, 0.02, size=g.shape)
+    n = len(g)
+    rad = np.full(n, 0.5)
+    # radii chosen so that lattice neighbours touch: r_i = min over neighbours of half distance
+    d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
+    np.fill_diagonal(d, np.inf)
+    rad = np.clip(0.5 * d.min(axis=1), 0.3, 0.5)
+    gap = d - (rad[:, None] + rad[None, :])
+    i1, i2 = np.nonzero(np.triu(gap <= 1e-3, 1))
+    Ly = ny * 1.0
+    sim = make("RotSphere", 1.25, 0.2, (0, 0, 0), (nx * 1.0, Ly, nz * 1.0), (0, 0, 0), dt)
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32))
+    sim.add_connections(np.ones(len(i1), np.int32), i1, i2)
+    mn, ms, mt, mb = strength
+    sim.add_rot_bond_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, mn, ms, mt, mb, True, True, 1.0)
+    if with_friction:
+        sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
+        sim.add_exclusion("bonds", "friction")
+    sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, Ly, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e5)
+    sim.add_wall_group("top_w", "top", 1e5)
+    sim.add_damping(0, 0.01, 50)
+    sim.add_damping(1, 0.01, 50)
+    sim._load_rate = load_rate
+    return sim
+
+
+def run_loaded(sim, steps, rate):
+    """Advance with a platen loader: both platens move toward each other by
+    ``rate`` per step (a pre-step runnable like WallLoaderRunnable)."""
+    for _ in range(steps):
+        sim.move_wall("top", (0, -rate, 0))
+        sim.move_wall("bottom", (0, rate, 0))
+        sim.step(1)
