@@ -118,7 +118,8 @@ class Clocks:
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]})
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 3 + k and s[3 + k].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 

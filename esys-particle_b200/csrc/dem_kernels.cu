@@ -495,16 +495,23 @@ __device__ __forceinline__ V lane_sum(V v) {
 }
 
 constexpr int kStepThreads = 256;
+constexpr int kStepWarps = kStepThreads / 32;
 
-template <bool ROT, int TPP>
-__global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
-  __shared__ double s_red[kStepThreads / 32][3];
+// Interaction families compiled into a k_step instance (the host picks the
+// smallest instance that covers the groups present, so a friction-only run
+// does not carry the registers of the bond law).
+enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4 };
+
+template <bool ROT, int TPP, int FEAT>
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(const StepArgs a) {
+  __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;
   if (*a.stop) return;  // an earlier step of this chunk asked the host to intervene
   const long long step = *a.step_counter + 1;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = tid / TPP;
   const int lane = threadIdx.x % TPP;
+  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool valid = i < a.P.n;
   const unsigned pf = valid ? a.P.pflags[i] : 0u;
   const bool alive = valid && (pf & PF_ALIVE);
@@ -515,12 +522,16 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
   if (alive) {
     p4 = in.pr[i];
     v4 = in.vm[i];
-    if (ROT) { w4 = in.wi[i]; q4 = in.qq[i]; }
+    if (ROT) {
+      w4 = in.wi[i];
+      if (FEAT & F_BOND) q4 = in.qq[i];
+    }
   }
   const V xi = xyz(p4);
   V F = mk(0.0, 0.0, 0.0), M = mk(0.0, 0.0, 0.0);
 
-  // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120)
+  // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
+  //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.
   for (int w = 0; w < a.nwall; ++w) {
     V c = mk(0.0, 0.0, 0.0);
     if (alive && lane == 0 && (pf & (1u << (PF_WALL_SHIFT + w)))) {
@@ -531,23 +542,16 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
         if (pf & (1u << (PF_INNER_SHIFT + w))) c = f;  // CWall::addForce(-F): m_force -= -F
       }
     }
-    // fixed-order block reduction of the wall's reaction
     double cx = c.x, cy = c.y, cz = c.z;
+    if (__any_sync(0xffffffffu, cx != 0.0 || cy != 0.0 || cz != 0.0)) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      cx += __shfl_down_sync(0xffffffffu, cx, o);
-      cy += __shfl_down_sync(0xffffffffu, cy, o);
-      cz += __shfl_down_sync(0xffffffffu, cz, o);
+      for (int o = 16; o > 0; o >>= 1) {
+        cx += __shfl_down_sync(0xffffffffu, cx, o);
+        cy += __shfl_down_sync(0xffffffffu, cy, o);
+        cz += __shfl_down_sync(0xffffffffu, cz, o);
+      }
     }
-    if ((threadIdx.x & 31) == 0) { s_red[threadIdx.x >> 5][0] = cx; s_red[threadIdx.x >> 5][1] = cy; s_red[threadIdx.x >> 5][2] = cz; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double sx = 0, sy = 0, sz = 0;
-      for (int k = 0; k < kStepThreads / 32; ++k) { sx += s_red[k][0]; sy += s_red[k][1]; sz += s_red[k][2]; }
-      double* dst = a.wall_partial + ((size_t)blockIdx.x * kMaxWalls + w) * 3;
-      dst[0] = sx; dst[1] = sy; dst[2] = sz;
-    }
-    __syncthreads();
+    if (wlane == 0) { s_red[warp][w][0] = cx; s_red[warp][w][1] = cy; s_red[warp][w][2] = cz; }
   }
 
   // 2. body forces (BodyForceGroup::calcForces, BodyForceGroup.hpp:54-65): F += g * m
@@ -556,7 +560,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
 
   // 3. dynamic pair groups (PIS_NE / PIS_ED::calcForces)
   V Fp = mk(0.0, 0.0, 0.0), Mp = mk(0.0, 0.0, 0.0);
-  if (alive) {
+  if ((FEAT & (F_ELASTIC | F_FRIC)) && alive) {
     for (int d = 0; d < a.ndyn; ++d) {
       const DynDev& G = a.dyn[d];
       const int e0 = G.adj_start[i], e1 = G.adj_start[i + 1];
@@ -570,30 +574,34 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
         const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
         const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
         if (G.kind == 0) {
-          V f;
-          if (law_elastic(elastic_k(G.k, G.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, f)) {
-            if (isp1) Fp += -1.0 * f; else Fp += f;
+          if constexpr ((FEAT & F_ELASTIC) != 0) {
+            V f;
+            if (law_elastic(elastic_k(G.k, G.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, f)) {
+              if (isp1) Fp += -1.0 * f; else Fp += f;
+            }
           }
-        } else if (ROT) {
-          const double4 vj = in.vm[j], wj = in.wi[j];
-          const double4 va = isp1 ? v4 : vj, vb = isp1 ? vj : v4;
-          const double4 wa = isp1 ? w4 : wj, wb = isp1 ? wj : w4;
-          const double4 h = G.hist_in[k];
-          double keff, kseff;
-          friction_k(G.k, G.ks, G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
-          FricOut o;
-          law_friction(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, xyz(va), xyz(wa), x2, pb.w, xyz(vb), xyz(wb),
-                       mk(h.x, h.y, h.z), (((int)h.w) & 1) != 0, o);
-          if (isp1) {
-            Fp += -1.0 * o.fn;
-            Mp += o.M1;
-            Fp += o.Ffric;
-            G.hist_out[k] = make_double4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
-                                         (o.slipping ? 1.0 : 0.0) + (o.touching ? 2.0 : 0.0));
-          } else {
-            Fp += o.fn;
-            Mp += o.M2;
-            Fp += -1.0 * o.Ffric;
+        } else {
+          if constexpr (ROT && (FEAT & F_FRIC) != 0) {
+            const double4 vj = in.vm[j], wj = in.wi[j];
+            const double4 va = isp1 ? v4 : vj, vb = isp1 ? vj : v4;
+            const double4 wa = isp1 ? w4 : wj, wb = isp1 ? wj : w4;
+            const double4 h = G.hist_in[k];
+            double keff, kseff;
+            friction_k(G.k, G.ks, G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
+            FricOut o;
+            law_friction(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, xyz(va), xyz(wa), x2, pb.w, xyz(vb), xyz(wb),
+                         mk(h.x, h.y, h.z), (((int)h.w) & 1) != 0, o);
+            if (isp1) {
+              Fp += -1.0 * o.fn;
+              Mp += o.M1;
+              Fp += o.Ffric;
+              G.hist_out[k] = make_double4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
+                                           (o.slipping ? 1.0 : 0.0) + (o.touching ? 2.0 : 0.0));
+            } else {
+              Fp += o.fn;
+              Mp += o.M2;
+              Fp += -1.0 * o.Ffric;
+            }
           }
         }
       }
@@ -602,46 +610,48 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
 
   // 4. bonded groups (PIS_EB::calcForces) + failure test (PIS_EB::update at the next step)
   V Fb = mk(0.0, 0.0, 0.0), Mb = mk(0.0, 0.0, 0.0);
-  if (ROT && alive) {
-    for (int d = 0; d < a.nbond; ++d) {
-      const BondDev& B = a.bond[d];
-      const int e0 = B.adj_start[i], e1 = B.adj_start[i + 1];
-      for (int e = e0 + lane; e < e1; e += TPP) {
-        const int2 en = B.adj[e];
-        const int k = en.y & 0x7fffffff;
-        if (B.broken_step[k] <= step) continue;  // removed by an earlier update
-        const int j = en.x;
-        const bool isp1 = en.y < 0;
-        const double4 pj = in.pr[j], qj = in.qq[j];
-        const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
-        const double4 qa = isp1 ? q4 : qj, qb = isp1 ? qj : q4;
-        const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
-        const double4 D0 = B.D0[k];
-        const V mD = xyz(D0);
-        const double dist0 = sqrt(dot(mD, mD));
-        const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
-        BondOut o;
-        law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
-        if (isp1) {
-          Fb += o.force;
-          Mb += o.moment1;
-          if (bond_broken(K, o, B.truncated)) {
-            B.broken_step[k] = (int)(step + 1);
-            a.P.flagged[i] = 1;
-            a.P.flagged[j] = 1;
-            int slot = atomicAdd(B.nevents, 1);
-            if (slot < B.cap_events) {
-              B.events[3 * slot] = a.P.id[i];
-              B.events[3 * slot + 1] = a.P.id[j];
-              B.events[3 * slot + 2] = (int)(step + 1);
-            } else {
-              atomicOr(a.ctrl, CTRL_OVERFLOW);
+  if constexpr (ROT && (FEAT & F_BOND) != 0) {
+    if (alive) {
+      for (int d = 0; d < a.nbond; ++d) {
+        const BondDev& B = a.bond[d];
+        const int e0 = B.adj_start[i], e1 = B.adj_start[i + 1];
+        for (int e = e0 + lane; e < e1; e += TPP) {
+          const int2 en = B.adj[e];
+          const int k = en.y & 0x7fffffff;
+          if (B.broken_step[k] <= step) continue;  // removed by an earlier update
+          const int j = en.x;
+          const bool isp1 = en.y < 0;
+          const double4 pj = in.pr[j], qj = in.qq[j];
+          const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
+          const double4 qa = isp1 ? q4 : qj, qb = isp1 ? qj : q4;
+          const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+          const double4 D0 = B.D0[k];
+          const V mD = xyz(D0);
+          const double dist0 = sqrt(dot(mD, mD));
+          const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
+          BondOut o;
+          law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
+          if (isp1) {
+            Fb += o.force;
+            Mb += o.moment1;
+            if (bond_broken(K, o, B.truncated)) {
+              B.broken_step[k] = (int)(step + 1);
+              a.P.flagged[i] = 1;
+              a.P.flagged[j] = 1;
+              int slot = atomicAdd(B.nevents, 1);
+              if (slot < B.cap_events) {
+                B.events[3 * slot] = a.P.id[i];
+                B.events[3 * slot + 1] = a.P.id[j];
+                B.events[3 * slot + 2] = (int)(step + 1);
+              } else {
+                atomicOr(a.ctrl, CTRL_OVERFLOW);
+              }
+              atomicOr(a.ctrl, CTRL_BROKE);
             }
-            atomicOr(a.ctrl, CTRL_BROKE);
+          } else {
+            Fb += -1.0 * o.force;
+            Mb += o.moment2;
           }
-        } else {
-          Fb += -1.0 * o.force;
-          Mb += o.moment2;
         }
       }
     }
@@ -651,8 +661,10 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
   if (TPP > 1) {
     Fp = lane_sum<TPP>(Fp);
     Mp = lane_sum<TPP>(Mp);
-    Fb = lane_sum<TPP>(Fb);
-    Mb = lane_sum<TPP>(Mb);
+    if (FEAT & F_BOND) {
+      Fb = lane_sum<TPP>(Fb);
+      Mb = lane_sum<TPP>(Mb);
+    }
   }
 
   if (alive && lane == 0) {
@@ -668,6 +680,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
     const double dt = a.dt;
     V v = xyz(v4), x = xi;
     if (ROT) {
+      if (!(FEAT & F_BOND)) q4 = in.qq[i];
       V w = xyz(w4);
       Qd q{q4.x, mk(q4.y, q4.z, q4.w)};
       if (pf & PF_ROT) {
@@ -704,26 +717,42 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const StepArgs a) {
     if (dot(dd, dd) > a.half_alpha_sq) atomicOr(a.ctrl, CTRL_REBUILD);
   }
 
-  // epilogue by the last block: wall reactions, step counter, stop flag, wall loaders
-  __threadfence();
+  // per-block wall reactions (fixed order over warps), then the last block finishes the step
+  const int nw3 = a.nwall * 3;
+  __syncthreads();
+  if (threadIdx.x < nw3) {
+    const int w = threadIdx.x / 3, c = threadIdx.x % 3;
+    double acc = 0.0;
+    for (int k = 0; k < kStepWarps; ++k) acc += s_red[k][w][c];
+    a.wall_partial[((size_t)blockIdx.x * kMaxWalls + w) * 3 + c] = acc;
+    __threadfence();
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned prev = atomicInc(a.block_counter, gridDim.x - 1);
     s_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    for (int w = 0; w < a.nwall; ++w) {
-      double sx = 0, sy = 0, sz = 0;
-      for (unsigned b = 0; b < gridDim.x; ++b) {
-        const volatile double* src = a.wall_partial + ((size_t)b * kMaxWalls + w) * 3;
-        sx += src[0]; sy += src[1]; sz += src[2];
-      }
-      a.wall_force[3 * w] = sx;
-      a.wall_force[3 * w + 1] = sy;
-      a.wall_force[3 * w + 2] = sz;
+  if (!s_last) return;
+  __threadfence();
+  // wall reactions: thread t sums blocks t, t+256, ... (fixed assignment), then a fixed tree
+  for (int wc = 0; wc < nw3; ++wc) {
+    const int w = wc / 3, c = wc % 3;
+    double acc = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+      acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (wlane == 0) s_red[warp][0][0] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
+      a.wall_force[3 * w + c] = t;
     }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
     for (int w = 0; w < a.nwall; ++w) {  // native wall loader: origin += v*dt per step (WallLoaderRunnable)
       WallDev* W = a.walls + w;
       if (a.wall_vel[3 * w] != 0.0 || a.wall_vel[3 * w + 1] != 0.0 || a.wall_vel[3 * w + 2] != 0.0) {
@@ -891,13 +920,26 @@ void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const
 
 int step_grid(int n, int tpp) { return nblk((long long)(n > 0 ? n : 1) * tpp, kStepThreads); }
 
+template <bool R, int FEAT>
+static void launch_step_tpp(const StepArgs& a, int tpp, int grid, cudaStream_t s) {
+  switch (tpp) {
+    case 1: k_step<R, 1, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 2: k_step<R, 2, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 4: k_step<R, 4, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
+    default: k_step<R, 8, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
+  }
+}
+
 void launch_step(const StepArgs& a, bool rot, int tpp, cudaStream_t s) {
   const int grid = step_grid(a.P.n, tpp);
-#define DEM_STEP_CASE(R, T) \
-  if (rot == R && tpp == T) { k_step<R, T><<<grid, kStepThreads, 0, s>>>(a); return; }
-  DEM_STEP_CASE(false, 1) DEM_STEP_CASE(false, 2) DEM_STEP_CASE(false, 4) DEM_STEP_CASE(false, 8)
-  DEM_STEP_CASE(true, 1) DEM_STEP_CASE(true, 2) DEM_STEP_CASE(true, 4) DEM_STEP_CASE(true, 8)
-#undef DEM_STEP_CASE
+  bool el = false, fr = false;
+  for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
+  const bool bd = a.nbond > 0;
+  if (!rot) return launch_step_tpp<false, F_ELASTIC>(a, tpp, grid, s);
+  if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC>(a, tpp, grid, s);
+  if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC>(a, tpp, grid, s);
+  if (bd && !el) return launch_step_tpp<true, F_FRIC | F_BOND>(a, tpp, grid, s);
+  return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BOND>(a, tpp, grid, s);
 }
 
 }  // namespace dem
