@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libesys_dem_b200.so")
-SOURCES = ["dem_kernels.cu", "dem_sim.cu", "packing.cpp"]
+SOURCES = ["dem_kernels.cu", "dem_sim.cu", "dem_noalloc.cu", "packing.cpp"]
 HEADERS = ["dem_device.cuh", "dem_kernels.h", "dem_laws.cuh", "dem_math.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -156,6 +156,22 @@ int dem_set_stream(dem_sim* h, void* stream);
  * [6] interactions evaluated per step now, [7] threads per particle in use.  Returns entries written. */
 int dem_get_counters(dem_sim* h, long long* out, int n);
 
+/* Allocation-free per-wall reaction forces, for callers that cannot call cudaMalloc: code that
+ * runs during CUDA graph capture, hosts that hand the library only memory from their own pool,
+ * real-time loops that forbid allocation.  No counterpart in the reference.
+ * Computes, for each wall, the sum over the given particles of the elastic wall contact force
+ * (the quantity the step accumulates into CWall::m_force, what dem_get_wall reports).
+ * particles: device, n rows of 4 doubles (x, y, z, radius), 16-byte aligned; walls: device, nwall
+ * rows of 7 doubles (origin xyz, normal xyz, normalK); reactions: device, nwall x 3 doubles;
+ * stream: a cudaStream_t (NULL = default stream).  Limits: 1 <= nwall <= 8, 0 <= n <= 16777216;
+ * larger sizes return DEM_ERR_ARG.  No memory is allocated: block partial sums live in a fixed
+ * 111 KiB (113,668-byte) __device__ array that every GPU loading the library keeps until exit.  The first call on
+ * each device looks up that array's address (make it before any stream capture).  All calls on a
+ * device share the array, so calls that overlap on the GPU race; the result of each call is
+ * written asynchronously on `stream`. */
+int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const double* walls, double* reactions,
+                               void* stream);
+
 /* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic, 1, 2, 4, 8),
  * "chunk" (steps launched per host round trip), "store_forces" (keep per-particle F/M),
  * "profile" (time the force/integration kernels with CUDA events). */
