@@ -195,6 +195,9 @@ def main():
     ap.add_argument("--dem-steps", type=int, default=200, help="timesteps per bench step")
     ap.add_argument("--tpp", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64],
+                    help="32: FP32 pair forces + FP64 integration (headline); 64: FP64 throughout")
+    ap.add_argument("--no-fp64-compare", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -217,40 +220,65 @@ def main():
 
     w = workload()
     n = len(w["ids"])
-    sim = setup(lambda *a: _capi.DemSim(*a), w, periodic=True)
     stream = torch.cuda.current_stream()
-    sim.set_stream(stream.cuda_stream)
-    sim.set_option("profile", 1)
-    if args.tpp:
-        sim.set_option("threads_per_particle", args.tpp)
-    sim.set_wall_velocity("bottom", (-0.01, 0, 0))
-    sim.set_wall_velocity("top", (0.01, 0, 0))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    def bench_step():
-        sim.step(args.dem_steps)
-        sim.apply_force_to_wall("top_w", (0.0, -NORMAL_LOAD, 0.0))
 
     def barrier():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        bench_step()
-        flush.zero_()
-    barrier()
-    c0 = sim.counters()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with Clocks(local) as clk:
+    def make_sim(precision):
+        sim = setup(lambda *a: _capi.DemSim(*a), w, periodic=True)
+        sim.set_stream(stream.cuda_stream)
+        sim.set_option("profile", 1)
+        sim.set_option("precision", precision)
+        if args.tpp:
+            sim.set_option("threads_per_particle", args.tpp)
+        sim.set_wall_velocity("bottom", (-0.01, 0, 0))
+        sim.set_wall_velocity("top", (0.01, 0, 0))
+        return sim
+
+    def bench_step(sim):
+        sim.step(args.dem_steps)
+        sim.apply_force_to_wall("top_w", (0.0, -NORMAL_LOAD, 0.0))
+
+    def timed(sim, clk=None):
+        for _ in range(args.warmup):
+            bench_step(sim)
+            flush.zero_()
+        barrier()
+        c0 = sim.counters()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
-            bench_step()
+            bench_step(sim)
             ev[k][1].record(stream)
         barrier()
-    c1 = sim.counters()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
+        c1 = sim.counters()
+        return c0, c1, sum(a.elapsed_time(b) for a, b in ev)
+
+    fp64 = None
+    if args.precision == 32 and not args.no_fp64_compare:
+        s64 = make_sim(64)
+        a0, a1, ms64 = timed(s64)
+        ns64 = (a1["step_kernel_ns"] - a0["step_kernel_ns"]) / max(1, a1["profiled_steps"] - a0["profiled_steps"])
+        fp64 = {"value": (a1["contact_updates"] - a0["contact_updates"]) / (ms64 / 1e3), "kernel_us": ns64 / 1e3,
+                "ms_per_step": ms64 / args.steps}
+        s64.close()
+    sim = make_sim(args.precision)
+    with Clocks(local) as clk:
+        c0, c1, ms = timed(sim)
+    err = None
+    if args.precision == 32:
+        # force error of the FP32 form vs FP64 on the developed state (same positions, velocities, history)
+        sim.set_option("precision", 64)
+        out = (C.c_double * 5)()
+        sim._chk(sim.lib.dem_precision_check(sim.h, out))
+        err = {"max_rel_force_err": out[0], "max_rel_moment_err": out[1], "median_particle_rel_err": out[2],
+               "p99_particle_rel_err": out[3], "particles": int(out[4])}
+        sim.set_option("precision", 32)
     contacts = c1["contact_updates"] - c0["contact_updates"]
     t_max = ms
     if dist is not None:
@@ -268,8 +296,9 @@ def main():
     step_ns = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / max(1, c1["profiled_steps"] - c0["profiled_steps"])
     m_fric = sim._chk(sim.lib.dem_num_pairs(sim.h, b"friction"))
     n_wall_cand = c1["contacts_per_step"] - m_fric
-    # algorithmic bytes per launch: particle 256 B (rot, FP64), RotFriction pair 60 B, wall candidate 4 B
-    alg_bytes = n * 256 + m_fric * 60 + n_wall_cand * 4
+    # algorithmic bytes per launch: particle 256 B (rot, FP64), RotFriction pair 60 B (FP32 history: 36 B),
+    # wall candidate 4 B
+    alg_bytes = n * 256 + m_fric * (36 if args.precision == 32 else 60) + n_wall_cand * 4
     achieved = alg_bytes / (step_ns * 1e-9) / 1e9
     peak, peak_kind = peaks()
     traffic = traffic_per_launch()
@@ -290,7 +319,7 @@ def main():
         s0 = time.perf_counter()
         sim.set_particles(pos=pin["pos"].data_ptr(), vel=pin["vel"].data_ptr(), angvel=pin["angvel"].data_ptr(),
                           quat=pin["quat"].data_ptr(), n=n)
-        bench_step()
+        bench_step(sim)
         sim.get_particles_raw(ids_pin.data_ptr(), *(pin[k].data_ptr() for k in ("pos", "vel", "angvel", "quat",
                                                                                  "force", "moment")))
         s1 = time.perf_counter()
@@ -317,7 +346,8 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RSI packing)",
+            "vs_baseline": None, "dtype": "f32-forces/f64-integration" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded RSI packing)",
             "config": {"workload": "rot-friction shear cell: 250,000 RotSpheres, lognormal r (0.5, 0.25) in "
                                    "[0.2,1.0], 100x50x100 periodic-x, kn=ks=1e4 mu=0.6, 2 elastic walls "
                                    "+-0.01 x, 1e3 servo load, dt=5e-5",
@@ -327,11 +357,15 @@ def main():
                        "l2": "flushed (256 MB write) between bench steps; working set ~90 MB stays L2-resident "
                              "within a bench step",
                        "parallelism": "replicas only" if world > 1 else "single GPU",
-                       "precision": "FP64 forces and integration (max rel force err vs FP64 = 0)"},
+                       "precision": ("FP32 pair forces (Kahan-compensated), FP64 positions / contact detection / "
+                                     "integration" if args.precision == 32 else "FP64 throughout"),
+                       "force_error_vs_fp64": err if err is not None else {"max_rel_force_err": 0.0},
+                       "fp64_form": fp64},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (traffic or {}).get("bytes_per_launch"),
-                         "kernel": "k_step<ROT=1,TPP>", "kernel_us": step_ns / 1e3,
+                         "kernel": f"k_step<ROT=1,TPP,FRIC,{'FP32' if args.precision == 32 else 'FP64'}>",
+                         "kernel_us": step_ns / 1e3,
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": n * (24 + 24 + 24 + 32),

@@ -13,8 +13,12 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libesys_dem_b200.so")
-SOURCES = ["dem_kernels.cu", "dem_sim.cu", "dem_noalloc.cu", "packing.cpp"]
-HEADERS = ["dem_device.cuh", "dem_kernels.h", "dem_laws.cuh", "dem_math.cuh"]
+# (source, FMA contraction): the FP64 path is built without FMA so that it rounds
+# like the reference; the FP32-force instances use FMA.
+SOURCES = [("dem_kernels.cu", False), ("dem_sim.cu", False), ("dem_noalloc.cu", False), ("dem_step_fp32.cu", True),
+           ("packing.cpp", False)]
+HEADERS = ["dem_device.cuh", "dem_kernels.h", "dem_laws.cuh", "dem_laws_f32.cuh", "dem_math.cuh", "dem_common.cuh",
+           "dem_step.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -29,7 +33,7 @@ def needs_build() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS]
+    deps = [os.path.join(SRC, f) for f, _ in SOURCES] + [os.path.join(SRC, f) for f in HEADERS]
     deps += [os.path.join(HERE, "..", "include", h) for h in ("esys_dem.h", "esys_geometry.h")]
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
@@ -38,16 +42,26 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
-           "-o", LIB + ".tmp"] + [os.path.join(SRC, f) for f in SOURCES]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    objs, procs = [], []
+    for f, fma in SOURCES:
+        obj = os.path.join(HERE, "_build", f + ".o")
+        cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", f"--fmad={'true' if fma else 'false'}",
+               "-Xcompiler", "-fPIC", "-c", os.path.join(SRC, f), "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((f, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+        objs.append(obj)
+    for f, p in procs:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {f}:\n" + out + err)
+        if verbose:
+            sys.stderr.write(err)
+    r = subprocess.run([nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp"] + objs, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

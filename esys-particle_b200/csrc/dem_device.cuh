@@ -48,6 +48,7 @@ struct ParticleBuf {
   double4* vm;  // vx, vy, vz, mass
   double4* wi;  // wx, wy, wz, rotational inertia
   double4* qq;  // quaternion scalar, x, y, z
+  float4* vw;   // FP32 form: 2 per particle, (vx, vy, vz, wx), (wy, wz, 0, 0): one 32-byte sector
 };
 
 struct Particles {
@@ -57,6 +58,8 @@ struct Particles {
   double4* oldpos;       // position at the last neighbour search
   double4* force;        // last accumulated force  (w unused)
   double4* moment;       // last accumulated moment (w unused)
+  double4* force_eval;   // FP32 forces of an evaluation-only pass (precision check)
+  double4* moment_eval;
   unsigned* pflags;      // PF_* bits
   unsigned char* flagged;// set on both particles of a broken bond (CParticle::flag)
   int* id;
@@ -79,6 +82,8 @@ struct DynDev {
   const int2* adj;      // (partner slot, pair index | 0x80000000 when this particle is p1)
   const double4* hist_in;   // RotFriction: Ffric xyz, w = slipping + 2*touching
   double4* hist_out;
+  const float4* hist32_in;  // the same in the FP32 form
+  float4* hist32_out;
 };
 
 struct BondDev {

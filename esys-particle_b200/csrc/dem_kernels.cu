@@ -16,105 +16,11 @@
 
 #include "dem_device.cuh"
 #include "dem_kernels.h"
+#include "dem_common.cuh"
 #include "dem_laws.cuh"
+#include "dem_step.cuh"
 
 namespace dem {
-
-// ---------------------------------------------------------------------------
-// helpers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int cell_coord(double x, double p0, double dim, int g) {
-  return int(floor((x - p0) / dim)) - g;  // NeighborTable::index (ntable.hpp:128-140)
-}
-
-// Cell of a position, -1 when outside the local table.  Periodic x wraps.
-__device__ __forceinline__ int cell_of(const Grid& g, double x, double y, double z) {
-  if (!(isfinite(x) && isfinite(y) && isfinite(z))) return -1;
-  int ix = cell_coord(x, g.p0x, g.dim, g.gx);
-  int iy = cell_coord(y, g.p0y, g.dim, g.gy);
-  int iz = cell_coord(z, g.p0z, g.dim, g.gz);
-  if (g.circx) ix = ((ix % g.nx) + g.nx) % g.nx;
-  if (ix >= 0 && ix < g.nx && iy >= 0 && iy < g.ny && iz >= 0 && iz < g.nz) return (ix * g.ny + iy) * g.nz + iz;
-  return -1;
-}
-
-// NeighborTable::isInInner (ntable.hpp:212-233).
-__device__ __forceinline__ bool inner_of(const Grid& g, double x, double y, double z) {
-  int ix = cell_coord(x, g.p0x, g.dim, g.gx);
-  int iy = cell_coord(y, g.p0y, g.dim, g.gy);
-  int iz = cell_coord(z, g.p0z, g.dim, g.gz);
-  bool inx = g.circx ? true : (ix > 0 && ix < g.nx - 1);
-  if (g.nz < 3) return inx && iy > 0 && iy < g.ny - 1;
-  return inx && iy > 0 && iy < g.ny - 1 && iz > 0 && iz < g.nz - 1;
-}
-
-// Position of p2 as seen from p1: its periodic image nearest p1.
-__device__ __forceinline__ V image_of(const Grid& g, const V& x1, V x2) {
-  if (g.circx) {
-    double dx = x1.x - x2.x;
-    if (dx > 0.5 * g.Lx) x2.x += g.Lx;
-    else if (dx < -0.5 * g.Lx) x2.x -= g.Lx;
-  }
-  return x2;
-}
-
-// Neighbour-list predicate of NeighborTable::addPairsToList (ntable.hpp:471-489),
-// evaluated in canonical orientation (lo = lower id).
-__device__ __forceinline__ bool near_pair(const Grid& g, const double4& plo, const double4& phi) {
-  V xl = xyz(plo), xh = image_of(g, xl, xyz(phi));
-  double dist2 = norm2(xl - xh);
-  double dmax = plo.w + phi.w + g.alpha;
-  return dist2 <= (dmax * dmax);
-}
-
-// Visit the particles of the 27 cells around cell c (wrapping x when periodic).
-template <class F>
-__device__ __forceinline__ void for_neighbour_cells(const Grid& g, int c, const int* cell_start, const int* cell_list,
-                                                    F&& f) {
-  const int iz = c % g.nz, iy = (c / g.nz) % g.ny, ix = c / (g.nz * g.ny);
-  for (int dx = -1; dx <= 1; ++dx) {
-    int jx = ix + dx;
-    if (g.circx) jx = (jx + g.nx) % g.nx;
-    else if (jx < 0 || jx >= g.nx) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
-      int jy = iy + dy;
-      if (jy < 0 || jy >= g.ny) continue;
-      for (int dz = -1; dz <= 1; ++dz) {
-        int jz = iz + dz;
-        if (jz < 0 || jz >= g.nz) continue;
-        int cc = (jx * g.ny + jy) * g.nz + jz;
-        for (int k = cell_start[cc]; k < cell_start[cc + 1]; ++k) f(cell_list[k]);
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ unsigned long long pair_key(int a, int b) {
-  return ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
-}
-
-// Lower bound of key in sorted keys[lo, hi).
-__device__ __forceinline__ int lower_bound_key(const unsigned long long* keys, int lo, int hi, unsigned long long key) {
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (keys[mid] < key) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ bool has_key(const unsigned long long* keys, int n, unsigned long long key) {
-  int p = lower_bound_key(keys, 0, n, key);
-  return p < n && keys[p] == key;
-}
-
-// An intact bond of an excluding group with this (p1 slot, p2 slot) key?
-__device__ __forceinline__ bool excluded(const ExclDev& ex, unsigned long long key) {
-  for (int e = 0; e < ex.n; ++e) {
-    int p = lower_bound_key(ex.keys[e], 0, ex.count[e], key);
-    if (p < ex.count[e] && ex.keys[e][p] == key && ex.broken_step[e][p] == kBondAlive) return true;
-  }
-  return false;
-}
 
 // Single-block exclusive scan of n ints (in place allowed); total written to *total.
 __global__ void k_scan(const int* in, int* out, int n, int* total) {
@@ -242,9 +148,10 @@ __global__ void k_pairs_count(Grid g, Particles P, int cur, const int* cell_star
 // Write the pairs (p1 = i) into [start[i], start[i]+count[i]) sorted by p2 slot
 // and carry RotFriction history from the previous list when the old
 // interaction is persistent (PIS_ED::update, pi_storage_ed.hpp:93-128).
+template <class H>
 __global__ void k_pairs_write(Grid g, Particles P, int cur, const int* cell_start, const int* cell_list, ExclDev ex,
                               const int* start, unsigned long long* keys, int kind, const unsigned long long* old_keys,
-                              int old_n, const double4* old_hist, double4* hist) {
+                              int old_n, const H* old_hist, H* hist) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   int c = P.cell[i];
@@ -267,7 +174,7 @@ __global__ void k_pairs_write(Grid g, Particles P, int cur, const int* cell_star
   if (kind != 1) return;
   for (int k = s; k < s + n; ++k) {
     const int j = (int)(keys[k] & 0xffffffffu);
-    double4 h = make_double4(0.0, 0.0, 0.0, 0.0);
+    H h{};
     int p = lower_bound_key(old_keys, 0, old_n, keys[k]);
     if (p < old_n && old_keys[p] == keys[k]) {
       V x1 = xyz(pi), x2 = image_of(g, x1, xyz(P.buf[cur].pr[j]));
@@ -365,8 +272,9 @@ __global__ void k_newlist_write(Grid g, Particles P, const int* cell_start, cons
 
 // Merge sorted lists A (m, with history) and B (nb new pairs, fresh history);
 // equal keys keep A first (stable), as the reference appends new interactions.
-__global__ void k_merge(const unsigned long long* A, const double4* Ah, int m, const unsigned long long* B, int nb,
-                        unsigned long long* out, double4* outh, int kind) {
+template <class H>
+__global__ void k_merge(const unsigned long long* A, const H* Ah, int m, const unsigned long long* B, int nb,
+                        unsigned long long* out, H* outh, int kind) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < m) {
     // number of B elements strictly less than A[k]
@@ -380,7 +288,7 @@ __global__ void k_merge(const unsigned long long* A, const double4* Ah, int m, c
     int lo = 0, hi = m;
     while (lo < hi) { int mid = (lo + hi) >> 1; if (A[mid] <= B[b]) lo = mid + 1; else hi = mid; }
     out[b + lo] = B[b];
-    if (kind == 1) outh[b + lo] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (kind == 1) outh[b + lo] = H{};
   }
 }
 
@@ -481,293 +389,6 @@ __global__ void k_move_tagged(Particles P, int cur, int tag, double dx, double d
 }
 
 // ---------------------------------------------------------------------------
-// the timestep
-// ---------------------------------------------------------------------------
-template <int TPP>
-__device__ __forceinline__ double lane_sum(double v) {
-#pragma unroll
-  for (int o = 1; o < TPP; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-template <int TPP>
-__device__ __forceinline__ V lane_sum(V v) {
-  return mk(lane_sum<TPP>(v.x), lane_sum<TPP>(v.y), lane_sum<TPP>(v.z));
-}
-
-constexpr int kStepThreads = 256;
-constexpr int kStepWarps = kStepThreads / 32;
-
-// Interaction families compiled into a k_step instance (the host picks the
-// smallest instance that covers the groups present, so a friction-only run
-// does not carry the registers of the bond law).
-enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4 };
-
-template <bool ROT, int TPP, int FEAT>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(const StepArgs a) {
-  __shared__ double s_red[kStepWarps][kMaxWalls][3];
-  __shared__ bool s_last;
-  if (*a.stop) return;  // an earlier step of this chunk asked the host to intervene
-  const long long step = *a.step_counter + 1;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = tid / TPP;
-  const int lane = threadIdx.x % TPP;
-  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const bool valid = i < a.P.n;
-  const unsigned pf = valid ? a.P.pflags[i] : 0u;
-  const bool alive = valid && (pf & PF_ALIVE);
-  const ParticleBuf in = a.P.buf[a.cur];
-  const ParticleBuf out = a.P.buf[a.cur ^ 1];
-
-  double4 p4 = make_double4(0, 0, 0, 0), v4 = p4, w4 = p4, q4 = make_double4(1, 0, 0, 0);
-  if (alive) {
-    p4 = in.pr[i];
-    v4 = in.vm[i];
-    if (ROT) {
-      w4 = in.wi[i];
-      if (FEAT & F_BOND) q4 = in.qq[i];
-    }
-  }
-  const V xi = xyz(p4);
-  V F = mk(0.0, 0.0, 0.0), M = mk(0.0, 0.0, 0.0);
-
-  // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
-  //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.
-  for (int w = 0; w < a.nwall; ++w) {
-    V c = mk(0.0, 0.0, 0.0);
-    if (alive && lane == 0 && (pf & (1u << (PF_WALL_SHIFT + w)))) {
-      const WallDev W = a.walls[w];
-      V f;
-      if (law_wall(W.k, mk(W.ox, W.oy, W.oz), mk(W.nx, W.ny, W.nz), xi, p4.w, f)) {
-        F += f;
-        if (pf & (1u << (PF_INNER_SHIFT + w))) c = f;  // CWall::addForce(-F): m_force -= -F
-      }
-    }
-    double cx = c.x, cy = c.y, cz = c.z;
-    if (__any_sync(0xffffffffu, cx != 0.0 || cy != 0.0 || cz != 0.0)) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        cx += __shfl_down_sync(0xffffffffu, cx, o);
-        cy += __shfl_down_sync(0xffffffffu, cy, o);
-        cz += __shfl_down_sync(0xffffffffu, cz, o);
-      }
-    }
-    if (wlane == 0) { s_red[warp][w][0] = cx; s_red[warp][w][1] = cy; s_red[warp][w][2] = cz; }
-  }
-
-  // 2. body forces (BodyForceGroup::calcForces, BodyForceGroup.hpp:54-65): F += g * m
-  if (alive && lane == 0)
-    for (int k = 0; k < a.ngrav; ++k) F += mk(a.grav[k][0], a.grav[k][1], a.grav[k][2]) * v4.w;
-
-  // 3. dynamic pair groups (PIS_NE / PIS_ED::calcForces)
-  V Fp = mk(0.0, 0.0, 0.0), Mp = mk(0.0, 0.0, 0.0);
-  if ((FEAT & (F_ELASTIC | F_FRIC)) && alive) {
-    for (int d = 0; d < a.ndyn; ++d) {
-      const DynDev& G = a.dyn[d];
-      const int e0 = G.adj_start[i], e1 = G.adj_start[i + 1];
-      for (int e = e0 + lane; e < e1; e += TPP) {
-        const int2 en = G.adj[e];
-        const int j = en.x;
-        const bool isp1 = en.y < 0;
-        const int k = en.y & 0x7fffffff;
-        const double4 pj = in.pr[j];
-        // canonical orientation: p1 = lower id
-        const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
-        const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
-        if (G.kind == 0) {
-          if constexpr ((FEAT & F_ELASTIC) != 0) {
-            V f;
-            if (law_elastic(elastic_k(G.k, G.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, f)) {
-              if (isp1) Fp += -1.0 * f; else Fp += f;
-            }
-          }
-        } else {
-          if constexpr (ROT && (FEAT & F_FRIC) != 0) {
-            const double4 vj = in.vm[j], wj = in.wi[j];
-            const double4 va = isp1 ? v4 : vj, vb = isp1 ? vj : v4;
-            const double4 wa = isp1 ? w4 : wj, wb = isp1 ? wj : w4;
-            const double4 h = G.hist_in[k];
-            double keff, kseff;
-            friction_k(G.k, G.ks, G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
-            FricOut o;
-            law_friction(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, xyz(va), xyz(wa), x2, pb.w, xyz(vb), xyz(wb),
-                         mk(h.x, h.y, h.z), (((int)h.w) & 1) != 0, o);
-            if (isp1) {
-              Fp += -1.0 * o.fn;
-              Mp += o.M1;
-              Fp += o.Ffric;
-              G.hist_out[k] = make_double4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
-                                           (o.slipping ? 1.0 : 0.0) + (o.touching ? 2.0 : 0.0));
-            } else {
-              Fp += o.fn;
-              Mp += o.M2;
-              Fp += -1.0 * o.Ffric;
-            }
-          }
-        }
-      }
-    }
-  }
-
-  // 4. bonded groups (PIS_EB::calcForces) + failure test (PIS_EB::update at the next step)
-  V Fb = mk(0.0, 0.0, 0.0), Mb = mk(0.0, 0.0, 0.0);
-  if constexpr (ROT && (FEAT & F_BOND) != 0) {
-    if (alive) {
-      for (int d = 0; d < a.nbond; ++d) {
-        const BondDev& B = a.bond[d];
-        const int e0 = B.adj_start[i], e1 = B.adj_start[i + 1];
-        for (int e = e0 + lane; e < e1; e += TPP) {
-          const int2 en = B.adj[e];
-          const int k = en.y & 0x7fffffff;
-          if (B.broken_step[k] <= step) continue;  // removed by an earlier update
-          const int j = en.x;
-          const bool isp1 = en.y < 0;
-          const double4 pj = in.pr[j], qj = in.qq[j];
-          const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
-          const double4 qa = isp1 ? q4 : qj, qb = isp1 ? qj : q4;
-          const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
-          const double4 D0 = B.D0[k];
-          const V mD = xyz(D0);
-          const double dist0 = sqrt(dot(mD, mD));
-          const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
-          BondOut o;
-          law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
-          if (isp1) {
-            Fb += o.force;
-            Mb += o.moment1;
-            if (bond_broken(K, o, B.truncated)) {
-              B.broken_step[k] = (int)(step + 1);
-              a.P.flagged[i] = 1;
-              a.P.flagged[j] = 1;
-              int slot = atomicAdd(B.nevents, 1);
-              if (slot < B.cap_events) {
-                B.events[3 * slot] = a.P.id[i];
-                B.events[3 * slot + 1] = a.P.id[j];
-                B.events[3 * slot + 2] = (int)(step + 1);
-              } else {
-                atomicOr(a.ctrl, CTRL_OVERFLOW);
-              }
-              atomicOr(a.ctrl, CTRL_BROKE);
-            }
-          } else {
-            Fb += -1.0 * o.force;
-            Mb += o.moment2;
-          }
-        }
-      }
-    }
-  }
-
-  // fixed-order combination of the lanes' partial sums
-  if (TPP > 1) {
-    Fp = lane_sum<TPP>(Fp);
-    Mp = lane_sum<TPP>(Mp);
-    if (FEAT & F_BOND) {
-      Fb = lane_sum<TPP>(Fb);
-      Mb = lane_sum<TPP>(Mb);
-    }
-  }
-
-  if (alive && lane == 0) {
-    F += Fp;
-    M += Mp;
-    F += Fb;
-    M += Mb;
-    const double2 iv = a.P.inv[i];
-    // 5. damping, last (SubLattice.hpp:2140-2145): "Damping" then "RotDamping"
-    if (a.damp_lin) F += damping_force(xyz(v4), F, iv.x, v4.w, a.visc_lin, a.dt_lin, a.iter_lin);
-    if (ROT && a.damp_rot) M += damping_force(xyz(w4), M, iv.y, w4.w, a.visc_rot, a.dt_rot, a.iter_rot);
-    // 6. integration (CRotParticle::integrate + rescale, RotParticle.cpp:277-321; Particle.cpp:257-274)
-    const double dt = a.dt;
-    V v = xyz(v4), x = xi;
-    if (ROT) {
-      if (!(FEAT & F_BOND)) q4 = in.qq[i];
-      V w = xyz(w4);
-      Qd q{q4.x, mk(q4.y, q4.z, q4.w)};
-      if (pf & PF_ROT) {
-        w += (dt * iv.y) * M;
-        const Qd dq = qmul(Qd{0.0, w}, q);
-        const double c = dt / 2.0;
-        q.s += c * dq.s;
-        q.v += c * dq.v;
-      } else {
-        w = mk(0.0, 0.0, 0.0);
-      }
-      const double module = sqrt(q.s * q.s + q.v.x * q.v.x + q.v.y * q.v.y + q.v.z * q.v.z);
-      if (module != 0.0) {
-        const double inverse = 1.0 / module;
-        q.s = inverse * q.s;
-        q.v = inverse * q.v;
-      }
-      out.wi[i] = d4(w, w4.w);
-      out.qq[i] = make_double4(q.s, q.v.x, q.v.y, q.v.z);
-    }
-    if (pf & PF_DYN) {
-      v += F * iv.x * dt;
-      x += v * dt;
-    }
-    out.pr[i] = d4(x, p4.w);
-    out.vm[i] = d4(v, v4.w);
-    if (a.store_forces) {
-      a.P.force[i] = d4(F, 0.0);
-      if (ROT) a.P.moment[i] = d4(M, 0.0);
-    }
-    // 7. displacement check for the next step (TSubLattice::checkNeighbors)
-    const double4 op = a.P.oldpos[i];
-    const V dd = mk(x.x - op.x, x.y - op.y, x.z - op.z);
-    if (dot(dd, dd) > a.half_alpha_sq) atomicOr(a.ctrl, CTRL_REBUILD);
-  }
-
-  // per-block wall reactions (fixed order over warps), then the last block finishes the step
-  const int nw3 = a.nwall * 3;
-  __syncthreads();
-  if (threadIdx.x < nw3) {
-    const int w = threadIdx.x / 3, c = threadIdx.x % 3;
-    double acc = 0.0;
-    for (int k = 0; k < kStepWarps; ++k) acc += s_red[k][w][c];
-    a.wall_partial[((size_t)blockIdx.x * kMaxWalls + w) * 3 + c] = acc;
-    __threadfence();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned prev = atomicInc(a.block_counter, gridDim.x - 1);
-    s_last = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  // wall reactions: thread t sums blocks t, t+256, ... (fixed assignment), then a fixed tree
-  for (int wc = 0; wc < nw3; ++wc) {
-    const int w = wc / 3, c = wc % 3;
-    double acc = 0.0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-      acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (wlane == 0) s_red[warp][0][0] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
-      a.wall_force[3 * w + c] = t;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    for (int w = 0; w < a.nwall; ++w) {  // native wall loader: origin += v*dt per step (WallLoaderRunnable)
-      WallDev* W = a.walls + w;
-      if (a.wall_vel[3 * w] != 0.0 || a.wall_vel[3 * w + 1] != 0.0 || a.wall_vel[3 * w + 2] != 0.0) {
-        W->ox += a.wall_vel[3 * w] * a.dt;
-        W->oy += a.wall_vel[3 * w + 1] * a.dt;
-        W->oz += a.wall_vel[3 * w + 2] * a.dt;
-      }
-    }
-    *a.step_counter = step;
-    volatile int* ctrl = a.ctrl;
-    if (*ctrl) *a.stop = 1;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // CEWallInteractionGroup::applyForce (EWallInteractionGroup.hpp:93-164): servo
 // iteration of one wall against its candidates' elastic contacts.  One block.
 // ---------------------------------------------------------------------------
@@ -853,13 +474,20 @@ void launch_pairs_count(const Grid& g, const Particles& P, int cur, const int* c
                         int* count, cudaStream_t s) {
   if (P.n) k_pairs_count<<<nblk(P.n, 128), 128, 0, s>>>(g, P, cur, cs, cl, ex, count);
 }
+template <class H>
 void launch_pairs_write(const Grid& g, const Particles& P, int cur, const int* cs, const int* cl, const ExclDev& ex,
                         const int* start, unsigned long long* keys, int kind, const unsigned long long* old_keys,
-                        int old_n, const double4* old_hist, double4* hist, cudaStream_t s) {
+                        int old_n, const H* old_hist, H* hist, cudaStream_t s) {
   if (P.n)
-    k_pairs_write<<<nblk(P.n, 128), 128, 0, s>>>(g, P, cur, cs, cl, ex, start, keys, kind, old_keys, old_n, old_hist,
-                                                  hist);
+    k_pairs_write<H><<<nblk(P.n, 128), 128, 0, s>>>(g, P, cur, cs, cl, ex, start, keys, kind, old_keys, old_n,
+                                                     old_hist, hist);
 }
+template void launch_pairs_write<double4>(const Grid&, const Particles&, int, const int*, const int*, const ExclDev&,
+                                          const int*, unsigned long long*, int, const unsigned long long*, int,
+                                          const double4*, double4*, cudaStream_t);
+template void launch_pairs_write<float4>(const Grid&, const Particles&, int, const int*, const int*, const ExclDev&,
+                                         const int*, unsigned long long*, int, const unsigned long long*, int,
+                                         const float4*, float4*, cudaStream_t);
 void launch_adj(const unsigned long long* keys, int m, int n, int* adj_count, int* p1_start, int* adj_start,
                 int* adj_cursor, int2* adj, int* total, cudaStream_t s) {
   cudaMemsetAsync(adj_count, 0, sizeof(int) * (n + 1), s);
@@ -880,9 +508,41 @@ void launch_newlist_write(const Grid& g, const Particles& P, const int* cs, cons
                           unsigned long long* out, cudaStream_t s) {
   if (P.n) k_newlist_write<<<nblk(P.n, 128), 128, 0, s>>>(g, P, cs, cl, ex, keys, m, check_in, start, out);
 }
-void launch_merge(const unsigned long long* A, const double4* Ah, int m, const unsigned long long* B, int nb,
-                  unsigned long long* out, double4* outh, int kind, cudaStream_t s) {
-  if (m + nb) k_merge<<<nblk(m + nb, 256), 256, 0, s>>>(A, Ah, m, B, nb, out, outh, kind);
+template <class H>
+void launch_merge(const unsigned long long* A, const H* Ah, int m, const unsigned long long* B, int nb,
+                  unsigned long long* out, H* outh, int kind, cudaStream_t s) {
+  if (m + nb) k_merge<H><<<nblk(m + nb, 256), 256, 0, s>>>(A, Ah, m, B, nb, out, outh, kind);
+}
+template void launch_merge<double4>(const unsigned long long*, const double4*, int, const unsigned long long*, int,
+                                    unsigned long long*, double4*, int, cudaStream_t);
+template void launch_merge<float4>(const unsigned long long*, const float4*, int, const unsigned long long*, int,
+                                   unsigned long long*, float4*, int, cudaStream_t);
+
+// FP32 copies of velocity and spin for the FP32-force form (one 32-byte record per particle).
+__global__ void k_sync_vw(Particles P, int cur) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  const double4 v = P.buf[cur].vm[i], w = P.buf[cur].wi[i];
+  P.buf[cur].vw[2 * i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)w.x);
+  P.buf[cur].vw[2 * i + 1] = make_float4((float)w.y, (float)w.z, 0.f, 0.f);
+}
+void launch_sync_vw(const Particles& P, int cur, cudaStream_t s) {
+  if (P.n) k_sync_vw<<<nblk(P.n, 256), 256, 0, s>>>(P, cur);
+}
+
+// History conversion when the precision form changes (FP64 <-> FP32 records).
+__global__ void k_hist_to_f32(int m, const double4* in, float4* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) { double4 h = in[k]; out[k] = make_float4((float)h.x, (float)h.y, (float)h.z, (float)h.w); }
+}
+__global__ void k_hist_to_f64(int m, const float4* in, double4* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) { float4 h = in[k]; out[k] = make_double4(h.x, h.y, h.z, h.w); }
+}
+void launch_hist_convert(int m, const double4* d, float4* f, bool to_f32, cudaStream_t s) {
+  if (!m) return;
+  if (to_f32) k_hist_to_f32<<<nblk(m, 256), 256, 0, s>>>(m, d, f);
+  else k_hist_to_f64<<<nblk(m, 256), 256, 0, s>>>(m, f, const_cast<double4*>(d));
 }
 void launch_clear_flags(int n, unsigned char* flagged, cudaStream_t s) {
   if (n) k_clear_flags<<<nblk(n, 256), 256, 0, s>>>(n, flagged);
@@ -918,28 +578,18 @@ void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const
   k_wall_servo<<<1, 1024, 0, s>>>(P, cur, w, walls, F[0], F[1], F[2]);
 }
 
-int step_grid(int n, int tpp) { return nblk((long long)(n > 0 ? n : 1) * tpp, kStepThreads); }
+int step_grid(int n, int tpp) { return step_blocks(n, tpp); }
 
-template <bool R, int FEAT>
-static void launch_step_tpp(const StepArgs& a, int tpp, int grid, cudaStream_t s) {
-  switch (tpp) {
-    case 1: k_step<R, 1, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
-    case 2: k_step<R, 2, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
-    case 4: k_step<R, 4, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
-    default: k_step<R, 8, FEAT><<<grid, kStepThreads, 0, s>>>(a); break;
-  }
-}
-
+// FP64 instances (this translation unit is built with --fmad=false).
 void launch_step(const StepArgs& a, bool rot, int tpp, cudaStream_t s) {
-  const int grid = step_grid(a.P.n, tpp);
   bool el = false, fr = false;
   for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
   const bool bd = a.nbond > 0;
-  if (!rot) return launch_step_tpp<false, F_ELASTIC>(a, tpp, grid, s);
-  if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC>(a, tpp, grid, s);
-  if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC>(a, tpp, grid, s);
-  if (bd && !el) return launch_step_tpp<true, F_FRIC | F_BOND>(a, tpp, grid, s);
-  return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BOND>(a, tpp, grid, s);
+  if (!rot) return launch_step_tpp<false, F_ELASTIC, false, false>(a, tpp, s);
+  if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC, false, false>(a, tpp, s);
+  if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC, false, false>(a, tpp, s);
+  if (bd && !el) return launch_step_tpp<true, F_FRIC | F_BOND, false, false>(a, tpp, s);
+  return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BOND, false, false>(a, tpp, s);
 }
 
 }  // namespace dem

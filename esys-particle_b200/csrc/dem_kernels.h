@@ -11,9 +11,10 @@ void launch_scatter_cells(const Particles& P, const int* cell_start, int* cursor
 void launch_sort_cells(int ncell, const int* cell_start, int* cell_list, cudaStream_t s);
 void launch_pairs_count(const Grid& g, const Particles& P, int cur, const int* cs, const int* cl, const ExclDev& ex,
                         int* count, cudaStream_t s);
+template <class H>
 void launch_pairs_write(const Grid& g, const Particles& P, int cur, const int* cs, const int* cl, const ExclDev& ex,
                         const int* start, unsigned long long* keys, int kind, const unsigned long long* old_keys,
-                        int old_n, const double4* old_hist, double4* hist, cudaStream_t s);
+                        int old_n, const H* old_hist, H* hist, cudaStream_t s);
 void launch_adj(const unsigned long long* keys, int m, int n, int* adj_count, int* p1_start, int* adj_start,
                 int* adj_cursor, int2* adj, int* total, cudaStream_t s);
 void launch_newlist_count(const Grid& g, const Particles& P, const int* cs, const int* cl, const ExclDev& ex,
@@ -21,8 +22,11 @@ void launch_newlist_count(const Grid& g, const Particles& P, const int* cs, cons
 void launch_newlist_write(const Grid& g, const Particles& P, const int* cs, const int* cl, const ExclDev& ex,
                           const unsigned long long* keys, int m, int check_in, const int* start,
                           unsigned long long* out, cudaStream_t s);
-void launch_merge(const unsigned long long* A, const double4* Ah, int m, const unsigned long long* B, int nb,
-                  unsigned long long* out, double4* outh, int kind, cudaStream_t s);
+template <class H>
+void launch_merge(const unsigned long long* A, const H* Ah, int m, const unsigned long long* B, int nb,
+                  unsigned long long* out, H* outh, int kind, cudaStream_t s);
+void launch_sync_vw(const Particles& P, int cur, cudaStream_t s);
+void launch_hist_convert(int m, const double4* d, float4* f, bool to_f32, cudaStream_t s);
 void launch_clear_flags(int n, unsigned char* flagged, cudaStream_t s);
 void launch_pairs_alive(const unsigned long long* keys, int m, const unsigned* pflags, int* keep, cudaStream_t s);
 void launch_compact(const unsigned long long* keys, const double4* hist, int m, const int* keep, const int* pos,
@@ -38,5 +42,6 @@ void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, c
 void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s);
 int step_grid(int n, int tpp);
 void launch_step(const StepArgs& a, bool rot, int tpp, cudaStream_t s);
+void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, cudaStream_t s);
 
 }  // namespace dem

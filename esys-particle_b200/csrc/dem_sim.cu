@@ -72,11 +72,13 @@ struct DynGroup {
   int update_ts = 0;
   DBuf<unsigned long long> keys, keys_spare, cand;
   DBuf<double4> hist[2], hist_spare;  // hist[c]: read by the step whose particle input buffer is c
+  DBuf<float4> hist32[2], hist32_spare;  // the same records in the FP32-force form
   DBuf<int> adj_start, adj_count, adj_cursor, p1_start;
   DBuf<int2> adj;
   void release() {
     keys.release(); keys_spare.release(); cand.release();
     hist[0].release(); hist[1].release(); hist_spare.release();
+    hist32[0].release(); hist32[1].release(); hist32_spare.release();
     adj_start.release(); adj_count.release(); adj_cursor.release(); p1_start.release(); adj.release();
   }
 };
@@ -107,6 +109,7 @@ struct DemSim {
   int tpp = 0;           // 0 = choose from the mean adjacency length
   int chunk = 64;        // steps launched per host round trip
   int store_forces = 1;
+  int fp32 = 0;          // 1 = FP32-force / FP64-integration form
   // particles
   int n = 0, cap = 0;
   Particles P{};
@@ -165,7 +168,8 @@ struct DemSim {
     for (auto& d : dyn) d.second.release();
     for (auto& b : bond) b.second.release();
     void* ps[] = {P.buf[0].pr, P.buf[0].vm, P.buf[0].wi, P.buf[0].qq, P.buf[1].pr, P.buf[1].vm, P.buf[1].wi,
-                  P.buf[1].qq, P.inv, P.oldpos, P.force, P.moment, P.pflags, P.flagged, P.id, P.tag, P.cell};
+                  P.buf[1].qq, P.buf[0].vw, P.buf[1].vw, P.inv, P.oldpos, P.force, P.moment, P.force_eval,
+                  P.moment_eval, P.pflags, P.flagged, P.id, P.tag, P.cell};
     for (void* p : ps) if (p) cudaFree(p);
     cell_count.release(); cell_start.release(); cell_cursor.release(); cell_list.release();
     scratch_i.release(); scratch_j.release(); scalars.release();
@@ -240,6 +244,7 @@ struct DemSim {
     for (int b = 0; b < 2; ++b) {
       grow_array(P.buf[b].pr, n, nc); grow_array(P.buf[b].vm, n, nc);
       grow_array(P.buf[b].wi, n, nc); grow_array(P.buf[b].qq, n, nc);
+      grow_array(P.buf[b].vw, 2 * n, 2 * nc);
     }
     grow_array(P.inv, n, nc); grow_array(P.oldpos, n, nc); grow_array(P.force, n, nc); grow_array(P.moment, n, nc);
     grow_array(P.pflags, n, nc); grow_array(P.flagged, n, nc); grow_array(P.id, n, nc); grow_array(P.tag, n, nc);
@@ -253,6 +258,9 @@ struct DemSim {
     std::vector<double2> inv;
     std::vector<unsigned> pf;
     std::vector<int> ids, tags;
+    // Slots follow the caller's order (the reference's particle-list order).  A spatial
+    // (Z-curve) slot order was measured: it raised L1 hits but mixed particle sizes
+    // within warps and made the step slower on the shear-cell packing.
     for (int i = 0; i < cnt; ++i) {
       // NeighborTable::insert drops particles outside the table (ntable.hpp:243-258)
       auto cc = [&](double x, double p0, int gg) { return int(std::floor((x - p0) / g.dim)) - gg; };
@@ -312,6 +320,77 @@ struct DemSim {
     for (auto& b : bond) build_adjacency(b.second.keys, b.second.nb, b.second.adj_start, b.second.adj_count,
                                          b.second.adj_cursor, b.second.p1_start, b.second.adj);
     sync();
+  }
+
+  // Switch between the FP64 form and the FP32-force form, converting friction history.
+  void set_precision(int want) {
+    want = want ? 1 : 0;
+    if (want == fp32) return;
+    for (auto& d : dyn) {
+      DynGroup& G = d.second;
+      if (G.kind != 1 || G.m == 0) continue;
+      const int m = G.m;
+      for (int b = 0; b < 2; ++b) { G.hist[b].reserve(m); G.hist32[b].reserve(m); }
+      launch_hist_convert(m, G.hist[cur].p, G.hist32[cur].p, want == 1, s);
+    }
+    sync();
+    fp32 = want;
+  }
+
+  // Precision check of the FP32-force form on the current state of an FP64 run:
+  // FP32 forces of this state (evaluation pass), then one FP64 step; returns
+  // [0] max|dF| / max|F|, [1] max|dM| / max|M|, [2] median and [3] 99th percentile of
+  // |dF_i| / |F_i| over particles with |F_i| > 1e-9 max|F|, [4] particles compared.
+  void precision_check(double* out) {
+    if (fp32) throw std::invalid_argument("precision check runs from the FP64 form");
+    if (first) { search_neighbors(); first = false; }
+    if (pending_ctrl & CTRL_REBUILD) search_neighbors();
+    update_interactions((pending_ctrl & CTRL_BROKE) != 0);
+    pending_ctrl = 0;
+    if (!P.force_eval) {
+      DEM_CUDA(cudaMalloc(&P.force_eval, sizeof(double4) * (size_t)cap));
+      DEM_CUDA(cudaMalloc(&P.moment_eval, sizeof(double4) * (size_t)cap));
+    }
+    const int t_pp = pick_tpp();
+    d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
+    launch_sync_vw(P, cur, s);
+    StepArgs ea = make_args(cur);
+    launch_step_fp32(ea, rot != 0, t_pp, true, s);
+    const int keep = chunk;
+    chunk = 1;
+    step(1);
+    chunk = keep;
+    std::vector<double4> f(n), fe(n), m(n), me(n);
+    std::vector<unsigned> pf(n);
+    DEM_CUDA(cudaMemcpyAsync(f.data(), P.force, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+    DEM_CUDA(cudaMemcpyAsync(fe.data(), P.force_eval, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+    DEM_CUDA(cudaMemcpyAsync(m.data(), P.moment, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+    DEM_CUDA(cudaMemcpyAsync(me.data(), P.moment_eval, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+    DEM_CUDA(cudaMemcpyAsync(pf.data(), P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s));
+    sync();
+    auto nrm = [](const double4& a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); };
+    auto dif = [](const double4& a, const double4& b) {
+      const double x = a.x - b.x, y = a.y - b.y, z = a.z - b.z;
+      return std::sqrt(x * x + y * y + z * z);
+    };
+    double fmax = 0, mmax = 0, dfmax = 0, dmmax = 0;
+    for (int i = 0; i < n; ++i) {
+      if (!(pf[i] & PF_ALIVE)) continue;
+      fmax = std::max(fmax, nrm(f[i])); mmax = std::max(mmax, nrm(m[i]));
+      dfmax = std::max(dfmax, dif(f[i], fe[i])); dmmax = std::max(dmmax, dif(m[i], me[i]));
+    }
+    std::vector<double> rel;
+    for (int i = 0; i < n; ++i) {
+      if (!(pf[i] & PF_ALIVE)) continue;
+      const double a = nrm(f[i]);
+      if (a > 1e-9 * fmax) rel.push_back(dif(f[i], fe[i]) / a);
+    }
+    std::sort(rel.begin(), rel.end());
+    out[0] = fmax > 0 ? dfmax / fmax : 0.0;
+    out[1] = mmax > 0 ? dmmax / mmax : 0.0;
+    out[2] = rel.empty() ? 0.0 : rel[rel.size() / 2];
+    out[3] = rel.empty() ? 0.0 : rel[std::min(rel.size() - 1, (size_t)(0.99 * rel.size()))];
+    out[4] = (double)rel.size();
   }
 
   // Bulk state update of existing particles (rows = slots when id is NULL).
@@ -395,12 +474,23 @@ struct DemSim {
     c_launches += 3;
     G.keys_spare.reserve(std::max(m, 1));
     if (G.kind == 1) G.hist_spare.reserve(std::max(m, 1));
-    launch_pairs_write(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind, G.keys.p, G.m,
-                       G.hist[cur].p, G.hist_spare.p, s);
+    if (fp32) {
+      if (G.kind == 1) G.hist32_spare.reserve(std::max(m, 1));
+      launch_pairs_write<float4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind,
+                                 G.keys.p, G.m, G.hist32[cur].p, G.hist32_spare.p, s);
+    } else {
+      launch_pairs_write<double4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind,
+                                  G.keys.p, G.m, G.hist[cur].p, G.hist_spare.p, s);
+    }
     std::swap(G.keys, G.keys_spare);
     if (G.kind == 1) {
-      std::swap(G.hist[cur], G.hist_spare);
-      G.hist[cur ^ 1].reserve(std::max(m, 1));
+      if (fp32) {
+        std::swap(G.hist32[cur], G.hist32_spare);
+        G.hist32[cur ^ 1].reserve(std::max(m, 1));
+      } else {
+        std::swap(G.hist[cur], G.hist_spare);
+        G.hist[cur ^ 1].reserve(std::max(m, 1));
+      }
     }
     G.m = m;
     build_adjacency(G.keys, m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
@@ -422,12 +512,22 @@ struct DemSim {
       launch_newlist_write(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_j.p, G.cand.p, s);
       const int m2 = G.m + nb;
       G.keys_spare.reserve(m2);
-      if (G.kind == 1) G.hist_spare.reserve(m2);
-      launch_merge(G.keys.p, G.hist[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist_spare.p, G.kind, s);
+      if (fp32) {
+        if (G.kind == 1) G.hist32_spare.reserve(m2);
+        launch_merge<float4>(G.keys.p, G.hist32[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist32_spare.p, G.kind, s);
+      } else {
+        if (G.kind == 1) G.hist_spare.reserve(m2);
+        launch_merge<double4>(G.keys.p, G.hist[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist_spare.p, G.kind, s);
+      }
       std::swap(G.keys, G.keys_spare);
       if (G.kind == 1) {
-        std::swap(G.hist[cur], G.hist_spare);
-        G.hist[cur ^ 1].reserve(m2);
+        if (fp32) {
+          std::swap(G.hist32[cur], G.hist32_spare);
+          G.hist32[cur ^ 1].reserve(m2);
+        } else {
+          std::swap(G.hist[cur], G.hist_spare);
+          G.hist[cur ^ 1].reserve(m2);
+        }
       }
       G.m = m2;
       build_adjacency(G.keys, G.m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
@@ -525,6 +625,7 @@ struct DemSim {
       D.scaling = G.scaling; D.meanR = G.meanR;
       D.adj_start = G.adj_start.p; D.adj = G.adj.p;
       D.hist_in = G.hist[c].p; D.hist_out = G.hist[c ^ 1].p;
+      D.hist32_in = G.hist32[c].p; D.hist32_out = G.hist32[c ^ 1].p;
     }
     a.nbond = 0;
     for (auto& b : bond) {
@@ -583,9 +684,11 @@ struct DemSim {
         if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
         DEM_CUDA(cudaEventRecord(ev0, s));
       }
+      if (fp32) launch_sync_vw(P, cur, s);
       for (int j = 0; j < k; ++j) {
         StepArgs a = make_args((cur + j) & 1);
-        launch_step(a, rot != 0, t_pp, s);
+        if (fp32) launch_step_fp32(a, rot != 0, t_pp, false, s);
+        else launch_step(a, rot != 0, t_pp, s);
       }
       DEM_CUDA(cudaGetLastError());
       if (profile) DEM_CUDA(cudaEventRecord(ev1, s));
@@ -622,6 +725,8 @@ namespace {
 template <class F>
 int guard(dem_sim* h, F&& f) {
   DemSim* s = reinterpret_cast<DemSim*>(h);
+  if (!s) return DEM_ERR_ARG;
+  (void)cudaGetLastError();  // every runtime call is checked where it is made; drop a reported, non-sticky error
   try {
     return f(*s);
   } catch (const dem::CudaError& e) {
@@ -984,9 +1089,14 @@ int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* sta
       dem::DynGroup& G = d->second;
       std::vector<unsigned long long> keys(G.m);
       std::vector<double4> hist(G.kind == 1 ? G.m : 0);
+      std::vector<float4> hist32(G.kind == 1 && s.fp32 ? G.m : 0);
       if (G.m) DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
-      if (G.kind == 1 && G.m) DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
+      if (G.kind == 1 && G.m) {
+        if (s.fp32) DEM_CUDA(cudaMemcpyAsync(hist32.data(), G.hist32[s.cur].p, sizeof(float4) * G.m, cudaMemcpyDeviceToHost, s.s));
+        else DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
+      }
       s.sync();
+      for (size_t q = 0; q < hist32.size(); ++q) hist[q] = make_double4(hist32[q].x, hist32[q].y, hist32[q].z, hist32[q].w);
       for (int i = 0; i < G.m; ++i) {
         id1[i] = s.h_id[(int)(keys[i] >> 32)];
         id2[i] = s.h_id[(int)(keys[i] & 0xffffffffu)];
@@ -1084,6 +1194,14 @@ int dem_set_particles(dem_sim* h, int n, const int* id, const double* pos, const
   return guard(h, [&](DemSim& s) { return s.set_particles(n, id, pos, vel, angvel, quat); });
 }
 
+int dem_precision_check(dem_sim* h, double* out) {
+  return guard(h, [&](DemSim& s) {
+    if (!out) throw std::invalid_argument("null output");
+    s.precision_check(out);
+    return DEM_OK;
+  });
+}
+
 int dem_set_option(dem_sim* h, const char* key, double value) {
   return guard(h, [&](DemSim& s) {
     std::string k = key ? key : "";
@@ -1098,6 +1216,9 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.store_forces = value != 0;
     } else if (k == "profile") {
       s.profile = value != 0;
+    } else if (k == "precision") {
+      if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");
+      s.set_precision(value == 32);
     } else {
       throw std::invalid_argument("unknown option " + k);
     }

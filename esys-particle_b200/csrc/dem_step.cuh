@@ -1,0 +1,428 @@
+// The timestep kernel k_step, shared by the FP64 form (dem_kernels.cu, built
+// with --fmad=false) and the FP32-force form (dem_step_fp32.cu).
+//
+// One launch = one CLatticeMaster::runOneStep force + integration phase for all
+// particles (TSubLattice::zeroForces / calcForces / integrate,
+// Parallel/SubLattice.hpp:2066-2236) plus the neighbour check of the next step
+// (checkNeighbors, :2473-2519).
+//
+// Template parameters:
+//   ROT   RotSphere (CRotParticle) vs NRotSphere (CParticle)
+//   TPP   lanes per particle (1, 2, 4, 8): they stride over the particle's
+//         adjacency and combine with a fixed-order butterfly
+//   FEAT  interaction families compiled in (F_ELASTIC, F_FRIC, F_BOND)
+//   FP32  pair forces in FP32 (positions, contact detection, overlap and
+//         integration in FP64; Kahan-compensated FP32 accumulation)
+//   EVAL  FP32 evaluation-only pass: forces of the current state into
+//         force_eval / moment_eval, nothing else written (precision check)
+#pragma once
+#include "dem_common.cuh"
+#include "dem_laws.cuh"
+#include "dem_laws_f32.cuh"
+
+namespace dem {
+
+template <int TPP>
+__device__ __forceinline__ double lane_sum(double v) {
+#pragma unroll
+  for (int o = 1; o < TPP; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int TPP>
+__device__ __forceinline__ float lane_sumf(float v) {
+#pragma unroll
+  for (int o = 1; o < TPP; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int TPP>
+__device__ __forceinline__ V lane_sum(V v) {
+  return mk(lane_sum<TPP>(v.x), lane_sum<TPP>(v.y), lane_sum<TPP>(v.z));
+}
+template <int TPP>
+__device__ __forceinline__ Vf lane_sumf(Vf v) {
+  return mk(lane_sumf<TPP>(v.x), lane_sumf<TPP>(v.y), lane_sumf<TPP>(v.z));
+}
+
+constexpr int kStepThreads = 256;
+constexpr int kStepWarps = kStepThreads / 32;
+
+// Interaction families compiled into a k_step instance (the host picks the
+// smallest instance that covers the groups present, so a friction-only run
+// does not carry the registers of the bond law).
+enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4 };
+
+template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(const StepArgs a) {
+  __shared__ double s_red[kStepWarps][kMaxWalls][3];
+  __shared__ bool s_last;
+  if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
+  const long long step = *a.step_counter + 1;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = tid / TPP;
+  const int lane = threadIdx.x % TPP;
+  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool valid = i < a.P.n;
+  const unsigned pf = valid ? a.P.pflags[i] : 0u;
+  const bool alive = valid && (pf & PF_ALIVE);
+  const ParticleBuf in = a.P.buf[a.cur];
+  const ParticleBuf out = a.P.buf[a.cur ^ 1];
+
+  double4 p4 = make_double4(0, 0, 0, 0), v4 = p4, w4 = p4, q4 = make_double4(1, 0, 0, 0);
+  if (alive) {
+    p4 = ldg4(in.pr + i);
+    v4 = ldg4(in.vm + i);
+    if (ROT) {
+      w4 = ldg4(in.wi + i);
+      if (FEAT & F_BOND) q4 = ldg4(in.qq + i);
+    }
+  }
+  const V xi = xyz(p4);
+  V F = mk(0.0, 0.0, 0.0), M = mk(0.0, 0.0, 0.0);
+
+  // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
+  //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.
+  for (int w = 0; w < a.nwall; ++w) {
+    V c = mk(0.0, 0.0, 0.0);
+    if (alive && lane == 0 && (pf & (1u << (PF_WALL_SHIFT + w)))) {
+      const WallDev W = a.walls[w];
+      V f;
+      if (law_wall(W.k, mk(W.ox, W.oy, W.oz), mk(W.nx, W.ny, W.nz), xi, p4.w, f)) {
+        F += f;
+        if (pf & (1u << (PF_INNER_SHIFT + w))) c = f;  // CWall::addForce(-F): m_force -= -F
+      }
+    }
+    if (!EVAL) {
+      double cx = c.x, cy = c.y, cz = c.z;
+      if (__any_sync(0xffffffffu, cx != 0.0 || cy != 0.0 || cz != 0.0)) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          cx += __shfl_down_sync(0xffffffffu, cx, o);
+          cy += __shfl_down_sync(0xffffffffu, cy, o);
+          cz += __shfl_down_sync(0xffffffffu, cz, o);
+        }
+      }
+      if (wlane == 0) { s_red[warp][w][0] = cx; s_red[warp][w][1] = cy; s_red[warp][w][2] = cz; }
+    }
+  }
+
+  // 2. body forces (BodyForceGroup::calcForces, BodyForceGroup.hpp:54-65): F += g * m
+  if (alive && lane == 0)
+    for (int k = 0; k < a.ngrav; ++k) F += mk(a.grav[k][0], a.grav[k][1], a.grav[k][2]) * v4.w;
+
+  // 3. dynamic pair groups (PIS_NE / PIS_ED::calcForces).  Contact is tested first from the
+  //    positions alone; the partner's velocity / spin and the pair's history are gathered only
+  //    for touching pairs (a non-touching RotFriction pair just resets its history).  Adjacency
+  //    entries and partner positions are fetched kBatch at a time to keep several gathers in
+  //    flight per thread.
+  V Fp = mk(0.0, 0.0, 0.0), Mp = mk(0.0, 0.0, 0.0);  // FP64 form
+  KSum3 Fk, Mk;                                      // FP32 form
+  Fk.zero();
+  Mk.zero();
+  if ((FEAT & (F_ELASTIC | F_FRIC)) && alive) {
+    constexpr int kBatch = FP32 ? 4 : 2;
+    const Vf vself = cvt<float>(xyz(v4)), wself = cvt<float>(xyz(w4));
+    for (int d = 0; d < a.ndyn; ++d) {
+      const DynDev& G = a.dyn[d];
+      const int e0 = __ldg(G.adj_start + i), e1 = __ldg(G.adj_start + i + 1);
+      for (int e = e0 + lane; e < e1; e += TPP * kBatch) {
+        int2 en[kBatch];
+        double4 pjs[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+          const int eb = e + b * TPP;
+          en[b] = eb < e1 ? __ldg(G.adj + eb) : make_int2(-1, 0);
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b)
+          pjs[b] = en[b].x >= 0 ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+          if (en[b].x < 0) continue;
+          const int j = en[b].x;
+          const bool isp1 = en[b].y < 0;
+          const int k = en[b].y & 0x7fffffff;
+          const double4 pj = pjs[b];
+          // canonical orientation: p1 = lower id
+          const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
+          const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+          const V D = x1 - x2;
+          const double eq_dist = pa.w + pb.w;
+          const bool touching = dot(D, D) < (eq_dist * eq_dist);  // the laws' contact test
+          if (G.kind == 0) {
+            if constexpr ((FEAT & F_ELASTIC) != 0) {
+              if (!touching) continue;
+              if constexpr (!FP32) {
+                V f;
+                if (law_elastic(elastic_k(G.k, G.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, f)) {
+                  if (isp1) Fp += -1.0 * f; else Fp += f;
+                }
+              } else {
+                Vf f;
+                if (law_elastic_f32(elastic_k(G.k, G.scaling, pa.w, pb.w), D, pa.w, pb.w, f)) Fk.add(isp1 ? -f : f);
+              }
+            }
+          } else {
+            if constexpr (ROT && (FEAT & F_FRIC) != 0) {
+              if (!touching) {  // CRotFrictionInteraction::calcSimpleForces, no-contact branch
+                if (isp1 && !EVAL) {
+                  if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                  else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+                }
+                continue;
+              }
+              double keff, kseff;
+              friction_k(G.k, G.ks, G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
+              if constexpr (!FP32) {
+                const double4 vj = ldg4(in.vm + j), wj = ldg4(in.wi + j);
+                const double4 va = isp1 ? v4 : vj, vb = isp1 ? vj : v4;
+                const double4 wa = isp1 ? w4 : wj, wb = isp1 ? wj : w4;
+                const double4 h = ldg4(G.hist_in + k);
+                FricOut o;
+                law_friction(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, xyz(va), xyz(wa), x2, pb.w, xyz(vb),
+                             xyz(wb), mk(h.x, h.y, h.z), (((int)h.w) & 1) != 0, o);
+                if (isp1) {
+                  Fp += -1.0 * o.fn;
+                  Mp += o.M1;
+                  Fp += o.Ffric;
+                  G.hist_out[k] = make_double4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
+                                               (o.slipping ? 1.0 : 0.0) + (o.touching ? 2.0 : 0.0));
+                } else {
+                  Fp += o.fn;
+                  Mp += o.M2;
+                  Fp += -1.0 * o.Ffric;
+                }
+              } else {
+                const float4 r0 = __ldg(in.vw + 2 * j), r1 = __ldg(in.vw + 2 * j + 1);
+                const Vf vj = mk(r0.x, r0.y, r0.z), wj = mk(r0.w, r1.x, r1.y);
+                Vf hF;
+                bool hs;
+                if (EVAL) {  // evaluation pass of an FP64 run: its FP64 history
+                  const double4 h = ldg4(G.hist_in + k);
+                  hF = mk((float)h.x, (float)h.y, (float)h.z);
+                  hs = (((int)h.w) & 1) != 0;
+                } else {
+                  const float4 h = __ldg(G.hist32_in + k);
+                  hF = mk(h.x, h.y, h.z);
+                  hs = (((int)h.w) & 1) != 0;
+                }
+                FricOutF o;
+                law_friction_f32(keff, kseff, G.mu_s, G.mu_d, (float)G.dt, D, pa.w, pb.w, isp1 ? vself : vj,
+                                 isp1 ? wself : wj, isp1 ? vj : vself, isp1 ? wj : wself, hF, hs, o);
+                if (isp1) {
+                  Fk.add(-o.fn);
+                  Fk.add(o.Ffric);
+                  Mk.add(o.M1);
+                  if (!EVAL)
+                    G.hist32_out[k] = make_float4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
+                                                  (o.slipping ? 1.f : 0.f) + (o.touching ? 2.f : 0.f));
+                } else {
+                  Fk.add(o.fn);
+                  Fk.add(-o.Ffric);
+                  Mk.add(o.M2);
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // 4. bonded groups (PIS_EB::calcForces) + failure test (PIS_EB::update at the next step)
+  V Fb = mk(0.0, 0.0, 0.0), Mb = mk(0.0, 0.0, 0.0);
+  if constexpr (ROT && (FEAT & F_BOND) != 0) {
+    if (alive) {
+      for (int d = 0; d < a.nbond; ++d) {
+        const BondDev& B = a.bond[d];
+        const int e0 = __ldg(B.adj_start + i), e1 = __ldg(B.adj_start + i + 1);
+        for (int e = e0 + lane; e < e1; e += TPP) {
+          const int2 en = __ldg(B.adj + e);
+          const int k = en.y & 0x7fffffff;
+          if (B.broken_step[k] <= step) continue;  // removed by an earlier update
+          const int j = en.x;
+          const bool isp1 = en.y < 0;
+          const double4 pj = ldg4(in.pr + j), qj = ldg4(in.qq + j);
+          const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
+          const double4 qa = isp1 ? q4 : qj, qb = isp1 ? qj : q4;
+          const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+          const double4 D0 = ldg4(B.D0 + k);
+          const V mD = xyz(D0);
+          const double dist0 = sqrt(dot(mD, mD));
+          const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
+          BondOut o;
+          law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
+          if (isp1) {
+            Fb += o.force;
+            Mb += o.moment1;
+            if (!EVAL && bond_broken(K, o, B.truncated)) {
+              B.broken_step[k] = (int)(step + 1);
+              a.P.flagged[i] = 1;
+              a.P.flagged[j] = 1;
+              int slot = atomicAdd(B.nevents, 1);
+              if (slot < B.cap_events) {
+                B.events[3 * slot] = a.P.id[i];
+                B.events[3 * slot + 1] = a.P.id[j];
+                B.events[3 * slot + 2] = (int)(step + 1);
+              } else {
+                atomicOr(a.ctrl, CTRL_OVERFLOW);
+              }
+              atomicOr(a.ctrl, CTRL_BROKE);
+            }
+          } else {
+            Fb += -1.0 * o.force;
+            Mb += o.moment2;
+          }
+        }
+      }
+    }
+  }
+
+  // fixed-order combination of the lanes' partial sums
+  if (TPP > 1) {
+    if (FP32) {
+      Fk.s = lane_sumf<TPP>(Fk.s);
+      Fk.c = lane_sumf<TPP>(Fk.c);
+      Mk.s = lane_sumf<TPP>(Mk.s);
+      Mk.c = lane_sumf<TPP>(Mk.c);
+    } else {
+      Fp = lane_sum<TPP>(Fp);
+      Mp = lane_sum<TPP>(Mp);
+    }
+    if (FEAT & F_BOND) {
+      Fb = lane_sum<TPP>(Fb);
+      Mb = lane_sum<TPP>(Mb);
+    }
+  }
+  if (FP32) {
+    Fp = Fk.value();
+    Mp = Mk.value();
+  }
+
+  if (alive && lane == 0) {
+    F += Fp;
+    M += Mp;
+    F += Fb;
+    M += Mb;
+    // 1/m and 1/I as the particle constructors compute them (Particle.cpp:95-99, RotParticle.cpp:35)
+    const double2 iv = make_double2(v4.w != 0.0 ? 1.0 / v4.w : 0.0, 1.0 / w4.w);
+    // 5. damping, last (SubLattice.hpp:2140-2145): "Damping" then "RotDamping"
+    if (a.damp_lin) F += damping_force(xyz(v4), F, iv.x, v4.w, a.visc_lin, a.dt_lin, a.iter_lin);
+    if (ROT && a.damp_rot) M += damping_force(xyz(w4), M, iv.y, w4.w, a.visc_rot, a.dt_rot, a.iter_rot);
+    if (EVAL) {
+      a.P.force_eval[i] = d4(F, 0.0);
+      if (ROT) a.P.moment_eval[i] = d4(M, 0.0);
+    } else {
+      // 6. integration (CRotParticle::integrate + rescale, RotParticle.cpp:277-321; Particle.cpp:257-274)
+      const double dt = a.dt;
+      V v = xyz(v4), x = xi;
+      V w = xyz(w4);
+      if (ROT) {
+        if (!(FEAT & F_BOND)) q4 = ldg4(in.qq + i);
+        Qd q{q4.x, mk(q4.y, q4.z, q4.w)};
+        if (pf & PF_ROT) {
+          w += (dt * iv.y) * M;
+          const Qd dq = qmul(Qd{0.0, w}, q);
+          const double c = dt / 2.0;
+          q.s += c * dq.s;
+          q.v += c * dq.v;
+        } else {
+          w = mk(0.0, 0.0, 0.0);
+        }
+        const double module = sqrt(q.s * q.s + q.v.x * q.v.x + q.v.y * q.v.y + q.v.z * q.v.z);
+        if (module != 0.0) {
+          const double inverse = 1.0 / module;
+          q.s = inverse * q.s;
+          q.v = inverse * q.v;
+        }
+        out.wi[i] = d4(w, w4.w);
+        out.qq[i] = make_double4(q.s, q.v.x, q.v.y, q.v.z);
+      }
+      if (pf & PF_DYN) {
+        v += F * iv.x * dt;
+        x += v * dt;
+      }
+      out.pr[i] = d4(x, p4.w);
+      out.vm[i] = d4(v, v4.w);
+      if (FP32) {
+        out.vw[2 * i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)w.x);
+        out.vw[2 * i + 1] = make_float4((float)w.y, (float)w.z, 0.f, 0.f);
+      }
+      if (a.store_forces) {
+        a.P.force[i] = d4(F, 0.0);
+        if (ROT) a.P.moment[i] = d4(M, 0.0);
+      }
+      // 7. displacement check for the next step (TSubLattice::checkNeighbors)
+      const double4 op = ldg4(a.P.oldpos + i);
+      const V dd = mk(x.x - op.x, x.y - op.y, x.z - op.z);
+      if (dot(dd, dd) > a.half_alpha_sq) atomicOr(a.ctrl, CTRL_REBUILD);
+    }
+  }
+  if (EVAL) return;
+
+  // per-block wall reactions (fixed order over warps), then the last block finishes the step
+  const int nw3 = a.nwall * 3;
+  __syncthreads();
+  if (threadIdx.x < nw3) {
+    const int w = threadIdx.x / 3, c = threadIdx.x % 3;
+    double acc = 0.0;
+    for (int k = 0; k < kStepWarps; ++k) acc += s_red[k][w][c];
+    a.wall_partial[((size_t)blockIdx.x * kMaxWalls + w) * 3 + c] = acc;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned prev = atomicInc(a.block_counter, gridDim.x - 1);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // wall reactions: thread t sums blocks t, t+256, ... (fixed assignment), then a fixed tree
+  for (int wc = 0; wc < nw3; ++wc) {
+    const int w = wc / 3, c = wc % 3;
+    double acc = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+      acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (wlane == 0) s_red[warp][0][0] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
+      a.wall_force[3 * w + c] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < a.nwall; ++w) {  // native wall loader: origin += v*dt per step (WallLoaderRunnable)
+      WallDev* W = a.walls + w;
+      if (a.wall_vel[3 * w] != 0.0 || a.wall_vel[3 * w + 1] != 0.0 || a.wall_vel[3 * w + 2] != 0.0) {
+        W->ox += a.wall_vel[3 * w] * a.dt;
+        W->oy += a.wall_vel[3 * w + 1] * a.dt;
+        W->oz += a.wall_vel[3 * w + 2] * a.dt;
+      }
+    }
+    *a.step_counter = step;
+    volatile int* ctrl = a.ctrl;
+    if (*ctrl) *a.stop = 1;
+  }
+}
+
+inline int step_blocks(int n, int tpp) {
+  long long t = (long long)(n > 0 ? n : 1) * tpp;
+  return (int)((t + kStepThreads - 1) / kStepThreads);
+}
+
+template <bool R, int FEAT, bool FP32, bool EVAL>
+inline void launch_step_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
+  const int grid = step_blocks(a.P.n, tpp);
+  switch (tpp) {
+    case 1: k_step<R, 1, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 2: k_step<R, 2, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 4: k_step<R, 4, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
+    default: k_step<R, 8, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
+  }
+}
+
+}  // namespace dem

@@ -1,0 +1,26 @@
+// FP32-force instances of the step kernel (see dem_step.cuh): pair forces in
+// FP32 with Kahan-compensated accumulation, positions / contact detection /
+// overlap / integration in FP64.  Built with FMA contraction (the FP32 form is
+// checked against FP64 at a stated relative tolerance, not bit for bit).
+#include "dem_kernels.h"
+#include "dem_step.cuh"
+
+namespace dem {
+
+void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, cudaStream_t s) {
+  bool el = false, fr = false;
+  for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
+  const bool bd = a.nbond > 0;
+  if (eval) {
+    if (!rot) return launch_step_tpp<false, F_ELASTIC, true, true>(a, tpp, s);
+    if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC, true, true>(a, tpp, s);
+    if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC, true, true>(a, tpp, s);
+    return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BOND, true, true>(a, tpp, s);
+  }
+  if (!rot) return launch_step_tpp<false, F_ELASTIC, true, false>(a, tpp, s);
+  if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC, true, false>(a, tpp, s);
+  if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC, true, false>(a, tpp, s);
+  return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BOND, true, false>(a, tpp, s);
+}
+
+}  // namespace dem

@@ -53,6 +53,7 @@ SIGNATURES = {
     "dem_set_particles": (C.c_int, [_P, C.c_int, _I, _D, _D, _D, _D]),
     "dem_set_stream": (C.c_int, [_P, C.c_void_p]),
     "dem_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
+    "dem_precision_check": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "dem_wall_reactions_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 

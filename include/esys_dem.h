@@ -156,6 +156,12 @@ int dem_set_stream(dem_sim* h, void* stream);
  * [6] interactions evaluated per step now, [7] threads per particle in use.  Returns entries written. */
 int dem_get_counters(dem_sim* h, long long* out, int n);
 
+/* Precision check of the FP32-force form, no reference counterpart: from the FP64 form, evaluates
+ * the FP32-form forces of the current state, then advances one FP64 step and compares.
+ * out[0] = max|dF|/max|F|, out[1] = max|dM|/max|M|, out[2] / out[3] = median / 99th percentile of
+ * |dF_i|/|F_i| over particles with |F_i| > 1e-9 max|F|, out[4] = particles compared. */
+int dem_precision_check(dem_sim* h, double* out);
+
 /* Allocation-free per-wall reaction forces, for callers that cannot call cudaMalloc: code that
  * runs during CUDA graph capture, hosts that hand the library only memory from their own pool,
  * real-time loops that forbid allocation.  No counterpart in the reference.
@@ -174,7 +180,9 @@ int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const 
 
 /* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic, 1, 2, 4, 8),
  * "chunk" (steps launched per host round trip), "store_forces" (keep per-particle F/M),
- * "profile" (time the force/integration kernels with CUDA events). */
+ * "profile" (time the force/integration kernels with CUDA events), "precision" (64 = FP64 form,
+ * 32 = FP32 pair forces with Kahan-compensated accumulation, FP64 positions / contact detection /
+ * integration). */
 int dem_set_option(dem_sim* h, const char* key, double value);
 
 #ifdef __cplusplus
