@@ -198,6 +198,8 @@ def main():
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64],
                     help="32: FP32 pair forces + FP64 integration (headline); 64: FP64 throughout")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
+                    help="step kernels: -1 automatic, 0 fused, 1 pair kernel + integration kernel")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -233,6 +235,7 @@ def main():
         sim.set_stream(stream.cuda_stream)
         sim.set_option("profile", 1)
         sim.set_option("precision", precision)
+        sim.set_option("split", args.split)
         if args.tpp:
             sim.set_option("threads_per_particle", args.tpp)
         sim.set_wall_velocity("bottom", (-0.01, 0, 0))

@@ -60,6 +60,8 @@ struct Particles {
   double4* moment;       // last accumulated moment (w unused)
   double4* force_eval;   // FP32 forces of an evaluation-only pass (precision check)
   double4* moment_eval;
+  double4* sum_f;        // split step: pair + bond force sums between the two kernels
+  double4* sum_m;
   unsigned* pflags;      // PF_* bits
   unsigned char* flagged;// set on both particles of a broken bond (CParticle::flag)
   int* id;

@@ -581,10 +581,17 @@ void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const
 int step_grid(int n, int tpp) { return step_blocks(n, tpp); }
 
 // FP64 instances (this translation unit is built with --fmad=false).
-void launch_step(const StepArgs& a, bool rot, int tpp, cudaStream_t s) {
+void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s) {
   bool el = false, fr = false;
   for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
   const bool bd = a.nbond > 0;
+  if (split) {
+    if (!rot) return launch_split_tpp<false, F_ELASTIC, false>(a, tpp, s);
+    if (!bd && fr && !el) return launch_split_tpp<true, F_FRIC, false>(a, tpp, s);
+    if (!bd && !fr) return launch_split_tpp<true, F_ELASTIC, false>(a, tpp, s);
+    if (bd && !el) return launch_split_tpp<true, F_FRIC | F_BOND, false>(a, tpp, s);
+    return launch_split_tpp<true, F_ELASTIC | F_FRIC | F_BOND, false>(a, tpp, s);
+  }
   if (!rot) return launch_step_tpp<false, F_ELASTIC, false, false>(a, tpp, s);
   if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC, false, false>(a, tpp, s);
   if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC, false, false>(a, tpp, s);

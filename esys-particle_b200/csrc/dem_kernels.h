@@ -41,7 +41,7 @@ void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* c
 void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, cudaStream_t s);
 void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s);
 int step_grid(int n, int tpp);
-void launch_step(const StepArgs& a, bool rot, int tpp, cudaStream_t s);
-void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, cudaStream_t s);
+void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s);
+void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, bool split, cudaStream_t s);
 
 }  // namespace dem

@@ -110,6 +110,7 @@ struct DemSim {
   int chunk = 64;        // steps launched per host round trip
   int store_forces = 1;
   int fp32 = 0;          // 1 = FP32-force / FP64-integration form
+  int split = -1;        // -1 automatic, 0 fused step kernel, 1 pair kernel + integration kernel
   // particles
   int n = 0, cap = 0;
   Particles P{};
@@ -169,7 +170,7 @@ struct DemSim {
     for (auto& b : bond) b.second.release();
     void* ps[] = {P.buf[0].pr, P.buf[0].vm, P.buf[0].wi, P.buf[0].qq, P.buf[1].pr, P.buf[1].vm, P.buf[1].wi,
                   P.buf[1].qq, P.buf[0].vw, P.buf[1].vw, P.inv, P.oldpos, P.force, P.moment, P.force_eval,
-                  P.moment_eval, P.pflags, P.flagged, P.id, P.tag, P.cell};
+                  P.moment_eval, P.sum_f, P.sum_m, P.pflags, P.flagged, P.id, P.tag, P.cell};
     for (void* p : ps) if (p) cudaFree(p);
     cell_count.release(); cell_start.release(); cell_cursor.release(); cell_list.release();
     scratch_i.release(); scratch_j.release(); scalars.release();
@@ -246,6 +247,7 @@ struct DemSim {
       grow_array(P.buf[b].wi, n, nc); grow_array(P.buf[b].qq, n, nc);
       grow_array(P.buf[b].vw, 2 * n, 2 * nc);
     }
+    grow_array(P.sum_f, n, nc); grow_array(P.sum_m, n, nc);
     grow_array(P.inv, n, nc); grow_array(P.oldpos, n, nc); grow_array(P.force, n, nc); grow_array(P.moment, n, nc);
     grow_array(P.pflags, n, nc); grow_array(P.flagged, n, nc); grow_array(P.id, n, nc); grow_array(P.tag, n, nc);
     grow_array(P.cell, n, nc);
@@ -355,7 +357,7 @@ struct DemSim {
     d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
     launch_sync_vw(P, cur, s);
     StepArgs ea = make_args(cur);
-    launch_step_fp32(ea, rot != 0, t_pp, true, s);
+    launch_step_fp32(ea, rot != 0, t_pp, true, false, s);
     const int keep = chunk;
     chunk = 1;
     step(1);
@@ -685,14 +687,15 @@ struct DemSim {
         DEM_CUDA(cudaEventRecord(ev0, s));
       }
       if (fp32) launch_sync_vw(P, cur, s);
+      const bool two = split == 1;  // automatic = fused: measured faster on the 250k shear cell
       for (int j = 0; j < k; ++j) {
         StepArgs a = make_args((cur + j) & 1);
-        if (fp32) launch_step_fp32(a, rot != 0, t_pp, false, s);
-        else launch_step(a, rot != 0, t_pp, s);
+        if (fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
+        else launch_step(a, rot != 0, t_pp, two, s);
       }
       DEM_CUDA(cudaGetLastError());
       if (profile) DEM_CUDA(cudaEventRecord(ev1, s));
-      c_launches += k;
+      c_launches += two ? 2LL * k : k;
       DEM_CUDA(cudaMemcpyAsync(h_ctrl, d_step.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
       DEM_CUDA(cudaMemcpyAsync(h_ctrl + 2, d_ctrl.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       sync();
@@ -1214,6 +1217,9 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.chunk = (int)value;
     } else if (k == "store_forces") {
       s.store_forces = value != 0;
+    } else if (k == "split") {
+      if (value != -1 && value != 0 && value != 1) throw std::invalid_argument("split must be -1, 0 or 1");
+      s.split = (int)value;
     } else if (k == "profile") {
       s.profile = value != 0;
     } else if (k == "precision") {

@@ -46,81 +46,45 @@ __device__ __forceinline__ Vf lane_sumf(Vf v) {
 constexpr int kStepThreads = 256;
 constexpr int kStepWarps = kStepThreads / 32;
 
+__host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
+  long long t = (long long)(n > 0 ? n : 1) * tpp;
+  return (int)((t + kStepThreads - 1) / kStepThreads);
+}
+
 // Interaction families compiled into a k_step instance (the host picks the
 // smallest instance that covers the groups present, so a friction-only run
 // does not carry the registers of the bond law).
 enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4 };
 
+// Sum of the pair-group and bond contributions on particle i (all TPP lanes of
+// the particle call this; on return every lane holds the combined sums).  The
+// order is fixed: each lane adds its entries in adjacency order, then a
+// butterfly combines the lanes.
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(const StepArgs a) {
-  __shared__ double s_red[kStepWarps][kMaxWalls][3];
-  __shared__ bool s_last;
-  if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
-  const long long step = *a.step_counter + 1;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = tid / TPP;
-  const int lane = threadIdx.x % TPP;
-  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const bool valid = i < a.P.n;
-  const unsigned pf = valid ? a.P.pflags[i] : 0u;
-  const bool alive = valid && (pf & PF_ALIVE);
-  const ParticleBuf in = a.P.buf[a.cur];
-  const ParticleBuf out = a.P.buf[a.cur ^ 1];
-
-  double4 p4 = make_double4(0, 0, 0, 0), v4 = p4, w4 = p4, q4 = make_double4(1, 0, 0, 0);
-  if (alive) {
-    p4 = ldg4(in.pr + i);
-    v4 = ldg4(in.vm + i);
-    if (ROT) {
-      w4 = ldg4(in.wi + i);
-      if (FEAT & F_BOND) q4 = ldg4(in.qq + i);
-    }
-  }
-  const V xi = xyz(p4);
-  V F = mk(0.0, 0.0, 0.0), M = mk(0.0, 0.0, 0.0);
-
-  // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
-  //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.
-  for (int w = 0; w < a.nwall; ++w) {
-    V c = mk(0.0, 0.0, 0.0);
-    if (alive && lane == 0 && (pf & (1u << (PF_WALL_SHIFT + w)))) {
-      const WallDev W = a.walls[w];
-      V f;
-      if (law_wall(W.k, mk(W.ox, W.oy, W.oz), mk(W.nx, W.ny, W.nz), xi, p4.w, f)) {
-        F += f;
-        if (pf & (1u << (PF_INNER_SHIFT + w))) c = f;  // CWall::addForce(-F): m_force -= -F
-      }
-    }
-    if (!EVAL) {
-      double cx = c.x, cy = c.y, cz = c.z;
-      if (__any_sync(0xffffffffu, cx != 0.0 || cy != 0.0 || cz != 0.0)) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          cx += __shfl_down_sync(0xffffffffu, cx, o);
-          cy += __shfl_down_sync(0xffffffffu, cy, o);
-          cz += __shfl_down_sync(0xffffffffu, cz, o);
-        }
-      }
-      if (wlane == 0) { s_red[warp][w][0] = cx; s_red[warp][w][1] = cy; s_red[warp][w][2] = cz; }
-    }
-  }
-
-  // 2. body forces (BodyForceGroup::calcForces, BodyForceGroup.hpp:54-65): F += g * m
-  if (alive && lane == 0)
-    for (int k = 0; k < a.ngrav; ++k) F += mk(a.grav[k][0], a.grav[k][1], a.grav[k][2]) * v4.w;
-
+__device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& in, int i, int lane, bool alive,
+                                          long long step, const double4& p4, const double4& q4, V& Fp, V& Mp) {
+  Fp = mk(0.0, 0.0, 0.0);
+  Mp = mk(0.0, 0.0, 0.0);
   // 3. dynamic pair groups (PIS_NE / PIS_ED::calcForces).  Contact is tested first from the
   //    positions alone; the partner's velocity / spin and the pair's history are gathered only
   //    for touching pairs (a non-touching RotFriction pair just resets its history).  Adjacency
   //    entries and partner positions are fetched kBatch at a time to keep several gathers in
   //    flight per thread.
-  V Fp = mk(0.0, 0.0, 0.0), Mp = mk(0.0, 0.0, 0.0);  // FP64 form
   KSum3 Fk, Mk;                                      // FP32 form
   Fk.zero();
   Mk.zero();
   if ((FEAT & (F_ELASTIC | F_FRIC)) && alive) {
-    constexpr int kBatch = FP32 ? 4 : 2;
-    const Vf vself = cvt<float>(xyz(v4)), wself = cvt<float>(xyz(w4));
+    constexpr int kBatch = 1;
+    Vf vself = mk(0.f, 0.f, 0.f), wself = vself;
+    double4 v4 = make_double4(0.0, 0.0, 0.0, 0.0), w4 = v4;
+    if (FP32) {
+      const float4 r0 = __ldg(in.vw + 2 * i), r1 = __ldg(in.vw + 2 * i + 1);
+      vself = mk(r0.x, r0.y, r0.z);
+      wself = mk(r0.w, r1.x, r1.y);
+    } else if (FEAT & F_FRIC) {
+      v4 = ldg4(in.vm + i);
+      if (ROT) w4 = ldg4(in.wi + i);
+    }
     for (int d = 0; d < a.ndyn; ++d) {
       const DynDev& G = a.dyn[d];
       const int e0 = __ldg(G.adj_start + i), e1 = __ldg(G.adj_start + i + 1);
@@ -229,7 +193,6 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
   }
 
   // 4. bonded groups (PIS_EB::calcForces) + failure test (PIS_EB::update at the next step)
-  V Fb = mk(0.0, 0.0, 0.0), Mb = mk(0.0, 0.0, 0.0);
   if constexpr (ROT && (FEAT & F_BOND) != 0) {
     if (alive) {
       for (int d = 0; d < a.nbond; ++d) {
@@ -252,8 +215,8 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
           BondOut o;
           law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
           if (isp1) {
-            Fb += o.force;
-            Mb += o.moment1;
+            Fp += o.force;
+            Mp += o.moment1;
             if (!EVAL && bond_broken(K, o, B.truncated)) {
               B.broken_step[k] = (int)(step + 1);
               a.P.flagged[i] = 1;
@@ -269,40 +232,80 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
               atomicOr(a.ctrl, CTRL_BROKE);
             }
           } else {
-            Fb += -1.0 * o.force;
-            Mb += o.moment2;
+            Fp += -1.0 * o.force;
+            Mp += o.moment2;
           }
         }
       }
     }
   }
 
-  // fixed-order combination of the lanes' partial sums
   if (TPP > 1) {
     if (FP32) {
       Fk.s = lane_sumf<TPP>(Fk.s);
       Fk.c = lane_sumf<TPP>(Fk.c);
       Mk.s = lane_sumf<TPP>(Mk.s);
       Mk.c = lane_sumf<TPP>(Mk.c);
-    } else {
-      Fp = lane_sum<TPP>(Fp);
-      Mp = lane_sum<TPP>(Mp);
     }
-    if (FEAT & F_BOND) {
-      Fb = lane_sum<TPP>(Fb);
-      Mb = lane_sum<TPP>(Mb);
-    }
+    Fp = lane_sum<TPP>(Fp);
+    Mp = lane_sum<TPP>(Mp);
   }
   if (FP32) {
-    Fp = Fk.value();
-    Mp = Mk.value();
+    // FP64-form sums (bonds) are added after the compensated FP32 pair sums
+    Fp = Fk.value() + Fp;
+    Mp = Mk.value() + Mp;
   }
+}
+
+// Walls, body force, the pair sums, damping and the integration of particle i
+// (TSubLattice::calcForces group order, then integrate + rescale).  Every thread
+// of the block calls this: the wall reactions are reduced across the block.
+template <bool ROT, int TPP, bool FP32, bool EVAL>
+__device__ __forceinline__ void finish_particle(const StepArgs& a, const ParticleBuf& in, const ParticleBuf& out, int i,
+                                                int lane, int wlane, int warp, unsigned pf, bool alive,
+                                                const double4& p4, double4 q4, bool q_loaded, const V& Fp, const V& Mp,
+                                                double (*s_red)[kMaxWalls][3]) {
+  double4 v4 = make_double4(0.0, 0.0, 0.0, 0.0), w4 = v4;
+  if (alive) {
+    v4 = ldg4(in.vm + i);
+    if (ROT) w4 = ldg4(in.wi + i);
+  }
+  const V xi = xyz(p4);
+  V F = mk(0.0, 0.0, 0.0), M = mk(0.0, 0.0, 0.0);
+
+  // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
+  //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.
+  for (int w = 0; w < a.nwall; ++w) {
+    V c = mk(0.0, 0.0, 0.0);
+    if (alive && lane == 0 && (pf & (1u << (PF_WALL_SHIFT + w)))) {
+      const WallDev W = a.walls[w];
+      V f;
+      if (law_wall(W.k, mk(W.ox, W.oy, W.oz), mk(W.nx, W.ny, W.nz), xi, p4.w, f)) {
+        F += f;
+        if (pf & (1u << (PF_INNER_SHIFT + w))) c = f;  // CWall::addForce(-F): m_force -= -F
+      }
+    }
+    if (!EVAL) {
+      double cx = c.x, cy = c.y, cz = c.z;
+      if (__any_sync(0xffffffffu, cx != 0.0 || cy != 0.0 || cz != 0.0)) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          cx += __shfl_down_sync(0xffffffffu, cx, o);
+          cy += __shfl_down_sync(0xffffffffu, cy, o);
+          cz += __shfl_down_sync(0xffffffffu, cz, o);
+        }
+      }
+      if (wlane == 0) { s_red[warp][w][0] += cx; s_red[warp][w][1] += cy; s_red[warp][w][2] += cz; }
+    }
+  }
+
+  // 2. body forces (BodyForceGroup::calcForces, BodyForceGroup.hpp:54-65): F += g * m
+  if (alive && lane == 0)
+    for (int k = 0; k < a.ngrav; ++k) F += mk(a.grav[k][0], a.grav[k][1], a.grav[k][2]) * v4.w;
 
   if (alive && lane == 0) {
     F += Fp;
     M += Mp;
-    F += Fb;
-    M += Mb;
     // 1/m and 1/I as the particle constructors compute them (Particle.cpp:95-99, RotParticle.cpp:35)
     const double2 iv = make_double2(v4.w != 0.0 ? 1.0 / v4.w : 0.0, 1.0 / w4.w);
     // 5. damping, last (SubLattice.hpp:2140-2145): "Damping" then "RotDamping"
@@ -317,7 +320,7 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
       V v = xyz(v4), x = xi;
       V w = xyz(w4);
       if (ROT) {
-        if (!(FEAT & F_BOND)) q4 = ldg4(in.qq + i);
+        if (!q_loaded) q4 = ldg4(in.qq + i);
         Qd q{q4.x, mk(q4.y, q4.z, q4.w)};
         if (pf & PF_ROT) {
           w += (dt * iv.y) * M;
@@ -357,8 +360,14 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
       if (dot(dd, dd) > a.half_alpha_sq) atomicOr(a.ctrl, CTRL_REBUILD);
     }
   }
-  if (EVAL) return;
+}
 
+// Per-block wall reactions (fixed order over warps), then the last block of the
+// launch finishes the step: wall totals, native wall loaders, step counter and
+// the stop word.  All threads of the block call this.
+__device__ __forceinline__ void step_epilogue(const StepArgs& a, int wlane, int warp, double (*s_red)[kMaxWalls][3],
+                                              bool* s_last) {
+  const long long step = *a.step_counter + 1;
   // per-block wall reactions (fixed order over warps), then the last block finishes the step
   const int nw3 = a.nwall * 3;
   __syncthreads();
@@ -372,10 +381,10 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned prev = atomicInc(a.block_counter, gridDim.x - 1);
-    s_last = (prev == gridDim.x - 1);
+    *s_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
-  if (!s_last) return;
+  if (!*s_last) return;
   __threadfence();
   // wall reactions: thread t sums blocks t, t+256, ... (fixed assignment), then a fixed tree
   for (int wc = 0; wc < nw3; ++wc) {
@@ -409,19 +418,149 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : 2) k_step(
   }
 }
 
+
+// Fused step: pair sums and integration in one launch (small systems).
+template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 : 2)) k_step(const StepArgs a) {
+  __shared__ double s_red[kStepWarps][kMaxWalls][3];
+  __shared__ bool s_last;
+  if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
+  const long long step = *a.step_counter + 1;
+  const int lane = threadIdx.x % TPP;
+  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const ParticleBuf in = a.P.buf[a.cur];
+  const ParticleBuf out = a.P.buf[a.cur ^ 1];
+  for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kStepThreads) (&s_red[0][0][0])[k] = 0.0;
+  __syncthreads();
+  // Persistent grid: one wave of blocks strides over tiles of kStepThreads / TPP particles.
+  const int ntiles = step_tiles(a.P.n, TPP);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int i = (tile * kStepThreads + threadIdx.x) / TPP;
+    const bool valid = i < a.P.n;
+    // All of the particle's own loads are issued at once: the flags and position into
+    // registers, the records needed after the pair loop into L1.
+    unsigned pf = 0u;
+    double4 p4 = make_double4(0, 0, 0, 0), q4 = make_double4(1, 0, 0, 0);
+    if (valid) {
+      pf = __ldg(a.P.pflags + i);
+      p4 = ldg4(in.pr + i);
+      if (lane == 0) {
+        prefetch_l1(in.vm + i);
+        if (ROT) { prefetch_l1(in.wi + i); prefetch_l1(in.qq + i); }
+        prefetch_l1(a.P.oldpos + i);
+        if (FP32 && ROT) prefetch_l1(in.vw + 2 * i);
+        for (int d = 0; d < a.ndyn; ++d) prefetch_l1(a.dyn[d].adj_start + i);
+      }
+      if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);
+    }
+    const bool alive = valid && (pf & PF_ALIVE);
+    V Fp, Mp;
+    pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp);
+    finish_particle<ROT, TPP, FP32, EVAL>(a, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
+                                          ROT && (FEAT & F_BOND), Fp, Mp, s_red);
+  }
+  if (EVAL) return;
+  step_epilogue(a, wlane, warp, s_red, &s_last);
+}
+
+// Split step, part 1: pair and bond sums of every particle into P.sum_f / P.sum_m
+// (no particle state written besides friction history and bond records).
+template <bool ROT, int TPP, int FEAT, bool FP32>
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 : 2)) k_pairs(const StepArgs a) {
+  if (*a.stop) return;
+  const long long step = *a.step_counter + 1;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) / TPP;
+  const int lane = threadIdx.x % TPP;
+  const bool valid = i < a.P.n;
+  const unsigned pf = valid ? __ldg(a.P.pflags + i) : 0u;
+  const bool alive = valid && (pf & PF_ALIVE);
+  const ParticleBuf in = a.P.buf[a.cur];
+  double4 p4 = make_double4(0, 0, 0, 0), q4 = make_double4(1, 0, 0, 0);
+  if (alive) {
+    p4 = ldg4(in.pr + i);
+    if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);
+  }
+  V Fp, Mp;
+  pair_sums<ROT, TPP, FEAT, FP32, false>(a, in, i, lane, alive, step, p4, q4, Fp, Mp);
+  if (alive && lane == 0) {
+    a.P.sum_f[i] = d4(Fp, 0.0);
+    if (ROT) a.P.sum_m[i] = d4(Mp, 0.0);
+  }
+}
+
+// Split step, part 2: walls, body forces, the stored pair sums, damping,
+// integration and the block/launch epilogue; one thread per particle.
+template <bool ROT, bool FP32>
+__global__ void __launch_bounds__(kStepThreads, 3) k_integrate(const StepArgs a) {
+  __shared__ double s_red[kStepWarps][kMaxWalls][3];
+  __shared__ bool s_last;
+  if (*a.stop) return;
+  for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kStepThreads) (&s_red[0][0][0])[k] = 0.0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool valid = i < a.P.n;
+  const unsigned pf = valid ? a.P.pflags[i] : 0u;
+  const bool alive = valid && (pf & PF_ALIVE);
+  const ParticleBuf in = a.P.buf[a.cur];
+  const ParticleBuf out = a.P.buf[a.cur ^ 1];
+  double4 p4 = make_double4(0, 0, 0, 0);
+  V Fp = mk(0.0, 0.0, 0.0), Mp = Fp;
+  if (alive) {
+    p4 = ldg4(in.pr + i);
+    Fp = xyz(ldg4(a.P.sum_f + i));
+    if (ROT) Mp = xyz(ldg4(a.P.sum_m + i));
+  }
+  finish_particle<ROT, 1, FP32, false>(a, in, out, i, 0, wlane, warp, pf, alive, p4, make_double4(1, 0, 0, 0), false,
+                                       Fp, Mp, s_red);
+  step_epilogue(a, wlane, warp, s_red, &s_last);
+}
+
 inline int step_blocks(int n, int tpp) {
   long long t = (long long)(n > 0 ? n : 1) * tpp;
   return (int)((t + kStepThreads - 1) / kStepThreads);
 }
 
-template <bool R, int FEAT, bool FP32, bool EVAL>
-inline void launch_step_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
+// Blocks of one wave of kernel K on the current device (cached per instance).
+template <class K>
+inline int one_wave(K kernel) {
+  static int cached = 0;
+  if (!cached) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStepThreads, 0);
+    cached = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+  }
+  return cached;
+}
+
+template <bool R, int FEAT, bool FP32>
+inline void launch_split_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
   const int grid = step_blocks(a.P.n, tpp);
   switch (tpp) {
-    case 1: k_step<R, 1, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
-    case 2: k_step<R, 2, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
-    case 4: k_step<R, 4, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
-    default: k_step<R, 8, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 1: k_pairs<R, 1, FEAT, FP32><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 2: k_pairs<R, 2, FEAT, FP32><<<grid, kStepThreads, 0, s>>>(a); break;
+    case 4: k_pairs<R, 4, FEAT, FP32><<<grid, kStepThreads, 0, s>>>(a); break;
+    default: k_pairs<R, 8, FEAT, FP32><<<grid, kStepThreads, 0, s>>>(a); break;
+  }
+  k_integrate<R, FP32><<<step_blocks(a.P.n, 1), kStepThreads, 0, s>>>(a);
+}
+
+template <bool R, int T, int FEAT, bool FP32, bool EVAL>
+inline void launch_fused(const StepArgs& a, cudaStream_t s) {
+  const int tiles = step_blocks(a.P.n, T);
+  const int wave = one_wave(k_step<R, T, FEAT, FP32, EVAL>);
+  k_step<R, T, FEAT, FP32, EVAL><<<tiles < wave ? tiles : wave, kStepThreads, 0, s>>>(a);
+}
+
+template <bool R, int FEAT, bool FP32, bool EVAL>
+inline void launch_step_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
+  switch (tpp) {
+    case 1: launch_fused<R, 1, FEAT, FP32, EVAL>(a, s); break;
+    case 2: launch_fused<R, 2, FEAT, FP32, EVAL>(a, s); break;
+    case 4: launch_fused<R, 4, FEAT, FP32, EVAL>(a, s); break;
+    default: launch_fused<R, 8, FEAT, FP32, EVAL>(a, s); break;
   }
 }
 

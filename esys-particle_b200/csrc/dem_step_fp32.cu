@@ -7,10 +7,16 @@
 
 namespace dem {
 
-void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, cudaStream_t s) {
+void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, bool split, cudaStream_t s) {
   bool el = false, fr = false;
   for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
   const bool bd = a.nbond > 0;
+  if (split && !eval) {
+    if (!rot) return launch_split_tpp<false, F_ELASTIC, true>(a, tpp, s);
+    if (!bd && fr && !el) return launch_split_tpp<true, F_FRIC, true>(a, tpp, s);
+    if (!bd && !fr) return launch_split_tpp<true, F_ELASTIC, true>(a, tpp, s);
+    return launch_split_tpp<true, F_ELASTIC | F_FRIC | F_BOND, true>(a, tpp, s);
+  }
   if (eval) {
     if (!rot) return launch_step_tpp<false, F_ELASTIC, true, true>(a, tpp, s);
     if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC, true, true>(a, tpp, s);

@@ -46,9 +46,11 @@ def test_fp32_force_error_elastic_nrot(gpu):
     assert err[0] <= 1e-5, err
 
 
-def test_fp32_trajectory_close_to_fp64(gpu):
+@pytest.mark.parametrize("split", [0, 1])
+def test_fp32_trajectory_close_to_fp64(gpu, split):
     a, b = S.friction_pack(gpu), S.friction_pack(gpu)
     b.set_option("precision", 32)
+    b.set_option("split", split)
     a.step(100)
     b.step(100)
     pa, pb = a.particles(), b.particles()

@@ -135,3 +135,25 @@ def test_out_of_domain_particle_is_deleted(gpu, orc):
                     s.particles()["id"]))
     assert res[0][0] == res[1][0] == 1
     assert np.array_equal(res[0][1], res[1][1])
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_split_and_fused_step_kernels(gpu, orc, split):
+    """The two-kernel step (pair sums, then integration) and the fused kernel agree with the oracle."""
+    a, b = S.friction_pack(gpu), S.friction_pack(orc)
+    a.set_option("split", split)
+    a.step(150)
+    b.step(150)
+    _cmp(a, b, ["friction"])
+    c, d = S.gravity_box(gpu, 6), S.gravity_box(orc, 6)
+    c.set_option("split", split)
+    c.step(150)
+    d.step(150)
+    _cmp(c, d, ["elastic"])
+    e, f = S.bonded_block(gpu, strength=(0.05, 0.1, 0.1, 0.05)), S.bonded_block(orc, strength=(0.05, 0.1, 0.1, 0.05))
+    e.set_option("split", split)
+    S.run_loaded(e, 300, 2e-4)
+    S.run_loaded(f, 300, 2e-4)
+    for x, y in zip(e.breaks(), f.breaks()):
+        assert np.array_equal(x, y)
+    _cmp(e, f, ["bonds", "friction"])
