@@ -130,6 +130,11 @@ struct StepArgs {
   double visc_lin, visc_rot, dt_lin, dt_rot;
   int iter_lin, iter_rot;
   int store_forces;
+  // adjoint recompute pass only (null otherwise): the pair + bond + wall + body force
+  // sums before damping, and the damping iterations (lin, rot) of every particle
+  double4* f_int;
+  double4* m_int;
+  unsigned char* damp_iters;
   double* wall_partial;     // [gridDim.x][kMaxWalls][3]
   double* wall_force;       // [kMaxWalls][3]: reaction of each wall group (adds into CWall::m_force)
   unsigned* block_counter;  // last-block detection (wraps to 0 by itself)

@@ -458,9 +458,73 @@ __global__ void k_wall_servo(Particles P, int cur, int w, WallDev* walls, double
 // ---------------------------------------------------------------------------
 static inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
-void launch_scan(const int* in, int* out, int n, int* total, cudaStream_t s) {
-  k_scan<<<1, 1024, 0, s>>>(in, out, n, total);
+// Block-local exclusive scan of one 8192-element chunk per block; the chunk total to bsum.
+__global__ void k_scan_chunks(const int* in, int* out, int n, int* bsum) {
+  __shared__ int warp_sums[32];
+  const int T = blockDim.x;
+  const int base = blockIdx.x * T * 8;
+  int v[8];
+  int local = 0;
+  const int start = base + threadIdx.x * 8;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int idx = start + k;
+    v[k] = idx < n ? in[idx] : 0;
+    local += v[k];
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int t = lane < (T >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warp_sums[lane] = t;
+  }
+  __syncthreads();
+  int excl = (w > 0 ? warp_sums[w - 1] : 0) + x - local;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int idx = start + k;
+    if (idx < n) out[idx] = excl;
+    excl += v[k];
+  }
+  if (threadIdx.x == T - 1) bsum[blockIdx.x] = excl;
 }
+
+__global__ void k_scan_add(int* out, int n, const int* boff) {
+  const int base = blockIdx.x * blockDim.x * 8;
+  const int off = boff[blockIdx.x];
+  for (int k = threadIdx.x; k < blockDim.x * 8; k += blockDim.x) {
+    const int idx = base + k;
+    if (idx < n) out[idx] += off;
+  }
+}
+
+// Exclusive scan of n ints (in place allowed), total to *total.  Up to one
+// 8192-element chunk: one block; beyond: chunk scans, a scan of the chunk totals
+// (in tmp, >= chunks + 1 ints) and an offset pass.
+void launch_scan(const int* in, int* out, int n, int* total, int* tmp, cudaStream_t s) {
+  constexpr int kChunk = 1024 * 8;
+  if (n <= kChunk || !tmp) {
+    k_scan<<<1, 1024, 0, s>>>(in, out, n, total);
+    return;
+  }
+  const int nb = (n + kChunk - 1) / kChunk;
+  k_scan_chunks<<<nb, 1024, 0, s>>>(in, out, n, tmp);
+  k_scan<<<1, 1024, 0, s>>>(tmp, tmp, nb, total);
+  k_scan_add<<<nb, 1024, 0, s>>>(out, n, tmp);
+}
+int scan_tmp_ints(int n) { return (n + 8191) / 8192 + 1; }
 void launch_bin(const Grid& g, const Particles& P, int cur, int* cell_count, cudaStream_t s) {
   if (P.n) k_bin<<<nblk(P.n, 256), 256, 0, s>>>(g, P, cur, cell_count);
 }
@@ -489,13 +553,13 @@ template void launch_pairs_write<float4>(const Grid&, const Particles&, int, con
                                          const int*, unsigned long long*, int, const unsigned long long*, int,
                                          const float4*, float4*, cudaStream_t);
 void launch_adj(const unsigned long long* keys, int m, int n, int* adj_count, int* p1_start, int* adj_start,
-                int* adj_cursor, int2* adj, int* total, cudaStream_t s) {
+                int* adj_cursor, int2* adj, int* total, int* tmp, cudaStream_t s) {
   cudaMemsetAsync(adj_count, 0, sizeof(int) * (n + 1), s);
   cudaMemsetAsync(adj_cursor, 0, sizeof(int) * (n + 1), s);
   int t = (m > n + 1 ? m : n + 1);
   k_adj_count<<<nblk(t, 256), 256, 0, s>>>(keys, m, n, adj_count, p1_start);
   if (n) k_adj_add_p1<<<nblk(n, 256), 256, 0, s>>>(n, p1_start, adj_count);
-  k_scan<<<1, 1024, 0, s>>>(adj_count, adj_start, n + 1, total);
+  launch_scan(adj_count, adj_start, n + 1, total, tmp, s);
   if (m) k_adj_fill<<<nblk(m, 256), 256, 0, s>>>(keys, m, p1_start, adj_start, adj_cursor, adj);
   if (n) k_adj_sort<<<nblk(n, 256), 256, 0, s>>>(n, p1_start, adj_start, adj);
 }

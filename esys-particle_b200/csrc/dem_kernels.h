@@ -5,7 +5,8 @@
 
 namespace dem {
 
-void launch_scan(const int* in, int* out, int n, int* total, cudaStream_t s);
+void launch_scan(const int* in, int* out, int n, int* total, int* tmp, cudaStream_t s);
+int scan_tmp_ints(int n);
 void launch_bin(const Grid& g, const Particles& P, int cur, int* cell_count, cudaStream_t s);
 void launch_scatter_cells(const Particles& P, const int* cell_start, int* cursor, int* cell_list, cudaStream_t s);
 void launch_sort_cells(int ncell, const int* cell_start, int* cell_list, cudaStream_t s);
@@ -16,7 +17,7 @@ void launch_pairs_write(const Grid& g, const Particles& P, int cur, const int* c
                         const int* start, unsigned long long* keys, int kind, const unsigned long long* old_keys,
                         int old_n, const H* old_hist, H* hist, cudaStream_t s);
 void launch_adj(const unsigned long long* keys, int m, int n, int* adj_count, int* p1_start, int* adj_start,
-                int* adj_cursor, int2* adj, int* total, cudaStream_t s);
+                int* adj_cursor, int2* adj, int* total, int* tmp, cudaStream_t s);
 void launch_newlist_count(const Grid& g, const Particles& P, const int* cs, const int* cl, const ExclDev& ex,
                           const unsigned long long* keys, int m, int check_in, int* count, cudaStream_t s);
 void launch_newlist_write(const Grid& g, const Particles& P, const int* cs, const int* cl, const ExclDev& ex,

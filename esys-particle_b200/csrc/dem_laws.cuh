@@ -106,11 +106,15 @@ __device__ __forceinline__ bool friction_persistent(const V& x1, double r1, cons
 // Scaled RotBond constants (ARotBondedInteraction.cpp:141-180 overridden by
 // CRotBondedInteraction ctor, Model/RotBondedInteraction.cpp:122-161).  dist0 is
 // |m_D|, the particle distance when the bond was created.
-struct BondK {
-  double kr, ks, kb, kt, max_n, max_s, max_b, max_t;
+template <class S>
+struct BondKT {
+  S kr, ks, kb, kt;
+  double max_n, max_s, max_b, max_t;
 };
-__device__ __forceinline__ BondK bond_k(double kr, double ks, double kt, double kb, double mn, double ms, double mt,
-                                        double mb, int scaling, int meanR, double dist0, double r1, double r2) {
+using BondK = BondKT<double>;
+template <class S>
+__device__ __forceinline__ BondKT<S> bond_k_t(S kr, S ks, S kt, S kb, double mn, double ms, double mt, double mb,
+                                              int scaling, int meanR, double dist0, double r1, double r2) {
   double effR = 1.0, effL = 1.0, effA = 1.0, J = 1.0, I = 1.0;
   if (scaling) {
     if (meanR) effR = 0.5 * dist0; else effR = fmin(r1, r2);
@@ -119,7 +123,7 @@ __device__ __forceinline__ BondK bond_k(double kr, double ks, double kt, double 
     J = 0.5 * effR * effR * effR * effR;
     I = 0.5 * J;
   }
-  BondK b;
+  BondKT<S> b;
   b.kr = kr * effA / effL;
   b.ks = ks * effA / effL;
   b.kb = kb * I / effL;
@@ -130,91 +134,104 @@ __device__ __forceinline__ BondK bond_k(double kr, double ks, double kt, double 
   b.max_t = mt * J / effR;
   return b;
 }
-
-// calc_angle (Model/ARotBondedInteraction.cpp:22-51).
-__device__ __forceinline__ double calc_angle(double s_in, double c_os) {
-  if (s_in > 0.0) return (c_os >= 1.0 || c_os <= -1.0) ? 0.0 : acos(c_os);
-  if (s_in == 0.0) return 0.0;
-  return (c_os >= 1.0 || c_os <= -1.0) ? 0.0 : -acos(c_os);
+__device__ __forceinline__ BondK bond_k(double kr, double ks, double kt, double kb, double mn, double ms, double mt,
+                                        double mb, int scaling, int meanR, double dist0, double r1, double r2) {
+  return bond_k_t<double>(kr, ks, kt, kb, mn, ms, mt, mb, scaling, meanR, dist0, r1, r2);
 }
 
-struct BondOut {
-  V force;    // applied to p1 (p2 gets -force)
-  V moment1;  // applied to p1
-  V moment2;  // applied to p2
-  double nF, shF, tM, bM;
+// calc_angle (Model/ARotBondedInteraction.cpp:22-51).
+template <class S>
+__device__ __forceinline__ S calc_angle(const S& s_in, const S& c_os) {
+  if (s_in > 0.0) return (c_os >= 1.0 || c_os <= -1.0) ? S(0.0) : acos(c_os);
+  if (s_in == 0.0) return S(0.0);
+  return (c_os >= 1.0 || c_os <= -1.0) ? S(0.0) : -acos(c_os);
+}
+
+template <class S>
+struct BondOutT {
+  V3<S> force;    // applied to p1 (p2 gets -force)
+  V3<S> moment1;  // applied to p1
+  V3<S> moment2;  // applied to p2
+  S nF, shF, tM, bM;
 };
+using BondOut = BondOutT<double>;
 
 // ARotBondedInteraction::calcForces (Model/ARotBondedInteraction.cpp:307-448).
-__device__ __forceinline__ void law_bond(const BondK& K, const V& m_D, const V& x1, double r1, const Qd& q1,
-                                         const V& x2, double r2, const Qd& q2, BondOut& o) {
+// Templated on the scalar S: S = double for the step kernels, a forward-mode
+// dual number for the adjoint (dem_adjoint.cu).
+template <class S>
+__device__ __forceinline__ void law_bond_t(const BondKT<S>& K, const V3<S>& m_D, const V3<S>& x1, double r1,
+                                           const Quat<S>& q1, const V3<S>& x2, double r2, const Quat<S>& q2,
+                                           BondOutT<S>& o) {
+  using VS = V3<S>;
+  using QS = Quat<S>;
   const double HALF_SQRT_2 = 0.5 * sqrt(2.0);
-  double s_fai = 0.0, c_fai = 0.0, c_pasi2 = 0.0, s_pasi2 = 0.0, sita = 0.0, pasi = 0.0;
-  const M3<double> mat0 = to_matrix(q1);
-  const V rbp = x2 - x1;
-  const double rbpNorm = norm(rbp);
-  const V rb = mul(mat0, x2 - x1);
-  const double rbNorm = norm(rb);
+  S s_fai = 0.0, c_fai = 0.0, c_pasi2 = 0.0, s_pasi2 = 0.0, sita = 0.0, pasi = 0.0;
+  const M3<S> mat0 = to_matrix(q1);
+  const VS rbp = x2 - x1;
+  const S rbpNorm = norm(rbp);
+  const VS rb = mul(mat0, x2 - x1);
+  const S rbNorm = norm(rb);
   const double r_0Norm = r1 + r2;
-  const V delta_r = (rbNorm - r_0Norm) * rb / rbNorm;
-  const V Fr = K.kr * delta_r;
-  const double gama_cos = dot(rb, m_D) / (rbNorm * norm(m_D));
-  double gama = 0.0;
+  const VS delta_r = (rbNorm - r_0Norm) * rb / rbNorm;
+  const VS Fr = K.kr * delta_r;
+  const S gama_cos = dot(rb, m_D) / (rbNorm * norm(m_D));
+  S gama = 0.0;
   if (gama_cos < 1.0 && gama_cos > -1.0) gama = acos(gama_cos);
-  const V rb_0 = cross(rb, m_D);
-  const V rb_b0 = cross(rb, rb_0);
-  const double rb_b0Norm = norm(rb_b0);
-  V Fst = mk(0.0, 0.0, 0.0);
+  const VS rb_0 = cross(rb, m_D);
+  const VS rb_b0 = cross(rb, rb_0);
+  const S rb_b0Norm = norm(rb_b0);
+  VS Fst = mk(S(0.0), S(0.0), S(0.0));
   if (rb_b0Norm != 0) Fst = K.ks * r_0Norm * gama * rb_b0 / rb_b0Norm;
-  V Mst = mk(0.0, 0.0, 0.0);
-  const double rb_0Norm = norm(rb_0);
+  VS Mst = mk(S(0.0), S(0.0), S(0.0));
+  const S rb_0Norm = norm(rb_0);
   if (rb_0Norm != 0) Mst = -norm(Fst) * rb_0 / rb_0Norm;
-  const double m0 = HALF_SQRT_2 * sqrt((rbNorm + rb.z) / rbNorm);
-  double m1 = -HALF_SQRT_2 * sqrt((rbNorm - rb.z) / rbNorm);
-  double m2 = -m1;
-  const double m3 = 0.0;
-  const double rbX2PlusRbY2 = rb.x * rb.x + rb.y * rb.y;
+  const S m0 = HALF_SQRT_2 * sqrt((rbNorm + rb.z) / rbNorm);
+  S m1 = -HALF_SQRT_2 * sqrt((rbNorm - rb.z) / rbNorm);
+  S m2 = -m1;
+  const S m3 = 0.0;
+  const S rbX2PlusRbY2 = rb.x * rb.x + rb.y * rb.y;
   if (rbX2PlusRbY2 != 0.0) {
-    const double denomSqrt = sqrt(rbX2PlusRbY2);
+    const S denomSqrt = sqrt(rbX2PlusRbY2);
     m1 = m1 * rb.y / denomSqrt;
     m2 = m2 * rb.x / denomSqrt;
   }
-  const Qd qm{m0, mk(m1, m2, m3)};
-  const M3<double> mat = to_matrix(qm);
-  const Qd rp = qmul(qinv(q1), q2);
-  const Qd r = qmul(qmul(qinv(qm), rp), qm);
-  const double temp0 = r.s * r.s + r.v.z * r.v.z;
+  const QS qm{m0, mk(m1, m2, m3)};
+  const M3<S> mat = to_matrix(qm);
+  const QS rp = qmul(qinv(q1), q2);
+  const QS r = qmul(qmul(qinv(qm), rp), qm);
+  const S temp0 = r.s * r.s + r.v.z * r.v.z;
   if (temp0 == 0.0) {
     pasi = 0.0;
   } else {
-    const double sqrtTemp0 = sqrt(temp0);
+    const S sqrtTemp0 = sqrt(temp0);
     c_pasi2 = r.s / sqrtTemp0;
     s_pasi2 = r.v.z / sqrtTemp0;
     pasi = 2.0 * calc_angle(s_pasi2, c_pasi2);
   }
-  const V Mtp = mk(0.0, 0.0, K.kt * pasi);
-  const V Mtr = mulT(mat, Mtp);
-  const double temp2 = r.v.x * r.v.x + r.v.y * r.v.y;
-  const double temp3 = r.v.x * r.v.z + r.s * r.v.y;
-  const double temp4 = r.v.y * r.v.z - r.s * r.v.x;
-  V Mbr = mk(0.0, 0.0, 0.0), Fsr = mk(0.0, 0.0, 0.0), Msr = mk(0.0, 0.0, 0.0);
+  const VS Mtp = mk(S(0.0), S(0.0), K.kt * pasi);
+  const VS Mtr = mulT(mat, Mtp);
+  const S temp2 = r.v.x * r.v.x + r.v.y * r.v.y;
+  const S temp3 = r.v.x * r.v.z + r.s * r.v.y;
+  const S temp4 = r.v.y * r.v.z - r.s * r.v.x;
+  VS Mbr = mk(S(0.0), S(0.0), S(0.0)), Fsr = Mbr, Msr = Mbr;
   if (temp2 != 0.0) {
-    const double temp1 = temp0 - temp2;
+    const S temp1 = temp0 - temp2;
     if (temp1 >= 1.0 || temp1 <= -1.0) sita = 0.0; else sita = acos(temp1);
     if (temp0 == 0.0) {
-      const double sqrtDenom = sqrt(temp2);
+      const S sqrtDenom = sqrt(temp2);
       c_fai = r.v.y / sqrtDenom;
       s_fai = -r.v.x / sqrtDenom;
     } else {
-      const double sqrtDenom = sqrt(temp0 * temp2);
+      const S sqrtDenom = sqrt(temp0 * temp2);
       c_fai = temp3 / sqrtDenom;
       s_fai = temp4 / sqrtDenom;
     }
-    const V Mbp = mk(-0.5 * K.kb * sita * s_fai, 0.5 * K.kb * sita * c_fai, 0.0);
+    const VS Mbp = mk(-0.5 * K.kb * sita * s_fai, 0.5 * K.kb * sita * c_fai, S(0.0));
     Mbr = mulT(mat, Mbp);
-    const V Fsp = mk(-0.5 * K.ks * c_fai * sita * r_0Norm, -0.5 * K.ks * s_fai * sita * r_0Norm, 0.0);
+    const VS Fsp = mk(-0.5 * K.ks * c_fai * sita * r_0Norm, -0.5 * K.ks * s_fai * sita * r_0Norm, S(0.0));
     Fsr = mulT(mat, Fsp);
-    const V Msp = mk(0.5 * K.ks * s_fai * sita * r_0Norm, -0.5 * K.ks * c_fai * sita * r_0Norm, 0.0);
+    const VS Msp = mk(0.5 * K.ks * s_fai * sita * r_0Norm, -0.5 * K.ks * c_fai * sita * r_0Norm, S(0.0));
     Msr = mulT(mat, Msp);
   }
   const double eq_rad1 = r1 / (r1 + r2);
@@ -226,9 +243,14 @@ __device__ __forceinline__ void law_bond(const BondK& K, const V& m_D, const V& 
   o.tM = norm(Mtr);
   o.bM = norm(Mbr);
   const double r0 = r1 + r2;
-  const V D = x1 - x2;
-  const double dist = sqrt(dot(D, D));
+  const VS D = x1 - x2;
+  const S dist = sqrt(dot(D, D));
   o.nF = ((dist < r0) ? -1.0 : 1.0) * norm(Fr);
+}
+
+__device__ __forceinline__ void law_bond(const BondK& K, const V& m_D, const V& x1, double r1, const Qd& q1,
+                                         const V& x2, double r2, const Qd& q2, BondOut& o) {
+  law_bond_t<double>(K, m_D, x1, r1, q1, x2, r2, q2, o);
 }
 
 // CRotBondedInteraction::broken (Model/RotBondedInteraction.cpp:175-219), beta1 = beta2 = 1.
@@ -258,7 +280,7 @@ __device__ __forceinline__ bool law_wall(double k, const V& o, const V& n, const
 // rotational form (Model/RotDamping.hpp:58-84) is the same iteration on (omega,
 // moment, 1/I, I).
 __device__ __forceinline__ V damping_force(const V& v, const V& frc, double s, double mass, double visc, double dt,
-                                           int maxiter) {
+                                           int maxiter, int* iterations = nullptr) {
   const double s_limit2 = 1e-12;
   const V vref = mk(0.0, 0.0, 0.0);
   V v_rel = mk(0.0, 0.0, 0.0);
@@ -270,6 +292,7 @@ __device__ __forceinline__ V damping_force(const V& v, const V& frc, double s, d
     v_rel = v - vref + s * dt * (frc - v_rel * visc * mass);
     error = norm2(v_rel - v_old);
   }
+  if (iterations) *iterations = count;
   if (count >= maxiter) v_rel = mk(0.0, 0.0, 0.0);
   return -1.0 * visc * v_rel * mass;
 }

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 namespace dem {
 
 template <class S>
@@ -32,6 +34,11 @@ template <class S>
 __host__ __device__ __forceinline__ V3<S> operator*(S f, const V3<S>& a) { return {f * a.x, f * a.y, f * a.z}; }
 template <class S>
 __host__ __device__ __forceinline__ V3<S> operator/(const V3<S>& a, S s) { return {a.x / s, a.y / s, a.z / s}; }
+// Mixed forms for non-double scalars (the adjoint's dual numbers): vector of S times a double.
+template <class S, typename std::enable_if<!std::is_same<S, double>::value, int>::type = 0>
+__host__ __device__ __forceinline__ V3<S> operator*(const V3<S>& a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class S, typename std::enable_if<!std::is_same<S, double>::value, int>::type = 0>
+__host__ __device__ __forceinline__ V3<S> operator*(double f, const V3<S>& a) { return {f * a.x, f * a.y, f * a.z}; }
 template <class S>
 __host__ __device__ __forceinline__ S dot(const V3<S>& a, const V3<S>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 template <class S>

@@ -119,7 +119,7 @@ struct DemSim {
   int cur = 0;
   // cells
   int ncell = 0;
-  DBuf<int> cell_count, cell_start, cell_cursor, cell_list, scratch_i, scratch_j, scalars;
+  DBuf<int> cell_count, cell_start, cell_cursor, cell_list, scratch_i, scratch_j, scalars, scan_tmp;
   // groups (std::map keeps the reference's name order)
   std::map<std::string, Wall> walls;
   std::map<std::string, WallGroup> wig;
@@ -173,7 +173,7 @@ struct DemSim {
                   P.moment_eval, P.sum_f, P.sum_m, P.pflags, P.flagged, P.id, P.tag, P.cell};
     for (void* p : ps) if (p) cudaFree(p);
     cell_count.release(); cell_start.release(); cell_cursor.release(); cell_list.release();
-    scratch_i.release(); scratch_j.release(); scalars.release();
+    scratch_i.release(); scratch_j.release(); scalars.release(); scan_tmp.release();
     d_walls.release(); d_wall_vel.release(); d_wall_partial.release(); d_wall_force.release();
     d_block_counter.release(); d_step.release(); d_ctrl.release(); d_stop.release();
     stage.release(); stage_slot.release();
@@ -433,7 +433,8 @@ struct DemSim {
   void search_neighbors() {
     DEM_CUDA(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * (ncell + 1), s));
     launch_bin(g, P, cur, cell_count.p, s);
-    launch_scan(cell_count.p, cell_start.p, ncell + 1, scalars.p, s);
+    scan_tmp.reserve(scan_tmp_ints(std::max(ncell + 1, n + 2)));
+    launch_scan(cell_count.p, cell_start.p, ncell + 1, scalars.p, scan_tmp.p, s);
     DEM_CUDA(cudaMemsetAsync(cell_cursor.p, 0, sizeof(int) * (ncell + 1), s));
     cell_list.reserve(std::max(n, 1));
     launch_scatter_cells(P, cell_start.p, cell_cursor.p, cell_list.p, s);
@@ -461,7 +462,8 @@ struct DemSim {
                        DBuf<int>& adj_cursor, DBuf<int>& p1_start, DBuf<int2>& adj) {
     adj_start.reserve(n + 2); adj_count.reserve(n + 2); adj_cursor.reserve(n + 2); p1_start.reserve(n + 2);
     adj.reserve(std::max(2 * m, 1));
-    launch_adj(keys.p, m, n, adj_count.p, p1_start.p, adj_start.p, adj_cursor.p, adj.p, scalars.p + 1, s);
+    scan_tmp.reserve(scan_tmp_ints(n + 2));
+    launch_adj(keys.p, m, n, adj_count.p, p1_start.p, adj_start.p, adj_cursor.p, adj.p, scalars.p + 1, scan_tmp.p, s);
     c_launches += 5;
   }
 
@@ -471,7 +473,8 @@ struct DemSim {
     ExclDev ex = excl_of(G);
     scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
     launch_pairs_count(g, P, cur, cell_start.p, cell_list.p, ex, scratch_i.p, s);
-    launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, s);
+    scan_tmp.reserve(scan_tmp_ints(n + 2));
+    launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, scan_tmp.p, s);
     const int m = read_int(scalars.p);
     c_launches += 3;
     G.keys_spare.reserve(std::max(m, 1));
@@ -505,7 +508,8 @@ struct DemSim {
     const int check_in = G.kind == 1;  // PIS_NE appends without the isIn test
     scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
     launch_newlist_count(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_i.p, s);
-    launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, s);
+    scan_tmp.reserve(scan_tmp_ints(n + 2));
+    launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, scan_tmp.p, s);
     const int nb = read_int(scalars.p);
     c_launches += 3;
     if (nb > 0) {

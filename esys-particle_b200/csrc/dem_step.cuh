@@ -308,9 +308,18 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
     M += Mp;
     // 1/m and 1/I as the particle constructors compute them (Particle.cpp:95-99, RotParticle.cpp:35)
     const double2 iv = make_double2(v4.w != 0.0 ? 1.0 / v4.w : 0.0, 1.0 / w4.w);
+    if (a.f_int) {
+      a.f_int[i] = d4(F, 0.0);
+      a.m_int[i] = d4(M, 0.0);
+    }
     // 5. damping, last (SubLattice.hpp:2140-2145): "Damping" then "RotDamping"
-    if (a.damp_lin) F += damping_force(xyz(v4), F, iv.x, v4.w, a.visc_lin, a.dt_lin, a.iter_lin);
-    if (ROT && a.damp_rot) M += damping_force(xyz(w4), M, iv.y, w4.w, a.visc_rot, a.dt_rot, a.iter_rot);
+    int it_lin = 0, it_rot = 0;
+    if (a.damp_lin) F += damping_force(xyz(v4), F, iv.x, v4.w, a.visc_lin, a.dt_lin, a.iter_lin, &it_lin);
+    if (ROT && a.damp_rot) M += damping_force(xyz(w4), M, iv.y, w4.w, a.visc_rot, a.dt_rot, a.iter_rot, &it_rot);
+    if (a.damp_iters) {
+      a.damp_iters[2 * i] = (unsigned char)(it_lin > 255 ? 255 : it_lin);
+      a.damp_iters[2 * i + 1] = (unsigned char)(it_rot > 255 ? 255 : it_rot);
+    }
     if (EVAL) {
       a.P.force_eval[i] = d4(F, 0.0);
       if (ROT) a.P.moment_eval[i] = d4(M, 0.0);

@@ -157,3 +157,12 @@ def test_split_and_fused_step_kernels(gpu, orc, split):
     for x, y in zip(e.breaks(), f.breaks()):
         assert np.array_equal(x, y)
     _cmp(e, f, ["bonds", "friction"])
+
+
+def test_large_pack_multiblock_scans(gpu, orc):
+    """More than 8192 particles and cells: the rebuild's scans run as multi-block scans."""
+    a = S.friction_pack(gpu, nx=24, ny=18, nz=24, seed=11)
+    b = S.friction_pack(orc, nx=24, ny=18, nz=24, seed=11)
+    a.step(30)
+    b.step(30)
+    _cmp(a, b, ["friction"])
