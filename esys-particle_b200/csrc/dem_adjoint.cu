@@ -1,0 +1,366 @@
+// Reverse-mode kernels of the differentiable loading window (dem_window_adjoint).
+//
+// The window is the FP64 step with the contact topology and the bond state
+// frozen: the pair lists of the dynamic groups, the intact bonds and the wall
+// candidates are those of the forward pass, and every branch of a law (touching,
+// slipping, acos guards, the damping iteration count) is the one the forward
+// pass took.  The state of particle i at step t is (x, v, omega, q) and the
+// friction history of each RotFriction pair; the outputs whose gradients are
+// wanted are the platen reactions (CWall::m_force after each step).
+//
+// One reverse step takes lambda_{t+1}, the adjoint of the state after step t,
+// to lambda_t, with the forward states of the step recomputed from checkpoints:
+//   k_adj_pre   per particle, hand-written: quaternion normalisation and update
+//               (CRotParticle::integrate + rescale, Model/RotParticle.cpp:277-321),
+//               the Euler velocity / position update (Model/Particle.cpp:257-274),
+//               the damping fixed point unrolled over the forward iteration count
+//               (Model/Damping.hpp:99-124, Model/RotDamping.hpp:58-84), the
+//               elastic walls (Model/EWallInteraction.hpp:42-78) and the loss
+//               term of the reactions.  Produces lF, lM: the adjoint of the
+//               force and moment sums before damping.
+//   k_adj_bond  per bond: the RotBond law (Model/ARotBondedInteraction.cpp:307-448)
+//               evaluated on 18-component dual numbers (x1, q1, x2, q2, kr, ks,
+//               kt, kb) and contracted with lF / lM of its two particles.
+//   k_adj_pair  per pair of a dynamic group: CElasticInteraction (7 components)
+//               or CRotFrictionInteraction (23: x1, x2, v1, v2, w1, w2, the
+//               tangential history, k, ks), contracted with lF / lM and the
+//               adjoint of the pair's next history; writes the history adjoint.
+//   k_adj_post  per particle: the bond and pair contributions gathered in
+//               adjacency order (no atomics, run-to-run reproducible).
+// Parameter gradients accumulate in per-bond / per-pair / per-particle slots
+// across the window and are reduced once, in a fixed order, at the end.
+#include "dem_adjoint.h"
+#include "dem_common.cuh"
+#include "dem_dual.cuh"
+#include "dem_laws.cuh"
+
+namespace dem {
+
+__device__ __forceinline__ V xyzv(const double4& a) { return mk(a.x, a.y, a.z); }
+
+// lambda_q . d[(0,w)(x)q]/dq and lambda_q . d[(0,w)(x)q]/dw (Quaternion.hpp operator*):
+// (0,w)(x)q = ( -w.qv , qs w + w x qv ) is bilinear in (w, q).
+__device__ __forceinline__ void omega_times_vjp(const V& w, const Qd& q, const Qd& lq, Qd& lq_out, V& lw_out) {
+  lq_out.s = dot(lq.v, w);
+  lq_out.v = -lq.s * w + cross(lq.v, w);
+  lw_out = -lq.s * q.v + q.s * lq.v + cross(q.v, lq.v);
+}
+
+// G = sum_{k<c} (-a)^k (the c-th damping iterate is G u) and dG/da.
+__device__ __forceinline__ void damp_series(double a, int c, double& G, double& dG) {
+  G = 0.0;
+  dG = 0.0;
+  double p = 1.0;   // (-a)^k
+  double dp = 0.0;  // d/da (-a)^k
+  for (int k = 0; k < c; ++k) {
+    G += p;
+    dG += dp;
+    dp = -(double)(k + 1) * p;
+    p *= -a;
+  }
+}
+
+// Reverse of one damping group on one particle: F_tot = F + D(v, F),
+// D = -visc m G (v + s dt F) when the fixed point converged in c < maxiter iterations.
+__device__ __forceinline__ void damping_vjp(const V& v, const V& F, double s, double m, double visc, double dt, int c,
+                                            int maxiter, const V& lFtot, V& lF, V& lv, double& gvisc) {
+  lF = lFtot;
+  if (c >= maxiter) return;  // v_rel = 0: no damping force
+  double G, dGa;
+  damp_series(s * dt * visc * m, c, G, dGa);
+  const V u = v + (s * dt) * F;
+  lF = lFtot * (1.0 - visc * m * G * s * dt);
+  lv = lv + (-visc * m * G) * lFtot;
+  const double dGdvisc = dGa * s * dt * m;
+  gvisc += dot(lFtot, (-m * (G + visc * dGdvisc)) * u);
+}
+
+__global__ void k_adj_pre(const AdjArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const unsigned pf = A.pflags[i];
+  if (!(pf & PF_ALIVE)) return;
+  const double dt = A.dt;
+  const double4 p4 = A.s0.pr[i], v4 = A.s0.vm[i];
+  const bool dyn = pf & PF_DYN;
+  const double m = v4.w;
+  const double invm = m != 0.0 ? 1.0 / m : 0.0;  // as the step kernel forms it
+  V lx = xyzv(A.lx[i]), lv = xyzv(A.lv[i]);
+
+  // position and velocity: v1 = v + F_tot/m dt, x1 = x + v1 dt
+  V lFtot = mk(0.0, 0.0, 0.0), lv_t = lv;
+  if (dyn) {
+    const V lv_tot = lv + dt * lx;
+    lFtot = (invm * dt) * lv_tot;
+    lv_t = lv_tot;
+  }
+  V lx_t = lx;
+  V lF = lFtot;
+  double gl = 0.0, gr = 0.0;
+  if (A.damp_lin)
+    damping_vjp(xyzv(v4), xyzv(A.f_int[i]), invm, m, A.visc_lin, A.dt_lin, A.iters[2 * i], A.iter_lin, lFtot, lF,
+                lv_t, gl);
+
+  V lM = mk(0.0, 0.0, 0.0), lw_t = lM;
+  Qd lq_t{0.0, lM};
+  if (A.rot) {
+    const double4 w4 = A.s0.wi[i], q4 = A.s0.qq[i], w1 = A.s1.wi[i];
+    const double I = w4.w, invI = 1.0 / I;
+    const V lw = xyzv(A.lw[i]);
+    const double4 lq4 = A.lq[i];
+    const Qd lq1{lq4.x, mk(lq4.y, lq4.z, lq4.w)};
+    const Qd q{q4.x, mk(q4.y, q4.z, q4.w)};
+    const bool rot = pf & PF_ROT;
+    // q' = q + dt/2 (0, w1) (x) q for rotating particles, then q1 = q' / |q'|
+    Qd qp = q;
+    const V wn = xyzv(w1);
+    if (rot) {
+      const Qd dq = qmul(Qd{0.0, wn}, q);
+      const double c = dt / 2.0;
+      qp.s = q.s + c * dq.s;
+      qp.v = q.v + c * dq.v;
+    }
+    const double nq = sqrt(qp.s * qp.s + dot(qp.v, qp.v));
+    const Qd qn{qp.s / nq, qp.v / nq};
+    const double pr = qn.s * lq1.s + dot(qn.v, lq1.v);
+    const Qd lqp{(lq1.s - qn.s * pr) / nq, (lq1.v - qn.v * pr) / nq};
+    lq_t = lqp;
+    if (rot) {
+      Qd aq;
+      V aw;
+      omega_times_vjp(wn, q, lqp, aq, aw);
+      const double c = dt / 2.0;
+      lq_t.s += c * aq.s;
+      lq_t.v += c * aq.v;
+      // w1 = w + dt/I M_tot; w1 feeds the output spin and the quaternion update
+      const V lw_tot = lw + c * aw;
+      const V lMtot = (dt * invI) * lw_tot;
+      lw_t = lw_tot;
+      lM = lMtot;
+      if (A.damp_rot)
+        damping_vjp(xyzv(w4), xyzv(A.m_int[i]), invI, I, A.visc_rot, A.dt_rot, A.iters[2 * i + 1], A.iter_rot, lMtot,
+                    lM, lw_t, gr);
+    }
+  }
+
+  // elastic walls: f = k' (r - d) n for d = (x - o).n < r; inner candidates feed the reactions
+  const V x = xyzv(p4);
+  for (int w = 0; w < A.nwall; ++w) {
+    if (!(pf & (1u << (PF_WALL_SHIFT + w)))) continue;
+    const WallDev W = A.walls[w];
+    const V o = mk(W.ox, W.oy, W.oz), nn = mk(W.nx, W.ny, W.nz);
+    const double d = dot(x - o, nn);
+    if (!(d < p4.w)) continue;
+    double f = 1.0;
+    f *= 3.141592654 * p4.w;
+    const double mk_ = f * W.k;
+    V lf = lF;
+    if (pf & (1u << (PF_INNER_SHIFT + w))) lf = lf + mk(A.gR[3 * w], A.gR[3 * w + 1], A.gR[3 * w + 2]);
+    lx_t = lx_t + (-mk_ * dot(nn, lf)) * nn;
+  }
+  A.lx[i] = d4(lx_t, 0.0);
+  A.lv[i] = d4(lv_t, 0.0);
+  A.lF[i] = d4(lF, 0.0);
+  if (A.rot) {
+    A.lw[i] = d4(lw_t, 0.0);
+    A.lq[i] = make_double4(lq_t.s, lq_t.v.x, lq_t.v.y, lq_t.v.z);
+    A.lM[i] = d4(lM, 0.0);
+  }
+  A.gvisc[2 * i] += gl;
+  A.gvisc[2 * i + 1] += gr;
+}
+
+using D18 = Dual<18>;
+
+__global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
+  const AdjBond& B = A.bond[gi];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B.nb) return;
+  double4* out = B.gb + 4 * (size_t)b;
+  if (B.broken_step[b] <= A.step) {  // removed before this step
+    out[0] = out[1] = out[2] = out[3] = make_double4(0.0, 0.0, 0.0, 0.0);
+    return;
+  }
+  const int2 e = B.ends[b];
+  const double4 p1 = A.s0.pr[e.x], p2 = A.s0.pr[e.y], qa = A.s0.qq[e.x], qb = A.s0.qq[e.y];
+  const V x1d = xyzv(p1), x2d = image_of(A.g, x1d, xyzv(p2));
+  const V3<D18> x1 = mk(D18::seed(x1d.x, 0), D18::seed(x1d.y, 1), D18::seed(x1d.z, 2));
+  const Quat<D18> q1{D18::seed(qa.x, 3), mk(D18::seed(qa.y, 4), D18::seed(qa.z, 5), D18::seed(qa.w, 6))};
+  const V3<D18> x2 = mk(D18::seed(x2d.x, 7), D18::seed(x2d.y, 8), D18::seed(x2d.z, 9));
+  const Quat<D18> q2{D18::seed(qb.x, 10), mk(D18::seed(qb.y, 11), D18::seed(qb.z, 12), D18::seed(qb.w, 13))};
+  const double4 D0 = B.D0[b];
+  const V3<D18> mD = mk(D18(D0.x), D18(D0.y), D18(D0.z));
+  const double dist0 = sqrt(D0.x * D0.x + D0.y * D0.y + D0.z * D0.z);
+  const BondKT<D18> K = bond_k_t<D18>(D18::seed(B.kr, 14), D18::seed(B.ks, 15), D18::seed(B.kt, 16),
+                                      D18::seed(B.kb, 17), B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, p1.w,
+                                      p2.w);
+  BondOutT<D18> o;
+  law_bond_t<D18>(K, mD, x1, p1.w, q1, x2, p2.w, q2, o);
+  // p1 gets +force and moment1, p2 gets -force and moment2
+  const V lFd = xyzv(A.lF[e.x]) - xyzv(A.lF[e.y]);
+  const V lM1 = xyzv(A.lM[e.x]), lM2 = xyzv(A.lM[e.y]);
+  const D18 w = o.force.x * lFd.x + o.force.y * lFd.y + o.force.z * lFd.z + o.moment1.x * lM1.x +
+                o.moment1.y * lM1.y + o.moment1.z * lM1.z + o.moment2.x * lM2.x + o.moment2.y * lM2.y +
+                o.moment2.z * lM2.z;
+  out[0] = make_double4(w.d[0], w.d[1], w.d[2], 0.0);
+  out[1] = make_double4(w.d[3], w.d[4], w.d[5], w.d[6]);
+  out[2] = make_double4(w.d[7], w.d[8], w.d[9], 0.0);
+  out[3] = make_double4(w.d[10], w.d[11], w.d[12], w.d[13]);
+  double* gp = B.gpar + 4 * (size_t)b;
+  gp[0] += w.d[14];
+  gp[1] += w.d[15];
+  gp[2] += w.d[16];
+  gp[3] += w.d[17];
+}
+
+using D7 = Dual<7>;
+using D23 = Dual<23>;
+
+__device__ __forceinline__ V3<D23> seed3(const V& a, int k) {
+  return mk(D23::seed(a.x, k), D23::seed(a.y, k + 1), D23::seed(a.z, k + 2));
+}
+__device__ __forceinline__ D23 dotd(const V3<D23>& a, const V& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+__global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
+  const AdjDyn& G = A.dyn[gi];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= G.m) return;
+  const unsigned long long key = G.keys[k];
+  const int s1 = (int)(key >> 32), s2 = (int)(key & 0xffffffffu);
+  double4* out = G.gpair + 6 * (size_t)k;
+  const double4 pa = A.s0.pr[s1], pb = A.s0.pr[s2];
+  const V x1d = xyzv(pa), x2d = image_of(A.g, x1d, xyzv(pb));
+  const V lF1 = xyzv(A.lF[s1]), lF2 = xyzv(A.lF[s2]);
+  for (int c = 0; c < 6; ++c) out[c] = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (G.kind == 0) {
+    // CElasticInteraction: p2 gets F, p1 gets -F
+    const V3<D7> x1 = mk(D7::seed(x1d.x, 0), D7::seed(x1d.y, 1), D7::seed(x1d.z, 2));
+    const V3<D7> x2 = mk(D7::seed(x2d.x, 3), D7::seed(x2d.y, 4), D7::seed(x2d.z, 5));
+    const D7 keff = elastic_k_t<D7>(D7::seed(G.k, 6), G.scaling, pa.w, pb.w);
+    V3<D7> F;
+    if (!law_elastic_t<D7>(keff, x1, pa.w, x2, pb.w, F)) return;
+    const V l = lF2 - lF1;
+    const D7 w = F.x * l.x + F.y * l.y + F.z * l.z;
+    out[0] = make_double4(w.d[0], w.d[1], w.d[2], 0.0);
+    out[1] = make_double4(w.d[3], w.d[4], w.d[5], 0.0);
+    G.gpar[2 * (size_t)k] += w.d[6];
+    return;
+  }
+  // CRotFrictionInteraction
+  const double4 h = G.hist_in[k];
+  const V lH = xyzv(G.lH[k]);
+  const V3<D23> x1 = seed3(x1d, 0), x2 = seed3(x2d, 3);
+  const V3<D23> v1 = seed3(xyzv(A.s0.vm[s1]), 6), v2 = seed3(xyzv(A.s0.vm[s2]), 9);
+  const V3<D23> w1 = seed3(xyzv(A.s0.wi[s1]), 12), w2 = seed3(xyzv(A.s0.wi[s2]), 15);
+  const V3<D23> H = seed3(xyzv(h), 18);
+  D23 keff, kseff;
+  friction_k_t<D23>(D23::seed(G.k, 21), D23::seed(G.ks, 22), G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
+  FricOutT<D23> o;
+  law_friction_t<D23>(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, v1, w1, x2, pb.w, v2, w2, H,
+                      (((int)h.w) & 1) != 0, o);
+  if (!o.touching) {  // the history is reset: nothing flows back through it
+    G.lH[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+    return;
+  }
+  // p1 gets -fn + Ffric and M1, p2 gets fn - Ffric and M2; the next history is Ffric
+  const V lM1 = xyzv(A.lM[s1]), lM2 = xyzv(A.lM[s2]);
+  const D23 w = dotd(o.fn, lF2 - lF1) + dotd(o.Ffric, lF1 - lF2 + lH) + dotd(o.M1, lM1) + dotd(o.M2, lM2);
+  out[0] = make_double4(w.d[0], w.d[1], w.d[2], 0.0);
+  out[1] = make_double4(w.d[3], w.d[4], w.d[5], 0.0);
+  out[2] = make_double4(w.d[6], w.d[7], w.d[8], 0.0);
+  out[3] = make_double4(w.d[9], w.d[10], w.d[11], 0.0);
+  out[4] = make_double4(w.d[12], w.d[13], w.d[14], 0.0);
+  out[5] = make_double4(w.d[15], w.d[16], w.d[17], 0.0);
+  G.lH[k] = make_double4(w.d[18], w.d[19], w.d[20], 0.0);
+  G.gpar[2 * (size_t)k] += w.d[21];
+  G.gpar[2 * (size_t)k + 1] += w.d[22];
+}
+
+__device__ __forceinline__ void add4(double4& a, const double4& b) {
+  a.x += b.x;
+  a.y += b.y;
+  a.z += b.z;
+  a.w += b.w;
+}
+
+__global__ void k_adj_post(const AdjArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  if (!(A.pflags[i] & PF_ALIVE)) return;
+  double4 gx = make_double4(0.0, 0.0, 0.0, 0.0), gv = gx, gw = gx, gq = gx;
+  for (int d = 0; d < A.ndyn; ++d) {
+    const AdjDyn& G = A.dyn[d];
+    for (int e = G.adj_start[i]; e < G.adj_start[i + 1]; ++e) {
+      const int2 en = G.adj[e];
+      const int k = en.y & 0x7fffffff;
+      const int side = en.y < 0 ? 0 : 1;  // this particle is p1 or p2 of the pair
+      const double4* r = G.gpair + 6 * (size_t)k;
+      add4(gx, r[side]);
+      if (G.kind == 1) {
+        add4(gv, r[2 + side]);
+        add4(gw, r[4 + side]);
+      }
+    }
+  }
+  for (int d = 0; d < A.nbond; ++d) {
+    const AdjBond& B = A.bond[d];
+    for (int e = B.adj_start[i]; e < B.adj_start[i + 1]; ++e) {
+      const int2 en = B.adj[e];
+      const int k = en.y & 0x7fffffff;
+      const double4* r = B.gb + 4 * (size_t)k;
+      if (en.y < 0) {
+        add4(gx, r[0]);
+        add4(gq, r[1]);
+      } else {
+        add4(gx, r[2]);
+        add4(gq, r[3]);
+      }
+    }
+  }
+  double4 t = A.lx[i];
+  A.lx[i] = make_double4(t.x + gx.x, t.y + gx.y, t.z + gx.z, 0.0);
+  t = A.lv[i];
+  A.lv[i] = make_double4(t.x + gv.x, t.y + gv.y, t.z + gv.z, 0.0);
+  if (A.rot) {
+    t = A.lw[i];
+    A.lw[i] = make_double4(t.x + gw.x, t.y + gw.y, t.z + gw.z, 0.0);
+    t = A.lq[i];
+    A.lq[i] = make_double4(t.x + gq.x, t.y + gq.y, t.z + gq.z, t.w + gq.w);
+  }
+}
+
+// acc[c] += sum over rows r of data[r * cols + c], in a fixed order (one block).
+__global__ void k_reduce_cols(const double* data, int rows, int cols, double* acc) {
+  __shared__ double red[32];
+  for (int c = 0; c < cols; ++c) {
+    double s = 0.0;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) s += data[(size_t)r * cols + c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+      acc[c] += t;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_adjoint_step(const AdjArgs& A, cudaStream_t s) {
+  const int nb = (A.n + 255) / 256;
+  if (nb == 0) return;
+  k_adj_pre<<<nb, 256, 0, s>>>(A);
+  for (int d = 0; d < A.nbond; ++d)
+    if (A.bond[d].nb) k_adj_bond<<<(A.bond[d].nb + 127) / 128, 128, 0, s>>>(A, d);
+  for (int d = 0; d < A.ndyn; ++d)
+    if (A.dyn[d].m) k_adj_pair<<<(A.dyn[d].m + 127) / 128, 128, 0, s>>>(A, d);
+  if (A.nbond || A.ndyn) k_adj_post<<<nb, 256, 0, s>>>(A);
+}
+
+void launch_reduce_cols(const double* data, int rows, int cols, double* acc, cudaStream_t s) {
+  if (rows > 0) k_reduce_cols<<<1, 1024, 0, s>>>(data, rows, cols, acc);
+}
+
+}  // namespace dem

@@ -1,0 +1,65 @@
+// Arguments of the reverse step of the differentiable window (dem_adjoint.cu).
+#pragma once
+#include "dem_device.cuh"
+
+namespace dem {
+
+// One dynamic group (NRotElastic or RotFriction) in the reverse step.
+struct AdjDyn {
+  int kind;  // 0 elastic, 1 rot friction
+  double k, ks, mu_s, mu_d, dt;
+  int scaling, meanR;
+  int m;                              // pairs (frozen over the window)
+  const unsigned long long* keys;     // (p1 slot << 32) | p2 slot, p1 = lower id
+  const int* adj_start;               // per-particle adjacency over the pairs
+  const int2* adj;
+  const double4* hist_in;             // friction history read by this step (forward recompute)
+  double4* lH;                        // adjoint of the history: in after step t, out before it
+  double4* gpair;                     // [m][6]: d/dx1, d/dx2, d/dv1, d/dv2, d/dw1, d/dw2 of this step
+  double* gpar;                       // [m][2]: d/dk, d/dks accumulated over the window
+};
+
+// One RotBond group in the reverse step.
+struct AdjBond {
+  double kr, ks, kt, kb, mn, ms, mt, mb;
+  int scaling, meanR;
+  int nb;
+  const int2* ends;                   // (p1 slot, p2 slot)
+  const double4* D0;
+  const int* broken_step;
+  const int* adj_start;
+  const int2* adj;
+  double4* gb;                        // [nb][4]: d/dx1, d/dq1, d/dx2, d/dq2 of this step
+  double* gpar;                       // [nb][4]: d/dkr, d/dks, d/dkt, d/dkb accumulated
+};
+
+struct AdjArgs {
+  Grid g;
+  int n;
+  int rot;
+  double dt;
+  long long step;                     // timestep number of the step being reversed (1-based)
+  const unsigned* pflags;
+  ParticleBuf s0;                     // state before the step
+  ParticleBuf s1;                     // state after the step
+  const double4* f_int;               // force / moment sums before damping (forward recompute)
+  const double4* m_int;
+  const unsigned char* iters;         // damping iterations (lin, rot) per particle
+  int damp_lin, damp_rot, iter_lin, iter_rot;
+  double visc_lin, visc_rot, dt_lin, dt_rot;
+  int nwall;
+  const WallDev* walls;               // wall planes during the step
+  const double* gR;                   // [kMaxWalls][3]: dLoss / d(reaction of each wall group) at this step
+  double4 *lx, *lv, *lw, *lq;         // state adjoint: in lambda_{t+1}, out lambda_t
+  double4 *lF, *lM;                   // adjoint of the force / moment sums before damping
+  double* gvisc;                      // [n][2]: d/d(linear, rotational viscosity) accumulated
+  int ndyn;
+  AdjDyn dyn[kMaxDyn];
+  int nbond;
+  AdjBond bond[kMaxBond];
+};
+
+void launch_adjoint_step(const AdjArgs& A, cudaStream_t s);
+void launch_reduce_cols(const double* data, int rows, int cols, double* acc, cudaStream_t s);
+
+}  // namespace dem

@@ -137,6 +137,8 @@ struct StepArgs {
   unsigned char* damp_iters;
   double* wall_partial;     // [gridDim.x][kMaxWalls][3]
   double* wall_force;       // [kMaxWalls][3]: reaction of each wall group (adds into CWall::m_force)
+  double* wall_hist;        // differentiable window only: [step - wall_hist_t0 - 1][kMaxWalls][3] reactions
+  long long wall_hist_t0;
   unsigned* block_counter;  // last-block detection (wraps to 0 by itself)
   long long* step_counter;  // timesteps completed on the device
   int* ctrl;                // CTRL_* bits raised by this chunk of steps

@@ -8,6 +8,10 @@
 
 namespace dem {
 
+// keep the FP64 overloads visible beside the dual ones inside this namespace
+using ::acos;
+using ::sqrt;
+
 template <int N>
 struct Dual {
   double v;
@@ -68,7 +72,13 @@ __host__ __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, double s
 template <int N>
 __host__ __device__ __forceinline__ Dual<N> operator*(double s, const Dual<N>& a) { return a * s; }
 template <int N>
-__host__ __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, double s) { return a * (1.0 / s); }
+__host__ __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, double s) {
+  Dual<N> r;
+  r.v = a.v / s;  // the primal is the IEEE quotient of the FP64 law
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = a.d[k] / s;
+  return r;
+}
 template <int N>
 __host__ __device__ __forceinline__ Dual<N> operator/(double s, const Dual<N>& a) { return Dual<N>(s) / a; }
 template <int N>

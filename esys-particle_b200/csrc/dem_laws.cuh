@@ -14,18 +14,24 @@ using V = V3<double>;
 using Qd = Quat<double>;
 
 // CElasticInteraction ctor scaling (Model/ElasticInteraction.cpp:25-49).
-__device__ __forceinline__ double elastic_k(double k, int scaling, double r1, double r2) {
+template <class S>
+__device__ __forceinline__ S elastic_k_t(S k, int scaling, double r1, double r2) {
   double effR = 1.0, effA = 1.0, effL = 1.0;
   double r0 = r1 + r2;
   if (scaling) { effR = 0.5 * r0; effL = r0; effA = effR * effR; }
   return k * effA / effL;
 }
+__device__ __forceinline__ double elastic_k(double k, int scaling, double r1, double r2) {
+  return elastic_k_t<double>(k, scaling, r1, r2);
+}
 
 // CElasticInteraction::calcForces (Model/ElasticInteraction.cpp:54-71).
 // Returns true when touching; F is the force applied to p2 (p1 gets -F).
-__device__ __forceinline__ bool law_elastic(double k_eff, const V& x1, double r1, const V& x2, double r2, V& F) {
-  V D = x1 - x2;
-  double dist = dot(D, D);
+template <class S>
+__device__ __forceinline__ bool law_elastic_t(S k_eff, const V3<S>& x1, double r1, const V3<S>& x2, double r2,
+                                              V3<S>& F) {
+  V3<S> D = x1 - x2;
+  S dist = dot(D, D);
   double eq_dist = r1 + r2;
   if (dist < (eq_dist * eq_dist)) {
     dist = sqrt(dist);
@@ -34,10 +40,14 @@ __device__ __forceinline__ bool law_elastic(double k_eff, const V& x1, double r1
   }
   return false;
 }
+__device__ __forceinline__ bool law_elastic(double k_eff, const V& x1, double r1, const V& x2, double r2, V& F) {
+  return law_elastic_t<double>(k_eff, x1, r1, x2, r2, F);
+}
 
 // CRotFrictionInteraction ctor scaling (Model/RotFricInteraction.cpp:103-146).
-__device__ __forceinline__ void friction_k(double k, double ks, int scaling, int meanR, double r1, double r2,
-                                           double& k_eff, double& ks_eff) {
+template <class S>
+__device__ __forceinline__ void friction_k_t(S k, S ks, int scaling, int meanR, double r1, double r2, S& k_eff,
+                                             S& ks_eff) {
   double effR = 1.0, effL = 1.0, effA = 1.0;
   double r0 = r1 + r2;
   if (scaling) {
@@ -48,33 +58,42 @@ __device__ __forceinline__ void friction_k(double k, double ks, int scaling, int
   k_eff = k * effA / effL;
   ks_eff = ks * effA / effL;
 }
+__device__ __forceinline__ void friction_k(double k, double ks, int scaling, int meanR, double r1, double r2,
+                                           double& k_eff, double& ks_eff) {
+  friction_k_t<double>(k, ks, scaling, meanR, r1, r2, k_eff, ks_eff);
+}
 
-struct FricOut {
-  V fn;        // normal force applied to p2 (p1 gets -fn)
-  V Ffric;     // tangential force after the update (p1 gets +Ffric, p2 gets -Ffric)
-  V M1, M2;    // moments on p1, p2
+template <class S>
+struct FricOutT {
+  V3<S> fn;     // normal force applied to p2 (p1 gets -fn)
+  V3<S> Ffric;  // tangential force after the update (p1 gets +Ffric, p2 gets -Ffric)
+  V3<S> M1, M2; // moments on p1, p2
   bool touching, slipping;
 };
+using FricOut = FricOutT<double>;
 
 // CRotFrictionInteraction::calcSimpleForces (Model/RotFricInteraction.cpp:171-231).
-__device__ __forceinline__ void law_friction(double k_eff, double ks_eff, double mu_s, double mu_d, double dt,
-                                             const V& x1, double r1, const V& v1, const V& w1, const V& x2, double r2,
-                                             const V& v2, const V& w2, V Ffric, bool slipping, FricOut& o) {
+template <class S>
+__device__ __forceinline__ void law_friction_t(S k_eff, S ks_eff, double mu_s, double mu_d, double dt,
+                                               const V3<S>& x1, double r1, const V3<S>& v1, const V3<S>& w1,
+                                               const V3<S>& x2, double r2, const V3<S>& v2, const V3<S>& w2,
+                                               V3<S> Ffric, bool slipping, FricOutT<S>& o) {
+  using VS = V3<S>;
   double mu_current = slipping ? mu_d : mu_s;
-  const V D = x1 - x2;
-  double dist = dot(D, D);
+  const VS D = x1 - x2;
+  S dist = dot(D, D);
   const double eq_dist = r1 + r2;
   if (dist < (eq_dist * eq_dist)) {
     dist = sqrt(dist);
-    const V force = D * (k_eff * (dist - eq_dist) / dist);
-    const V pos = x2 + (r2 / eq_dist) * D;
-    const V vp1 = v1 + cross(w1, pos - x1);
-    const V vp2 = v2 + cross(w2, pos - x2);
-    V ds = (vp2 - vp1) * dt;
+    const VS force = D * (k_eff * (dist - eq_dist) / dist);
+    const VS pos = x2 + (r2 / eq_dist) * D;
+    const VS vp1 = v1 + cross(w1, pos - x1);
+    const VS vp2 = v2 + cross(w2, pos - x2);
+    VS ds = (vp2 - vp1) * dt;
     ds -= ((dot(ds, D)) / (norm2(D))) * D;
     Ffric += ks_eff * ds;
-    const double FfricNorm = norm(Ffric);
-    const double forceNorm = norm(force);
+    const S FfricNorm = norm(Ffric);
+    const S forceNorm = norm(force);
     if (FfricNorm > forceNorm * mu_current) {
       Ffric = Ffric * ((mu_d * forceNorm) / FfricNorm);
       o.slipping = true;
@@ -87,12 +106,17 @@ __device__ __forceinline__ void law_friction(double k_eff, double ks_eff, double
     o.Ffric = Ffric;
     o.touching = true;
   } else {
-    o.Ffric = mk(0.0, 0.0, 0.0);
-    o.fn = mk(0.0, 0.0, 0.0);
-    o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+    o.Ffric = mk(S(0.0), S(0.0), S(0.0));
+    o.fn = o.Ffric;
+    o.M1 = o.M2 = o.Ffric;
     o.slipping = false;
     o.touching = false;
   }
+}
+__device__ __forceinline__ void law_friction(double k_eff, double ks_eff, double mu_s, double mu_d, double dt,
+                                             const V& x1, double r1, const V& v1, const V& w1, const V& x2, double r2,
+                                             const V& v2, const V& w2, V Ffric, bool slipping, FricOut& o) {
+  law_friction_t<double>(k_eff, ks_eff, mu_s, mu_d, dt, x1, r1, v1, w1, x2, r2, v2, w2, Ffric, slipping, o);
 }
 
 // CRotFrictionInteraction::isPersistent (Model/RotFricInteraction.cpp:345-351).

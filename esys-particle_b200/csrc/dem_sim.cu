@@ -22,11 +22,16 @@
 
 #include "../../include/esys_dem.h"
 #include "dem_device.cuh"
+#include "dem_adjoint.h"
 #include "dem_kernels.h"
 
 namespace dem {
 
 struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+// An operation that the simulation's current state does not allow (DEM_ERR_STATE).
+struct StateError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
@@ -168,6 +173,7 @@ struct DemSim {
     cudaStreamSynchronize(s);
     for (auto& d : dyn) d.second.release();
     for (auto& b : bond) b.second.release();
+    win.release();
     void* ps[] = {P.buf[0].pr, P.buf[0].vm, P.buf[0].wi, P.buf[0].qq, P.buf[1].pr, P.buf[1].vm, P.buf[1].wi,
                   P.buf[1].qq, P.buf[0].vw, P.buf[1].vw, P.inv, P.oldpos, P.force, P.moment, P.force_eval,
                   P.moment_eval, P.sum_f, P.sum_m, P.pflags, P.flagged, P.id, P.tag, P.cell};
@@ -668,15 +674,21 @@ struct DemSim {
   }
 
   // CLatticeMaster::runOneStep x nsteps (LatticeMaster.cpp:2602-2740), without savers and runnables.
+  // The head of one runOneStep: the first step's forced search, checkNeighbors +
+  // searchNeighbors (LatticeMaster.cpp:1864-1908) and updateInteractions.
+  bool prepare() {
+    if (first) { search_neighbors(); first = false; }
+    if (pending_ctrl & CTRL_REBUILD) search_neighbors();
+    update_interactions((pending_ctrl & CTRL_BROKE) != 0);
+    if (pending_ctrl & CTRL_OVERFLOW) { err = "bond-break event log overflowed"; return false; }
+    pending_ctrl = 0;
+    return true;
+  }
+
   int step(int nsteps) {
     int done = 0;
     while (done < nsteps) {
-      if (first) { search_neighbors(); first = false; }
-      // checkNeighbors + searchNeighbors (LatticeMaster.cpp:1864-1908)
-      if (pending_ctrl & CTRL_REBUILD) search_neighbors();
-      update_interactions((pending_ctrl & CTRL_BROKE) != 0);
-      if (pending_ctrl & CTRL_OVERFLOW) { err = "bond-break event log overflowed"; return -2; }
-      pending_ctrl = 0;
+      if (!prepare()) return -2;
       // launch a chunk of force + integration steps
       const int k = std::min(chunk, nsteps - done);
       const int t_pp = pick_tpp();
@@ -722,6 +734,358 @@ struct DemSim {
     }
     return 0;
   }
+
+  // ---- differentiable loading window -------------------------------------
+  // Forward: T FP64 steps from the current state with the topology frozen
+  // (no neighbour rebuild and no bond break may fall inside the window),
+  // checkpoints of the particle state, friction histories and wall planes every
+  // K steps, and the reaction of every wall group after every step.
+  // Adjoint: the reverse pass over the stored window, segment by segment from
+  // the last, each segment's forward states recomputed from its checkpoint.
+  struct Window {
+    bool valid = false;
+    int T = 0, K = 0, nseg = 0, n = 0, ts = 0, cur0 = 0;
+    long long t0 = 0;
+    int m[kMaxDyn] = {0, 0};
+    DBuf<double4> ck, ck_hist[kMaxDyn], st, st_hist[kMaxDyn], st_f, st_m, lam, gb[kMaxBond], lH[kMaxDyn],
+        gpair[kMaxDyn];
+    DBuf<WallDev> ck_walls, st_walls, save_walls;
+    DBuf<unsigned char> st_it;
+    DBuf<double> R, gR, gvisc, gpar_b[kMaxBond], gpar_d[kMaxDyn], acc, save_wf;
+    DBuf<long long> ck_step;
+    void release() {
+      ck.release(); st.release(); st_f.release(); st_m.release(); lam.release();
+      for (int d = 0; d < kMaxDyn; ++d) {
+        ck_hist[d].release(); st_hist[d].release(); lH[d].release(); gpair[d].release(); gpar_d[d].release();
+      }
+      for (int b = 0; b < kMaxBond; ++b) { gb[b].release(); gpar_b[b].release(); }
+      ck_walls.release(); st_walls.release(); save_walls.release(); st_it.release();
+      R.release(); gR.release(); gvisc.release(); acc.release(); save_wf.release(); ck_step.release();
+      valid = false;
+    }
+  } win;
+
+  static ParticleBuf view4(double4* base, int n) { return ParticleBuf{base, base + n, base + 2 * (size_t)n, base + 3 * (size_t)n, nullptr}; }
+  void copy_state(const ParticleBuf& dst, const ParticleBuf& src) {
+    const size_t b = sizeof(double4) * (size_t)n;
+    DEM_CUDA(cudaMemcpyAsync(dst.pr, src.pr, b, cudaMemcpyDeviceToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(dst.vm, src.vm, b, cudaMemcpyDeviceToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(dst.wi, src.wi, b, cudaMemcpyDeviceToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(dst.qq, src.qq, b, cudaMemcpyDeviceToDevice, s));
+  }
+  std::vector<DynGroup*> dyn_list() { std::vector<DynGroup*> v; for (auto& d : dyn) v.push_back(&d.second); return v; }
+  std::vector<BondGroup*> bond_list() { std::vector<BondGroup*> v; for (auto& b : bond) v.push_back(&b.second); return v; }
+  int window_num_params() const { return 4 * (int)bond.size() + 2 * (int)dyn.size() + 2; }
+
+  void window_check_ctrl(int ctrl, bool last) {
+    if (ctrl & CTRL_BROKE) throw StateError("a bond broke inside the differentiable window (the bond state must stay frozen)");
+    if (ctrl & CTRL_OVERFLOW) throw StateError("bond-break event log overflowed inside the differentiable window");
+    if ((ctrl & CTRL_REBUILD) && !last)
+      throw StateError("a neighbour rebuild fell inside the differentiable window (shorten it or enlarge verletDist)");
+  }
+
+  int window_forward(int T, int K, double* R_host) {
+    if (T < 1 || K < 1) throw std::invalid_argument("window length and checkpoint interval must be >= 1");
+    if (fp32) throw std::invalid_argument("the differentiable window runs the FP64 form (set precision 64)");
+    if (iter_lin > 255 || iter_rot > 255) throw std::invalid_argument("window damping needs maxIterations <= 255");
+    win.valid = false;
+    if (!prepare()) return DEM_ERR_OVERFLOW;
+    const int nd = (int)dyn.size();
+    auto dl = dyn_list();
+    win.T = T; win.K = std::min(K, T); win.nseg = (T + win.K - 1) / win.K; win.n = n; win.t0 = t;
+    win.ts = timestamp; win.cur0 = cur;
+    win.ck.reserve((size_t)win.nseg * 4 * std::max(n, 1));
+    win.ck_walls.reserve((size_t)win.nseg * kMaxWalls);
+    win.R.reserve((size_t)T * kMaxWalls * 3);
+    for (int d = 0; d < nd; ++d) {
+      win.m[d] = dl[d]->m;
+      if (dl[d]->kind == 1) win.ck_hist[d].reserve((size_t)win.nseg * std::max(win.m[d], 1));
+    }
+    DEM_CUDA(cudaMemsetAsync(win.R.p, 0, sizeof(double) * T * kMaxWalls * 3, s));
+    const int t_pp = pick_tpp();
+    d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
+    const bool two = split == 1;
+    const long long cps = contacts_per_step();
+    for (int c = 0; c < win.nseg; ++c) {
+      const int len = std::min(win.K, T - c * win.K);
+      copy_state(view4(win.ck.p + (size_t)c * 4 * n, n), P.buf[cur]);
+      for (int d = 0; d < nd; ++d)
+        if (dl[d]->kind == 1 && win.m[d])
+          DEM_CUDA(cudaMemcpyAsync(win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist[cur].p,
+                                   sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+      if (!wig.empty())
+        DEM_CUDA(cudaMemcpyAsync(win.ck_walls.p + (size_t)c * kMaxWalls, d_walls.p, sizeof(WallDev) * wig.size(),
+                                 cudaMemcpyDeviceToDevice, s));
+      DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+      DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
+      for (int j = 0; j < len; ++j) {
+        StepArgs a = make_args((cur + j) & 1);
+        a.wall_hist = win.R.p;
+        a.wall_hist_t0 = win.t0;
+        launch_step(a, rot != 0, t_pp, two, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+      c_launches += two ? 2LL * len : len;
+      DEM_CUDA(cudaMemcpyAsync(h_ctrl, d_step.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(h_ctrl + 2, d_ctrl.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      sync();
+      long long dev_t;
+      std::memcpy(&dev_t, h_ctrl, sizeof(long long));
+      const int ran = (int)(dev_t - t);
+      if (ran < 0 || ran > len) throw StateError("device step counter out of sequence in the window");
+      // the steps that ran are real steps of the simulation, whether the window stands or not
+      t = dev_t;
+      cur = (cur + ran) & 1;
+      c_steps += ran;
+      c_contacts += (long long)ran * cps;
+      pending_ctrl = h_ctrl[2];
+      window_check_ctrl(h_ctrl[2], c == win.nseg - 1 && ran == len);
+      if (ran != len) throw StateError("device step counter out of sequence in the window");
+    }
+    if (R_host) {
+      std::vector<double> r((size_t)T * kMaxWalls * 3);
+      DEM_CUDA(cudaMemcpyAsync(r.data(), win.R.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, s));
+      sync();
+      const int nw = (int)wig.size();
+      for (int k = 0; k < T; ++k)
+        for (int w = 0; w < nw; ++w)
+          for (int c = 0; c < 3; ++c) R_host[((size_t)k * nw + w) * 3 + c] = r[((size_t)k * kMaxWalls + w) * 3 + c];
+    }
+    win.valid = true;
+    return 0;
+  }
+
+  void window_require() {
+    if (!win.valid) throw StateError("no differentiable window has been run");
+    if (t != win.t0 + win.T || timestamp != win.ts || n != win.n)
+      throw StateError("the simulation moved on since the window was run");
+  }
+
+  // Reverse pass.  gR_host: [T][nwall][3] dLoss/dReaction; grad_params: window_num_params()
+  // values (bond groups x (kr, ks, kt, kb), dynamic groups x (k, ks), linear and rotational
+  // viscosity); per-particle outputs in dem_get_particles order (any may be null).
+  void window_adjoint(const double* gR_host, double* grad_params, double* gvel, double* gang, double* gpos,
+                      double* gquat) {
+    window_require();
+    if (!gR_host) throw std::invalid_argument("null reaction gradient");
+    const int T = win.T, K = win.K, nw = (int)wig.size();
+    auto dl = dyn_list();
+    auto bl = bond_list();
+    const int nd = (int)dl.size(), nbg = (int)bl.size();
+    const int nn = std::max(n, 1);
+    // device buffers
+    win.st.reserve((size_t)(K + 1) * 4 * nn);
+    win.st_f.reserve((size_t)K * nn);
+    win.st_m.reserve((size_t)K * nn);
+    win.st_it.reserve((size_t)K * 2 * nn);
+    win.st_walls.reserve((size_t)K * kMaxWalls);
+    win.lam.reserve((size_t)6 * nn);
+    win.gvisc.reserve((size_t)2 * nn);
+    win.gR.reserve((size_t)T * kMaxWalls * 3);
+    win.acc.reserve(64);
+    win.save_walls.reserve(kMaxWalls);
+    win.save_wf.reserve(kMaxWalls * 3);
+    for (int d = 0; d < nd; ++d) {
+      const int m = std::max(win.m[d], 1);
+      if (dl[d]->kind == 1) win.st_hist[d].reserve((size_t)(K + 1) * m);
+      win.lH[d].reserve(m);
+      win.gpair[d].reserve((size_t)6 * m);
+      win.gpar_d[d].reserve((size_t)2 * m);
+      DEM_CUDA(cudaMemsetAsync(win.lH[d].p, 0, sizeof(double4) * m, s));
+      DEM_CUDA(cudaMemsetAsync(win.gpar_d[d].p, 0, sizeof(double) * 2 * m, s));
+    }
+    for (int b = 0; b < nbg; ++b) {
+      const int m = std::max(bl[b]->nb, 1);
+      win.gb[b].reserve((size_t)4 * m);
+      win.gpar_b[b].reserve((size_t)4 * m);
+      DEM_CUDA(cudaMemsetAsync(win.gpar_b[b].p, 0, sizeof(double) * 4 * m, s));
+    }
+    DEM_CUDA(cudaMemsetAsync(win.lam.p, 0, sizeof(double4) * 6 * nn, s));
+    DEM_CUDA(cudaMemsetAsync(win.gvisc.p, 0, sizeof(double) * 2 * nn, s));
+    DEM_CUDA(cudaMemsetAsync(win.acc.p, 0, sizeof(double) * 64, s));
+    {
+      std::vector<double> g((size_t)T * kMaxWalls * 3, 0.0);
+      for (int k = 0; k < T; ++k)
+        for (int w = 0; w < nw; ++w)
+          for (int c = 0; c < 3; ++c) g[((size_t)k * kMaxWalls + w) * 3 + c] = gR_host[((size_t)k * nw + w) * 3 + c];
+      DEM_CUDA(cudaMemcpyAsync(win.gR.p, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice, s));
+      sync();
+    }
+    // the live device state the recompute touches: wall planes, reactions, step counter
+    if (nw) DEM_CUDA(cudaMemcpyAsync(win.save_walls.p, d_walls.p, sizeof(WallDev) * nw, cudaMemcpyDeviceToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(win.save_wf.p, d_wall_force.p, sizeof(double) * kMaxWalls * 3, cudaMemcpyDeviceToDevice, s));
+    const int t_pp = pick_tpp();
+    d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
+    const bool two = split == 1;
+    double4* lam = win.lam.p;
+    AdjArgs A{};
+    A.g = g; A.n = n; A.rot = rot; A.dt = dt; A.pflags = P.pflags;
+    A.damp_lin = damp_lin; A.damp_rot = damp_rot; A.iter_lin = iter_lin; A.iter_rot = iter_rot;
+    A.visc_lin = visc_lin; A.visc_rot = visc_rot; A.dt_lin = dt; A.dt_rot = dt;
+    A.nwall = nw;
+    A.lx = lam; A.lv = lam + nn; A.lw = lam + 2 * (size_t)nn; A.lq = lam + 3 * (size_t)nn;
+    A.lF = lam + 4 * (size_t)nn; A.lM = lam + 5 * (size_t)nn;
+    A.gvisc = win.gvisc.p;
+    A.ndyn = nd;
+    for (int d = 0; d < nd; ++d) {
+      DynGroup& G = *dl[d];
+      AdjDyn& D = A.dyn[d];
+      D.kind = G.kind; D.k = G.k; D.ks = G.ks; D.mu_s = G.mu_s; D.mu_d = G.mu_d; D.dt = G.dt;
+      D.scaling = G.scaling; D.meanR = G.meanR; D.m = win.m[d];
+      D.keys = G.keys.p; D.adj_start = G.adj_start.p; D.adj = G.adj.p;
+      D.lH = win.lH[d].p; D.gpair = win.gpair[d].p; D.gpar = win.gpar_d[d].p;
+    }
+    A.nbond = nbg;
+    for (int b = 0; b < nbg; ++b) {
+      BondGroup& B = *bl[b];
+      AdjBond& D = A.bond[b];
+      D.kr = B.kr; D.ks = B.ks; D.kt = B.kt; D.kb = B.kb; D.mn = B.mn; D.ms = B.ms; D.mt = B.mt; D.mb = B.mb;
+      D.scaling = B.scaling; D.meanR = B.meanR; D.nb = B.nb;
+      D.ends = B.ends.p; D.D0 = B.D0.p; D.broken_step = B.broken_step.p;
+      D.adj_start = B.adj_start.p; D.adj = B.adj.p;
+      D.gb = win.gb[b].p; D.gpar = win.gpar_b[b].p;
+    }
+    for (int c = win.nseg - 1; c >= 0; --c) {
+      const int len = std::min(K, T - c * K);
+      const long long tc = win.t0 + (long long)c * K;
+      // recompute the segment's forward states from its checkpoint
+      copy_state(view4(win.st.p, n), view4(win.ck.p + (size_t)c * 4 * n, n));
+      for (int d = 0; d < nd; ++d)
+        if (dl[d]->kind == 1 && win.m[d])
+          DEM_CUDA(cudaMemcpyAsync(win.st_hist[d].p, win.ck_hist[d].p + (size_t)c * win.m[d],
+                                   sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+      if (nw)
+        DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p + (size_t)c * kMaxWalls, sizeof(WallDev) * nw,
+                                 cudaMemcpyDeviceToDevice, s));
+      long long tcv = tc;
+      DEM_CUDA(cudaMemcpyAsync(d_step.p, &tcv, sizeof(long long), cudaMemcpyHostToDevice, s));
+      DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+      DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
+      for (int j = 0; j < len; ++j) {
+        if (nw)
+          DEM_CUDA(cudaMemcpyAsync(win.st_walls.p + (size_t)j * kMaxWalls, d_walls.p, sizeof(WallDev) * nw,
+                                   cudaMemcpyDeviceToDevice, s));
+        StepArgs a = make_args(0);
+        a.P.buf[0] = view4(win.st.p + (size_t)j * 4 * n, n);
+        a.P.buf[1] = view4(win.st.p + (size_t)(j + 1) * 4 * n, n);
+        a.cur = 0;
+        for (int d = 0; d < nd; ++d)
+          if (dl[d]->kind == 1) {
+            a.dyn[d].hist_in = win.st_hist[d].p + (size_t)j * std::max(win.m[d], 1);
+            a.dyn[d].hist_out = win.st_hist[d].p + (size_t)(j + 1) * std::max(win.m[d], 1);
+          }
+        a.f_int = win.st_f.p + (size_t)j * n;
+        a.m_int = win.st_m.p + (size_t)j * n;
+        a.damp_iters = win.st_it.p + (size_t)j * 2 * n;
+        a.store_forces = 0;
+        launch_step(a, rot != 0, t_pp, two, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+      c_launches += two ? 2LL * len : len;
+      // reverse the segment
+      for (int j = len - 1; j >= 0; --j) {
+        A.step = tc + j + 1;
+        A.s0 = view4(win.st.p + (size_t)j * 4 * n, n);
+        A.s1 = view4(win.st.p + (size_t)(j + 1) * 4 * n, n);
+        A.f_int = win.st_f.p + (size_t)j * n;
+        A.m_int = win.st_m.p + (size_t)j * n;
+        A.iters = win.st_it.p + (size_t)j * 2 * n;
+        A.walls = win.st_walls.p + (size_t)j * kMaxWalls;
+        A.gR = win.gR.p + (size_t)(c * K + j) * kMaxWalls * 3;
+        for (int d = 0; d < nd; ++d)
+          A.dyn[d].hist_in = dl[d]->kind == 1 ? win.st_hist[d].p + (size_t)j * std::max(win.m[d], 1) : nullptr;
+        launch_adjoint_step(A, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+    }
+    // parameter gradients: one fixed-order reduction each
+    int off = 0;
+    for (int b = 0; b < nbg; ++b, off += 4) launch_reduce_cols(win.gpar_b[b].p, bl[b]->nb, 4, win.acc.p + off, s);
+    for (int d = 0; d < nd; ++d, off += 2) launch_reduce_cols(win.gpar_d[d].p, win.m[d], 2, win.acc.p + off, s);
+    launch_reduce_cols(win.gvisc.p, n, 2, win.acc.p + off, s);
+    off += 2;
+    DEM_CUDA(cudaGetLastError());
+    // restore the live device state
+    if (nw) DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.save_walls.p, sizeof(WallDev) * nw, cudaMemcpyDeviceToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_wall_force.p, win.save_wf.p, sizeof(double) * kMaxWalls * 3, cudaMemcpyDeviceToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_step.p, &t, sizeof(long long), cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+    DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
+    std::vector<double> acc(off);
+    std::vector<double4> lh((size_t)4 * n);
+    std::vector<unsigned> pf(n);
+    DEM_CUDA(cudaMemcpyAsync(acc.data(), win.acc.p, sizeof(double) * off, cudaMemcpyDeviceToHost, s));
+    if (n) {
+      DEM_CUDA(cudaMemcpyAsync(lh.data(), lam, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(lh.data() + n, lam + nn, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(lh.data() + 2 * (size_t)n, lam + 2 * (size_t)nn, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(lh.data() + 3 * (size_t)n, lam + 3 * (size_t)nn, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s));
+    }
+    sync();
+    if (grad_params) for (int k = 0; k < off; ++k) grad_params[k] = acc[k];
+    int k = 0;
+    for (int i = 0; i < n; ++i) {
+      if (!(pf[i] & PF_ALIVE)) continue;
+      const double4 x = lh[i], v = lh[n + i], w = lh[2 * (size_t)n + i], q = lh[3 * (size_t)n + i];
+      if (gpos) { gpos[3 * k] = x.x; gpos[3 * k + 1] = x.y; gpos[3 * k + 2] = x.z; }
+      if (gvel) { gvel[3 * k] = v.x; gvel[3 * k + 1] = v.y; gvel[3 * k + 2] = v.z; }
+      if (gang) {
+        gang[3 * k] = rot ? w.x : 0.0; gang[3 * k + 1] = rot ? w.y : 0.0; gang[3 * k + 2] = rot ? w.z : 0.0;
+      }
+      if (gquat) {
+        gquat[4 * k] = rot ? q.x : 0.0; gquat[4 * k + 1] = rot ? q.y : 0.0;
+        gquat[4 * k + 2] = rot ? q.z : 0.0; gquat[4 * k + 3] = rot ? q.w : 0.0;
+      }
+      ++k;
+    }
+  }
+
+  void set_group_param(const std::string& group, const std::string& key, double v) {
+    auto b = bond.find(group);
+    if (b != bond.end()) {
+      BondGroup& B = b->second;
+      if (key == "normalK") B.kr = v;
+      else if (key == "shearK") B.ks = v;
+      else if (key == "torsionK") B.kt = v;
+      else if (key == "bendingK") B.kb = v;
+      else throw std::invalid_argument("unknown RotBond parameter " + key);
+      return;
+    }
+    auto d = dyn.find(group);
+    if (d != dyn.end()) {
+      DynGroup& G = d->second;
+      if (key == "normalK") G.k = v;
+      else if (key == "shearK" && G.kind == 1) G.ks = v;
+      else if (key == "dynamicMu" && G.kind == 1) G.mu_d = v;
+      else if (key == "staticMu" && G.kind == 1) G.mu_s = v;
+      else throw std::invalid_argument("unknown parameter " + key + " of group " + group);
+      return;
+    }
+    if (group == "Damping" && damp_lin && key == "viscosity") { visc_lin = v; return; }
+    if (group == "RotDamping" && damp_rot && key == "viscosity") { visc_rot = v; return; }
+    throw std::invalid_argument("unknown group " + group);
+  }
+
+  // Put the simulation back to the state at the start of the window.
+  void window_rewind() {
+    if (!win.valid) throw StateError("no differentiable window has been run");
+    if (timestamp != win.ts || n != win.n) throw StateError("the topology changed since the window was run");
+    auto dl = dyn_list();
+    cur = win.cur0;
+    copy_state(P.buf[cur], view4(win.ck.p, n));
+    for (int d = 0; d < (int)dl.size(); ++d)
+      if (dl[d]->kind == 1 && win.m[d])
+        DEM_CUDA(cudaMemcpyAsync(dl[d]->hist[cur].p, win.ck_hist[d].p, sizeof(double4) * win.m[d],
+                                 cudaMemcpyDeviceToDevice, s));
+    if (!wig.empty())
+      DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p, sizeof(WallDev) * wig.size(), cudaMemcpyDeviceToDevice, s));
+    t = win.t0;
+    DEM_CUDA(cudaMemcpyAsync(d_step.p, &t, sizeof(long long), cudaMemcpyHostToDevice, s));
+    pending_ctrl = 0;
+    sync();
+    download_walls();
+  }
 };
 
 }  // namespace dem
@@ -742,6 +1106,9 @@ int guard(dem_sim* h, F&& f) {
   } catch (const std::invalid_argument& e) {
     s->err = e.what();
     return DEM_ERR_ARG;
+  } catch (const dem::StateError& e) {
+    s->err = e.what();
+    return DEM_ERR_STATE;
   } catch (const std::exception& e) {
     s->err = e.what();
     return DEM_ERR_INTERNAL;
@@ -1232,6 +1599,37 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
     } else {
       throw std::invalid_argument("unknown option " + k);
     }
+    return DEM_OK;
+  });
+}
+
+int dem_set_group_param(dem_sim* h, const char* group, const char* key, double value) {
+  return guard(h, [&](DemSim& s) {
+    if (!group || !key) throw std::invalid_argument("null group or key");
+    s.set_group_param(group, key, value);
+    return DEM_OK;
+  });
+}
+
+int dem_window_num_params(dem_sim* h) {
+  return guard(h, [&](DemSim& s) { return s.window_num_params(); });
+}
+
+int dem_window_forward(dem_sim* h, int nsteps, int checkpoint_every, double* reactions) {
+  return guard(h, [&](DemSim& s) { return s.window_forward(nsteps, checkpoint_every, reactions); });
+}
+
+int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_params, double* grad_vel,
+                       double* grad_angvel, double* grad_pos, double* grad_quat) {
+  return guard(h, [&](DemSim& s) {
+    s.window_adjoint(grad_reactions, grad_params, grad_vel, grad_angvel, grad_pos, grad_quat);
+    return DEM_OK;
+  });
+}
+
+int dem_window_rewind(dem_sim* h) {
+  return guard(h, [&](DemSim& s) {
+    s.window_rewind();
     return DEM_OK;
   });
 }

@@ -409,6 +409,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a, int wlane, int 
       double t = 0.0;
       for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
       a.wall_force[3 * w + c] = t;
+      if (a.wall_hist) a.wall_hist[(size_t)(step - a.wall_hist_t0 - 1) * (kMaxWalls * 3) + 3 * w + c] = t;
     }
     __syncthreads();
   }

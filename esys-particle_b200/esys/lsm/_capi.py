@@ -55,6 +55,11 @@ SIGNATURES = {
     "dem_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "dem_precision_check": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "dem_wall_reactions_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dem_set_group_param": (C.c_int, [_P, _S, _S, C.c_double]),
+    "dem_window_num_params": (C.c_int, [_P]),
+    "dem_window_forward": (C.c_int, [_P, C.c_int, C.c_int, _D]),
+    "dem_window_adjoint": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
+    "dem_window_rewind": (C.c_int, [_P]),
 }
 
 _lib = None
@@ -106,6 +111,10 @@ class DemSim:
         if rc != 0:
             raise DemError(f"dem_create failed ({rc}): no usable GPU or invalid domain")
         self.rot = pt == 1
+        self.wall_groups = []  # wall interaction groups, in the library's (name) order
+        self._bond_prm = {}    # RotBond group -> [normalK, shearK, torsionK, bendingK]
+        self._dyn_prm = {}     # dynamic group -> (kind, [normalK, shearK])
+        self._damp_prm = {}    # "Damping" / "RotDamping" -> viscosity
 
     def _chk(self, rc):
         if rc < 0:
@@ -142,25 +151,30 @@ class DemSim:
 
     def add_elastic_group(self, name, k, scaling=True):
         self._chk(self.lib.dem_add_elastic_group(self.h, name.encode(), float(k), int(scaling)))
+        self._dyn_prm[name] = (0, [float(k), 0.0])
 
     def add_rot_friction_group(self, name, k, mu_s, mu_d, k_s, dt, scaling=True, meanR_scaling=True):
         self._chk(self.lib.dem_add_rot_friction_group(self.h, name.encode(), float(k), float(mu_s), float(mu_d),
                                                       float(k_s), float(dt), int(scaling), int(meanR_scaling)))
+        self._dyn_prm[name] = (1, [float(k), float(k_s)])
 
     def add_rot_bond_group(self, name, tag, kr, ks, kt, kb, max_n, max_s, max_t, max_b, scaling=True,
                            meanR_scaling=True, truncated=1.0):
         self._chk(self.lib.dem_add_rot_bond_group(self.h, name.encode(), int(tag), float(kr), float(ks), float(kt),
                                                   float(kb), float(max_n), float(max_s), float(max_t), float(max_b),
                                                   int(scaling), int(meanR_scaling), float(truncated)))
+        self._bond_prm[name] = [float(kr), float(ks), float(kt), float(kb)]
 
     def add_wall_group(self, name, wall, k):
         self._chk(self.lib.dem_add_wall_group(self.h, name.encode(), wall.encode(), float(k)))
+        self.wall_groups = sorted(set(self.wall_groups) | {name})
 
     def add_gravity(self, name, g):
         self._chk(self.lib.dem_add_gravity(self.h, name.encode(), _dp(_v3(g))))
 
     def add_damping(self, rot, visc, max_iter=100):
         self._chk(self.lib.dem_add_damping(self.h, int(rot), float(visc), int(max_iter)))
+        self._damp_prm["RotDamping" if rot else "Damping"] = float(visc)
 
     def add_exclusion(self, bonded, dynamic):
         self._chk(self.lib.dem_add_exclusion(self.h, bonded.encode(), dynamic.encode()))
@@ -259,3 +273,78 @@ class DemSim:
     @property
     def timestep(self):
         return int(self.lib.dem_timestep(self.h))
+
+    # ---- parameters and the differentiable loading window ----
+    def set_group_param(self, group, key, value):
+        """dem_set_group_param: one unscaled parameter of an existing group."""
+        self._chk(self.lib.dem_set_group_param(self.h, group.encode(), key.encode(), float(value)))
+        for slot, (g, k) in enumerate(self.param_layout()):
+            if g == group and k == key:
+                self._set_param_value(slot, float(value))
+
+    _BOND_KEYS = ("normalK", "shearK", "torsionK", "bendingK")
+
+    def param_layout(self):
+        """(group, key) of each dem_window_adjoint parameter gradient, in the library's
+        order; key None marks a slot without a parameter (the elastic law has no shearK,
+        and an absent damping group has no viscosity)."""
+        out = [(g, k) for g in sorted(self._bond_prm) for k in self._BOND_KEYS]
+        for g in sorted(self._dyn_prm):
+            out += [(g, "normalK"), (g, "shearK" if self._dyn_prm[g][0] == 1 else None)]
+        out += [("Damping", "viscosity" if "Damping" in self._damp_prm else None),
+                ("RotDamping", "viscosity" if "RotDamping" in self._damp_prm else None)]
+        return out
+
+    def param_values(self):
+        vals = [v for g in sorted(self._bond_prm) for v in self._bond_prm[g]]
+        for g in sorted(self._dyn_prm):
+            vals += list(self._dyn_prm[g][1])
+        vals += [self._damp_prm.get("Damping", 0.0), self._damp_prm.get("RotDamping", 0.0)]
+        return np.array(vals, dtype=np.float64)
+
+    def _set_param_value(self, slot, value):
+        nb = 4 * len(self._bond_prm)
+        if slot < nb:
+            self._bond_prm[sorted(self._bond_prm)[slot // 4]][slot % 4] = value
+            return
+        slot -= nb
+        nd = 2 * len(self._dyn_prm)
+        if slot < nd:
+            self._dyn_prm[sorted(self._dyn_prm)[slot // 2]][1][slot % 2] = value
+            return
+        self._damp_prm[("Damping", "RotDamping")[slot - nd]] = value
+
+    def set_params(self, values):
+        """Apply a full parameter vector in param_layout() order."""
+        for (g, k), v in zip(self.param_layout(), np.asarray(values, dtype=np.float64)):
+            if k is not None:
+                self.set_group_param(g, k, v)
+
+    def window_num_params(self):
+        return self._chk(self.lib.dem_window_num_params(self.h))
+
+    def window_forward(self, nsteps, checkpoint_every=100):
+        """Run a differentiable window; returns the wall-group reactions [nsteps, groups, 3]."""
+        r = np.zeros((int(nsteps), len(self.wall_groups), 3))
+        self._chk(self.lib.dem_window_forward(self.h, int(nsteps), int(checkpoint_every), _dp(r)))
+        return r
+
+    def window_adjoint(self, grad_reactions):
+        """Reverse pass of the last window.  Returns the parameter gradients
+        (dem_window_num_params values) and dLoss/d(initial pos, vel, angvel, quat) rows
+        sorted by particle id, with the ids."""
+        g = np.ascontiguousarray(grad_reactions, dtype=np.float64)
+        n = self.num_particles()
+        out = {"params": np.zeros(self.window_num_params()), "id": np.zeros(n, np.int32)}
+        for k, w in (("pos", 3), ("vel", 3), ("angvel", 3), ("quat", 4)):
+            out[k] = np.zeros((n, w))
+        self._chk(self.lib.dem_window_adjoint(self.h, _dp(g), _dp(out["params"]), _dp(out["vel"]),
+                                              _dp(out["angvel"]), _dp(out["pos"]), _dp(out["quat"])))
+        self._chk(self.lib.dem_get_particles(self.h, _ip(out["id"]), None, None, None, None, None, None))
+        order = np.argsort(out["id"], kind="stable")
+        for k in ("id", "pos", "vel", "angvel", "quat"):
+            out[k] = out[k][order]
+        return out
+
+    def window_rewind(self):
+        self._chk(self.lib.dem_window_rewind(self.h))

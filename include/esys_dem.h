@@ -29,7 +29,8 @@ enum {
   DEM_ERR_ARG = -1,      /* invalid argument (unknown group or wall, bad sizes, wrong particle type) */
   DEM_ERR_OVERFLOW = -2, /* a device-side log ran out of room */
   DEM_ERR_CUDA = -3,     /* CUDA error or no GPU */
-  DEM_ERR_INTERNAL = -4
+  DEM_ERR_INTERNAL = -4,
+  DEM_ERR_STATE = -5     /* not allowed in the current state (e.g. a bond broke inside a differentiable window) */
 };
 
 /* Particle types: 0 = "NRotSphere" (CParticle), 1 = "RotSphere" (CRotParticle). */
@@ -184,6 +185,41 @@ int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const 
  * 32 = FP32 pair forces with Kahan-compensated accumulation, FP64 positions / contact detection /
  * integration). */
 int dem_set_option(dem_sim* h, const char* key, double value);
+
+/* ---- Parameters and the differentiable loading window -------------------------------- */
+
+/* Sets one parameter of an existing group for every interaction in it, like
+ * LsmMpi.setInteractionParameter -> TParallelInteractionStorage::forAllInteractionsSet
+ * (Parallel/LatticeMaster.cpp:4290-4301, pis/pi_storage.hpp:277-292).  The reference only
+ * binds "k" of CElasticInteraction (Model/ElasticInteraction.cpp:169-180); here the keys are
+ * the *Prms attribute names: RotBond "normalK", "shearK", "torsionK", "bendingK"; RotFriction
+ * "normalK", "shearK", "staticMu", "dynamicMu"; NRotElastic "normalK"; the damping groups
+ * "Damping" / "RotDamping" take "viscosity".  Values are unscaled group parameters: the
+ * per-interaction scaling of each law's constructor is applied to them at every step. */
+int dem_set_group_param(dem_sim* h, const char* group, const char* key, double value);
+
+/* Number of parameter gradients dem_window_adjoint writes: 4 per RotBond group (normalK,
+ * shearK, torsionK, bendingK), 2 per dynamic group (normalK, shearK; elastic: normalK, 0) in
+ * group-name order, then the linear and rotational damping viscosities. */
+int dem_window_num_params(dem_sim* h);
+
+/* Runs nsteps FP64 steps (the dem_step sequence) as a differentiable window: the neighbour
+ * lists, wall candidates and bond set are frozen (DEM_ERR_STATE if a rebuild or a bond break
+ * falls inside the window), the state is checkpointed every checkpoint_every steps, and the
+ * reaction of every wall group after every step (CWall::m_force, EWallInteractionGroup.hpp:
+ * 47-53) is written to reactions[nsteps][wall groups in name order][3] (may be null). */
+int dem_window_forward(dem_sim* h, int nsteps, int checkpoint_every, double* reactions);
+
+/* Reverse pass of the last window: grad_reactions[nsteps][wall groups][3] is dLoss/dReaction;
+ * grad_params receives dem_window_num_params values; grad_vel / grad_angvel / grad_pos (n x 3)
+ * and grad_quat (n x 4) receive dLoss/d(initial state) in dem_get_particles order.  Any output
+ * may be null.  The simulation must not have stepped since dem_window_forward. */
+int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_params, double* grad_vel,
+                       double* grad_angvel, double* grad_pos, double* grad_quat);
+
+/* Restores the state at the start of the last window (particles, friction histories, wall
+ * planes, timestep), so that the window can be run again with other parameters. */
+int dem_window_rewind(dem_sim* h);
 
 #ifdef __cplusplus
 }

@@ -109,7 +109,7 @@ struct PairGroup {            /* one dynamic (NE or ED) or bonded (EB) interacti
   std::vector<PairGroup*> exig;                                 /* excluding groups */
   int update_ts = 0;
 };
-struct Wall { V3 o, n, F; };
+struct Wall { V3 o, n, F; V3 vel; bool loader = false; };
 struct WallGroup { std::string wall; double k; std::vector<WallI> its; };
 struct Damp { double visc; int maxiter; double dt; };
 
@@ -681,6 +681,15 @@ static void one_step(Sim& s) {
   for (int i = 0; i < s.P.n(); ++i) if (s.P.alive[i]) rescale(s, i);
 }
 
+static void move_loaded_walls(Sim& s) {
+  for (auto& w : s.walls)
+    if (w.second.loader) {
+      w.second.o.x += w.second.vel.x * s.dt;
+      w.second.o.y += w.second.vel.y * s.dt;
+      w.second.o.z += w.second.vel.z * s.dt;
+    }
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -849,7 +858,64 @@ int orc_step(void* h, int n) {
     if (check_neighbors(s)) search_neighbors(s);
     update_interactions(s);
     one_step(s);
+    move_loaded_walls(s);
   }
+  return 0;
+}
+/* LsmMpi.setInteractionParameter -> forAllInteractionsSet (LatticeMaster.cpp:4290-4301,
+ * pi_storage.hpp:277-292), widened to the parameters the differentiable window uses: a group's
+ * unscaled parameter is replaced and every existing interaction's scaled constant is recomputed
+ * with its constructor's formula (new interactions pick the new value up by themselves). */
+int orc_set_group_param(void* h, const char* group, const char* key, double v) {
+  Sim& s = *(Sim*)h;
+  const std::string g = group, k = key;
+  if ((g == "Damping" || g == "RotDamping") && k == "viscosity" && s.damping.count(g)) { s.damping[g].visc = v; return 0; }
+  auto b = s.bpis.find(g);
+  if (b != s.bpis.end()) {
+    PairGroup& G = *b->second;
+    if (k == "normalK") G.kr = v; else if (k == "shearK") G.ks = v;
+    else if (k == "torsionK") G.kt = v; else if (k == "bendingK") G.kb = v;
+    else { s.err = "unknown RotBond parameter " + k; return -1; }
+    for (auto& bd : G.bd) {
+      const double dist = std::sqrt(dot(bd.D, bd.D));
+      double effR = 1.0, effL = 1.0, effA = 1.0, J = 1.0, I = 1.0;
+      if (G.scaling) {
+        if (G.meanR) effR = 0.5 * dist; else effR = std::fmin(s.P.rad[bd.p1], s.P.rad[bd.p2]);
+        effL = dist; effA = effR * effR;
+        J = 0.5 * effR * effR * effR * effR; I = 0.5 * J;
+      }
+      bd.kr = G.kr * effA / effL; bd.ks = G.ks * effA / effL; bd.kb = G.kb * I / effL; bd.kt = G.kt * J / effL;
+    }
+    return 0;
+  }
+  auto d = s.dpis.find(g);
+  if (d != s.dpis.end()) {
+    PairGroup& G = *d->second;
+    if (G.kind == 0 && k == "normalK") {
+      G.k = v;
+      for (auto& e : G.el) e = [&] { Elastic n = make_elastic(s, G, e.p1, e.p2); n.force = e.force; n.touching = e.touching; return n; }();
+      return 0;
+    }
+    if (G.kind == 1 && (k == "normalK" || k == "shearK")) {
+      (k == "normalK" ? G.fk : G.fks) = v;
+      for (auto& f : G.fr) {
+        Fric n = make_fric(s, G, f.p1, f.p2);
+        f.k = n.k; f.ks = n.ks;
+      }
+      return 0;
+    }
+  }
+  s.err = "unknown group or parameter " + g + "." + k;
+  return -1;
+}
+/* Wall loader: the wall moves by v*dt after every step (the constant-speed phase of
+ * WallLoaderRunnable, Doc/Tutorial/examples/WallLoader.py.tex, run as a post-step hook). */
+int orc_set_wall_velocity(void* h, const char* name, const double* v) {
+  Sim& s = *(Sim*)h;
+  auto it = s.walls.find(name);
+  if (it == s.walls.end()) { s.err = "no such wall"; return -1; }
+  it->second.vel = V3(v[0], v[1], v[2]);
+  it->second.loader = v[0] != 0.0 || v[1] != 0.0 || v[2] != 0.0;
   return 0;
 }
 int orc_move_wall(void* h, const char* name, const double* d) {
@@ -977,3 +1043,491 @@ int orc_move_tagged(void* h, int tag, int mask, const double* d) {
 }
 long long orc_timestep(void* h) { return ((Sim*)h)->t; }
 }
+
+/* ==== Forward-mode dual-number window ==========================================
+ * Checker of the differentiable window: the step above restated on FP64 dual
+ * numbers (a value and kSeeds tangents) over a window of steps with the
+ * interaction lists, wall candidates and bond set frozen, as the GPU window
+ * freezes them.  Seeded on group parameters or initial velocities, it gives the
+ * exact derivative of every wall-group reaction along the branch the values
+ * take.  The primal arithmetic is the FP64 restatement's, operation by
+ * operation, so the values equal orc_step's.  Each law cites the same reference
+ * lines as its FP64 form above.
+ */
+namespace orc {
+namespace dual {
+
+constexpr int kSeeds = 8;
+
+struct Du {
+  double v = 0.0;
+  double d[kSeeds] = {};
+  Du() {}
+  Du(double x) : v(x) {}
+};
+static inline Du operator+(const Du& a, const Du& b) { Du r(a.v + b.v); for (int k = 0; k < kSeeds; ++k) r.d[k] = a.d[k] + b.d[k]; return r; }
+static inline Du operator-(const Du& a, const Du& b) { Du r(a.v - b.v); for (int k = 0; k < kSeeds; ++k) r.d[k] = a.d[k] - b.d[k]; return r; }
+static inline Du operator-(const Du& a) { Du r(-a.v); for (int k = 0; k < kSeeds; ++k) r.d[k] = -a.d[k]; return r; }
+static inline Du operator*(const Du& a, const Du& b) {
+  Du r(a.v * b.v);
+  for (int k = 0; k < kSeeds; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+static inline Du operator/(const Du& a, const Du& b) {
+  Du r(a.v / b.v);
+  for (int k = 0; k < kSeeds; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+  return r;
+}
+static inline Du& operator+=(Du& a, const Du& b) { a = a + b; return a; }
+static inline bool operator<(const Du& a, const Du& b) { return a.v < b.v; }
+static inline bool operator>(const Du& a, const Du& b) { return a.v > b.v; }
+static inline bool operator<=(const Du& a, const Du& b) { return a.v <= b.v; }
+static inline bool operator>=(const Du& a, const Du& b) { return a.v >= b.v; }
+static inline bool operator==(const Du& a, const Du& b) { return a.v == b.v; }
+static inline bool operator!=(const Du& a, const Du& b) { return a.v != b.v; }
+static inline Du dsqrt(const Du& a) {
+  Du r(std::sqrt(a.v));
+  const double g = r.v > 0.0 ? 0.5 / r.v : 0.0;
+  for (int k = 0; k < kSeeds; ++k) r.d[k] = a.d[k] * g;
+  return r;
+}
+static inline Du dacos(const Du& a) {
+  Du r(std::acos(a.v));
+  const double g = -1.0 / std::sqrt(1.0 - a.v * a.v);
+  for (int k = 0; k < kSeeds; ++k) r.d[k] = a.d[k] * g;
+  return r;
+}
+
+/* vec3.hpp / Quaternion.hpp / Matrix3.hpp on dual scalars (same operation order as V3, Q, M3) */
+struct DV {
+  Du x, y, z;
+  DV() {}
+  DV(const Du& a, const Du& b, const Du& c) : x(a), y(b), z(c) {}
+  explicit DV(const V3& a) : x(a.x), y(a.y), z(a.z) {}
+};
+static inline DV operator+(const DV& a, const DV& b) { return DV(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline DV operator-(const DV& a, const DV& b) { return DV(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline DV operator-(const DV& a) { return DV(-a.x, -a.y, -a.z); }
+static inline DV operator*(const DV& a, const Du& s) { return DV(a.x * s, a.y * s, a.z * s); }
+static inline DV operator*(const Du& f, const DV& a) { return DV(f * a.x, f * a.y, f * a.z); }
+static inline DV operator/(const DV& a, const Du& s) { return DV(a.x / s, a.y / s, a.z / s); }
+static inline DV& operator+=(DV& a, const DV& b) { a.x = a.x + b.x; a.y = a.y + b.y; a.z = a.z + b.z; return a; }
+static inline DV& operator-=(DV& a, const DV& b) { a.x = a.x - b.x; a.y = a.y - b.y; a.z = a.z - b.z; return a; }
+static inline Du ddot(const DV& a, const DV& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline DV dcross(const DV& l, const DV& r) {
+  return DV(l.y * r.z - l.z * r.y, l.z * r.x - l.x * r.z, l.x * r.y - l.y * r.x);
+}
+static inline Du dnorm2(const DV& a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+static inline Du dnorm(const DV& a) { return dsqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+struct DQ { Du s = 1.0; DV v; DQ() {} DQ(const Du& a, const DV& b) : s(a), v(b) {} };
+static inline DQ dqmul(const DQ& a, const DQ& b) {
+  return DQ(a.s * b.s - ddot(a.v, b.v), a.s * b.v + b.s * a.v + dcross(a.v, b.v));
+}
+static inline DQ dqinv(const DQ& a) { return DQ(a.s, -a.v); }
+struct DM { Du m[3][3]; };
+static inline DM dto_matrix(const DQ& q) {
+  DM r; const Du s = q.s, x = q.v.x, y = q.v.y, z = q.v.z;
+  r.m[0][0] = s * s + x * x - y * y - z * z;
+  r.m[0][1] = 2.0 * (x * y + s * z);
+  r.m[0][2] = 2.0 * (x * z - s * y);
+  r.m[1][0] = 2.0 * (x * y - s * z);
+  r.m[1][1] = s * s - x * x + y * y - z * z;
+  r.m[1][2] = 2.0 * (y * z + s * x);
+  r.m[2][0] = 2.0 * (x * z + s * y);
+  r.m[2][1] = 2.0 * (y * z - s * x);
+  r.m[2][2] = s * s - x * x - y * y + z * z;
+  return r;
+}
+static inline DM dtrans(const DM& a) { DM r; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[j][i]; return r; }
+static inline DV dmul(const DM& a, const DV& v) {
+  return DV(a.m[0][0] * v.x + a.m[0][1] * v.y + a.m[0][2] * v.z,
+            a.m[1][0] * v.x + a.m[1][1] * v.y + a.m[1][2] * v.z,
+            a.m[2][0] * v.x + a.m[2][1] * v.y + a.m[2][2] * v.z);
+}
+
+struct DState {
+  std::vector<DV> pos, vel, angvel, force, moment;
+  std::vector<DQ> quat;
+};
+
+struct Params {  /* seeded group parameters */
+  std::map<std::string, Du> k, ks, kt, kb;   /* per group: normalK, shearK, torsionK, bendingK */
+  Du visc_lin, visc_rot;
+};
+
+static DV dimage_of(const Sim& s, const DV& p1, DV p2) {
+  if (s.circx) {
+    const double dx = p1.x.v - p2.x.v;
+    if (dx > 0.5 * s.Lx) p2.x = p2.x + s.Lx;
+    else if (dx < -0.5 * s.Lx) p2.x = p2.x - s.Lx;
+  }
+  return p2;
+}
+
+/* CElasticInteraction ctor scaling + calcForces (Model/ElasticInteraction.cpp:25-71) */
+static void d_elastic(const Sim& s, const PairGroup& g, const Elastic& e, const Du& k, DState& st) {
+  double effR = 1.0, effA = 1.0, effL = 1.0;
+  const double r0 = s.P.rad[e.p1] + s.P.rad[e.p2];
+  if (g.scaling) { effR = 0.5 * r0; effL = r0; effA = effR * effR; }
+  const Du keff = k * effA / effL;
+  const DV x1 = st.pos[e.p1], x2 = dimage_of(s, x1, st.pos[e.p2]);
+  DV D = x1 - x2;
+  Du dist = ddot(D, D);
+  const double eq_dist = r0;
+  if (dist < (eq_dist * eq_dist)) {
+    dist = dsqrt(dist);
+    DV F = D * (keff * (dist - eq_dist) / dist);
+    st.force[e.p2] += F;
+    st.force[e.p1] += -1.0 * F;
+  }
+}
+
+struct DFric { DV Ffric; bool slipping, touching; };
+
+/* CRotFrictionInteraction ctor scaling + calcSimpleForces (Model/RotFricInteraction.cpp:103-231) */
+static void d_fric(const Sim& s, const PairGroup& g, const Fric& f0, DFric& f, const Du& k, const Du& ks, DState& st) {
+  double effR = 1.0, effL = 1.0, effA = 1.0;
+  const double r1 = s.P.rad[f0.p1], r2 = s.P.rad[f0.p2];
+  const double r0 = r1 + r2;
+  if (g.scaling) {
+    if (g.meanR) effR = 0.5 * r0; else effR = std::fmin(r1, r2);
+    effL = r0; effA = effR * effR;
+  }
+  const Du fk = k * effA / effL, fks = ks * effA / effL;
+  const double mu_current = f.slipping ? f0.mu_d : f0.mu_s;
+  const DV x1 = st.pos[f0.p1], x2 = dimage_of(s, x1, st.pos[f0.p2]);
+  const DV D = x1 - x2;
+  Du dist = ddot(D, D);
+  const double eq_dist = r1 + r2;
+  if (dist < (eq_dist * eq_dist)) {
+    dist = dsqrt(dist);
+    const DV force(D * (fk * (dist - eq_dist) / dist));
+    const DV pos(x2 + (r2 / eq_dist) * D);
+    st.force[f0.p2] += force;
+    st.force[f0.p1] += -1.0 * force;
+    const DV vp1 = st.vel[f0.p1] + dcross(st.angvel[f0.p1], pos - x1);
+    const DV vp2 = st.vel[f0.p2] + dcross(st.angvel[f0.p2], pos - x2);
+    DV ds((vp2 - vp1) * f0.dt);
+    ds -= ((ddot(ds, D)) / (dnorm2(D))) * D;
+    f.Ffric += fks * ds;
+    const Du FfricNorm = dnorm(f.Ffric);
+    const Du forceNorm = dnorm(force);
+    if (FfricNorm > forceNorm * mu_current) {
+      f.Ffric = f.Ffric * ((f0.mu_d * forceNorm) / FfricNorm);
+      f.slipping = true;
+    } else {
+      f.slipping = false;
+    }
+    const DV Moment1(dcross(pos - x1, f.Ffric));
+    const DV Moment2(dcross(pos - x2, -f.Ffric));
+    st.moment[f0.p1] += Moment1;
+    st.moment[f0.p2] += Moment2;
+    st.force[f0.p1] += f.Ffric;
+    st.force[f0.p2] += -1.0 * f.Ffric;
+    f.touching = true;
+  } else {
+    f.Ffric = DV(V3(0, 0, 0));
+    f.slipping = false;
+    f.touching = false;
+  }
+}
+
+static Du d_calc_angle(const Du& s_in, const Du& c_os) {   /* ARotBondedInteraction.cpp:22-51 */
+  if (s_in > 0.0) return (c_os >= 1.0 || c_os <= -1.0) ? Du(0.0) : dacos(c_os);
+  if (s_in == 0.0) return Du(0.0);
+  return (c_os >= 1.0 || c_os <= -1.0) ? Du(0.0) : -dacos(c_os);
+}
+
+/* Bond ctor scaling (RotBondedInteraction.cpp:122-161) + ARotBondedInteraction::calcForces
+ * (ARotBondedInteraction.cpp:307-448) + CRotBondedInteraction::broken (:175-219).
+ * Returns true when the bond would break. */
+static bool d_bond(const Sim& s, const PairGroup& g, const Bond& b, const Du& gkr, const Du& gks, const Du& gkt,
+                   const Du& gkb, DState& st) {
+  const double dist0 = std::sqrt(dot(b.D, b.D));
+  double effR = 1.0, effL = 1.0, effA = 1.0, J = 1.0, I = 1.0;
+  if (g.scaling) {
+    if (g.meanR) effR = 0.5 * dist0; else effR = std::fmin(s.P.rad[b.p1], s.P.rad[b.p2]);
+    effL = dist0; effA = effR * effR;
+    J = 0.5 * effR * effR * effR * effR; I = 0.5 * J;
+  }
+  const Du kr = gkr * effA / effL, ks = gks * effA / effL, kb = gkb * I / effL, kt = gkt * J / effL;
+  const double HALF_SQRT_2 = 0.5 * std::sqrt(2.0);
+  Du s_fai = 0.0, c_fai = 0.0, c_pasi2 = 0.0, s_pasi2 = 0.0, sita = 0.0, pasi = 0.0;
+  const DQ q1 = st.quat[b.p1], q2 = st.quat[b.p2];
+  const DV x1 = st.pos[b.p1], x2 = dimage_of(s, x1, st.pos[b.p2]);
+  const double r1 = s.P.rad[b.p1], r2 = s.P.rad[b.p2];
+  const DV mD(b.D);
+  const DM mat0 = dto_matrix(q1);
+  const DV rbp = x2 - x1;
+  const Du rbpNorm = dnorm(rbp);
+  const DV rb = dmul(mat0, x2 - x1);
+  const Du rbNorm = dnorm(rb);
+  const double r_0Norm = r1 + r2;
+  const DV delta_r = (rbNorm - r_0Norm) * rb / rbNorm;
+  const DV Fr = kr * delta_r;
+  const Du gama_cos = ddot(rb, mD) / (rbNorm * dnorm(mD));
+  Du gama = 0.0;
+  if (gama_cos < 1.0 && gama_cos > -1.0) gama = dacos(gama_cos);
+  const DV rb_0 = dcross(rb, mD);
+  const DV rb_b0 = dcross(rb, rb_0);
+  const Du rb_b0Norm = dnorm(rb_b0);
+  DV Fst(V3(0, 0, 0));
+  if (rb_b0Norm != 0.0) Fst = ks * r_0Norm * gama * rb_b0 / rb_b0Norm;
+  DV Mst(V3(0, 0, 0));
+  const Du rb_0Norm = dnorm(rb_0);
+  if (rb_0Norm != 0.0) Mst = -dnorm(Fst) * rb_0 / rb_0Norm;
+  const Du m0 = HALF_SQRT_2 * dsqrt((rbNorm + rb.z) / rbNorm);
+  Du m1 = -HALF_SQRT_2 * dsqrt((rbNorm - rb.z) / rbNorm);
+  Du m2 = -m1;
+  const Du m3 = 0.0;
+  const Du rbX2PlusRbY2 = rb.x * rb.x + rb.y * rb.y;
+  if (rbX2PlusRbY2 != 0.0) {
+    const Du denomSqrt = dsqrt(rbX2PlusRbY2);
+    m1 = m1 * rb.y / denomSqrt;
+    m2 = m2 * rb.x / denomSqrt;
+  }
+  const DQ qm(m0, DV(m1, m2, m3));
+  const DM mat = dto_matrix(qm);
+  const DM matTrans = dtrans(mat);
+  const DQ rp = dqmul(dqinv(q1), q2);
+  const DQ r = dqmul(dqmul(dqinv(qm), rp), qm);
+  const Du temp0 = r.s * r.s + r.v.z * r.v.z;
+  if (temp0 == 0.0) {
+    pasi = 0.0;
+  } else {
+    const Du sqrtTemp0 = dsqrt(temp0);
+    c_pasi2 = r.s / sqrtTemp0;
+    s_pasi2 = r.v.z / sqrtTemp0;
+    pasi = 2.0 * d_calc_angle(s_pasi2, c_pasi2);
+  }
+  const DV Mtp(Du(0.0), Du(0.0), kt * pasi);
+  const DV Mtr = dmul(matTrans, Mtp);
+  const Du temp2 = r.v.x * r.v.x + r.v.y * r.v.y;
+  const Du temp3 = r.v.x * r.v.z + r.s * r.v.y;
+  const Du temp4 = r.v.y * r.v.z - r.s * r.v.x;
+  DV Mbr(V3(0, 0, 0)), Fsr(V3(0, 0, 0)), Msr(V3(0, 0, 0));
+  if (temp2 != 0.0) {
+    const Du temp1 = temp0 - temp2;
+    if (temp1 >= 1.0 || temp1 <= -1.0) sita = 0.0; else sita = dacos(temp1);
+    if (temp0 == 0.0) {
+      const Du sqrtDenom = dsqrt(temp2);
+      c_fai = r.v.y / sqrtDenom;
+      s_fai = -r.v.x / sqrtDenom;
+    } else {
+      const Du sqrtDenom = dsqrt(temp0 * temp2);
+      c_fai = temp3 / sqrtDenom;
+      s_fai = temp4 / sqrtDenom;
+    }
+    const DV Mbp(-0.5 * kb * sita * s_fai, 0.5 * kb * sita * c_fai, Du(0.0));
+    Mbr = dmul(matTrans, Mbp);
+    const DV Fsp(-0.5 * ks * c_fai * sita * r_0Norm, -0.5 * ks * s_fai * sita * r_0Norm, Du(0.0));
+    Fsr = dmul(matTrans, Fsp);
+    const DV Msp(0.5 * ks * s_fai * sita * r_0Norm, -0.5 * ks * c_fai * sita * r_0Norm, Du(0.0));
+    Msr = dmul(matTrans, Msp);
+  }
+  const double eq_rad1 = r1 / (r1 + r2);
+  const double eq_rad2 = r2 / (r1 + r2);
+  const DM mat0Trans = dtrans(mat0);
+  const DV force = dmul(mat0Trans, Fr + Fst + Fsr);
+  const DV moment = dmul(mat0Trans, Mbr + Mtr + Msr * eq_rad1 * rbpNorm + Mst * eq_rad1 * rbpNorm);
+  const DV moment2 = dmul(mat0Trans, Msr * eq_rad2 * rbpNorm + Mst * eq_rad2 * rbpNorm - Mbr - Mtr);
+  const double shF = dnorm(Fst + Fsr).v, tM = dnorm(Mtr).v, bM = dnorm(Mbr).v;
+  const double r0 = r1 + r2;
+  const DV D = x1 - x2;
+  const double dist = std::sqrt(ddot(D, D).v);
+  const double nF = ((dist < r0) ? -1.0 : 1.0) * dnorm(Fr).v;
+  st.force[b.p2] += -1.0 * force;
+  st.force[b.p1] += force;
+  st.moment[b.p1] += moment;
+  st.moment[b.p2] += moment2;
+  const double shearStress = shF / b.max_s + b.beta2 * tM / b.max_t;
+  const double normalStress = nF / b.max_n + b.beta1 * bM / b.max_b;
+  return (normalStress > b.truncated) || (shearStress > (1.0 - normalStress));
+}
+
+/* CDamping / CRotDamping::calcForces (Model/Damping.hpp:99-124, Model/RotDamping.hpp:58-84), vref = 0 */
+static DV d_damping(const DV& v, const DV& frc, const Du& sm, const Du& mass, const Du& visc, double dt, int maxiter) {
+  const double s_limit2 = 1e-12;
+  DV v_rel(V3(0, 0, 0));
+  double error = 1.0;
+  int count = 0;
+  while ((error * error > s_limit2) & (count < maxiter)) {
+    count++;
+    DV v_old = v_rel;
+    v_rel = v + sm * dt * (frc - v_rel * visc * mass);
+    error = dnorm2(v_rel - v_old).v;
+  }
+  if (count >= maxiter) v_rel = DV(V3(0, 0, 0));
+  return -1.0 * visc * v_rel * mass;
+}
+
+}  // namespace dual
+}  // namespace orc
+
+extern "C" {
+
+/* Dual-number window of nsteps steps from the current state.  seeds[k] names the k-th tangent:
+ * "param:<group>:<key>" (RotBond normalK / shearK / torsionK / bendingK, dynamic-group normalK /
+ * shearK, "Damping" or "RotDamping" viscosity), "vel:<id>:<c>", "angvel:<id>:<c>" or
+ * "pos:<id>:<c>".  R[nsteps][wall groups][3] receives the reaction of each wall group (name
+ * order) after each step, dR[nsteps][wall groups][3][nseed] its derivatives.  The simulation
+ * itself is not advanced (only the head of its next step, the pending neighbour search and
+ * interaction update, is done).  Returns -5 if a rebuild or a bond break falls inside the window. */
+int orc_window_dual(void* h, int nsteps, int nseed, const char* const* seeds, double* R, double* dR) {
+  using namespace orc::dual;
+  Sim& s = *(Sim*)h;
+  if (nsteps < 1 || nseed < 0 || nseed > kSeeds) { s.err = "bad window size or seed count"; return -1; }
+  if (s.first) { search_neighbors(s); s.first = false; }
+  if (check_neighbors(s)) search_neighbors(s);
+  update_interactions(s);
+  const int n = s.P.n();
+  DState st;
+  st.pos.resize(n); st.vel.resize(n); st.angvel.resize(n); st.force.resize(n); st.moment.resize(n); st.quat.resize(n);
+  for (int i = 0; i < n; ++i) {
+    st.pos[i] = DV(s.P.pos[i]); st.vel[i] = DV(s.P.vel[i]); st.angvel[i] = DV(s.P.angvel[i]);
+    st.quat[i] = DQ(Du(s.P.quat[i].s), DV(s.P.quat[i].v));
+  }
+  Params prm;
+  for (auto& b : s.bpis) { prm.k[b.first] = b.second->kr; prm.ks[b.first] = b.second->ks; prm.kt[b.first] = b.second->kt; prm.kb[b.first] = b.second->kb; }
+  for (auto& d : s.dpis) {
+    if (d.second->kind == 0) prm.k[d.first] = d.second->k;
+    else { prm.k[d.first] = d.second->fk; prm.ks[d.first] = d.second->fks; }
+  }
+  if (s.damping.count("Damping")) prm.visc_lin = s.damping["Damping"].visc;
+  if (s.damping.count("RotDamping")) prm.visc_rot = s.damping["RotDamping"].visc;
+  for (int k = 0; k < nseed; ++k) {
+    std::string sd = seeds[k];
+    size_t a = sd.find(':'), b = sd.rfind(':');
+    if (a == std::string::npos || b == a) { s.err = "bad seed " + sd; return -1; }
+    std::string kind = sd.substr(0, a), mid = sd.substr(a + 1, b - a - 1), last = sd.substr(b + 1);
+    if (kind == "param") {
+      Du* p = nullptr;
+      if ((mid == "Damping" || mid == "RotDamping") && last == "viscosity") p = mid == "Damping" ? &prm.visc_lin : &prm.visc_rot;
+      else if (last == "normalK" && prm.k.count(mid)) p = &prm.k[mid];
+      else if (last == "shearK" && prm.ks.count(mid)) p = &prm.ks[mid];
+      else if (last == "torsionK" && prm.kt.count(mid)) p = &prm.kt[mid];
+      else if (last == "bendingK" && prm.kb.count(mid)) p = &prm.kb[mid];
+      if (!p) { s.err = "unknown parameter seed " + sd; return -1; }
+      p->d[k] = 1.0;
+    } else {
+      auto it = s.id2slot.find(std::atoi(mid.c_str()));
+      const int c = std::atoi(last.c_str());
+      if (it == s.id2slot.end() || c < 0 || c > 2) { s.err = "bad particle seed " + sd; return -1; }
+      DV* v = kind == "vel" ? &st.vel[it->second] : kind == "angvel" ? &st.angvel[it->second]
+                             : kind == "pos" ? &st.pos[it->second] : nullptr;
+      if (!v) { s.err = "bad seed kind " + sd; return -1; }
+      (c == 0 ? v->x : c == 1 ? v->y : v->z).d[k] = 1.0;
+    }
+  }
+  std::map<std::string, std::vector<DFric>> hist;
+  for (auto& d : s.dpis)
+    if (d.second->kind == 1)
+      for (auto& f : d.second->fr) hist[d.first].push_back(DFric{DV(f.Ffric), f.slipping, f.touching});
+  std::map<std::string, V3> wo;
+  for (auto& w : s.walls) wo[w.first] = w.second.o;
+  const int ng = (int)s.wig.size();
+  const double half = 0.5 * s.alpha, srsqr = half * half;
+  for (int j = 0; j < nsteps; ++j) {
+    if (j > 0) {  /* checkNeighbors at the head of step j: a rebuild would unfreeze the topology */
+      double mdsqr = 0;
+      for (int i = 0; i < n && mdsqr < srsqr; ++i) {
+        if (!s.P.alive[i]) continue;
+        V3 d(st.pos[i].x.v - s.P.oldpos[i].x, st.pos[i].y.v - s.P.oldpos[i].y, st.pos[i].z.v - s.P.oldpos[i].z);
+        double sq = dot(d, d);
+        mdsqr = (mdsqr < sq) ? sq : mdsqr;
+      }
+      if (mdsqr > srsqr) { s.err = "a neighbour rebuild falls inside the window"; return -5; }
+    }
+    for (int i = 0; i < n; ++i) { st.force[i] = DV(V3(0, 0, 0)); st.moment[i] = DV(V3(0, 0, 0)); }
+    int gi = 0;
+    for (auto& wg : s.wig) {   /* walls (EWallInteraction.hpp:42-78), reaction per group */
+      const Wall& w = s.walls[wg.second.wall];
+      const DV o(wo[wg.second.wall]), nn(w.n);
+      DV acc(V3(0, 0, 0));
+      for (auto& wi : wg.second.its) {
+        const Du dist = ddot(st.pos[wi.p] - o, nn);
+        const double r = s.P.rad[wi.p];
+        if (dist < r) {
+          const DV force = Du(wi.k) * (r - dist) * nn;
+          st.force[wi.p] += force;
+          if (wi.inner) acc -= -1.0 * force;
+        }
+      }
+      for (int c = 0; c < 3; ++c) {
+        const Du& v = c == 0 ? acc.x : c == 1 ? acc.y : acc.z;
+        const size_t o3 = ((size_t)j * ng + gi) * 3 + c;
+        R[o3] = v.v;
+        for (int k = 0; k < nseed; ++k) dR[o3 * nseed + k] = v.d[k];
+      }
+      ++gi;
+    }
+    for (auto& g : s.gravity)
+      for (int i = 0; i < n; ++i) if (s.P.alive[i]) st.force[i] += DV(g.second) * Du(s.P.mass[i]);
+    for (auto& d : s.dpis) {
+      if (d.second->kind == 0) {
+        for (auto& e : d.second->el) d_elastic(s, *d.second, e, prm.k[d.first], st);
+      } else {
+        auto& hv = hist[d.first];
+        for (size_t q = 0; q < d.second->fr.size(); ++q)
+          d_fric(s, *d.second, d.second->fr[q], hv[q], prm.k[d.first], prm.ks[d.first], st);
+      }
+    }
+    for (auto& b : s.bpis)
+      for (auto& bd : b.second->bd)
+        if (d_bond(s, *b.second, bd, prm.k[b.first], prm.ks[b.first], prm.kt[b.first], prm.kb[b.first], st)) {
+          s.err = "a bond breaks inside the window";
+          return -5;
+        }
+    for (auto& d : s.damping) {
+      if (d.first == "Damping") {
+        for (int i : s.damp_list)
+          st.force[i] += d_damping(st.vel[i], st.force[i], Du(s.P.invmass[i]), Du(s.P.mass[i]), prm.visc_lin,
+                                   d.second.dt, d.second.maxiter);
+      } else {
+        for (int i : s.damp_list)
+          st.moment[i] += d_damping(st.angvel[i], st.moment[i], Du(1.0 / s.P.inert[i]), Du(s.P.inert[i]),
+                                    prm.visc_rot, d.second.dt, d.second.maxiter);
+      }
+    }
+    const double dt = s.dt;
+    for (int i = 0; i < n; ++i) {   /* integrate (Particle.cpp:257-274, RotParticle.cpp:277-293) */
+      if (!s.P.alive[i]) continue;
+      if (s.rotmode) {
+        if (s.P.rot[i]) {
+          st.angvel[i] += Du(dt * s.P.invinert[i]) * st.moment[i];
+          const DQ w(Du(0.0), st.angvel[i]);
+          const DQ dq = dqmul(w, st.quat[i]);
+          const double c = dt / 2.0;
+          st.quat[i].s = st.quat[i].s + c * dq.s;
+          st.quat[i].v += Du(c) * dq.v;
+        } else {
+          st.angvel[i] = DV(V3(0, 0, 0));
+        }
+      }
+      if (s.P.dyn[i]) {
+        st.vel[i] += st.force[i] * Du(s.P.invmass[i]) * Du(dt);
+        st.pos[i] += st.vel[i] * Du(dt);
+      }
+    }
+    if (s.rotmode)   /* rescale (RotParticle.cpp:305-321) */
+      for (int i = 0; i < n; ++i) {
+        if (!s.P.alive[i]) continue;
+        DQ& q = st.quat[i];
+        const Du module = dsqrt(q.s * q.s + q.v.x * q.v.x + q.v.y * q.v.y + q.v.z * q.v.z);
+        if (module != 0.0) {
+          const Du inverse = Du(1.0) / module;
+          q = DQ(inverse * q.s, inverse * q.v);
+        }
+      }
+    for (auto& w : s.walls)   /* wall loaders move after the step */
+      if (w.second.loader) {
+        V3& o = wo[w.first];
+        o.x += w.second.vel.x * dt;
+        o.y += w.second.vel.y * dt;
+        o.z += w.second.vel.z * dt;
+      }
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -54,6 +54,9 @@ def _lib(backend: str):
         "add_exclusion": (C.c_int, [_P, _S, _S]),
         "step": (C.c_int, [_P, C.c_int]),
         "move_wall": (C.c_int, [_P, _S, _D]),
+        "set_wall_velocity": (C.c_int, [_P, _S, _D]),
+        "set_group_param": (C.c_int, [_P, _S, _S, C.c_double]),
+        "window_dual": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_char_p), _D, _D]),
         "apply_force_to_wall": (C.c_int, [_P, _S, _D]),
         "get_wall": (C.c_int, [_P, _S, _D, _D]),
         "num_particles": (C.c_int, [_P]),
@@ -166,6 +169,30 @@ class OracleSim:
 
     def apply_force_to_wall(self, group, force):
         self._chk(self.f["apply_force_to_wall"](self.h, group.encode(), _dp(_v3(force))))
+
+    def set_wall_velocity(self, name, v):
+        if "set_wall_velocity" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no wall loader")
+        self._chk(self.f["set_wall_velocity"](self.h, name.encode(), _dp(_v3(v))))
+        self._loaders = getattr(self, "_loaders", set()) | {name}
+
+    def set_group_param(self, group, key, value):
+        if "set_group_param" not in self.f:
+            raise NotImplementedError(f"{self.backend} cannot change group parameters")
+        self._chk(self.f["set_group_param"](self.h, group.encode(), key.encode(), float(value)))
+
+    def window_dual(self, nsteps, seeds, ngroups):
+        """Forward-mode dual-number window (the restatement only): wall-group reactions
+        R[nsteps, ngroups, 3] and their derivatives dR[nsteps, ngroups, 3, len(seeds)]
+        with respect to the named seeds (see orc_window_dual)."""
+        if "window_dual" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no dual window")
+        ns = len(seeds)
+        R = np.zeros((nsteps, ngroups, 3))
+        dR = np.zeros((nsteps, ngroups, 3, max(ns, 1)))
+        arr = (C.c_char_p * max(ns, 1))(*[x.encode() for x in seeds])
+        self._chk(self.f["window_dual"](self.h, int(nsteps), ns, arr, _dp(R), _dp(dR)))
+        return R, dR[..., :ns]
 
     def move_tagged(self, tag, d, mask=-1):
         self._chk(self.f["move_tagged"](self.h, tag, mask, _dp(_v3(d))))

@@ -110,3 +110,92 @@ def run_loaded(sim, steps, rate):
         sim.move_wall("top", (0, -rate, 0))
         sim.move_wall("bottom", (0, rate, 0))
         sim.step(1)
+
+
+WINDOW_SEEDS = ("param:bonds:normalK", "param:bonds:shearK", "param:bonds:torsionK", "param:bonds:bendingK",
+                "param:Damping:viscosity", "param:RotDamping:viscosity")
+WINDOW_PARAMS = (("bonds", "normalK"), ("bonds", "shearK"), ("bonds", "torsionK"), ("bonds", "bendingK"),
+                 ("Damping", "viscosity"), ("RotDamping", "viscosity"))
+
+
+def mse_target(R, seed=7):
+    """A seeded target curve for the platen-force MSE: the window's own
+    reactions smoothed and scaled by a seeded factor per wall."""
+    rng = np.random.default_rng(seed)
+    k = np.ones(9) / 9.0
+    sm = np.empty_like(R)
+    for g in range(R.shape[1]):
+        for c in range(3):
+            sm[:, g, c] = np.convolve(R[:, g, c], k, mode="same")
+    return sm * rng.uniform(0.8, 1.2, size=(1, R.shape[1], 1))
+
+
+def mse(R, tgt):
+    return float(((R - tgt) ** 2).mean())
+
+
+def mse_grad(R, tgt):
+    return 2.0 * (R - tgt) / R.size
+
+
+def window_block(make, nx=4, ny=5, nz=4, seed=4, dt=1e-4, kr=1e5, ks=1e5, kt=1e5, kb=1e5, visc=1.0, vscale=1.0,
+                 platen_speed=0.5, friction=False, vel=None, angvel=None, tilt=(0.5, 0.3)):
+    """Bonded block for the differentiable window: a cubic lattice of RotSpheres
+    (r ~ U[0.49, 0.5]) with every lattice neighbour bonded, strengths far above
+    the loads (elastic regime, no breaks), platens that
+    start just touching the block and move inward at ``platen_speed`` (so the
+    reactions are carried by the bonds), seeded initial linear and angular
+    velocities (``vel`` / ``angvel`` override them, rows by id) and the
+    stiffness / damping parameters as arguments.  The defaults give every
+    parameter a loss sensitivity well above the FP64 rounding noise of a
+    200-step window, so that central differences at h = 1e-6 relative resolve
+    the gradient (torsion / bending stiffness as large as the normal one, and a
+    damping viscosity that changes the reactions by percents).  The lattice is tilted by
+    ``tilt`` (radians about x, then y) so that no bond lies near the z axis,
+    where the RotBond law's frame quaternion (ARotBondedInteraction.cpp:349-364)
+    takes square roots of cancelling differences and its derivatives are
+    ill-conditioned in any arithmetic."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) * 1.0
+    ax, ay = tilt
+    rx = np.array([[1, 0, 0], [0, np.cos(ax), -np.sin(ax)], [0, np.sin(ax), np.cos(ax)]])
+    ry = np.array([[np.cos(ay), 0, np.sin(ay)], [0, 1, 0], [-np.sin(ay), 0, np.cos(ay)]])
+    c = pos.mean(axis=0)
+    pos = (pos - c) @ (ry @ rx).T
+    pos = pos - pos.min(axis=0) + 1.0
+    n = len(g)
+    rad = rng.uniform(0.49, 0.5, size=n)
+    d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
+    np.fill_diagonal(d, np.inf)
+    gap = d - (rad[:, None] + rad[None, :])
+    i1, i2 = np.nonzero(np.triu(gap <= 0.021, 1))   # every lattice neighbour: a connected solid
+    v0 = rng.normal(0, vscale, size=(n, 3)) if vel is None else np.asarray(vel, dtype=np.float64)
+    w0 = rng.normal(0, vscale, size=(n, 3)) if angvel is None else np.asarray(angvel, dtype=np.float64)
+    top = pos.max(axis=0) + 1.0
+    sim = make("RotSphere", 1.25, 0.2, (0, 0, 0), tuple(float(x) for x in top), (0, 0, 0), dt)
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=v0, angvel=w0)
+    sim.add_connections(np.ones(len(i1), np.int32), i1, i2)
+    sim.add_rot_bond_group("bonds", 1, kr, ks, kt, kb, 1e6, 1e6, 1e6, 1e6, True, True, 1.0)
+    if friction:
+        sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
+        sim.add_exclusion("bonds", "friction")
+    sim.add_wall("bottom", (0, float((pos[:, 1] - rad).min()), 0), (0, 1, 0))
+    sim.add_wall("top", (0, float((pos[:, 1] + rad).max()), 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e5)
+    sim.add_wall_group("top_w", "top", 1e5)
+    sim.add_damping(0, visc, 50)
+    sim.add_damping(1, visc, 50)
+    sim.set_wall_velocity("bottom", (0, platen_speed, 0))
+    sim.set_wall_velocity("top", (0, -platen_speed, 0))
+    return sim
+
+
+def wall_force_history(sim, nsteps, groups=("bottom_w", "top_w"), walls=("bottom", "top")):
+    """Step one at a time and collect each wall's reaction after every step."""
+    out = np.zeros((nsteps, len(walls), 3))
+    for t in range(nsteps):
+        sim.step(1)
+        for k, w in enumerate(walls):
+            out[t, k] = sim.wall(w)[1]
+    return out
