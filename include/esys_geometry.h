@@ -18,6 +18,14 @@ extern "C" {
 int lsm_pack_rsi(unsigned long long seed, int n, const double* bmin, const double* bmax, int periodic_x, int dist,
                  double p0, double p1, double rmin, double rmax, int max_attempts, double* pos, double* rad);
 
+/* Dense random packing by gap filling (the role of Geometry/RandomBoxPacker.hpp: a seed
+ * packing, then spheres fitted to touch their four nearest neighbours, or three and the nearest
+ * box face, FittedParticleIterator::generateNext).  Radii of fitted spheres lie in
+ * [rmin, rmax]; stops at n spheres or after max_failures consecutive rejected trials.  Returns
+ * the number placed or -1 on bad arguments. */
+int lsm_pack_fit(unsigned long long seed, int n, const double* bmin, const double* bmax, double rmin, double rmax,
+                 int max_failures, double* pos, double* rad);
+
 #ifdef __cplusplus
 }
 #endif
