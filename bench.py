@@ -161,6 +161,107 @@ def cpu_reference_sample(w, steps, timeout_s=60.0):
     return {"value": (m + ncand) * done / dt, "steps": done, "seconds": dt, "pairs": int(m), "walls": ncand}
 
 
+# ---- differentiable calibration window (adjoint leg) --------------------------------------
+W_DT, W_STEPS, W_CKPT = 1e-5, 2000, 100
+W_KN, W_KS, W_KT, W_KB, W_VISC = 1e5, 1e5, 1e3, 1e3, 0.05
+
+
+def window_workload(n=50_000, seed=4):
+    """Bonded block: n RotSpheres fitted into 40 x 80 x 40 (radii in [0.2, 1.0]), every pair
+    within a 1e-3 gap bonded; seeded small initial velocities."""
+    from esys.lsm import geometry as G
+
+    pos, rad = G.fit_pack(n, (0, 0, 0), (40, 80, 40), 0.2, 1.0, seed=seed, max_failures=5000)
+    i1, i2 = G.distance_connections(pos, rad, 1e-3)
+    rng = np.random.default_rng(seed + 100)
+    m = len(rad)
+    return dict(pos=pos, rad=rad, mass=(4.0 / 3.0) * PI_REF * rad ** 3, ids=np.arange(m, dtype=np.int32),
+                vel=rng.normal(0, 0.01, size=(m, 3)), angvel=rng.normal(0, 0.01, size=(m, 3)), i1=i1, i2=i2)
+
+
+def window_setup(make, w):
+    sim = make("RotSphere", 2.2, 0.2, (0, 0, 0), (40, 80, 40), (0, 0, 0), W_DT)
+    n = len(w["ids"])
+    sim.add_particles(w["ids"], w["pos"], w["rad"], w["mass"], tag=np.zeros(n, np.int32), vel=w["vel"],
+                      angvel=w["angvel"])
+    sim.add_connections(np.ones(len(w["i1"]), np.int32), w["i1"], w["i2"])
+    sim.add_rot_bond_group("bonds", 1, W_KN, W_KS, W_KT, W_KB, 1e6, 1e6, 1e6, 1e6, True, True, 1.0)
+    y0 = float((w["pos"][:, 1] - w["rad"]).min())
+    y1 = float((w["pos"][:, 1] + w["rad"]).max())
+    sim.add_wall("bottom", (0, y0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, y1, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e5)
+    sim.add_wall_group("top_w", "top", 1e5)
+    sim.add_damping(0, W_VISC, 100)
+    sim.add_damping(1, W_VISC, 100)
+    sim.set_wall_velocity("bottom", (0, 1.0, 0))
+    sim.set_wall_velocity("top", (0, -1.0, 0))
+    return sim
+
+
+def window_target(R, seed=4):
+    """Seeded target curve: a smooth ramp per platen with the window's own scale."""
+    rng = np.random.default_rng(seed)
+    t = np.linspace(0.0, 1.0, R.shape[0])[:, None, None]
+    return np.abs(R).max() * rng.uniform(0.5, 1.0, size=(1, R.shape[1], 3)) * t * np.sign(R.mean(axis=0) + 1e-300)
+
+
+def adjoint_leg(stream):
+    """Forward window + reverse sweep on the C4-style bonded block; adjoint grads/s vs the
+    central-difference alternative (two forward windows per gradient component)."""
+    from esys.lsm import _capi
+
+    w = window_workload()
+    sim = window_setup(lambda *a: _capi.DemSim(*a), w)
+    sim.set_stream(stream.cuda_stream)
+    sim.set_option("precision", 64)
+    sim.step(1)  # set-up step (first neighbour search), not part of the window
+    n = sim.num_particles()
+    t0 = time.perf_counter()
+    R = sim.window_forward(W_STEPS, W_CKPT)
+    t1 = time.perf_counter()
+    tgt = window_target(R)
+    gR = 2.0 * (R - tgt) / R.size
+    g = sim.window_adjoint(gR)
+    t2 = time.perf_counter()
+    loss0 = float(((R - tgt) ** 2).mean())
+    # a plain forward window (the unit cost of a finite difference)
+    sim.window_rewind()
+    t3 = time.perf_counter()
+    sim.window_forward(W_STEPS, W_STEPS)
+    t4 = time.perf_counter()
+    # central difference of the loss in normalK at h = 1e-6 relative, beside the adjoint's value
+    layout = sim.param_layout()
+    slot = layout.index(("bonds", "normalK"))
+    losses = []
+    for sgn in (1, -1):
+        sim.window_rewind()
+        sim.set_group_param("bonds", "normalK", W_KN * (1 + sgn * 1e-6))
+        r = sim.window_forward(W_STEPS, W_STEPS)
+        losses.append(float(((r - tgt) ** 2).mean()))
+    sim.window_rewind()
+    sim.set_group_param("bonds", "normalK", W_KN)
+    g_fd = (losses[0] - losses[1]) / (2e-6 * W_KN)
+    grads = len(g["params"]) + 3 * n  # parameters and initial linear velocities (spins come too, uncounted)
+    t_adj = t2 - t0
+    t_fwd = t4 - t3
+    bonds = len(w["i1"])
+    sim.close()
+    return {
+        "workload": f"bonded block: {n} RotSpheres fitted in 40x80x40 (r in [0.2,1.0]), {bonds} RotBonds "
+                    f"(kn=ks=1e5, kt=kb=1e3, elastic regime), 2 elastic platens at 1.0/s, linear+rotational "
+                    f"damping 0.05, dt=1e-5, {W_STEPS}-step window, checkpoints every {W_CKPT}",
+        "loss": "MSE of the platen reaction histories vs a seeded ramp target", "loss_value": loss0,
+        "dtype": "f64", "gradient_components": grads,
+        "forward_with_checkpoints_s": t1 - t0, "reverse_sweep_s": t2 - t1, "plain_forward_s": t_fwd,
+        "adjoint_grads_per_s": grads / t_adj, "fd_grads_per_s": 1.0 / (2.0 * t_fwd),
+        "adjoint_vs_fd_speedup": (grads / t_adj) / (1.0 / (2.0 * t_fwd)),
+        "fd_check": {"param": "bonds.normalK", "h_rel": 1e-6, "adjoint": float(g["params"][slot]),
+                     "central_difference": g_fd,
+                     "rel_err": abs(float(g["params"][slot]) - g_fd) / max(abs(g_fd), 1e-300)},
+    }
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -198,6 +299,7 @@ def main():
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64],
                     help="32: FP32 pair forces + FP64 integration (headline); 64: FP64 throughout")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-window leg")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
                     help="step kernels: -1 automatic, 0 fused, 1 pair kernel + integration kernel")
     args = ap.parse_args()
@@ -337,6 +439,10 @@ def main():
         dist.all_reduce(cc)
         e2e_val = float(cc.item()) / float(t.item())
 
+    adj = None
+    if not args.no_adjoint:
+        adj = adjoint_leg(stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_reference_sample(w, steps=30, timeout_s=25.0)
@@ -375,6 +481,7 @@ def main():
                     "d2h_bytes_per_step": n * (6 * 32 + 4)},
             "gpu_launches": c1["launches"] - c0["launches"],
             "clocks": clk.summary(),
+            "adjoint": adj,
         }
         print(json.dumps(line))
     sim.close()
