@@ -16,10 +16,10 @@ LIB = os.path.join(HERE, "lib", "libesys_dem_b200.so")
 # (source, FMA contraction): the FP64 path is built without FMA so that it rounds
 # like the reference; the FP32-force instances use FMA.
 SOURCES = [("dem_kernels.cu", False), ("dem_sim.cu", False), ("dem_noalloc.cu", False), ("dem_step_fp32.cu", True),
-           ("dem_adjoint.cu", False),
+           ("dem_adjoint.cu", False), ("dem_batch.cu", False), ("dem_batch_fp32.cu", True),
            ("packing.cpp", False)]
 HEADERS = ["dem_device.cuh", "dem_kernels.h", "dem_laws.cuh", "dem_laws_f32.cuh", "dem_math.cuh", "dem_common.cuh",
-           "dem_step.cuh", "dem_adjoint.h", "dem_dual.cuh"]
+           "dem_step.cuh", "dem_adjoint.h", "dem_dual.cuh", "dem_batch.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

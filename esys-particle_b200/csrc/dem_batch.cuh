@@ -1,0 +1,157 @@
+// Batched ensemble step: many independent specimens (each one simulated worker
+// with its own particles, interaction groups, walls and step counter) advance
+// together, one launch per timestep for all of them.
+//
+// The launch is a persistent one-wave grid over the concatenated particle tiles
+// of every specimen.  A tile maps to its specimen through a prefix table of tile
+// counts; the specimen's step arguments (the same StepArgs its own k_step
+// launch would get, for both buffer parities) are read from a device table, so
+// a captured graph of launches stays valid while the table's contents change.
+// Per tile the work is exactly k_step's per-particle work (pair_sums +
+// finish_particle), hence per-particle results equal a specimen run alone.  The
+// wall reactions are reduced per tile; the last tile of a specimen to finish
+// (counted on the specimen's own counter) completes that specimen's step: wall
+// totals, wall loaders, its step counter and its stop word.  A specimen whose
+// stop word is set, or which has reached its target step, skips the launch.
+#pragma once
+#include "dem_step.cuh"
+
+namespace dem {
+
+__device__ __forceinline__ int batch_specimen(const BatchArgs& B, int tile) {
+  int lo = 0, hi = B.nspec;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(B.tile_start + mid) <= tile) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Per-tile wall partials, then the last tile of the specimen finishes its step
+// (the same fixed-order reduction as step_epilogue, over the specimen's tiles).
+__device__ __forceinline__ void batch_tile_epilogue(const StepArgs& a, long long step, int ltile, int ntiles,
+                                                    int wlane, int warp, double (*s_red)[kMaxWalls][3],
+                                                    bool* s_last) {
+  const int nw3 = a.nwall * 3;
+  __syncthreads();
+  if (threadIdx.x < nw3) {
+    const int w = threadIdx.x / 3, c = threadIdx.x % 3;
+    double acc = 0.0;
+    for (int k = 0; k < kStepWarps; ++k) acc += s_red[k][w][c];
+    a.wall_partial[((size_t)ltile * kMaxWalls + w) * 3 + c] = acc;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicInc(a.block_counter, (unsigned)ntiles - 1u);
+    *s_last = (prev == (unsigned)ntiles - 1u);
+  }
+  __syncthreads();
+  if (!*s_last) return;
+  __threadfence();
+  for (int wc = 0; wc < nw3; ++wc) {
+    const int w = wc / 3, c = wc % 3;
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < ntiles; b += blockDim.x)
+      acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __syncthreads();
+    if (wlane == 0) s_red[warp][0][0] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
+      a.wall_force[3 * w + c] = t;
+      if (a.wall_hist) a.wall_hist[(size_t)(step - a.wall_hist_t0 - 1) * (kMaxWalls * 3) + 3 * w + c] = t;
+    }
+  }
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < a.nwall; ++w) {  // native wall loader: origin += v*dt per step
+      WallDev* W = a.walls + w;
+      if (a.wall_vel[3 * w] != 0.0 || a.wall_vel[3 * w + 1] != 0.0 || a.wall_vel[3 * w + 2] != 0.0) {
+        W->ox += a.wall_vel[3 * w] * a.dt;
+        W->oy += a.wall_vel[3 * w + 1] * a.dt;
+        W->oz += a.wall_vel[3 * w + 2] * a.dt;
+      }
+    }
+    *a.step_counter = step;
+    volatile int* ctrl = a.ctrl;
+    if (*ctrl) *a.stop = 1;
+  }
+}
+
+template <bool ROT, int TPP, int FEAT, bool FP32>
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 : 2)) k_step_batch(const BatchArgs B) {
+  __shared__ double s_red[kStepWarps][kMaxWalls][3];
+  __shared__ bool s_last;
+  const int lane = threadIdx.x % TPP;
+  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int tile = blockIdx.x; tile < B.total_tiles; tile += gridDim.x) {
+    const int sp = batch_specimen(B, tile);
+    const StepArgs& a0 = B.args[2 * sp];
+    // The specimen's counter and stop word change only in its own last tile, after every
+    // tile of this launch has read them: the decision below is uniform over its tiles.
+    const long long done = *(volatile long long*)a0.step_counter;
+    if (*(volatile int*)a0.stop || done >= __ldg(B.target + sp)) continue;
+    const int cur = (int)((done - __ldg(B.base_t + sp) + __ldg(B.base_cur + sp)) & 1);
+    const StepArgs& a = B.args[2 * sp + cur];
+    const long long step = done + 1;
+    const int t0 = __ldg(B.tile_start + sp);
+    const int ltile = tile - t0, ntiles = __ldg(B.tile_start + sp + 1) - t0;
+    const ParticleBuf in = a.P.buf[a.cur];
+    const ParticleBuf out = a.P.buf[a.cur ^ 1];
+    __syncthreads();  // the previous tile's epilogue has finished with s_red
+    for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kStepThreads) (&s_red[0][0][0])[k] = 0.0;
+    __syncthreads();
+    const int i = (ltile * kStepThreads + threadIdx.x) / TPP;
+    const bool valid = i < a.P.n;
+    unsigned pf = 0u;
+    double4 p4 = make_double4(0, 0, 0, 0), q4 = make_double4(1, 0, 0, 0);
+    if (valid) {
+      pf = __ldg(a.P.pflags + i);
+      p4 = ldg4(in.pr + i);
+      if (lane == 0) {
+        prefetch_l1(in.vm + i);
+        if (ROT) { prefetch_l1(in.wi + i); prefetch_l1(in.qq + i); }
+        prefetch_l1(a.P.oldpos + i);
+        if (FP32 && ROT) prefetch_l1(in.vw + 2 * i);
+      }
+      if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);
+    }
+    const bool alive = valid && (pf & PF_ALIVE);
+    V Fp, Mp;
+    pair_sums<ROT, TPP, FEAT, FP32, false>(a, in, i, lane, alive, step, p4, q4, Fp, Mp);
+    finish_particle<ROT, TPP, FP32, false>(a, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
+                                           ROT && (FEAT & F_BOND), Fp, Mp, s_red);
+    batch_tile_epilogue(a, step, ltile, ntiles, wlane, warp, s_red, &s_last);
+  }
+}
+
+template <bool R, int T, int FEAT, bool FP32>
+inline void launch_batch_fixed(const BatchArgs& B, cudaStream_t s) {
+  const int wave = one_wave(k_step_batch<R, T, FEAT, FP32>);
+  const int grid = B.total_tiles < wave ? B.total_tiles : wave;
+  if (grid > 0) k_step_batch<R, T, FEAT, FP32><<<grid, kStepThreads, 0, s>>>(B);
+}
+
+template <bool R, int FEAT, bool FP32>
+inline void launch_batch_tpp(const BatchArgs& B, int tpp, cudaStream_t s) {
+  switch (tpp) {
+    case 1: launch_batch_fixed<R, 1, FEAT, FP32>(B, s); break;
+    case 2: launch_batch_fixed<R, 2, FEAT, FP32>(B, s); break;
+    case 4: launch_batch_fixed<R, 4, FEAT, FP32>(B, s); break;
+    default: launch_batch_fixed<R, 8, FEAT, FP32>(B, s); break;
+  }
+}
+
+// Instances: non-rotational elastic; rotational friction, friction + bonds, and the general one.
+template <bool FP32>
+inline void launch_batch_any(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, int tpp, cudaStream_t s) {
+  if (!rot) return launch_batch_tpp<false, F_ELASTIC, FP32>(B, tpp, s);
+  if (!bd && fr && !el) return launch_batch_tpp<true, F_FRIC, FP32>(B, tpp, s);
+  if (bd && !el) return launch_batch_tpp<true, F_FRIC | F_BOND, FP32>(B, tpp, s);
+  return launch_batch_tpp<true, F_ELASTIC | F_FRIC | F_BOND, FP32>(B, tpp, s);
+}
+
+}  // namespace dem

@@ -145,4 +145,15 @@ struct StepArgs {
   int* stop;                // set by the last block when ctrl != 0: later steps of the chunk skip
 };
 
+// Batched ensemble step (dem_batch.cuh): the specimens' step arguments in a device table.
+struct BatchArgs {
+  int nspec;
+  int total_tiles;
+  const StepArgs* args;     // [nspec][2]: step arguments for input buffer 0 and 1
+  const int* tile_start;    // [nspec + 1]: prefix of step_tiles(n, TPP)
+  const long long* base_t;  // [nspec]: the specimen's step counter when the table was written
+  const int* base_cur;      // [nspec]: its input buffer then
+  const long long* target;  // [nspec]: last timestep to compute in this call
+};
+
 }  // namespace dem

@@ -1088,6 +1088,233 @@ struct DemSim {
   }
 };
 
+// ---- batched ensemble (many independent workers, one launch per timestep) ----
+// Each specimen is a complete DemSim: its rebuilds, interaction updates, bond
+// failures and step counter stay its own, so each advances exactly as it would
+// alone.  Between chunks the host runs every specimen's runOneStep head
+// (prepare); within a chunk one k_step_batch launch per timestep advances every
+// specimen that has not stopped or reached its target.  Chunks are replayed from
+// a captured CUDA graph (the kernels read everything through a fixed device
+// table, so one graph per chunk length serves every chunk).
+struct Ensemble {
+  std::string err;
+  std::vector<DemSim*> sims;
+  std::vector<cudaStream_t> saved;
+  cudaStream_t s = nullptr;
+  int tpp = 0, chunk = 64, use_graph = 1, profile = 0;
+  int rot = 0, fp32 = 0;
+  bool el = false, fr = false, bd = false;
+  DBuf<StepArgs> d_args;
+  DBuf<int> d_tile_start, d_base_cur, d_status_ctrl;
+  DBuf<long long> d_base_t, d_target, d_status_t;
+  StepArgs* h_args = nullptr;   // pinned staging of the table
+  long long* h_t = nullptr;     // pinned status
+  int* h_ctrl = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;  // chunk length -> instantiated graph
+  int graph_tpp = -1, graph_tiles = -1;
+  long long c_steps = 0, c_contacts = 0, c_launches = 0, c_chunks = 0, c_rebuild_calls = 0;
+  double prof_ms = 0.0;
+  long long prof_steps = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  Ensemble(DemSim* const* list, int n) {
+    if (n < 1) throw std::invalid_argument("an ensemble needs at least one specimen");
+    for (int k = 0; k < n; ++k) {
+      if (!list[k]) throw std::invalid_argument("null specimen handle");
+      for (int j = 0; j < k; ++j)
+        if (list[j] == list[k]) throw std::invalid_argument("a specimen appears twice in the ensemble");
+      sims.push_back(list[k]);
+    }
+    rot = sims[0]->rot;
+    for (DemSim* d : sims)
+      if (d->rot != rot) throw std::invalid_argument("ensemble specimens must share the particle type");
+    DEM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const int ns = (int)sims.size();
+    d_args.reserve((size_t)2 * ns);
+    d_tile_start.reserve(ns + 1);
+    d_base_cur.reserve(ns);
+    d_base_t.reserve(ns);
+    d_target.reserve(ns);
+    d_status_t.reserve(ns);
+    d_status_ctrl.reserve(ns);
+    DEM_CUDA(cudaMallocHost(&h_args, sizeof(StepArgs) * 2 * ns));
+    DEM_CUDA(cudaMallocHost(&h_t, sizeof(long long) * ns));
+    DEM_CUDA(cudaMallocHost(&h_ctrl, sizeof(int) * ns));
+  }
+  ~Ensemble() {
+    if (s) cudaStreamSynchronize(s);
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    d_args.release(); d_tile_start.release(); d_base_cur.release(); d_status_ctrl.release();
+    d_base_t.release(); d_target.release(); d_status_t.release();
+    if (h_args) cudaFreeHost(h_args);
+    if (h_t) cudaFreeHost(h_t);
+    if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (s) cudaStreamDestroy(s);
+  }
+
+  // Work of the specimens runs on the ensemble's stream for the duration of a call.
+  void borrow() {
+    saved.clear();
+    for (DemSim* d : sims) {
+      d->sync();
+      saved.push_back(d->s);
+      d->s = s;
+    }
+  }
+  void give_back() {
+    cudaStreamSynchronize(s);
+    for (size_t k = 0; k < sims.size() && k < saved.size(); ++k) sims[k]->s = saved[k];
+    saved.clear();
+  }
+
+  int pick_tpp() const {
+    if (tpp) return tpp;
+    long long e = 0, np = 0;
+    for (DemSim* d : sims) {
+      for (auto& g : d->dyn) e += 2LL * g.second.m;
+      for (auto& b : d->bond) e += 2LL * b.second.nb;
+      np += d->n;
+    }
+    const double mean = np ? (double)e / np : 0.0;
+    if (mean >= 12) return 8;
+    if (mean >= 6) return 4;
+    if (mean >= 2.5) return 2;
+    return 1;
+  }
+
+  void launch_chunk(const BatchArgs& B, int k, int t_pp) {
+    auto one = [&]() {
+      if (fp32) launch_batch_step_fp32(B, rot != 0, el, fr, bd, t_pp, s);
+      else launch_batch_step(B, rot != 0, el, fr, bd, t_pp, s);
+    };
+    if (!use_graph) {
+      for (int j = 0; j < k; ++j) one();
+      DEM_CUDA(cudaGetLastError());
+      return;
+    }
+    if (graph_tpp != t_pp || graph_tiles != B.total_tiles) {
+      // a new launch shape runs once uncaptured first (it sets up the per-instance occupancy
+      // query), then later chunks are captured and replayed
+      for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+      graphs.clear();
+      graph_tpp = t_pp;
+      graph_tiles = B.total_tiles;
+      for (int j = 0; j < k; ++j) one();
+      DEM_CUDA(cudaGetLastError());
+      return;
+    }
+    auto it = graphs.find(k);
+    if (it == graphs.end()) {
+      cudaGraph_t g = nullptr;
+      DEM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      for (int j = 0; j < k; ++j) one();
+      const cudaError_t le = cudaGetLastError();
+      const cudaError_t ce = cudaStreamEndCapture(s, &g);
+      DEM_CUDA(le);
+      DEM_CUDA(ce);
+      cudaGraphExec_t ex = nullptr;
+      const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      DEM_CUDA(ie);
+      it = graphs.emplace(k, ex).first;
+    }
+    DEM_CUDA(cudaGraphLaunch(it->second, s));
+  }
+
+  int step(int nsteps) {
+    if (nsteps < 0) throw std::invalid_argument("negative step count");
+    const int ns = (int)sims.size();
+    fp32 = sims[0]->fp32;
+    for (DemSim* d : sims)
+      if (d->fp32 != fp32) throw std::invalid_argument("ensemble specimens must share the precision form");
+    borrow();
+    struct Back { Ensemble* e; ~Back() { e->give_back(); } } back{this};
+    std::vector<long long> target(ns);
+    for (int k = 0; k < ns; ++k) target[k] = sims[k]->t + nsteps;
+    const int t_pp = pick_tpp();
+    while (true) {
+      long long remaining = 0;
+      for (int k = 0; k < ns; ++k) remaining = std::max(remaining, target[k] - sims[k]->t);
+      if (remaining <= 0) break;
+      // every unfinished specimen's runOneStep head (its own rebuild / interaction update)
+      el = fr = bd = false;
+      std::vector<int> tile_start(ns + 1, 0);
+      std::vector<int> base_cur(ns);
+      std::vector<long long> base_t(ns);
+      std::vector<long long> cps(ns);
+      for (int k = 0; k < ns; ++k) {
+        DemSim& d = *sims[k];
+        if (d.t < target[k]) {
+          if (!d.prepare()) { err = "specimen " + std::to_string(k) + ": " + d.err; return DEM_ERR_OVERFLOW; }
+        }
+        for (auto& g : d.dyn) (g.second.kind == 0 ? el : fr) = true;
+        if (!d.bond.empty()) bd = true;
+        tile_start[k + 1] = tile_start[k] + step_grid(d.n, t_pp);
+        d.d_wall_partial.reserve((size_t)step_grid(d.n, t_pp) * kMaxWalls * 3);
+        h_args[2 * k] = d.make_args(0);
+        h_args[2 * k + 1] = d.make_args(1);
+        h_args[2 * k].store_forces = h_args[2 * k + 1].store_forces = d.store_forces;
+        base_cur[k] = d.cur;
+        base_t[k] = d.t;
+        cps[k] = d.contacts_per_step();
+      }
+      DEM_CUDA(cudaMemcpyAsync(d_args.p, h_args, sizeof(StepArgs) * 2 * ns, cudaMemcpyHostToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_tile_start.p, tile_start.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_base_cur.p, base_cur.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_base_t.p, base_t.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_target.p, target.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
+      launch_batch_reset(d_args.p, ns, s);
+      if (fp32) launch_batch_sync_vw(d_args.p, d_base_cur.p, ns, s);
+      const int k = (int)std::min<long long>(chunk, remaining);
+      BatchArgs B{};
+      B.nspec = ns;
+      B.total_tiles = tile_start[ns];
+      B.args = d_args.p;
+      B.tile_start = d_tile_start.p;
+      B.base_t = d_base_t.p;
+      B.base_cur = d_base_cur.p;
+      B.target = d_target.p;
+      if (profile) {
+        if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
+        DEM_CUDA(cudaEventRecord(ev0, s));
+      }
+      launch_chunk(B, k, t_pp);
+      if (profile) DEM_CUDA(cudaEventRecord(ev1, s));
+      launch_batch_status(d_args.p, ns, d_status_t.p, d_status_ctrl.p, s);
+      DEM_CUDA(cudaMemcpyAsync(h_t, d_status_t.p, sizeof(long long) * ns, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(h_ctrl, d_status_ctrl.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaStreamSynchronize(s));
+      c_launches += k + 3 + (fp32 ? 1 : 0);
+      ++c_chunks;
+      long long ran_total = 0;
+      for (int j = 0; j < ns; ++j) {
+        DemSim& d = *sims[j];
+        const long long ran = h_t[j] - d.t;
+        if (ran < 0 || ran > k) { err = "specimen " + std::to_string(j) + ": step counter out of sequence"; return -3; }
+        d.t = h_t[j];
+        d.cur = (int)((d.cur + ran) & 1);
+        d.c_steps += ran;
+        d.c_contacts += ran * cps[j];
+        d.pending_ctrl = h_ctrl[j];
+        c_steps += ran;
+        c_contacts += ran * cps[j];
+        ran_total += ran;
+        if (h_ctrl[j] & CTRL_REBUILD) ++c_rebuild_calls;
+      }
+      if (profile) {
+        float ms = 0.f;
+        DEM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        prof_ms += ms;
+        prof_steps += k;
+      }
+      if (ran_total == 0) { err = "no specimen advanced in a chunk"; return -3; }
+    }
+    return 0;
+  }
+};
+
 }  // namespace dem
 
 using dem::DemSim;
@@ -1631,6 +1858,95 @@ int dem_window_rewind(dem_sim* h) {
   return guard(h, [&](DemSim& s) {
     s.window_rewind();
     return DEM_OK;
+  });
+}
+
+int dem_ensemble_create(dem_ensemble** out, dem_sim* const* sims, int n) {
+  if (!out) return DEM_ERR_ARG;
+  *out = nullptr;
+  try {
+    std::vector<DemSim*> v;
+    for (int k = 0; k < n; ++k) v.push_back(reinterpret_cast<DemSim*>(sims ? sims[k] : nullptr));
+    *out = reinterpret_cast<dem_ensemble*>(new dem::Ensemble(v.data(), n));
+    return DEM_OK;
+  } catch (const dem::CudaError&) {
+    return DEM_ERR_CUDA;
+  } catch (const std::invalid_argument&) {
+    return DEM_ERR_ARG;
+  } catch (const std::exception&) {
+    return DEM_ERR_INTERNAL;
+  }
+}
+
+int dem_ensemble_destroy(dem_ensemble* e) {
+  delete reinterpret_cast<dem::Ensemble*>(e);
+  return DEM_OK;
+}
+
+const char* dem_ensemble_last_error(dem_ensemble* e) {
+  return e ? reinterpret_cast<dem::Ensemble*>(e)->err.c_str() : "null ensemble";
+}
+
+}  // extern "C"
+
+namespace {
+template <class F>
+int eguard(dem_ensemble* h, F&& f) {
+  dem::Ensemble* e = reinterpret_cast<dem::Ensemble*>(h);
+  if (!e) return DEM_ERR_ARG;
+  try {
+    cudaGetLastError();
+    return f(*e);
+  } catch (const dem::CudaError& x) {
+    e->err = x.what();
+    return DEM_ERR_CUDA;
+  } catch (const std::invalid_argument& x) {
+    e->err = x.what();
+    return DEM_ERR_ARG;
+  } catch (const dem::StateError& x) {
+    e->err = x.what();
+    return DEM_ERR_STATE;
+  } catch (const std::exception& x) {
+    e->err = x.what();
+    return DEM_ERR_INTERNAL;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int dem_ensemble_step(dem_ensemble* h, int nsteps) {
+  return eguard(h, [&](dem::Ensemble& e) { return e.step(nsteps); });
+}
+
+int dem_ensemble_set_option(dem_ensemble* h, const char* key, double value) {
+  return eguard(h, [&](dem::Ensemble& e) {
+    const std::string k = key ? key : "";
+    if (k == "threads_per_particle") {
+      const int v = (int)value;
+      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8) throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8");
+      e.tpp = v;
+    } else if (k == "chunk") {
+      if (value < 1) throw std::invalid_argument("chunk must be >= 1");
+      e.chunk = (int)value;
+    } else if (k == "graph") {
+      e.use_graph = value != 0;
+    } else if (k == "profile") {
+      e.profile = value != 0;
+    } else {
+      throw std::invalid_argument("unknown ensemble option " + k);
+    }
+    return DEM_OK;
+  });
+}
+
+int dem_ensemble_get_counters(dem_ensemble* h, long long* out, int n) {
+  return eguard(h, [&](dem::Ensemble& e) {
+    if (!out) throw std::invalid_argument("null output");
+    const long long v[8] = {e.c_steps, e.c_contacts, e.c_launches, e.c_chunks, (long long)(e.prof_ms * 1e6),
+                            e.prof_steps, (long long)e.pick_tpp(), e.c_rebuild_calls};
+    for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
+    return std::min(n, 8);
   });
 }
 

@@ -268,3 +268,56 @@ extern "C" int lsm_pack_fit(unsigned long long seed, int n, const double* bmin, 
   }
   return placed;
 }
+
+// Pairs (i, j), i < j, whose gap |x_i - x_j| - r_i - r_j is at most max_gap (the rule of
+// Geometry/DistConnections.hpp), found through a cell grid of size 2 r_max + max_gap.  Writes
+// up to cap pairs in (i, j) order and returns the total count (call again with a larger cap
+// when it exceeds cap), or -1 on bad arguments.
+extern "C" long long lsm_dist_connections(int n, const double* pos, const double* rad, double max_gap,
+                                          long long cap, int* out_i, int* out_j) {
+  if (n < 0 || (n > 0 && (!pos || !rad)) || max_gap < 0 || cap < 0 || (cap > 0 && (!out_i || !out_j))) return -1;
+  if (n < 2) return 0;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, rmax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) { mn[k] = std::min(mn[k], pos[3 * i + k]); mx[k] = std::max(mx[k], pos[3 * i + k]); }
+    rmax = std::max(rmax, rad[i]);
+  }
+  const double cs = 2.0 * rmax + max_gap;
+  long long nc[3];
+  for (int k = 0; k < 3; ++k) nc[k] = std::max(1LL, (long long)std::floor((mx[k] - mn[k]) / cs) + 1);
+  std::vector<long long> key(n);
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) {
+    long long c[3];
+    for (int k = 0; k < 3; ++k) c[k] = std::min(nc[k] - 1, (long long)((pos[3 * i + k] - mn[k]) / cs));
+    key[i] = (c[0] * nc[1] + c[1]) * nc[2] + c[2];
+    order[i] = i;
+  }
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
+  std::vector<long long> skey(n);
+  for (int i = 0; i < n; ++i) skey[i] = key[order[i]];
+  std::vector<std::pair<int, int>> found;
+  for (int i = 0; i < n; ++i) {
+    const long long k0 = key[i];
+    const long long cx = k0 / (nc[1] * nc[2]), cy = (k0 / nc[2]) % nc[1], cz = k0 % nc[2];
+    for (long long dx = -1; dx <= 1; ++dx)
+      for (long long dy = -1; dy <= 1; ++dy)
+        for (long long dz = -1; dz <= 1; ++dz) {
+          const long long x = cx + dx, y = cy + dy, z = cz + dz;
+          if (x < 0 || y < 0 || z < 0 || x >= nc[0] || y >= nc[1] || z >= nc[2]) continue;
+          const long long kk = (x * nc[1] + y) * nc[2] + z;
+          auto lo = std::lower_bound(skey.begin(), skey.end(), kk);
+          for (auto it = lo; it != skey.end() && *it == kk; ++it) {
+            const int j = order[it - skey.begin()];
+            if (j <= i) continue;
+            const double d0 = pos[3 * i] - pos[3 * j], d1 = pos[3 * i + 1] - pos[3 * j + 1],
+                         d2 = pos[3 * i + 2] - pos[3 * j + 2];
+            if (std::sqrt(d0 * d0 + d1 * d1 + d2 * d2) - rad[i] - rad[j] <= max_gap) found.push_back({i, j});
+          }
+        }
+  }
+  std::sort(found.begin(), found.end());
+  const long long m = (long long)found.size();
+  for (long long k = 0; k < m && k < cap; ++k) { out_i[k] = found[k].first; out_j[k] = found[k].second; }
+  return m;
+}

@@ -60,6 +60,12 @@ SIGNATURES = {
     "dem_window_forward": (C.c_int, [_P, C.c_int, C.c_int, _D]),
     "dem_window_adjoint": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
     "dem_window_rewind": (C.c_int, [_P]),
+    "dem_ensemble_create": (C.c_int, [C.POINTER(_P), C.POINTER(_P), C.c_int]),
+    "dem_ensemble_destroy": (C.c_int, [_P]),
+    "dem_ensemble_last_error": (_S, [_P]),
+    "dem_ensemble_step": (C.c_int, [_P, C.c_int]),
+    "dem_ensemble_set_option": (C.c_int, [_P, _S, C.c_double]),
+    "dem_ensemble_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
 }
 
 _lib = None
@@ -348,3 +354,50 @@ class DemSim:
 
     def window_rewind(self):
         self._chk(self.lib.dem_window_rewind(self.h))
+
+
+class Ensemble:
+    """Many independent workers advanced together (dem_ensemble_*): one kernel launch per
+    timestep for all specimens, chunks replayed from a captured CUDA graph.  Each specimen
+    advances exactly as its own ``step`` would advance it.  Keeps references to the member
+    ``DemSim`` objects so that they outlive it."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        if not self.sims:
+            raise DemError("an ensemble needs at least one specimen")
+        self.lib = self.sims[0].lib
+        self.h = _P()
+        arr = (_P * len(self.sims))(*[x.h for x in self.sims])
+        rc = self.lib.dem_ensemble_create(C.byref(self.h), arr, len(self.sims))
+        if rc != 0:
+            raise DemError(f"dem_ensemble_create failed ({rc}): specimens must share particle type")
+
+    def _chk(self, rc):
+        if rc < 0:
+            raise DemError(self.lib.dem_ensemble_last_error(self.h).decode())
+        return rc
+
+    def step(self, n=1):
+        self._chk(self.lib.dem_ensemble_step(self.h, int(n)))
+
+    def set_option(self, key, value):
+        self._chk(self.lib.dem_ensemble_set_option(self.h, key.encode(), float(value)))
+
+    def counters(self):
+        out = (C.c_longlong * 8)()
+        self._chk(self.lib.dem_ensemble_get_counters(self.h, out, 8))
+        keys = ("specimen_steps", "contact_updates", "launches", "chunks", "step_kernel_ns", "profiled_steps",
+                "threads_per_particle", "rebuild_requests")
+        return dict(zip(keys, list(out)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dem_ensemble_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

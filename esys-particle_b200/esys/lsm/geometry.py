@@ -26,6 +26,9 @@ def _lib():
         lib.lsm_pack_rsi.restype = C.c_int
         lib.lsm_pack_fit.argtypes = [C.c_ulonglong, C.c_int, _D, _D, C.c_double, C.c_double, C.c_int, _D, _D]
         lib.lsm_pack_fit.restype = C.c_int
+        lib.lsm_dist_connections.argtypes = [C.c_int, _D, _D, C.c_double, C.c_longlong, C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int)]
+        lib.lsm_dist_connections.restype = C.c_longlong
         lib._geometry_bound = True
     return lib
 
@@ -59,40 +62,19 @@ def fit_pack(n, bmin, bmax, rmin=0.2, rmax=1.0, seed=0, max_failures=2000):
 
 def distance_connections(pos, rad, max_gap):
     """Pairs (i, j), i < j, whose gap |x_i - x_j| - r_i - r_j is at most max_gap
-    (Geometry/DistConnections.hpp), vectorised over a cell sort."""
-    pos = np.asarray(pos, np.float64)
-    rad = np.asarray(rad, np.float64)
+    (Geometry/DistConnections.hpp), sorted by (i, j); the library's cell-grid search."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    rad = np.ascontiguousarray(rad, np.float64)
     n = len(rad)
-    if n < 2:
-        return np.zeros(0, np.int64), np.zeros(0, np.int64)
-    cell = 2.0 * rad.max() + max_gap
-    key3 = np.floor((pos - pos.min(0)) / cell).astype(np.int64)
-    dims = key3.max(0) + 3
-    lin = lambda k: (k[:, 0] * dims[1] + k[:, 1]) * dims[2] + k[:, 2]
-    key3 = key3 + 1
-    keys = lin(key3)
-    order = np.argsort(keys, kind="stable")
-    sk = keys[order]
-    out_i, out_j = [], []
-    for dx in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            for dz in (-1, 0, 1):
-                nk = lin(key3 + np.array([dx, dy, dz]))
-                lo = np.searchsorted(sk, nk, "left")
-                hi = np.searchsorted(sk, nk, "right")
-                cnt = hi - lo
-                if cnt.sum() == 0:
-                    continue
-                src = np.repeat(np.arange(n), cnt)
-                off = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
-                dst = order[np.repeat(lo, cnt) + off]
-                keep = src < dst
-                src, dst = src[keep], dst[keep]
-                gap = np.linalg.norm(pos[src] - pos[dst], axis=1) - rad[src] - rad[dst]
-                ok = gap <= max_gap
-                out_i.append(src[ok])
-                out_j.append(dst[ok])
-    i = np.concatenate(out_i)
-    j = np.concatenate(out_j)
-    o = np.lexsort((j, i))
-    return i[o], j[o]
+    lib = _lib()
+    I = C.POINTER(C.c_int)
+    cap = 8 * n
+    while True:
+        a, b = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        m = lib.lsm_dist_connections(n, pos.ctypes.data_as(_D), rad.ctypes.data_as(_D), float(max_gap), cap,
+                                     a.ctypes.data_as(I), b.ctypes.data_as(I))
+        if m < 0:
+            raise ValueError("bad connection arguments")
+        if m <= cap:
+            return a[:m].astype(np.int64), b[:m].astype(np.int64)
+        cap = int(m)

@@ -23,6 +23,7 @@ extern "C" {
 #endif
 
 typedef struct dem_sim dem_sim;
+typedef struct dem_ensemble dem_ensemble;
 
 enum {
   DEM_OK = 0,
@@ -220,6 +221,29 @@ int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_pa
 /* Restores the state at the start of the last window (particles, friction histories, wall
  * planes, timestep), so that the window can be run again with other parameters. */
 int dem_window_rewind(dem_sim* h);
+
+/* ---- Batched ensemble --------------------------------------------------------------------
+ * No counterpart in the reference, where each specimen is its own MPI job.  An ensemble advances
+ * n independent workers (each a dem_sim set up as usual, all RotSphere or all NRotSphere, all in
+ * the same precision form) together: one kernel launch per timestep covers every specimen's
+ * particles, and chunks of launches are replayed from a captured CUDA graph.  Each specimen keeps
+ * its own rebuilds, interaction updates, bond failures, walls and timestep, so it advances
+ * exactly as dem_step would advance it alone.  The ensemble borrows the handles: destroy it
+ * before any of them, and do not call a member handle while an ensemble call runs. */
+int dem_ensemble_create(dem_ensemble** out, dem_sim* const* sims, int n);
+int dem_ensemble_destroy(dem_ensemble* e);
+const char* dem_ensemble_last_error(dem_ensemble* e);
+
+/* nsteps timesteps of every specimen (each runs its own runOneStep sequence). */
+int dem_ensemble_step(dem_ensemble* e, int nsteps);
+
+/* "threads_per_particle" (0 automatic, 1, 2, 4, 8), "chunk" (timesteps per graph replay),
+ * "graph" (1 replay captured graphs, 0 plain launches), "profile" (CUDA-event timing). */
+int dem_ensemble_set_option(dem_ensemble* e, const char* key, double value);
+
+/* out[0..7] = specimen-timesteps, contact updates, kernel launches, chunks, batched-step device ns,
+ * profiled timesteps, threads per particle in use, rebuild requests. */
+int dem_ensemble_get_counters(dem_ensemble* e, long long* out, int n);
 
 #ifdef __cplusplus
 }

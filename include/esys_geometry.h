@@ -26,6 +26,12 @@ int lsm_pack_rsi(unsigned long long seed, int n, const double* bmin, const doubl
 int lsm_pack_fit(unsigned long long seed, int n, const double* bmin, const double* bmax, double rmin, double rmax,
                  int max_failures, double* pos, double* rad);
 
+/* Pairs (i, j), i < j, with gap |x_i - x_j| - r_i - r_j <= max_gap (Geometry/DistConnections.hpp,
+ * the Python ConnectionFinder); writes up to cap pairs sorted by (i, j) and returns the total
+ * number found (call again with a larger cap if it exceeds cap), or -1 on bad arguments. */
+long long lsm_dist_connections(int n, const double* pos, const double* rad, double max_gap, long long cap, int* out_i,
+                               int* out_j);
+
 #ifdef __cplusplus
 }
 #endif
