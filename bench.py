@@ -262,6 +262,133 @@ def adjoint_leg(stream):
     }
 
 
+# ---- batched ensemble leg ------------------------------------------------------------------
+E_DT = 1e-5
+E_RHO = 2.2  # spheres per unit volume of the fitting packer (radii in [0.2, 1.0], 300 failures)
+
+
+def cylinder_specimen(k, seed=5):
+    """Specimen k: a bonded cylinder (height 4R) cut from a fitting-packer block, its particle
+    count log-uniform in [2,000, 40,000]; bond stiffness and strengths log-uniform."""
+    from esys.lsm import geometry as G
+
+    rng = np.random.default_rng(seed + k)
+    n_t = float(np.exp(rng.uniform(np.log(2000), np.log(40000))))
+    R = (n_t / (E_RHO * 4.0 * np.pi)) ** (1.0 / 3.0)
+    H = 4.0 * R
+    pos, rad = G.fit_pack(int(2 * n_t) + 100, (-R, 0, -R), (R, H, R), 0.2, 1.0, seed=seed * 1000 + k,
+                          max_failures=300)
+    keep = pos[:, 0] ** 2 + pos[:, 2] ** 2 <= R * R
+    pos, rad = pos[keep], rad[keep]
+    i1, i2 = G.distance_connections(pos, rad, 1e-3)
+    kn, ks = np.exp(rng.uniform(np.log(1e4), np.log(1e6), size=2))
+    sn, ss = np.exp(rng.uniform(np.log(0.1), np.log(2.0), size=2))
+    m = len(rad)
+    return dict(n=m, pos=pos, rad=rad, i1=i1, i2=i2, R=R, H=H, kn=kn, ks=ks, sn=sn, ss=ss,
+                vel=np.zeros((m, 3)), angvel=np.zeros((m, 3)))
+
+
+def cylinder_sim(make, sp, grid=2.2, skin=0.2):
+    """Per specimen as the bonded-block compression: RotBond (kt = kb = 1e3, torsion / bending
+    strengths = shear / normal), RotFriction for post-break contacts with the bond exclusion,
+    elastic platens closing by 1e-7 of the height per step (the bonded-block compression rate:
+    1e-4 x 200 / 1000 per step on a height of 200), light damping; at rest initially."""
+    R, H = sp["R"], sp["H"]
+    sim = make("RotSphere", grid, skin, (-R - 1, -1, -R - 1), (R + 1, H + 1, R + 1), (0, 0, 0), E_DT)
+    n = sp["n"]
+    sim.add_particles(np.arange(n, dtype=np.int32), sp["pos"], sp["rad"], (4.0 / 3.0) * PI_REF * sp["rad"] ** 3,
+                      tag=np.zeros(n, np.int32), vel=sp["vel"], angvel=sp["angvel"])
+    sim.add_connections(np.ones(len(sp["i1"]), np.int32), sp["i1"], sp["i2"])
+    sim.add_rot_bond_group("bonds", 1, sp["kn"], sp["ks"], 1e3, 1e3, sp["sn"], sp["ss"], sp["ss"], sp["sn"],
+                           True, True, 1.0)
+    sim.add_rot_friction_group("friction", sp["kn"], 0.6, 0.6, sp["ks"], E_DT, True, True)
+    sim.add_exclusion("bonds", "friction")
+    y0 = float((sp["pos"][:, 1] - sp["rad"]).min())
+    y1 = float((sp["pos"][:, 1] + sp["rad"]).max())
+    sim.add_wall("bottom", (0, y0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, y1, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e5)
+    sim.add_wall_group("top_w", "top", 1e5)
+    sim.add_damping(0, 0.01, 100)
+    sim.add_damping(1, 0.01, 100)
+    v = 0.5 * 1e-7 * H / E_DT
+    sim.set_wall_velocity("bottom", (0, v, 0))
+    sim.set_wall_velocity("top", (0, -v, 0))
+    return sim
+
+
+def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100):
+    """FP32-force batched ensemble (autotuned, graph-replayed) vs the plain FP64 GPU form
+    (each specimen stepped by itself)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from esys.lsm import _capi
+    from esys.lsm.autotune import autotune_ensemble
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(8) as ex:
+        specs = list(ex.map(cylinder_specimen, range(nspec)))
+    t_setup = time.perf_counter() - t0
+    make = lambda *a: _capi.DemSim(*a)
+    best, table = autotune_ensemble(lambda sp, g, sk: cylinder_sim(make, sp, g, sk), specs, 1.0,
+                                    skins=(0.1, 0.2, 0.35), cell_factors=(1.0,), tpps=(2, 4, 8), sample=24,
+                                    warmup=30, trial=80)
+    sims = [cylinder_sim(make, sp, best["grid_spacing"], best["verlet_dist"]) for sp in specs]
+    for s in sims:
+        s.set_option("precision", 32)
+    e = _capi.Ensemble(sims)
+    e.set_option("threads_per_particle", best["threads_per_particle"])
+    e.set_option("profile", 1)
+    e.step(100)  # warm-up: first searches, graph capture
+    c0 = e.counters()
+    t0 = time.perf_counter()
+    e.step(steps)
+    dt = time.perf_counter() - t0
+    c1 = e.counters()
+    value = (c1["contact_updates"] - c0["contact_updates"]) / dt
+    kern_ms = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / 1e6
+    # FP32 force error vs FP64 on the developed states of a few specimens
+    errs = []
+    for s in sims[:: max(1, nspec // 8)]:
+        s.set_option("precision", 64)
+        out = (C.c_double * 5)()
+        s._chk(s.lib.dem_precision_check(s.h, out))
+        errs.append(out[0])
+        s.set_option("precision", 32)
+    breaks = int(sum(len(s.breaks()[0]) for s in sims))
+    e.close()
+    for s in sims:
+        s.close()
+    # plain FP64 GPU form: a size-stratified sample of the specimens, each stepped alone
+    idx = np.argsort([sp["n"] for sp in specs])[np.linspace(0, nspec - 1, min(fp64_sample, nspec)).astype(int)]
+    c64 = 0
+    t64 = 0.0
+    for k in idx:
+        s = cylinder_sim(make, specs[k], 2.2, 0.2)
+        s.set_option("precision", 64)
+        s.step(20)
+        a = s.counters()
+        t0 = time.perf_counter()
+        s.step(fp64_steps)
+        t64 += time.perf_counter() - t0
+        c64 += s.counters()["contact_updates"] - a["contact_updates"]
+        s.close()
+    plain = c64 / t64
+    return {
+        "workload": f"{nspec} bonded cylinders (height 4R), particle counts log-uniform in [2,000, 40,000] "
+                    f"(total {sum(sp['n'] for sp in specs)}), radii in [0.2, 1.0] by the fitting packer, "
+                    f"kn, ks log-uniform [1e4, 1e6], strengths log-uniform [0.1, 2.0], RotFriction + exclusion, "
+                    f"platens closing, dt=1e-5",
+        "metric": "contact-updates/s", "value": value, "steps": steps, "seconds": dt,
+        "batched_kernel_share": kern_ms / (dt * 1e3), "dtype": "f32-forces/f64-integration",
+        "max_rel_force_err_vs_fp64": max(errs) if errs else None, "bond_breaks": breaks,
+        "autotuned": best, "autotune_trials": len(table), "setup_s": t_setup,
+        "plain_fp64_gpu": {"value": plain, "sample": f"{len(idx)} specimens (size-stratified) x {fp64_steps} steps "
+                                                      f"each, one dem_step per specimen"},
+        "speedup_vs_plain_fp64": value / plain,
+    }
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -300,6 +427,8 @@ def main():
                     help="32: FP32 pair forces + FP64 integration (headline); 64: FP64 throughout")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-window leg")
+    ap.add_argument("--ensemble-specimens", type=int, default=128, help="0 skips the batched-ensemble leg")
+    ap.add_argument("--ensemble-steps", type=int, default=400, help="timed timesteps of the ensemble leg")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
                     help="step kernels: -1 automatic, 0 fused, 1 pair kernel + integration kernel")
     args = ap.parse_args()
@@ -442,6 +571,9 @@ def main():
     adj = None
     if not args.no_adjoint:
         adj = adjoint_leg(stream)
+    ens = None
+    if args.ensemble_specimens > 0:
+        ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -482,6 +614,7 @@ def main():
             "gpu_launches": c1["launches"] - c0["launches"],
             "clocks": clk.summary(),
             "adjoint": adj,
+            "ensemble": ens,
         }
         print(json.dumps(line))
     sim.close()
