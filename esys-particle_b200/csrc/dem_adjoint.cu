@@ -228,6 +228,14 @@ __global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
   const unsigned long long key = G.keys[k];
   const int s1 = (int)(key >> 32), s2 = (int)(key & 0xffffffffu);
   double4* out = G.gpair + 6 * (size_t)k;
+  if (G.xbond) {  // a pair skipped by the step while its excluding bond holds
+    const int xb = G.xbond[k];
+    if (xb >= 0 && A.bond[xb >> 28].broken_step[xb & 0x0fffffff] > A.step) {
+      for (int c = 0; c < 6; ++c) out[c] = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (G.kind == 1) G.lH[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+      return;
+    }
+  }
   const double4 pa = A.s0.pr[s1], pb = A.s0.pr[s2];
   const V x1d = xyzv(pa), x2d = image_of(A.g, x1d, xyzv(pb));
   const V lF1 = xyzv(A.lF[s1]), lF2 = xyzv(A.lF[s2]);

@@ -77,7 +77,7 @@ __device__ __forceinline__ void batch_tile_epilogue(const StepArgs& a, long long
     }
     *a.step_counter = step;
     volatile int* ctrl = a.ctrl;
-    if (*ctrl) *a.stop = 1;
+    if (*ctrl & ~a.stop_skip) *a.stop = 1;
   }
 }
 

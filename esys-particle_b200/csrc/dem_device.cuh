@@ -86,6 +86,10 @@ struct DynDev {
   double4* hist_out;
   const float4* hist32_in;  // the same in the FP32 form
   float4* hist32_out;
+  // device bond hand-off only (else null): per pair, the bond that excluded it when the list
+  // was built, (bond group << 28) | bond index, or -1.  Such a pair is skipped while that
+  // bond is intact and becomes an ordinary pair at the step after the bond fails.
+  const int* xbond;
 };
 
 struct BondDev {
@@ -108,6 +112,7 @@ struct ExclDev {
   const unsigned long long* keys[kMaxBond];
   const int* broken_step[kMaxBond];
   int count[kMaxBond];
+  int group[kMaxBond];  // the bond group's index in StepArgs::bond
 };
 
 struct StepArgs {
@@ -130,6 +135,12 @@ struct StepArgs {
   double visc_lin, visc_rot, dt_lin, dt_rot;
   int iter_lin, iter_rot;
   int store_forces;
+  // device bond hand-off: a bond failure does not stop the chunk; the pairs it excluded turn
+  // into ordinary pairs (DynDev::xbond) and every particle refreshes its wall candidacy at the
+  // step after a failure (brk_step: last step with a failure)
+  int handoff;
+  int* brk_step;
+  int stop_skip;            // CTRL_* bits that do not stop the chunk (0: every raised bit stops it)
   // adjoint recompute pass only (null otherwise): the pair + bond + wall + body force
   // sums before damping, and the damping iterations (lin, rot) of every particle
   double4* f_int;

@@ -184,6 +184,36 @@ __global__ void k_pairs_write(Grid g, Particles P, int cur, const int* cell_star
   }
 }
 
+// Device bond hand-off: for every pair of a freshly built list, the bond that excludes it
+// (an intact bond of an excluding group, TSubLattice::setExIG), (group << 28) | index, or -1.
+__global__ void k_pairs_xbond(const unsigned long long* keys, int m, ExclDev ex, int* xbond) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const unsigned long long key = keys[k];
+  int r = -1;
+  for (int e = 0; e < ex.n && r < 0; ++e) {
+    const int p = lower_bound_key(ex.keys[e], 0, ex.count[e], key);
+    if (p < ex.count[e] && ex.keys[e][p] == key && ex.broken_step[e][p] == kBondAlive) r = (ex.group[e] << 28) | p;
+  }
+  xbond[k] = r;
+}
+void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex, int* xbond, cudaStream_t s) {
+  if (m > 0) k_pairs_xbond<<<(m + 255) / 256, 256, 0, s>>>(keys, m, ex, xbond);
+}
+
+// Wall candidates counted from the particles' flags; intact bonds counted from the break log.
+__global__ void k_count_candidates(int n, const unsigned* pflags, int* ncand) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned pf = pflags[i];
+  if (!(pf & PF_ALIVE)) return;
+  const int c = __popc((pf >> PF_WALL_SHIFT) & 0xffu);
+  if (c) atomicAdd(ncand, c);
+}
+void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s) {
+  if (n > 0) k_count_candidates<<<(n + 255) / 256, 256, 0, s>>>(n, pflags, ncand);
+}
+
 // ---------------------------------------------------------------------------
 // adjacency (both directions) from a key-sorted pair list
 // ---------------------------------------------------------------------------

@@ -41,6 +41,8 @@ void launch_set_state(const Particles& P, int cur, int cnt, const int* slots, co
 void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* ctrl, cudaStream_t s);
 void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, cudaStream_t s);
 void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s);
+void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex, int* xbond, cudaStream_t s);
+void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s);
 int step_grid(int n, int tpp);
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s);
 void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, bool split, cudaStream_t s);

@@ -80,8 +80,9 @@ struct DynGroup {
   DBuf<float4> hist32[2], hist32_spare;  // the same records in the FP32-force form
   DBuf<int> adj_start, adj_count, adj_cursor, p1_start;
   DBuf<int2> adj;
+  DBuf<int> xbond;  // device bond hand-off: excluding bond of each pair
   void release() {
-    keys.release(); keys_spare.release(); cand.release();
+    keys.release(); keys_spare.release(); cand.release(); xbond.release();
     hist[0].release(); hist[1].release(); hist_spare.release();
     hist32[0].release(); hist32[1].release(); hist32_spare.release();
     adj_start.release(); adj_count.release(); adj_cursor.release(); p1_start.release(); adj.release();
@@ -116,6 +117,8 @@ struct DemSim {
   int store_forces = 1;
   int fp32 = 0;          // 1 = FP32-force / FP64-integration form
   int split = -1;        // -1 automatic, 0 fused step kernel, 1 pair kernel + integration kernel
+  int handoff = 0;       // device bond hand-off (dem_set_option "bond_handoff")
+  DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
   // particles
   int n = 0, cap = 0;
   Particles P{};
@@ -351,10 +354,7 @@ struct DemSim {
   // |dF_i| / |F_i| over particles with |F_i| > 1e-9 max|F|, [4] particles compared.
   void precision_check(double* out) {
     if (fp32) throw std::invalid_argument("precision check runs from the FP64 form");
-    if (first) { search_neighbors(); first = false; }
-    if (pending_ctrl & CTRL_REBUILD) search_neighbors();
-    update_interactions((pending_ctrl & CTRL_BROKE) != 0);
-    pending_ctrl = 0;
+    if (!prepare()) throw StateError(err);
     if (!P.force_eval) {
       DEM_CUDA(cudaMalloc(&P.force_eval, sizeof(double4) * (size_t)cap));
       DEM_CUDA(cudaMalloc(&P.moment_eval, sizeof(double4) * (size_t)cap));
@@ -459,6 +459,7 @@ struct DemSim {
       ex.keys[ex.n] = it->second.keys.p;
       ex.broken_step[ex.n] = it->second.broken_step.p;
       ex.count[ex.n] = it->second.nb;
+      ex.group[ex.n] = (int)std::distance(bond.begin(), it);
       ex.n++;
     }
     return ex;
@@ -476,7 +477,9 @@ struct DemSim {
   // PIS_NE::update / PIS_ED::update after a rebuild: the full pair list with history carried
   // for persistent RotFriction interactions (pi_storage_ne.hpp:49-80, pi_storage_ed.hpp:84-129).
   void dyn_full_update(DynGroup& G) {
-    ExclDev ex = excl_of(G);
+    const ExclDev ex_bonds = excl_of(G);
+    // with the device hand-off the list keeps the bond-excluded pairs (marked in xbond)
+    const ExclDev ex = handoff ? ExclDev{} : ex_bonds;
     scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
     launch_pairs_count(g, P, cur, cell_start.p, cell_list.p, ex, scratch_i.p, s);
     scan_tmp.reserve(scan_tmp_ints(n + 2));
@@ -504,6 +507,10 @@ struct DemSim {
       }
     }
     G.m = m;
+    if (handoff) {
+      G.xbond.reserve(std::max(m, 1));
+      launch_pairs_xbond(G.keys.p, m, ex_bonds, G.xbond.p, s);
+    }
     build_adjacency(G.keys, m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
   }
 
@@ -602,6 +609,45 @@ struct DemSim {
     }
   }
 
+  // With the device hand-off a bond failure needs no host update: only the interaction
+  // counters (wall candidates, intact bonds) are brought up to date, in one read.
+  void refresh_counts() {
+    DEM_CUDA(cudaMemsetAsync(scalars.p + 2, 0, sizeof(int), s));
+    launch_count_candidates(n, P.pflags, scalars.p + 2, s);
+    int k = 3;
+    for (auto& b : bond) {
+      if (k >= 8) break;
+      DEM_CUDA(cudaMemcpyAsync(scalars.p + k, b.second.nevents.p, sizeof(int), cudaMemcpyDeviceToDevice, s));
+      ++k;
+    }
+    int host[8] = {0};
+    DEM_CUDA(cudaMemcpyAsync(host, scalars.p, sizeof(int) * k, cudaMemcpyDeviceToHost, s));
+    sync();
+    wall_cand = host[2];
+    k = 3;
+    for (auto& b : bond) {
+      if (k >= 8) break;
+      bond_alive[b.first] = b.second.nb - host[k++];
+    }
+    c_launches += 1;
+  }
+
+  void set_handoff(bool on) {
+    if (on == (handoff != 0)) return;
+    if (on)
+      for (auto& d : dyn)
+        if (d.second.kind != 1)
+          throw std::invalid_argument("the device bond hand-off needs every dynamic group to be RotFriction");
+    handoff = on;
+    if (!d_brk.p) {
+      d_brk.reserve(2);
+    }
+    DEM_CUDA(cudaMemsetAsync(d_brk.p, 0xff, sizeof(int) * 2, s));
+    launch_clear_flags(n, P.flagged, s);
+    // the dynamic lists are rebuilt in the new form before the next step
+    if (!first) pending_ctrl |= CTRL_REBUILD;
+  }
+
   // interactions evaluated per step: Verlet pairs + intact bonds + wall candidates
   long long contacts_per_step() const {
     long long c = wall_cand;
@@ -638,6 +684,7 @@ struct DemSim {
       D.adj_start = G.adj_start.p; D.adj = G.adj.p;
       D.hist_in = G.hist[c].p; D.hist_out = G.hist[c ^ 1].p;
       D.hist32_in = G.hist32[c].p; D.hist32_out = G.hist32[c ^ 1].p;
+      D.xbond = handoff ? G.xbond.p : nullptr;
     }
     a.nbond = 0;
     for (auto& b : bond) {
@@ -652,6 +699,9 @@ struct DemSim {
     a.visc_lin = visc_lin; a.visc_rot = visc_rot; a.dt_lin = dt; a.dt_rot = dt;
     a.iter_lin = iter_lin; a.iter_rot = iter_rot;
     a.store_forces = store_forces;
+    a.handoff = handoff;
+    a.brk_step = d_brk.p;
+    a.stop_skip = handoff ? CTRL_BROKE : 0;
     a.wall_partial = d_wall_partial.p;
     a.wall_force = d_wall_force.p;
     a.block_counter = d_block_counter.p;
@@ -679,7 +729,8 @@ struct DemSim {
   bool prepare() {
     if (first) { search_neighbors(); first = false; }
     if (pending_ctrl & CTRL_REBUILD) search_neighbors();
-    update_interactions((pending_ctrl & CTRL_BROKE) != 0);
+    if (handoff && (pending_ctrl & CTRL_BROKE) && timestamp == last_ns) refresh_counts();
+    else update_interactions((pending_ctrl & CTRL_BROKE) != 0);
     if (pending_ctrl & CTRL_OVERFLOW) { err = "bond-break event log overflowed"; return false; }
     pending_ctrl = 0;
     return true;
@@ -934,6 +985,7 @@ struct DemSim {
       D.scaling = G.scaling; D.meanR = G.meanR; D.m = win.m[d];
       D.keys = G.keys.p; D.adj_start = G.adj_start.p; D.adj = G.adj.p;
       D.lH = win.lH[d].p; D.gpair = win.gpair[d].p; D.gpar = win.gpar_d[d].p;
+      D.xbond = handoff ? G.xbond.p : nullptr;
     }
     A.nbond = nbg;
     for (int b = 0; b < nbg; ++b) {
@@ -1689,6 +1741,17 @@ int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* sta
     if (d != s.dyn.end()) {
       dem::DynGroup& G = d->second;
       std::vector<unsigned long long> keys(G.m);
+      std::vector<int> xb(s.handoff ? G.m : 0);
+      std::vector<std::vector<int>> bsteps;
+      if (s.handoff) {
+        if (G.m) DEM_CUDA(cudaMemcpyAsync(xb.data(), G.xbond.p, sizeof(int) * G.m, cudaMemcpyDeviceToHost, s.s));
+        for (auto& b : s.bond) {
+          bsteps.emplace_back(b.second.nb);
+          if (b.second.nb)
+            DEM_CUDA(cudaMemcpyAsync(bsteps.back().data(), b.second.broken_step.p, sizeof(int) * b.second.nb,
+                                     cudaMemcpyDeviceToHost, s.s));
+        }
+      }
       std::vector<double4> hist(G.kind == 1 ? G.m : 0);
       std::vector<float4> hist32(G.kind == 1 && s.fp32 ? G.m : 0);
       if (G.m) DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
@@ -1698,21 +1761,25 @@ int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* sta
       }
       s.sync();
       for (size_t q = 0; q < hist32.size(); ++q) hist[q] = make_double4(hist32[q].x, hist32[q].y, hist32[q].z, hist32[q].w);
+      int o = 0;
       for (int i = 0; i < G.m; ++i) {
-        id1[i] = s.h_id[(int)(keys[i] >> 32)];
-        id2[i] = s.h_id[(int)(keys[i] & 0xffffffffu)];
+        // device hand-off: a pair whose excluding bond still holds is not in the reference's list
+        if (s.handoff && xb[i] >= 0 && bsteps[xb[i] >> 28][xb[i] & 0x0fffffff] > s.t) continue;
+        id1[o] = s.h_id[(int)(keys[i] >> 32)];
+        id2[o] = s.h_id[(int)(keys[i] & 0xffffffffu)];
         if (state) {
-          for (int c = 0; c < 5; ++c) state[5 * i + c] = 0.0;
+          for (int c = 0; c < 5; ++c) state[5 * o + c] = 0.0;
           if (G.kind == 1) {
             const int fl = (int)hist[i].w;
             const bool touching = (fl & 2) != 0;
-            if (touching) { state[5 * i] = hist[i].x; state[5 * i + 1] = hist[i].y; state[5 * i + 2] = hist[i].z; }
-            state[5 * i + 3] = (fl & 1) ? 1.0 : 0.0;
-            state[5 * i + 4] = touching ? 1.0 : 0.0;
+            if (touching) { state[5 * o] = hist[i].x; state[5 * o + 1] = hist[i].y; state[5 * o + 2] = hist[i].z; }
+            state[5 * o + 3] = (fl & 1) ? 1.0 : 0.0;
+            state[5 * o + 4] = touching ? 1.0 : 0.0;
           }
         }
+        ++o;
       }
-      return G.m;
+      return o;
     }
     auto b = s.bond.find(group);
     if (b == s.bond.end()) throw std::invalid_argument("no such group");
@@ -1820,6 +1887,8 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.split = (int)value;
     } else if (k == "profile") {
       s.profile = value != 0;
+    } else if (k == "bond_handoff") {
+      s.set_handoff(value != 0);
     } else if (k == "precision") {
       if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");
       s.set_precision(value == 32);

@@ -105,6 +105,16 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           const int j = en[b].x;
           const bool isp1 = en[b].y < 0;
           const int k = en[b].y & 0x7fffffff;
+          if (G.xbond) {  // device bond hand-off: skipped while the bond that excluded it holds
+            const int xb = __ldg(G.xbond + k);
+            if (xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step) {
+              if (isp1 && !EVAL) {
+                if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+              }
+              continue;
+            }
+          }
           const double4 pj = pjs[b];
           // canonical orientation: p1 = lower id
           const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
@@ -230,6 +240,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                 atomicOr(a.ctrl, CTRL_OVERFLOW);
               }
               atomicOr(a.ctrl, CTRL_BROKE);
+              if (a.handoff) a.brk_step[step & 1] = (int)step;
             }
           } else {
             Fp += -1.0 * o.force;
@@ -272,6 +283,26 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
   }
   const V xi = xyz(p4);
   V F = mk(0.0, 0.0, 0.0), M = mk(0.0, 0.0, 0.0);
+
+  // 0. device bond hand-off: the step after a bond failure refreshes wall candidacy the way
+  //    CEWallInteractionGroup::Update does in that step's updateInteractions
+  //    (EWallInteractionGroup.hpp:57-82, NeighborTable::getParticlesAtPlane ntable.hpp:674-690)
+  if (a.handoff && alive) {
+    const long long step = *a.step_counter + 1;
+    if (a.brk_step[(step - 1) & 1] == (int)(step - 1)) {
+      pf &= ~(0xffffu << PF_WALL_SHIFT);
+      const bool inner = inner_of(a.g, p4.x, p4.y, p4.z);
+      for (int w = 0; w < a.nwall; ++w) {
+        const WallDev W = a.walls[w];
+        const double dist = dot(xi - mk(W.ox, W.oy, W.oz), mk(W.nx, W.ny, W.nz));
+        if (fabs(dist) < a.g.dim) {
+          pf |= 1u << (PF_WALL_SHIFT + w);
+          if (inner) pf |= 1u << (PF_INNER_SHIFT + w);
+        }
+      }
+      if (lane == 0 && !EVAL) a.P.pflags[i] = pf;
+    }
+  }
 
   // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
   //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.
@@ -424,7 +455,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a, int wlane, int 
     }
     *a.step_counter = step;
     volatile int* ctrl = a.ctrl;
-    if (*ctrl) *a.stop = 1;
+    if (*ctrl & ~a.stop_skip) *a.stop = 1;
   }
 }
 

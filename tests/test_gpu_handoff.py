@@ -1,0 +1,102 @@
+"""Device bond hand-off (dem_set_option "bond_handoff"): bond failures need no host update.
+
+The RotFriction list keeps the pairs that an intact bond excludes, skips them while the
+bond holds and treats them as ordinary pairs from the step after it fails; wall candidacy
+is refreshed on the device at that step.  The reference instead appends a "new list" of
+both-flagged pairs at that step (ntable.hpp:628-664, pi_storage_ed.hpp:130-155).  Bar:
+particle state, forces and bond-break events bit-identical to the host hand-off; the
+reported friction pairs are the host list's touching pairs, the host list only adding
+new-list pairs that never touched.  All tests need a GPU.
+"""
+import numpy as np
+import pytest
+
+import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu(dem_lib):
+    from esys.lsm import _capi
+
+    return lambda *a: _capi.DemSim(*a)
+
+
+def _pairs(sim):
+    a, b, st = sim.pairs("friction")
+    return {(int(x), int(y)): tuple(r) for x, y, r in zip(a, b, st)}
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_handoff_equals_host_handoff(gpu, precision):
+    host = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
+    dev = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
+    for s in (host, dev):
+        s.set_option("precision", precision)
+    dev.set_option("bond_handoff", 1)
+    S.run_loaded(host, 150, 0.002)
+    S.run_loaded(dev, 150, 0.002)
+    ph, pd = host.particles(), dev.particles()
+    for k in ("id", "pos", "vel", "angvel", "quat", "force", "moment"):
+        assert np.array_equal(ph[k], pd[k]), k
+    bh, bd = host.breaks(), dev.breaks()
+    assert len(bh[0]) > 0
+    for u, v in zip(bh, bd):
+        assert np.array_equal(u, v)
+    hp, dp = _pairs(host), _pairs(dev)
+    assert set(dp) <= set(hp)
+    for k in dp:
+        assert hp[k] == dp[k], k
+    for k in set(hp) - set(dp):  # new-list pairs that never came into contact
+        assert hp[k][4] == 0.0 and hp[k][0] == hp[k][1] == hp[k][2] == 0.0, k
+    assert np.array_equal(host.wall("top")[1], dev.wall("top")[1])
+
+
+def test_handoff_does_not_stop_chunks(gpu):
+    host = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
+    dev = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
+    dev.set_option("bond_handoff", 1)
+    for s in (host, dev):
+        s.set_wall_velocity("top", (0, -200.0, 0))
+        s.set_wall_velocity("bottom", (0, 200.0, 0))
+        s.step(120)
+    assert np.array_equal(host.particles()["pos"], dev.particles()["pos"])
+    assert len(host.breaks()[0]) > 0
+    assert dev.counters()["launches"] < host.counters()["launches"]
+
+
+def test_handoff_ensemble_equals_specimens_alone(gpu):
+    from esys.lsm import _capi
+
+    def specs():
+        out = [S.bonded_block(gpu, nx=5, ny=6 + k, nz=5, seed=50 + k, strength=(0.2 + 0.2 * k, 0.5, 0.5, 0.3))
+               for k in range(3)]
+        for s in out:
+            s.set_option("bond_handoff", 1)
+            s.set_option("threads_per_particle", 4)
+            s.set_wall_velocity("top", (0, -100.0, 0))
+            s.set_wall_velocity("bottom", (0, 100.0, 0))
+        return out
+
+    a, b = specs(), specs()
+    e = _capi.Ensemble(a)
+    e.set_option("threads_per_particle", 4)
+    e.step(150)
+    for s in b:
+        s.step(150)
+    for x, y in zip(a, b):
+        px, py = x.particles(), y.particles()
+        for k in ("pos", "vel", "angvel", "quat", "force", "moment"):
+            assert np.array_equal(px[k], py[k]), k
+        for u, v in zip(x.breaks(), y.breaks()):
+            assert np.array_equal(u, v)
+    e.close()
+
+
+def test_handoff_needs_friction_only_groups(gpu):
+    from esys.lsm._capi import DemError
+
+    g = S.gravity_box(gpu, n_side=4)
+    with pytest.raises(DemError, match="RotFriction"):
+        g.set_option("bond_handoff", 1)
