@@ -314,6 +314,7 @@ def cylinder_sim(make, sp, grid=2.2, skin=0.2):
     v = 0.5 * 1e-7 * H / E_DT
     sim.set_wall_velocity("bottom", (0, v, 0))
     sim.set_wall_velocity("top", (0, -v, 0))
+    sim.set_option("bond_handoff", 1)
     return sim
 
 

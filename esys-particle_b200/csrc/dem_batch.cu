@@ -5,8 +5,9 @@
 
 namespace dem {
 
-void launch_batch_step(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, int tpp, cudaStream_t s) {
-  launch_batch_any<false>(B, rot, el, fr, bd, tpp, s);
+void launch_batch_step(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, bool gather, int tpp,
+                       cudaStream_t s) {
+  launch_batch_any<false>(B, rot, el, fr, bd, gather, tpp, s);
 }
 
 // Clear every specimen's control and stop words before a chunk of steps.

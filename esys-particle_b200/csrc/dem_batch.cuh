@@ -128,6 +128,43 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 
   }
 }
 
+// Batched bond pass: tiles of kBondPassThreads bonds over (specimen, bond group) items; an
+// item without bonds has no tiles, so the last item whose first tile is <= tile owns it.
+template <bool FP32>
+__global__ void __launch_bounds__(kBondPassThreads) k_bond_pass_batch(const BatchArgs B) {
+  const int items = B.nspec * kMaxBond;
+  for (int tile = blockIdx.x; tile < B.total_btiles; tile += gridDim.x) {
+    int lo = 0, hi = items;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(B.btile_start + mid) <= tile) lo = mid; else hi = mid;
+    }
+    const int sp = lo / kMaxBond, d = lo % kMaxBond;
+    const StepArgs& a0 = B.args[2 * sp];
+    const long long done = *(volatile long long*)a0.step_counter;
+    if (*(volatile int*)a0.stop || done >= __ldg(B.target + sp)) continue;
+    const int cur = (int)((done - __ldg(B.base_t + sp) + __ldg(B.base_cur + sp)) & 1);
+    const StepArgs& a = B.args[2 * sp + cur];
+    const int k = (tile - __ldg(B.btile_start + lo)) * kBondPassThreads + threadIdx.x;
+    if (k < a.bond[d].nb_launch) bond_pass_one<false>(a, a.bond[d], k, done + 1);
+  }
+}
+
+template <bool FP32>
+inline void launch_bond_pass_batch(const BatchArgs& B, cudaStream_t s) {
+  if (B.total_btiles <= 0) return;
+  static int wave = 0;  // per translation unit: one instance each
+  if (!wave) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bond_pass_batch<FP32>, kBondPassThreads, 0);
+    wave = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+  }
+  const int grid = B.total_btiles < wave ? B.total_btiles : wave;
+  k_bond_pass_batch<FP32><<<grid, kBondPassThreads, 0, s>>>(B);
+}
+
 template <bool R, int T, int FEAT, bool FP32>
 inline void launch_batch_fixed(const BatchArgs& B, cudaStream_t s) {
   const int wave = one_wave(k_step_batch<R, T, FEAT, FP32>);
@@ -147,9 +184,15 @@ inline void launch_batch_tpp(const BatchArgs& B, int tpp, cudaStream_t s) {
 
 // Instances: non-rotational elastic; rotational friction, friction + bonds, and the general one.
 template <bool FP32>
-inline void launch_batch_any(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, int tpp, cudaStream_t s) {
+inline void launch_batch_any(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, bool gather, int tpp,
+                             cudaStream_t s) {
   if (!rot) return launch_batch_tpp<false, F_ELASTIC, FP32>(B, tpp, s);
   if (!bd && fr && !el) return launch_batch_tpp<true, F_FRIC, FP32>(B, tpp, s);
+  if (gather) {
+    launch_bond_pass_batch<FP32>(B, s);
+    if (!el) return launch_batch_tpp<true, F_FRIC | F_BGATHER, FP32>(B, tpp, s);
+    return launch_batch_tpp<true, F_ELASTIC | F_FRIC | F_BGATHER, FP32>(B, tpp, s);
+  }
   if (bd && !el) return launch_batch_tpp<true, F_FRIC | F_BOND, FP32>(B, tpp, s);
   return launch_batch_tpp<true, F_ELASTIC | F_FRIC | F_BOND, FP32>(B, tpp, s);
 }

@@ -5,8 +5,9 @@
 
 namespace dem {
 
-void launch_batch_step_fp32(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, int tpp, cudaStream_t s) {
-  launch_batch_any<true>(B, rot, el, fr, bd, tpp, s);
+void launch_batch_step_fp32(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, bool gather, int tpp,
+                       cudaStream_t s) {
+  launch_batch_any<true>(B, rot, el, fr, bd, gather, tpp, s);
 }
 
 }  // namespace dem

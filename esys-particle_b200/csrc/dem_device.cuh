@@ -32,6 +32,7 @@ constexpr int kMaxGrav = 4;
 constexpr int kMaxDyn = 2;
 constexpr int kMaxBond = 2;
 constexpr int kBondAlive = 0x7fffffff;
+constexpr int kBondPassThreads = 128;  // bonds per block of the bond pass
 
 struct Grid {
   double p0x, p0y, p0z;  // origin of the global grid (the grown bounding box minimum)
@@ -102,6 +103,9 @@ struct BondDev {
   int* events;              // (id1, id2, step) triples
   int* nevents;
   int cap_events;
+  double4* bf;              // bond pass (else null): per bond the force on p1, the moment on p1 and on p2
+  int nb_launch;            // bonds in the group (the bond pass's extent)
+  const int2* ends;         // (p1 slot, p2 slot) of each bond, p1 = lower id
 };
 
 // Intact bonds of the groups that exclude pairs from a dynamic group
@@ -165,6 +169,8 @@ struct BatchArgs {
   const long long* base_t;  // [nspec]: the specimen's step counter when the table was written
   const int* base_cur;      // [nspec]: its input buffer then
   const long long* target;  // [nspec]: last timestep to compute in this call
+  int total_btiles;         // bond pass: tiles of kBondPassThreads bonds over (specimen, bond group)
+  const int* btile_start;   // [nspec * kMaxBond + 1]
 };
 
 }  // namespace dem

@@ -679,16 +679,21 @@ void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t 
   bool el = false, fr = false;
   for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
   const bool bd = a.nbond > 0;
+  const bool gather = bd && a.bond[0].bf;  // bonds evaluated once by the bond pass
+  if (gather) launch_bond_pass<false, false>(a, s);
   if (split) {
     if (!rot) return launch_split_tpp<false, F_ELASTIC, false>(a, tpp, s);
     if (!bd && fr && !el) return launch_split_tpp<true, F_FRIC, false>(a, tpp, s);
     if (!bd && !fr) return launch_split_tpp<true, F_ELASTIC, false>(a, tpp, s);
+    if (gather) return launch_split_tpp<true, F_ELASTIC | F_FRIC | F_BGATHER, false>(a, tpp, s);
     if (bd && !el) return launch_split_tpp<true, F_FRIC | F_BOND, false>(a, tpp, s);
     return launch_split_tpp<true, F_ELASTIC | F_FRIC | F_BOND, false>(a, tpp, s);
   }
   if (!rot) return launch_step_tpp<false, F_ELASTIC, false, false>(a, tpp, s);
   if (!bd && fr && !el) return launch_step_tpp<true, F_FRIC, false, false>(a, tpp, s);
   if (!bd && !fr) return launch_step_tpp<true, F_ELASTIC, false, false>(a, tpp, s);
+  if (gather && !el) return launch_step_tpp<true, F_FRIC | F_BGATHER, false, false>(a, tpp, s);
+  if (gather) return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BGATHER, false, false>(a, tpp, s);
   if (bd && !el) return launch_step_tpp<true, F_FRIC | F_BOND, false, false>(a, tpp, s);
   return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_BOND, false, false>(a, tpp, s);
 }

@@ -99,8 +99,10 @@ struct BondGroup {
   DBuf<double4> D0;
   DBuf<int> broken_step, adj_start, adj_count, adj_cursor, p1_start, events, nevents;
   DBuf<int2> adj;
+  DBuf<double4> bf;  // bond pass results (3 records per bond)
   int cap_events = 0;
   void release() {
+    bf.release();
     keys.release(); ends.release(); D0.release(); broken_step.release(); adj_start.release(); adj_count.release();
     adj_cursor.release(); p1_start.release(); events.release(); nevents.release(); adj.release();
   }
@@ -118,6 +120,7 @@ struct DemSim {
   int fp32 = 0;          // 1 = FP32-force / FP64-integration form
   int split = -1;        // -1 automatic, 0 fused step kernel, 1 pair kernel + integration kernel
   int handoff = 0;       // device bond hand-off (dem_set_option "bond_handoff")
+  int bond_pass = 1;     // bonds evaluated once per step by their own pass, then gathered
   DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
   // particles
   int n = 0, cap = 0;
@@ -694,6 +697,12 @@ struct DemSim {
       D.truncated = B.truncated; D.scaling = B.scaling; D.meanR = B.meanR;
       D.adj_start = B.adj_start.p; D.adj = B.adj.p; D.D0 = B.D0.p; D.broken_step = B.broken_step.p;
       D.events = B.events.p; D.nevents = B.nevents.p; D.cap_events = B.cap_events;
+      D.nb_launch = B.nb;
+      D.ends = B.ends.p;
+      if (bond_pass) {
+        B.bf.reserve((size_t)3 * std::max(B.nb, 1));
+        D.bf = B.bf.p;
+      }
     }
     a.damp_lin = damp_lin; a.damp_rot = damp_rot;
     a.visc_lin = visc_lin; a.visc_rot = visc_rot; a.dt_lin = dt; a.dt_rot = dt;
@@ -1155,15 +1164,15 @@ struct Ensemble {
   cudaStream_t s = nullptr;
   int tpp = 0, chunk = 64, use_graph = 1, profile = 0;
   int rot = 0, fp32 = 0;
-  bool el = false, fr = false, bd = false;
+  bool el = false, fr = false, bd = false, gather = false;
   DBuf<StepArgs> d_args;
-  DBuf<int> d_tile_start, d_base_cur, d_status_ctrl;
+  DBuf<int> d_tile_start, d_btile_start, d_base_cur, d_status_ctrl;
   DBuf<long long> d_base_t, d_target, d_status_t;
   StepArgs* h_args = nullptr;   // pinned staging of the table
   long long* h_t = nullptr;     // pinned status
   int* h_ctrl = nullptr;
   std::map<int, cudaGraphExec_t> graphs;  // chunk length -> instantiated graph
-  int graph_tpp = -1, graph_tiles = -1;
+  int graph_tpp = -1, graph_tiles = -1, graph_gather = -1;
   long long c_steps = 0, c_contacts = 0, c_launches = 0, c_chunks = 0, c_rebuild_calls = 0;
   double prof_ms = 0.0;
   long long prof_steps = 0;
@@ -1184,6 +1193,7 @@ struct Ensemble {
     const int ns = (int)sims.size();
     d_args.reserve((size_t)2 * ns);
     d_tile_start.reserve(ns + 1);
+    d_btile_start.reserve((size_t)ns * kMaxBond + 1);
     d_base_cur.reserve(ns);
     d_base_t.reserve(ns);
     d_target.reserve(ns);
@@ -1196,7 +1206,7 @@ struct Ensemble {
   ~Ensemble() {
     if (s) cudaStreamSynchronize(s);
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
-    d_args.release(); d_tile_start.release(); d_base_cur.release(); d_status_ctrl.release();
+    d_args.release(); d_tile_start.release(); d_btile_start.release(); d_base_cur.release(); d_status_ctrl.release();
     d_base_t.release(); d_target.release(); d_status_t.release();
     if (h_args) cudaFreeHost(h_args);
     if (h_t) cudaFreeHost(h_t);
@@ -1238,21 +1248,22 @@ struct Ensemble {
 
   void launch_chunk(const BatchArgs& B, int k, int t_pp) {
     auto one = [&]() {
-      if (fp32) launch_batch_step_fp32(B, rot != 0, el, fr, bd, t_pp, s);
-      else launch_batch_step(B, rot != 0, el, fr, bd, t_pp, s);
+      if (fp32) launch_batch_step_fp32(B, rot != 0, el, fr, bd, gather, t_pp, s);
+      else launch_batch_step(B, rot != 0, el, fr, bd, gather, t_pp, s);
     };
     if (!use_graph) {
       for (int j = 0; j < k; ++j) one();
       DEM_CUDA(cudaGetLastError());
       return;
     }
-    if (graph_tpp != t_pp || graph_tiles != B.total_tiles) {
+    if (graph_tpp != t_pp || graph_tiles != B.total_tiles || graph_gather != (int)gather) {
       // a new launch shape runs once uncaptured first (it sets up the per-instance occupancy
       // query), then later chunks are captured and replayed
       for (auto& g : graphs) cudaGraphExecDestroy(g.second);
       graphs.clear();
       graph_tpp = t_pp;
       graph_tiles = B.total_tiles;
+      graph_gather = gather;
       for (int j = 0; j < k; ++j) one();
       DEM_CUDA(cudaGetLastError());
       return;
@@ -1292,7 +1303,9 @@ struct Ensemble {
       if (remaining <= 0) break;
       // every unfinished specimen's runOneStep head (its own rebuild / interaction update)
       el = fr = bd = false;
+      gather = true;
       std::vector<int> tile_start(ns + 1, 0);
+      std::vector<int> btile_start((size_t)ns * kMaxBond + 1, 0);
       std::vector<int> base_cur(ns);
       std::vector<long long> base_t(ns);
       std::vector<long long> cps(ns);
@@ -1302,7 +1315,19 @@ struct Ensemble {
           if (!d.prepare()) { err = "specimen " + std::to_string(k) + ": " + d.err; return DEM_ERR_OVERFLOW; }
         }
         for (auto& g : d.dyn) (g.second.kind == 0 ? el : fr) = true;
-        if (!d.bond.empty()) bd = true;
+        if (!d.bond.empty()) {
+          bd = true;
+          if (!d.bond_pass) gather = false;
+        }
+        {
+          int q = 0;
+          for (auto& b : d.bond) {
+            if (q >= kMaxBond) break;
+            const size_t it = (size_t)k * kMaxBond + q;
+            btile_start[it + 1] = (b.second.nb + kBondPassThreads - 1) / kBondPassThreads;
+            ++q;
+          }
+        }
         tile_start[k + 1] = tile_start[k] + step_grid(d.n, t_pp);
         d.d_wall_partial.reserve((size_t)step_grid(d.n, t_pp) * kMaxWalls * 3);
         h_args[2 * k] = d.make_args(0);
@@ -1312,6 +1337,10 @@ struct Ensemble {
         base_t[k] = d.t;
         cps[k] = d.contacts_per_step();
       }
+      gather = gather && bd;
+      for (size_t it = 0; it < (size_t)ns * kMaxBond; ++it) btile_start[it + 1] += btile_start[it];
+      DEM_CUDA(cudaMemcpyAsync(d_btile_start.p, btile_start.data(), sizeof(int) * btile_start.size(),
+                               cudaMemcpyHostToDevice, s));
       DEM_CUDA(cudaMemcpyAsync(d_args.p, h_args, sizeof(StepArgs) * 2 * ns, cudaMemcpyHostToDevice, s));
       DEM_CUDA(cudaMemcpyAsync(d_tile_start.p, tile_start.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, s));
       DEM_CUDA(cudaMemcpyAsync(d_base_cur.p, base_cur.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
@@ -1328,6 +1357,8 @@ struct Ensemble {
       B.base_t = d_base_t.p;
       B.base_cur = d_base_cur.p;
       B.target = d_target.p;
+      B.btile_start = d_btile_start.p;
+      B.total_btiles = btile_start[(size_t)ns * kMaxBond];
       if (profile) {
         if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
         DEM_CUDA(cudaEventRecord(ev0, s));
@@ -1889,6 +1920,8 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.profile = value != 0;
     } else if (k == "bond_handoff") {
       s.set_handoff(value != 0);
+    } else if (k == "bond_pass") {
+      s.bond_pass = value != 0;
     } else if (k == "precision") {
       if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");
       s.set_precision(value == 32);

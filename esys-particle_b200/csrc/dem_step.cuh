@@ -16,6 +16,9 @@
 //   EVAL  FP32 evaluation-only pass: forces of the current state into
 //         force_eval / moment_eval, nothing else written (precision check)
 #pragma once
+#include <map>
+#include <mutex>
+
 #include "dem_common.cuh"
 #include "dem_laws.cuh"
 #include "dem_laws_f32.cuh"
@@ -54,7 +57,9 @@ __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
 // Interaction families compiled into a k_step instance (the host picks the
 // smallest instance that covers the groups present, so a friction-only run
 // does not carry the registers of the bond law).
-enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4 };
+// F_BGATHER: bonds were evaluated by the bond pass (k_bond_pass, once per bond); the particle
+// gathers their forces and moments in its adjacency order instead of evaluating the law.
+enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8 };
 
 // Sum of the pair-group and bond contributions on particle i (all TPP lanes of
 // the particle call this; on return every lane holds the combined sums).  The
@@ -203,6 +208,27 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
   }
 
   // 4. bonded groups (PIS_EB::calcForces) + failure test (PIS_EB::update at the next step)
+  if constexpr (ROT && (FEAT & F_BGATHER) != 0) {
+    if (alive) {
+      for (int d = 0; d < a.nbond; ++d) {
+        const BondDev& B = a.bond[d];
+        const int e0 = __ldg(B.adj_start + i), e1 = __ldg(B.adj_start + i + 1);
+        for (int e = e0 + lane; e < e1; e += TPP) {
+          const int2 en = __ldg(B.adj + e);
+          const int k = en.y & 0x7fffffff;
+          if (B.broken_step[k] <= step) continue;  // removed by an earlier update
+          const double4* r = B.bf + 3 * (size_t)k;
+          if (en.y < 0) {
+            Fp += xyz(ldg4(r));
+            Mp += xyz(ldg4(r + 1));
+          } else {
+            Fp += -1.0 * xyz(ldg4(r));
+            Mp += xyz(ldg4(r + 2));
+          }
+        }
+      }
+    }
+  }
   if constexpr (ROT && (FEAT & F_BOND) != 0) {
     if (alive) {
       for (int d = 0; d < a.nbond; ++d) {
@@ -460,6 +486,54 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a, int wlane, int 
 }
 
 
+// Bond pass: bond k of group d evaluated once, in its canonical orientation, for the
+// particle pass to gather (F_BGATHER); the failure test and its records as the p1 side of
+// the in-line evaluation writes them.  The same law and operation order as in pair_sums,
+// so the gathered values equal what either side would compute.
+template <bool EVAL>
+__device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& B, int k, long long step) {
+  if (B.broken_step[k] <= step) return;
+  const ParticleBuf in = a.P.buf[a.cur];
+  const int2 e = __ldg(B.ends + k);
+  const double4 pa = ldg4(in.pr + e.x), pb = ldg4(in.pr + e.y);
+  const double4 qa = ldg4(in.qq + e.x), qb = ldg4(in.qq + e.y);
+  const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+  const double4 D0 = ldg4(B.D0 + k);
+  const V mD = xyz(D0);
+  const double dist0 = sqrt(dot(mD, mD));
+  const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
+  BondOut o;
+  law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
+  double4* r = B.bf + 3 * (size_t)k;
+  r[0] = d4(o.force, 0.0);
+  r[1] = d4(o.moment1, 0.0);
+  r[2] = d4(o.moment2, 0.0);
+  if (!EVAL && bond_broken(K, o, B.truncated)) {
+    const int i = e.x, j = e.y;
+    B.broken_step[k] = (int)(step + 1);
+    a.P.flagged[i] = 1;
+    a.P.flagged[j] = 1;
+    const int slot = atomicAdd(B.nevents, 1);
+    if (slot < B.cap_events) {
+      B.events[3 * slot] = a.P.id[i];
+      B.events[3 * slot + 1] = a.P.id[j];
+      B.events[3 * slot + 2] = (int)(step + 1);
+    } else {
+      atomicOr(a.ctrl, CTRL_OVERFLOW);
+    }
+    atomicOr(a.ctrl, CTRL_BROKE);
+    if (a.handoff) a.brk_step[step & 1] = (int)step;
+  }
+}
+
+template <bool EVAL, bool FP32>  // FP32: instance of the FP32-force form's translation unit
+__global__ void __launch_bounds__(kBondPassThreads) k_bond_pass(const StepArgs a, int d, int nb) {
+  if (!EVAL && *a.stop) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nb) return;
+  bond_pass_one<EVAL>(a, a.bond[d], k, *a.step_counter + 1);
+}
+
 // Fused step: pair sums and integration in one launch (small systems).
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
 __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 : 2)) k_step(const StepArgs a) {
@@ -562,18 +636,23 @@ inline int step_blocks(int n, int tpp) {
   return (int)((t + kStepThreads - 1) / kStepThreads);
 }
 
-// Blocks of one wave of kernel K on the current device (cached per instance).
+// Blocks of one wave of kernel K on the current device, cached per kernel (every
+// instance of k_step shares one function type, so the cache is keyed by address).
 template <class K>
 inline int one_wave(K kernel) {
-  static int cached = 0;
-  if (!cached) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStepThreads, 0);
-    cached = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
-  }
-  return cached;
+  static std::mutex mu;
+  static std::map<const void*, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const void* key = reinterpret_cast<const void*>(kernel);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStepThreads, 0);
+  const int v = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+  cache[key] = v;
+  return v;
 }
 
 template <bool R, int FEAT, bool FP32>
@@ -593,6 +672,15 @@ inline void launch_fused(const StepArgs& a, cudaStream_t s) {
   const int tiles = step_blocks(a.P.n, T);
   const int wave = one_wave(k_step<R, T, FEAT, FP32, EVAL>);
   k_step<R, T, FEAT, FP32, EVAL><<<tiles < wave ? tiles : wave, kStepThreads, 0, s>>>(a);
+}
+
+template <bool EVAL, bool FP32>
+inline void launch_bond_pass(const StepArgs& a, cudaStream_t s) {
+  for (int d = 0; d < a.nbond; ++d) {
+    const int nb = a.bond[d].nb_launch;
+    if (nb > 0)
+      k_bond_pass<EVAL, FP32><<<(nb + kBondPassThreads - 1) / kBondPassThreads, kBondPassThreads, 0, s>>>(a, d, nb);
+  }
 }
 
 template <bool R, int FEAT, bool FP32, bool EVAL>
