@@ -10,6 +10,8 @@ void launch_batch_step(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, 
   launch_batch_any<false>(B, rot, el, fr, bd, gather, tpp, s);
 }
 
+void launch_batch_bond_pass(const BatchArgs& B, cudaStream_t s) { launch_bond_pass_batch<false>(B, s); }
+
 // Clear every specimen's control and stop words before a chunk of steps.
 __global__ void k_batch_reset(const StepArgs* args, int nspec) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;

@@ -14,6 +14,7 @@
 // totals, wall loaders, its step counter and its stop word.  A specimen whose
 // stop word is set, or which has reached its target step, skips the launch.
 #pragma once
+#include "dem_kernels.h"
 #include "dem_step.cuh"
 
 namespace dem {
@@ -189,7 +190,7 @@ inline void launch_batch_any(const BatchArgs& B, bool rot, bool el, bool fr, boo
   if (!rot) return launch_batch_tpp<false, F_ELASTIC, FP32>(B, tpp, s);
   if (!bd && fr && !el) return launch_batch_tpp<true, F_FRIC, FP32>(B, tpp, s);
   if (gather) {
-    launch_bond_pass_batch<FP32>(B, s);
+    launch_batch_bond_pass(B, s);  // FP64, uncontracted (dem_batch.cu), for both precision forms
     if (!el) return launch_batch_tpp<true, F_FRIC | F_BGATHER, FP32>(B, tpp, s);
     return launch_batch_tpp<true, F_ELASTIC | F_FRIC | F_BGATHER, FP32>(B, tpp, s);
   }

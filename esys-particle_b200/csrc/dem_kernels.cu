@@ -675,6 +675,14 @@ void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const
 int step_grid(int n, int tpp) { return step_blocks(n, tpp); }
 
 // FP64 instances (this translation unit is built with --fmad=false).
+// The bond pass of both precision forms, built here without FMA contraction: the RotBond law's
+// acos of a cosine near 1 turns a last-bit difference into ~1e-8 rad, so a contracted build
+// would not reproduce the FP64 form's bond forces.
+void launch_bond_pass_f64(const StepArgs& a, bool eval, cudaStream_t s) {
+  if (eval) launch_bond_pass<true, false>(a, s);
+  else launch_bond_pass<false, false>(a, s);
+}
+
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s) {
   bool el = false, fr = false;
   for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;

@@ -45,12 +45,14 @@ void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex
 void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s);
 int step_grid(int n, int tpp);
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s);
+void launch_bond_pass_f64(const StepArgs& a, bool eval, cudaStream_t s);
 void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, bool split, cudaStream_t s);
 
 // batched ensemble (dem_batch.cu, dem_batch_fp32.cu)
 void launch_batch_step(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, bool gather, int tpp, cudaStream_t s);
 void launch_batch_step_fp32(const BatchArgs& B, bool rot, bool el, bool fr, bool bd, bool gather, int tpp,
                             cudaStream_t s);
+void launch_batch_bond_pass(const BatchArgs& B, cudaStream_t s);
 void launch_batch_reset(const StepArgs* args, int nspec, cudaStream_t s);
 void launch_batch_status(const StepArgs* args, int nspec, long long* t, int* ctrl, cudaStream_t s);
 void launch_batch_sync_vw(const StepArgs* args, const int* base_cur, int nspec, cudaStream_t s);

@@ -391,17 +391,23 @@ struct DemSim {
       dfmax = std::max(dfmax, dif(f[i], fe[i])); dmmax = std::max(dmmax, dif(m[i], me[i]));
     }
     std::vector<double> rel;
+    double gmax = 0.0, grel = 0.0;
     for (int i = 0; i < n; ++i) {
       if (!(pf[i] & PF_ALIVE)) continue;
       const double a = nrm(f[i]);
       if (a > 1e-9 * fmax) rel.push_back(dif(f[i], fe[i]) / a);
+      gmax = std::max(gmax, fe[i].w);
     }
+    for (int i = 0; i < n; ++i)
+      if ((pf[i] & PF_ALIVE) && fe[i].w > 1e-9 * gmax) grel = std::max(grel, dif(f[i], fe[i]) / fe[i].w);
     std::sort(rel.begin(), rel.end());
     out[0] = fmax > 0 ? dfmax / fmax : 0.0;
     out[1] = mmax > 0 ? dmmax / mmax : 0.0;
     out[2] = rel.empty() ? 0.0 : rel[rel.size() / 2];
     out[3] = rel.empty() ? 0.0 : rel[std::min(rel.size() - 1, (size_t)(0.99 * rel.size()))];
     out[4] = (double)rel.size();
+    out[5] = gmax > 0 ? dfmax / gmax : 0.0;  // relative to the largest contact-force sum
+    out[6] = grel;                           // worst particle, relative to its own contact-force sum
   }
 
   // Bulk state update of existing particles (rows = slots when id is NULL).
@@ -699,7 +705,7 @@ struct DemSim {
       D.events = B.events.p; D.nevents = B.nevents.p; D.cap_events = B.cap_events;
       D.nb_launch = B.nb;
       D.ends = B.ends.p;
-      if (bond_pass) {
+      if (bond_pass || fp32) {  // the FP32 form always takes its bonds from the FP64 bond pass
         B.bf.reserve((size_t)3 * std::max(B.nb, 1));
         D.bf = B.bf.p;
       }
@@ -1896,8 +1902,20 @@ int dem_set_particles(dem_sim* h, int n, const int* id, const double* pos, const
 int dem_precision_check(dem_sim* h, double* out) {
   return guard(h, [&](DemSim& s) {
     if (!out) throw std::invalid_argument("null output");
-    s.precision_check(out);
+    double v[7];
+    s.precision_check(v);
+    for (int k = 0; k < 5; ++k) out[k] = v[k];
     return DEM_OK;
+  });
+}
+
+int dem_precision_report(dem_sim* h, double* out, int n) {
+  return guard(h, [&](DemSim& s) {
+    if (!out || n < 0) throw std::invalid_argument("null output");
+    double v[7];
+    s.precision_check(v);
+    for (int k = 0; k < n && k < 7; ++k) out[k] = v[k];
+    return std::min(n, 7);
   });
 }
 

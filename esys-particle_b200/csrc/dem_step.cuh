@@ -67,9 +67,11 @@ enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8 };
 // butterfly combines the lanes.
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
 __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& in, int i, int lane, bool alive,
-                                          long long step, const double4& p4, const double4& q4, V& Fp, V& Mp) {
+                                          long long step, const double4& p4, const double4& q4, V& Fp, V& Mp,
+                                          double* gross = nullptr) {
   Fp = mk(0.0, 0.0, 0.0);
   Mp = mk(0.0, 0.0, 0.0);
+  double Gs = 0.0;  // evaluation pass: sum of the contributions' magnitudes (the particle's force scale)
   // 3. dynamic pair groups (PIS_NE / PIS_ED::calcForces).  Contact is tested first from the
   //    positions alone; the partner's velocity / spin and the pair's history are gathered only
   //    for touching pairs (a non-touching RotFriction pair just resets its history).  Adjacency
@@ -137,7 +139,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                 }
               } else {
                 Vf f;
-                if (law_elastic_f32(elastic_k(G.k, G.scaling, pa.w, pb.w), D, pa.w, pb.w, f)) Fk.add(isp1 ? -f : f);
+                if (law_elastic_f32(elastic_k(G.k, G.scaling, pa.w, pb.w), D, pa.w, pb.w, f)) {
+                  Fk.add(isp1 ? -f : f);
+                  if (EVAL) Gs += (double)norm(f);
+                }
               }
             }
           } else {
@@ -191,6 +196,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                   Fk.add(-o.fn);
                   Fk.add(o.Ffric);
                   Mk.add(o.M1);
+                  if (EVAL) Gs += (double)norm(o.fn) + (double)norm(o.Ffric);
                   if (!EVAL)
                     G.hist32_out[k] = make_float4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
                                                   (o.slipping ? 1.f : 0.f) + (o.touching ? 2.f : 0.f));
@@ -198,6 +204,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                   Fk.add(o.fn);
                   Fk.add(-o.Ffric);
                   Mk.add(o.M2);
+                  if (EVAL) Gs += (double)norm(o.fn) + (double)norm(o.Ffric);
                 }
               }
             }
@@ -225,6 +232,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
             Fp += -1.0 * xyz(ldg4(r));
             Mp += xyz(ldg4(r + 2));
           }
+          if (EVAL) Gs += norm(xyz(ldg4(r)));
         }
       }
     }
@@ -250,6 +258,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
           BondOut o;
           law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
+          if (EVAL) Gs += norm(o.force);
           if (isp1) {
             Fp += o.force;
             Mp += o.moment1;
@@ -286,12 +295,14 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
     }
     Fp = lane_sum<TPP>(Fp);
     Mp = lane_sum<TPP>(Mp);
+    if (EVAL) Gs = lane_sum<TPP>(Gs);
   }
   if (FP32) {
     // FP64-form sums (bonds) are added after the compensated FP32 pair sums
     Fp = Fk.value() + Fp;
     Mp = Mk.value() + Mp;
   }
+  if (EVAL && gross) *gross = Gs;
 }
 
 // Walls, body force, the pair sums, damping and the integration of particle i
@@ -570,9 +581,12 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 
     }
     const bool alive = valid && (pf & PF_ALIVE);
     V Fp, Mp;
-    pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp);
+    double gross = 0.0;
+    pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp, &gross);
     finish_particle<ROT, TPP, FP32, EVAL>(a, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
                                           ROT && (FEAT & F_BOND), Fp, Mp, s_red);
+    // evaluation pass: the particle's contact-force scale beside its force (w of the record)
+    if (EVAL && alive && lane == 0) reinterpret_cast<double*>(a.P.force_eval + i)[3] = gross;
   }
   if (EVAL) return;
   step_epilogue(a, wlane, warp, s_red, &s_last);

@@ -12,10 +12,7 @@ void launch_step_fp32(const StepArgs& a, bool rot, int tpp, bool eval, bool spli
   for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
   const bool bd = a.nbond > 0;
   const bool gather = bd && a.bond[0].bf;  // bonds evaluated once by the bond pass
-  if (gather) {
-    if (eval) launch_bond_pass<true, true>(a, s);
-    else launch_bond_pass<false, true>(a, s);
-  }
+  if (gather) launch_bond_pass_f64(a, eval, s);  // FP64, uncontracted: the FP64 form's bond forces
   if (split && !eval) {
     if (!rot) return launch_split_tpp<false, F_ELASTIC, true>(a, tpp, s);
     if (!bd && fr && !el) return launch_split_tpp<true, F_FRIC, true>(a, tpp, s);

@@ -54,6 +54,7 @@ SIGNATURES = {
     "dem_set_stream": (C.c_int, [_P, C.c_void_p]),
     "dem_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "dem_precision_check": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "dem_precision_report": (C.c_int, [_P, C.POINTER(C.c_double), C.c_int]),
     "dem_wall_reactions_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dem_set_group_param": (C.c_int, [_P, _S, _S, C.c_double]),
     "dem_window_num_params": (C.c_int, [_P]),
@@ -279,6 +280,15 @@ class DemSim:
     @property
     def timestep(self):
         return int(self.lib.dem_timestep(self.h))
+
+    def precision_report(self):
+        """FP32-force error vs FP64 on the current state (dem_precision_report); run from the
+        FP64 form."""
+        out = (C.c_double * 7)()
+        self._chk(self.lib.dem_precision_report(self.h, out, 7))
+        keys = ("max_rel_force_err", "max_rel_moment_err", "median_particle_rel_err", "p99_particle_rel_err",
+                "particles", "rel_to_force_scale", "worst_rel_to_own_scale")
+        return dict(zip(keys, list(out)))
 
     # ---- parameters and the differentiable loading window ----
     def set_group_param(self, group, key, value):

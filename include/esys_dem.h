@@ -164,6 +164,12 @@ int dem_get_counters(dem_sim* h, long long* out, int n);
  * |dF_i|/|F_i| over particles with |F_i| > 1e-9 max|F|, out[4] = particles compared. */
 int dem_precision_check(dem_sim* h, double* out);
 
+/* dem_precision_check with two more figures, out[0..n-1] (n <= 7): out[0..4] as above; out[5] =
+ * max |dF| / the largest per-particle contact-force sum (sum of |f| over the particle's pair and
+ * bond contributions: the system's force scale, which stays meaningful where net forces cancel);
+ * out[6] = max over particles of |dF| / that particle's own contact-force sum.  Returns the count. */
+int dem_precision_report(dem_sim* h, double* out, int n);
+
 /* Allocation-free per-wall reaction forces, for callers that cannot call cudaMalloc: code that
  * runs during CUDA graph capture, hosts that hand the library only memory from their own pool,
  * real-time loops that forbid allocation.  No counterpart in the reference.

@@ -72,3 +72,19 @@ def test_fp32_switch_midway_keeps_history(gpu):
     a.step(40)
     pa, pb = a.particles(), b.particles()
     assert np.abs(pa["vel"] - pb["vel"]).max() <= 1e-4 * np.abs(pa["vel"]).max()
+
+
+def test_fp32_bonded_block_force_error(gpu):
+    """Bonded, loaded, breaking block: the FP32 form takes its bond forces from the FP64
+    (uncontracted) bond pass, so only the RotFriction contacts carry FP32 rounding; the error
+    stays far under 1e-5 both against the largest force and per particle against its own
+    contact-force scale."""
+    s = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
+    s.set_option("precision", 32)
+    S.run_loaded(s, 120, 0.002)
+    assert len(s.breaks()[0]) > 0
+    s.set_option("precision", 64)
+    r = s.precision_report()
+    assert r["max_rel_force_err"] <= 1e-6, r
+    assert r["rel_to_force_scale"] <= 1e-6, r
+    assert r["worst_rel_to_own_scale"] <= 1e-5, r
