@@ -428,8 +428,8 @@ def main():
                     help="32: FP32 pair forces + FP64 integration (headline); 64: FP64 throughout")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-window leg")
-    ap.add_argument("--ensemble-specimens", type=int, default=128, help="0 skips the batched-ensemble leg")
-    ap.add_argument("--ensemble-steps", type=int, default=400, help="timed timesteps of the ensemble leg")
+    ap.add_argument("--ensemble-specimens", type=int, default=512, help="0 skips the batched-ensemble leg")
+    ap.add_argument("--ensemble-steps", type=int, default=1000, help="timed timesteps of the ensemble leg")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
                     help="step kernels: -1 automatic, 0 fused, 1 pair kernel + integration kernel")
     args = ap.parse_args()
