@@ -170,8 +170,20 @@ __global__ void k_adj_pre(const AdjArgs A) {
   A.gvisc[2 * i + 1] += gr;
 }
 
-using D18 = Dual<18>;
+// Tangent slot of input gi in the pass whose inputs are [base, base + N): a unit tangent there,
+// a constant elsewhere (the slot index is compared, never used as an array index, so the dual
+// stays in registers).
+template <int N>
+__device__ __forceinline__ Dual<N> seed_in(double v, int gi, int base) {
+  Dual<N> r(v);
+#pragma unroll
+  for (int s = 0; s < N; ++s) r.d[s] = (gi - base == s) ? 1.0 : 0.0;
+  return r;
+}
 
+// RotBond VJP by forward-mode duals, NT tangents per pass over the 18 inputs (x1, q1, x2, q2,
+// kr, ks, kt, kb): narrow duals keep the law's intermediates in registers.
+template <int NT>
 __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
   const AdjBond& B = A.bond[gi];
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,34 +196,45 @@ __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
   const int2 e = B.ends[b];
   const double4 p1 = A.s0.pr[e.x], p2 = A.s0.pr[e.y], qa = A.s0.qq[e.x], qb = A.s0.qq[e.y];
   const V x1d = xyzv(p1), x2d = image_of(A.g, x1d, xyzv(p2));
-  const V3<D18> x1 = mk(D18::seed(x1d.x, 0), D18::seed(x1d.y, 1), D18::seed(x1d.z, 2));
-  const Quat<D18> q1{D18::seed(qa.x, 3), mk(D18::seed(qa.y, 4), D18::seed(qa.z, 5), D18::seed(qa.w, 6))};
-  const V3<D18> x2 = mk(D18::seed(x2d.x, 7), D18::seed(x2d.y, 8), D18::seed(x2d.z, 9));
-  const Quat<D18> q2{D18::seed(qb.x, 10), mk(D18::seed(qb.y, 11), D18::seed(qb.z, 12), D18::seed(qb.w, 13))};
   const double4 D0 = B.D0[b];
-  const V3<D18> mD = mk(D18(D0.x), D18(D0.y), D18(D0.z));
   const double dist0 = sqrt(D0.x * D0.x + D0.y * D0.y + D0.z * D0.z);
-  const BondKT<D18> K = bond_k_t<D18>(D18::seed(B.kr, 14), D18::seed(B.ks, 15), D18::seed(B.kt, 16),
-                                      D18::seed(B.kb, 17), B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, p1.w,
-                                      p2.w);
-  BondOutT<D18> o;
-  law_bond_t<D18>(K, mD, x1, p1.w, q1, x2, p2.w, q2, o);
   // p1 gets +force and moment1, p2 gets -force and moment2
   const V lFd = xyzv(A.lF[e.x]) - xyzv(A.lF[e.y]);
   const V lM1 = xyzv(A.lM[e.x]), lM2 = xyzv(A.lM[e.y]);
-  const D18 w = o.force.x * lFd.x + o.force.y * lFd.y + o.force.z * lFd.z + o.moment1.x * lM1.x +
-                o.moment1.y * lM1.y + o.moment1.z * lM1.z + o.moment2.x * lM2.x + o.moment2.y * lM2.y +
-                o.moment2.z * lM2.z;
-  out[0] = make_double4(w.d[0], w.d[1], w.d[2], 0.0);
-  out[1] = make_double4(w.d[3], w.d[4], w.d[5], w.d[6]);
-  out[2] = make_double4(w.d[7], w.d[8], w.d[9], 0.0);
-  out[3] = make_double4(w.d[10], w.d[11], w.d[12], w.d[13]);
+  double g[18];
+#pragma unroll 1
+  for (int base = 0; base < 18; base += NT) {
+    using DN = Dual<NT>;
+    const V3<DN> x1 = mk(seed_in<NT>(x1d.x, 0, base), seed_in<NT>(x1d.y, 1, base), seed_in<NT>(x1d.z, 2, base));
+    const Quat<DN> q1{seed_in<NT>(qa.x, 3, base),
+                      mk(seed_in<NT>(qa.y, 4, base), seed_in<NT>(qa.z, 5, base), seed_in<NT>(qa.w, 6, base))};
+    const V3<DN> x2 = mk(seed_in<NT>(x2d.x, 7, base), seed_in<NT>(x2d.y, 8, base), seed_in<NT>(x2d.z, 9, base));
+    const Quat<DN> q2{seed_in<NT>(qb.x, 10, base),
+                      mk(seed_in<NT>(qb.y, 11, base), seed_in<NT>(qb.z, 12, base), seed_in<NT>(qb.w, 13, base))};
+    const V3<DN> mD = mk(DN(D0.x), DN(D0.y), DN(D0.z));
+    const BondKT<DN> K = bond_k_t<DN>(seed_in<NT>(B.kr, 14, base), seed_in<NT>(B.ks, 15, base),
+                                      seed_in<NT>(B.kt, 16, base), seed_in<NT>(B.kb, 17, base), B.mn, B.ms, B.mt,
+                                      B.mb, B.scaling, B.meanR, dist0, p1.w, p2.w);
+    BondOutT<DN> o;
+    law_bond_t<DN>(K, mD, x1, p1.w, q1, x2, p2.w, q2, o);
+    const DN w = o.force.x * lFd.x + o.force.y * lFd.y + o.force.z * lFd.z + o.moment1.x * lM1.x +
+                 o.moment1.y * lM1.y + o.moment1.z * lM1.z + o.moment2.x * lM2.x + o.moment2.y * lM2.y +
+                 o.moment2.z * lM2.z;
+#pragma unroll
+    for (int k = 0; k < NT; ++k)
+      if (base + k < 18) g[base + k] = w.d[k];
+  }
+  out[0] = make_double4(g[0], g[1], g[2], 0.0);
+  out[1] = make_double4(g[3], g[4], g[5], g[6]);
+  out[2] = make_double4(g[7], g[8], g[9], 0.0);
+  out[3] = make_double4(g[10], g[11], g[12], g[13]);
   double* gp = B.gpar + 4 * (size_t)b;
-  gp[0] += w.d[14];
-  gp[1] += w.d[15];
-  gp[2] += w.d[16];
-  gp[3] += w.d[17];
+  gp[0] += g[14];
+  gp[1] += g[15];
+  gp[2] += g[16];
+  gp[3] += g[17];
 }
+
 
 using D7 = Dual<7>;
 using D23 = Dual<23>;
@@ -361,7 +384,15 @@ void launch_adjoint_step(const AdjArgs& A, cudaStream_t s) {
   if (nb == 0) return;
   k_adj_pre<<<nb, 256, 0, s>>>(A);
   for (int d = 0; d < A.nbond; ++d)
-    if (A.bond[d].nb) k_adj_bond<<<(A.bond[d].nb + 127) / 128, 128, 0, s>>>(A, d);
+    if (A.bond[d].nb) {
+      const int g = (A.bond[d].nb + 127) / 128;
+      switch (A.bond_tangents) {  // tangents per dual pass (18 = one pass)
+        case 3: k_adj_bond<3><<<g, 128, 0, s>>>(A, d); break;
+        case 6: k_adj_bond<6><<<g, 128, 0, s>>>(A, d); break;
+        case 9: k_adj_bond<9><<<g, 128, 0, s>>>(A, d); break;
+        default: k_adj_bond<18><<<g, 128, 0, s>>>(A, d); break;
+      }
+    }
   for (int d = 0; d < A.ndyn; ++d)
     if (A.dyn[d].m) k_adj_pair<<<(A.dyn[d].m + 127) / 128, 128, 0, s>>>(A, d);
   if (A.nbond || A.ndyn) k_adj_post<<<nb, 256, 0, s>>>(A);

@@ -58,6 +58,7 @@ struct AdjArgs {
   AdjDyn dyn[kMaxDyn];
   int nbond;
   AdjBond bond[kMaxBond];
+  int bond_tangents;                  // dual tangents per pass of the RotBond VJP (3, 6, 9 or 18)
 };
 
 void launch_adjoint_step(const AdjArgs& A, cudaStream_t s);

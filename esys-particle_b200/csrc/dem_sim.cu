@@ -121,6 +121,7 @@ struct DemSim {
   int split = -1;        // -1 automatic, 0 fused step kernel, 1 pair kernel + integration kernel
   int handoff = 0;       // device bond hand-off (dem_set_option "bond_handoff")
   int bond_pass = 1;     // bonds evaluated once per step by their own pass, then gathered
+  int adj_tangents = 6;  // dual tangents per pass of the adjoint's RotBond VJP (6: fastest measured)
   DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
   // particles
   int n = 0, cap = 0;
@@ -989,6 +990,7 @@ struct DemSim {
     A.damp_lin = damp_lin; A.damp_rot = damp_rot; A.iter_lin = iter_lin; A.iter_rot = iter_rot;
     A.visc_lin = visc_lin; A.visc_rot = visc_rot; A.dt_lin = dt; A.dt_rot = dt;
     A.nwall = nw;
+    A.bond_tangents = adj_tangents;
     A.lx = lam; A.lv = lam + nn; A.lw = lam + 2 * (size_t)nn; A.lq = lam + 3 * (size_t)nn;
     A.lF = lam + 4 * (size_t)nn; A.lM = lam + 5 * (size_t)nn;
     A.gvisc = win.gvisc.p;
@@ -1940,6 +1942,10 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.set_handoff(value != 0);
     } else if (k == "bond_pass") {
       s.bond_pass = value != 0;
+    } else if (k == "adjoint_bond_tangents") {
+      const int v = (int)value;
+      if (v != 3 && v != 6 && v != 9 && v != 18) throw std::invalid_argument("adjoint_bond_tangents must be 3, 6, 9, 18");
+      s.adj_tangents = v;
     } else if (k == "precision") {
       if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");
       s.set_precision(value == 32);
