@@ -267,6 +267,11 @@ E_DT = 1e-5
 E_RHO = 2.2  # spheres per unit volume of the fitting packer (radii in [0.2, 1.0], 300 failures)
 
 
+def specimen_target_count(k, seed=5):
+    """The particle count specimen k aims at (its first seeded draw)."""
+    return float(np.exp(np.random.default_rng(seed + k).uniform(np.log(2000), np.log(40000))))
+
+
 def cylinder_specimen(k, seed=5):
     """Specimen k: a bonded cylinder (height 4R) cut from a fitting-packer block, its particle
     count log-uniform in [2,000, 40,000]; bond stiffness and strengths log-uniform."""
@@ -318,17 +323,24 @@ def cylinder_sim(make, sp, grid=2.2, skin=0.2):
     return sim
 
 
-def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100):
+def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None):
     """FP32-force batched ensemble (autotuned, graph-replayed) vs the plain FP64 GPU form
-    (each specimen stepped by itself)."""
+    (each specimen stepped by itself).  Under torchrun each rank takes a size-balanced share of
+    the specimens (no exchange while they run); counts are summed and times maxed at the end."""
     from concurrent.futures import ThreadPoolExecutor
+
+    import torch
 
     from esys.lsm import _capi
     from esys.lsm.autotune import autotune_ensemble
+    from esys.lsm.parallel import partition_specimens
 
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    mine = partition_specimens([specimen_target_count(k) for k in range(nspec)], world)[rank]
     t0 = time.perf_counter()
     with ThreadPoolExecutor(8) as ex:
-        specs = list(ex.map(cylinder_specimen, range(nspec)))
+        specs = list(ex.map(cylinder_specimen, mine))
     t_setup = time.perf_counter() - t0
     make = lambda *a: _capi.DemSim(*a)
     best, table = autotune_ensemble(lambda sp, g, sk: cylinder_sim(make, sp, g, sk), specs, 1.0,
@@ -341,12 +353,22 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100):
     e.set_option("threads_per_particle", best["threads_per_particle"])
     e.set_option("profile", 1)
     e.step(100)  # warm-up: first searches, graph capture
+    if dist is not None:
+        torch.cuda.synchronize()
+        dist.barrier()
     c0 = e.counters()
     t0 = time.perf_counter()
     e.step(steps)
     dt = time.perf_counter() - t0
     c1 = e.counters()
-    value = (c1["contact_updates"] - c0["contact_updates"]) / dt
+    contacts = float(c1["contact_updates"] - c0["contact_updates"])
+    if dist is not None:
+        tt = torch.tensor([dt, contacts], device="cuda", dtype=torch.float64)
+        t_max = tt[:1].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
+        dt, contacts = float(t_max.item()), float(tt[1].item())
+    value = contacts / dt
     kern_ms = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / 1e6
     # FP32 force error vs FP64 on the developed states of a few specimens
     errs = []
@@ -359,7 +381,8 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100):
     for s in sims:
         s.close()
     # plain FP64 GPU form: a size-stratified sample of the specimens, each stepped alone
-    idx = np.argsort([sp["n"] for sp in specs])[np.linspace(0, nspec - 1, min(fp64_sample, nspec)).astype(int)]
+    nloc = len(specs)
+    idx = np.argsort([sp["n"] for sp in specs])[np.linspace(0, nloc - 1, min(max(1, fp64_sample // world), nloc)).astype(int)]
     c64 = 0
     t64 = 0.0
     for k in idx:
@@ -372,10 +395,16 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100):
         t64 += time.perf_counter() - t0
         c64 += s.counters()["contact_updates"] - a["contact_updates"]
         s.close()
+    if dist is not None:  # every GPU runs its own sample: aggregate rate = sum of counts / max time
+        tt = torch.tensor([t64, float(c64)], device="cuda", dtype=torch.float64)
+        t_max = tt[:1].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
+        t64, c64 = float(t_max.item()), float(tt[1].item())
     plain = c64 / t64
     return {
         "workload": f"{nspec} bonded cylinders (height 4R), particle counts log-uniform in [2,000, 40,000] "
-                    f"(total {sum(sp['n'] for sp in specs)}), radii in [0.2, 1.0] by the fitting packer, "
+                    f"({sum(sp['n'] for sp in specs)} on rank 0 of {world}), radii in [0.2, 1.0] by the fitting packer, "
                     f"kn, ks log-uniform [1e4, 1e6], strengths log-uniform [0.1, 2.0], RotFriction + exclusion, "
                     f"platens closing, dt=1e-5",
         "metric": "contact-updates/s", "value": value, "steps": steps, "seconds": dt,
@@ -384,8 +413,10 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100):
         "force_error_sample": f"{len(errs)} specimens, FP32 forces vs FP64 on their developed states",
         "bond_breaks": breaks,
         "autotuned": best, "autotune_trials": len(table), "setup_s": t_setup,
-        "plain_fp64_gpu": {"value": plain, "sample": f"{len(idx)} specimens (size-stratified) x {fp64_steps} steps "
-                                                      f"each, one dem_step per specimen"},
+        "plain_fp64_gpu": {"value": plain, "sample": f"{len(idx)} specimens per GPU (size-stratified) x "
+                                                      f"{fp64_steps} steps each, one dem_step per specimen"},
+        "scaling": "weak over specimens: each GPU advances its size-balanced share, no exchange" if world > 1
+                   else "single GPU",
         "speedup_vs_plain_fp64": value / plain,
     }
 
@@ -571,7 +602,7 @@ def main():
         adj = adjoint_leg(stream)
     ens = None
     if args.ensemble_specimens > 0:
-        ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps)
+        ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps, dist=dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
