@@ -83,7 +83,8 @@ __device__ __forceinline__ void batch_tile_epilogue(const StepArgs& a, long long
 }
 
 template <bool ROT, int TPP, int FEAT, bool FP32>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 : 2)) k_step_batch(const BatchArgs B) {
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? 3 : 2)))
+    k_step_batch(const BatchArgs B) {
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;
   const int lane = threadIdx.x % TPP;
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 
 // Batched bond pass: tiles of kBondPassThreads bonds over (specimen, bond group) items; an
 // item without bonds has no tiles, so the last item whose first tile is <= tile owns it.
 template <bool FP32>
-__global__ void __launch_bounds__(kBondPassThreads) k_bond_pass_batch(const BatchArgs B) {
+__global__ void __launch_bounds__(kBondPassThreads, 4) k_bond_pass_batch(const BatchArgs B) {
   const int items = B.nspec * kMaxBond;
   for (int tile = blockIdx.x; tile < B.total_btiles; tile += gridDim.x) {
     int lo = 0, hi = items;

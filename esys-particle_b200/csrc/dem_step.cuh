@@ -538,7 +538,7 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
 }
 
 template <bool EVAL, bool FP32>  // FP32: instance of the FP32-force form's translation unit
-__global__ void __launch_bounds__(kBondPassThreads) k_bond_pass(const StepArgs a, int d, int nb) {
+__global__ void __launch_bounds__(kBondPassThreads, 4) k_bond_pass(const StepArgs a, int d, int nb) {
   if (!EVAL && *a.stop) return;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nb) return;
@@ -547,7 +547,8 @@ __global__ void __launch_bounds__(kBondPassThreads) k_bond_pass(const StepArgs a
 
 // Fused step: pair sums and integration in one launch (small systems).
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : (FP32 ? 3 : 2)) k_step(const StepArgs a) {
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? 3 : 2)))
+    k_step(const StepArgs a) {
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;
   if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
