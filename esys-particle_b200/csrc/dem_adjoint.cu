@@ -32,6 +32,7 @@
 #include "dem_adjoint.h"
 #include "dem_common.cuh"
 #include "dem_dual.cuh"
+#include "dem_bond_vjp.cuh"
 #include "dem_laws.cuh"
 
 namespace dem {
@@ -236,6 +237,40 @@ __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
 }
 
 
+// RotBond VJP by the hand-written reverse of the law (dem_bond_vjp.cuh).
+__global__ void __launch_bounds__(128) k_adj_bond_rev(const AdjArgs A, int gi) {
+  const AdjBond& B = A.bond[gi];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B.nb) return;
+  double4* out = B.gb + 4 * (size_t)b;
+  if (B.broken_step[b] <= A.step) {  // removed before this step
+    out[0] = out[1] = out[2] = out[3] = make_double4(0.0, 0.0, 0.0, 0.0);
+    return;
+  }
+  const int2 e = B.ends[b];
+  const double4 p1 = A.s0.pr[e.x], p2 = A.s0.pr[e.y], qa = A.s0.qq[e.x], qb = A.s0.qq[e.y];
+  const V x1 = xyzv(p1), x2 = image_of(A.g, x1, xyzv(p2));
+  const double4 D0 = B.D0[b];
+  const V mD = xyzv(D0);
+  const double dist0 = sqrt(D0.x * D0.x + D0.y * D0.y + D0.z * D0.z);
+  const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, p1.w, p2.w);
+  const BondK U = bond_k(1.0, 1.0, 1.0, 1.0, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, p1.w, p2.w);
+  const V lFd = xyzv(A.lF[e.x]) - xyzv(A.lF[e.y]);
+  const V lM1 = xyzv(A.lM[e.x]), lM2 = xyzv(A.lM[e.y]);
+  BondVjp g;
+  law_bond_vjp(K, mD, x1, p1.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, p2.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, lFd, lM1,
+               lM2, g);
+  out[0] = make_double4(g.x1.x, g.x1.y, g.x1.z, 0.0);
+  out[1] = make_double4(g.q1.s, g.q1.v.x, g.q1.v.y, g.q1.v.z);
+  out[2] = make_double4(g.x2.x, g.x2.y, g.x2.z, 0.0);
+  out[3] = make_double4(g.q2.s, g.q2.v.x, g.q2.v.y, g.q2.v.z);
+  double* gp = B.gpar + 4 * (size_t)b;  // the scaled stiffness is the group's times a constant factor
+  gp[0] += g.kr * U.kr;
+  gp[1] += g.ks * U.ks;
+  gp[2] += g.kt * U.kt;
+  gp[3] += g.kb * U.kb;
+}
+
 using D7 = Dual<7>;
 using D23 = Dual<23>;
 
@@ -386,7 +421,8 @@ void launch_adjoint_step(const AdjArgs& A, cudaStream_t s) {
   for (int d = 0; d < A.nbond; ++d)
     if (A.bond[d].nb) {
       const int g = (A.bond[d].nb + 127) / 128;
-      switch (A.bond_tangents) {  // tangents per dual pass (18 = one pass)
+      switch (A.bond_tangents) {  // 0: hand-written reverse; else tangents per dual pass (18 = one pass)
+        case 0: k_adj_bond_rev<<<g, 128, 0, s>>>(A, d); break;
         case 3: k_adj_bond<3><<<g, 128, 0, s>>>(A, d); break;
         case 6: k_adj_bond<6><<<g, 128, 0, s>>>(A, d); break;
         case 9: k_adj_bond<9><<<g, 128, 0, s>>>(A, d); break;

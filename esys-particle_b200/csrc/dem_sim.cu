@@ -121,7 +121,7 @@ struct DemSim {
   int split = -1;        // -1 automatic, 0 fused step kernel, 1 pair kernel + integration kernel
   int handoff = 0;       // device bond hand-off (dem_set_option "bond_handoff")
   int bond_pass = 1;     // bonds evaluated once per step by their own pass, then gathered
-  int adj_tangents = 6;  // dual tangents per pass of the adjoint's RotBond VJP (6: fastest measured)
+  int adj_tangents = 0;  // adjoint RotBond VJP: 0 hand-written reverse, else dual tangents per pass
   DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
   // particles
   int n = 0, cap = 0;
@@ -1944,7 +1944,8 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.bond_pass = value != 0;
     } else if (k == "adjoint_bond_tangents") {
       const int v = (int)value;
-      if (v != 3 && v != 6 && v != 9 && v != 18) throw std::invalid_argument("adjoint_bond_tangents must be 3, 6, 9, 18");
+      if (v != 0 && v != 3 && v != 6 && v != 9 && v != 18)
+        throw std::invalid_argument("adjoint_bond_tangents must be 0 (hand-written reverse), 3, 6, 9 or 18");
       s.adj_tangents = v;
     } else if (k == "precision") {
       if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");

@@ -168,8 +168,10 @@ def test_torch_window_function(gpu):
     Rb = b.window_forward(60, 16)
     assert np.array_equal(Rb, R.detach().numpy())
     gb = b.window_adjoint(S.mse_grad(Rb, tgt.numpy()))
-    assert np.allclose(theta.grad.numpy(), gb["params"], rtol=1e-12, atol=0)
-    assert np.allclose(v0.grad.numpy(), gb["vel"], rtol=1e-12, atol=1e-300)
+    # torch forms dLoss/dR by its own mean backward: equal to the last bits, so compare to 1e-10
+    # of each output's scale
+    assert np.abs(theta.grad.numpy() - gb["params"]).max() <= 1e-10 * np.abs(gb["params"]).max()
+    assert np.abs(v0.grad.numpy() - gb["vel"]).max() <= 1e-10 * np.abs(gb["vel"]).max()
     # a second call rewinds to the window start: same reactions for the same inputs
     R2 = win(theta.detach(), v0.detach(), w0)
     assert torch.equal(R2, R.detach())
@@ -225,3 +227,18 @@ def test_elastic_nonrotational_window_matches_dual_numbers(gpu, orc):
     layout = a.param_layout()
     idx = [layout.index(("elastic", "normalK")), layout.index(("Damping", "viscosity"))]
     _grad_vs(g["params"][idx], gd, 1e-6)
+
+
+def test_hand_written_bond_reverse_matches_dual_numbers(gpu):
+    """The RotBond VJP in the reverse sweep (hand-written reverse of the law, the default)
+    against the same VJP by forward-mode duals (6 tangents per pass)."""
+    out = {}
+    for nt in (0, 6):
+        a = S.window_block(gpu)
+        a.set_option("adjoint_bond_tangents", nt)
+        R = a.window_forward(T, 32)
+        tgt = S.mse_target(R)
+        out[nt] = a.window_adjoint(S.mse_grad(R, tgt))
+    for k in ("params", "vel", "angvel", "pos", "quat"):
+        scale = np.abs(out[6][k]).max()
+        assert np.abs(out[0][k] - out[6][k]).max() <= 1e-9 * scale, k
