@@ -707,3 +707,131 @@ void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t 
 }
 
 }  // namespace dem
+
+namespace dem {
+
+// ---------------------------------------------------------------------------
+// Field savers: per-particle and per-interaction scalar fields, computed on the
+// device (operation order of the reference's accessors, this unit being built
+// without FMA contraction).  Dead slots get NaN and are skipped by the host.
+// ---------------------------------------------------------------------------
+// CParticle::getKineticEnergy etc. (Model/Particle.h:116,134; Model/RotParticle.h:198-200)
+__global__ void k_particle_field(Particles P, int cur, int rot, int field, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  if (!(P.pflags[i] & PF_ALIVE)) { out[i] = __longlong_as_double(0x7ff8000000000000LL); return; }
+  const double4 p = P.buf[cur].pr[i], vm = P.buf[cur].vm[i];
+  const V v = xyz(vm);
+  double r = 0.0;
+  switch (field) {
+    case 0: {  // e_kin
+      if (rot) {
+        const double4 wi = P.buf[cur].wi[i];
+        const V w = xyz(wi);
+        r = (0.5 * vm.w) * dot(v, v) + dot((0.5 * wi.w) * w, w);
+      } else {
+        r = dot((0.5 * vm.w) * v, v);
+      }
+      break;
+    }
+    case 1: r = rot ? (0.5 * vm.w) * dot(v, v) : dot((0.5 * vm.w) * v, v); break;  // e_kin_linear
+    case 2: { const double4 wi = P.buf[cur].wi[i]; const V w = xyz(wi); r = rot ? dot((0.5 * wi.w) * w, w) : 0.0; break; }
+    case 3: r = norm(v); break;                                                     // v_abs
+    case 4: r = p.w; break;                                                         // radius
+    case 5: r = (double)P.id[i]; break;                                             // id
+    default: r = (double)P.tag[i]; break;                                           // tag
+  }
+  out[i] = r;
+}
+void launch_particle_field(const Particles& P, int cur, int rot, int field, double* out, cudaStream_t s) {
+  if (P.n) k_particle_field<<<nblk(P.n, 256), 256, 0, s>>>(P, cur, rot, field, out);
+}
+
+// Pair fields of a dynamic group from the state its last force evaluation read (buffer `prev`)
+// and the history it wrote: field 0 count, 1 potential_energy, 2 slipping, 3 sticking
+// (CElasticInteraction, Model/ElasticInteraction.cpp:76-96; CRotFrictionInteraction,
+// Model/RotFricInteraction.cpp:384-452).
+template <class H>
+__global__ void k_pair_field(Grid g, Particles P, int prev, const unsigned long long* keys, int m, int kind,
+                             double k, double ks, int scaling, int meanR, const H* hist, int field, double* out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  const int s1 = (int)(keys[q] >> 32), s2 = (int)(keys[q] & 0xffffffffu);
+  const double4 pa = P.buf[prev].pr[s1], pb = P.buf[prev].pr[s2];
+  const V x1 = xyz(pa), x2 = image_of(g, x1, xyz(pb));
+  const V D = x1 - x2;
+  const double d2 = dot(D, D), eq = pa.w + pb.w;
+  double r = 0.0;
+  if (kind == 0) {
+    const bool touching = d2 < eq * eq;
+    if (field == 0) r = touching ? 1.0 : 0.0;
+    else if (field == 1 && touching) {
+      const double ke = elastic_k(k, scaling, pa.w, pb.w);
+      const double dist = sqrt(d2);
+      const V F = D * (ke * (dist - eq) / dist);
+      r = dot(0.5 * F, F) / ke;
+    }
+  } else {
+    const H h = hist[q];
+    const int fl = (int)h.w;
+    const bool touching = (fl & 2) != 0, slipping = (fl & 1) != 0;
+    if (field == 0) r = touching ? 1.0 : 0.0;
+    else if (field == 2) r = slipping ? 1.0 : 0.0;
+    else if (field == 3) r = (touching && !slipping) ? 1.0 : 0.0;
+    else if (field == 1 && touching) {
+      double ke, kse;
+      friction_k(k, ks, scaling, meanR, pa.w, pb.w, ke, kse);
+      const double dist = sqrt(d2);
+      const V Fn = D * (ke * (dist - eq) / dist);
+      const V Ff = mk((double)h.x, (double)h.y, (double)h.z);
+      r = dot(0.5 * Fn, Fn) / ke + dot(0.5 * Ff, Ff) / kse;
+    }
+  }
+  out[q] = r;
+}
+void launch_pair_field(const Grid& g, const Particles& P, int prev, const unsigned long long* keys, int m, int kind,
+                       double k, double ks, int scaling, int meanR, const double4* hist, const float4* hist32,
+                       int field, double* out, cudaStream_t s) {
+  if (m <= 0) return;
+  if (hist32) k_pair_field<float4><<<nblk(m, 256), 256, 0, s>>>(g, P, prev, keys, m, kind, k, ks, scaling, meanR, hist32, field, out);
+  else k_pair_field<double4><<<nblk(m, 256), 256, 0, s>>>(g, P, prev, keys, m, kind, k, ks, scaling, meanR, hist, field, out);
+}
+
+// Bond fields from the state the last force evaluation read: 0 count, 1 potential_energy,
+// 2 e_pot_normal, 3 e_pot_shear, 4 e_pot_twist, 5 e_pot_bend, 6 breaking_criterion
+// (ARotBondedInteraction.cpp:456-485, CRotBondedInteraction::getCriterion :221-227).  NaN for
+// bonds removed before that evaluation.
+__global__ void k_bond_field(Grid g, Particles P, int prev, long long t, BondDev B, int nb, int field, double* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nb) return;
+  if (B.broken_step[k] <= t) { out[k] = __longlong_as_double(0x7ff8000000000000LL); return; }
+  if (field == 0) { out[k] = 1.0; return; }
+  const int2 e = B.ends[k];
+  const double4 pa = P.buf[prev].pr[e.x], pb = P.buf[prev].pr[e.y], qa = P.buf[prev].qq[e.x], qb = P.buf[prev].qq[e.y];
+  const V x1 = xyz(pa), x2 = image_of(g, x1, xyz(pb));
+  const V mD = xyz(B.D0[k]);
+  const double dist0 = sqrt(dot(mD, mD));
+  const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
+  BondOut o;
+  law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
+  const double pr = (K.kr != 0.0) ? 0.5 * (o.nF * o.nF) / K.kr : 0.0;
+  const double ps = (K.ks != 0.0) ? 0.5 * (o.shF * o.shF) / K.ks : 0.0;
+  const double pt = (K.kt != 0.0) ? 0.5 * (o.tM * o.tM) / K.kt : 0.0;
+  const double pb_ = (K.kb != 0.0) ? 0.5 * (o.bM * o.bM) / K.kb : 0.0;
+  double r;
+  switch (field) {
+    case 1: r = pr + ps + pt + pb_; break;
+    case 2: r = pr; break;
+    case 3: r = ps; break;
+    case 4: r = pt; break;
+    case 5: r = pb_; break;
+    default: r = o.nF / K.max_n + o.shF / K.max_s + o.tM / K.max_t + o.bM / K.max_b; break;
+  }
+  out[k] = r;
+}
+void launch_bond_field(const Grid& g, const Particles& P, int prev, long long t, const BondDev& B, int nb, int field,
+                       double* out, cudaStream_t s) {
+  if (nb > 0) k_bond_field<<<nblk(nb, 256), 256, 0, s>>>(g, P, prev, t, B, nb, field, out);
+}
+
+}  // namespace dem

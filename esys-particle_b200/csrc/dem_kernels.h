@@ -43,6 +43,12 @@ void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, c
 void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s);
 void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex, int* xbond, cudaStream_t s);
 void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s);
+void launch_particle_field(const Particles& P, int cur, int rot, int field, double* out, cudaStream_t s);
+void launch_pair_field(const Grid& g, const Particles& P, int prev, const unsigned long long* keys, int m, int kind,
+                       double k, double ks, int scaling, int meanR, const double4* hist, const float4* hist32,
+                       int field, double* out, cudaStream_t s);
+void launch_bond_field(const Grid& g, const Particles& P, int prev, long long t, const BondDev& B, int nb, int field,
+                       double* out, cudaStream_t s);
 int step_grid(int n, int tpp);
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s);
 void launch_bond_pass_f64(const StepArgs& a, bool eval, cudaStream_t s);

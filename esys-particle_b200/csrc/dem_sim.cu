@@ -163,6 +163,7 @@ struct DemSim {
   long long wall_cand = 0;               // wall-candidate interactions at the last update
   std::map<std::string, int> bond_alive; // intact bonds per group at the last update
   DBuf<double> stage;                    // host-state staging (dem_set_particles)
+  DBuf<double> scratch_d;                // field-saver values
   DBuf<int> stage_slot;
 
   DemSim() {
@@ -189,7 +190,7 @@ struct DemSim {
     scratch_i.release(); scratch_j.release(); scalars.release(); scan_tmp.release();
     d_walls.release(); d_wall_vel.release(); d_wall_partial.release(); d_wall_force.release();
     d_block_counter.release(); d_step.release(); d_ctrl.release(); d_stop.release();
-    stage.release(); stage_slot.release();
+    stage.release(); stage_slot.release(); scratch_d.release();
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -1954,6 +1955,105 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       throw std::invalid_argument("unknown option " + k);
     }
     return DEM_OK;
+  });
+}
+
+int dem_particle_scalar_field(dem_sim* h, const char* field, double* values) {
+  return guard(h, [&](DemSim& s) {
+    static const char* names[] = {"e_kin", "e_kin_linear", "e_kin_rot", "v_abs", "radius", "id", "tag"};
+    const std::string f = field ? field : "";
+    int code = -1;
+    for (int k = 0; k < 7; ++k)
+      if (f == names[k]) code = k;
+    if (code < 0) throw std::invalid_argument("unknown particle scalar field " + f);
+    if (!values) throw std::invalid_argument("null output");
+    const int n = s.n;
+    s.scratch_d.reserve(std::max(n, 1));
+    launch_particle_field(s.P, s.cur, s.rot, code, s.scratch_d.p, s.s);
+    std::vector<double> v(n);
+    std::vector<unsigned> pf(n);
+    if (n) {
+      DEM_CUDA(cudaMemcpyAsync(v.data(), s.scratch_d.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s.s));
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), s.P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s.s));
+    }
+    s.sync();
+    int k = 0;
+    for (int i = 0; i < n; ++i)
+      if (pf[i] & dem::PF_ALIVE) values[k++] = v[i];
+    return k;
+  });
+}
+
+int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* field, double* values) {
+  return guard(h, [&](DemSim& s) {
+    const std::string gname = group ? group : "", f = field ? field : "";
+    if (!values) throw std::invalid_argument("null output");
+    const int prev = s.cur ^ 1;  // the particle buffer the last force evaluation read
+    auto d = s.dyn.find(gname);
+    if (d != s.dyn.end()) {
+      dem::DynGroup& G = d->second;
+      int code = f == "count" ? 0 : f == "potential_energy" ? 1 : -1;
+      if (G.kind == 1 && f == "slipping") code = 2;
+      if (G.kind == 1 && f == "sticking") code = 3;
+      if (code < 0) throw std::invalid_argument("unknown interaction scalar field " + f + " of group " + gname);
+      std::vector<double> v(G.m, 0.0);
+      if (s.t > 0 && G.m) {
+        s.scratch_d.reserve(G.m);
+        launch_pair_field(s.g, s.P, prev, G.keys.p, G.m, G.kind, G.k, G.ks, G.scaling, G.meanR,
+                          G.kind == 1 && !s.fp32 ? G.hist[s.cur].p : nullptr,
+                          G.kind == 1 && s.fp32 ? G.hist32[s.cur].p : nullptr, code, s.scratch_d.p, s.s);
+        DEM_CUDA(cudaMemcpyAsync(v.data(), s.scratch_d.p, sizeof(double) * G.m, cudaMemcpyDeviceToHost, s.s));
+      }
+      // the pairs dem_get_pairs reports (the device hand-off keeps bond-held pairs it does not report)
+      std::vector<int> xb(s.handoff ? G.m : 0);
+      std::vector<std::vector<int>> bsteps;
+      if (s.handoff) {
+        if (G.m) DEM_CUDA(cudaMemcpyAsync(xb.data(), G.xbond.p, sizeof(int) * G.m, cudaMemcpyDeviceToHost, s.s));
+        for (auto& b : s.bond) {
+          bsteps.emplace_back(b.second.nb);
+          if (b.second.nb)
+            DEM_CUDA(cudaMemcpyAsync(bsteps.back().data(), b.second.broken_step.p, sizeof(int) * b.second.nb,
+                                     cudaMemcpyDeviceToHost, s.s));
+        }
+      }
+      s.sync();
+      int k = 0;
+      for (int q = 0; q < G.m; ++q) {
+        if (s.handoff && xb[q] >= 0 && bsteps[xb[q] >> 28][xb[q] & 0x0fffffff] > s.t) continue;
+        values[k++] = v[q];
+      }
+      return k;
+    }
+    auto b = s.bond.find(gname);
+    if (b == s.bond.end()) throw std::invalid_argument("no such group " + gname);
+    static const char* names[] = {"count", "potential_energy", "e_pot_normal", "e_pot_shear", "e_pot_twist",
+                                  "e_pot_bend", "breaking_criterion"};
+    int code = -1;
+    for (int k = 0; k < 7; ++k)
+      if (f == names[k]) code = k;
+    if (code < 0) throw std::invalid_argument("unknown RotBond scalar field " + f);
+    dem::BondGroup& B = b->second;
+    std::vector<double> v(B.nb, 0.0);
+    std::vector<int> bs(B.nb);
+    if (B.nb) {
+      DEM_CUDA(cudaMemcpyAsync(bs.data(), B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToHost, s.s));
+      if (s.t > 0 || code == 0) {
+        s.scratch_d.reserve(B.nb);
+        const dem::StepArgs a = s.make_args(s.cur);
+        int gi = 0;
+        for (auto& it : s.bond) {
+          if (it.first == gname) break;
+          ++gi;
+        }
+        launch_bond_field(s.g, s.P, prev, s.t, a.bond[gi], B.nb, code, s.scratch_d.p, s.s);
+        DEM_CUDA(cudaMemcpyAsync(v.data(), s.scratch_d.p, sizeof(double) * B.nb, cudaMemcpyDeviceToHost, s.s));
+      }
+    }
+    s.sync();
+    int k = 0;
+    for (int i = 0; i < B.nb; ++i)
+      if (bs[i] > s.t) values[k++] = v[i];
+    return k;
   });
 }
 

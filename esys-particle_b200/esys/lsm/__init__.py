@@ -15,12 +15,14 @@ from __future__ import annotations
 import numpy as np
 
 from . import _capi
+from .fields import (FieldSaver, InteractionScalarFieldSaverPrms, ParticleScalarFieldSaverPrms,
+                     WallVectorFieldSaverPrms)
 from .util import BoundingBox, Vec3
 
 __all__ = [
     "LsmMpi", "NRotSphere", "RotSphere", "Runnable", "NRotElasticPrms", "RotFrictionPrms", "RotBondPrms",
     "NRotElasticWallPrms", "LinDampingPrms", "RotDampingPrms", "GravityPrms", "Vec3", "BoundingBox",
-    "ConnectionFinder",
+    "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
 ]
 
 
@@ -185,6 +187,7 @@ class LsmMpi:
         self._nsteps = 0
         self._sim = None
         self._pre, self._post = [], []
+        self._savers, self._saved0 = [], False
         self._pending = []  # particles created before setSpatialDomain
         self._walls = {}
         self._wig_of_wall = {}
@@ -331,21 +334,43 @@ class LsmMpi:
     def addPostTimeStepRunnable(self, r):
         self._post.append(r)
 
+    # -- field savers (LsmMpiPy.cpp:2160-2175, 3272-3297; saved in runOneStep after the step,
+    #    LatticeMaster.cpp:2612-2700) --
+    def createFieldSaver(self, prms):
+        self._savers.append(FieldSaver(prms))
+
+    def _save_fields(self, t):
+        for f in self._savers:
+            if f.need_save(t):
+                f.save(self._sim)
+
     def runTimeStep(self):
         s = self._require()
+        if s.timestep == 0 and not self._saved0:
+            self._save_fields(0)
+            self._saved0 = True
         for r in self._pre:
             r.run()
         s.step(1)
+        self._save_fields(s.timestep)
         for r in self._post:
             r.run()
 
     def run(self):
         s = self._require()
-        if not self._pre and not self._post:
-            s.step(max(0, self._nsteps - s.timestep))
+        if self._pre or self._post:
+            while s.timestep < self._nsteps:
+                self.runTimeStep()
             return
-        while s.timestep < self._nsteps:
-            self.runTimeStep()
+        if s.timestep == 0 and not self._saved0:
+            self._save_fields(0)
+            self._saved0 = True
+        while s.timestep < self._nsteps:  # step in stretches up to the next save
+            nxt = [f.next_save(s.timestep) for f in self._savers]
+            nxt = [x for x in nxt if x is not None]
+            stop = min([self._nsteps] + nxt)
+            s.step(stop - s.timestep)
+            self._save_fields(s.timestep)
 
     def exit(self):
         if self._sim is not None:

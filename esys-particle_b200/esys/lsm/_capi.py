@@ -57,6 +57,8 @@ SIGNATURES = {
     "dem_precision_report": (C.c_int, [_P, C.POINTER(C.c_double), C.c_int]),
     "dem_wall_reactions_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dem_set_group_param": (C.c_int, [_P, _S, _S, C.c_double]),
+    "dem_particle_scalar_field": (C.c_int, [_P, _S, _D]),
+    "dem_interaction_scalar_field": (C.c_int, [_P, _S, _S, _D]),
     "dem_window_num_params": (C.c_int, [_P]),
     "dem_window_forward": (C.c_int, [_P, C.c_int, C.c_int, _D]),
     "dem_window_adjoint": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
@@ -280,6 +282,31 @@ class DemSim:
     @property
     def timestep(self):
         return int(self.lib.dem_timestep(self.h))
+
+    def particle_scalar_field(self, field, sort=True):
+        """(ids, values) of a particle scalar field (dem_particle_scalar_field), by id when sort."""
+        n = self.num_particles()
+        v = np.zeros(max(n, 1))
+        self._chk(self.lib.dem_particle_scalar_field(self.h, field.encode(), _dp(v)))
+        ids = np.zeros(max(n, 1), np.int32)
+        self._chk(self.lib.dem_get_particles(self.h, _ip(ids), None, None, None, None, None, None))
+        ids, v = ids[:n], v[:n]
+        if sort:
+            o = np.argsort(ids, kind="stable")
+            return ids[o], v[o]
+        return ids, v
+
+    def interaction_scalar_field(self, group, field):
+        """(id1, id2, values) of an interaction scalar field of one group, in the group's list
+        order (dem_get_pairs order)."""
+        m = self._chk(self.lib.dem_num_pairs(self.h, group.encode()))
+        a, b = np.zeros(max(m, 1), np.int32), np.zeros(max(m, 1), np.int32)
+        k = self._chk(self.lib.dem_get_pairs(self.h, group.encode(), _ip(a), _ip(b), None))
+        v = np.zeros(max(m, 1))
+        kv = self._chk(self.lib.dem_interaction_scalar_field(self.h, group.encode(), field.encode(), _dp(v)))
+        if kv != k:
+            raise DemError("interaction list changed between calls")
+        return a[:k], b[:k], v[:k]
 
     def precision_report(self):
         """FP32-force error vs FP64 on the current state (dem_precision_report); run from the

@@ -193,6 +193,24 @@ int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const 
  * integration). */
 int dem_set_option(dem_sim* h, const char* key, double value);
 
+/* ---- Field savers ----------------------------------------------------------------------- */
+
+/* Per-particle scalar field, computed on the device in the reference's accessor arithmetic
+ * (CParticle / CRotParticle::getScalarFieldFunction, Model/Particle.cpp:140-160,
+ * Model/RotParticle.cpp:422-456): "e_kin", "e_kin_linear", "e_kin_rot", "v_abs", "radius",
+ * "id", "tag".  values[] in dem_get_particles order; returns the count. */
+int dem_particle_scalar_field(dem_sim* h, const char* field, double* values);
+
+/* Per-interaction scalar field of one group, from the state its last force evaluation read:
+ * NRotElastic "count", "potential_energy"; RotFriction "count", "potential_energy", "slipping",
+ * "sticking" (Model/RotFricInteraction.cpp:384-452, 486-508); RotBond "count",
+ * "potential_energy", "e_pot_normal", "e_pot_shear", "e_pot_twist", "e_pot_bend",
+ * "breaking_criterion" (Model/ARotBondedInteraction.cpp:456-485, RotBondedInteraction.cpp:
+ * 221-256).  values[] in dem_get_pairs order; returns the count.  NRotElastic's
+ * potential_energy is 0 for a pair not touching at that evaluation (the reference keeps the
+ * last contact force of such a pair until the next rebuild). */
+int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* field, double* values);
+
 /* ---- Parameters and the differentiable loading window -------------------------------- */
 
 /* Sets one parameter of an existing group for every interaction in it, like

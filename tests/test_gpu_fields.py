@@ -1,0 +1,121 @@
+"""Field savers on the GPU: per-particle and per-interaction scalar fields against the
+state they are computed from and against the CPU oracle, and the files the savers write.
+All tests need a GPU."""
+import os
+
+import numpy as np
+import pytest
+
+import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu(dem_lib):
+    from esys.lsm import _capi
+
+    return lambda *a: _capi.DemSim(*a)
+
+
+@pytest.fixture(scope="module")
+def orc(oracle_libs):
+    return lambda *a: oracle_libs.OracleSim("orc", *a)
+
+
+def test_kinetic_energy_fields_match_reference_formulas(gpu):
+    """e_kin = (0.5 m)(v.v) + ((0.5 I) w).w for RotSpheres (Model/RotParticle.h:198-200),
+    bit for bit from the particles' own state."""
+    s = S.friction_pack(gpu)
+    s.step(40)
+    p = s.particles()
+    ids, ek = s.particle_scalar_field("e_kin")
+    _, el = s.particle_scalar_field("e_kin_linear")
+    _, er = s.particle_scalar_field("e_kin_rot")
+    _, va = s.particle_scalar_field("v_abs")
+    assert np.array_equal(ids, p["id"])
+    v, w = p["vel"], p["angvel"]
+    vv = v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2]
+    assert np.array_equal(ek, el + er)
+    assert np.array_equal(va, np.sqrt(vv))
+    _, r = s.particle_scalar_field("radius")
+    m = (4.0 / 3.0) * S.PI_REF * r * r * r
+    assert np.array_equal(el, (0.5 * m) * vv)
+
+
+def test_friction_fields_match_oracle_state(gpu, orc):
+    a, b = S.friction_pack(gpu), S.friction_pack(orc)
+    a.step(60)
+    b.step(60)
+    i1, i2, cnt = a.interaction_scalar_field("friction", "count")
+    _, _, slip = a.interaction_scalar_field("friction", "slipping")
+    _, _, stick = a.interaction_scalar_field("friction", "sticking")
+    _, _, epot = a.interaction_scalar_field("friction", "potential_energy")
+    o1, o2, st = b.pairs("friction")
+    ref = {(int(x), int(y)): r for x, y, r in zip(o1, o2, st)}
+    for k, (x, y) in enumerate(zip(i1, i2)):
+        r = ref[(int(x), int(y))]
+        assert cnt[k] == r[4] and slip[k] == r[3] and stick[k] == (1.0 if r[4] and not r[3] else 0.0)
+    assert cnt.sum() > 0 and (epot >= 0).all() and (epot[cnt == 0] == 0).all() and epot.max() > 0
+
+
+def test_bond_fields_match_oracle_criterion(gpu, orc):
+    a = S.bonded_block(gpu, strength=(5.0, 5.0, 5.0, 5.0))
+    b = S.bonded_block(orc, strength=(5.0, 5.0, 5.0, 5.0))
+    S.run_loaded(a, 40, 0.001)
+    S.run_loaded(b, 40, 0.001)
+    i1, i2, crit = a.interaction_scalar_field("bonds", "breaking_criterion")
+    _, _, cnt = a.interaction_scalar_field("bonds", "count")
+    _, _, ep = a.interaction_scalar_field("bonds", "potential_energy")
+    parts = [a.interaction_scalar_field("bonds", f)[2] for f in ("e_pot_normal", "e_pot_shear", "e_pot_twist",
+                                                                 "e_pot_bend")]
+    assert np.all(cnt == 1.0)
+    assert np.allclose(ep, parts[0] + parts[1] + parts[2] + parts[3], rtol=1e-14, atol=0)
+    o1, o2, st = b.pairs("bonds")
+    ref = {(int(x), int(y)): r[3] for x, y, r in zip(o1, o2, st)}
+    got = np.array([crit[k] for k in range(len(i1))])
+    want = np.array([ref[(int(x), int(y))] for x, y in zip(i1, i2)])
+    assert np.abs(got - want).max() <= 1e-8 * np.abs(want).max()
+
+
+def test_lsm_field_savers_write_reference_formats(dem_lib, tmp_path):
+    from esys.lsm import (InteractionScalarFieldSaverPrms, LsmMpi, NRotElasticWallPrms, ParticleScalarFieldSaverPrms,
+                          RotFrictionPrms, RotSphere, WallVectorFieldSaverPrms)
+    from esys.lsm.util import BoundingBox, Vec3
+
+    sim = LsmMpi(numWorkerProcesses=1, mpiDimList=[1, 1, 1])
+    sim.initNeighbourSearch("RotSphere", 1.2, 0.2)
+    sim.setTimeStepSize(5e-5)
+    sim.setSpatialDomain(BoundingBox(Vec3(0, -1, 0), Vec3(6, 6, 6)))
+    rng = np.random.default_rng(3)
+    parts = []
+    for k in range(80):
+        p = RotSphere(k, Vec3(*(rng.uniform(0.5, 5.5, 3))), 0.3, 0.1)
+        p.setLinearVelocity(Vec3(*rng.normal(0, 0.3, 3)))
+        parts.append(p)
+    sim.createParticles(parts)
+    sim.createInteractionGroup(RotFrictionPrms("friction", 1e4, 0.6, 0.6, 1e4))
+    sim.createWall("floor", Vec3(0, 0, 0), Vec3(0, 1, 0))
+    sim.createInteractionGroup(NRotElasticWallPrms("floor_w", "floor", 1e4))
+    f1, f2, f3, f4 = (str(tmp_path / n) for n in ("ek.dat", "ekmax.dat", "count.dat", "wall.dat"))
+    sim.createFieldSaver(ParticleScalarFieldSaverPrms("e_kin", f1, "SUM", 0, 100, 10))
+    sim.createFieldSaver(ParticleScalarFieldSaverPrms("v_abs", f2, "MAX", 5, 100, 25))
+    sim.createFieldSaver(InteractionScalarFieldSaverPrms("friction", "count", f3, "SUM", 0, 100, 20))
+    sim.createFieldSaver(WallVectorFieldSaverPrms("floor", "Force", f4, "RAW_SERIES", 0, 100, 50))
+    sim.setNumTimeSteps(100)
+    sim.run()
+    ek = open(f1).read().splitlines()
+    assert len(ek) == 11 and all(float(x) > 0 for x in ek)
+    assert len(open(f2).read().splitlines()) == 4          # steps 5, 30, 55, 80
+    cnt = open(f3).read().splitlines()
+    assert len(cnt) == 6 and cnt[0] == "%.10e" % 0.0      # nothing touching before the first step
+    wall = open(f4).read().splitlines()
+    assert len(wall) == 3 and len(wall[1].split()) == 3
+    # the e_kin lines are the id-ordered sums of the particle field, printed as %g
+    sim2 = sim._sim
+    _, ekin = sim2.particle_scalar_field("e_kin")
+    s = 0.0
+    for x in ekin.tolist():
+        s += x
+    assert ek[-1] == "%g" % s
+    sim.exit()
