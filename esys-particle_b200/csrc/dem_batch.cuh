@@ -83,7 +83,7 @@ __device__ __forceinline__ void batch_tile_epilogue(const StepArgs& a, long long
 }
 
 template <bool ROT, int TPP, int FEAT, bool FP32>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? 3 : 2)))
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? kFp32Blocks : 2)))
     k_step_batch(const BatchArgs B) {
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;

@@ -48,6 +48,10 @@ __device__ __forceinline__ Vf lane_sumf(Vf v) {
 
 constexpr int kStepThreads = 256;
 constexpr int kStepWarps = kStepThreads / 32;
+#ifndef DEM_FP32_BLOCKS
+#define DEM_FP32_BLOCKS 3
+#endif
+constexpr int kFp32Blocks = DEM_FP32_BLOCKS;  // resident blocks per SM targeted by the FP32 pair instances
 
 __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
   long long t = (long long)(n > 0 ? n : 1) * tpp;
@@ -547,7 +551,7 @@ __global__ void __launch_bounds__(kBondPassThreads, 4) k_bond_pass(const StepArg
 
 // Fused step: pair sums and integration in one launch (small systems).
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? 3 : 2)))
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? kFp32Blocks : 2)))
     k_step(const StepArgs a) {
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;
