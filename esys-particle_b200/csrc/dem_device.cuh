@@ -145,6 +145,7 @@ struct StepArgs {
   int handoff;
   int* brk_step;
   int stop_skip;            // CTRL_* bits that do not stop the chunk (0: every raised bit stops it)
+  int replay;               // recompute of steps already taken: bond failures are not logged again
   // adjoint recompute pass only (null otherwise): the pair + bond + wall + body force
   // sums before damping, and the damping iterations (lin, rot) of every particle
   double4* f_int;

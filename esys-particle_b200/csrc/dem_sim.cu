@@ -805,13 +805,19 @@ struct DemSim {
 
   // ---- differentiable loading window -------------------------------------
   // Forward: T FP64 steps from the current state with the topology frozen
-  // (no neighbour rebuild and no bond break may fall inside the window),
+  // (no neighbour rebuild may fall inside the window; a bond failure may only
+  // with the device bond hand-off, and is then a fixed event of the window),
   // checkpoints of the particle state, friction histories and wall planes every
   // K steps, and the reaction of every wall group after every step.
   // Adjoint: the reverse pass over the stored window, segment by segment from
   // the last, each segment's forward states recomputed from its checkpoint.
+  // With failures inside the window the recompute replays them: the bonds'
+  // failure steps are already recorded (a bond is evaluated while its failure
+  // step lies ahead, exactly as in the forward), the wall candidacy and the
+  // last-failure record are restored per segment, and nothing is logged again.
   struct Window {
     bool valid = false;
+    bool brk = false;  // bond failures may fall inside the window (device hand-off)
     int T = 0, K = 0, nseg = 0, n = 0, ts = 0, cur0 = 0;
     long long t0 = 0;
     int m[kMaxDyn] = {0, 0};
@@ -821,7 +827,13 @@ struct DemSim {
     DBuf<unsigned char> st_it;
     DBuf<double> R, gR, gvisc, gpar_b[kMaxBond], gpar_d[kMaxDyn], acc, save_wf;
     DBuf<long long> ck_step;
+    DBuf<unsigned> ck_pf, st_pf, save_pf;  // wall candidacy: per checkpoint, per recomputed step, live
+    DBuf<int> ck_brk, save_brk, bs0[kMaxBond], nev0;
+    DBuf<unsigned char> flag0;
     void release() {
+      ck_pf.release(); st_pf.release(); save_pf.release(); ck_brk.release(); save_brk.release(); nev0.release();
+      flag0.release();
+      for (int b = 0; b < kMaxBond; ++b) bs0[b].release();
       ck.release(); st.release(); st_f.release(); st_m.release(); lam.release();
       for (int d = 0; d < kMaxDyn; ++d) {
         ck_hist[d].release(); st_hist[d].release(); lH[d].release(); gpair[d].release(); gpar_d[d].release();
@@ -846,7 +858,8 @@ struct DemSim {
   int window_num_params() const { return 4 * (int)bond.size() + 2 * (int)dyn.size() + 2; }
 
   void window_check_ctrl(int ctrl, bool last) {
-    if (ctrl & CTRL_BROKE) throw StateError("a bond broke inside the differentiable window (the bond state must stay frozen)");
+    if ((ctrl & CTRL_BROKE) && !handoff)
+      throw StateError("a bond broke inside the differentiable window (enable the device bond hand-off to keep it)");
     if (ctrl & CTRL_OVERFLOW) throw StateError("bond-break event log overflowed inside the differentiable window");
     if ((ctrl & CTRL_REBUILD) && !last)
       throw StateError("a neighbour rebuild fell inside the differentiable window (shorten it or enlarge verletDist)");
@@ -862,7 +875,24 @@ struct DemSim {
     auto dl = dyn_list();
     win.T = T; win.K = std::min(K, T); win.nseg = (T + win.K - 1) / win.K; win.n = n; win.t0 = t;
     win.ts = timestamp; win.cur0 = cur;
+    win.brk = handoff != 0;
     win.ck.reserve((size_t)win.nseg * 4 * std::max(n, 1));
+    if (win.brk) {  // what a rewind must put back: failure records, event counts, flags
+      win.ck_pf.reserve((size_t)win.nseg * std::max(n, 1));
+      win.ck_brk.reserve((size_t)win.nseg * 2);
+      win.nev0.reserve(kMaxBond);
+      win.flag0.reserve(std::max(n, 1));
+      int b = 0;
+      for (auto& bg : bond) {
+        BondGroup& B = bg.second;
+        win.bs0[b].reserve(std::max(B.nb, 1));
+        if (B.nb)
+          DEM_CUDA(cudaMemcpyAsync(win.bs0[b].p, B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(win.nev0.p + b, B.nevents.p, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        ++b;
+      }
+      if (n) DEM_CUDA(cudaMemcpyAsync(win.flag0.p, P.flagged, n, cudaMemcpyDeviceToDevice, s));
+    }
     win.ck_walls.reserve((size_t)win.nseg * kMaxWalls);
     win.R.reserve((size_t)T * kMaxWalls * 3);
     for (int d = 0; d < nd; ++d) {
@@ -877,6 +907,11 @@ struct DemSim {
     for (int c = 0; c < win.nseg; ++c) {
       const int len = std::min(win.K, T - c * win.K);
       copy_state(view4(win.ck.p + (size_t)c * 4 * n, n), P.buf[cur]);
+      if (win.brk) {
+        if (n) DEM_CUDA(cudaMemcpyAsync(win.ck_pf.p + (size_t)c * n, P.pflags, sizeof(unsigned) * n,
+                                        cudaMemcpyDeviceToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(win.ck_brk.p + 2 * c, d_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+      }
       for (int d = 0; d < nd; ++d)
         if (dl[d]->kind == 1 && win.m[d])
           DEM_CUDA(cudaMemcpyAsync(win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist[cur].p,
@@ -953,6 +988,13 @@ struct DemSim {
     win.acc.reserve(64);
     win.save_walls.reserve(kMaxWalls);
     win.save_wf.reserve(kMaxWalls * 3);
+    if (win.brk) {
+      win.st_pf.reserve((size_t)K * nn);
+      win.save_pf.reserve(nn);
+      win.save_brk.reserve(2);
+      if (n) DEM_CUDA(cudaMemcpyAsync(win.save_pf.p, P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(win.save_brk.p, d_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
     for (int d = 0; d < nd; ++d) {
       const int m = std::max(win.m[d], 1);
       if (dl[d]->kind == 1) win.st_hist[d].reserve((size_t)(K + 1) * m);
@@ -1027,6 +1069,11 @@ struct DemSim {
       if (nw)
         DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p + (size_t)c * kMaxWalls, sizeof(WallDev) * nw,
                                  cudaMemcpyDeviceToDevice, s));
+      if (win.brk) {
+        if (n) DEM_CUDA(cudaMemcpyAsync(P.pflags, win.ck_pf.p + (size_t)c * n, sizeof(unsigned) * n,
+                                        cudaMemcpyDeviceToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(d_brk.p, win.ck_brk.p + 2 * c, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+      }
       long long tcv = tc;
       DEM_CUDA(cudaMemcpyAsync(d_step.p, &tcv, sizeof(long long), cudaMemcpyHostToDevice, s));
       DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
@@ -1048,7 +1095,11 @@ struct DemSim {
         a.m_int = win.st_m.p + (size_t)j * n;
         a.damp_iters = win.st_it.p + (size_t)j * 2 * n;
         a.store_forces = 0;
+        a.replay = 1;
         launch_step(a, rot != 0, t_pp, two, s);
+        if (win.brk && n)  // the wall candidacy this step used (refreshed in it after a failure)
+          DEM_CUDA(cudaMemcpyAsync(win.st_pf.p + (size_t)j * n, P.pflags, sizeof(unsigned) * n,
+                                   cudaMemcpyDeviceToDevice, s));
       }
       DEM_CUDA(cudaGetLastError());
       c_launches += two ? 2LL * len : len;
@@ -1061,6 +1112,7 @@ struct DemSim {
         A.m_int = win.st_m.p + (size_t)j * n;
         A.iters = win.st_it.p + (size_t)j * 2 * n;
         A.walls = win.st_walls.p + (size_t)j * kMaxWalls;
+        A.pflags = win.brk ? win.st_pf.p + (size_t)j * n : P.pflags;
         A.gR = win.gR.p + (size_t)(c * K + j) * kMaxWalls * 3;
         for (int d = 0; d < nd; ++d)
           A.dyn[d].hist_in = dl[d]->kind == 1 ? win.st_hist[d].p + (size_t)j * std::max(win.m[d], 1) : nullptr;
@@ -1076,6 +1128,10 @@ struct DemSim {
     off += 2;
     DEM_CUDA(cudaGetLastError());
     // restore the live device state
+    if (win.brk) {
+      if (n) DEM_CUDA(cudaMemcpyAsync(P.pflags, win.save_pf.p, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_brk.p, win.save_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
     if (nw) DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.save_walls.p, sizeof(WallDev) * nw, cudaMemcpyDeviceToDevice, s));
     DEM_CUDA(cudaMemcpyAsync(d_wall_force.p, win.save_wf.p, sizeof(double) * kMaxWalls * 3, cudaMemcpyDeviceToDevice, s));
     DEM_CUDA(cudaMemcpyAsync(d_step.p, &t, sizeof(long long), cudaMemcpyHostToDevice, s));
@@ -1150,10 +1206,26 @@ struct DemSim {
                                  cudaMemcpyDeviceToDevice, s));
     if (!wig.empty())
       DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p, sizeof(WallDev) * wig.size(), cudaMemcpyDeviceToDevice, s));
+    if (win.brk) {  // undo the window's bond failures
+      int b = 0;
+      for (auto& bg : bond) {
+        BondGroup& B = bg.second;
+        if (B.nb)
+          DEM_CUDA(cudaMemcpyAsync(B.broken_step.p, win.bs0[b].p, sizeof(int) * B.nb, cudaMemcpyDeviceToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(B.nevents.p, win.nev0.p + b, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        ++b;
+      }
+      if (n) {
+        DEM_CUDA(cudaMemcpyAsync(P.flagged, win.flag0.p, n, cudaMemcpyDeviceToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(P.pflags, win.ck_pf.p, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, s));
+      }
+      DEM_CUDA(cudaMemcpyAsync(d_brk.p, win.ck_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
     t = win.t0;
     DEM_CUDA(cudaMemcpyAsync(d_step.p, &t, sizeof(long long), cudaMemcpyHostToDevice, s));
     pending_ctrl = 0;
     sync();
+    if (win.brk) refresh_counts();
     download_walls();
   }
 };

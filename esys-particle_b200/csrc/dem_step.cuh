@@ -270,15 +270,17 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
               B.broken_step[k] = (int)(step + 1);
               a.P.flagged[i] = 1;
               a.P.flagged[j] = 1;
-              int slot = atomicAdd(B.nevents, 1);
-              if (slot < B.cap_events) {
-                B.events[3 * slot] = a.P.id[i];
-                B.events[3 * slot + 1] = a.P.id[j];
-                B.events[3 * slot + 2] = (int)(step + 1);
-              } else {
-                atomicOr(a.ctrl, CTRL_OVERFLOW);
+              if (!a.replay) {
+                int slot = atomicAdd(B.nevents, 1);
+                if (slot < B.cap_events) {
+                  B.events[3 * slot] = a.P.id[i];
+                  B.events[3 * slot + 1] = a.P.id[j];
+                  B.events[3 * slot + 2] = (int)(step + 1);
+                } else {
+                  atomicOr(a.ctrl, CTRL_OVERFLOW);
+                }
+                atomicOr(a.ctrl, CTRL_BROKE);
               }
-              atomicOr(a.ctrl, CTRL_BROKE);
               if (a.handoff) a.brk_step[step & 1] = (int)step;
             }
           } else {
@@ -528,15 +530,17 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
     B.broken_step[k] = (int)(step + 1);
     a.P.flagged[i] = 1;
     a.P.flagged[j] = 1;
-    const int slot = atomicAdd(B.nevents, 1);
-    if (slot < B.cap_events) {
-      B.events[3 * slot] = a.P.id[i];
-      B.events[3 * slot + 1] = a.P.id[j];
-      B.events[3 * slot + 2] = (int)(step + 1);
-    } else {
-      atomicOr(a.ctrl, CTRL_OVERFLOW);
+    if (!a.replay) {
+      const int slot = atomicAdd(B.nevents, 1);
+      if (slot < B.cap_events) {
+        B.events[3 * slot] = a.P.id[i];
+        B.events[3 * slot + 1] = a.P.id[j];
+        B.events[3 * slot + 2] = (int)(step + 1);
+      } else {
+        atomicOr(a.ctrl, CTRL_OVERFLOW);
+      }
+      atomicOr(a.ctrl, CTRL_BROKE);
     }
-    atomicOr(a.ctrl, CTRL_BROKE);
     if (a.handoff) a.brk_step[step & 1] = (int)step;
   }
 }

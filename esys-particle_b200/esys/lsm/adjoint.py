@@ -1,7 +1,9 @@
 """Differentiable loading windows: platen reactions as a torch.autograd.Function.
 
 A window is ``nsteps`` FP64 steps of the GPU worker with the contact topology
-and bond state frozen (dem_window_forward).  Its output is the reaction of every
+frozen (dem_window_forward).  Bonds may fail inside it when the device bond
+hand-off is on; the failures are then fixed events of the window (the bond
+state is frozen for the derivative).  Its output is the reaction of every
 wall interaction group after every step, ``R[t, group, 3]`` (the values
 ``LsmMpi.getWallForce`` would report, Model/EWallInteractionGroup.hpp:47-53); its
 differentiable inputs are the interaction parameters in the library's layout

@@ -229,8 +229,11 @@ int dem_set_group_param(dem_sim* h, const char* group, const char* key, double v
 int dem_window_num_params(dem_sim* h);
 
 /* Runs nsteps FP64 steps (the dem_step sequence) as a differentiable window: the neighbour
- * lists, wall candidates and bond set are frozen (DEM_ERR_STATE if a rebuild or a bond break
- * falls inside the window), the state is checkpointed every checkpoint_every steps, and the
+ * lists are frozen (DEM_ERR_STATE if a rebuild falls inside the window).  A bond failure
+ * inside the window needs the device bond hand-off (dem_set_option "bond_handoff"; else
+ * DEM_ERR_STATE): the failures are then events of the window, the same in the forward run
+ * and in the adjoint's recompute, and the gradient is that of the branch taken.  The state
+ * is checkpointed every checkpoint_every steps, and the
  * reaction of every wall group after every step (CWall::m_force, EWallInteractionGroup.hpp:
  * 47-53) is written to reactions[nsteps][wall groups in name order][3] (may be null). */
 int dem_window_forward(dem_sim* h, int nsteps, int checkpoint_every, double* reactions);
@@ -243,7 +246,8 @@ int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_pa
                        double* grad_angvel, double* grad_pos, double* grad_quat);
 
 /* Restores the state at the start of the last window (particles, friction histories, wall
- * planes, timestep), so that the window can be run again with other parameters. */
+ * planes, timestep, and the bond failures, event log and wall candidacy the window changed),
+ * so that the window can be run again with other parameters. */
 int dem_window_rewind(dem_sim* h);
 
 /* ---- Batched ensemble --------------------------------------------------------------------

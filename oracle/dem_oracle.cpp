@@ -1372,7 +1372,10 @@ extern "C" {
  * "pos:<id>:<c>".  R[nsteps][wall groups][3] receives the reaction of each wall group (name
  * order) after each step, dR[nsteps][wall groups][3][nseed] its derivatives.  The simulation
  * itself is not advanced (only the head of its next step, the pending neighbour search and
- * interaction update, is done).  Returns -5 if a rebuild or a bond break falls inside the window. */
+ * interaction update, is done).  A bond failure inside the window is followed as the reference
+ * handles it (erase, flags, new list to the RotFriction groups, wall candidates refreshed); the
+ * derivatives are those of the branch taken.  Returns -5 if a rebuild falls inside the window
+ * or a failure would feed new-list pairs to an elastic group. */
 int orc_window_dual(void* h, int nsteps, int nseed, const char* const* seeds, double* R, double* dR) {
   using namespace orc::dual;
   Sim& s = *(Sim*)h;
@@ -1427,6 +1430,17 @@ int orc_window_dual(void* h, int nsteps, int nseed, const char* const* seeds, do
   for (auto& w : s.walls) wo[w.first] = w.second.o;
   const int ng = (int)s.wig.size();
   const double half = 0.5 * s.alpha, srsqr = half * half;
+  /* Bond failures inside the window are taken as the forward's events: the failed bond leaves
+   * its storage at the head of the next step and the "new list" of pairs between flagged
+   * particles joins the dynamic groups (TSubLattice::updateInteractions, SubLattice.hpp:2416-2466),
+   * all held in window-local copies so the simulation itself is left as it was. */
+  std::map<std::string, std::vector<char>> gone;        /* bond erased inside the window */
+  std::map<std::string, std::vector<int>> failed;       /* bonds that failed in the last step */
+  std::map<std::string, std::vector<Fric>> extra;       /* new-list pairs appended inside the window */
+  std::set<std::pair<int, int>> released, added;        /* failed bonds' ids; appended pairs' ids */
+  std::map<std::string, std::vector<WallI>> wits;       /* wall candidates, refreshed after a failure */
+  for (auto& b : s.bpis) gone[b.first].assign(b.second->bd.size(), 0);
+  for (auto& wg : s.wig) wits[wg.first] = wg.second.its;
   for (int j = 0; j < nsteps; ++j) {
     if (j > 0) {  /* checkNeighbors at the head of step j: a rebuild would unfreeze the topology */
       double mdsqr = 0;
@@ -1438,13 +1452,55 @@ int orc_window_dual(void* h, int nsteps, int nseed, const char* const* seeds, do
       }
       if (mdsqr > srsqr) { s.err = "a neighbour rebuild falls inside the window"; return -5; }
     }
+    bool changed = false;
+    for (auto& f : failed) {   /* PIS_EB::update (pi_storage_eb.hpp:23-49) */
+      for (int q : f.second) {
+        const Bond& b = s.bpis[f.first]->bd[q];
+        gone[f.first][q] = 1;
+        released.insert({s.P.id[b.p1], s.P.id[b.p2]});
+        s.P.flag[b.p1] = 1;
+        s.P.flag[b.p2] = 1;
+        changed = true;
+      }
+      f.second.clear();
+    }
+    if (changed) {
+      for (auto& d : s.dpis) {   /* PIS_ED::update without a rebuild: the new list (pi_storage_ed.hpp:84-161) */
+        const std::vector<std::pair<int, int>> pl = new_list(s);
+        for (auto& p : pl) {
+          const int a = s.P.id[p.first], b = s.P.id[p.second];
+          bool excl = false;
+          for (auto* e : d.second->exig) excl = excl || (e->idset.count({a, b}) && !released.count({a, b}));
+          if (excl || d.second->idset.count({a, b}) || added.count({a, b})) continue;
+          if (d.second->kind != 1) { s.err = "a bond failure inside the window feeds an elastic group"; return -5; }
+          extra[d.first].push_back(make_fric(s, *d.second, p.first, p.second));
+          hist[d.first].push_back(DFric{DV(V3(0, 0, 0)), false, false});
+          added.insert({a, b});
+        }
+      }
+      for (auto& wg : s.wig) {   /* CEWallInteractionGroup::Update at the current positions */
+        std::vector<WallI>& its = wits[wg.first];
+        its.clear();
+        const Wall& w = s.walls[wg.second.wall];
+        const V3 o = wo[wg.second.wall];
+        for (int i = 0; i < n; ++i) {
+          if (!s.P.alive[i]) continue;
+          const V3 x(st.pos[i].x.v, st.pos[i].y.v, st.pos[i].z.v);
+          if (std::fabs(dot(x - o, w.n)) < s.nrange) {
+            double f = 1.0;
+            f *= 3.141592654 * s.P.rad[i];
+            its.push_back(WallI{i, f * wg.second.k, is_inner(s, x)});
+          }
+        }
+      }
+    }
     for (int i = 0; i < n; ++i) { st.force[i] = DV(V3(0, 0, 0)); st.moment[i] = DV(V3(0, 0, 0)); }
     int gi = 0;
     for (auto& wg : s.wig) {   /* walls (EWallInteraction.hpp:42-78), reaction per group */
       const Wall& w = s.walls[wg.second.wall];
       const DV o(wo[wg.second.wall]), nn(w.n);
       DV acc(V3(0, 0, 0));
-      for (auto& wi : wg.second.its) {
+      for (auto& wi : wits[wg.first]) {
         const Du dist = ddot(st.pos[wi.p] - o, nn);
         const double r = s.P.rad[wi.p];
         if (dist < r) {
@@ -1468,16 +1524,22 @@ int orc_window_dual(void* h, int nsteps, int nseed, const char* const* seeds, do
         for (auto& e : d.second->el) d_elastic(s, *d.second, e, prm.k[d.first], st);
       } else {
         auto& hv = hist[d.first];
-        for (size_t q = 0; q < d.second->fr.size(); ++q)
+        const size_t m0 = d.second->fr.size();
+        for (size_t q = 0; q < m0; ++q)
           d_fric(s, *d.second, d.second->fr[q], hv[q], prm.k[d.first], prm.ks[d.first], st);
+        auto ex = extra.find(d.first);
+        if (ex != extra.end())
+          for (size_t q = 0; q < ex->second.size(); ++q)
+            d_fric(s, *d.second, ex->second[q], hv[m0 + q], prm.k[d.first], prm.ks[d.first], st);
       }
     }
-    for (auto& b : s.bpis)
-      for (auto& bd : b.second->bd)
-        if (d_bond(s, *b.second, bd, prm.k[b.first], prm.ks[b.first], prm.kt[b.first], prm.kb[b.first], st)) {
-          s.err = "a bond breaks inside the window";
-          return -5;
-        }
+    for (auto& b : s.bpis) {
+      const std::vector<char>& gb = gone[b.first];
+      for (size_t q = 0; q < b.second->bd.size(); ++q)
+        if (!gb[q] && d_bond(s, *b.second, b.second->bd[q], prm.k[b.first], prm.ks[b.first], prm.kt[b.first],
+                             prm.kb[b.first], st))
+          failed[b.first].push_back((int)q);
+    }
     for (auto& d : s.damping) {
       if (d.first == "Damping") {
         for (int i : s.damp_list)

@@ -139,14 +139,15 @@ def mse_grad(R, tgt):
 
 
 def window_block(make, nx=4, ny=5, nz=4, seed=4, dt=1e-4, kr=1e5, ks=1e5, kt=1e5, kb=1e5, visc=1.0, vscale=1.0,
-                 platen_speed=0.5, friction=False, vel=None, angvel=None, tilt=(0.5, 0.3)):
+                 platen_speed=0.5, friction=False, vel=None, angvel=None, tilt=(0.5, 0.3), strength=1e6):
     """Bonded block for the differentiable window: a cubic lattice of RotSpheres
     (r ~ U[0.49, 0.5]) with every lattice neighbour bonded, strengths far above
     the loads (elastic regime, no breaks), platens that
     start just touching the block and move inward at ``platen_speed`` (so the
     reactions are carried by the bonds), seeded initial linear and angular
     velocities (``vel`` / ``angvel`` override them, rows by id) and the
-    stiffness / damping parameters as arguments.  The defaults give every
+    stiffness / damping parameters as arguments.  A ``strength`` (all four
+    bond strengths) near the loads makes bonds fail inside the window.  The defaults give every
     parameter a loss sensitivity well above the FP64 rounding noise of a
     200-step window, so that central differences at h = 1e-6 relative resolve
     the gradient (torsion / bending stiffness as large as the normal one, and a
@@ -176,7 +177,7 @@ def window_block(make, nx=4, ny=5, nz=4, seed=4, dt=1e-4, kr=1e5, ks=1e5, kt=1e5
     sim = make("RotSphere", 1.25, 0.2, (0, 0, 0), tuple(float(x) for x in top), (0, 0, 0), dt)
     sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=v0, angvel=w0)
     sim.add_connections(np.ones(len(i1), np.int32), i1, i2)
-    sim.add_rot_bond_group("bonds", 1, kr, ks, kt, kb, 1e6, 1e6, 1e6, 1e6, True, True, 1.0)
+    sim.add_rot_bond_group("bonds", 1, kr, ks, kt, kb, strength, strength, strength, strength, True, True, 1.0)
     if friction:
         sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
         sim.add_exclusion("bonds", "friction")

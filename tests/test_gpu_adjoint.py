@@ -242,3 +242,78 @@ def test_hand_written_bond_reverse_matches_dual_numbers(gpu):
     for k in ("params", "vel", "angvel", "pos", "quat"):
         scale = np.abs(out[6][k]).max()
         assert np.abs(out[0][k] - out[6][k]).max() <= 1e-9 * scale, k
+
+
+# ---- bond failures inside the window (device bond hand-off) ----
+BRK = dict(friction=True, strength=2000.0)   # ~20 of 184 bonds fail between steps 11 and 58
+
+
+def _breaking(gpu):
+    a = S.window_block(gpu, **BRK)
+    a.set_option("bond_handoff", 1)
+    return a
+
+
+@pytest.fixture(scope="module")
+def brk_run(gpu, orc):
+    a = _breaking(gpu)
+    R = a.window_forward(T, 32)
+    ev = a.breaks()
+    tgt = S.mse_target(R)
+    g = a.window_adjoint(S.mse_grad(R, tgt))
+    b = S.window_block(orc, **BRK)
+    lo, hi = _seed_particles(b)
+    Rd, dR = b.window_dual(T, list(S.WINDOW_SEEDS) + [f"vel:{lo}:1", f"angvel:{hi}:0"], 2)
+    gd = np.einsum("tgc,tgck->k", S.mse_grad(Rd, tgt), dR)
+    c = S.window_block(orc, **BRK)
+    c.step(T)
+    return a, R, ev, tgt, g, Rd, gd, c.breaks(), (lo, hi)
+
+
+def test_window_with_bond_failures_matches_oracle(brk_run):
+    a, R, ev, tgt, g, Rd, gd, ev_orc, _ = brk_run
+    assert len(ev[0]) >= 10
+    for u, v in zip(ev, ev_orc):
+        assert np.array_equal(u, v)
+    assert np.abs(R - Rd).max() <= 1e-7 * np.abs(Rd).max()
+
+
+def test_adjoint_with_bond_failures_matches_dual_numbers(brk_run):
+    a, R, ev, tgt, g, Rd, gd, _, (lo, hi) = brk_run
+    layout = a.param_layout()
+    idx = [layout.index(k) for k in S.WINDOW_PARAMS]
+    _grad_vs(g["params"][idx], gd[:6], 1e-5)
+    _grad_vs(np.array([g["vel"][lo, 1], g["angvel"][hi, 0]]), gd[6:], 1e-5)
+
+
+def test_bond_failures_checkpoint_interval_does_not_change_gradients(gpu):
+    """The recompute replays the failures (wall candidacy and last-failure record restored
+    per segment), so segments of 1 step and one segment of the whole window agree."""
+    out = []
+    for K in (1, 13, T):
+        a = _breaking(gpu)
+        R = a.window_forward(T, K)
+        tgt = S.mse_target(R)
+        out.append(a.window_adjoint(S.mse_grad(R, tgt)))
+        assert len(a.breaks()[0]) >= 10       # the recompute logged nothing again
+    for o in out[1:]:
+        for k in ("params", "vel", "angvel", "pos", "quat"):
+            assert np.array_equal(o[k], out[0][k]), k
+
+
+def test_rewind_undoes_bond_failures(gpu):
+    a = _breaking(gpu)
+    R1 = a.window_forward(T, 40)
+    e1 = a.breaks()
+    p1 = a.particles()
+    a.window_rewind()
+    assert len(a.breaks()[0]) == 0
+    R2 = a.window_forward(T, 40)
+    assert np.array_equal(R1, R2)
+    for u, v in zip(e1, a.breaks()):
+        assert np.array_equal(u, v)
+    p2 = a.particles()
+    for k in ("pos", "vel", "angvel", "quat"):
+        assert np.array_equal(p1[k], p2[k]), k
+    a.step(5)                      # the failures are handed on to the ordinary stepping
+    assert a.timestep == T + 5

@@ -91,3 +91,44 @@ def test_dual_velocity_gradient_vs_central_differences(orc, dual_run, k, field, 
         return S.mse(S.wall_force_history(S.window_block(orc, vel=v, angvel=w), T), tgt)
 
     check_gradient(g[k], loss_at, (v0 if field == "vel" else w0)[pid, c])
+
+
+# ---- bond failures inside the window: the forward's events, fixed for the derivative ----
+BRK = dict(friction=True, strength=2000.0)   # ~20 of 184 bonds fail between steps 11 and 58
+
+
+def test_dual_window_follows_bond_failures(orc):
+    """Values equal the restatement's FP64 steps bit for bit through the failures (the
+    failed bond leaves, its particles' new-list pairs join the friction group, the wall
+    candidates are refreshed), and the failures happen inside the window."""
+    a = S.window_block(orc, **BRK)
+    R, dR = a.window_dual(T, list(S.WINDOW_SEEDS), 2)
+    ref = S.wall_force_history(a, T)
+    assert np.array_equal(R, ref)
+    steps = a.breaks()[2]
+    assert len(steps) >= 10 and steps.min() > 1 and steps.max() < T
+
+
+@pytest.fixture(scope="module")
+def dual_brk(orc):
+    a = S.window_block(orc, **BRK)
+    R, dR = a.window_dual(T, list(S.WINDOW_SEEDS), 2)
+    tgt = S.mse_target(R)
+    return tgt, np.einsum("tgc,tgck->k", S.mse_grad(R, tgt), dR)
+
+
+# normalK, shearK, torsionK and the linear viscosity move the loss well above the rounding
+# noise of a window with failing bonds and slipping contacts; bendingK and the rotational
+# viscosity do not (their best central differences stay near 2e-4)
+@pytest.mark.parametrize("k", [0, 1, 2, 4])
+def test_dual_gradient_with_bond_failures_vs_central_differences(orc, dual_brk, k):
+    tgt, g = dual_brk
+    group, key = S.WINDOW_PARAMS[k]
+    base = {"normalK": 1e5, "shearK": 1e5, "torsionK": 1e5, "viscosity": 1.0}[key]
+
+    def loss_at(x):
+        b = S.window_block(orc, **BRK)
+        b.set_group_param(group, key, x)
+        return S.mse(S.wall_force_history(b, T), tgt)
+
+    check_gradient(g[k], loss_at, base)
