@@ -313,7 +313,13 @@ __global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
     return;
   }
   // CRotFrictionInteraction
-  const double4 h = G.hist_in[k];
+  double4 h;
+  if (G.hist32_in) {
+    const float4 f = G.hist32_in[k];
+    h = make_double4(f.x, f.y, f.z, f.w);
+  } else {
+    h = G.hist_in[k];
+  }
   const V lH = xyzv(G.lH[k]);
   const V3<D23> x1 = seed3(x1d, 0), x2 = seed3(x2d, 3);
   const V3<D23> v1 = seed3(xyzv(A.s0.vm[s1]), 6), v2 = seed3(xyzv(A.s0.vm[s2]), 9);

@@ -14,6 +14,7 @@ struct AdjDyn {
   const int* adj_start;               // per-particle adjacency over the pairs
   const int2* adj;
   const double4* hist_in;             // friction history read by this step (forward recompute)
+  const float4* hist32_in;            // the same when the window runs the FP32-force form
   const int* xbond;                   // device bond hand-off: excluding bond of each pair (else null)
   double4* lH;                        // adjoint of the history: in after step t, out before it
   double4* gpair;                     // [m][6]: d/dx1, d/dx2, d/dv1, d/dv2, d/dw1, d/dw2 of this step

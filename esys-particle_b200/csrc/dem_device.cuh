@@ -146,6 +146,7 @@ struct StepArgs {
   int* brk_step;
   int stop_skip;            // CTRL_* bits that do not stop the chunk (0: every raised bit stops it)
   int replay;               // recompute of steps already taken: bond failures are not logged again
+  unsigned* pf_log;         // window recompute (else null): the PF_* bits each particle used in this step
   // adjoint recompute pass only (null otherwise): the pair + bond + wall + body force
   // sums before damping, and the damping iterations (lin, rot) of every particle
   double4* f_int;

@@ -830,7 +830,11 @@ struct DemSim {
     DBuf<unsigned> ck_pf, st_pf, save_pf;  // wall candidacy: per checkpoint, per recomputed step, live
     DBuf<int> ck_brk, save_brk, bs0[kMaxBond], nev0;
     DBuf<unsigned char> flag0;
+    DBuf<float4> st_vw, st_hist32[kMaxDyn];  // FP32 form: velocity shadows and histories of the recompute
+    bool fp32 = false;
     void release() {
+      st_vw.release();
+      for (int d = 0; d < kMaxDyn; ++d) st_hist32[d].release();
       ck_pf.release(); st_pf.release(); save_pf.release(); ck_brk.release(); save_brk.release(); nev0.release();
       flag0.release();
       for (int b = 0; b < kMaxBond; ++b) bs0[b].release();
@@ -846,6 +850,12 @@ struct DemSim {
   } win;
 
   static ParticleBuf view4(double4* base, int n) { return ParticleBuf{base, base + n, base + 2 * (size_t)n, base + 3 * (size_t)n, nullptr}; }
+  // state j of the segment being recomputed (with its FP32 velocity shadow in the FP32 form)
+  ParticleBuf st_view(int j) {
+    ParticleBuf b = view4(win.st.p + (size_t)j * 4 * n, n);
+    if (win.fp32) b.vw = win.st_vw.p + (size_t)j * 2 * std::max(n, 1);
+    return b;
+  }
   void copy_state(const ParticleBuf& dst, const ParticleBuf& src) {
     const size_t b = sizeof(double4) * (size_t)n;
     DEM_CUDA(cudaMemcpyAsync(dst.pr, src.pr, b, cudaMemcpyDeviceToDevice, s));
@@ -867,7 +877,6 @@ struct DemSim {
 
   int window_forward(int T, int K, double* R_host) {
     if (T < 1 || K < 1) throw std::invalid_argument("window length and checkpoint interval must be >= 1");
-    if (fp32) throw std::invalid_argument("the differentiable window runs the FP64 form (set precision 64)");
     if (iter_lin > 255 || iter_rot > 255) throw std::invalid_argument("window damping needs maxIterations <= 255");
     win.valid = false;
     if (!prepare()) return DEM_ERR_OVERFLOW;
@@ -876,6 +885,7 @@ struct DemSim {
     win.T = T; win.K = std::min(K, T); win.nseg = (T + win.K - 1) / win.K; win.n = n; win.t0 = t;
     win.ts = timestamp; win.cur0 = cur;
     win.brk = handoff != 0;
+    win.fp32 = fp32 != 0;
     win.ck.reserve((size_t)win.nseg * 4 * std::max(n, 1));
     if (win.brk) {  // what a rewind must put back: failure records, event counts, flags
       win.ck_pf.reserve((size_t)win.nseg * std::max(n, 1));
@@ -904,6 +914,7 @@ struct DemSim {
     d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
     const bool two = split == 1;
     const long long cps = contacts_per_step();
+    if (fp32) launch_sync_vw(P, cur, s);
     for (int c = 0; c < win.nseg; ++c) {
       const int len = std::min(win.K, T - c * win.K);
       copy_state(view4(win.ck.p + (size_t)c * 4 * n, n), P.buf[cur]);
@@ -913,9 +924,13 @@ struct DemSim {
         DEM_CUDA(cudaMemcpyAsync(win.ck_brk.p + 2 * c, d_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
       }
       for (int d = 0; d < nd; ++d)
-        if (dl[d]->kind == 1 && win.m[d])
-          DEM_CUDA(cudaMemcpyAsync(win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist[cur].p,
-                                   sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+        if (dl[d]->kind == 1 && win.m[d]) {
+          if (fp32)  // FP32 records widened exactly
+            launch_hist_convert(win.m[d], win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist32[cur].p, false, s);
+          else
+            DEM_CUDA(cudaMemcpyAsync(win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist[cur].p,
+                                     sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+        }
       if (!wig.empty())
         DEM_CUDA(cudaMemcpyAsync(win.ck_walls.p + (size_t)c * kMaxWalls, d_walls.p, sizeof(WallDev) * wig.size(),
                                  cudaMemcpyDeviceToDevice, s));
@@ -925,7 +940,8 @@ struct DemSim {
         StepArgs a = make_args((cur + j) & 1);
         a.wall_hist = win.R.p;
         a.wall_hist_t0 = win.t0;
-        launch_step(a, rot != 0, t_pp, two, s);
+        if (fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
+        else launch_step(a, rot != 0, t_pp, two, s);
       }
       DEM_CUDA(cudaGetLastError());
       c_launches += two ? 2LL * len : len;
@@ -978,6 +994,7 @@ struct DemSim {
     const int nn = std::max(n, 1);
     // device buffers
     win.st.reserve((size_t)(K + 1) * 4 * nn);
+    if (win.fp32) win.st_vw.reserve((size_t)(K + 1) * 2 * nn);
     win.st_f.reserve((size_t)K * nn);
     win.st_m.reserve((size_t)K * nn);
     win.st_it.reserve((size_t)K * 2 * nn);
@@ -997,7 +1014,10 @@ struct DemSim {
     }
     for (int d = 0; d < nd; ++d) {
       const int m = std::max(win.m[d], 1);
-      if (dl[d]->kind == 1) win.st_hist[d].reserve((size_t)(K + 1) * m);
+      if (dl[d]->kind == 1) {
+        if (win.fp32) win.st_hist32[d].reserve((size_t)(K + 1) * m);
+        else win.st_hist[d].reserve((size_t)(K + 1) * m);
+      }
       win.lH[d].reserve(m);
       win.gpair[d].reserve((size_t)6 * m);
       win.gpar_d[d].reserve((size_t)2 * m);
@@ -1062,10 +1082,19 @@ struct DemSim {
       const long long tc = win.t0 + (long long)c * K;
       // recompute the segment's forward states from its checkpoint
       copy_state(view4(win.st.p, n), view4(win.ck.p + (size_t)c * 4 * n, n));
+      if (win.fp32) {  // the velocity shadow of the checkpoint, as the forward kept it
+        Particles Q = P;
+        Q.buf[0] = st_view(0);
+        launch_sync_vw(Q, 0, s);
+      }
       for (int d = 0; d < nd; ++d)
-        if (dl[d]->kind == 1 && win.m[d])
-          DEM_CUDA(cudaMemcpyAsync(win.st_hist[d].p, win.ck_hist[d].p + (size_t)c * win.m[d],
-                                   sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+        if (dl[d]->kind == 1 && win.m[d]) {
+          if (win.fp32)
+            launch_hist_convert(win.m[d], win.ck_hist[d].p + (size_t)c * win.m[d], win.st_hist32[d].p, true, s);
+          else
+            DEM_CUDA(cudaMemcpyAsync(win.st_hist[d].p, win.ck_hist[d].p + (size_t)c * win.m[d],
+                                     sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+        }
       if (nw)
         DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p + (size_t)c * kMaxWalls, sizeof(WallDev) * nw,
                                  cudaMemcpyDeviceToDevice, s));
@@ -1083,31 +1112,36 @@ struct DemSim {
           DEM_CUDA(cudaMemcpyAsync(win.st_walls.p + (size_t)j * kMaxWalls, d_walls.p, sizeof(WallDev) * nw,
                                    cudaMemcpyDeviceToDevice, s));
         StepArgs a = make_args(0);
-        a.P.buf[0] = view4(win.st.p + (size_t)j * 4 * n, n);
-        a.P.buf[1] = view4(win.st.p + (size_t)(j + 1) * 4 * n, n);
+        a.P.buf[0] = st_view(j);
+        a.P.buf[1] = st_view(j + 1);
         a.cur = 0;
         for (int d = 0; d < nd; ++d)
           if (dl[d]->kind == 1) {
-            a.dyn[d].hist_in = win.st_hist[d].p + (size_t)j * std::max(win.m[d], 1);
-            a.dyn[d].hist_out = win.st_hist[d].p + (size_t)(j + 1) * std::max(win.m[d], 1);
+            const size_t m = std::max(win.m[d], 1);
+            if (win.fp32) {
+              a.dyn[d].hist32_in = win.st_hist32[d].p + j * m;
+              a.dyn[d].hist32_out = win.st_hist32[d].p + (j + 1) * m;
+            } else {
+              a.dyn[d].hist_in = win.st_hist[d].p + j * m;
+              a.dyn[d].hist_out = win.st_hist[d].p + (j + 1) * m;
+            }
           }
         a.f_int = win.st_f.p + (size_t)j * n;
         a.m_int = win.st_m.p + (size_t)j * n;
         a.damp_iters = win.st_it.p + (size_t)j * 2 * n;
         a.store_forces = 0;
         a.replay = 1;
-        launch_step(a, rot != 0, t_pp, two, s);
-        if (win.brk && n)  // the wall candidacy this step used (refreshed in it after a failure)
-          DEM_CUDA(cudaMemcpyAsync(win.st_pf.p + (size_t)j * n, P.pflags, sizeof(unsigned) * n,
-                                   cudaMemcpyDeviceToDevice, s));
+        if (win.brk) a.pf_log = win.st_pf.p + (size_t)j * n;  // the wall candidacy this step used
+        if (win.fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
+        else launch_step(a, rot != 0, t_pp, two, s);
       }
       DEM_CUDA(cudaGetLastError());
       c_launches += two ? 2LL * len : len;
       // reverse the segment
       for (int j = len - 1; j >= 0; --j) {
         A.step = tc + j + 1;
-        A.s0 = view4(win.st.p + (size_t)j * 4 * n, n);
-        A.s1 = view4(win.st.p + (size_t)(j + 1) * 4 * n, n);
+        A.s0 = st_view(j);
+        A.s1 = st_view(j + 1);
         A.f_int = win.st_f.p + (size_t)j * n;
         A.m_int = win.st_m.p + (size_t)j * n;
         A.iters = win.st_it.p + (size_t)j * 2 * n;
@@ -1115,7 +1149,11 @@ struct DemSim {
         A.pflags = win.brk ? win.st_pf.p + (size_t)j * n : P.pflags;
         A.gR = win.gR.p + (size_t)(c * K + j) * kMaxWalls * 3;
         for (int d = 0; d < nd; ++d)
-          A.dyn[d].hist_in = dl[d]->kind == 1 ? win.st_hist[d].p + (size_t)j * std::max(win.m[d], 1) : nullptr;
+          if (dl[d]->kind == 1) {
+            const size_t m = std::max(win.m[d], 1);
+            A.dyn[d].hist_in = win.fp32 ? nullptr : win.st_hist[d].p + j * m;
+            A.dyn[d].hist32_in = win.fp32 ? win.st_hist32[d].p + j * m : nullptr;
+          }
         launch_adjoint_step(A, s);
       }
       DEM_CUDA(cudaGetLastError());
@@ -1200,10 +1238,15 @@ struct DemSim {
     auto dl = dyn_list();
     cur = win.cur0;
     copy_state(P.buf[cur], view4(win.ck.p, n));
+    if (fp32) launch_sync_vw(P, cur, s);
     for (int d = 0; d < (int)dl.size(); ++d)
-      if (dl[d]->kind == 1 && win.m[d])
-        DEM_CUDA(cudaMemcpyAsync(dl[d]->hist[cur].p, win.ck_hist[d].p, sizeof(double4) * win.m[d],
-                                 cudaMemcpyDeviceToDevice, s));
+      if (dl[d]->kind == 1 && win.m[d]) {
+        if (fp32)
+          launch_hist_convert(win.m[d], win.ck_hist[d].p, dl[d]->hist32[cur].p, true, s);
+        else
+          DEM_CUDA(cudaMemcpyAsync(dl[d]->hist[cur].p, win.ck_hist[d].p, sizeof(double4) * win.m[d],
+                                   cudaMemcpyDeviceToDevice, s));
+      }
     if (!wig.empty())
       DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p, sizeof(WallDev) * wig.size(), cudaMemcpyDeviceToDevice, s));
     if (win.brk) {  // undo the window's bond failures

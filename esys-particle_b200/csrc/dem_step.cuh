@@ -346,6 +346,7 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
       if (lane == 0 && !EVAL) a.P.pflags[i] = pf;
     }
   }
+  if (a.pf_log && lane == 0 && i < a.P.n) a.pf_log[i] = pf;
 
   // 1. elastic walls, in group-name order (TSubLattice::calcForces, SubLattice.hpp:2116-2120).
   //    The walls' reactions are reduced in a fixed order: warp shuffle, then warps, then blocks.

@@ -317,3 +317,40 @@ def test_rewind_undoes_bond_failures(gpu):
         assert np.array_equal(p1[k], p2[k]), k
     a.step(5)                      # the failures are handed on to the ordinary stepping
     assert a.timestep == T + 5
+
+
+# ---- the window in the FP32-force form ----
+def test_fp32_form_window_matches_fp64_dual_numbers(gpu, orc):
+    """FP32 pair forces in the forward and its recompute (RotFriction contacts and RotBonds,
+    bonds failing inside the window under the hand-off); the reverse linearises each law in
+    FP64 at the FP32 trajectory.  Bar: 1e-4 relative of the FP64 dual-number derivatives,
+    the spec's bar against FP64 differences."""
+    a = _breaking(gpu)
+    a.set_option("precision", 32)
+    R = a.window_forward(T, 32)
+    b = S.window_block(orc, **BRK)
+    lo, hi = _seed_particles(b)
+    Rd, dR = b.window_dual(T, list(S.WINDOW_SEEDS) + [f"vel:{lo}:1", f"angvel:{hi}:0"], 2)
+    # the FP32 forces move the reactions by ~1e-7 of their scale
+    assert np.abs(R - Rd).max() <= 1e-5 * np.abs(Rd).max()
+    tgt = S.mse_target(Rd)
+    g = a.window_adjoint(S.mse_grad(R, tgt))
+    gd = np.einsum("tgc,tgck->k", S.mse_grad(Rd, tgt), dR)
+    layout = a.param_layout()
+    idx = [layout.index(k) for k in S.WINDOW_PARAMS]
+    _grad_vs(g["params"][idx], gd[:6], 1e-4)
+    _grad_vs(np.array([g["vel"][lo, 1], g["angvel"][hi, 0]]), gd[6:], 1e-4)
+
+
+def test_fp32_form_window_checkpoints_and_rewind(gpu):
+    out = []
+    for K in (1, T):
+        a = _breaking(gpu)
+        a.set_option("precision", 32)
+        R = a.window_forward(T, K)
+        tgt = S.mse_target(R)
+        out.append(a.window_adjoint(S.mse_grad(R, tgt)))
+        a.window_rewind()
+        assert np.array_equal(a.window_forward(T, K), R)
+    for k in ("params", "vel", "angvel"):
+        assert np.array_equal(out[0][k], out[1][k]), k
