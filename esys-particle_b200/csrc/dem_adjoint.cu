@@ -76,9 +76,7 @@ __device__ __forceinline__ void damping_vjp(const V& v, const V& F, double s, do
   gvisc += dot(lFtot, (-m * (G + visc * dGdvisc)) * u);
 }
 
-__global__ void k_adj_pre(const AdjArgs A) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+__device__ __forceinline__ void adj_pre_one(const AdjArgs& A, int i) {
   const unsigned pf = A.pflags[i];
   if (!(pf & PF_ALIVE)) return;
   const double dt = A.dt;
@@ -171,6 +169,11 @@ __global__ void k_adj_pre(const AdjArgs A) {
   A.gvisc[2 * i + 1] += gr;
 }
 
+__global__ void k_adj_pre(const AdjArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < A.n) adj_pre_one(A, i);
+}
+
 // Tangent slot of input gi in the pass whose inputs are [base, base + N): a unit tangent there,
 // a constant elsewhere (the slot index is compared, never used as an array index, so the dual
 // stays in registers).
@@ -238,10 +241,8 @@ __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
 
 
 // RotBond VJP by the hand-written reverse of the law (dem_bond_vjp.cuh).
-__global__ void __launch_bounds__(128) k_adj_bond_rev(const AdjArgs A, int gi) {
+__device__ __forceinline__ void adj_bond_rev_one(const AdjArgs& A, int gi, int b) {
   const AdjBond& B = A.bond[gi];
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B.nb) return;
   double4* out = B.gb + 4 * (size_t)b;
   if (B.broken_step[b] <= A.step) {  // removed before this step
     out[0] = out[1] = out[2] = out[3] = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -271,6 +272,11 @@ __global__ void __launch_bounds__(128) k_adj_bond_rev(const AdjArgs A, int gi) {
   gp[3] += g.kb * U.kb;
 }
 
+__global__ void __launch_bounds__(128) k_adj_bond_rev(const AdjArgs A, int gi) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < A.bond[gi].nb) adj_bond_rev_one(A, gi, b);
+}
+
 using D7 = Dual<7>;
 using D23 = Dual<23>;
 
@@ -279,10 +285,8 @@ __device__ __forceinline__ V3<D23> seed3(const V& a, int k) {
 }
 __device__ __forceinline__ D23 dotd(const V3<D23>& a, const V& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-__global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
+__device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   const AdjDyn& G = A.dyn[gi];
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= G.m) return;
   const unsigned long long key = G.keys[k];
   const int s1 = (int)(key >> 32), s2 = (int)(key & 0xffffffffu);
   double4* out = G.gpair + 6 * (size_t)k;
@@ -348,6 +352,11 @@ __global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
   G.gpar[2 * (size_t)k + 1] += w.d[22];
 }
 
+__global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < A.dyn[gi].m) adj_pair_one(A, gi, k);
+}
+
 __device__ __forceinline__ void add4(double4& a, const double4& b) {
   a.x += b.x;
   a.y += b.y;
@@ -355,9 +364,7 @@ __device__ __forceinline__ void add4(double4& a, const double4& b) {
   a.w += b.w;
 }
 
-__global__ void k_adj_post(const AdjArgs A) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+__device__ __forceinline__ void adj_post_one(const AdjArgs& A, int i) {
   if (!(A.pflags[i] & PF_ALIVE)) return;
   double4 gx = make_double4(0.0, 0.0, 0.0, 0.0), gv = gx, gw = gx, gq = gx;
   for (int d = 0; d < A.ndyn; ++d) {
@@ -401,6 +408,11 @@ __global__ void k_adj_post(const AdjArgs A) {
   }
 }
 
+__global__ void k_adj_post(const AdjArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < A.n) adj_post_one(A, i);
+}
+
 // acc[c] += sum over rows r of data[r * cols + c], in a fixed order (one block).
 __global__ void k_reduce_cols(const double* data, int rows, int cols, double* acc) {
   __shared__ double red[32];
@@ -442,6 +454,139 @@ void launch_adjoint_step(const AdjArgs& A, cudaStream_t s) {
 
 void launch_reduce_cols(const double* data, int rows, int cols, double* acc, cudaStream_t s) {
   if (rows > 0) k_reduce_cols<<<1, 1024, 0, s>>>(data, rows, cols, acc);
+}
+
+// ---- batched ensemble windows ----------------------------------------------------------
+
+__device__ __forceinline__ ParticleBuf win_view(const WinSpec& w, int j) {
+  const size_t n = (size_t)w.n;
+  double4* b = w.st + (size_t)j * 4 * n;
+  return ParticleBuf{b, b + n, b + 2 * n, b + 3 * n, w.st_vw ? w.st_vw + (size_t)j * 2 * (n > 0 ? n : 1) : nullptr};
+}
+
+// One thread per specimen: the base arguments with step j's buffers, and the wall planes
+// step j starts from (the recompute moves them through the wall loaders as the forward did).
+__global__ void k_window_step_expand(const StepArgs* base, StepArgs* out, const WinSpec* ws, int nspec, int j) {
+  const int sp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sp >= nspec) return;
+  const WinSpec& w = ws[sp];
+  StepArgs a = base[sp];
+  const size_t n = (size_t)w.n;
+  a.P.buf[0] = win_view(w, j);
+  a.P.buf[1] = win_view(w, j + 1);
+  a.cur = 0;
+  for (int d = 0; d < a.ndyn; ++d) {
+    const size_t h = (size_t)w.hstride[d];
+    if (w.st_hist32[d]) {
+      a.dyn[d].hist32_in = w.st_hist32[d] + j * h;
+      a.dyn[d].hist32_out = w.st_hist32[d] + (j + 1) * h;
+    } else if (w.st_hist[d]) {
+      a.dyn[d].hist_in = w.st_hist[d] + j * h;
+      a.dyn[d].hist_out = w.st_hist[d] + (j + 1) * h;
+    }
+  }
+  a.f_int = w.st_f + j * n;
+  a.m_int = w.st_m + j * n;
+  a.damp_iters = w.st_it + j * 2 * n;
+  a.pf_log = w.st_pf ? w.st_pf + j * n : nullptr;
+  a.store_forces = 0;
+  a.replay = 1;
+  a.wall_hist = nullptr;
+  out[2 * sp] = a;
+  out[2 * sp + 1] = a;
+  for (int k = 0; k < w.nwall; ++k) w.st_walls[(size_t)j * kMaxWalls + k] = w.walls[k];
+}
+
+__global__ void k_window_adj_expand(const AdjArgs* base, AdjArgs* out, const WinSpec* ws, int nspec, int c, int j) {
+  const int sp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sp >= nspec) return;
+  const WinSpec& w = ws[sp];
+  AdjArgs A = base[sp];
+  const size_t n = (size_t)w.n;
+  A.step = w.t0 + (long long)c * w.K + j + 1;
+  A.s0 = win_view(w, j);
+  A.s1 = win_view(w, j + 1);
+  A.f_int = w.st_f + j * n;
+  A.m_int = w.st_m + j * n;
+  A.iters = w.st_it + j * 2 * n;
+  A.walls = w.st_walls + (size_t)j * kMaxWalls;
+  if (w.st_pf) A.pflags = w.st_pf + j * n;
+  A.gR = w.gR + ((size_t)c * w.K + j) * kMaxWalls * 3;
+  for (int d = 0; d < A.ndyn; ++d) {
+    const size_t h = (size_t)w.hstride[d];
+    A.dyn[d].hist_in = w.st_hist[d] ? w.st_hist[d] + j * h : nullptr;
+    A.dyn[d].hist32_in = w.st_hist32[d] ? w.st_hist32[d] + j * h : nullptr;
+  }
+  out[sp] = A;
+}
+
+void launch_window_step_expand(const StepArgs* base, StepArgs* out, const WinSpec* ws, int nspec, int j,
+                               cudaStream_t s) {
+  if (nspec > 0) k_window_step_expand<<<(nspec + 63) / 64, 64, 0, s>>>(base, out, ws, nspec, j);
+}
+void launch_window_adj_expand(const AdjArgs* base, AdjArgs* out, const WinSpec* ws, int nspec, int c, int j,
+                              cudaStream_t s) {
+  if (nspec > 0) k_window_adj_expand<<<(nspec + 63) / 64, 64, 0, s>>>(base, out, ws, nspec, c, j);
+}
+
+// The item (specimen, or specimen x group) whose tile range holds `tile`: the last item whose
+// first tile is <= tile (items without tiles share their successor's first tile).
+__device__ __forceinline__ int batch_item(const int* start, int items, int tile) {
+  int lo = 0, hi = items;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(start + mid) <= tile) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_adj_pre_batch(const AdjBatch B) {
+  for (int tile = blockIdx.x; tile < B.total_ptiles; tile += gridDim.x) {
+    const int sp = batch_item(B.ptile_start, B.nspec, tile);
+    const AdjArgs& A = B.args[sp];
+    const int i = (tile - __ldg(B.ptile_start + sp)) * 256 + threadIdx.x;
+    if (i < A.n) adj_pre_one(A, i);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_adj_post_batch(const AdjBatch B) {
+  for (int tile = blockIdx.x; tile < B.total_ptiles; tile += gridDim.x) {
+    const int sp = batch_item(B.ptile_start, B.nspec, tile);
+    const AdjArgs& A = B.args[sp];
+    const int i = (tile - __ldg(B.ptile_start + sp)) * 256 + threadIdx.x;
+    if (i < A.n) adj_post_one(A, i);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_adj_bond_rev_batch(const AdjBatch B) {
+  for (int tile = blockIdx.x; tile < B.total_btiles; tile += gridDim.x) {
+    const int it = batch_item(B.btile_start, B.nspec * kMaxBond, tile);
+    const int sp = it / kMaxBond, gi = it % kMaxBond;
+    const AdjArgs& A = B.args[sp];
+    const int b = (tile - __ldg(B.btile_start + it)) * 128 + threadIdx.x;
+    if (gi < A.nbond && b < A.bond[gi].nb) adj_bond_rev_one(A, gi, b);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_adj_pair_batch(const AdjBatch B) {
+  for (int tile = blockIdx.x; tile < B.total_dtiles; tile += gridDim.x) {
+    const int it = batch_item(B.dtile_start, B.nspec * kMaxDyn, tile);
+    const int sp = it / kMaxDyn, gi = it % kMaxDyn;
+    const AdjArgs& A = B.args[sp];
+    const int k = (tile - __ldg(B.dtile_start + it)) * 128 + threadIdx.x;
+    if (gi < A.ndyn && k < A.dyn[gi].m) adj_pair_one(A, gi, k);
+  }
+}
+
+// Grids of one tile per block up to a cap; the kernels stride over any remainder.
+static inline int batch_grid(int tiles) { return tiles < 1048576 ? tiles : 1048576; }
+
+void launch_adjoint_step_batch(const AdjBatch& B, bool bonds, bool pairs, cudaStream_t s) {
+  if (B.total_ptiles <= 0) return;
+  k_adj_pre_batch<<<batch_grid(B.total_ptiles), 256, 0, s>>>(B);
+  if (bonds && B.total_btiles > 0) k_adj_bond_rev_batch<<<batch_grid(B.total_btiles), 128, 0, s>>>(B);
+  if (pairs && B.total_dtiles > 0) k_adj_pair_batch<<<batch_grid(B.total_dtiles), 128, 0, s>>>(B);
+  if (bonds || pairs) k_adj_post_batch<<<batch_grid(B.total_ptiles), 256, 0, s>>>(B);
 }
 
 }  // namespace dem

@@ -63,6 +63,46 @@ struct AdjArgs {
 };
 
 void launch_adjoint_step(const AdjArgs& A, cudaStream_t s);
+
+// ---- batched ensemble windows: every specimen's reverse step in one launch per kernel ----
+// One specimen's window buffers, indexed by the step j of the segment being reversed.
+struct WinSpec {
+  int n;                          // particles
+  int K;                          // checkpoint interval
+  long long t0;                   // step counter at the window's start
+  double4* st;                    // [K + 1][4 n] recomputed states (pr, vm, wi, qq blocks)
+  float4* st_vw;                  // [K + 1][2 n] FP32 velocity shadows (FP32 form, else null)
+  double4* st_f;                  // [K][n] pre-damping force sums
+  double4* st_m;                  // [K][n] pre-damping moment sums
+  unsigned char* st_it;           // [K][2 n] damping iterations
+  WallDev* st_walls;              // [K][kMaxWalls] wall planes during each step
+  unsigned* st_pf;                // [K][n] wall candidacy per step (bond failures inside the window, else null)
+  double4* st_hist[kMaxDyn];      // [K + 1][hstride] friction histories (FP64 form)
+  float4* st_hist32[kMaxDyn];     // the same in the FP32 form
+  int hstride[kMaxDyn];           // max(pairs, 1)
+  const double* gR;               // [T][kMaxWalls][3] loss gradient of the reactions
+  const WallDev* walls;           // live wall planes (their state before each recomputed step)
+  int nwall;
+};
+
+struct AdjBatch {
+  int nspec;
+  const AdjArgs* args;            // [nspec]: this step's reverse arguments
+  const int* ptile_start;         // [nspec + 1]: particle tiles of 256
+  int total_ptiles;
+  const int* btile_start;         // [nspec * kMaxBond + 1]: bond tiles of 128 per (specimen, group)
+  int total_btiles;
+  const int* dtile_start;         // [nspec * kMaxDyn + 1]: pair tiles of 128 per (specimen, group)
+  int total_dtiles;
+};
+
+// Step j's recompute arguments (both buffer parities) and wall planes, from each specimen's base.
+void launch_window_step_expand(const StepArgs* base, StepArgs* out, const WinSpec* ws, int nspec, int j,
+                               cudaStream_t s);
+// Step j of segment c's reverse arguments, from each specimen's base.
+void launch_window_adj_expand(const AdjArgs* base, AdjArgs* out, const WinSpec* ws, int nspec, int c, int j,
+                              cudaStream_t s);
+void launch_adjoint_step_batch(const AdjBatch& B, bool bonds, bool pairs, cudaStream_t s);
 void launch_reduce_cols(const double* data, int rows, int cols, double* acc, cudaStream_t s);
 
 }  // namespace dem

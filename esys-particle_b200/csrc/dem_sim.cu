@@ -818,6 +818,7 @@ struct DemSim {
   struct Window {
     bool valid = false;
     bool brk = false;  // bond failures may fall inside the window (device hand-off)
+    long long tcv = 0;  // step counter at the start of the segment being recomputed (copy source)
     int T = 0, K = 0, nseg = 0, n = 0, ts = 0, cur0 = 0;
     long long t0 = 0;
     int m[kMaxDyn] = {0, 0};
@@ -875,11 +876,13 @@ struct DemSim {
       throw StateError("a neighbour rebuild fell inside the differentiable window (shorten it or enlarge verletDist)");
   }
 
-  int window_forward(int T, int K, double* R_host) {
+  // Forward, in parts shared with the batched ensemble.  Prologue: the runOneStep head, the
+  // checkpoint buffers and what a rewind must put back.  False: the head failed (err is set).
+  bool win_begin(int T, int K) {
     if (T < 1 || K < 1) throw std::invalid_argument("window length and checkpoint interval must be >= 1");
     if (iter_lin > 255 || iter_rot > 255) throw std::invalid_argument("window damping needs maxIterations <= 255");
     win.valid = false;
-    if (!prepare()) return DEM_ERR_OVERFLOW;
+    if (!prepare()) return false;
     const int nd = (int)dyn.size();
     auto dl = dyn_list();
     win.T = T; win.K = std::min(K, T); win.nseg = (T + win.K - 1) / win.K; win.n = n; win.t0 = t;
@@ -910,30 +913,70 @@ struct DemSim {
       if (dl[d]->kind == 1) win.ck_hist[d].reserve((size_t)win.nseg * std::max(win.m[d], 1));
     }
     DEM_CUDA(cudaMemsetAsync(win.R.p, 0, sizeof(double) * T * kMaxWalls * 3, s));
+    if (fp32) launch_sync_vw(P, cur, s);
+    return true;
+  }
+
+  // Checkpoint c: particle records, friction histories, wall planes, and under the hand-off
+  // the wall candidacy and the last-failure record.
+  void win_checkpoint(int c) {
+    const int nd = (int)dyn.size();
+    auto dl = dyn_list();
+    copy_state(view4(win.ck.p + (size_t)c * 4 * n, n), P.buf[cur]);
+    if (win.brk) {
+      if (n) DEM_CUDA(cudaMemcpyAsync(win.ck_pf.p + (size_t)c * n, P.pflags, sizeof(unsigned) * n,
+                                      cudaMemcpyDeviceToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(win.ck_brk.p + 2 * c, d_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
+    for (int d = 0; d < nd; ++d)
+      if (dl[d]->kind == 1 && win.m[d]) {
+        if (fp32)  // FP32 records widened exactly
+          launch_hist_convert(win.m[d], win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist32[cur].p, false, s);
+        else
+          DEM_CUDA(cudaMemcpyAsync(win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist[cur].p,
+                                   sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+      }
+    if (!wig.empty())
+      DEM_CUDA(cudaMemcpyAsync(win.ck_walls.p + (size_t)c * kMaxWalls, d_walls.p, sizeof(WallDev) * wig.size(),
+                               cudaMemcpyDeviceToDevice, s));
+  }
+
+  // Segment c of len steps ended with the device counter at dev_t and control bits ctrl.
+  // The steps that ran are real steps of the simulation, whether the window stands or not.
+  void win_segment_done(int c, int len, long long dev_t, int ctrl, long long cps) {
+    const long long ran = dev_t - t;
+    if (ran < 0 || ran > len) throw StateError("device step counter out of sequence in the window");
+    t = dev_t;
+    cur = (int)((cur + ran) & 1);
+    c_steps += ran;
+    c_contacts += ran * cps;
+    pending_ctrl = ctrl;
+    window_check_ctrl(ctrl, c == win.nseg - 1 && ran == len);
+    if (ran != len) throw StateError("device step counter out of sequence in the window");
+  }
+
+  void win_finish(double* R_host) {
+    if (R_host) {
+      std::vector<double> r((size_t)win.T * kMaxWalls * 3);
+      DEM_CUDA(cudaMemcpyAsync(r.data(), win.R.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, s));
+      sync();
+      const int nw = (int)wig.size();
+      for (int k = 0; k < win.T; ++k)
+        for (int w = 0; w < nw; ++w)
+          for (int c = 0; c < 3; ++c) R_host[((size_t)k * nw + w) * 3 + c] = r[((size_t)k * kMaxWalls + w) * 3 + c];
+    }
+    win.valid = true;
+  }
+
+  int window_forward(int T, int K, double* R_host) {
+    if (!win_begin(T, K)) return DEM_ERR_OVERFLOW;
     const int t_pp = pick_tpp();
     d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
     const bool two = split == 1;
     const long long cps = contacts_per_step();
-    if (fp32) launch_sync_vw(P, cur, s);
     for (int c = 0; c < win.nseg; ++c) {
-      const int len = std::min(win.K, T - c * win.K);
-      copy_state(view4(win.ck.p + (size_t)c * 4 * n, n), P.buf[cur]);
-      if (win.brk) {
-        if (n) DEM_CUDA(cudaMemcpyAsync(win.ck_pf.p + (size_t)c * n, P.pflags, sizeof(unsigned) * n,
-                                        cudaMemcpyDeviceToDevice, s));
-        DEM_CUDA(cudaMemcpyAsync(win.ck_brk.p + 2 * c, d_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
-      }
-      for (int d = 0; d < nd; ++d)
-        if (dl[d]->kind == 1 && win.m[d]) {
-          if (fp32)  // FP32 records widened exactly
-            launch_hist_convert(win.m[d], win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist32[cur].p, false, s);
-          else
-            DEM_CUDA(cudaMemcpyAsync(win.ck_hist[d].p + (size_t)c * win.m[d], dl[d]->hist[cur].p,
-                                     sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
-        }
-      if (!wig.empty())
-        DEM_CUDA(cudaMemcpyAsync(win.ck_walls.p + (size_t)c * kMaxWalls, d_walls.p, sizeof(WallDev) * wig.size(),
-                                 cudaMemcpyDeviceToDevice, s));
+      const int len = std::min(win.K, win.T - c * win.K);
+      win_checkpoint(c);
       DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
       DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
       for (int j = 0; j < len; ++j) {
@@ -950,27 +993,9 @@ struct DemSim {
       sync();
       long long dev_t;
       std::memcpy(&dev_t, h_ctrl, sizeof(long long));
-      const int ran = (int)(dev_t - t);
-      if (ran < 0 || ran > len) throw StateError("device step counter out of sequence in the window");
-      // the steps that ran are real steps of the simulation, whether the window stands or not
-      t = dev_t;
-      cur = (cur + ran) & 1;
-      c_steps += ran;
-      c_contacts += (long long)ran * cps;
-      pending_ctrl = h_ctrl[2];
-      window_check_ctrl(h_ctrl[2], c == win.nseg - 1 && ran == len);
-      if (ran != len) throw StateError("device step counter out of sequence in the window");
+      win_segment_done(c, len, dev_t, h_ctrl[2], cps);
     }
-    if (R_host) {
-      std::vector<double> r((size_t)T * kMaxWalls * 3);
-      DEM_CUDA(cudaMemcpyAsync(r.data(), win.R.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, s));
-      sync();
-      const int nw = (int)wig.size();
-      for (int k = 0; k < T; ++k)
-        for (int w = 0; w < nw; ++w)
-          for (int c = 0; c < 3; ++c) R_host[((size_t)k * nw + w) * 3 + c] = r[((size_t)k * kMaxWalls + w) * 3 + c];
-    }
-    win.valid = true;
+    win_finish(R_host);
     return 0;
   }
 
@@ -980,11 +1005,10 @@ struct DemSim {
       throw StateError("the simulation moved on since the window was run");
   }
 
-  // Reverse pass.  gR_host: [T][nwall][3] dLoss/dReaction; grad_params: window_num_params()
-  // values (bond groups x (kr, ks, kt, kb), dynamic groups x (k, ks), linear and rotational
-  // viscosity); per-particle outputs in dem_get_particles order (any may be null).
-  void window_adjoint(const double* gR_host, double* grad_params, double* gvel, double* gang, double* gpos,
-                      double* gquat) {
+  // Reverse, in parts shared with the batched ensemble.  Prologue: buffers, the loss gradient
+  // gR_host [T][nwall][3], the live device state the recompute touches, and the reverse
+  // arguments that do not depend on the step.
+  AdjArgs adj_begin(const double* gR_host) {
     window_require();
     if (!gR_host) throw std::invalid_argument("null reaction gradient");
     const int T = win.T, K = win.K, nw = (int)wig.size();
@@ -992,7 +1016,6 @@ struct DemSim {
     auto bl = bond_list();
     const int nd = (int)dl.size(), nbg = (int)bl.size();
     const int nn = std::max(n, 1);
-    // device buffers
     win.st.reserve((size_t)(K + 1) * 4 * nn);
     if (win.fp32) win.st_vw.reserve((size_t)(K + 1) * 2 * nn);
     win.st_f.reserve((size_t)K * nn);
@@ -1041,12 +1064,8 @@ struct DemSim {
       DEM_CUDA(cudaMemcpyAsync(win.gR.p, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice, s));
       sync();
     }
-    // the live device state the recompute touches: wall planes, reactions, step counter
     if (nw) DEM_CUDA(cudaMemcpyAsync(win.save_walls.p, d_walls.p, sizeof(WallDev) * nw, cudaMemcpyDeviceToDevice, s));
     DEM_CUDA(cudaMemcpyAsync(win.save_wf.p, d_wall_force.p, sizeof(double) * kMaxWalls * 3, cudaMemcpyDeviceToDevice, s));
-    const int t_pp = pick_tpp();
-    d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
-    const bool two = split == 1;
     double4* lam = win.lam.p;
     AdjArgs A{};
     A.g = g; A.n = n; A.rot = rot; A.dt = dt; A.pflags = P.pflags;
@@ -1077,95 +1096,133 @@ struct DemSim {
       D.adj_start = B.adj_start.p; D.adj = B.adj.p;
       D.gb = win.gb[b].p; D.gpar = win.gpar_b[b].p;
     }
-    for (int c = win.nseg - 1; c >= 0; --c) {
-      const int len = std::min(K, T - c * K);
-      const long long tc = win.t0 + (long long)c * K;
-      // recompute the segment's forward states from its checkpoint
-      copy_state(view4(win.st.p, n), view4(win.ck.p + (size_t)c * 4 * n, n));
-      if (win.fp32) {  // the velocity shadow of the checkpoint, as the forward kept it
-        Particles Q = P;
-        Q.buf[0] = st_view(0);
-        launch_sync_vw(Q, 0, s);
-      }
-      for (int d = 0; d < nd; ++d)
-        if (dl[d]->kind == 1 && win.m[d]) {
-          if (win.fp32)
-            launch_hist_convert(win.m[d], win.ck_hist[d].p + (size_t)c * win.m[d], win.st_hist32[d].p, true, s);
-          else
-            DEM_CUDA(cudaMemcpyAsync(win.st_hist[d].p, win.ck_hist[d].p + (size_t)c * win.m[d],
-                                     sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
-        }
-      if (nw)
-        DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p + (size_t)c * kMaxWalls, sizeof(WallDev) * nw,
-                                 cudaMemcpyDeviceToDevice, s));
-      if (win.brk) {
-        if (n) DEM_CUDA(cudaMemcpyAsync(P.pflags, win.ck_pf.p + (size_t)c * n, sizeof(unsigned) * n,
-                                        cudaMemcpyDeviceToDevice, s));
-        DEM_CUDA(cudaMemcpyAsync(d_brk.p, win.ck_brk.p + 2 * c, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
-      }
-      long long tcv = tc;
-      DEM_CUDA(cudaMemcpyAsync(d_step.p, &tcv, sizeof(long long), cudaMemcpyHostToDevice, s));
-      DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
-      DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
-      for (int j = 0; j < len; ++j) {
-        if (nw)
-          DEM_CUDA(cudaMemcpyAsync(win.st_walls.p + (size_t)j * kMaxWalls, d_walls.p, sizeof(WallDev) * nw,
-                                   cudaMemcpyDeviceToDevice, s));
-        StepArgs a = make_args(0);
-        a.P.buf[0] = st_view(j);
-        a.P.buf[1] = st_view(j + 1);
-        a.cur = 0;
-        for (int d = 0; d < nd; ++d)
-          if (dl[d]->kind == 1) {
-            const size_t m = std::max(win.m[d], 1);
-            if (win.fp32) {
-              a.dyn[d].hist32_in = win.st_hist32[d].p + j * m;
-              a.dyn[d].hist32_out = win.st_hist32[d].p + (j + 1) * m;
-            } else {
-              a.dyn[d].hist_in = win.st_hist[d].p + j * m;
-              a.dyn[d].hist_out = win.st_hist[d].p + (j + 1) * m;
-            }
-          }
-        a.f_int = win.st_f.p + (size_t)j * n;
-        a.m_int = win.st_m.p + (size_t)j * n;
-        a.damp_iters = win.st_it.p + (size_t)j * 2 * n;
-        a.store_forces = 0;
-        a.replay = 1;
-        if (win.brk) a.pf_log = win.st_pf.p + (size_t)j * n;  // the wall candidacy this step used
-        if (win.fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
-        else launch_step(a, rot != 0, t_pp, two, s);
-      }
-      DEM_CUDA(cudaGetLastError());
-      c_launches += two ? 2LL * len : len;
-      // reverse the segment
-      for (int j = len - 1; j >= 0; --j) {
-        A.step = tc + j + 1;
-        A.s0 = st_view(j);
-        A.s1 = st_view(j + 1);
-        A.f_int = win.st_f.p + (size_t)j * n;
-        A.m_int = win.st_m.p + (size_t)j * n;
-        A.iters = win.st_it.p + (size_t)j * 2 * n;
-        A.walls = win.st_walls.p + (size_t)j * kMaxWalls;
-        A.pflags = win.brk ? win.st_pf.p + (size_t)j * n : P.pflags;
-        A.gR = win.gR.p + (size_t)(c * K + j) * kMaxWalls * 3;
-        for (int d = 0; d < nd; ++d)
-          if (dl[d]->kind == 1) {
-            const size_t m = std::max(win.m[d], 1);
-            A.dyn[d].hist_in = win.fp32 ? nullptr : win.st_hist[d].p + j * m;
-            A.dyn[d].hist32_in = win.fp32 ? win.st_hist32[d].p + j * m : nullptr;
-          }
-        launch_adjoint_step(A, s);
-      }
-      DEM_CUDA(cudaGetLastError());
+    return A;
+  }
+
+  // Segment c's start state from its checkpoint, into the recompute buffers; the device
+  // step counter at the segment's first step.
+  void adj_restore(int c) {
+    const int nd = (int)dyn.size(), nw = (int)wig.size();
+    auto dl = dyn_list();
+    copy_state(view4(win.st.p, n), view4(win.ck.p + (size_t)c * 4 * n, n));
+    if (win.fp32) {  // the velocity shadow of the checkpoint, as the forward kept it
+      Particles Q = P;
+      Q.buf[0] = st_view(0);
+      launch_sync_vw(Q, 0, s);
     }
-    // parameter gradients: one fixed-order reduction each
+    for (int d = 0; d < nd; ++d)
+      if (dl[d]->kind == 1 && win.m[d]) {
+        if (win.fp32)
+          launch_hist_convert(win.m[d], win.ck_hist[d].p + (size_t)c * win.m[d], win.st_hist32[d].p, true, s);
+        else
+          DEM_CUDA(cudaMemcpyAsync(win.st_hist[d].p, win.ck_hist[d].p + (size_t)c * win.m[d],
+                                   sizeof(double4) * win.m[d], cudaMemcpyDeviceToDevice, s));
+      }
+    if (nw)
+      DEM_CUDA(cudaMemcpyAsync(d_walls.p, win.ck_walls.p + (size_t)c * kMaxWalls, sizeof(WallDev) * nw,
+                               cudaMemcpyDeviceToDevice, s));
+    if (win.brk) {
+      if (n) DEM_CUDA(cudaMemcpyAsync(P.pflags, win.ck_pf.p + (size_t)c * n, sizeof(unsigned) * n,
+                                      cudaMemcpyDeviceToDevice, s));
+      DEM_CUDA(cudaMemcpyAsync(d_brk.p, win.ck_brk.p + 2 * c, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
+    win.tcv = win.t0 + (long long)c * win.K;
+    DEM_CUDA(cudaMemcpyAsync(d_step.p, &win.tcv, sizeof(long long), cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
+    DEM_CUDA(cudaMemsetAsync(d_stop.p, 0, sizeof(int), s));
+  }
+
+  // Step arguments of recomputed step j of a segment: state j -> j + 1 in the recompute
+  // buffers, the pre-damping sums and damping iterations stored, nothing logged again.
+  StepArgs adj_recompute_args(int j) {
+    const int nd = (int)dyn.size();
+    auto dl = dyn_list();
+    StepArgs a = make_args(0);
+    a.P.buf[0] = st_view(j);
+    a.P.buf[1] = st_view(j + 1);
+    a.cur = 0;
+    for (int d = 0; d < nd; ++d)
+      if (dl[d]->kind == 1) {
+        const size_t m = std::max(win.m[d], 1);
+        if (win.fp32) {
+          a.dyn[d].hist32_in = win.st_hist32[d].p + j * m;
+          a.dyn[d].hist32_out = win.st_hist32[d].p + (j + 1) * m;
+        } else {
+          a.dyn[d].hist_in = win.st_hist[d].p + j * m;
+          a.dyn[d].hist_out = win.st_hist[d].p + (j + 1) * m;
+        }
+      }
+    a.f_int = win.st_f.p + (size_t)j * n;
+    a.m_int = win.st_m.p + (size_t)j * n;
+    a.damp_iters = win.st_it.p + (size_t)j * 2 * n;
+    a.store_forces = 0;
+    a.replay = 1;
+    if (win.brk) a.pf_log = win.st_pf.p + (size_t)j * n;  // the wall candidacy this step used
+    return a;
+  }
+
+  // The step-dependent reverse arguments of step j of segment c.
+  void adj_fill(AdjArgs& A, int c, int j) {
+    const int nd = (int)dyn.size();
+    auto dl = dyn_list();
+    A.step = win.t0 + (long long)c * win.K + j + 1;
+    A.s0 = st_view(j);
+    A.s1 = st_view(j + 1);
+    A.f_int = win.st_f.p + (size_t)j * n;
+    A.m_int = win.st_m.p + (size_t)j * n;
+    A.iters = win.st_it.p + (size_t)j * 2 * n;
+    A.walls = win.st_walls.p + (size_t)j * kMaxWalls;
+    A.pflags = win.brk ? win.st_pf.p + (size_t)j * n : P.pflags;
+    A.gR = win.gR.p + (size_t)(c * win.K + j) * kMaxWalls * 3;
+    for (int d = 0; d < nd; ++d)
+      if (dl[d]->kind == 1) {
+        const size_t m = std::max(win.m[d], 1);
+        A.dyn[d].hist_in = win.fp32 ? nullptr : win.st_hist[d].p + j * m;
+        A.dyn[d].hist32_in = win.fp32 ? win.st_hist32[d].p + j * m : nullptr;
+      }
+  }
+
+  // The window's buffers as the batched ensemble's expansion kernels index them.
+  WinSpec win_spec() const {
+    WinSpec w{};
+    w.n = n;
+    w.K = win.K;
+    w.t0 = win.t0;
+    w.st = win.st.p;
+    w.st_vw = win.fp32 ? win.st_vw.p : nullptr;
+    w.st_f = win.st_f.p;
+    w.st_m = win.st_m.p;
+    w.st_it = win.st_it.p;
+    w.st_walls = win.st_walls.p;
+    w.st_pf = win.brk ? win.st_pf.p : nullptr;
+    w.gR = win.gR.p;
+    w.walls = d_walls.p;
+    w.nwall = (int)wig.size();
+    int d = 0;
+    for (auto& g : dyn) {
+      w.hstride[d] = std::max(win.m[d], 1);
+      if (g.second.kind == 1) {
+        w.st_hist[d] = win.fp32 ? nullptr : win.st_hist[d].p;
+        w.st_hist32[d] = win.fp32 ? win.st_hist32[d].p : nullptr;
+      }
+      ++d;
+    }
+    return w;
+  }
+
+  // Parameter reductions, the live device state put back, the gradients to the host.
+  void adj_finish(double* grad_params, double* gvel, double* gang, double* gpos, double* gquat) {
+    auto dl = dyn_list();
+    auto bl = bond_list();
+    const int nd = (int)dl.size(), nbg = (int)bl.size(), nw = (int)wig.size();
+    const int nn = std::max(n, 1);
+    double4* lam = win.lam.p;
     int off = 0;
     for (int b = 0; b < nbg; ++b, off += 4) launch_reduce_cols(win.gpar_b[b].p, bl[b]->nb, 4, win.acc.p + off, s);
     for (int d = 0; d < nd; ++d, off += 2) launch_reduce_cols(win.gpar_d[d].p, win.m[d], 2, win.acc.p + off, s);
     launch_reduce_cols(win.gvisc.p, n, 2, win.acc.p + off, s);
     off += 2;
     DEM_CUDA(cudaGetLastError());
-    // restore the live device state
     if (win.brk) {
       if (n) DEM_CUDA(cudaMemcpyAsync(P.pflags, win.save_pf.p, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, s));
       DEM_CUDA(cudaMemcpyAsync(d_brk.p, win.save_brk.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
@@ -1203,6 +1260,38 @@ struct DemSim {
       }
       ++k;
     }
+  }
+
+  // Reverse pass.  gR_host: [T][nwall][3] dLoss/dReaction; grad_params: window_num_params()
+  // values (bond groups x (kr, ks, kt, kb), dynamic groups x (k, ks), linear and rotational
+  // viscosity); per-particle outputs in dem_get_particles order (any may be null).
+  void window_adjoint(const double* gR_host, double* grad_params, double* gvel, double* gang, double* gpos,
+                      double* gquat) {
+    AdjArgs A = adj_begin(gR_host);
+    const int K = win.K, T = win.T, nw = (int)wig.size();
+    const int t_pp = pick_tpp();
+    d_wall_partial.reserve((size_t)step_grid(n, t_pp) * kMaxWalls * 3);
+    const bool two = split == 1;
+    for (int c = win.nseg - 1; c >= 0; --c) {
+      const int len = std::min(K, T - c * K);
+      adj_restore(c);  // recompute the segment's forward states from its checkpoint
+      for (int j = 0; j < len; ++j) {
+        if (nw)
+          DEM_CUDA(cudaMemcpyAsync(win.st_walls.p + (size_t)j * kMaxWalls, d_walls.p, sizeof(WallDev) * nw,
+                                   cudaMemcpyDeviceToDevice, s));
+        const StepArgs a = adj_recompute_args(j);
+        if (win.fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
+        else launch_step(a, rot != 0, t_pp, two, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+      c_launches += two ? 2LL * len : len;
+      for (int j = len - 1; j >= 0; --j) {  // reverse the segment
+        adj_fill(A, c, j);
+        launch_adjoint_step(A, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+    }
+    adj_finish(grad_params, gvel, gang, gpos, gquat);
   }
 
   void set_group_param(const std::string& group, const std::string& key, double v) {
@@ -1329,6 +1418,8 @@ struct Ensemble {
   }
   ~Ensemble() {
     if (s) cudaStreamSynchronize(s);
+    d_wbase.release(); d_wtab.release(); d_abase.release(); d_atab.release(); d_wspec.release();
+    d_ptile.release(); d_bptile.release(); d_dtile.release();
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     d_args.release(); d_tile_start.release(); d_btile_start.release(); d_base_cur.release(); d_status_ctrl.release();
     d_base_t.release(); d_target.release(); d_status_t.release();
@@ -1410,91 +1501,136 @@ struct Ensemble {
     DEM_CUDA(cudaGraphLaunch(it->second, s));
   }
 
-  int step(int nsteps) {
-    if (nsteps < 0) throw std::invalid_argument("negative step count");
+  // Families present over the specimens (the batch instance to launch).
+  void scan_families() {
+    el = fr = bd = false;
+    gather = true;
+    for (DemSim* d : sims) {
+      for (auto& g : d->dyn) (g.second.kind == 0 ? el : fr) = true;
+      if (!d->bond.empty()) {
+        bd = true;
+        if (!d->bond_pass) gather = false;
+      }
+    }
+    gather = gather && bd;
+  }
+
+  // Bond-pass tiles per (specimen, bond group) and step tiles per specimen, uploaded.
+  int upload_tiles(int t_pp, std::vector<int>& tile_start) {
     const int ns = (int)sims.size();
+    tile_start.assign(ns + 1, 0);
+    std::vector<int> btile_start((size_t)ns * kMaxBond + 1, 0);
+    for (int k = 0; k < ns; ++k) {
+      DemSim& d = *sims[k];
+      int q = 0;
+      for (auto& b : d.bond) {
+        if (q >= kMaxBond) break;
+        btile_start[(size_t)k * kMaxBond + q + 1] = (b.second.nb + kBondPassThreads - 1) / kBondPassThreads;
+        ++q;
+      }
+      tile_start[k + 1] = tile_start[k] + step_grid(d.n, t_pp);
+      d.d_wall_partial.reserve((size_t)step_grid(d.n, t_pp) * kMaxWalls * 3);
+    }
+    for (size_t it = 0; it < (size_t)ns * kMaxBond; ++it) btile_start[it + 1] += btile_start[it];
+    DEM_CUDA(cudaMemcpyAsync(d_btile_start.p, btile_start.data(), sizeof(int) * btile_start.size(),
+                             cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_tile_start.p, tile_start.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, s));
+    return btile_start[(size_t)ns * kMaxBond];
+  }
+
+  // One chunk of up to k steps for every specimen below its target: the step table (with the
+  // window's reaction record when `window`), a graph replay, and every specimen's counter and
+  // control word read back into h_t / h_ctrl.  `head`: run each unfinished specimen's
+  // runOneStep head first.  Returns false if a head failed (err is set).
+  bool run_chunk(const std::vector<long long>& target, int k, int t_pp, bool head, bool window, std::vector<long long>& cps) {
+    const int ns = (int)sims.size();
+    std::vector<int> base_cur(ns);
+    std::vector<long long> base_t(ns);
+    cps.assign(ns, 0);
+    if (head)
+      for (int q = 0; q < ns; ++q) {
+        DemSim& d = *sims[q];
+        if (d.t < target[q] && !d.prepare()) { err = "specimen " + std::to_string(q) + ": " + d.err; return false; }
+      }
+    // tiles after the heads (bond counts may change), step arguments after the tiles (the
+    // wall-partial scratch they point to is sized there)
+    scan_families();
+    std::vector<int> tile_start;
+    const int total_btiles = upload_tiles(t_pp, tile_start);
+    for (int q = 0; q < ns; ++q) {
+      DemSim& d = *sims[q];
+      h_args[2 * q] = d.make_args(0);
+      h_args[2 * q + 1] = d.make_args(1);
+      h_args[2 * q].store_forces = h_args[2 * q + 1].store_forces = d.store_forces;
+      if (window) {
+        for (int c = 0; c < 2; ++c) {
+          h_args[2 * q + c].wall_hist = d.win.R.p;
+          h_args[2 * q + c].wall_hist_t0 = d.win.t0;
+        }
+      }
+      base_cur[q] = d.cur;
+      base_t[q] = d.t;
+      cps[q] = d.contacts_per_step();
+    }
+    DEM_CUDA(cudaMemcpyAsync(d_args.p, h_args, sizeof(StepArgs) * 2 * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_base_cur.p, base_cur.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_base_t.p, base_t.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_target.p, target.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
+    launch_batch_reset(d_args.p, ns, s);
+    if (fp32) launch_batch_sync_vw(d_args.p, d_base_cur.p, ns, s);
+    BatchArgs B{};
+    B.nspec = ns;
+    B.total_tiles = tile_start[ns];
+    B.args = d_args.p;
+    B.tile_start = d_tile_start.p;
+    B.base_t = d_base_t.p;
+    B.base_cur = d_base_cur.p;
+    B.target = d_target.p;
+    B.btile_start = d_btile_start.p;
+    B.total_btiles = total_btiles;
+    if (profile) {
+      if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
+      DEM_CUDA(cudaEventRecord(ev0, s));
+    }
+    launch_chunk(B, k, t_pp);
+    if (profile) DEM_CUDA(cudaEventRecord(ev1, s));
+    launch_batch_status(d_args.p, ns, d_status_t.p, d_status_ctrl.p, s);
+    DEM_CUDA(cudaMemcpyAsync(h_t, d_status_t.p, sizeof(long long) * ns, cudaMemcpyDeviceToHost, s));
+    DEM_CUDA(cudaMemcpyAsync(h_ctrl, d_status_ctrl.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+    DEM_CUDA(cudaStreamSynchronize(s));
+    c_launches += k + 3 + (fp32 ? 1 : 0);
+    ++c_chunks;
+    if (profile) {
+      float ms = 0.f;
+      DEM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      prof_ms += ms;
+      prof_steps += k;
+    }
+    return true;
+  }
+
+  void check_form() {
     fp32 = sims[0]->fp32;
     for (DemSim* d : sims)
       if (d->fp32 != fp32) throw std::invalid_argument("ensemble specimens must share the precision form");
+  }
+
+  int step(int nsteps) {
+    if (nsteps < 0) throw std::invalid_argument("negative step count");
+    const int ns = (int)sims.size();
+    check_form();
     borrow();
     struct Back { Ensemble* e; ~Back() { e->give_back(); } } back{this};
     std::vector<long long> target(ns);
     for (int k = 0; k < ns; ++k) target[k] = sims[k]->t + nsteps;
     const int t_pp = pick_tpp();
+    std::vector<long long> cps;
     while (true) {
       long long remaining = 0;
       for (int k = 0; k < ns; ++k) remaining = std::max(remaining, target[k] - sims[k]->t);
       if (remaining <= 0) break;
-      // every unfinished specimen's runOneStep head (its own rebuild / interaction update)
-      el = fr = bd = false;
-      gather = true;
-      std::vector<int> tile_start(ns + 1, 0);
-      std::vector<int> btile_start((size_t)ns * kMaxBond + 1, 0);
-      std::vector<int> base_cur(ns);
-      std::vector<long long> base_t(ns);
-      std::vector<long long> cps(ns);
-      for (int k = 0; k < ns; ++k) {
-        DemSim& d = *sims[k];
-        if (d.t < target[k]) {
-          if (!d.prepare()) { err = "specimen " + std::to_string(k) + ": " + d.err; return DEM_ERR_OVERFLOW; }
-        }
-        for (auto& g : d.dyn) (g.second.kind == 0 ? el : fr) = true;
-        if (!d.bond.empty()) {
-          bd = true;
-          if (!d.bond_pass) gather = false;
-        }
-        {
-          int q = 0;
-          for (auto& b : d.bond) {
-            if (q >= kMaxBond) break;
-            const size_t it = (size_t)k * kMaxBond + q;
-            btile_start[it + 1] = (b.second.nb + kBondPassThreads - 1) / kBondPassThreads;
-            ++q;
-          }
-        }
-        tile_start[k + 1] = tile_start[k] + step_grid(d.n, t_pp);
-        d.d_wall_partial.reserve((size_t)step_grid(d.n, t_pp) * kMaxWalls * 3);
-        h_args[2 * k] = d.make_args(0);
-        h_args[2 * k + 1] = d.make_args(1);
-        h_args[2 * k].store_forces = h_args[2 * k + 1].store_forces = d.store_forces;
-        base_cur[k] = d.cur;
-        base_t[k] = d.t;
-        cps[k] = d.contacts_per_step();
-      }
-      gather = gather && bd;
-      for (size_t it = 0; it < (size_t)ns * kMaxBond; ++it) btile_start[it + 1] += btile_start[it];
-      DEM_CUDA(cudaMemcpyAsync(d_btile_start.p, btile_start.data(), sizeof(int) * btile_start.size(),
-                               cudaMemcpyHostToDevice, s));
-      DEM_CUDA(cudaMemcpyAsync(d_args.p, h_args, sizeof(StepArgs) * 2 * ns, cudaMemcpyHostToDevice, s));
-      DEM_CUDA(cudaMemcpyAsync(d_tile_start.p, tile_start.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, s));
-      DEM_CUDA(cudaMemcpyAsync(d_base_cur.p, base_cur.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
-      DEM_CUDA(cudaMemcpyAsync(d_base_t.p, base_t.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
-      DEM_CUDA(cudaMemcpyAsync(d_target.p, target.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
-      launch_batch_reset(d_args.p, ns, s);
-      if (fp32) launch_batch_sync_vw(d_args.p, d_base_cur.p, ns, s);
       const int k = (int)std::min<long long>(chunk, remaining);
-      BatchArgs B{};
-      B.nspec = ns;
-      B.total_tiles = tile_start[ns];
-      B.args = d_args.p;
-      B.tile_start = d_tile_start.p;
-      B.base_t = d_base_t.p;
-      B.base_cur = d_base_cur.p;
-      B.target = d_target.p;
-      B.btile_start = d_btile_start.p;
-      B.total_btiles = btile_start[(size_t)ns * kMaxBond];
-      if (profile) {
-        if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
-        DEM_CUDA(cudaEventRecord(ev0, s));
-      }
-      launch_chunk(B, k, t_pp);
-      if (profile) DEM_CUDA(cudaEventRecord(ev1, s));
-      launch_batch_status(d_args.p, ns, d_status_t.p, d_status_ctrl.p, s);
-      DEM_CUDA(cudaMemcpyAsync(h_t, d_status_t.p, sizeof(long long) * ns, cudaMemcpyDeviceToHost, s));
-      DEM_CUDA(cudaMemcpyAsync(h_ctrl, d_status_ctrl.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
-      DEM_CUDA(cudaStreamSynchronize(s));
-      c_launches += k + 3 + (fp32 ? 1 : 0);
-      ++c_chunks;
+      if (!run_chunk(target, k, t_pp, true, false, cps)) return DEM_ERR_OVERFLOW;
       long long ran_total = 0;
       for (int j = 0; j < ns; ++j) {
         DemSim& d = *sims[j];
@@ -1510,14 +1646,146 @@ struct Ensemble {
         ran_total += ran;
         if (h_ctrl[j] & CTRL_REBUILD) ++c_rebuild_calls;
       }
-      if (profile) {
-        float ms = 0.f;
-        DEM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-        prof_ms += ms;
-        prof_steps += k;
-      }
       if (ran_total == 0) { err = "no specimen advanced in a chunk"; return -3; }
     }
+    return 0;
+  }
+
+  // ---- batched differentiable windows --------------------------------------------------
+  // Every specimen runs the same window (nsteps from its own current step, checkpoints every
+  // K) as DemSim::window_forward would alone: the forward in batched chunks, one per
+  // checkpoint segment; the reverse with one launch per kernel and step for all specimens,
+  // the per-step arguments expanded on the device from each specimen's base.
+  DBuf<StepArgs> d_wbase, d_wtab;
+  DBuf<AdjArgs> d_abase, d_atab;
+  DBuf<WinSpec> d_wspec;
+  DBuf<int> d_ptile, d_bptile, d_dtile;
+
+  static std::string where(int k, const std::string& what) { return "specimen " + std::to_string(k) + ": " + what; }
+
+  int window_forward(int T, int K, double* const* R) {
+    const int ns = (int)sims.size();
+    check_form();
+    borrow();
+    struct Back { Ensemble* e; ~Back() { e->give_back(); } } back{this};
+    for (int k = 0; k < ns; ++k) {
+      try {
+        if (!sims[k]->win_begin(T, K)) { err = where(k, sims[k]->err); return DEM_ERR_OVERFLOW; }
+      } catch (const StateError& e) { throw StateError(where(k, e.what())); }
+    }
+    const int Kc = sims[0]->win.K, nseg = sims[0]->win.nseg;
+    const int t_pp = pick_tpp();
+    std::vector<long long> target(ns), cps;
+    for (int c = 0; c < nseg; ++c) {
+      const int len = std::min(Kc, T - c * Kc);
+      for (int k = 0; k < ns; ++k) {
+        sims[k]->win_checkpoint(c);
+        target[k] = sims[k]->t + len;
+      }
+      run_chunk(target, len, t_pp, false, true, cps);
+      for (int k = 0; k < ns; ++k) {
+        try {
+          sims[k]->win_segment_done(c, len, h_t[k], h_ctrl[k], cps[k]);
+        } catch (const StateError& e) { throw StateError(where(k, e.what())); }
+        c_steps += len;
+        c_contacts += len * cps[k];
+      }
+    }
+    for (int k = 0; k < ns; ++k) sims[k]->win_finish(R ? R[k] : nullptr);
+    return 0;
+  }
+
+  int window_adjoint(const double* const* gR, double* const* grad_params, double* const* gvel,
+                     double* const* gang) {
+    const int ns = (int)sims.size();
+    if (!gR) throw std::invalid_argument("null reaction gradients");
+    check_form();
+    for (int k = 0; k < ns; ++k) {
+      sims[k]->window_require();
+      if (sims[k]->win.T != sims[0]->win.T || sims[k]->win.K != sims[0]->win.K)
+        throw StateError(where(k, "its window differs from the other specimens'"));
+    }
+    borrow();
+    struct Back { Ensemble* e; ~Back() { e->give_back(); } } back{this};
+    const int T = sims[0]->win.T, K = sims[0]->win.K, nseg = sims[0]->win.nseg;
+    const int t_pp = pick_tpp();
+    std::vector<AdjArgs> abase(ns);
+    std::vector<WinSpec> spec(ns);
+    std::vector<int> ptile(ns + 1, 0), bptile((size_t)ns * kMaxBond + 1, 0), dtile((size_t)ns * kMaxDyn + 1, 0);
+    bool bonds = false, pairs = false;
+    scan_families();
+    std::vector<int> tile_start;
+    const int total_btiles = upload_tiles(t_pp, tile_start);  // sizes the wall-partial scratch make_args points to
+    for (int k = 0; k < ns; ++k) {
+      DemSim& d = *sims[k];
+      abase[k] = d.adj_begin(gR[k]);
+      spec[k] = d.win_spec();
+      h_args[k] = d.make_args(0);  // the recompute's base: live groups, walls, counters
+      ptile[k + 1] = ptile[k] + (d.n + 255) / 256;
+      for (int b = 0; b < abase[k].nbond; ++b) {
+        bptile[(size_t)k * kMaxBond + b + 1] = (abase[k].bond[b].nb + 127) / 128;
+        bonds = bonds || abase[k].bond[b].nb > 0;
+      }
+      for (int g = 0; g < abase[k].ndyn; ++g) {
+        dtile[(size_t)k * kMaxDyn + g + 1] = (abase[k].dyn[g].m + 127) / 128;
+        pairs = pairs || abase[k].dyn[g].m > 0;
+      }
+    }
+    for (size_t it = 0; it < (size_t)ns * kMaxBond; ++it) bptile[it + 1] += bptile[it];
+    for (size_t it = 0; it < (size_t)ns * kMaxDyn; ++it) dtile[it + 1] += dtile[it];
+    d_wbase.reserve(ns); d_wtab.reserve((size_t)2 * ns); d_abase.reserve(ns); d_atab.reserve(ns); d_wspec.reserve(ns);
+    d_ptile.reserve(ns + 1); d_bptile.reserve((size_t)ns * kMaxBond + 1); d_dtile.reserve((size_t)ns * kMaxDyn + 1);
+    DEM_CUDA(cudaMemcpyAsync(d_wbase.p, h_args, sizeof(StepArgs) * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_abase.p, abase.data(), sizeof(AdjArgs) * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_wspec.p, spec.data(), sizeof(WinSpec) * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_ptile.p, ptile.data(), sizeof(int) * ptile.size(), cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_bptile.p, bptile.data(), sizeof(int) * bptile.size(), cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_dtile.p, dtile.data(), sizeof(int) * dtile.size(), cudaMemcpyHostToDevice, s));
+    std::vector<int> zeros(ns, 0);
+    std::vector<long long> zt(ns, 0), target(ns);
+    DEM_CUDA(cudaMemcpyAsync(d_base_cur.p, zeros.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+    DEM_CUDA(cudaMemcpyAsync(d_base_t.p, zt.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
+    BatchArgs B{};
+    B.nspec = ns;
+    B.total_tiles = tile_start[ns];
+    B.args = d_wtab.p;
+    B.tile_start = d_tile_start.p;
+    B.base_t = d_base_t.p;
+    B.base_cur = d_base_cur.p;
+    B.target = d_target.p;
+    B.btile_start = d_btile_start.p;
+    B.total_btiles = total_btiles;
+    AdjBatch AB{};
+    AB.nspec = ns;
+    AB.args = d_atab.p;
+    AB.ptile_start = d_ptile.p;
+    AB.total_ptiles = ptile[ns];
+    AB.btile_start = d_bptile.p;
+    AB.total_btiles = bptile[(size_t)ns * kMaxBond];
+    AB.dtile_start = d_dtile.p;
+    AB.total_dtiles = dtile[(size_t)ns * kMaxDyn];
+    for (int c = nseg - 1; c >= 0; --c) {
+      const int len = std::min(K, T - c * K);
+      for (int k = 0; k < ns; ++k) {
+        sims[k]->adj_restore(c);
+        target[k] = sims[k]->win.t0 + (long long)c * K + len;
+      }
+      DEM_CUDA(cudaMemcpyAsync(d_target.p, target.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s));
+      for (int j = 0; j < len; ++j) {  // recompute every specimen's segment, one step at a time
+        launch_window_step_expand(d_wbase.p, d_wtab.p, d_wspec.p, ns, j, s);
+        if (fp32) launch_batch_step_fp32(B, rot != 0, el, fr, bd, gather, t_pp, s);
+        else launch_batch_step(B, rot != 0, el, fr, bd, gather, t_pp, s);
+      }
+      for (int j = len - 1; j >= 0; --j) {  // and reverse it
+        launch_window_adj_expand(d_abase.p, d_atab.p, d_wspec.p, ns, c, j, s);
+        launch_adjoint_step_batch(AB, bonds, pairs, s);
+      }
+      DEM_CUDA(cudaGetLastError());
+      c_launches += (long long)len * (3 + (gather ? 1 : 0)) + (long long)len * (2 + (bonds ? 1 : 0) + (pairs ? 1 : 0) + ((bonds || pairs) ? 1 : 0));
+    }
+    for (int k = 0; k < ns; ++k)
+      sims[k]->adj_finish(grad_params ? grad_params[k] : nullptr, gvel ? gvel[k] : nullptr,
+                          gang ? gang[k] : nullptr, nullptr, nullptr);
     return 0;
   }
 };
@@ -2259,6 +2527,15 @@ extern "C" {
 
 int dem_ensemble_step(dem_ensemble* h, int nsteps) {
   return eguard(h, [&](dem::Ensemble& e) { return e.step(nsteps); });
+}
+
+int dem_ensemble_window_forward(dem_ensemble* h, int nsteps, int checkpoint_every, double* const* reactions) {
+  return eguard(h, [&](dem::Ensemble& e) { return e.window_forward(nsteps, checkpoint_every, reactions); });
+}
+
+int dem_ensemble_window_adjoint(dem_ensemble* h, const double* const* grad_reactions, double* const* grad_params,
+                                double* const* grad_vel, double* const* grad_angvel) {
+  return eguard(h, [&](dem::Ensemble& e) { return e.window_adjoint(grad_reactions, grad_params, grad_vel, grad_angvel); });
 }
 
 int dem_ensemble_set_option(dem_ensemble* h, const char* key, double value) {

@@ -67,6 +67,8 @@ SIGNATURES = {
     "dem_ensemble_destroy": (C.c_int, [_P]),
     "dem_ensemble_last_error": (_S, [_P]),
     "dem_ensemble_step": (C.c_int, [_P, C.c_int]),
+    "dem_ensemble_window_forward": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_D)]),
+    "dem_ensemble_window_adjoint": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "dem_ensemble_set_option": (C.c_int, [_P, _S, C.c_double]),
     "dem_ensemble_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
 }
@@ -420,6 +422,40 @@ class Ensemble:
 
     def set_option(self, key, value):
         self._chk(self.lib.dem_ensemble_set_option(self.h, key.encode(), float(value)))
+
+    @staticmethod
+    def _ptrs(arrays):
+        return (_D * len(arrays))(*[_dp(a) for a in arrays])
+
+    def window_forward(self, nsteps, checkpoint_every=100):
+        """Every specimen's differentiable window (dem_ensemble_window_forward); returns each
+        specimen's wall-group reactions [nsteps, groups, 3]."""
+        R = [np.zeros((int(nsteps), len(x.wall_groups), 3)) for x in self.sims]
+        self._chk(self.lib.dem_ensemble_window_forward(self.h, int(nsteps), int(checkpoint_every), self._ptrs(R)))
+        return R
+
+    def window_adjoint(self, grad_reactions):
+        """Batched reverse pass (dem_ensemble_window_adjoint).  Returns per specimen the
+        parameter gradients and dLoss/d(initial vel, angvel), rows sorted by particle id."""
+        g = [np.ascontiguousarray(x, dtype=np.float64) for x in grad_reactions]
+        if len(g) != len(self.sims):
+            raise DemError("one reaction gradient per specimen")
+        outs = []
+        for x in self.sims:
+            n = x.num_particles()
+            outs.append({"params": np.zeros(x.window_num_params()), "vel": np.zeros((n, 3)),
+                         "angvel": np.zeros((n, 3))})
+        self._chk(self.lib.dem_ensemble_window_adjoint(
+            self.h, self._ptrs(g), self._ptrs([o["params"] for o in outs]), self._ptrs([o["vel"] for o in outs]),
+            self._ptrs([o["angvel"] for o in outs])))
+        for x, o in zip(self.sims, outs):
+            ids = np.zeros(x.num_particles(), np.int32)
+            x._chk(x.lib.dem_get_particles(x.h, _ip(ids), None, None, None, None, None, None))
+            order = np.argsort(ids, kind="stable")
+            o["id"] = ids[order]
+            o["vel"] = o["vel"][order]
+            o["angvel"] = o["angvel"][order]
+        return outs
 
     def counters(self):
         out = (C.c_longlong * 8)()

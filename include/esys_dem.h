@@ -265,6 +265,21 @@ const char* dem_ensemble_last_error(dem_ensemble* e);
 /* nsteps timesteps of every specimen (each runs its own runOneStep sequence). */
 int dem_ensemble_step(dem_ensemble* e, int nsteps);
 
+/* Batched differentiable windows: every specimen runs dem_window_forward(nsteps,
+ * checkpoint_every) from its own current step, the forward in batched launches; reactions[k]
+ * (may be null, as may the array) receives specimen k's [nsteps][wall groups][3] reactions.
+ * A failure of any specimen (a rebuild inside the window, ...) fails the call with the
+ * specimen's index in the message. */
+int dem_ensemble_window_forward(dem_ensemble* e, int nsteps, int checkpoint_every, double* const* reactions);
+
+/* The reverse pass of every specimen's last window together: one launch per reverse kernel
+ * and timestep covers all specimens (recompute included).  Per specimen k, grad_reactions[k]
+ * is its dLoss/dReaction as in dem_window_adjoint; grad_params[k] (dem_window_num_params
+ * values), grad_vel[k] and grad_angvel[k] (n x 3) receive its gradients (any may be null).
+ * Results equal each specimen's own dem_window_adjoint. */
+int dem_ensemble_window_adjoint(dem_ensemble* e, const double* const* grad_reactions, double* const* grad_params,
+                                double* const* grad_vel, double* const* grad_angvel);
+
 /* "threads_per_particle" (0 automatic, 1, 2, 4, 8), "chunk" (timesteps per graph replay),
  * "graph" (1 replay captured graphs, 0 plain launches), "profile" (CUDA-event timing). */
 int dem_ensemble_set_option(dem_ensemble* e, const char* key, double value);
