@@ -323,7 +323,81 @@ def cylinder_sim(make, sp, grid=2.2, skin=0.2):
     return sim
 
 
-def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None):
+def window_bytes(n, m, nb, T, K):
+    """Device bytes of one specimen's window: checkpoints every K of T steps (particle records,
+    friction histories, wall candidacy) and the reverse pass's recompute of K + 1 states (records,
+    FP32 velocity shadows and histories), pre-damping sums, damping counts and adjoints."""
+    nseg = -(-T // K)
+    return (n * (nseg * 132 + (K + 1) * 160 + K * 70 + 256) + m * (nseg * 32 + (K + 1) * 16 + 240)
+            + nb * 170)
+
+
+def ensemble_window_leg(sims, tpp, nsteps, every):
+    """Batched differentiable window over the last ``nsteps`` steps of every specimen (FP32
+    forces, FP64 integration and reverse): the window forward in batched chunks, then the
+    reverse pass with one launch per kernel and step for all specimens of a batch.  Specimens
+    are taken in batches that fit the free device memory.  Loss per specimen: MSE of its
+    platen reactions vs a seeded ramp."""
+    import torch
+
+    from esys.lsm import _capi
+
+    for s in sims:  # a fresh neighbour search: the whole verletDist/2 budget for the window
+        s.search_neighbors()
+    sizes = []
+    for s in sims:
+        n = s.num_particles()
+        nb = len(s.pairs("bonds")[0])
+        m = len(s.pairs("friction")[0]) + nb  # the friction list also holds the bond-excluded pairs
+        sizes.append(window_bytes(n, m, nb, nsteps, every))
+    budget = 0.6 * torch.cuda.mem_get_info()[0]
+    batches, cur, used = [], [], 0
+    for k, b in enumerate(sizes):
+        if cur and used + b > budget:
+            batches.append(cur)
+            cur, used = [], 0
+        cur.append(k)
+        used += b
+    if cur:
+        batches.append(cur)
+    t_fwd = t_rev = 0.0
+    comps = 0
+    loss = 0.0
+    for grp in batches:
+        e = _capi.Ensemble([sims[k] for k in grp])
+        e.set_option("threads_per_particle", tpp)
+        t0 = time.perf_counter()
+        R = e.window_forward(nsteps, every)
+        t1 = time.perf_counter()
+        gR = []
+        for r in R:
+            tgt = window_target(r)
+            loss += float(((r - tgt) ** 2).mean())
+            gR.append(2.0 * (r - tgt) / r.size)
+        G = e.window_adjoint(gR)
+        t2 = time.perf_counter()
+        t_fwd += t1 - t0
+        t_rev += t2 - t1
+        comps += sum(len(g["params"]) + g["vel"].size for g in G)
+        e.close()
+        for k in grp:
+            sims[k].window_release()
+    return {
+        "workload": f"last {nsteps} steps of every specimen, checkpoints every {every}, "
+                    f"{len(batches)} batch(es) by device memory",
+        "loss": "per specimen: MSE of its platen reactions vs a seeded ramp",
+        "dtype": "f32-forces/f64-integration forward and recompute, f64 reverse",
+        "specimens": len(sims), "batches": len(batches), "window_bytes_estimate": int(sum(sizes)),
+        "gradient_components": comps, "forward_with_checkpoints_s": t_fwd, "reverse_sweep_s": t_rev,
+        "adjoint_grads_per_s": comps / (t_fwd + t_rev),
+        # central differences: each batched forward window yields one perturbed loss per specimen
+        "fd_grads_per_s": len(sims) / (2.0 * t_fwd),
+        "adjoint_vs_fd_speedup": (comps / (t_fwd + t_rev)) / (len(sims) / (2.0 * t_fwd)),
+        "loss_sum": loss,
+    }
+
+
+def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window=200, window_every=20):
     """FP32-force batched ensemble (autotuned, graph-replayed) vs the plain FP64 GPU form
     (each specimen stepped by itself).  Under torchrun each rank takes a size-balanced share of
     the specimens (no exchange while they run); counts are summed and times maxed at the end."""
@@ -378,6 +452,12 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None):
         s.set_option("precision", 32)
     breaks = int(sum(len(s.breaks()[0]) for s in sims))
     e.close()
+    adj = None
+    if window > 0:
+        try:
+            adj = ensemble_window_leg(sims, best["threads_per_particle"], window, window_every)
+        except _capi.DemError as x:
+            adj = {"failed": str(x)}
     for s in sims:
         s.close()
     # plain FP64 GPU form: a size-stratified sample of the specimens, each stepped alone
@@ -418,6 +498,7 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None):
         "scaling": "weak over specimens: each GPU advances its size-balanced share, no exchange" if world > 1
                    else "single GPU",
         "speedup_vs_plain_fp64": value / plain,
+        "batched_adjoint": adj,
     }
 
 
@@ -461,6 +542,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-window leg")
     ap.add_argument("--ensemble-specimens", type=int, default=512, help="0 skips the batched-ensemble leg")
     ap.add_argument("--ensemble-steps", type=int, default=1000, help="timed timesteps of the ensemble leg")
+    ap.add_argument("--ensemble-window", type=int, default=200,
+                    help="steps of the batched differentiable window after the ensemble run (0 skips)")
+    ap.add_argument("--ensemble-window-every", type=int, default=20, help="checkpoint interval of that window")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
                     help="step kernels: -1 automatic, 0 fused, 1 pair kernel + integration kernel")
     args = ap.parse_args()
@@ -602,7 +686,8 @@ def main():
         adj = adjoint_leg(stream)
     ens = None
     if args.ensemble_specimens > 0:
-        ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps, dist=dist)
+        ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps, dist=dist, window=args.ensemble_window,
+                           window_every=args.ensemble_window_every)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

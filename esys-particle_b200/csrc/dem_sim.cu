@@ -2471,6 +2471,21 @@ int dem_window_rewind(dem_sim* h) {
   });
 }
 
+int dem_window_release(dem_sim* h) {
+  return guard(h, [&](DemSim& s) {
+    s.sync();
+    s.win.release();
+    return DEM_OK;
+  });
+}
+
+int dem_search_neighbors(dem_sim* h) {
+  return guard(h, [&](DemSim& s) {
+    s.pending_ctrl |= dem::CTRL_REBUILD;
+    return DEM_OK;
+  });
+}
+
 int dem_ensemble_create(dem_ensemble** out, dem_sim* const* sims, int n) {
   if (!out) return DEM_ERR_ARG;
   *out = nullptr;

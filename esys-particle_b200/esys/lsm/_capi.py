@@ -67,6 +67,8 @@ SIGNATURES = {
     "dem_ensemble_destroy": (C.c_int, [_P]),
     "dem_ensemble_last_error": (_S, [_P]),
     "dem_ensemble_step": (C.c_int, [_P, C.c_int]),
+    "dem_search_neighbors": (C.c_int, [_P]),
+    "dem_window_release": (C.c_int, [_P]),
     "dem_ensemble_window_forward": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_D)]),
     "dem_ensemble_window_adjoint": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "dem_ensemble_set_option": (C.c_int, [_P, _S, C.c_double]),
@@ -393,6 +395,15 @@ class DemSim:
 
     def window_rewind(self):
         self._chk(self.lib.dem_window_rewind(self.h))
+
+    def window_release(self):
+        """Free the last window's checkpoints and reverse-pass buffers."""
+        self._chk(self.lib.dem_window_release(self.h))
+
+    def search_neighbors(self):
+        """Neighbour search and interaction update at the head of the next step (force-neutral;
+        restarts the verletDist/2 displacement budget)."""
+        self._chk(self.lib.dem_search_neighbors(self.h))
 
 
 class Ensemble:

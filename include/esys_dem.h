@@ -100,6 +100,14 @@ int dem_set_timestep(dem_sim* h, double dt);
  * integrate).  Field savers and Python runnables are the caller's. */
 int dem_step(dem_sim* h, int nsteps);
 
+/* ASubLattice::searchNeighbors (Parallel/ASubLattice.h; TSubLattice::searchNeighbors,
+ * Parallel/SubLattice.hpp:2360-2408) on demand: the neighbour search and interaction update
+ * that a displacement beyond verletDist/2 triggers, run at the head of the next step.  It
+ * changes no force (pairs that leave the lists are not touching; pairs that join start with
+ * the zero history they would have); it restarts the displacement budget, e.g. before a
+ * differentiable window. */
+int dem_search_neighbors(dem_sim* h);
+
 /* TSubLattice::moveWallBy (Parallel/SubLattice.hpp:2878-2895) -> CWall::moveBy (Model/Wall.h:54-60). */
 int dem_move_wall(dem_sim* h, const char* name, const double* d);
 
@@ -249,6 +257,9 @@ int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_pa
  * planes, timestep, and the bond failures, event log and wall candidacy the window changed),
  * so that the window can be run again with other parameters. */
 int dem_window_rewind(dem_sim* h);
+
+/* Frees the last window's checkpoints and reverse-pass buffers (no rewind or adjoint after). */
+int dem_window_release(dem_sim* h);
 
 /* ---- Batched ensemble --------------------------------------------------------------------
  * No counterpart in the reference, where each specimen is its own MPI job.  An ensemble advances

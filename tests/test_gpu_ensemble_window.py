@@ -80,3 +80,23 @@ def test_ensemble_window_names_the_failing_specimen(gpu):
     with pytest.raises(DemError, match="specimen 1: a bond broke"):
         e.window_forward(T, K)
     e.close()
+
+
+def test_search_neighbors_is_force_neutral(gpu):
+    """An extra neighbour search (dem_search_neighbors) changes no force: only non-touching
+    pairs leave or join the lists.  Per-particle sums may regroup (lanes take other pairs),
+    so the bar is the last bits, 1e-12 of each field's scale after 60 steps."""
+    a, b = _specimens(gpu, 64, strengths=(2000.0,))[0], _specimens(gpu, 64, strengths=(2000.0,))[0]
+    a.step(20)
+    b.step(20)
+    c0 = b.counters()["rebuilds"] - a.counters()["rebuilds"]
+    b.search_neighbors()
+    a.step(60)
+    b.step(60)
+    assert b.counters()["rebuilds"] - a.counters()["rebuilds"] == c0 + 1
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel", "angvel"):
+        scale = np.abs(pa[k]).max()
+        assert np.abs(pa[k] - pb[k]).max() <= 1e-12 * scale, k
+    for u, v in zip(a.breaks(), b.breaks()):
+        assert np.array_equal(u, v)
