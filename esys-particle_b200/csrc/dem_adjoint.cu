@@ -33,6 +33,7 @@
 #include "dem_common.cuh"
 #include "dem_dual.cuh"
 #include "dem_bond_vjp.cuh"
+#include "dem_pair_vjp.cuh"
 #include "dem_laws.cuh"
 
 namespace dem {
@@ -302,6 +303,47 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   const V x1d = xyzv(pa), x2d = image_of(A.g, x1d, xyzv(pb));
   const V lF1 = xyzv(A.lF[s1]), lF2 = xyzv(A.lF[s2]);
   for (int c = 0; c < 6; ++c) out[c] = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (!A.pair_duals) {  // hand-written reverse of the law (dem_pair_vjp.cuh), the default
+    if (G.kind == 0) {
+      ElasticVjp e;
+      law_elastic_vjp(elastic_k(G.k, G.scaling, pa.w, pb.w), x1d, pa.w, x2d, pb.w, lF2 - lF1, e);
+      if (!e.touching) return;
+      out[0] = d4(e.x1, 0.0);
+      out[1] = d4(e.x2, 0.0);
+      G.gpar[2 * (size_t)k] += e.k_eff * elastic_k(1.0, G.scaling, pa.w, pb.w);  // k_eff = k x factor
+      return;
+    }
+    double4 h;
+    if (G.hist32_in) {
+      const float4 f = G.hist32_in[k];
+      h = make_double4(f.x, f.y, f.z, f.w);
+    } else {
+      h = G.hist_in[k];
+    }
+    double keff, kseff, uk, uks;
+    friction_k(G.k, G.ks, G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
+    friction_k(1.0, 1.0, G.scaling, G.meanR, pa.w, pb.w, uk, uks);
+    const V lH = xyzv(G.lH[k]);
+    const V lM1 = xyzv(A.lM[s1]), lM2 = xyzv(A.lM[s2]);
+    FricVjp f;
+    law_friction_vjp(keff, kseff, G.mu_s, G.mu_d, G.dt, x1d, pa.w, xyzv(A.s0.vm[s1]), xyzv(A.s0.wi[s1]), x2d, pb.w,
+                     xyzv(A.s0.vm[s2]), xyzv(A.s0.wi[s2]), xyzv(h), (((int)h.w) & 1) != 0, lF2 - lF1,
+                     lF1 - lF2 + lH, lM1, lM2, f);
+    if (!f.touching) {  // the history is reset: nothing flows back through it
+      G.lH[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+      return;
+    }
+    out[0] = d4(f.x1, 0.0);
+    out[1] = d4(f.x2, 0.0);
+    out[2] = d4(f.v1, 0.0);
+    out[3] = d4(f.v2, 0.0);
+    out[4] = d4(f.w1, 0.0);
+    out[5] = d4(f.w2, 0.0);
+    G.lH[k] = d4(f.H, 0.0);
+    G.gpar[2 * (size_t)k] += f.k_eff * uk;
+    G.gpar[2 * (size_t)k + 1] += f.ks_eff * uks;
+    return;
+  }
   if (G.kind == 0) {
     // CElasticInteraction: p2 gets F, p1 gets -F
     const V3<D7> x1 = mk(D7::seed(x1d.x, 0), D7::seed(x1d.y, 1), D7::seed(x1d.z, 2));

@@ -59,7 +59,8 @@ struct AdjArgs {
   AdjDyn dyn[kMaxDyn];
   int nbond;
   AdjBond bond[kMaxBond];
-  int bond_tangents;                  // dual tangents per pass of the RotBond VJP (3, 6, 9 or 18)
+  int bond_tangents;                  // RotBond VJP: 0 hand-written reverse, else dual tangents per pass (3, 6, 9, 18)
+  int pair_duals;                     // pair-law VJPs: 0 hand-written reverse, 1 forward-mode duals
 };
 
 void launch_adjoint_step(const AdjArgs& A, cudaStream_t s);

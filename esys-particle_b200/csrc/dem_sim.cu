@@ -122,6 +122,7 @@ struct DemSim {
   int handoff = 0;       // device bond hand-off (dem_set_option "bond_handoff")
   int bond_pass = 1;     // bonds evaluated once per step by their own pass, then gathered
   int adj_tangents = 0;  // adjoint RotBond VJP: 0 hand-written reverse, else dual tangents per pass
+  int adj_pair_duals = 0;  // adjoint pair-law VJPs: 0 hand-written reverse, 1 forward-mode duals
   DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
   // particles
   int n = 0, cap = 0;
@@ -1073,6 +1074,7 @@ struct DemSim {
     A.visc_lin = visc_lin; A.visc_rot = visc_rot; A.dt_lin = dt; A.dt_rot = dt;
     A.nwall = nw;
     A.bond_tangents = adj_tangents;
+    A.pair_duals = adj_pair_duals;
     A.lx = lam; A.lv = lam + nn; A.lw = lam + 2 * (size_t)nn; A.lq = lam + 3 * (size_t)nn;
     A.lF = lam + 4 * (size_t)nn; A.lM = lam + 5 * (size_t)nn;
     A.gvisc = win.gvisc.p;
@@ -2331,6 +2333,8 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       if (v != 0 && v != 3 && v != 6 && v != 9 && v != 18)
         throw std::invalid_argument("adjoint_bond_tangents must be 0 (hand-written reverse), 3, 6, 9 or 18");
       s.adj_tangents = v;
+    } else if (k == "adjoint_pair_duals") {
+      s.adj_pair_duals = value != 0;
     } else if (k == "precision") {
       if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");
       s.set_precision(value == 32);

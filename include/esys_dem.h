@@ -198,7 +198,11 @@ int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const 
  * "chunk" (steps launched per host round trip), "store_forces" (keep per-particle F/M),
  * "profile" (time the force/integration kernels with CUDA events), "precision" (64 = FP64 form,
  * 32 = FP32 pair forces with Kahan-compensated accumulation, FP64 positions / contact detection /
- * integration). */
+ * integration), "split" (1: pair kernel + integration kernel), "bond_pass" (1: each bond
+ * evaluated once per step and gathered), "bond_handoff" (1: bond failures handed to the friction
+ * lists on the device), "adjoint_bond_tangents" (0: hand-written RotBond reverse; 3, 6, 9, 18:
+ * forward-mode dual tangents per pass), "adjoint_pair_duals" (0: hand-written pair-law
+ * reverses; 1: forward-mode duals). */
 int dem_set_option(dem_sim* h, const char* key, double value);
 
 /* ---- Field savers ----------------------------------------------------------------------- */

@@ -112,6 +112,15 @@ def run_loaded(sim, steps, rate):
         sim.step(1)
 
 
+def loaded_friction_pack(make, **kw):
+    """friction_pack with its floor and roof moved onto the pack (up to ~0.09 overlap), so
+    that the wall reactions of a short window are carried by the frictional contacts."""
+    sim = friction_pack(make, vscale=0.2, **kw)
+    sim.move_wall("floor", (0, 0.12, 0))
+    sim.move_wall("roof", (0, -0.12, 0))
+    return sim
+
+
 WINDOW_SEEDS = ("param:bonds:normalK", "param:bonds:shearK", "param:bonds:torsionK", "param:bonds:bendingK",
                 "param:Damping:viscosity", "param:RotDamping:viscosity")
 WINDOW_PARAMS = (("bonds", "normalK"), ("bonds", "shearK"), ("bonds", "torsionK"), ("bonds", "bendingK"),

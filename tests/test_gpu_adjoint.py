@@ -192,8 +192,8 @@ def test_window_refuses_a_bond_break(gpu):
 
 def test_friction_window_matches_dual_numbers(gpu, orc):
     """RotFriction contacts (with their tangential history) inside the window."""
-    a = S.friction_pack(gpu, vscale=0.2)
-    b = S.friction_pack(orc, vscale=0.2)
+    a = S.loaded_friction_pack(gpu)
+    b = S.loaded_friction_pack(orc)
     a.step(20)
     b.step(20)
     n = 40
@@ -203,6 +203,7 @@ def test_friction_window_matches_dual_numbers(gpu, orc):
     seeds = ["param:friction:normalK", "param:friction:shearK", "param:Damping:viscosity",
              "param:RotDamping:viscosity"]
     Rd, dR = b.window_dual(n, seeds, 2)
+    assert np.abs(Rd).max() > 0 and np.abs(dR).max() > 0   # the walls carry load
     assert np.abs(R - Rd).max() <= 1e-9 * np.abs(Rd).max()
     gd = np.einsum("tgc,tgck->k", S.mse_grad(Rd, tgt), dR)
     layout = a.param_layout()
@@ -354,3 +355,30 @@ def test_fp32_form_window_checkpoints_and_rewind(gpu):
         assert np.array_equal(a.window_forward(T, K), R)
     for k in ("params", "vel", "angvel"):
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("case", ["friction", "elastic", "bonded_failing"])
+def test_hand_written_pair_reverse_matches_dual_numbers(gpu, case):
+    """The RotFriction and NRotElastic VJPs of the reverse sweep (hand-written reverses, the
+    default) against the same VJPs by forward-mode duals."""
+    out = {}
+    for duals in (0, 1):
+        if case == "friction":
+            a = S.loaded_friction_pack(gpu)
+            a.step(20)
+            n, ng = 40, 2
+        elif case == "elastic":
+            a = S.gravity_box(gpu, n_side=5)
+            a.step(50)
+            n, ng = 60, 6
+        else:
+            a = _breaking(gpu)
+            n, ng = T, 2
+        a.set_option("adjoint_pair_duals", duals)
+        R = a.window_forward(n, 16)
+        tgt = S.mse_target(R)
+        out[duals] = a.window_adjoint(S.mse_grad(R, tgt))
+    for k in ("params", "vel", "angvel", "pos"):
+        scale = np.abs(out[1][k]).max()
+        assert scale > 0 or k == "angvel", k
+        assert np.abs(out[0][k] - out[1][k]).max() <= 1e-10 * max(scale, 1e-300), k
