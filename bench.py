@@ -83,26 +83,66 @@ def setup(make, w, periodic=True):
 
 
 class Clocks:
-    """Sample nvidia-smi clocks and throttle reasons during the timed region."""
+    """Sample SM clocks, power and throttle reasons during the timed region.
+
+    Through NVML in-process (the library nvidia-smi reads), on the GPU this process runs on
+    (matched by UUID): spawning nvidia-smi from a thread forks a process that holds a large
+    CUDA context, and those forks stalled the timed host loop.  nvidia-smi is the fallback."""
+
+    # NVML clocks-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
 
     def __init__(self, index=0):
         self.samples, self._stop, self.index = [], False, index
 
+    def _nvml(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.index).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+        def sample():
+            sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+            pw = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+            bits = int(reasons(h))
+            return [sm, mx, pw, bits]
+
+        return sample
+
     def __enter__(self):
+        try:
+            sample = self._nvml()
+        except Exception:
+            sample = None
+        self.source = "nvml" if sample is not None else "nvidia-smi"
+
         def run():
             q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap")
             while not self._stop:
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([x.strip() for x in out.split(",")])
+                    if sample is not None:
+                        self.samples.append(sample())
+                    else:
+                        out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                             timeout=5).stdout.strip()
+                        if out:
+                            v = [x.strip() for x in out.split(",")]
+                            bits = sum(b for b, k in zip((0x8, 0x40, 0x20, 0x4), v[3:7]) if k == "Active")
+                            self.samples.append([float(v[0]), float(v[1]), float(v[2]), bits])
                 except Exception:
                     pass
-                time.sleep(0.2)
+                time.sleep(0.05 if sample is not None else 0.2)
 
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
@@ -115,13 +155,12 @@ class Clocks:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4)
-                          if len(s) > 3 + k and s[3 + k].strip() == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        sm = [s[0] for s in self.samples]
+        mx = [s[1] for s in self.samples]
+        reasons = sorted({name for s in self.samples for bit, name in self.REASONS.items() if s[3] & bit})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": reasons,
+                "samples": len(self.samples), "power_w_median": float(np.median([s[2] for s in self.samples])),
+                "source": self.source}
 
 
 def peaks():
