@@ -273,7 +273,7 @@ __device__ __forceinline__ void adj_bond_rev_one(const AdjArgs& A, int gi, int b
   gp[3] += g.kb * U.kb;
 }
 
-__global__ void __launch_bounds__(128) k_adj_bond_rev(const AdjArgs A, int gi) {
+__global__ void __launch_bounds__(128, 3) k_adj_bond_rev(const AdjArgs A, int gi) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < A.bond[gi].nb) adj_bond_rev_one(A, gi, b);
 }
@@ -286,6 +286,9 @@ __device__ __forceinline__ V3<D23> seed3(const V& a, int k) {
 }
 __device__ __forceinline__ D23 dotd(const V3<D23>& a, const V& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
+// DUALS selects the VJP form at compile time: the dual-number form's registers would otherwise
+// set the hand-written form's occupancy too.
+template <bool DUALS>
 __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   const AdjDyn& G = A.dyn[gi];
   const unsigned long long key = G.keys[k];
@@ -303,7 +306,7 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   const V x1d = xyzv(pa), x2d = image_of(A.g, x1d, xyzv(pb));
   const V lF1 = xyzv(A.lF[s1]), lF2 = xyzv(A.lF[s2]);
   for (int c = 0; c < 6; ++c) out[c] = make_double4(0.0, 0.0, 0.0, 0.0);
-  if (!A.pair_duals) {  // hand-written reverse of the law (dem_pair_vjp.cuh), the default
+  if (!DUALS) {  // hand-written reverse of the law (dem_pair_vjp.cuh), the default
     if (G.kind == 0) {
       ElasticVjp e;
       law_elastic_vjp(elastic_k(G.k, G.scaling, pa.w, pb.w), x1d, pa.w, x2d, pb.w, lF2 - lF1, e);
@@ -394,9 +397,10 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   G.gpar[2 * (size_t)k + 1] += w.d[22];
 }
 
-__global__ void __launch_bounds__(128) k_adj_pair(const AdjArgs A, int gi) {
+template <bool DUALS>
+__global__ void __launch_bounds__(128, DUALS ? 1 : 4) k_adj_pair(const AdjArgs A, int gi) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < A.dyn[gi].m) adj_pair_one(A, gi, k);
+  if (k < A.dyn[gi].m) adj_pair_one<DUALS>(A, gi, k);
 }
 
 __device__ __forceinline__ void add4(double4& a, const double4& b) {
@@ -490,7 +494,10 @@ void launch_adjoint_step(const AdjArgs& A, cudaStream_t s) {
       }
     }
   for (int d = 0; d < A.ndyn; ++d)
-    if (A.dyn[d].m) k_adj_pair<<<(A.dyn[d].m + 127) / 128, 128, 0, s>>>(A, d);
+    if (A.dyn[d].m) {
+      if (A.pair_duals) k_adj_pair<true><<<(A.dyn[d].m + 127) / 128, 128, 0, s>>>(A, d);
+      else k_adj_pair<false><<<(A.dyn[d].m + 127) / 128, 128, 0, s>>>(A, d);
+    }
   if (A.nbond || A.ndyn) k_adj_post<<<nb, 256, 0, s>>>(A);
 }
 
@@ -600,7 +607,7 @@ __global__ void __launch_bounds__(256) k_adj_post_batch(const AdjBatch B) {
   }
 }
 
-__global__ void __launch_bounds__(128) k_adj_bond_rev_batch(const AdjBatch B) {
+__global__ void __launch_bounds__(128, 3) k_adj_bond_rev_batch(const AdjBatch B) {
   for (int tile = blockIdx.x; tile < B.total_btiles; tile += gridDim.x) {
     const int it = batch_item(B.btile_start, B.nspec * kMaxBond, tile);
     const int sp = it / kMaxBond, gi = it % kMaxBond;
@@ -610,13 +617,14 @@ __global__ void __launch_bounds__(128) k_adj_bond_rev_batch(const AdjBatch B) {
   }
 }
 
-__global__ void __launch_bounds__(128) k_adj_pair_batch(const AdjBatch B) {
+template <bool DUALS>
+__global__ void __launch_bounds__(128, DUALS ? 1 : 4) k_adj_pair_batch(const AdjBatch B) {
   for (int tile = blockIdx.x; tile < B.total_dtiles; tile += gridDim.x) {
     const int it = batch_item(B.dtile_start, B.nspec * kMaxDyn, tile);
     const int sp = it / kMaxDyn, gi = it % kMaxDyn;
     const AdjArgs& A = B.args[sp];
     const int k = (tile - __ldg(B.dtile_start + it)) * 128 + threadIdx.x;
-    if (gi < A.ndyn && k < A.dyn[gi].m) adj_pair_one(A, gi, k);
+    if (gi < A.ndyn && k < A.dyn[gi].m) adj_pair_one<DUALS>(A, gi, k);
   }
 }
 
@@ -627,7 +635,10 @@ void launch_adjoint_step_batch(const AdjBatch& B, bool bonds, bool pairs, cudaSt
   if (B.total_ptiles <= 0) return;
   k_adj_pre_batch<<<batch_grid(B.total_ptiles), 256, 0, s>>>(B);
   if (bonds && B.total_btiles > 0) k_adj_bond_rev_batch<<<batch_grid(B.total_btiles), 128, 0, s>>>(B);
-  if (pairs && B.total_dtiles > 0) k_adj_pair_batch<<<batch_grid(B.total_dtiles), 128, 0, s>>>(B);
+  if (pairs && B.total_dtiles > 0) {
+    if (B.pair_duals) k_adj_pair_batch<true><<<batch_grid(B.total_dtiles), 128, 0, s>>>(B);
+    else k_adj_pair_batch<false><<<batch_grid(B.total_dtiles), 128, 0, s>>>(B);
+  }
   if (bonds || pairs) k_adj_post_batch<<<batch_grid(B.total_ptiles), 256, 0, s>>>(B);
 }
 

@@ -95,6 +95,7 @@ struct AdjBatch {
   int total_btiles;
   const int* dtile_start;         // [nspec * kMaxDyn + 1]: pair tiles of 128 per (specimen, group)
   int total_dtiles;
+  int pair_duals;                 // pair-law VJPs by forward-mode duals (else hand-written), as AdjArgs
 };
 
 // Step j's recompute arguments (both buffer parities) and wall planes, from each specimen's base.

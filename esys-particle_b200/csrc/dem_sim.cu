@@ -1766,6 +1766,10 @@ struct Ensemble {
     AB.total_btiles = bptile[(size_t)ns * kMaxBond];
     AB.dtile_start = d_dtile.p;
     AB.total_dtiles = dtile[(size_t)ns * kMaxDyn];
+    AB.pair_duals = abase[0].pair_duals;
+    for (int k = 1; k < ns; ++k)
+      if (abase[k].pair_duals != AB.pair_duals)
+        throw std::invalid_argument("ensemble specimens must share the adjoint_pair_duals option");
     for (int c = nseg - 1; c >= 0; --c) {
       const int len = std::min(K, T - c * K);
       for (int k = 0; k < ns; ++k) {
