@@ -193,9 +193,9 @@ __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
   const AdjBond& B = A.bond[gi];
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B.nb) return;
-  double4* out = B.gb + 4 * (size_t)b;
+  double4* out = B.gb + 3 * (size_t)b;
   if (B.broken_step[b] <= A.step) {  // removed before this step
-    out[0] = out[1] = out[2] = out[3] = make_double4(0.0, 0.0, 0.0, 0.0);
+    out[0] = out[1] = out[2] = make_double4(0.0, 0.0, 0.0, 0.0);
     return;
   }
   const int2 e = B.ends[b];
@@ -229,10 +229,10 @@ __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
     for (int k = 0; k < NT; ++k)
       if (base + k < 18) g[base + k] = w.d[k];
   }
-  out[0] = make_double4(g[0], g[1], g[2], 0.0);
-  out[1] = make_double4(g[3], g[4], g[5], g[6]);
-  out[2] = make_double4(g[7], g[8], g[9], 0.0);
-  out[3] = make_double4(g[10], g[11], g[12], g[13]);
+  // the law depends on x2 - x1 only: d/dx2 = -d/dx1 (not stored)
+  out[0] = make_double4(g[0], g[1], g[2], g[3]);
+  out[1] = make_double4(g[4], g[5], g[6], g[10]);
+  out[2] = make_double4(g[11], g[12], g[13], 0.0);
   double* gp = B.gpar + 4 * (size_t)b;
   gp[0] += g[14];
   gp[1] += g[15];
@@ -244,9 +244,9 @@ __global__ void __launch_bounds__(128) k_adj_bond(const AdjArgs A, int gi) {
 // RotBond VJP by the hand-written reverse of the law (dem_bond_vjp.cuh).
 __device__ __forceinline__ void adj_bond_rev_one(const AdjArgs& A, int gi, int b) {
   const AdjBond& B = A.bond[gi];
-  double4* out = B.gb + 4 * (size_t)b;
+  double4* out = B.gb + 3 * (size_t)b;
   if (B.broken_step[b] <= A.step) {  // removed before this step
-    out[0] = out[1] = out[2] = out[3] = make_double4(0.0, 0.0, 0.0, 0.0);
+    out[0] = out[1] = out[2] = make_double4(0.0, 0.0, 0.0, 0.0);
     return;
   }
   const int2 e = B.ends[b];
@@ -262,10 +262,10 @@ __device__ __forceinline__ void adj_bond_rev_one(const AdjArgs& A, int gi, int b
   BondVjp g;
   law_bond_vjp(K, mD, x1, p1.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, p2.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, lFd, lM1,
                lM2, g);
-  out[0] = make_double4(g.x1.x, g.x1.y, g.x1.z, 0.0);
-  out[1] = make_double4(g.q1.s, g.q1.v.x, g.q1.v.y, g.q1.v.z);
-  out[2] = make_double4(g.x2.x, g.x2.y, g.x2.z, 0.0);
-  out[3] = make_double4(g.q2.s, g.q2.v.x, g.q2.v.y, g.q2.v.z);
+  // the law depends on x2 - x1 only: d/dx2 = -d/dx1 (not stored)
+  out[0] = make_double4(g.x1.x, g.x1.y, g.x1.z, g.q1.s);
+  out[1] = make_double4(g.q1.v.x, g.q1.v.y, g.q1.v.z, g.q2.s);
+  out[2] = make_double4(g.q2.v.x, g.q2.v.y, g.q2.v.z, 0.0);
   double* gp = B.gpar + 4 * (size_t)b;  // the scaled stiffness is the group's times a constant factor
   gp[0] += g.kr * U.kr;
   gp[1] += g.ks * U.ks;
@@ -293,11 +293,14 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   const AdjDyn& G = A.dyn[gi];
   const unsigned long long key = G.keys[k];
   const int s1 = (int)(key >> 32), s2 = (int)(key & 0xffffffffu);
-  double4* out = G.gpair + 6 * (size_t)k;
+  // Record of a touching pair: (d/dx1, d/dv1.x), (d/dv1.yz, d/dw1.xy), (d/dw1.z, d/dw2); the laws
+  // depend on x1 - x2 and v1 - v2 only, so d/dx2 = -d/dx1 and d/dv2 = -d/dv1.  gact[k] = 0 marks a
+  // pair with nothing to gather (not touching, or held by its excluding bond): no record written.
+  double4* out = G.gpair + 3 * (size_t)k;
+  G.gact[k] = 0;
   if (G.xbond) {  // a pair skipped by the step while its excluding bond holds
     const int xb = G.xbond[k];
     if (xb >= 0 && A.bond[xb >> 28].broken_step[xb & 0x0fffffff] > A.step) {
-      for (int c = 0; c < 6; ++c) out[c] = make_double4(0.0, 0.0, 0.0, 0.0);
       if (G.kind == 1) G.lH[k] = make_double4(0.0, 0.0, 0.0, 0.0);
       return;
     }
@@ -305,14 +308,13 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   const double4 pa = A.s0.pr[s1], pb = A.s0.pr[s2];
   const V x1d = xyzv(pa), x2d = image_of(A.g, x1d, xyzv(pb));
   const V lF1 = xyzv(A.lF[s1]), lF2 = xyzv(A.lF[s2]);
-  for (int c = 0; c < 6; ++c) out[c] = make_double4(0.0, 0.0, 0.0, 0.0);
   if (!DUALS) {  // hand-written reverse of the law (dem_pair_vjp.cuh), the default
     if (G.kind == 0) {
       ElasticVjp e;
       law_elastic_vjp(elastic_k(G.k, G.scaling, pa.w, pb.w), x1d, pa.w, x2d, pb.w, lF2 - lF1, e);
       if (!e.touching) return;
       out[0] = d4(e.x1, 0.0);
-      out[1] = d4(e.x2, 0.0);
+      G.gact[k] = 1;
       G.gpar[2 * (size_t)k] += e.k_eff * elastic_k(1.0, G.scaling, pa.w, pb.w);  // k_eff = k x factor
       return;
     }
@@ -336,12 +338,10 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
       G.lH[k] = make_double4(0.0, 0.0, 0.0, 0.0);
       return;
     }
-    out[0] = d4(f.x1, 0.0);
-    out[1] = d4(f.x2, 0.0);
-    out[2] = d4(f.v1, 0.0);
-    out[3] = d4(f.v2, 0.0);
-    out[4] = d4(f.w1, 0.0);
-    out[5] = d4(f.w2, 0.0);
+    out[0] = make_double4(f.x1.x, f.x1.y, f.x1.z, f.v1.x);
+    out[1] = make_double4(f.v1.y, f.v1.z, f.w1.x, f.w1.y);
+    out[2] = make_double4(f.w1.z, f.w2.x, f.w2.y, f.w2.z);
+    G.gact[k] = 1;
     G.lH[k] = d4(f.H, 0.0);
     G.gpar[2 * (size_t)k] += f.k_eff * uk;
     G.gpar[2 * (size_t)k + 1] += f.ks_eff * uks;
@@ -357,7 +357,7 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
     const V l = lF2 - lF1;
     const D7 w = F.x * l.x + F.y * l.y + F.z * l.z;
     out[0] = make_double4(w.d[0], w.d[1], w.d[2], 0.0);
-    out[1] = make_double4(w.d[3], w.d[4], w.d[5], 0.0);
+    G.gact[k] = 1;
     G.gpar[2 * (size_t)k] += w.d[6];
     return;
   }
@@ -386,12 +386,10 @@ __device__ __forceinline__ void adj_pair_one(const AdjArgs& A, int gi, int k) {
   // p1 gets -fn + Ffric and M1, p2 gets fn - Ffric and M2; the next history is Ffric
   const V lM1 = xyzv(A.lM[s1]), lM2 = xyzv(A.lM[s2]);
   const D23 w = dotd(o.fn, lF2 - lF1) + dotd(o.Ffric, lF1 - lF2 + lH) + dotd(o.M1, lM1) + dotd(o.M2, lM2);
-  out[0] = make_double4(w.d[0], w.d[1], w.d[2], 0.0);
-  out[1] = make_double4(w.d[3], w.d[4], w.d[5], 0.0);
-  out[2] = make_double4(w.d[6], w.d[7], w.d[8], 0.0);
-  out[3] = make_double4(w.d[9], w.d[10], w.d[11], 0.0);
-  out[4] = make_double4(w.d[12], w.d[13], w.d[14], 0.0);
-  out[5] = make_double4(w.d[15], w.d[16], w.d[17], 0.0);
+  out[0] = make_double4(w.d[0], w.d[1], w.d[2], w.d[6]);
+  out[1] = make_double4(w.d[7], w.d[8], w.d[12], w.d[13]);
+  out[2] = make_double4(w.d[14], w.d[15], w.d[16], w.d[17]);
+  G.gact[k] = 1;
   G.lH[k] = make_double4(w.d[18], w.d[19], w.d[20], 0.0);
   G.gpar[2 * (size_t)k] += w.d[21];
   G.gpar[2 * (size_t)k + 1] += w.d[22];
@@ -403,13 +401,6 @@ __global__ void __launch_bounds__(128, DUALS ? 1 : 4) k_adj_pair(const AdjArgs A
   if (k < A.dyn[gi].m) adj_pair_one<DUALS>(A, gi, k);
 }
 
-__device__ __forceinline__ void add4(double4& a, const double4& b) {
-  a.x += b.x;
-  a.y += b.y;
-  a.z += b.z;
-  a.w += b.w;
-}
-
 __device__ __forceinline__ void adj_post_one(const AdjArgs& A, int i) {
   if (!(A.pflags[i] & PF_ALIVE)) return;
   double4 gx = make_double4(0.0, 0.0, 0.0, 0.0), gv = gx, gw = gx, gq = gx;
@@ -418,12 +409,16 @@ __device__ __forceinline__ void adj_post_one(const AdjArgs& A, int i) {
     for (int e = G.adj_start[i]; e < G.adj_start[i + 1]; ++e) {
       const int2 en = G.adj[e];
       const int k = en.y & 0x7fffffff;
-      const int side = en.y < 0 ? 0 : 1;  // this particle is p1 or p2 of the pair
-      const double4* r = G.gpair + 6 * (size_t)k;
-      add4(gx, r[side]);
+      if (!G.gact[k]) continue;
+      const double4* r = G.gpair + 3 * (size_t)k;
+      const double4 r0 = r[0];
+      const double sg = en.y < 0 ? 1.0 : -1.0;  // this particle is p1 (d/dx1) or p2 (d/dx2 = -d/dx1)
+      gx.x += sg * r0.x; gx.y += sg * r0.y; gx.z += sg * r0.z;
       if (G.kind == 1) {
-        add4(gv, r[2 + side]);
-        add4(gw, r[4 + side]);
+        const double4 r1 = r[1], r2 = r[2];
+        gv.x += sg * r0.w; gv.y += sg * r1.x; gv.z += sg * r1.y;
+        if (en.y < 0) { gw.x += r1.z; gw.y += r1.w; gw.z += r2.x; }
+        else { gw.x += r2.y; gw.y += r2.z; gw.z += r2.w; }
       }
     }
   }
@@ -432,13 +427,15 @@ __device__ __forceinline__ void adj_post_one(const AdjArgs& A, int i) {
     for (int e = B.adj_start[i]; e < B.adj_start[i + 1]; ++e) {
       const int2 en = B.adj[e];
       const int k = en.y & 0x7fffffff;
-      const double4* r = B.gb + 4 * (size_t)k;
-      if (en.y < 0) {
-        add4(gx, r[0]);
-        add4(gq, r[1]);
-      } else {
-        add4(gx, r[2]);
-        add4(gq, r[3]);
+      const double4* r = B.gb + 3 * (size_t)k;
+      const double4 r0 = r[0], r1 = r[1];
+      if (en.y < 0) {  // p1: d/dx1, d/dq1
+        gx.x += r0.x; gx.y += r0.y; gx.z += r0.z;
+        gq.x += r0.w; gq.y += r1.x; gq.z += r1.y; gq.w += r1.z;
+      } else {         // p2: d/dx2 = -d/dx1, d/dq2
+        const double4 r2 = r[2];
+        gx.x -= r0.x; gx.y -= r0.y; gx.z -= r0.z;
+        gq.x += r1.w; gq.y += r2.x; gq.z += r2.y; gq.w += r2.z;
       }
     }
   }

@@ -17,7 +17,9 @@ struct AdjDyn {
   const float4* hist32_in;            // the same when the window runs the FP32-force form
   const int* xbond;                   // device bond hand-off: excluding bond of each pair (else null)
   double4* lH;                        // adjoint of the history: in after step t, out before it
-  double4* gpair;                     // [m][6]: d/dx1, d/dx2, d/dv1, d/dv2, d/dw1, d/dw2 of this step
+  double4* gpair;                     // [m][3]: d/dx1, d/dv1, d/dw1, d/dw2 of this step, packed (d/dx2 = -d/dx1,
+                                      // d/dv2 = -d/dv1)
+  unsigned char* gact;                // [m]: 1 when this step's record was written (a touching pair)
   double* gpar;                       // [m][2]: d/dk, d/dks accumulated over the window
 };
 
@@ -31,7 +33,7 @@ struct AdjBond {
   const int* broken_step;
   const int* adj_start;
   const int2* adj;
-  double4* gb;                        // [nb][4]: d/dx1, d/dq1, d/dx2, d/dq2 of this step
+  double4* gb;                        // [nb][3]: d/dx1, d/dq1, d/dq2 of this step, packed (d/dx2 = -d/dx1)
   double* gpar;                       // [nb][4]: d/dkr, d/dks, d/dkt, d/dkb accumulated
 };
 

@@ -831,7 +831,7 @@ struct DemSim {
     DBuf<long long> ck_step;
     DBuf<unsigned> ck_pf, st_pf, save_pf;  // wall candidacy: per checkpoint, per recomputed step, live
     DBuf<int> ck_brk, save_brk, bs0[kMaxBond], nev0;
-    DBuf<unsigned char> flag0;
+    DBuf<unsigned char> flag0, gact[kMaxDyn];
     DBuf<float4> st_vw, st_hist32[kMaxDyn];  // FP32 form: velocity shadows and histories of the recompute
     bool fp32 = false;
     void release() {
@@ -839,6 +839,7 @@ struct DemSim {
       for (int d = 0; d < kMaxDyn; ++d) st_hist32[d].release();
       ck_pf.release(); st_pf.release(); save_pf.release(); ck_brk.release(); save_brk.release(); nev0.release();
       flag0.release();
+      for (int d = 0; d < kMaxDyn; ++d) gact[d].release();
       for (int b = 0; b < kMaxBond; ++b) bs0[b].release();
       ck.release(); st.release(); st_f.release(); st_m.release(); lam.release();
       for (int d = 0; d < kMaxDyn; ++d) {
@@ -1043,14 +1044,15 @@ struct DemSim {
         else win.st_hist[d].reserve((size_t)(K + 1) * m);
       }
       win.lH[d].reserve(m);
-      win.gpair[d].reserve((size_t)6 * m);
+      win.gpair[d].reserve((size_t)3 * m);
+      win.gact[d].reserve(m);
       win.gpar_d[d].reserve((size_t)2 * m);
       DEM_CUDA(cudaMemsetAsync(win.lH[d].p, 0, sizeof(double4) * m, s));
       DEM_CUDA(cudaMemsetAsync(win.gpar_d[d].p, 0, sizeof(double) * 2 * m, s));
     }
     for (int b = 0; b < nbg; ++b) {
       const int m = std::max(bl[b]->nb, 1);
-      win.gb[b].reserve((size_t)4 * m);
+      win.gb[b].reserve((size_t)3 * m);
       win.gpar_b[b].reserve((size_t)4 * m);
       DEM_CUDA(cudaMemsetAsync(win.gpar_b[b].p, 0, sizeof(double) * 4 * m, s));
     }
@@ -1085,7 +1087,7 @@ struct DemSim {
       D.kind = G.kind; D.k = G.k; D.ks = G.ks; D.mu_s = G.mu_s; D.mu_d = G.mu_d; D.dt = G.dt;
       D.scaling = G.scaling; D.meanR = G.meanR; D.m = win.m[d];
       D.keys = G.keys.p; D.adj_start = G.adj_start.p; D.adj = G.adj.p;
-      D.lH = win.lH[d].p; D.gpair = win.gpair[d].p; D.gpar = win.gpar_d[d].p;
+      D.lH = win.lH[d].p; D.gpair = win.gpair[d].p; D.gact = win.gact[d].p; D.gpar = win.gpar_d[d].p;
       D.xbond = handoff ? G.xbond.p : nullptr;
     }
     A.nbond = nbg;
