@@ -13,8 +13,11 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <iostream>
 #include <map>
 #include <set>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -61,6 +64,7 @@ struct DBuf {
 
 struct Wall {
   double o[3], n[3];
+  double old[3];  // CWall::m_oldpos: the origin at creation (restart checkpoints carry it)
 };
 
 struct WallGroup {
@@ -128,6 +132,7 @@ struct DemSim {
   int n = 0, cap = 0;
   Particles P{};
   std::vector<int> h_id;                 // slot -> id
+  std::vector<double> h_initpos;         // slot -> CParticle::m_initpos (x, y, z), for restart checkpoints
   std::unordered_map<int, int> id2slot;  // id -> slot (of particles ever added)
   int cur = 0;
   // cells
@@ -319,7 +324,11 @@ struct DemSim {
       DEM_CUDA(cudaMemsetAsync(P.flagged + n, 0, add, s));
       DEM_CUDA(cudaMemsetAsync(P.force + n, 0, sizeof(double4) * add, s));
       DEM_CUDA(cudaMemsetAsync(P.moment + n, 0, sizeof(double4) * add, s));
-      for (int i = 0; i < add; ++i) { id2slot[ids[i]] = n + i; h_id.push_back(ids[i]); }
+      for (int i = 0; i < add; ++i) {
+        id2slot[ids[i]] = n + i;
+        h_id.push_back(ids[i]);
+        h_initpos.insert(h_initpos.end(), {pr[i].x, pr[i].y, pr[i].z});
+      }
       n += add;
       P.n = n;
       sync();
@@ -1298,6 +1307,360 @@ struct DemSim {
     adj_finish(grad_params, gvel, gang, gpos, gquat);
   }
 
+  // ---- restart checkpoints: the worker's file of TSubLattice::saveCheckPointData /
+  // loadCheckPointData (Parallel/SubLattice.hpp:3600-3790), written and read with the same
+  // iostream formatting (the caller sets the precision, 12 digits by default).
+  //
+  // Scaled RotBond constants as CRotBondedInteraction's constructor forms them
+  // (Model/RotBondedInteraction.cpp:122-161); the restart record carries them.
+  static void bond_scaled(const BondGroup& B, double dist0, double r1, double r2, double* k) {
+    double effR = 1.0, effL = 1.0, effA = 1.0, J = 1.0, I = 1.0;
+    if (B.scaling) {
+      effR = B.meanR ? 0.5 * dist0 : std::min(r1, r2);
+      effL = dist0;
+      effA = effR * effR;
+      J = 0.5 * effR * effR * effR * effR;
+      I = 0.5 * J;
+    }
+    k[0] = B.kr * effA / effL;  // kr
+    k[1] = B.ks * effA / effL;  // ks
+    k[2] = B.kb * I / effL;     // kb
+    k[3] = B.kt * J / effL;     // kt
+    k[4] = B.mn * effA;         // max_nForce
+    k[5] = B.ms * effA;         // max_shForce
+    k[6] = B.mt * J / effR;     // max_tMoment
+    k[7] = B.mb * I / effR;     // max_bMoment
+  }
+
+  void save_checkpoint(std::ostream& os) {
+    download_walls();
+    std::vector<double4> pr(n), vm(n), wi(n), qq(n), op(n), fo(n);
+    std::vector<unsigned> pf(n);
+    std::vector<int> tg(n);
+    if (n) {
+      const ParticleBuf& b = P.buf[cur];
+      DEM_CUDA(cudaMemcpyAsync(pr.data(), b.pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(vm.data(), b.vm, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(wi.data(), b.wi, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(qq.data(), b.qq, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(op.data(), P.oldpos, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      if (store_forces) DEM_CUDA(cudaMemcpyAsync(fo.data(), P.force, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(tg.data(), P.tag, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    }
+    sync();
+    const char d = ' ';
+    // ParallelParticleArray::saveCheckPointData (ppa/src/pp_array.hpp:1217-1236)
+    os << g.p0x << d << g.p0y << d << g.p0z << "\n";
+    os << g.gx << " " << g.gy << " " << g.gz << "\n";
+    int alive = 0;
+    for (int i = 0; i < n; ++i) alive += (pf[i] & PF_ALIVE) ? 1 : 0;
+    os << alive << "\n";
+    for (int i = 0; i < n; ++i) {
+      if (!(pf[i] & PF_ALIVE)) continue;
+      // CParticle::saveCheckPointData (Model/Particle.cpp:461-475); one worker: no circular shift
+      os << pr[i].x << d << pr[i].y << d << pr[i].z << d << pr[i].w << d << h_id[i] << d << tg[i] << d << vm[i].w << d
+         << h_initpos[3 * (size_t)i] << d << h_initpos[3 * (size_t)i + 1] << d << h_initpos[3 * (size_t)i + 2] << d
+         << op[i].x << d << op[i].y << d << op[i].z << d << vm[i].x << d << vm[i].y << d << vm[i].z << d
+         << fo[i].x << d << fo[i].y << d << fo[i].z << d << 0.0 << d << 0.0 << d << 0.0 << d
+         << ((pf[i] & PF_DYN) ? 1 : 0);
+      if (rot)  // CRotParticle::saveCheckPointData (Model/RotParticle.cpp:510-519)
+        os << d << wi[i].w << d << qq[i].x << d << qq[i].y << d << qq[i].z << d << qq[i].w << d << wi[i].x << d
+           << wi[i].y << d << wi[i].z << d << ((pf[i] & PF_ROT) ? 1 : 0);
+      os << "\n";
+    }
+    // bonded groups: PIS_EB::saveCheckPointData (pis/pi_storage_eb.hpp:79-97) per group, name order
+    os << bond.size() << "\n";
+    for (auto& it : bond) {
+      BondGroup& B = it.second;
+      std::vector<int2> ends(B.nb);
+      std::vector<double4> D0(B.nb);
+      std::vector<int> bs(B.nb);
+      if (B.nb) {
+        DEM_CUDA(cudaMemcpyAsync(ends.data(), B.ends.p, sizeof(int2) * B.nb, cudaMemcpyDeviceToHost, s));
+        DEM_CUDA(cudaMemcpyAsync(D0.data(), B.D0.p, sizeof(double4) * B.nb, cudaMemcpyDeviceToHost, s));
+        DEM_CUDA(cudaMemcpyAsync(bs.data(), B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToHost, s));
+      }
+      sync();
+      // a bond that failed in the last step stays listed until the next update, as in the reference
+      int intact = 0;
+      for (int k = 0; k < B.nb; ++k) intact += bs[k] > t ? 1 : 0;
+      os << "RotBonded" << "\n";
+      os << intact;
+      for (int k = 0; k < B.nb; ++k) {
+        if (!(bs[k] > t)) continue;
+        const int i = ends[k].x, j = ends[k].y;
+        const double dist0 = std::sqrt(D0[k].x * D0[k].x + D0[k].y * D0[k].y + D0[k].z * D0[k].z);
+        double c[8];
+        bond_scaled(B, dist0, pr[i].w, pr[j].w, c);
+        // CRotBondedInteraction::saveRestartData (Model/RotBondedInteraction.cpp:379-399)
+        os << "\n" << h_id[i] << " " << h_id[j] << " " << 1 << " " << c[0] << " " << c[1] << " " << c[2] << " " << c[3]
+           << " " << (B.scaling ? 1 : 0) << " " << (B.meanR ? 1 : 0) << " " << B.truncated << " " << 1.0 << " " << 1.0
+           << " " << c[4] << " " << c[5] << " " << c[6] << " " << c[7] << " " << D0[k].x << d << D0[k].y << d
+           << D0[k].z << " " << B.tag << "\n";
+      }
+      os << "\n";
+    }
+    // dynamic groups that save (PIS_ED; PIS_NE saves nothing): PIS_ED::saveCheckPointData
+    // (pis/pi_storage_ed.hpp:202-214).  The reference writes the record count and the first record
+    // with no separator; a newline is written here so that the count can be read back.
+    int nsave = 0;
+    for (auto& it : dyn) nsave += it.second.kind == 1 ? 1 : 0;
+    os << nsave << "\n";
+    for (auto& it : dyn) {
+      DynGroup& G = it.second;
+      if (G.kind != 1) continue;
+      std::vector<unsigned long long> keys(G.m);
+      std::vector<double4> h(G.m);
+      std::vector<int> xb(handoff ? G.m : 0);
+      if (G.m) {
+        DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s));
+        if (fp32) {
+          std::vector<float4> h32(G.m);
+          DEM_CUDA(cudaMemcpyAsync(h32.data(), G.hist32[cur].p, sizeof(float4) * G.m, cudaMemcpyDeviceToHost, s));
+          sync();
+          for (int k = 0; k < G.m; ++k) h[k] = make_double4(h32[k].x, h32[k].y, h32[k].z, h32[k].w);
+        } else {
+          DEM_CUDA(cudaMemcpyAsync(h.data(), G.hist[cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s));
+        }
+        if (handoff) DEM_CUDA(cudaMemcpyAsync(xb.data(), G.xbond.p, sizeof(int) * G.m, cudaMemcpyDeviceToHost, s));
+      }
+      std::vector<std::vector<int>> bsteps;
+      if (handoff)
+        for (auto& b : bond) {
+          bsteps.emplace_back(b.second.nb);
+          if (b.second.nb)
+            DEM_CUDA(cudaMemcpyAsync(bsteps.back().data(), b.second.broken_step.p, sizeof(int) * b.second.nb,
+                                     cudaMemcpyDeviceToHost, s));
+        }
+      sync();
+      std::vector<int> listed;
+      for (int k = 0; k < G.m; ++k) {
+        // the device bond hand-off keeps bond-held pairs that the reference's list does not have
+        if (handoff && xb[k] >= 0 && bsteps[xb[k] >> 28][xb[k] & 0x0fffffff] > t) continue;
+        listed.push_back(k);
+      }
+      os << "RotFriction" << "\n";
+      os << listed.size() << "\n";
+      for (int k : listed) {
+        const int i = (int)(keys[k] >> 32), j = (int)(keys[k] & 0xffffffffu);
+        const double r1 = pr[i].w, r2 = pr[j].w;
+        // scaled stiffnesses as CRotFrictionInteraction's constructor forms them (Model/RotFricInteraction.cpp:103-146)
+        double effR = 1.0, effL = 1.0, effA = 1.0;
+        const double r0 = r1 + r2;
+        if (G.scaling) {
+          effR = G.meanR ? 0.5 * r0 : std::min(r1, r2);
+          effL = r0;
+          effA = effR * effR;
+        }
+        const int flags = (int)h[k].w;
+        // CRotFrictionInteraction::saveRestartData (Model/RotFricInteraction.cpp:597-614)
+        os << G.k * effA / effL << " " << r0 << " " << G.mu_d << " " << G.mu_s << " " << G.ks * effA / effL << " "
+           << G.dt << " " << (G.scaling ? 1 : 0) << " " << (G.meanR ? 1 : 0) << " " << h_id[i] << " " << h_id[j] << " "
+           << (flags & 1) << " " << ((flags >> 1) & 1) << " " << h[k].x << " " << h[k].y << " " << h[k].z << "\n";
+      }
+      os << "\n";
+    }
+    // walls (name, CWall::writeCheckPoint, Model/Wall.cpp:118-121), then the empty body and mesh sections
+    os << "Walls " << walls.size() << "\n";
+    for (auto& w : walls) {
+      const Wall& W = w.second;
+      os << w.first << "\n";
+      os << W.o[0] << d << W.o[1] << d << W.o[2] << " " << W.old[0] << d << W.old[1] << d << W.old[2] << " "
+         << W.n[0] << d << W.n[1] << d << W.n[2] << "\n";
+    }
+    os << "Spheres " << 0 << "\n";
+    os << "TriMesh " << 0 << "\n";
+    os << "Mesh2D " << 0 << "\n";
+  }
+
+  // Reads a worker file into this worker: particles (into an empty worker), each bonded group's
+  // bonds with their creation vectors, each RotFriction group's pairs with their tangential
+  // history (carried through the neighbour search that follows, for the pairs still touching, as
+  // PIS_ED::update keeps them), and the walls.  The groups themselves come from the script, as in
+  // the reference; the per-interaction constants in the file are not read back (they follow from
+  // the groups' parameters).  timestep: the master's step counter (CheckPointInfo).
+  void load_checkpoint(std::istream& is, long long timestep) {
+    if (n) throw StateError("a checkpoint is loaded into a worker without particles");
+    auto fail = [&](const std::string& what) { throw std::invalid_argument("checkpoint: " + what); };
+    double bp[3];
+    int bi[3];
+    is >> bp[0] >> bp[1] >> bp[2] >> bi[0] >> bi[1] >> bi[2];
+    int np = 0;
+    is >> np;
+    if (!is || np < 0) fail("bad particle block header");
+    std::vector<int> ids(np), tags(np), flags(np);
+    std::vector<double> pos(3 * (size_t)np), rad(np), mass(np), vel(3 * (size_t)np), angvel(3 * (size_t)np),
+        quat(4 * (size_t)np), initpos(3 * (size_t)np);
+    for (int i = 0; i < np; ++i) {
+      double op[3], f[3], sh[3];
+      int dynb = 1, rotb = 1;
+      is >> pos[3 * i] >> pos[3 * i + 1] >> pos[3 * i + 2] >> rad[i] >> ids[i] >> tags[i] >> mass[i] >> initpos[3 * i]
+         >> initpos[3 * i + 1] >> initpos[3 * i + 2] >> op[0] >> op[1] >> op[2] >> vel[3 * i] >> vel[3 * i + 1]
+         >> vel[3 * i + 2] >> f[0] >> f[1] >> f[2] >> sh[0] >> sh[1] >> sh[2] >> dynb;
+      for (int k = 0; k < 3; ++k) initpos[3 * i + k] += sh[k];
+      quat[4 * i] = 1.0;
+      if (rot) {
+        double inert;
+        is >> inert >> quat[4 * i] >> quat[4 * i + 1] >> quat[4 * i + 2] >> quat[4 * i + 3] >> angvel[3 * i]
+           >> angvel[3 * i + 1] >> angvel[3 * i + 2] >> rotb;
+      }
+      if (!is) fail("bad particle record " + std::to_string(i));
+      flags[i] = (dynb ? 0 : 1) | (rotb ? 0 : 2);
+    }
+    add_particles(np, ids.data(), tags.data(), pos.data(), rad.data(), mass.data(), vel.data(),
+                  rot ? angvel.data() : nullptr, rot ? quat.data() : nullptr, flags.data());
+    for (int i = 0; i < np; ++i) {
+      auto sl = id2slot.find(ids[i]);
+      if (sl != id2slot.end())
+        for (int k = 0; k < 3; ++k) h_initpos[3 * (size_t)sl->second + k] = initpos[3 * i + k];
+    }
+    std::vector<double4> pr(n);
+    if (n) DEM_CUDA(cudaMemcpyAsync(pr.data(), P.buf[cur].pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+    sync();
+    // bonded groups, name order (the reference's map order)
+    unsigned nbg = 0;
+    is >> nbg;
+    if (!is || nbg != bond.size()) fail("the number of bonded groups differs from the script's");
+    for (auto& it : bond) {
+      BondGroup& B = it.second;
+      std::string type;
+      int nconn = 0;
+      is >> type >> nconn;
+      if (!is || type != "RotBonded") fail("expected RotBonded interactions, got " + type);
+      std::vector<std::pair<unsigned long long, double4>> rec;
+      for (int q = 0; q < nconn; ++q) {
+        int a, b, init, scl, mr, tag;
+        double kr, ks, kb, kt, tr, b1, b2, mn, ms, mt, mb, Dx, Dy, Dz;
+        is >> a >> b >> init >> kr >> ks >> kb >> kt >> scl >> mr >> tr >> b1 >> b2 >> mn >> ms >> mt >> mb >> Dx >> Dy
+           >> Dz >> tag;
+        if (!is) fail("bad RotBonded record " + std::to_string(q));
+        if (a > b) { std::swap(a, b); Dx = -Dx; Dy = -Dy; Dz = -Dz; }  // p1 is the lower id
+        auto ia = id2slot.find(a), ib = id2slot.find(b);
+        if (ia == id2slot.end() || ib == id2slot.end()) continue;  // "particles ... not present"
+        rec.push_back({((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second,
+                       make_double4(Dx, Dy, Dz, 0.0)});
+      }
+      std::sort(rec.begin(), rec.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+      rec.erase(std::unique(rec.begin(), rec.end(), [](const auto& x, const auto& y) { return x.first == y.first; }),
+                rec.end());
+      B.nb = (int)rec.size();
+      const int nb = std::max(B.nb, 1);
+      B.keys.reserve(nb); B.ends.reserve(nb); B.D0.reserve(nb); B.broken_step.reserve(nb);
+      B.cap_events = std::max(1024, B.nb);
+      B.events.reserve(3 * B.cap_events); B.nevents.reserve(1);
+      std::vector<unsigned long long> keys(B.nb);
+      std::vector<int2> ends(B.nb);
+      std::vector<double4> D0(B.nb);
+      std::vector<int> alive(B.nb, kBondAlive);
+      for (int k = 0; k < B.nb; ++k) {
+        keys[k] = rec[k].first;
+        ends[k] = make_int2((int)(keys[k] >> 32), (int)(keys[k] & 0xffffffffu));
+        D0[k] = rec[k].second;
+      }
+      if (B.nb) {
+        DEM_CUDA(cudaMemcpyAsync(B.keys.p, keys.data(), sizeof(unsigned long long) * B.nb, cudaMemcpyHostToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(B.ends.p, ends.data(), sizeof(int2) * B.nb, cudaMemcpyHostToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(B.D0.p, D0.data(), sizeof(double4) * B.nb, cudaMemcpyHostToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(B.broken_step.p, alive.data(), sizeof(int) * B.nb, cudaMemcpyHostToDevice, s));
+      }
+      DEM_CUDA(cudaMemsetAsync(B.nevents.p, 0, sizeof(int), s));
+      build_adjacency(B.keys, B.nb, B.adj_start, B.adj_count, B.adj_cursor, B.p1_start, B.adj);
+      sync();
+    }
+    // RotFriction groups: the pairs and histories become the list the next search updates
+    unsigned nsave = 0;
+    is >> nsave;
+    unsigned want = 0;
+    for (auto& it : dyn) want += it.second.kind == 1 ? 1 : 0;
+    if (!is || nsave != want) fail("the number of RotFriction groups differs from the script's");
+    for (auto& it : dyn) {
+      DynGroup& G = it.second;
+      if (G.kind != 1) continue;
+      std::string type;
+      is >> type;
+      if (!is || type != "RotFriction") fail("expected RotFriction interactions, got " + type);
+      // One record per line up to the group's blank line.  The first line is the record count
+      // (this library's files) or, in the reference's files, the count run together with the
+      // first record's scaled normal stiffness, which is not read back.
+      std::string line;
+      std::getline(is, line);  // the rest of the type line
+      std::vector<std::string> lines;
+      long long count = -1;
+      while (std::getline(is, line)) {
+        if (line.find_first_not_of(" \t\r") == std::string::npos) {
+          if (count >= 0 || !lines.empty()) break;
+          continue;
+        }
+        std::istringstream ls(line);
+        std::vector<std::string> tok;
+        for (std::string w; ls >> w;) tok.push_back(w);
+        if (count < 0 && lines.empty() && tok.size() == 1) { count = std::stoll(tok[0]); if (count == 0) break; continue; }
+        lines.push_back(line);
+        if (count >= 0 && (long long)lines.size() == count) break;
+      }
+      std::vector<std::pair<unsigned long long, double4>> rec;
+      for (size_t q = 0; q < lines.size(); ++q) {
+        std::istringstream ls(lines[q]);
+        std::string k;  // scaled normal stiffness (or the count run together with it): not read back
+        double r0, mud, mus, ks, dtg, fx, fy, fz;
+        int scl, mr, a, b, slip, touch;
+        ls >> k >> r0 >> mud >> mus >> ks >> dtg >> scl >> mr >> a >> b >> slip >> touch >> fx >> fy >> fz;
+        if (!ls) fail("bad RotFriction record " + std::to_string(q));
+        if (a > b) { std::swap(a, b); fx = -fx; fy = -fy; fz = -fz; }  // the history is the force on p1
+        auto ia = id2slot.find(a), ib = id2slot.find(b);
+        if (ia == id2slot.end() || ib == id2slot.end()) continue;
+        rec.push_back({((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second,
+                       make_double4(fx, fy, fz, (double)((slip ? 1 : 0) + (touch ? 2 : 0)))});
+      }
+      std::sort(rec.begin(), rec.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+      rec.erase(std::unique(rec.begin(), rec.end(), [](const auto& x, const auto& y) { return x.first == y.first; }),
+                rec.end());
+      G.m = (int)rec.size();
+      const int m = std::max(G.m, 1);
+      G.keys.reserve(m);
+      for (int c = 0; c < 2; ++c) G.hist[c].reserve(m);
+      if (fp32) for (int c = 0; c < 2; ++c) G.hist32[c].reserve(m);
+      std::vector<unsigned long long> keys(G.m);
+      std::vector<double4> h(G.m);
+      for (int q = 0; q < G.m; ++q) { keys[q] = rec[q].first; h[q] = rec[q].second; }
+      if (G.m) {
+        DEM_CUDA(cudaMemcpyAsync(G.keys.p, keys.data(), sizeof(unsigned long long) * G.m, cudaMemcpyHostToDevice, s));
+        DEM_CUDA(cudaMemcpyAsync(G.hist[cur].p, h.data(), sizeof(double4) * G.m, cudaMemcpyHostToDevice, s));
+        if (fp32) launch_hist_convert(G.m, G.hist[cur].p, G.hist32[cur].p, true, s);
+      }
+      sync();
+    }
+    // walls
+    std::string token;
+    int nw = 0;
+    is >> token >> nw;
+    if (!is || token != "Walls") fail("expected Walls, got " + token);
+    download_walls();
+    for (int k = 0; k < nw; ++k) {
+      std::string name;
+      Wall W;
+      is >> name >> W.o[0] >> W.o[1] >> W.o[2] >> W.old[0] >> W.old[1] >> W.old[2] >> W.n[0] >> W.n[1] >> W.n[2];
+      if (!is) fail("bad wall record");
+      walls[name] = W;
+    }
+    upload_walls();
+    for (const char* sec : {"Spheres", "TriMesh", "Mesh2D"}) {
+      int cnt = 0;
+      is >> token >> cnt;
+      if (!is || token != sec) fail(std::string("expected ") + sec + ", got " + token);
+      if (cnt != 0) fail(std::string(sec) + " are not part of this worker");
+    }
+    // CLatticeMaster::loadCheckPointData (Parallel/LatticeMaster.cpp:780-820): the step counter,
+    // then searchNeighbors(true) and updateInteractions
+    t = timestep;
+    DEM_CUDA(cudaMemcpyAsync(d_step.p, &t, sizeof(long long), cudaMemcpyHostToDevice, s));
+    sync();
+    search_neighbors();
+    resize_adjacency();
+    pending_ctrl = 0;
+  }
+
   void set_group_param(const std::string& group, const std::string& key, double v) {
     auto b = bond.find(group);
     if (b != bond.end()) {
@@ -1877,7 +2240,7 @@ int dem_add_wall(dem_sim* h, const char* name, const double* o, const double* nr
   return guard(h, [&](DemSim& s) {
     s.download_walls();
     dem::Wall w;
-    for (int k = 0; k < 3; ++k) { w.o[k] = o[k]; w.n[k] = nrm[k]; }
+    for (int k = 0; k < 3; ++k) { w.o[k] = o[k]; w.n[k] = nrm[k]; w.old[k] = o[k]; }
     s.walls[name] = w;
     s.upload_walls();
     return DEM_OK;
@@ -2477,6 +2840,29 @@ int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_pa
 int dem_window_rewind(dem_sim* h) {
   return guard(h, [&](DemSim& s) {
     s.window_rewind();
+    return DEM_OK;
+  });
+}
+
+int dem_save_checkpoint(dem_sim* h, const char* path, int precision) {
+  return guard(h, [&](DemSim& s) {
+    if (!path) throw std::invalid_argument("null path");
+    std::ofstream os(path);
+    if (!os) throw std::invalid_argument(std::string("cannot open ") + path + " for writing");
+    os.precision(precision > 0 ? precision : 12);  // CheckPointer::saveRestartable (Parallel/CheckPointer.cpp:48-66)
+    s.save_checkpoint(os);
+    os.close();
+    if (!os) throw std::runtime_error(std::string("writing ") + path + " failed");
+    return DEM_OK;
+  });
+}
+
+int dem_load_checkpoint(dem_sim* h, const char* path, long long timestep) {
+  return guard(h, [&](DemSim& s) {
+    if (!path) throw std::invalid_argument("null path");
+    std::ifstream is(path);
+    if (!is) throw std::invalid_argument(std::string("cannot open ") + path);
+    s.load_checkpoint(is, timestep);
     return DEM_OK;
   });
 }

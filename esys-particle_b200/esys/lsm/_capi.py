@@ -68,6 +68,8 @@ SIGNATURES = {
     "dem_ensemble_last_error": (_S, [_P]),
     "dem_ensemble_step": (C.c_int, [_P, C.c_int]),
     "dem_search_neighbors": (C.c_int, [_P]),
+    "dem_save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
+    "dem_load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
     "dem_window_release": (C.c_int, [_P]),
     "dem_ensemble_window_forward": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_D)]),
     "dem_ensemble_window_adjoint": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
@@ -399,6 +401,14 @@ class DemSim:
     def window_release(self):
         """Free the last window's checkpoints and reverse-pass buffers."""
         self._chk(self.lib.dem_window_release(self.h))
+
+    def save_checkpoint(self, path, precision=12):
+        """Write the worker file of a restart checkpoint (dem_save_checkpoint)."""
+        self._chk(self.lib.dem_save_checkpoint(self.h, os.fsencode(path), int(precision)))
+
+    def load_checkpoint(self, path, timestep):
+        """Read a worker file into this (particle-less) worker and set its step counter."""
+        self._chk(self.lib.dem_load_checkpoint(self.h, os.fsencode(path), int(timestep)))
 
     def search_neighbors(self):
         """Neighbour search and interaction update at the head of the next step (force-neutral;

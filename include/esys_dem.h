@@ -262,6 +262,27 @@ int dem_window_adjoint(dem_sim* h, const double* grad_reactions, double* grad_pa
  * so that the window can be run again with other parameters. */
 int dem_window_rewind(dem_sim* h);
 
+/* Restart checkpoints: the worker's file of TSubLattice::saveCheckPointData
+ * (Parallel/SubLattice.hpp:3600-3673), in its text layout and iostream formatting with
+ * `precision` significant digits (CheckPointer::saveRestartable, Parallel/CheckPointer.cpp:48-66;
+ * 12 if <= 0): the particle block (ParallelParticleArray::saveCheckPointData, CRotParticle
+ * records), each RotBond group's restart records, each RotFriction group's pair records with
+ * their tangential history, the walls.  The master's info file (CheckPointInfo) is the caller's
+ * (esys.lsm.LsmMpi.createRestartCheckPointer writes both).  One difference: the reference writes
+ * a RotFriction group's record count and first record with no separator between them; a newline
+ * is written here so that the count reads back. */
+int dem_save_checkpoint(dem_sim* h, const char* path, int precision);
+
+/* TSubLattice::loadCheckPointData (Parallel/SubLattice.hpp:3675-3790) into a worker without
+ * particles whose groups the script has created (as in the reference): particles, the bonds of
+ * each RotBond group with their creation vectors, each RotFriction group's pairs and histories,
+ * the walls (created or replaced); then, as CLatticeMaster::loadCheckPointData
+ * (Parallel/LatticeMaster.cpp:780-820), the step counter is set to `timestep` and the neighbour
+ * search and interaction update run.  Pair histories survive for the pairs still touching, as
+ * PIS_ED::update keeps them.  The per-interaction constants in the file are not read back: they
+ * follow from the groups' parameters. */
+int dem_load_checkpoint(dem_sim* h, const char* path, long long timestep);
+
 /* Frees the last window's checkpoints and reverse-pass buffers (no rewind or adjoint after). */
 int dem_window_release(dem_sim* h);
 

@@ -66,6 +66,8 @@ def _lib(backend: str):
         "num_breaks": (C.c_int, [_P]),
         "get_breaks": (C.c_int, [_P, _I, _I, _I]),
         "move_tagged": (C.c_int, [_P, C.c_int, C.c_int, _D]),
+        "save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
+        "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
         "timestep": (C.c_longlong, [_P]),
     }
     fns = {}
@@ -193,6 +195,18 @@ class OracleSim:
         arr = (C.c_char_p * max(ns, 1))(*[x.encode() for x in seeds])
         self._chk(self.f["window_dual"](self.h, int(nsteps), ns, arr, _dp(R), _dp(dR)))
         return R, dR[..., :ns]
+
+    def save_checkpoint(self, path, precision=12):
+        """Restart checkpoint worker file written by the reference's own writers (reference backend)."""
+        if "save_checkpoint" not in self.f:
+            raise NotImplementedError(f"{self.backend} does not write checkpoints")
+        self._chk(self.f["save_checkpoint"](self.h, str(path).encode(), int(precision)))
+
+    def load_checkpoint(self, path, timestep):
+        """Load a restart checkpoint worker file with the reference's own readers (reference backend)."""
+        if "load_checkpoint" not in self.f:
+            raise NotImplementedError(f"{self.backend} does not read checkpoints")
+        self._chk(self.f["load_checkpoint"](self.h, str(path).encode(), int(timestep)))
 
     def move_tagged(self, tag, d, mask=-1):
         self._chk(self.f["move_tagged"](self.h, tag, mask, _dp(_v3(d))))

@@ -26,6 +26,7 @@
  * name-ordered maps exactly as TSubLattice does (Parallel/SubLattice.h:86-96).
  */
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <set>
 #include <string>
@@ -96,6 +97,8 @@ struct ASim {
   virtual int get_breaks(int* id1, int* id2, int* step) = 0;
   virtual int move_tagged(int tag, int mask, const double* d) = 0;
   virtual long long timestep() = 0;
+  virtual int save_checkpoint(const char* path, int precision) = 0;
+  virtual int load_checkpoint(const char* path, long long timestep) = 0;
 };
 
 template <class T>
@@ -206,6 +209,64 @@ struct RefSim : public ASim {
       oneStep();
     }
     return 0;
+  }
+
+  /* TSubLattice::saveCheckPointData (Parallel/SubLattice.hpp:3600-3673): the reference's own
+   * writers (particle array, bonded and saving dynamic storages, walls) in its order. */
+  int save_checkpoint(const char* path, int precision) override {
+    std::ofstream os(path);
+    if (!os) { err = "cannot open checkpoint file"; return -1; }
+    os.precision(precision);
+    const std::string delim = "\n";
+    ppa->saveCheckPointData(os);
+    os << bpis.size() << delim;
+    for (auto& b : bpis) { b.second->saveCheckPointData(os); os << delim; }
+    int count_save = 0;
+    for (auto& d : dpis) if (d.second->willSave()) count_save++;
+    os << count_save << delim;
+    for (auto& d : dpis)
+      if (d.second->willSave()) { d.second->saveCheckPointData(os); os << delim; }
+    os << "Walls " << walls.size() << delim;
+    for (auto& w : walls) { os << w.first << delim; w.second->writeCheckPoint(os, delim); }
+    os << "Spheres " << 0 << delim << "TriMesh " << 0 << delim << "Mesh2D " << 0 << delim;
+    return os ? 0 : -1;
+  }
+  /* TSubLattice::loadCheckPointData (Parallel/SubLattice.hpp:3675-3790), then the master's
+   * searchNeighbors(true) + updateInteractions (Parallel/LatticeMaster.cpp:780-820).  A wall that
+   * the script created is loaded in place, so that its interaction groups keep pointing at it. */
+  int load_checkpoint(const char* path, long long timestep) override {
+    std::ifstream is(path);
+    if (!is) { err = "cannot open checkpoint file"; return -1; }
+    ppa->loadCheckPointData(is);
+    ppa->rebuild();
+    unsigned nb = 0, nd = 0;
+    is >> nb;
+    if (nb != bpis.size()) { err = "bonded group count differs"; return -1; }
+    for (auto& b : bpis) b.second->loadCheckPointData(is);
+    is >> nd;
+    if (nd != dpis.size()) { err = "dynamic group count differs"; return -1; }
+    for (auto& d : dpis) d.second->loadCheckPointData(is);
+    std::string token;
+    int nw = 0;
+    is >> token >> nw;
+    if (token != "Walls") { err = "expected Walls"; return -1; }
+    for (int i = 0; i < nw; ++i) {
+      std::string name;
+      is >> name;
+      auto it = walls.find(name);
+      if (it != walls.end()) {
+        it->second->loadCheckPoint(is);
+      } else {
+        CWall* w = new CWall();
+        w->loadCheckPoint(is);
+        walls[name] = w;
+      }
+    }
+    t = timestep;
+    first = false;
+    searchNeighbors();
+    updateInteractions();
+    return is ? 0 : -1;
   }
 
   int add_particles(int n, const int* id, const int* tag, const double* pos, const double* rad, const double* mass,
@@ -490,6 +551,8 @@ int ref_get_pairs(void* h, const char* g, int* a, int* b, double* st) { return s
 int ref_num_breaks(void* h) { return static_cast<ASim*>(h)->num_breaks(); }
 int ref_get_breaks(void* h, int* a, int* b, int* s) { return static_cast<ASim*>(h)->get_breaks(a, b, s); }
 int ref_move_tagged(void* h, int tag, int mask, const double* d) { return static_cast<ASim*>(h)->move_tagged(tag, mask, d); }
+int ref_save_checkpoint(void* h, const char* path, int precision) { return static_cast<ASim*>(h)->save_checkpoint(path, precision); }
+int ref_load_checkpoint(void* h, const char* path, long long t) { return static_cast<ASim*>(h)->load_checkpoint(path, t); }
 long long ref_timestep(void* h) { return static_cast<ASim*>(h)->timestep(); }
 }
 

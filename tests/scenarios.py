@@ -103,6 +103,69 @@ def bonded_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, strength=(0.5, 1.0, 1.
     return sim
 
 
+def bonded_block_script(make, nx=5, ny=6, nz=5, dt=1e-5, strength=(0.5, 1.0, 1.0, 0.5), with_friction=True):
+    """The restart script of bonded_block: the same domain, groups, walls and damping, and no
+    particles or connections (they come from the checkpoint, as with LsmMpi.loadCheckPoint)."""
+    Ly = ny * 1.0
+    sim = make("RotSphere", 1.25, 0.2, (0, 0, 0), (nx * 1.0, Ly, nz * 1.0), (0, 0, 0), dt)
+    mn, ms, mt, mb = strength
+    sim.add_rot_bond_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, mn, ms, mt, mb, True, True, 1.0)
+    if with_friction:
+        sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
+        sim.add_exclusion("bonds", "friction")
+    sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, Ly, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e5)
+    sim.add_wall_group("top_w", "top", 1e5)
+    sim.add_damping(0, 0.01, 50)
+    sim.add_damping(1, 0.01, 50)
+    return sim
+
+
+def parse_checkpoint(path):
+    """Restart-checkpoint worker file -> dict: particles {id: fields}, bonds {(id1, id2): fields},
+    friction {(id1, id2): fields}, walls {name: 9 values}.  Reads this library's files and the
+    reference's (whose RotFriction record count runs into the first record's first field)."""
+    lines = open(path).read().split("\n")
+    pos = [0]
+
+    def nxt(blank_ok=False):
+        while pos[0] < len(lines):
+            ln = lines[pos[0]].split()
+            pos[0] += 1
+            if ln or blank_ok:
+                return ln
+        raise ValueError("unexpected end of checkpoint")
+
+    out = {"base": nxt() + nxt(), "particles": {}, "bonds": {}, "friction": {}, "walls": {}}
+    for _ in range(int(nxt()[0])):
+        t = nxt()
+        out["particles"][int(t[4])] = [float(x) for x in t]
+    for _ in range(int(nxt()[0])):
+        assert nxt()[0] == "RotBonded"
+        for _ in range(int(nxt()[0])):
+            t = nxt()
+            out["bonds"][(int(t[0]), int(t[1]))] = [float(x) for x in t]
+    for _ in range(int(nxt()[0])):
+        assert nxt()[0] == "RotFriction"
+        t = nxt()
+        recs = []
+        if len(t) == 1:
+            recs = [nxt() for _ in range(int(t[0]))]
+        else:
+            while t:
+                recs.append(t)
+                t = nxt(blank_ok=True)
+        for r in recs:
+            out["friction"][(int(r[8]), int(r[9]))] = [float(x) for x in r[1:]]
+    t = nxt()
+    assert t[0] == "Walls"
+    for _ in range(int(t[1])):
+        name = nxt()[0]
+        out["walls"][name] = [float(x) for x in nxt()]
+    return out
+
+
 def run_loaded(sim, steps, rate):
     """Advance with a platen loader: both platens move toward each other by
     ``rate`` per step (a pre-step runnable like WallLoaderRunnable)."""
