@@ -1474,6 +1474,63 @@ struct DemSim {
     os << "Mesh2D " << 0 << "\n";
   }
 
+  // Snapshot (visualisation / post-processing) file of TSubLattice::saveSnapShotData
+  // (Parallel/SubLattice.hpp:3552-3594): 9 significant digits, CParticle / CRotParticle
+  // snapshot records (Model/Particle.cpp:443-456, Model/RotParticle.cpp:494-503), then each bonded
+  // group's (id1, id2, tag) records (pis/pi_storage_eb.hpp:54-71, BondedInteractionCpData).
+  void save_snapshot(std::ostream& os) {
+    const std::streamsize oldprec = os.precision(9);
+    std::vector<double4> pr(n), vm(n), wi(n), qq(n), op(n), fo(n);
+    std::vector<unsigned> pf(n);
+    std::vector<int> tg(n);
+    if (n) {
+      const ParticleBuf& b = P.buf[cur];
+      DEM_CUDA(cudaMemcpyAsync(pr.data(), b.pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(vm.data(), b.vm, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(wi.data(), b.wi, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(qq.data(), b.qq, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(op.data(), P.oldpos, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      if (store_forces) DEM_CUDA(cudaMemcpyAsync(fo.data(), P.force, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(tg.data(), P.tag, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    }
+    sync();
+    const char d = ' ';
+    int alive = 0;
+    for (int i = 0; i < n; ++i) alive += (pf[i] & PF_ALIVE) ? 1 : 0;
+    os << alive << "\n";
+    for (int i = 0; i < n; ++i) {
+      if (!(pf[i] & PF_ALIVE)) continue;
+      os << pr[i].x << d << pr[i].y << d << pr[i].z << d << pr[i].w << d << h_id[i] << d << tg[i] << d << vm[i].w << d
+         << h_initpos[3 * (size_t)i] << d << h_initpos[3 * (size_t)i + 1] << d << h_initpos[3 * (size_t)i + 2] << d
+         << op[i].x << d << op[i].y << d << op[i].z << d << vm[i].x << d << vm[i].y << d << vm[i].z << d
+         << fo[i].x << d << fo[i].y << d << fo[i].z << d << 0.0 << d << 0.0 << d << 0.0;
+      if (rot)
+        os << d << qq[i].x << d << qq[i].y << d << qq[i].z << d << qq[i].w << d << wi[i].x << d << wi[i].y << d
+           << wi[i].z;
+      os << "\n";
+    }
+    os << bond.size() << "\n";
+    for (auto& it : bond) {
+      BondGroup& B = it.second;
+      std::vector<int2> ends(B.nb);
+      std::vector<int> bs(B.nb);
+      if (B.nb) {
+        DEM_CUDA(cudaMemcpyAsync(ends.data(), B.ends.p, sizeof(int2) * B.nb, cudaMemcpyDeviceToHost, s));
+        DEM_CUDA(cudaMemcpyAsync(bs.data(), B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToHost, s));
+      }
+      sync();
+      int intact = 0;
+      for (int k = 0; k < B.nb; ++k) intact += bs[k] > t ? 1 : 0;
+      os << "RotBonded" << "\n" << intact;
+      for (int k = 0; k < B.nb; ++k)
+        if (bs[k] > t) os << "\n" << h_id[ends[k].x] << d << h_id[ends[k].y] << d << B.tag;
+      os << "\n";
+    }
+    os << "TMIG " << 0 << "\n";
+    os.precision(oldprec);
+  }
+
   // Reads a worker file into this worker: particles (into an empty worker), each bonded group's
   // bonds with their creation vectors, each RotFriction group's pairs with their tangential
   // history (carried through the neighbour search that follows, for the pairs still touching, as
@@ -2851,6 +2908,18 @@ int dem_save_checkpoint(dem_sim* h, const char* path, int precision) {
     if (!os) throw std::invalid_argument(std::string("cannot open ") + path + " for writing");
     os.precision(precision > 0 ? precision : 12);  // CheckPointer::saveRestartable (Parallel/CheckPointer.cpp:48-66)
     s.save_checkpoint(os);
+    os.close();
+    if (!os) throw std::runtime_error(std::string("writing ") + path + " failed");
+    return DEM_OK;
+  });
+}
+
+int dem_save_snapshot(dem_sim* h, const char* path) {
+  return guard(h, [&](DemSim& s) {
+    if (!path) throw std::invalid_argument("null path");
+    std::ofstream os(path);
+    if (!os) throw std::invalid_argument(std::string("cannot open ") + path + " for writing");
+    s.save_snapshot(os);
     os.close();
     if (!os) throw std::runtime_error(std::string("writing ") + path + " failed");
     return DEM_OK;

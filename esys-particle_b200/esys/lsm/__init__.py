@@ -15,6 +15,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import _capi
+from .checkpoint import CheckPointer, CheckPointPrms, RestartCheckPointPrms, read_info, walls_in, worker_file
 from .fields import (FieldSaver, InteractionScalarFieldSaverPrms, ParticleScalarFieldSaverPrms,
                      WallVectorFieldSaverPrms)
 from .util import BoundingBox, Vec3
@@ -23,6 +24,7 @@ __all__ = [
     "LsmMpi", "NRotSphere", "RotSphere", "Runnable", "NRotElasticPrms", "RotFrictionPrms", "RotBondPrms",
     "NRotElasticWallPrms", "LinDampingPrms", "RotDampingPrms", "GravityPrms", "Vec3", "BoundingBox",
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
+    "CheckPointPrms", "RestartCheckPointPrms",
 ]
 
 
@@ -191,6 +193,7 @@ class LsmMpi:
         self._pending = []  # particles created before setSpatialDomain
         self._walls = {}
         self._wig_of_wall = {}
+        self._bbox, self._circ = None, (False, False, False)
 
     # -- set-up (LsmMpiPy.cpp:2187-2300) --
     def initNeighbourSearch(self, particleType, gridSpacing, verletDist):
@@ -227,6 +230,7 @@ class LsmMpi:
         if any(circDimList[1:]):
             raise NotImplementedError("periodic y or z is not on the GPU path (x only)")
         mn, mx = bBox.getMinPt(), bBox.getMaxPt()
+        self._bbox, self._circ = (list(mn), list(mx)), tuple(bool(c) for c in circDimList)
         self._sim = self._backend(self._ptype, self._grid, self._skin, list(mn), list(mx),
                                  (1 if circDimList[0] else 0, 0, 0), self._dt)
         if self._pending:
@@ -338,6 +342,30 @@ class LsmMpi:
     #    LatticeMaster.cpp:2612-2700) --
     def createFieldSaver(self, prms):
         self._savers.append(FieldSaver(prms))
+
+    # -- checkpoints (LsmMpiPy.cpp:847-884, 2807-2840; CheckPointController) --
+    def createRestartCheckPointer(self, prms):
+        self._savers.append(CheckPointer(self, prms, restart=True))
+
+    # the reference gathers the workers' data through the master; with one worker the files are the same
+    createCheckPointerWriteThroughMaster = createRestartCheckPointer
+
+    def createCheckPointer(self, prms):
+        """Snapshots for visualisation / post-processing (LsmMpiPy::createSnapShots)."""
+        self._savers.append(CheckPointer(self, prms, restart=False))
+
+    def loadCheckPoint(self, fileName):
+        """CLatticeMaster::loadCheckPointData (Parallel/LatticeMaster.cpp:780-820): the info file's
+        geometry (if no spatial domain was set), the step counter, and the worker file into this
+        particle-less worker, whose interaction groups the script has created."""
+        info = read_info(fileName)
+        if self._sim is None:
+            self.setSpatialDomain(BoundingBox(Vec3(*info["bbox_min"]), Vec3(*info["bbox_max"])), info["periodic"])
+        wf = worker_file(fileName, info)
+        self._sim.load_checkpoint(wf, info["t"])
+        for name in walls_in(wf):
+            self._walls[name] = True
+        self._saved0 = True  # the initial-state savers ran in the original run
 
     def _save_fields(self, t):
         for f in self._savers:

@@ -70,6 +70,7 @@ SIGNATURES = {
     "dem_search_neighbors": (C.c_int, [_P]),
     "dem_save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
     "dem_load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
+    "dem_save_snapshot": (C.c_int, [_P, _S]),
     "dem_window_release": (C.c_int, [_P]),
     "dem_ensemble_window_forward": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_D)]),
     "dem_ensemble_window_adjoint": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
@@ -405,6 +406,10 @@ class DemSim:
     def save_checkpoint(self, path, precision=12):
         """Write the worker file of a restart checkpoint (dem_save_checkpoint)."""
         self._chk(self.lib.dem_save_checkpoint(self.h, os.fsencode(path), int(precision)))
+
+    def save_snapshot(self, path):
+        """Write the worker file of a snapshot (dem_save_snapshot)."""
+        self._chk(self.lib.dem_save_snapshot(self.h, os.fsencode(path)))
 
     def load_checkpoint(self, path, timestep):
         """Read a worker file into this (particle-less) worker and set its step counter."""

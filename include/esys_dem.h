@@ -273,6 +273,11 @@ int dem_window_rewind(dem_sim* h);
  * is written here so that the count reads back. */
 int dem_save_checkpoint(dem_sim* h, const char* path, int precision);
 
+/* Snapshot (visualisation) file of TSubLattice::saveSnapShotData (Parallel/SubLattice.hpp:3552-3594):
+ * 9 significant digits; particle snapshot records, then each RotBond group's (id1, id2, tag) records.
+ * The master's info file is the caller's (esys.lsm.LsmMpi.createCheckPointer writes both). */
+int dem_save_snapshot(dem_sim* h, const char* path);
+
 /* TSubLattice::loadCheckPointData (Parallel/SubLattice.hpp:3675-3790) into a worker without
  * particles whose groups the script has created (as in the reference): particles, the bonds of
  * each RotBond group with their creation vectors, each RotFriction group's pairs and histories,
