@@ -78,7 +78,7 @@ struct WallDev {
 // One dynamic interaction group (PIS_NE elastic or PIS_ED rot friction) as
 // seen by the step kernel: a per-particle adjacency over the group's pairs.
 struct DynDev {
-  int kind;             // 0 NRotElastic, 1 RotFriction
+  int kind;             // 0 NRotElastic, 1 RotFriction, 2 NRotFriction (CFrictionInteraction; mu in mu_s)
   double k, ks, mu_s, mu_d, dt;
   int scaling, meanR;
   const int* adj_start; // n+1
@@ -94,6 +94,8 @@ struct DynDev {
 };
 
 struct BondDev {
+  int kind;                 // 0 RotBond (ARotBondedInteraction), 1 NRotBond (CBondedInteraction)
+  double knb, rbreak;       // NRotBond: normal stiffness (unscaled), relative breaking distance (< 0: unbreakable)
   double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
   int scaling, meanR;
   const int* adj_start;

@@ -684,11 +684,19 @@ void launch_bond_pass_f64(const StepArgs& a, bool eval, cudaStream_t s) {
 }
 
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s) {
-  bool el = false, fr = false;
-  for (int d = 0; d < a.ndyn; ++d) (a.dyn[d].kind == 0 ? el : fr) = true;
+  bool el = false, fr = false, widened = false;
+  for (int d = 0; d < a.ndyn; ++d) {
+    if (a.dyn[d].kind == 2) widened = true;
+    (a.dyn[d].kind == 0 ? el : fr) = true;
+  }
+  for (int d = 0; d < a.nbond; ++d) widened = widened || a.bond[d].kind == 1;
   const bool bd = a.nbond > 0;
   const bool gather = bd && a.bond[0].bf;  // bonds evaluated once by the bond pass
   if (gather) launch_bond_pass<false, false>(a, s);
+  if (widened) {  // NRotFriction / NRotBond groups: one general instance per particle type
+    if (!rot) return launch_step_tpp<false, F_ELASTIC | F_NFRIC | F_BGATHER, false, false>(a, tpp, s);
+    return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_NFRIC | F_BGATHER, false, false>(a, tpp, s);
+  }
   if (split) {
     if (!rot) return launch_split_tpp<false, F_ELASTIC, false>(a, tpp, s);
     if (!bd && fr && !el) return launch_split_tpp<true, F_FRIC, false>(a, tpp, s);

@@ -119,6 +119,76 @@ __device__ __forceinline__ void law_friction(double k_eff, double ks_eff, double
   law_friction_t<double>(k_eff, ks_eff, mu_s, mu_d, dt, x1, r1, v1, w1, x2, r2, v2, w2, Ffric, slipping, o);
 }
 
+// CBondedInteraction (NRotBond): constructor scaling (Model/BondedInteraction.cpp:43-69) and
+// calcForces (:126-140).  The rest length is r1 + r2; F is applied to p2, -F to p1 (no moments:
+// CParticle::applyForce adds the force only, Model/Particle.cpp:391-400).
+__device__ __forceinline__ double nbond_k(double k, int scaling, double r1, double r2) {
+  double effR = 1.0, effA = 1.0, effL = 1.0;
+  const double r0 = r1 + r2;
+  if (scaling) {
+    effR = 0.5 * r0;
+    effL = r0;
+    effA = effR * effR;
+  }
+  return k * effA / effL;
+}
+__device__ __forceinline__ void law_nbond(double k_eff, const V& x1, double r1, const V& x2, double r2, V& F,
+                                          double& dist) {
+  const V D = x1 - x2;
+  const double r0 = r1 + r2;
+  dist = sqrt(dot(D, D));
+  F = D * (k_eff * (dist - r0) / dist);
+}
+// CBondedInteraction::broken (:101-114): extension beyond r0 * rbreak; rbreak < 0 marks the group
+// unbreakable (ParallelInteractionStorage_EB::setUnbreakable, SubLattice.hpp:1818-1821).
+__device__ __forceinline__ bool nbond_broken(double dist, double r1, double r2, double rbreak) {
+  const double r0 = r1 + r2;
+  return rbreak >= 0.0 && (dist - r0) > r0 * rbreak;
+}
+
+// CFrictionInteraction (NRotFriction): constructor scaling (Model/FrictionInteraction.cpp:57-75)
+// and calcForces (:93-149): an elastic normal force and a tangential force from the relative
+// translation only, one friction coefficient; forces only (no moments).
+__device__ __forceinline__ void nfriction_k(double k, double ks, int scaling, double r1, double r2, double& k_eff,
+                                            double& ks_eff) {
+  double f = 1.0;
+  if (scaling) f = 0.5 * (r1 + r2);
+  k_eff = f * k;
+  ks_eff = f * ks;
+}
+__device__ __forceinline__ void law_nfriction(double k_eff, double ks_eff, double mu, double dt, const V& x1, double r1,
+                                              const V& v1, const V& x2, double r2, const V& v2, V Ffric,
+                                              FricOut& o) {
+  const V D = x1 - x2;
+  const double eq_dist = r1 + r2;
+  double dist = dot(D, D);
+  if (dist < (eq_dist * eq_dist)) {
+    dist = sqrt(dist);
+    const V force = D * (k_eff * (dist - eq_dist) / dist);
+    const V d1 = v1 * dt;
+    const V d2 = v2 * dt;
+    V ds = d2 - d1;
+    ds -= ((dot(ds, D)) / (norm2(D))) * D;
+    Ffric += ks_eff * ds;
+    const double FfricNorm = norm(Ffric);
+    const double forceNorm = norm(force);
+    if (FfricNorm > forceNorm * mu) {
+      Ffric = Ffric * ((mu * forceNorm) / FfricNorm);
+      o.slipping = true;
+    } else {
+      o.slipping = false;
+    }
+    o.fn = force;
+    o.Ffric = Ffric;
+    o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+    o.touching = true;
+  } else {
+    o.Ffric = o.fn = o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+    o.slipping = false;
+    o.touching = false;
+  }
+}
+
 // CRotFrictionInteraction::isPersistent (Model/RotFricInteraction.cpp:345-351).
 __device__ __forceinline__ bool friction_persistent(const V& x1, double r1, const V& x2, double r2) {
   V D = x1 - x2;

@@ -94,6 +94,8 @@ struct DynGroup {
 };
 
 struct BondGroup {
+  int kind = 0;                 // 0 RotBond, 1 NRotBond (CBondedInteraction)
+  double knb = 0, rbreak = 0;   // NRotBond: normalK, relative breaking distance (< 0: unbreakable)
   int tag;
   double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
   int scaling, meanR;
@@ -352,9 +354,12 @@ struct DemSim {
   void set_precision(int want) {
     want = want ? 1 : 0;
     if (want == fp32) return;
+    if (want)
+      for (auto& d : dyn)
+        if (d.second.kind == 2) throw std::invalid_argument("NRotFriction groups run in the FP64 form only");
     for (auto& d : dyn) {
       DynGroup& G = d.second;
-      if (G.kind != 1 || G.m == 0) continue;
+      if (G.kind == 0 || G.m == 0) continue;
       const int m = G.m;
       for (int b = 0; b < 2; ++b) { G.hist[b].reserve(m); G.hist32[b].reserve(m); }
       launch_hist_convert(m, G.hist[cur].p, G.hist32[cur].p, want == 1, s);
@@ -508,17 +513,17 @@ struct DemSim {
     const int m = read_int(scalars.p);
     c_launches += 3;
     G.keys_spare.reserve(std::max(m, 1));
-    if (G.kind == 1) G.hist_spare.reserve(std::max(m, 1));
+    if (G.kind != 0) G.hist_spare.reserve(std::max(m, 1));
     if (fp32) {
-      if (G.kind == 1) G.hist32_spare.reserve(std::max(m, 1));
-      launch_pairs_write<float4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind,
+      if (G.kind != 0) G.hist32_spare.reserve(std::max(m, 1));
+      launch_pairs_write<float4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind != 0 ? 1 : 0,
                                  G.keys.p, G.m, G.hist32[cur].p, G.hist32_spare.p, s);
     } else {
-      launch_pairs_write<double4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind,
+      launch_pairs_write<double4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind != 0 ? 1 : 0,
                                   G.keys.p, G.m, G.hist[cur].p, G.hist_spare.p, s);
     }
     std::swap(G.keys, G.keys_spare);
-    if (G.kind == 1) {
+    if (G.kind != 0) {
       if (fp32) {
         std::swap(G.hist32[cur], G.hist32_spare);
         G.hist32[cur ^ 1].reserve(std::max(m, 1));
@@ -539,7 +544,7 @@ struct DemSim {
   // (ntable.hpp:628-664; pi_storage_ne.hpp:80-98, pi_storage_ed.hpp:130-155).
   void dyn_new_update(DynGroup& G) {
     ExclDev ex = excl_of(G);
-    const int check_in = G.kind == 1;  // PIS_NE appends without the isIn test
+    const int check_in = G.kind != 0;  // PIS_NE appends without the isIn test
     scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
     launch_newlist_count(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_i.p, s);
     scan_tmp.reserve(scan_tmp_ints(n + 2));
@@ -553,14 +558,14 @@ struct DemSim {
       const int m2 = G.m + nb;
       G.keys_spare.reserve(m2);
       if (fp32) {
-        if (G.kind == 1) G.hist32_spare.reserve(m2);
-        launch_merge<float4>(G.keys.p, G.hist32[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist32_spare.p, G.kind, s);
+        if (G.kind != 0) G.hist32_spare.reserve(m2);
+        launch_merge<float4>(G.keys.p, G.hist32[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist32_spare.p, G.kind != 0 ? 1 : 0, s);
       } else {
-        if (G.kind == 1) G.hist_spare.reserve(m2);
-        launch_merge<double4>(G.keys.p, G.hist[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist_spare.p, G.kind, s);
+        if (G.kind != 0) G.hist_spare.reserve(m2);
+        launch_merge<double4>(G.keys.p, G.hist[cur].p, G.m, G.cand.p, nb, G.keys_spare.p, G.hist_spare.p, G.kind != 0 ? 1 : 0, s);
       }
       std::swap(G.keys, G.keys_spare);
-      if (G.kind == 1) {
+      if (G.kind != 0) {
         if (fp32) {
           std::swap(G.hist32[cur], G.hist32_spare);
           G.hist32[cur ^ 1].reserve(m2);
@@ -657,8 +662,8 @@ struct DemSim {
     if (on == (handoff != 0)) return;
     if (on)
       for (auto& d : dyn)
-        if (d.second.kind != 1)
-          throw std::invalid_argument("the device bond hand-off needs every dynamic group to be RotFriction");
+        if (d.second.kind == 0)
+          throw std::invalid_argument("the device bond hand-off needs every dynamic group to be RotFriction or NRotFriction");
     handoff = on;
     if (!d_brk.p) {
       d_brk.reserve(2);
@@ -667,6 +672,15 @@ struct DemSim {
     launch_clear_flags(n, P.flagged, s);
     // the dynamic lists are rebuilt in the new form before the next step
     if (!first) pending_ctrl |= CTRL_REBUILD;
+  }
+
+  // NRotFriction groups or NRotBond groups present: the FP64 general instances run the step
+  // (bonds through the bond pass); the FP32 form, the batched ensemble and differentiable
+  // windows are not built for them.
+  bool widened() const {
+    for (auto& d : dyn) if (d.second.kind == 2) return true;
+    for (auto& b : bond) if (b.second.kind == 1) return true;
+    return false;
   }
 
   // interactions evaluated per step: Verlet pairs + intact bonds + wall candidates
@@ -711,13 +725,15 @@ struct DemSim {
     for (auto& b : bond) {
       BondGroup& B = b.second;
       BondDev& D = a.bond[a.nbond++];
+      D.kind = B.kind; D.knb = B.knb; D.rbreak = B.rbreak;
       D.kr = B.kr; D.ks = B.ks; D.kt = B.kt; D.kb = B.kb; D.mn = B.mn; D.ms = B.ms; D.mt = B.mt; D.mb = B.mb;
       D.truncated = B.truncated; D.scaling = B.scaling; D.meanR = B.meanR;
       D.adj_start = B.adj_start.p; D.adj = B.adj.p; D.D0 = B.D0.p; D.broken_step = B.broken_step.p;
       D.events = B.events.p; D.nevents = B.nevents.p; D.cap_events = B.cap_events;
       D.nb_launch = B.nb;
       D.ends = B.ends.p;
-      if (bond_pass || fp32) {  // the FP32 form always takes its bonds from the FP64 bond pass
+      // the FP32 form and the widened laws always take their bonds from the FP64 bond pass
+      if (bond_pass || fp32 || widened()) {
         B.bf.reserve((size_t)3 * std::max(B.nb, 1));
         D.bf = B.bf.p;
       }
@@ -892,6 +908,7 @@ struct DemSim {
   bool win_begin(int T, int K) {
     if (T < 1 || K < 1) throw std::invalid_argument("window length and checkpoint interval must be >= 1");
     if (iter_lin > 255 || iter_rot > 255) throw std::invalid_argument("window damping needs maxIterations <= 255");
+    if (widened()) throw std::invalid_argument("the differentiable window covers NRotElastic, RotFriction and RotBond groups");
     win.valid = false;
     if (!prepare()) return false;
     const int nd = (int)dyn.size();
@@ -1385,6 +1402,29 @@ struct DemSim {
       // a bond that failed in the last step stays listed until the next update, as in the reference
       int intact = 0;
       for (int k = 0; k < B.nb; ++k) intact += bs[k] > t ? 1 : 0;
+      if (B.kind == 1) {
+        // CBondedInteraction::saveRestartData (Model/BondedInteraction.cpp:283-293); m_dist is the
+        // distance of the last force evaluation, whose positions are the other particle buffer
+        std::vector<double4> pl(n);
+        if (n) DEM_CUDA(cudaMemcpyAsync(pl.data(), P.buf[cur ^ 1].pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+        sync();
+        os << "Bonded" << "\n" << intact;
+        for (int k = 0; k < B.nb; ++k) {
+          if (!(bs[k] > t)) continue;
+          const int i = ends[k].x, j = ends[k].y;
+          const double r0 = pr[i].w + pr[j].w;
+          double effR = 1.0, effA = 1.0, effL = 1.0;
+          if (B.scaling) { effR = 0.5 * r0; effL = r0; effA = effR * effR; }
+          double dx = pl[i].x - pl[j].x, dy = pl[i].y - pl[j].y, dz = pl[i].z - pl[j].z;
+          if (g.circx) {  // minimum image, as the step kernel forms the pair
+            if (dx > 0.5 * g.Lx) dx -= g.Lx; else if (dx < -0.5 * g.Lx) dx += g.Lx;
+          }
+          os << "\n" << B.knb * effA / effL << " " << r0 << " " << std::sqrt(dx * dx + dy * dy + dz * dz) << " "
+             << r0 * B.rbreak << " " << (B.scaling ? 1 : 0) << " " << h_id[i] << " " << h_id[j] << " " << B.tag << "\n";
+        }
+        os << "\n";
+        continue;
+      }
       os << "RotBonded" << "\n";
       os << intact;
       for (int k = 0; k < B.nb; ++k) {
@@ -1405,11 +1445,11 @@ struct DemSim {
     // (pis/pi_storage_ed.hpp:202-214).  The reference writes the record count and the first record
     // with no separator; a newline is written here so that the count can be read back.
     int nsave = 0;
-    for (auto& it : dyn) nsave += it.second.kind == 1 ? 1 : 0;
+    for (auto& it : dyn) nsave += it.second.kind != 0 ? 1 : 0;
     os << nsave << "\n";
     for (auto& it : dyn) {
       DynGroup& G = it.second;
-      if (G.kind != 1) continue;
+      if (G.kind == 0) continue;
       std::vector<unsigned long long> keys(G.m);
       std::vector<double4> h(G.m);
       std::vector<int> xb(handoff ? G.m : 0);
@@ -1440,11 +1480,19 @@ struct DemSim {
         if (handoff && xb[k] >= 0 && bsteps[xb[k] >> 28][xb[k] & 0x0fffffff] > t) continue;
         listed.push_back(k);
       }
-      os << "RotFriction" << "\n";
+      os << (G.kind == 1 ? "RotFriction" : "Friction") << "\n";
       os << listed.size() << "\n";
       for (int k : listed) {
         const int i = (int)(keys[k] >> 32), j = (int)(keys[k] & 0xffffffffu);
         const double r1 = pr[i].w, r2 = pr[j].w;
+        if (G.kind == 2) {  // CFrictionInteraction::saveRestartData (Model/FrictionInteraction.cpp:628-643)
+          const double f = G.scaling ? 0.5 * (r1 + r2) : 1.0;
+          const int fl = (int)h[k].w;
+          os << f * G.k << " " << r1 + r2 << " " << G.mu_s << " " << f * G.ks << " " << G.dt << " "
+             << (G.scaling ? 1 : 0) << " " << h_id[i] << " " << h_id[j] << " " << (fl & 1) << " " << ((fl >> 1) & 1)
+             << " " << h[k].x << " " << h[k].y << " " << h[k].z << "\n";
+          continue;
+        }
         // scaled stiffnesses as CRotFrictionInteraction's constructor forms them (Model/RotFricInteraction.cpp:103-146)
         double effR = 1.0, effL = 1.0, effA = 1.0;
         const double r0 = r1 + r2;
@@ -1584,9 +1632,20 @@ struct DemSim {
       std::string type;
       int nconn = 0;
       is >> type >> nconn;
-      if (!is || type != "RotBonded") fail("expected RotBonded interactions, got " + type);
+      const std::string want_type = B.kind == 1 ? "Bonded" : "RotBonded";
+      if (!is || type != want_type) fail("expected " + want_type + " interactions, got " + type);
       std::vector<std::pair<unsigned long long, double4>> rec;
-      for (int q = 0; q < nconn; ++q) {
+      for (int q = 0; q < nconn && B.kind == 1; ++q) {  // CBondedInteraction::loadRestartData (:300-312)
+        double k, r0, dist, brk;
+        int scl, a, b, tag;
+        is >> k >> r0 >> dist >> brk >> scl >> a >> b >> tag;
+        if (!is) fail("bad Bonded record " + std::to_string(q));
+        if (a > b) std::swap(a, b);
+        auto ia = id2slot.find(a), ib = id2slot.find(b);
+        if (ia == id2slot.end() || ib == id2slot.end()) continue;
+        rec.push_back({((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second, make_double4(0, 0, 0, 0)});
+      }
+      for (int q = 0; q < nconn && B.kind == 0; ++q) {
         int a, b, init, scl, mr, tag;
         double kr, ks, kb, kt, tr, b1, b2, mn, ms, mt, mb, Dx, Dy, Dz;
         is >> a >> b >> init >> kr >> ks >> kb >> kt >> scl >> mr >> tr >> b1 >> b2 >> mn >> ms >> mt >> mb >> Dx >> Dy
@@ -1629,14 +1688,15 @@ struct DemSim {
     unsigned nsave = 0;
     is >> nsave;
     unsigned want = 0;
-    for (auto& it : dyn) want += it.second.kind == 1 ? 1 : 0;
-    if (!is || nsave != want) fail("the number of RotFriction groups differs from the script's");
+    for (auto& it : dyn) want += it.second.kind != 0 ? 1 : 0;
+    if (!is || nsave != want) fail("the number of friction groups differs from the script's");
     for (auto& it : dyn) {
       DynGroup& G = it.second;
-      if (G.kind != 1) continue;
+      if (G.kind == 0) continue;
       std::string type;
       is >> type;
-      if (!is || type != "RotFriction") fail("expected RotFriction interactions, got " + type);
+      const std::string want_type = G.kind == 1 ? "RotFriction" : "Friction";
+      if (!is || type != want_type) fail("expected " + want_type + " interactions, got " + type);
       // One record per line up to the group's blank line.  The first line is the record count
       // (this library's files) or, in the reference's files, the count run together with the
       // first record's scaled normal stiffness, which is not read back.
@@ -1661,9 +1721,12 @@ struct DemSim {
         std::istringstream ls(lines[q]);
         std::string k;  // scaled normal stiffness (or the count run together with it): not read back
         double r0, mud, mus, ks, dtg, fx, fy, fz;
-        int scl, mr, a, b, slip, touch;
-        ls >> k >> r0 >> mud >> mus >> ks >> dtg >> scl >> mr >> a >> b >> slip >> touch >> fx >> fy >> fz;
-        if (!ls) fail("bad RotFriction record " + std::to_string(q));
+        int scl, mr = 0, a, b, slip, touch;
+        if (G.kind == 1)
+          ls >> k >> r0 >> mud >> mus >> ks >> dtg >> scl >> mr >> a >> b >> slip >> touch >> fx >> fy >> fz;
+        else  // CFrictionInteraction::loadRestartData (Model/FrictionInteraction.cpp:651-666)
+          ls >> k >> r0 >> mud >> ks >> dtg >> scl >> a >> b >> slip >> touch >> fx >> fy >> fz;
+        if (!ls) fail("bad " + want_type + " record " + std::to_string(q));
         if (a > b) { std::swap(a, b); fx = -fx; fy = -fy; fz = -fz; }  // the history is the force on p1
         auto ia = id2slot.find(a), ib = id2slot.find(b);
         if (ia == id2slot.end() || ib == id2slot.end()) continue;
@@ -1733,9 +1796,9 @@ struct DemSim {
     if (d != dyn.end()) {
       DynGroup& G = d->second;
       if (key == "normalK") G.k = v;
-      else if (key == "shearK" && G.kind == 1) G.ks = v;
-      else if (key == "dynamicMu" && G.kind == 1) G.mu_d = v;
-      else if (key == "staticMu" && G.kind == 1) G.mu_s = v;
+      else if (key == "shearK" && G.kind != 0) G.ks = v;
+      else if (key == "dynamicMu" && G.kind != 0) G.mu_d = v;
+      else if (key == "staticMu" && G.kind != 0) G.mu_s = v;
       else throw std::invalid_argument("unknown parameter " + key + " of group " + group);
       return;
     }
@@ -1824,8 +1887,10 @@ struct Ensemble {
       sims.push_back(list[k]);
     }
     rot = sims[0]->rot;
-    for (DemSim* d : sims)
+    for (DemSim* d : sims) {
       if (d->rot != rot) throw std::invalid_argument("ensemble specimens must share the particle type");
+      if (d->widened()) throw std::invalid_argument("the batched ensemble covers NRotElastic, RotFriction and RotBond groups");
+    }
     DEM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     const int ns = (int)sims.size();
     d_args.reserve((size_t)2 * ns);
@@ -2246,6 +2311,50 @@ int guard(dem_sim* h, F&& f) {
 }
 }  // namespace
 
+// The bonds of a new bonded group from the connections of its tag, p1 the lower id
+// (PIS_E::tryInsert, pi_storage_e.hpp:222-263); `set` fills the group's parameters.
+template <class F>
+static void add_bond_group(DemSim& s, const char* name, int tag, F&& set) {
+    if ((int)s.bond.size() >= dem::kMaxBond) throw std::invalid_argument("too many bonded interaction groups");
+    std::vector<unsigned> pf(s.n);
+    if (s.n) {
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), s.P.pflags, sizeof(unsigned) * s.n, cudaMemcpyDeviceToHost, s.s));
+      s.sync();
+    }
+    std::set<std::pair<int, int>> seen;
+    std::vector<unsigned long long> keys;
+    const std::vector<int>& c = s.temp_conn[tag];
+    for (size_t i = 0; i + 1 < c.size(); i += 2) {
+      int a = std::min(c[i], c[i + 1]), b = std::max(c[i], c[i + 1]);
+      if (!seen.insert({a, b}).second) continue;
+      auto ia = s.id2slot.find(a), ib = s.id2slot.find(b);
+      if (ia == s.id2slot.end() || ib == s.id2slot.end()) continue;
+      if (!(pf[ia->second] & dem::PF_ALIVE) || !(pf[ib->second] & dem::PF_ALIVE)) continue;
+      keys.push_back(((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second);
+    }
+    std::sort(keys.begin(), keys.end());
+    dem::BondGroup& B = s.bond[name];
+    B.tag = tag;
+    set(B);
+    B.nb = (int)keys.size();
+    const int nb = std::max(B.nb, 1);
+    B.keys.reserve(nb); B.ends.reserve(nb); B.D0.reserve(nb); B.broken_step.reserve(nb);
+    B.cap_events = std::max(1024, B.nb);
+    B.events.reserve(3 * B.cap_events); B.nevents.reserve(1);
+    std::vector<int2> ends(B.nb);
+    for (int i = 0; i < B.nb; ++i) ends[i] = make_int2((int)(keys[i] >> 32), (int)(keys[i] & 0xffffffffu));
+    std::vector<int> alive(B.nb, dem::kBondAlive);
+    if (B.nb) {
+      DEM_CUDA(cudaMemcpyAsync(B.keys.p, keys.data(), sizeof(unsigned long long) * B.nb, cudaMemcpyHostToDevice, s.s));
+      DEM_CUDA(cudaMemcpyAsync(B.ends.p, ends.data(), sizeof(int2) * B.nb, cudaMemcpyHostToDevice, s.s));
+      DEM_CUDA(cudaMemcpyAsync(B.broken_step.p, alive.data(), sizeof(int) * B.nb, cudaMemcpyHostToDevice, s.s));
+    }
+    DEM_CUDA(cudaMemsetAsync(B.nevents.p, 0, sizeof(int), s.s));
+    dem::launch_bonds_init(B.nb, B.ends.p, s.P.buf[s.cur].pr, B.D0.p, s.s);
+    s.build_adjacency(B.keys, B.nb, B.adj_start, B.adj_count, B.adj_cursor, B.p1_start, B.adj);
+    s.sync();
+}
+
 extern "C" {
 
 int dem_create(dem_sim** out, int particle_type, double grid_spacing, double verlet_dist, const double* bbox_min,
@@ -2327,49 +2436,42 @@ int dem_add_rot_friction_group(dem_sim* h, const char* name, double k, double mu
   });
 }
 
+// TSubLattice::addPairIG, type "Friction" (Parallel/SubLattice.hpp:1055-1076): CFrictionIGP in its
+// packing order (k, mu, k_s, dt, scaling).
+int dem_add_nrot_friction_group(dem_sim* h, const char* name, double k, double mu, double ks, double dt, int scaling) {
+  return guard(h, [&](DemSim& s) {
+    if ((int)s.dyn.size() >= dem::kMaxDyn) throw std::invalid_argument("too many dynamic interaction groups");
+    if (s.fp32) throw std::invalid_argument("NRotFriction groups run in the FP64 form only");
+    dem::DynGroup& G = s.dyn[name];
+    G.kind = 2; G.k = k; G.mu_s = mu; G.mu_d = mu; G.ks = ks; G.dt = dt; G.scaling = scaling != 0; G.meanR = 0;
+    s.resize_adjacency();
+    return DEM_OK;
+  });
+}
+
 // TRotSubLattice::addRotBondedIG (RotSubLattice.hpp:116-186) with PIS_E::tryInsert (pi_storage_e.hpp:222-263).
 int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
                            double mn, double ms, double mt, double mb, int scaling, int meanR, double truncated) {
   return guard(h, [&](DemSim& s) {
     if (!s.rot) throw std::invalid_argument("RotBond needs RotSphere particles");
-    if ((int)s.bond.size() >= dem::kMaxBond) throw std::invalid_argument("too many bonded interaction groups");
-    std::vector<unsigned> pf(s.n);
-    if (s.n) {
-      DEM_CUDA(cudaMemcpyAsync(pf.data(), s.P.pflags, sizeof(unsigned) * s.n, cudaMemcpyDeviceToHost, s.s));
-      s.sync();
-    }
-    std::set<std::pair<int, int>> seen;
-    std::vector<unsigned long long> keys;
-    const std::vector<int>& c = s.temp_conn[tag];
-    for (size_t i = 0; i + 1 < c.size(); i += 2) {
-      int a = std::min(c[i], c[i + 1]), b = std::max(c[i], c[i + 1]);
-      if (!seen.insert({a, b}).second) continue;
-      auto ia = s.id2slot.find(a), ib = s.id2slot.find(b);
-      if (ia == s.id2slot.end() || ib == s.id2slot.end()) continue;
-      if (!(pf[ia->second] & dem::PF_ALIVE) || !(pf[ib->second] & dem::PF_ALIVE)) continue;
-      keys.push_back(((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second);
-    }
-    std::sort(keys.begin(), keys.end());
-    dem::BondGroup& B = s.bond[name];
-    B.tag = tag; B.kr = kr; B.ks = ks; B.kt = kt; B.kb = kb; B.mn = mn; B.ms = ms; B.mt = mt; B.mb = mb;
-    B.scaling = scaling != 0; B.meanR = meanR != 0; B.truncated = truncated;
-    B.nb = (int)keys.size();
-    const int nb = std::max(B.nb, 1);
-    B.keys.reserve(nb); B.ends.reserve(nb); B.D0.reserve(nb); B.broken_step.reserve(nb);
-    B.cap_events = std::max(1024, B.nb);
-    B.events.reserve(3 * B.cap_events); B.nevents.reserve(1);
-    std::vector<int2> ends(B.nb);
-    for (int i = 0; i < B.nb; ++i) ends[i] = make_int2((int)(keys[i] >> 32), (int)(keys[i] & 0xffffffffu));
-    std::vector<int> alive(B.nb, dem::kBondAlive);
-    if (B.nb) {
-      DEM_CUDA(cudaMemcpyAsync(B.keys.p, keys.data(), sizeof(unsigned long long) * B.nb, cudaMemcpyHostToDevice, s.s));
-      DEM_CUDA(cudaMemcpyAsync(B.ends.p, ends.data(), sizeof(int2) * B.nb, cudaMemcpyHostToDevice, s.s));
-      DEM_CUDA(cudaMemcpyAsync(B.broken_step.p, alive.data(), sizeof(int) * B.nb, cudaMemcpyHostToDevice, s.s));
-    }
-    DEM_CUDA(cudaMemsetAsync(B.nevents.p, 0, sizeof(int), s.s));
-    dem::launch_bonds_init(B.nb, B.ends.p, s.P.buf[s.cur].pr, B.D0.p, s.s);
-    s.build_adjacency(B.keys, B.nb, B.adj_start, B.adj_count, B.adj_cursor, B.p1_start, B.adj);
-    s.sync();
+    add_bond_group(s, name, tag, [&](dem::BondGroup& B) {
+      B.kind = 0;
+      B.kr = kr; B.ks = ks; B.kt = kt; B.kb = kb; B.mn = mn; B.ms = ms; B.mt = mt; B.mb = mb;
+      B.scaling = scaling != 0; B.meanR = meanR != 0; B.truncated = truncated;
+    });
+    return DEM_OK;
+  });
+}
+
+// TSubLattice::addBondedIG (Parallel/SubLattice.hpp:1791-1831): CBondedIGP (tag, k, rbreak, scaling);
+// rbreak < 0 makes the group unbreakable.
+int dem_add_nrot_bond_group(dem_sim* h, const char* name, int tag, double k, double rbreak, int scaling) {
+  return guard(h, [&](DemSim& s) {
+    add_bond_group(s, name, tag, [&](dem::BondGroup& B) {
+      B.kind = 1;
+      B.knb = k; B.rbreak = rbreak; B.scaling = scaling != 0; B.meanR = 0;
+      B.kr = B.ks = B.kt = B.kb = B.mn = B.ms = B.mt = B.mb = 0.0; B.truncated = 1.0;
+    });
     return DEM_OK;
   });
 }
@@ -2420,10 +2522,10 @@ int dem_add_exclusion(dem_sim* h, const char* bonded, const char* dynamic) {
     if (G.m > 0) {  // clean out pairs that are now excluded, keeping the others' history
       dem::BondGroup& B = s.bond[bonded];
       std::vector<unsigned long long> keys(G.m), bk(B.nb);
-      std::vector<double4> hist(G.kind == 1 ? G.m : 0);
+      std::vector<double4> hist(G.kind != 0 ? G.m : 0);
       std::vector<int> bs(B.nb);
       DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
-      if (G.kind == 1) DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
+      if (G.kind != 0) DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
       if (B.nb) {
         DEM_CUDA(cudaMemcpyAsync(bk.data(), B.keys.p, sizeof(unsigned long long) * B.nb, cudaMemcpyDeviceToHost, s.s));
         DEM_CUDA(cudaMemcpyAsync(bs.data(), B.broken_step.p, sizeof(int) * B.nb, cudaMemcpyDeviceToHost, s.s));
@@ -2434,12 +2536,12 @@ int dem_add_exclusion(dem_sim* h, const char* bonded, const char* dynamic) {
       for (int i = 0; i < G.m; ++i) {
         auto p = std::lower_bound(bk.begin(), bk.end(), keys[i]);
         bool ex = p != bk.end() && *p == keys[i] && bs[p - bk.begin()] == dem::kBondAlive;
-        if (!ex) { k2.push_back(keys[i]); if (G.kind == 1) h2.push_back(hist[i]); }
+        if (!ex) { k2.push_back(keys[i]); if (G.kind != 0) h2.push_back(hist[i]); }
       }
       G.m = (int)k2.size();
       if (G.m) {
         DEM_CUDA(cudaMemcpyAsync(G.keys.p, k2.data(), sizeof(unsigned long long) * G.m, cudaMemcpyHostToDevice, s.s));
-        if (G.kind == 1) DEM_CUDA(cudaMemcpyAsync(G.hist[s.cur].p, h2.data(), sizeof(double4) * G.m, cudaMemcpyHostToDevice, s.s));
+        if (G.kind != 0) DEM_CUDA(cudaMemcpyAsync(G.hist[s.cur].p, h2.data(), sizeof(double4) * G.m, cudaMemcpyHostToDevice, s.s));
       }
       s.build_adjacency(G.keys, G.m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
       s.sync();
@@ -2603,10 +2705,10 @@ int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* sta
                                      cudaMemcpyDeviceToHost, s.s));
         }
       }
-      std::vector<double4> hist(G.kind == 1 ? G.m : 0);
-      std::vector<float4> hist32(G.kind == 1 && s.fp32 ? G.m : 0);
+      std::vector<double4> hist(G.kind != 0 ? G.m : 0);
+      std::vector<float4> hist32(G.kind != 0 && s.fp32 ? G.m : 0);
       if (G.m) DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
-      if (G.kind == 1 && G.m) {
+      if (G.kind != 0 && G.m) {
         if (s.fp32) DEM_CUDA(cudaMemcpyAsync(hist32.data(), G.hist32[s.cur].p, sizeof(float4) * G.m, cudaMemcpyDeviceToHost, s.s));
         else DEM_CUDA(cudaMemcpyAsync(hist.data(), G.hist[s.cur].p, sizeof(double4) * G.m, cudaMemcpyDeviceToHost, s.s));
       }
@@ -2620,7 +2722,7 @@ int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* sta
         id2[o] = s.h_id[(int)(keys[i] & 0xffffffffu)];
         if (state) {
           for (int c = 0; c < 5; ++c) state[5 * o + c] = 0.0;
-          if (G.kind == 1) {
+          if (G.kind != 0) {
             const int fl = (int)hist[i].w;
             const bool touching = (fl & 2) != 0;
             if (touching) { state[5 * o] = hist[i].x; state[5 * o + 1] = hist[i].y; state[5 * o + 2] = hist[i].z; }
@@ -2805,16 +2907,17 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto d = s.dyn.find(gname);
     if (d != s.dyn.end()) {
       dem::DynGroup& G = d->second;
+      if (G.kind == 2) throw std::invalid_argument("interaction fields of NRotFriction groups are not built");
       int code = f == "count" ? 0 : f == "potential_energy" ? 1 : -1;
-      if (G.kind == 1 && f == "slipping") code = 2;
-      if (G.kind == 1 && f == "sticking") code = 3;
+      if (G.kind != 0 && f == "slipping") code = 2;
+      if (G.kind != 0 && f == "sticking") code = 3;
       if (code < 0) throw std::invalid_argument("unknown interaction scalar field " + f + " of group " + gname);
       std::vector<double> v(G.m, 0.0);
       if (s.t > 0 && G.m) {
         s.scratch_d.reserve(G.m);
         launch_pair_field(s.g, s.P, prev, G.keys.p, G.m, G.kind, G.k, G.ks, G.scaling, G.meanR,
-                          G.kind == 1 && !s.fp32 ? G.hist[s.cur].p : nullptr,
-                          G.kind == 1 && s.fp32 ? G.hist32[s.cur].p : nullptr, code, s.scratch_d.p, s.s);
+                          G.kind != 0 && !s.fp32 ? G.hist[s.cur].p : nullptr,
+                          G.kind != 0 && s.fp32 ? G.hist32[s.cur].p : nullptr, code, s.scratch_d.p, s.s);
         DEM_CUDA(cudaMemcpyAsync(v.data(), s.scratch_d.p, sizeof(double) * G.m, cudaMemcpyDeviceToHost, s.s));
       }
       // the pairs dem_get_pairs reports (the device hand-off keeps bond-held pairs it does not report)
@@ -2839,6 +2942,7 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     }
     auto b = s.bond.find(gname);
     if (b == s.bond.end()) throw std::invalid_argument("no such group " + gname);
+    if (b->second.kind == 1) throw std::invalid_argument("interaction fields of NRotBond groups are not built");
     static const char* names[] = {"count", "potential_energy", "e_pot_normal", "e_pot_shear", "e_pot_twist",
                                   "e_pot_bend", "breaking_criterion"};
     int code = -1;

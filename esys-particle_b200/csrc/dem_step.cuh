@@ -63,7 +63,8 @@ __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
 // does not carry the registers of the bond law).
 // F_BGATHER: bonds were evaluated by the bond pass (k_bond_pass, once per bond); the particle
 // gathers their forces and moments in its adjacency order instead of evaluating the law.
-enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8 };
+// F_NFRIC: NRotFriction groups (FP64 only).
+enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8, F_NFRIC = 16 };
 
 // Sum of the pair-group and bond contributions on particle i (all TPP lanes of
 // the particle call this; on return every lane holds the combined sums).  The
@@ -84,7 +85,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
   KSum3 Fk, Mk;                                      // FP32 form
   Fk.zero();
   Mk.zero();
-  if ((FEAT & (F_ELASTIC | F_FRIC)) && alive) {
+  if ((FEAT & (F_ELASTIC | F_FRIC | F_NFRIC)) && alive) {
     constexpr int kBatch = 1;
     Vf vself = mk(0.f, 0.f, 0.f), wself = vself;
     double4 v4 = make_double4(0.0, 0.0, 0.0, 0.0), w4 = v4;
@@ -92,7 +93,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
       const float4 r0 = __ldg(in.vw + 2 * i), r1 = __ldg(in.vw + 2 * i + 1);
       vself = mk(r0.x, r0.y, r0.z);
       wself = mk(r0.w, r1.x, r1.y);
-    } else if (FEAT & F_FRIC) {
+    } else if (FEAT & (F_FRIC | F_NFRIC)) {
       v4 = ldg4(in.vm + i);
       if (ROT) w4 = ldg4(in.wi + i);
     }
@@ -148,6 +149,31 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                   if (EVAL) Gs += (double)norm(f);
                 }
               }
+            }
+          } else if (G.kind == 2) {
+            if constexpr (!FP32 && (FEAT & F_NFRIC) != 0) {  // CFrictionInteraction::calcForces
+              if (!touching) {
+                if (isp1 && !EVAL) G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+                continue;
+              }
+              double keff, kseff;
+              nfriction_k(G.k, G.ks, G.scaling, pa.w, pb.w, keff, kseff);
+              const double4 vj = ldg4(in.vm + j);
+              const double4 va = isp1 ? v4 : vj, vb = isp1 ? vj : v4;
+              const double4 h = ldg4(G.hist_in + k);
+              FricOut o;
+              law_nfriction(keff, kseff, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
+              if (isp1) {  // p1: -force, then +Ffric; p2: +force, then -Ffric
+                Fp += -1.0 * o.fn;
+                Fp += o.Ffric;
+                if (!EVAL)
+                  G.hist_out[k] = make_double4(o.Ffric.x, o.Ffric.y, o.Ffric.z,
+                                               (o.slipping ? 1.0 : 0.0) + (o.touching ? 2.0 : 0.0));
+              } else {
+                Fp += o.fn;
+                Fp += -1.0 * o.Ffric;
+              }
+              if (EVAL) Gs += norm(o.fn) + norm(o.Ffric);
             }
           } else {
             if constexpr (ROT && (FEAT & F_FRIC) != 0) {
@@ -219,7 +245,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
   }
 
   // 4. bonded groups (PIS_EB::calcForces) + failure test (PIS_EB::update at the next step)
-  if constexpr (ROT && (FEAT & F_BGATHER) != 0) {
+  if constexpr ((FEAT & F_BGATHER) != 0) {
     if (alive) {
       for (int d = 0; d < a.nbond; ++d) {
         const BondDev& B = a.bond[d];
@@ -231,10 +257,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           const double4* r = B.bf + 3 * (size_t)k;
           if (en.y < 0) {
             Fp += xyz(ldg4(r));
-            Mp += xyz(ldg4(r + 1));
+            if (ROT) Mp += xyz(ldg4(r + 1));
           } else {
             Fp += -1.0 * xyz(ldg4(r));
-            Mp += xyz(ldg4(r + 2));
+            if (ROT) Mp += xyz(ldg4(r + 2));
           }
           if (EVAL) Gs += norm(xyz(ldg4(r)));
         }
@@ -513,6 +539,34 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
   if (B.broken_step[k] <= step) return;
   const ParticleBuf in = a.P.buf[a.cur];
   const int2 e = __ldg(B.ends + k);
+  if (B.kind == 1) {  // NRotBond: force on p2 F, on p1 -F, no moments
+    const double4 pa = ldg4(in.pr + e.x), pb = ldg4(in.pr + e.y);
+    const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+    V F;
+    double dist;
+    law_nbond(nbond_k(B.knb, B.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, F, dist);
+    double4* r = B.bf + 3 * (size_t)k;
+    r[0] = d4(-1.0 * F, 0.0);
+    r[1] = r[2] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (!EVAL && nbond_broken(dist, pa.w, pb.w, B.rbreak)) {
+      B.broken_step[k] = (int)(step + 1);
+      a.P.flagged[e.x] = 1;
+      a.P.flagged[e.y] = 1;
+      if (!a.replay) {
+        const int slot = atomicAdd(B.nevents, 1);
+        if (slot < B.cap_events) {
+          B.events[3 * slot] = a.P.id[e.x];
+          B.events[3 * slot + 1] = a.P.id[e.y];
+          B.events[3 * slot + 2] = (int)(step + 1);
+        } else {
+          atomicOr(a.ctrl, CTRL_OVERFLOW);
+        }
+        atomicOr(a.ctrl, CTRL_BROKE);
+      }
+      if (a.handoff) a.brk_step[step & 1] = (int)step;
+    }
+    return;
+  }
   const double4 pa = ldg4(in.pr + e.x), pb = ldg4(in.pr + e.y);
   const double4 qa = ldg4(in.qq + e.x), qb = ldg4(in.qq + e.y);
   const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
@@ -556,7 +610,8 @@ __global__ void __launch_bounds__(kBondPassThreads, 4) k_bond_pass(const StepArg
 
 // Fused step: pair sums and integration in one launch (small systems).
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
-__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? kFp32Blocks : 2)))
+__global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
+                                                : ((FEAT & F_NFRIC) ? 2 : ((FEAT & F_BGATHER) ? 4 : (FP32 ? kFp32Blocks : 2))))
     k_step(const StepArgs a) {
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;

@@ -24,7 +24,7 @@ __all__ = [
     "LsmMpi", "NRotSphere", "RotSphere", "Runnable", "NRotElasticPrms", "RotFrictionPrms", "RotBondPrms",
     "NRotElasticWallPrms", "LinDampingPrms", "RotDampingPrms", "GravityPrms", "Vec3", "BoundingBox",
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
-    "CheckPointPrms", "RestartCheckPointPrms",
+    "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms",
 ]
 
 
@@ -107,6 +107,18 @@ class RotBondPrms:  # InteractionParamsPy.cpp:414-547, 2048-2170
         self.normalBrkForce, self.shearBrkForce = float(normalBrkForce), float(shearBrkForce)
         self.torsionBrkForce, self.bendingBrkForce = float(torsionBrkForce), float(bendingBrkForce)
         self.scaling, self.meanR_scaling, self.truncated = bool(scaling), bool(meanR_scaling), float(truncated)
+
+
+class NRotFrictionPrms:  # InteractionParamsPy.cpp:1446-1480 (CFrictionIGP)
+    def __init__(self, name, normalK, dynamicMu, shearK, scaling=True):
+        self.name, self.normalK, self.dynamicMu, self.shearK = name, float(normalK), float(dynamicMu), float(shearK)
+        self.scaling = bool(scaling)
+
+
+class NRotBondPrms:  # InteractionParamsPy.cpp:1090-1130 (CBondedIGP)
+    def __init__(self, name, normalK, breakDistance, tag, scaling=True):
+        self.name, self.normalK, self.breakDistance, self.tag = name, float(normalK), float(breakDistance), int(tag)
+        self.scaling = bool(scaling)
 
 
 class NRotElasticWallPrms:  # WallPrmsPy.cpp:213-243
@@ -284,6 +296,10 @@ class LsmMpi:
             s.add_rot_bond_group(prms.name, prms.tag, prms.normalK, prms.shearK, prms.torsionK, prms.bendingK,
                                  prms.normalBrkForce, prms.shearBrkForce, prms.torsionBrkForce, prms.bendingBrkForce,
                                  prms.scaling, prms.meanR_scaling, prms.truncated)
+        elif isinstance(prms, NRotFrictionPrms):  # LsmMpiPy::createNRotFrictionInteractGrp sets dt
+            s.add_nrot_friction_group(prms.name, prms.normalK, prms.dynamicMu, prms.shearK, self._dt, prms.scaling)
+        elif isinstance(prms, NRotBondPrms):
+            s.add_nrot_bond_group(prms.name, prms.tag, prms.normalK, prms.breakDistance, prms.scaling)
         elif isinstance(prms, NRotElasticWallPrms):
             s.add_wall_group(prms.name, prms.wallName, prms.normalK)
             self._wig_of_wall[prms.name] = prms.wallName

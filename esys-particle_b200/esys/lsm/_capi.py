@@ -31,6 +31,8 @@ SIGNATURES = {
     "dem_add_elastic_group": (C.c_int, [_P, _S, C.c_double, C.c_int]),
     "dem_add_rot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 5 + [C.c_int, C.c_int]),
     "dem_add_rot_bond_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 8 + [C.c_int, C.c_int, C.c_double]),
+    "dem_add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
+    "dem_add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
     "dem_add_wall_group": (C.c_int, [_P, _S, _S, C.c_double]),
     "dem_add_gravity": (C.c_int, [_P, _S, _D]),
     "dem_add_damping": (C.c_int, [_P, C.c_int, C.c_double, C.c_int]),
@@ -173,6 +175,16 @@ class DemSim:
         self._chk(self.lib.dem_add_rot_friction_group(self.h, name.encode(), float(k), float(mu_s), float(mu_d),
                                                       float(k_s), float(dt), int(scaling), int(meanR_scaling)))
         self._dyn_prm[name] = (1, [float(k), float(k_s)])
+
+    def add_nrot_friction_group(self, name, k, mu, k_s, dt, scaling=True):
+        self._chk(self.lib.dem_add_nrot_friction_group(self.h, name.encode(), float(k), float(mu), float(k_s),
+                                                       float(dt), int(scaling)))
+        self._dyn_prm[name] = (2, [float(k), float(k_s)])
+
+    def add_nrot_bond_group(self, name, tag, k, rbreak, scaling=True):
+        self._chk(self.lib.dem_add_nrot_bond_group(self.h, name.encode(), int(tag), float(k), float(rbreak),
+                                                   int(scaling)))
+        self._bond_prm[name] = [float(k), 0.0, 0.0, 0.0]
 
     def add_rot_bond_group(self, name, tag, kr, ks, kt, kb, max_n, max_s, max_t, max_b, scaling=True,
                            meanR_scaling=True, truncated=1.0):

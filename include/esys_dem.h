@@ -72,6 +72,18 @@ int dem_add_elastic_group(dem_sim* h, const char* name, double k, int scaling);
 int dem_add_rot_friction_group(dem_sim* h, const char* name, double k, double mu_s, double mu_d, double ks,
                                double dt, int scaling, int meanR_scaling);
 
+/* TSubLattice::addPairIG, type "Friction" (NRotFrictionPrms; Parallel/SubLattice.hpp:1055-1076):
+ * CFrictionInteraction (Model/FrictionInteraction.cpp:57-149) with CFrictionIGP's packing order
+ * k, mu, k_s, dt, scaling.  Elastic normal force and tangential friction from the relative
+ * translation, forces only.  FP64 form; no differentiable window or batched ensemble. */
+int dem_add_nrot_friction_group(dem_sim* h, const char* name, double k, double mu, double ks, double dt, int scaling);
+
+/* TSubLattice::addBondedIG (NRotBondPrms; Parallel/SubLattice.hpp:1791-1831): CBondedInteraction
+ * (Model/BondedInteraction.cpp:43-140) between connections of `tag`; rest length r1 + r2, failure
+ * when the extension exceeds (r1 + r2) * rbreak; rbreak < 0: unbreakable.  Forces only.  No
+ * differentiable window or batched ensemble. */
+int dem_add_nrot_bond_group(dem_sim* h, const char* name, int tag, double k, double rbreak, int scaling);
+
 /* TRotSubLattice::addRotBondedIG (Parallel/RotSubLattice.hpp:116-186): bonds from the stored
  * connections with this tag, CRotBondedIGP fields in packing order; beta1 = beta2 = 1. */
 int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,

@@ -66,6 +66,8 @@ def _lib(backend: str):
         "num_breaks": (C.c_int, [_P]),
         "get_breaks": (C.c_int, [_P, _I, _I, _I]),
         "move_tagged": (C.c_int, [_P, C.c_int, C.c_int, _D]),
+        "add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
+        "add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
         "save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
         "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
         "timestep": (C.c_longlong, [_P]),
@@ -150,6 +152,18 @@ class OracleSim:
                            meanR_scaling=True, truncated=1.0):
         self._chk(self.f["add_rot_bond_group"](self.h, name.encode(), tag, kr, ks, kt, kb, max_n, max_s, max_t,
                                                max_b, int(scaling), int(meanR_scaling), truncated))
+
+    def add_nrot_friction_group(self, name, k, mu, k_s, dt, scaling=True):
+        """NRotFriction (CFrictionInteraction) group (reference backend)."""
+        if "add_nrot_friction_group" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no NRotFriction groups")
+        self._chk(self.f["add_nrot_friction_group"](self.h, name.encode(), k, mu, k_s, dt, int(scaling)))
+
+    def add_nrot_bond_group(self, name, tag, k, rbreak, scaling=True):
+        """NRotBond (CBondedInteraction) group (reference backend)."""
+        if "add_nrot_bond_group" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no NRotBond groups")
+        self._chk(self.f["add_nrot_bond_group"](self.h, name.encode(), int(tag), k, rbreak, int(scaling)))
 
     def add_wall_group(self, name, wall, k):
         self._chk(self.f["add_wall_group"](self.h, name.encode(), wall.encode(), k))

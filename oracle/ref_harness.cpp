@@ -38,10 +38,12 @@
 #include "Foundation/vec3.h"
 #include "Foundation/Quaternion.h"
 #include "Model/BodyForceGroup.h"
+#include "Model/BondedInteraction.h"
 #include "Model/Damping.h"
 #include "Model/DampingIGP.h"
 #include "Model/EWallInteractionGroup.h"
 #include "Model/ElasticInteraction.h"
+#include "Model/FrictionInteraction.h"
 #include "Model/Particle.h"
 #include "Model/RotBondedInteraction.h"
 #include "Model/RotDamping.h"
@@ -67,6 +69,14 @@ struct Exposed : public Base {
 
 struct BreakEvent { int id1, id2, step; };
 
+/* Read access to CFrictionInteraction's tangential force and flags (protected members), through
+ * pointers to members formed in a derived class. */
+struct FricAccess : CFrictionInteraction {
+  static Vec3 CFrictionInteraction::*ffric() { return &FricAccess::m_Ffric; }
+  static bool CFrictionInteraction::*slipping() { return &FricAccess::m_is_slipping; }
+  static bool CFrictionInteraction::*touching() { return &FricAccess::m_is_touching; }
+};
+
 struct ASim {
   virtual ~ASim() {}
   std::string err;
@@ -81,6 +91,8 @@ struct ASim {
   virtual int add_rot_bond(const char* name, int tag, double kr, double ks, double kt, double kb, double mn,
                            double ms, double mt, double mb, int scaling, int meanR, double trunc) = 0;
   virtual int add_wall_group(const char* name, const char* wall, double k) = 0;
+  virtual int add_nrot_friction(const char* name, double k, double mu, double ks, double dt, int scaling) = 0;
+  virtual int add_nrot_bond(const char* name, int tag, double k, double rbreak, int scaling) = 0;
   virtual int add_gravity(const char* name, const double* g) = 0;
   virtual int add_damping(int rot, double visc, int maxiter) = 0;
   virtual int add_exclusion(const char* b, const char* d) = 0;
@@ -119,6 +131,8 @@ struct RefSim : public ASim {
   /* typed handles for queries */
   std::map<std::string, Exposed<ParallelInteractionStorage_NE<T, CElasticInteraction>>*> elastic;
   std::map<std::string, void*> fric, bond;
+  std::map<std::string, Exposed<ParallelInteractionStorage_ED<T, CFrictionInteraction>>*> nfric;
+  std::map<std::string, Exposed<ParallelInteractionStorage_EB<T, CBondedInteraction>>*> nbond;
 
   RefSim(double gs, double vd, const double* mn, const double* mx, const int* circ, double dt_)
       : comm(MPI_COMM_WORLD), dt(dt_), nrange(gs), alpha(vd) {
@@ -168,15 +182,19 @@ struct RefSim : public ASim {
     bool need_update = false;
     for (auto& b : bpis) {
       std::set<std::pair<int, int>> before, after;
-      auto* eb = static_cast<Exposed<ParallelInteractionStorage_EB<T, CRotBondedInteraction>>*>(bond[b.first]);
-      if constexpr (kRot) collect_ids(eb, before);
+      auto collect = [&](std::set<std::pair<int, int>>& s) {
+        if (nbond.count(b.first)) {
+          collect_ids(nbond[b.first], s);
+        } else if constexpr (kRot) {
+          collect_ids(static_cast<Exposed<ParallelInteractionStorage_EB<T, CRotBondedInteraction>>*>(bond[b.first]), s);
+        }
+      };
+      collect(before);
       bool n = b.second->update();
       if (n) {
-        if constexpr (kRot) {
-          collect_ids(eb, after);
-          for (auto& p : before)
-            if (!after.count(p)) breaks.push_back({p.first, p.second, (int)t});
-        }
+        collect(after);
+        for (auto& p : before)
+          if (!after.count(p)) breaks.push_back({p.first, p.second, (int)t});
       }
       need_update = need_update || n;
     }
@@ -344,6 +362,26 @@ struct RefSim : public ASim {
     err = "RotBond needs RotSphere particles";
     return -1;
   }
+  /* TSubLattice::addPairIG, type "Friction" (Parallel/SubLattice.hpp:1055-1076) */
+  int add_nrot_friction(const char* name, double k, double mu, double ks, double dt_, int scaling) override {
+    CFrictionIGP p(name, k, mu, ks, dt_, scaling != 0);
+    auto* s = new Exposed<ParallelInteractionStorage_ED<T, CFrictionInteraction>>(ppa, p);
+    dpis[name] = s;
+    nfric[name] = s;
+    return 0;
+  }
+  /* TSubLattice::addBondedIG (Parallel/SubLattice.hpp:1791-1831) */
+  int add_nrot_bond(const char* name, int tag, double k, double rbreak, int scaling) override {
+    CBondedIGP p(name, tag, k, rbreak, scaling != 0);
+    auto* s = new Exposed<ParallelInteractionStorage_EB<T, CBondedInteraction>>(ppa, p);
+    if (rbreak < 0) s->setUnbreakable(true);
+    std::vector<int>& conns = temp_conn[tag];
+    std::vector<int> vi(2, -1);
+    for (size_t i = 0; i + 1 < conns.size(); i += 2) { vi[0] = conns[i]; vi[1] = conns[i + 1]; s->tryInsert(vi); }
+    bpis[name] = s;
+    nbond[name] = s;
+    return 0;
+  }
   int add_wall_group(const char* name, const char* wall, double k) override {
     auto it = walls.find(wall);
     if (it == walls.end()) { err = std::string("wall name '") + wall + "' not found in map of walls"; return -1; }
@@ -439,6 +477,8 @@ struct RefSim : public ASim {
   }
   int num_pairs(const char* group) override {
     if (elastic.count(group)) return (int)elastic[group]->list().size();
+    if (nfric.count(group)) return (int)nfric[group]->list().size();
+    if (nbond.count(group)) return (int)nbond[group]->list().size();
     if constexpr (kRot) {
       if (fric.count(group))
         return (int)static_cast<Exposed<ParallelInteractionStorage_ED<T, CRotFrictionInteraction>>*>(fric[group])->list().size();
@@ -452,6 +492,29 @@ struct RefSim : public ASim {
    * elastic -> last force on p2 (3), 0, touching; bond -> force on p1 (3), failure criterion, 0 */
   int get_pairs(const char* group, int* id1, int* id2, double* state) override {
     int i = 0;
+    if (nfric.count(group)) {  /* NRotFriction: tangential force (3), slipping, touching */
+      for (auto& in : nfric[group]->list()) {
+        auto v = in.getAllID();
+        id1[i] = v[0]; id2[i] = v[1];
+        if (state) {
+          const Vec3 f = in.*FricAccess::ffric();
+          for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k];
+          state[5 * i + 3] = (in.*FricAccess::slipping()) ? 1.0 : 0.0;
+          state[5 * i + 4] = (in.*FricAccess::touching()) ? 1.0 : 0.0;
+        }
+        ++i;
+      }
+      return i;
+    }
+    if (nbond.count(group)) {  /* NRotBond: force on p2 (3), failure criterion, 0 */
+      for (auto& in : nbond[group]->list()) {
+        auto v = in.getAllID();
+        id1[i] = v[0]; id2[i] = v[1];
+        if (state) { Vec3 f = in.getForce(); for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k]; state[5 * i + 3] = in.getCriterion(); state[5 * i + 4] = 0; }
+        ++i;
+      }
+      return i;
+    }
     if (elastic.count(group)) {
       for (auto& in : elastic[group]->list()) {
         auto v = in.getAllID();
@@ -534,6 +597,12 @@ int ref_add_rot_bond_group(void* h, const char* name, int tag, double kr, double
   return static_cast<ASim*>(h)->add_rot_bond(name, tag, kr, ks, kt, kb, mn, ms, mt, mb, scaling, meanR, trunc);
 }
 int ref_add_wall_group(void* h, const char* name, const char* wall, double k) { return static_cast<ASim*>(h)->add_wall_group(name, wall, k); }
+int ref_add_nrot_friction_group(void* h, const char* name, double k, double mu, double ks, double dt, int scaling) {
+  return static_cast<ASim*>(h)->add_nrot_friction(name, k, mu, ks, dt, scaling);
+}
+int ref_add_nrot_bond_group(void* h, const char* name, int tag, double k, double rbreak, int scaling) {
+  return static_cast<ASim*>(h)->add_nrot_bond(name, tag, k, rbreak, scaling);
+}
 int ref_add_gravity(void* h, const char* name, const double* g) { return static_cast<ASim*>(h)->add_gravity(name, g); }
 int ref_add_damping(void* h, int rot, double visc, int maxiter) { return static_cast<ASim*>(h)->add_damping(rot, visc, maxiter); }
 int ref_add_exclusion(void* h, const char* b, const char* d) { return static_cast<ASim*>(h)->add_exclusion(b, d); }

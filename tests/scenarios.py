@@ -42,6 +42,75 @@ def gravity_box(make, n_side=6, seed=1, steps_dt=1e-4, layers=None, gap=1.0):
     return sim
 
 
+def nrot_friction_pack(make, rot=False, n_side=5, seed=8, dt=1e-4, vscale=0.5):
+    """Jittered lattice of spheres in contact under gravity with an NRotFriction group
+    (CFrictionInteraction: k = ks = 1000, mu = 0.6), linear damping, floor and side walls; random
+    initial velocities so that contacts slide.  NRotSphere, or RotSphere (forces only, as the
+    reference's applyForce gives no moments)."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(n_side), np.arange(n_side), np.arange(n_side), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) * 0.95 + rng.uniform(-0.03, 0.03, size=g.shape)
+    rad = rng.uniform(0.46, 0.5, size=len(g))
+    n = len(g)
+    L = n_side * 0.95
+    sim = make("RotSphere" if rot else "NRotSphere", 1.2, 0.2, (0, 0, 0), (L, L, 2 * L), (0, 0, 0), dt)
+    vel = rng.normal(0, vscale, size=(n, 3))
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=vel)
+    sim.add_nrot_friction_group("friction", 1000.0, 0.6, 1000.0, dt, True)
+    sim.add_gravity("gravity", (0, 0, -9.81))
+    sim.add_damping(0, 0.01, 100)
+    for name, o, nrm in (("xlo", (0, 0, 0), (1, 0, 0)), ("xhi", (L, 0, 0), (-1, 0, 0)),
+                         ("zlo", (0, 0, 0), (0, 0, 1))):
+        sim.add_wall(name, o, nrm)
+        sim.add_wall_group(name + "_w", name, 1000.0)
+    return sim
+
+
+def nrot_bonded_block(make, nx=5, ny=6, nz=5, seed=9, dt=1e-4, k=1e4, rbreak=0.02, load_rate=0.01):
+    """NRotSphere block with NRotBond (CBondedInteraction) between lattice neighbours (gap within
+    0.015), failing on extension beyond r0 * rbreak, and an NRotFriction group for the contacts
+    after failure (excluded while the bond holds); platens at y, closed by run_loaded."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) * 1.0 + rng.uniform(-0.01, 0.01, size=g.shape)
+    n = len(g)
+    rad = np.full(n, 0.495)
+    d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
+    np.fill_diagonal(d, np.inf)
+    i1, i2 = np.nonzero(np.triu(d - 2 * 0.495 <= 0.015, 1))
+    vel = rng.normal(0, 0.05, size=(n, 3))
+    Ly = ny * 1.0
+    sim = make("NRotSphere", 1.25, 0.2, (0, 0, 0), (nx * 1.0, Ly, nz * 1.0), (0, 0, 0), dt)
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=vel)
+    sim.add_connections(np.ones(len(i1), np.int32), i1, i2)
+    sim.add_nrot_bond_group("bonds", 1, k, rbreak, True)
+    sim.add_nrot_friction_group("friction", k, 0.6, k, dt, True)
+    sim.add_exclusion("bonds", "friction")
+    sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, Ly, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", k)
+    sim.add_wall_group("top_w", "top", k)
+    sim.add_damping(0, 0.05, 100)
+    sim._load_rate = load_rate
+    return sim
+
+
+def nrot_bonded_block_script(make, nx=5, ny=6, nz=5, dt=1e-4, k=1e4, rbreak=0.02, load_rate=0.01):
+    """The restart script of nrot_bonded_block: its groups, walls and damping, no particles."""
+    Ly = ny * 1.0
+    sim = make("NRotSphere", 1.25, 0.2, (0, 0, 0), (nx * 1.0, Ly, nz * 1.0), (0, 0, 0), dt)
+    sim.add_nrot_bond_group("bonds", 1, k, rbreak, True)
+    sim.add_nrot_friction_group("friction", k, 0.6, k, dt, True)
+    sim.add_exclusion("bonds", "friction")
+    sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, Ly, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", k)
+    sim.add_wall_group("top_w", "top", k)
+    sim.add_damping(0, 0.05, 100)
+    sim._load_rate = load_rate
+    return sim
+
+
 def friction_pack(make, nx=6, ny=5, nz=6, seed=2, periodic=False, dt=5e-5, vscale=0.5, squeeze=0.93):
     """Small rotational frictional pack: slightly overlapping jittered lattice of
     RotSpheres (lognormal radii), RotFriction kn=ks=1e4 mu=0.6, elastic floor and
@@ -142,12 +211,16 @@ def parse_checkpoint(path):
         t = nxt()
         out["particles"][int(t[4])] = [float(x) for x in t]
     for _ in range(int(nxt()[0])):
-        assert nxt()[0] == "RotBonded"
+        typ = nxt()[0]
+        assert typ in ("RotBonded", "Bonded"), typ
+        ids = (0, 1) if typ == "RotBonded" else (5, 6)   # RotBonded: id1 id2 first; Bonded: after 5 values
         for _ in range(int(nxt()[0])):
             t = nxt()
-            out["bonds"][(int(t[0]), int(t[1]))] = [float(x) for x in t]
+            out["bonds"][(int(t[ids[0]]), int(t[ids[1]]))] = [float(x) for x in t]
     for _ in range(int(nxt()[0])):
-        assert nxt()[0] == "RotFriction"
+        typ = nxt()[0]
+        assert typ in ("RotFriction", "Friction"), typ
+        ids = (8, 9) if typ == "RotFriction" else (6, 7)
         t = nxt()
         recs = []
         if len(t) == 1:
@@ -157,7 +230,7 @@ def parse_checkpoint(path):
                 recs.append(t)
                 t = nxt(blank_ok=True)
         for r in recs:
-            out["friction"][(int(r[8]), int(r[9]))] = [float(x) for x in r[1:]]
+            out["friction"][(int(r[ids[0]]), int(r[ids[1]]))] = [float(x) for x in r[1:]]
     t = nxt()
     assert t[0] == "Walls"
     for _ in range(int(t[1])):
