@@ -362,6 +362,69 @@ def cylinder_sim(make, sp, grid=2.2, skin=0.2):
     return sim
 
 
+def nrot_friction_leg(stream, steps=1000, ref_steps=20):
+    """The widened pair law on the headline packing: the 250,000 spheres as NRotSpheres with an
+    NRotFriction group (CFrictionInteraction, k = ks = 1e4, mu = 0.6), the elastic walls moving
+    at -+0.01 in x; the GPU's FP64 form (the law's only form) against the reference's own C++
+    (oracle/_ref, one core, non-periodic as for the headline's baseline)."""
+    import torch
+
+    from esys.lsm import _capi
+
+    w = workload()
+
+    def build(make, periodic):
+        sim = make("NRotSphere", GRID, SKIN, w["bmin"], w["bmax"], (1 if periodic else 0, 0, 0), DT)
+        sim.add_particles(w["ids"], w["pos"], w["rad"], w["mass"], tag=np.zeros(len(w["ids"]), np.int32),
+                          vel=w["vel"])
+        sim.add_nrot_friction_group("friction", KN, MU, KS, DT, True)
+        sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+        sim.add_wall("top", (0, 50, 0), (0, -1, 0))
+        sim.add_wall_group("bottom_w", "bottom", KWALL)
+        sim.add_wall_group("top_w", "top", KWALL)
+        return sim
+
+    sim = build(lambda *a: _capi.DemSim(*a), True)
+    sim.set_stream(stream.cuda_stream)
+    sim.set_option("profile", 1)
+    sim.set_wall_velocity("bottom", (-0.01, 0, 0))
+    sim.set_wall_velocity("top", (0.01, 0, 0))
+    sim.step(200)
+    torch.cuda.synchronize()
+    c0 = sim.counters()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    c1 = sim.counters()
+    ms = e0.elapsed_time(e1)
+    value = (c1["contact_updates"] - c0["contact_updates"]) / (ms / 1e3)
+    kus = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / max(1, c1["profiled_steps"] - c0["profiled_steps"]) / 1e3
+    touching = int(sim.pairs("friction")[2][:, 4].sum())
+    sim.close()
+    ref = None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if oracle.available("ref"):
+        r = build(lambda *a: oracle.OracleSim("ref", *a), False)
+        r.step(1)
+        m = r.f["num_pairs"](r.h, b"friction")
+        ncand = int((np.abs(w["pos"][:, 1]) < GRID).sum() + (np.abs(w["pos"][:, 1] - 50.0) < GRID).sum())
+        t0 = time.perf_counter()
+        r.step(ref_steps)
+        dt = time.perf_counter() - t0
+        ref = {"value": (m + ncand) * ref_steps / dt, "steps": ref_steps, "cores": 1, "kind": "reference"}
+    return {
+        "workload": "the headline's 250,000-sphere packing as NRotSpheres, NRotFriction k=ks=1e4 mu=0.6, "
+                    "2 elastic walls -+0.01 x, dt=5e-5",
+        "metric": "contact-updates/s", "value": value, "steps": steps, "dtype": "f64", "kernel_us": kus,
+        "touching_pairs": touching, "cpu_reference": ref,
+        "speedup_vs_cpu_reference": value / ref["value"] if ref else None,
+    }
+
+
 def window_bytes(n, m, nb, T, K):
     """Device bytes of one specimen's window: checkpoints every K of T steps (particle records,
     friction histories, wall candidacy) and the reverse pass's recompute of K + 1 states (records,
@@ -579,6 +642,7 @@ def main():
                     help="32: FP32 pair forces + FP64 integration (headline); 64: FP64 throughout")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-window leg")
+    ap.add_argument("--no-widened", action="store_true", help="skip the NRotFriction leg")
     ap.add_argument("--ensemble-specimens", type=int, default=512, help="0 skips the batched-ensemble leg")
     ap.add_argument("--ensemble-steps", type=int, default=1000, help="timed timesteps of the ensemble leg")
     ap.add_argument("--ensemble-window", type=int, default=200,
@@ -723,6 +787,9 @@ def main():
     adj = None
     if not args.no_adjoint:
         adj = adjoint_leg(stream)
+    nrot = None
+    if not args.no_widened and world == 1:
+        nrot = nrot_friction_leg(stream)
     ens = None
     if args.ensemble_specimens > 0:
         ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps, dist=dist, window=args.ensemble_window,
@@ -767,6 +834,7 @@ def main():
             "gpu_launches": c1["launches"] - c0["launches"],
             "clocks": clk.summary(),
             "adjoint": adj,
+            "nrot_friction": nrot,
             "ensemble": ens,
         }
         print(json.dumps(line))
