@@ -140,6 +140,10 @@ struct StepArgs {
   int damp_lin, damp_rot;   // damping groups present
   double visc_lin, visc_rot, dt_lin, dt_rot;
   int iter_lin, iter_rot;
+  // local damping groups (CLocalDamping / CRotLocalDamping): present, viscosity, and whether the
+  // LocalDamping group's name sorts before "Damping" (the damping map's order)
+  int damp_loc, damp_rotloc, loc_before_lin;
+  double visc_loc, visc_rotloc;
   int store_forces;
   // device bond hand-off: a bond failure does not stop the chunk; the pairs it excluded turn
   // into ordinary pairs (DynDev::xbond) and every particle refreshes its wall candidacy at the

@@ -391,4 +391,18 @@ __device__ __forceinline__ V damping_force(const V& v, const V& frc, double s, d
   return -1.0 * visc * v_rel * mass;
 }
 
+// CLocalDamping::calcForces (Model/LocalDamping.hpp:82-118) and CRotLocalDamping::calcForces
+// (Model/RotLocalDamping.hpp:82-117): each component of the accumulated force (moment) with the
+// sign of the velocity (spin) component, zero where that component is zero, times -visc.
+__device__ __forceinline__ V local_damping_force(const V& v, const V& frc, double visc) {
+  double fx = fabs(frc.x), fy = fabs(frc.y), fz = fabs(frc.z);
+  if (v.x < 0) fx *= -1.;
+  if (v.x == 0) fx = 0.0;
+  if (v.y < 0) fy *= -1.;
+  if (v.y == 0) fy = 0.0;
+  if (v.z < 0) fz *= -1.;
+  if (v.z == 0) fz = 0.0;
+  return -1.0 * visc * mk(fx, fy, fz);
+}
+
 }  // namespace dem

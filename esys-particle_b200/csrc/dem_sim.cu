@@ -148,6 +148,9 @@ struct DemSim {
   std::map<std::string, BondGroup> bond;
   std::map<int, std::vector<int>> temp_conn;
   int damp_lin = 0, damp_rot = 0, iter_lin = 100, iter_rot = 100;
+  std::string loc_name;            // LocalDamping group present (its name orders it against "Damping")
+  int damp_rotloc = 0;              // RotLocalDamping group present
+  double visc_loc = 0.0, visc_rotloc = 0.0;
   double visc_lin = 0, visc_rot = 0;
   // device control
   DBuf<WallDev> d_walls;
@@ -739,6 +742,8 @@ struct DemSim {
       }
     }
     a.damp_lin = damp_lin; a.damp_rot = damp_rot;
+    a.damp_loc = !loc_name.empty(); a.damp_rotloc = damp_rotloc; a.visc_loc = visc_loc; a.visc_rotloc = visc_rotloc;
+    a.loc_before_lin = !loc_name.empty() && loc_name < std::string("Damping");
     a.visc_lin = visc_lin; a.visc_rot = visc_rot; a.dt_lin = dt; a.dt_rot = dt;
     a.iter_lin = iter_lin; a.iter_rot = iter_rot;
     a.store_forces = store_forces;
@@ -909,6 +914,8 @@ struct DemSim {
     if (T < 1 || K < 1) throw std::invalid_argument("window length and checkpoint interval must be >= 1");
     if (iter_lin > 255 || iter_rot > 255) throw std::invalid_argument("window damping needs maxIterations <= 255");
     if (widened()) throw std::invalid_argument("the differentiable window covers NRotElastic, RotFriction and RotBond groups");
+    if (!loc_name.empty() || damp_rotloc)
+      throw std::invalid_argument("the differentiable window covers the viscous damping groups, not local damping");
     win.valid = false;
     if (!prepare()) return false;
     const int nd = (int)dyn.size();
@@ -2506,6 +2513,23 @@ int dem_add_damping(dem_sim* h, int rot, double visc, int max_iter) {
       s.damp_rot = 1; s.visc_rot = visc; s.iter_rot = max_iter;
     } else {
       s.damp_lin = 1; s.visc_lin = visc; s.iter_lin = max_iter;
+    }
+    return DEM_OK;
+  });
+}
+
+// TSubLattice::doAddDamping "LocalDamping" (Parallel/SubLattice.hpp:1765-1769) and
+// TRotSubLattice::doAddDamping "RotLocalDamping" (Parallel/RotSubLattice.hpp:95-104).
+int dem_add_local_damping(dem_sim* h, const char* name, int rot, double visc) {
+  return guard(h, [&](DemSim& s) {
+    if (rot) {
+      if (!s.rot) throw std::invalid_argument("RotLocalDamping needs RotSphere particles");
+      s.damp_rotloc = 1; s.visc_rotloc = visc;
+    } else {
+      const std::string n = name ? name : "";
+      if (n.empty() || n == "Damping" || n == "RotDamping" || n == "RotLocalDamping")
+        throw std::invalid_argument("a LocalDamping group needs a name of its own");
+      s.loc_name = n; s.visc_loc = visc;
     }
     return DEM_OK;
   });

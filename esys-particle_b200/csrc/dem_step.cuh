@@ -413,10 +413,15 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
       a.f_int[i] = d4(F, 0.0);
       a.m_int[i] = d4(M, 0.0);
     }
-    // 5. damping, last (SubLattice.hpp:2140-2145): "Damping" then "RotDamping"
+    // 5. damping, last (SubLattice.hpp:2140-2145), in the damping map's name order: on the force
+    //    "Damping" and a LocalDamping group (by its own name); on the moment "RotDamping" then
+    //    "RotLocalDamping"
     int it_lin = 0, it_rot = 0;
+    if (a.damp_loc && a.loc_before_lin) F += local_damping_force(xyz(v4), F, a.visc_loc);
     if (a.damp_lin) F += damping_force(xyz(v4), F, iv.x, v4.w, a.visc_lin, a.dt_lin, a.iter_lin, &it_lin);
+    if (a.damp_loc && !a.loc_before_lin) F += local_damping_force(xyz(v4), F, a.visc_loc);
     if (ROT && a.damp_rot) M += damping_force(xyz(w4), M, iv.y, w4.w, a.visc_rot, a.dt_rot, a.iter_rot, &it_rot);
+    if (ROT && a.damp_rotloc) M += local_damping_force(xyz(w4), M, a.visc_rotloc);
     if (a.damp_iters) {
       a.damp_iters[2 * i] = (unsigned char)(it_lin > 255 ? 255 : it_lin);
       a.damp_iters[2 * i + 1] = (unsigned char)(it_rot > 255 ? 255 : it_rot);

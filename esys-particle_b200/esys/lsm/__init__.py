@@ -24,7 +24,8 @@ __all__ = [
     "LsmMpi", "NRotSphere", "RotSphere", "Runnable", "NRotElasticPrms", "RotFrictionPrms", "RotBondPrms",
     "NRotElasticWallPrms", "LinDampingPrms", "RotDampingPrms", "GravityPrms", "Vec3", "BoundingBox",
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
-    "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms",
+    "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms", "LocalDampingPrms",
+    "RotLocalDampingPrms",
 ]
 
 
@@ -132,6 +133,15 @@ class LinDampingPrms:  # InteractionParamsPy.cpp:46-53, 998-1016
 
 
 class RotDampingPrms(LinDampingPrms):
+    pass
+
+
+class LocalDampingPrms:  # InteractionParamsPy.cpp:1033-1048 (CLocalDampingIGP "LocalDamping")
+    def __init__(self, name, viscosity):
+        self.name, self.viscosity = name, float(viscosity)
+
+
+class RotLocalDampingPrms(LocalDampingPrms):  # InteractionParamsPy.cpp:1050-1065 ("RotLocalDamping")
     pass
 
 
@@ -303,6 +313,10 @@ class LsmMpi:
         elif isinstance(prms, NRotElasticWallPrms):
             s.add_wall_group(prms.name, prms.wallName, prms.normalK)
             self._wig_of_wall[prms.name] = prms.wallName
+        elif isinstance(prms, RotLocalDampingPrms):
+            s.add_local_damping(prms.name, 1, prms.viscosity)
+        elif isinstance(prms, LocalDampingPrms):
+            s.add_local_damping(prms.name, 0, prms.viscosity)
         elif isinstance(prms, RotDampingPrms):
             s.add_damping(1, prms.viscosity, prms.maxIterations)
         elif isinstance(prms, LinDampingPrms):
@@ -312,6 +326,13 @@ class LsmMpi:
         else:
             raise NotImplementedError(f"{type(prms).__name__} is not on the GPU path")
         return prms.name
+
+    # LsmMpiPy::createDamping / createLocalDamping / createRotLocalDamping / createGravity
+    # (LsmMpiPy.cpp:706-737): the older spellings of createInteractionGroup for these groups
+    def createDamping(self, prms):
+        return self.createInteractionGroup(prms)
+
+    createLocalDamping = createRotLocalDamping = createGravity = createDamping
 
     def createExclusion(self, interactionName1, interactionName2):
         self._require().add_exclusion(interactionName1, interactionName2)

@@ -100,6 +100,14 @@ int dem_add_gravity(dem_sim* h, const char* name, const double* g);
  * (Parallel/SubLattice.hpp:1748-1784, Parallel/RotSubLattice.hpp:79-109); v_ref = 0. */
 int dem_add_damping(dem_sim* h, int rotational, double viscosity, int max_iterations);
 
+/* TSubLattice::doAddDamping "LocalDamping" / TRotSubLattice::doAddDamping "RotLocalDamping"
+ * (Parallel/SubLattice.hpp:1765-1769, Parallel/RotSubLattice.hpp:95-104): CLocalDamping /
+ * CRotLocalDamping (Model/LocalDamping.hpp:82-118, Model/RotLocalDamping.hpp:82-117) with this
+ * viscosity.  Applied with the other damping groups in their name order ("Damping" and the
+ * LocalDamping group's own name on the force; "RotDamping" then "RotLocalDamping" on the moment).
+ * Not part of the differentiable window. */
+int dem_add_local_damping(dem_sim* h, const char* name, int rot, double visc);
+
 /* TSubLattice::setExIG (Parallel/SubLattice.hpp:1980-2009): pairs bonded in `bonded` are
  * excluded from the dynamic group `dynamic` while the bond is intact. */
 int dem_add_exclusion(dem_sim* h, const char* bonded, const char* dynamic);

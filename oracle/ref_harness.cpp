@@ -44,6 +44,9 @@
 #include "Model/EWallInteractionGroup.h"
 #include "Model/ElasticInteraction.h"
 #include "Model/FrictionInteraction.h"
+#include "Model/LocalDamping.h"
+#include "Model/LocalDampingIGP.h"
+#include "Model/RotLocalDamping.h"
 #include "Model/Particle.h"
 #include "Model/RotBondedInteraction.h"
 #include "Model/RotDamping.h"
@@ -95,6 +98,7 @@ struct ASim {
   virtual int add_nrot_bond(const char* name, int tag, double k, double rbreak, int scaling) = 0;
   virtual int add_gravity(const char* name, const double* g) = 0;
   virtual int add_damping(int rot, double visc, int maxiter) = 0;
+  virtual int add_local_damping(const char* name, int rot, double visc) = 0;
   virtual int add_exclusion(const char* b, const char* d) = 0;
   virtual int step(int n) = 0;
   virtual int move_wall(const char* name, const double* d) = 0;
@@ -414,6 +418,26 @@ struct RefSim : public ASim {
     s->update();
     return 0;
   }
+  /* TSubLattice::doAddDamping "LocalDamping" (Parallel/SubLattice.hpp:1765-1769) and
+   * TRotSubLattice::doAddDamping "RotLocalDamping" (Parallel/RotSubLattice.hpp:95-104) */
+  int add_local_damping(const char* name, int rot, double visc) override {
+    if (rot) {
+      if constexpr (kRot) {
+        CLocalDampingIGP p("RotLocalDamping", name, visc, dt);
+        auto* s = new ParallelInteractionStorage_Single<T, CRotLocalDamping<T>>(ppa, p);
+        damping["RotLocalDamping"] = s;
+        s->update();
+        return 0;
+      }
+      err = "RotLocalDamping needs RotSphere particles";
+      return -1;
+    }
+    CLocalDampingIGP p("LocalDamping", name, visc, dt);
+    auto* s = new ParallelInteractionStorage_Single<T, CLocalDamping<T>>(ppa, p);
+    damping[name] = s;
+    s->update();
+    return 0;
+  }
   /* TSubLattice::setExIG (Parallel/SubLattice.hpp:1980-2009) */
   int add_exclusion(const char* s1, const char* s2) override {
     auto ex = bpis.find(s1);
@@ -597,6 +621,9 @@ int ref_add_rot_bond_group(void* h, const char* name, int tag, double kr, double
   return static_cast<ASim*>(h)->add_rot_bond(name, tag, kr, ks, kt, kb, mn, ms, mt, mb, scaling, meanR, trunc);
 }
 int ref_add_wall_group(void* h, const char* name, const char* wall, double k) { return static_cast<ASim*>(h)->add_wall_group(name, wall, k); }
+int ref_add_local_damping(void* h, const char* name, int rot, double visc) {
+  return static_cast<ASim*>(h)->add_local_damping(name, rot, visc);
+}
 int ref_add_nrot_friction_group(void* h, const char* name, double k, double mu, double ks, double dt, int scaling) {
   return static_cast<ASim*>(h)->add_nrot_friction(name, k, mu, ks, dt, scaling);
 }

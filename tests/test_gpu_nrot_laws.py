@@ -111,3 +111,25 @@ def test_nrot_restart_continues_like_the_reference(gpu, ref, tmp_path):
     last = a.timestep + 70
     ea, eb = ({e for e in zip(*(x.tolist() for x in log)) if e[2] <= last} for log in (g2.breaks(), r2.breaks()))
     assert ea == eb and len(eb) > 0
+
+
+@pytest.mark.parametrize("name", ["Alocal", "zlocal"])  # sorts before / after "Damping" in the damping map
+def test_local_damping_matches_reference(gpu, ref, name):
+    """LocalDamping (with the viscous linear damping, ordered by group name) on an NRotSphere
+    gravity packing, and LocalDamping + RotLocalDamping with both viscous dampings on a
+    rotational friction pack."""
+    a, b = S.gravity_box(gpu, n_side=5), S.gravity_box(ref, n_side=5)
+    for s in (a, b):
+        s.add_local_damping(name, 0, 0.3)
+        s.step(200)
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel"):
+        _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
+    a, b = S.loaded_friction_pack(gpu), S.loaded_friction_pack(ref)
+    for s in (a, b):
+        s.add_local_damping(name, 0, 0.2)
+        s.add_local_damping("rotlocal", 1, 0.2)
+        s.step(150)
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel", "angvel"):
+        _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
