@@ -171,14 +171,18 @@ __global__ void k_pairs_write(Grid g, Particles P, int cur, const int* cell_star
     keys[b + 1] = key;
     ++n;
   });
-  if (kind != 1) return;
+  // history: kind 0 none; 1 carried for persistent pairs (PIS_ED::update); 2 reset (a history-bearing
+  // law in a PIS_NE storage, rebuilt from scratch at every rebuild)
+  if (kind == 0) return;
   for (int k = s; k < s + n; ++k) {
     const int j = (int)(keys[k] & 0xffffffffu);
     H h{};
-    int p = lower_bound_key(old_keys, 0, old_n, keys[k]);
-    if (p < old_n && old_keys[p] == keys[k]) {
-      V x1 = xyz(pi), x2 = image_of(g, x1, xyz(P.buf[cur].pr[j]));
-      if (friction_persistent(x1, pi.w, x2, P.buf[cur].pr[j].w)) h = old_hist[p];
+    if (kind == 1) {
+      int p = lower_bound_key(old_keys, 0, old_n, keys[k]);
+      if (p < old_n && old_keys[p] == keys[k]) {
+        V x1 = xyz(pi), x2 = image_of(g, x1, xyz(P.buf[cur].pr[j]));
+        if (friction_persistent(x1, pi.w, x2, P.buf[cur].pr[j].w)) h = old_hist[p];
+      }
     }
     hist[k] = h;
   }
@@ -311,14 +315,14 @@ __global__ void k_merge(const unsigned long long* A, const H* Ah, int m, const u
     int lo = 0, hi = nb;
     while (lo < hi) { int mid = (lo + hi) >> 1; if (B[mid] < A[k]) lo = mid + 1; else hi = mid; }
     out[k + lo] = A[k];
-    if (kind == 1) outh[k + lo] = Ah[k];
+    if (kind != 0) outh[k + lo] = Ah[k];
   } else if (k < m + nb) {
     int b = k - m;
     // number of A elements <= B[b]
     int lo = 0, hi = m;
     while (lo < hi) { int mid = (lo + hi) >> 1; if (A[mid] <= B[b]) lo = mid + 1; else hi = mid; }
     out[b + lo] = B[b];
-    if (kind == 1) outh[b + lo] = H{};
+    if (kind != 0) outh[b + lo] = H{};
   }
 }
 
@@ -341,7 +345,7 @@ __global__ void k_compact(const unsigned long long* keys, const double4* hist, i
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= m || !keep[k]) return;
   okeys[pos[k]] = keys[k];
-  if (kind == 1) ohist[pos[k]] = hist[k];
+  if (kind != 0) ohist[pos[k]] = hist[k];
 }
 
 // Bonds whose particle vanished are erased (PIS_E::rebuild); no break event.
@@ -686,14 +690,14 @@ void launch_bond_pass_f64(const StepArgs& a, bool eval, cudaStream_t s) {
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s) {
   bool el = false, fr = false, widened = false;
   for (int d = 0; d < a.ndyn; ++d) {
-    if (a.dyn[d].kind == 2) widened = true;
+    if (a.dyn[d].kind >= 2) widened = true;  // NRotFriction, HertzMindlin
     (a.dyn[d].kind == 0 ? el : fr) = true;
   }
   for (int d = 0; d < a.nbond; ++d) widened = widened || a.bond[d].kind == 1;
   const bool bd = a.nbond > 0;
   const bool gather = bd && a.bond[0].bf;  // bonds evaluated once by the bond pass
   if (gather) launch_bond_pass<false, false>(a, s);
-  if (widened) {  // NRotFriction / NRotBond groups: one general instance per particle type
+  if (widened) {  // NRotFriction / HertzMindlin / NRotBond groups: one general instance per particle type
     if (!rot) return launch_step_tpp<false, F_ELASTIC | F_NFRIC | F_BGATHER, false, false>(a, tpp, s);
     return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_NFRIC | F_BGATHER, false, false>(a, tpp, s);
   }

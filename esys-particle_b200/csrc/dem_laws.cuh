@@ -391,6 +391,47 @@ __device__ __forceinline__ V damping_force(const V& v, const V& frc, double s, d
   return -1.0 * visc * v_rel * mass;
 }
 
+// CHertzMindlinInteraction::calcForces (Model/HertzMindlinInteraction.cpp:108-172): Hertz normal
+// force 4/3 E sqrt(R) dn^1.5 along D/|D| with R = 1 / (1/r1 + 1/r2), Mindlin tangential stiffness
+// on the relative translation, one friction coefficient; forces only.  Here fn is the force on p1
+// (p2 gets -fn) and Ffric the tangential force on p1 (p2 gets -Ffric).
+__device__ __forceinline__ void law_hertz_mindlin(double E, double nu, double mu, double dt, const V& x1, double r1,
+                                                  const V& v1, const V& x2, double r2, const V& v2, V Ffric,
+                                                  FricOut& o) {
+  const V D = x1 - x2;
+  double dist = dot(D, D);
+  const double eq_dist = r1 + r2;
+  if (dist < (eq_dist * eq_dist)) {
+    const double R_ij = 1.0 / (1.0 / r1 + 1.0 / r2);
+    dist = sqrt(dist);
+    const double dn = eq_dist - dist;
+    const V dir = D / norm(D);
+    const double norm_fn = 4.0 / 3.0 * E * sqrt(R_ij) * pow(dn, 1.5);
+    const V fn = dir * norm_fn;
+    const V d1 = v1 * dt;
+    const V d2 = v2 * dt;
+    V ds = d2 - d1;
+    ds -= dot(ds, dir) * dir;
+    Ffric += 2.0 / 3.0 * 8.0 * E / 2.0 / (1.0 + nu) * sqrt(R_ij) * sqrt(dn) * ds;
+    const double FfricNorm = norm(Ffric);
+    const double forceNorm = norm(fn);
+    if (FfricNorm > forceNorm * mu) {
+      Ffric = Ffric * ((mu * forceNorm) / FfricNorm);
+      o.slipping = true;
+    } else {
+      o.slipping = false;
+    }
+    o.fn = fn;
+    o.Ffric = Ffric;
+    o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+    o.touching = true;
+  } else {
+    o.Ffric = o.fn = o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+    o.slipping = false;
+    o.touching = false;
+  }
+}
+
 // CLocalDamping::calcForces (Model/LocalDamping.hpp:82-118) and CRotLocalDamping::calcForces
 // (Model/RotLocalDamping.hpp:82-117): each component of the accumulated force (moment) with the
 // sign of the velocity (spin) component, zero where that component is zero, times -visc.

@@ -359,7 +359,7 @@ struct DemSim {
     if (want == fp32) return;
     if (want)
       for (auto& d : dyn)
-        if (d.second.kind == 2) throw std::invalid_argument("NRotFriction groups run in the FP64 form only");
+        if (d.second.kind >= 2) throw std::invalid_argument("NRotFriction and HertzMindlin groups run in the FP64 form only");
     for (auto& d : dyn) {
       DynGroup& G = d.second;
       if (G.kind == 0 || G.m == 0) continue;
@@ -519,10 +519,10 @@ struct DemSim {
     if (G.kind != 0) G.hist_spare.reserve(std::max(m, 1));
     if (fp32) {
       if (G.kind != 0) G.hist32_spare.reserve(std::max(m, 1));
-      launch_pairs_write<float4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind != 0 ? 1 : 0,
+      launch_pairs_write<float4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, hist_mode(G),
                                  G.keys.p, G.m, G.hist32[cur].p, G.hist32_spare.p, s);
     } else {
-      launch_pairs_write<double4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, G.kind != 0 ? 1 : 0,
+      launch_pairs_write<double4>(g, P, cur, cell_start.p, cell_list.p, ex, scratch_j.p, G.keys_spare.p, hist_mode(G),
                                   G.keys.p, G.m, G.hist[cur].p, G.hist_spare.p, s);
     }
     std::swap(G.keys, G.keys_spare);
@@ -547,7 +547,7 @@ struct DemSim {
   // (ntable.hpp:628-664; pi_storage_ne.hpp:80-98, pi_storage_ed.hpp:130-155).
   void dyn_new_update(DynGroup& G) {
     ExclDev ex = excl_of(G);
-    const int check_in = G.kind != 0;  // PIS_NE appends without the isIn test
+    const int check_in = G.kind == 1 || G.kind == 2;  // PIS_ED tests isIn; PIS_NE appends without it
     scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
     launch_newlist_count(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_i.p, s);
     scan_tmp.reserve(scan_tmp_ints(n + 2));
@@ -665,7 +665,7 @@ struct DemSim {
     if (on == (handoff != 0)) return;
     if (on)
       for (auto& d : dyn)
-        if (d.second.kind == 0)
+        if (d.second.kind == 0 || d.second.kind == 3)
           throw std::invalid_argument("the device bond hand-off needs every dynamic group to be RotFriction or NRotFriction");
     handoff = on;
     if (!d_brk.p) {
@@ -680,8 +680,13 @@ struct DemSim {
   // NRotFriction groups or NRotBond groups present: the FP64 general instances run the step
   // (bonds through the bond pass); the FP32 form, the batched ensemble and differentiable
   // windows are not built for them.
+  // History handling of a dynamic group's list at a rebuild: 0 none (NRotElastic), 1 carried for
+  // persistent pairs (PIS_ED groups: RotFriction, NRotFriction), 2 reset (HertzMindlin, whose
+  // history lives in a PIS_NE storage that rebuilds its list from scratch).
+  static int hist_mode(const DynGroup& G) { return G.kind == 0 ? 0 : (G.kind == 3 ? 2 : 1); }
+
   bool widened() const {
-    for (auto& d : dyn) if (d.second.kind == 2) return true;
+    for (auto& d : dyn) if (d.second.kind >= 2) return true;
     for (auto& b : bond) if (b.second.kind == 1) return true;
     return false;
   }
@@ -1452,11 +1457,11 @@ struct DemSim {
     // (pis/pi_storage_ed.hpp:202-214).  The reference writes the record count and the first record
     // with no separator; a newline is written here so that the count can be read back.
     int nsave = 0;
-    for (auto& it : dyn) nsave += it.second.kind != 0 ? 1 : 0;
+    for (auto& it : dyn) nsave += (it.second.kind == 1 || it.second.kind == 2) ? 1 : 0;
     os << nsave << "\n";
     for (auto& it : dyn) {
       DynGroup& G = it.second;
-      if (G.kind == 0) continue;
+      if (G.kind == 0 || G.kind == 3) continue;  // PIS_NE storages do not save
       std::vector<unsigned long long> keys(G.m);
       std::vector<double4> h(G.m);
       std::vector<int> xb(handoff ? G.m : 0);
@@ -1695,11 +1700,11 @@ struct DemSim {
     unsigned nsave = 0;
     is >> nsave;
     unsigned want = 0;
-    for (auto& it : dyn) want += it.second.kind != 0 ? 1 : 0;
+    for (auto& it : dyn) want += (it.second.kind == 1 || it.second.kind == 2) ? 1 : 0;
     if (!is || nsave != want) fail("the number of friction groups differs from the script's");
     for (auto& it : dyn) {
       DynGroup& G = it.second;
-      if (G.kind == 0) continue;
+      if (G.kind == 0 || G.kind == 3) continue;
       std::string type;
       is >> type;
       const std::string want_type = G.kind == 1 ? "RotFriction" : "Friction";
@@ -2456,6 +2461,20 @@ int dem_add_nrot_friction_group(dem_sim* h, const char* name, double k, double m
   });
 }
 
+// TSubLattice::addPairIG, type "HertzMindlin" (Parallel/SubLattice.hpp:1324-1339): CHertzMindlinIGP in
+// its packing order (E, nu, mu, dt), a PIS_NE storage.
+int dem_add_hertz_mindlin_group(dem_sim* h, const char* name, double E, double nu, double mu, double dt) {
+  return guard(h, [&](DemSim& s) {
+    if ((int)s.dyn.size() >= dem::kMaxDyn) throw std::invalid_argument("too many dynamic interaction groups");
+    if (s.fp32) throw std::invalid_argument("HertzMindlin groups run in the FP64 form only");
+    if (s.handoff) throw std::invalid_argument("the device bond hand-off needs RotFriction or NRotFriction groups");
+    dem::DynGroup& G = s.dyn[name];
+    G.kind = 3; G.k = E; G.ks = nu; G.mu_s = mu; G.mu_d = mu; G.dt = dt; G.scaling = 0; G.meanR = 0;
+    s.resize_adjacency();
+    return DEM_OK;
+  });
+}
+
 // TRotSubLattice::addRotBondedIG (RotSubLattice.hpp:116-186) with PIS_E::tryInsert (pi_storage_e.hpp:222-263).
 int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
                            double mn, double ms, double mt, double mb, int scaling, int meanR, double truncated) {
@@ -2931,7 +2950,7 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto d = s.dyn.find(gname);
     if (d != s.dyn.end()) {
       dem::DynGroup& G = d->second;
-      if (G.kind == 2) throw std::invalid_argument("interaction fields of NRotFriction groups are not built");
+      if (G.kind >= 2) throw std::invalid_argument("interaction fields of NRotFriction and HertzMindlin groups are not built");
       int code = f == "count" ? 0 : f == "potential_energy" ? 1 : -1;
       if (G.kind != 0 && f == "slipping") code = 2;
       if (G.kind != 0 && f == "sticking") code = 3;

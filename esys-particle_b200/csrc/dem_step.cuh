@@ -63,7 +63,7 @@ __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
 // does not carry the registers of the bond law).
 // F_BGATHER: bonds were evaluated by the bond pass (k_bond_pass, once per bond); the particle
 // gathers their forces and moments in its adjacency order instead of evaluating the law.
-// F_NFRIC: NRotFriction groups (FP64 only).
+// F_NFRIC: NRotFriction and HertzMindlin groups (FP64 only).
 enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8, F_NFRIC = 16 };
 
 // Sum of the pair-group and bond contributions on particle i (all TPP lanes of
@@ -150,19 +150,26 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                 }
               }
             }
-          } else if (G.kind == 2) {
-            if constexpr (!FP32 && (FEAT & F_NFRIC) != 0) {  // CFrictionInteraction::calcForces
+          } else if (G.kind >= 2) {
+            // NRotFriction (CFrictionInteraction::calcForces) or HertzMindlin
+            // (CHertzMindlinInteraction::calcForces): forces only, history of the tangential force
+            if constexpr (!FP32 && (FEAT & F_NFRIC) != 0) {
               if (!touching) {
                 if (isp1 && !EVAL) G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
                 continue;
               }
-              double keff, kseff;
-              nfriction_k(G.k, G.ks, G.scaling, pa.w, pb.w, keff, kseff);
               const double4 vj = ldg4(in.vm + j);
               const double4 va = isp1 ? v4 : vj, vb = isp1 ? vj : v4;
               const double4 h = ldg4(G.hist_in + k);
               FricOut o;
-              law_nfriction(keff, kseff, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
+              if (G.kind == 2) {
+                double keff, kseff;
+                nfriction_k(G.k, G.ks, G.scaling, pa.w, pb.w, keff, kseff);
+                law_nfriction(keff, kseff, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
+              } else {  // E in k, nu in ks; the normal force on p1 is +fn: negated for the common form
+                law_hertz_mindlin(G.k, G.ks, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
+                o.fn = -1.0 * o.fn;
+              }
               if (isp1) {  // p1: -force, then +Ffric; p2: +force, then -Ffric
                 Fp += -1.0 * o.fn;
                 Fp += o.Ffric;

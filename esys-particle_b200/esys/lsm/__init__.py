@@ -25,7 +25,7 @@ __all__ = [
     "NRotElasticWallPrms", "LinDampingPrms", "RotDampingPrms", "GravityPrms", "Vec3", "BoundingBox",
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
     "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms", "LocalDampingPrms",
-    "RotLocalDampingPrms",
+    "RotLocalDampingPrms", "HertzMindlinPrms",
 ]
 
 
@@ -134,6 +134,12 @@ class LinDampingPrms:  # InteractionParamsPy.cpp:46-53, 998-1016
 
 class RotDampingPrms(LinDampingPrms):
     pass
+
+
+class HertzMindlinPrms:  # InteractionParamsPy.cpp:1350-1380 (CHertzMindlinIGP)
+    def __init__(self, name, youngsModulus, poissonsRatio, dynamicMu):
+        self.name, self.youngsModulus, self.poissonsRatio = name, float(youngsModulus), float(poissonsRatio)
+        self.dynamicMu = float(dynamicMu)
 
 
 class LocalDampingPrms:  # InteractionParamsPy.cpp:1033-1048 (CLocalDampingIGP "LocalDamping")
@@ -308,6 +314,8 @@ class LsmMpi:
                                  prms.scaling, prms.meanR_scaling, prms.truncated)
         elif isinstance(prms, NRotFrictionPrms):  # LsmMpiPy::createNRotFrictionInteractGrp sets dt
             s.add_nrot_friction_group(prms.name, prms.normalK, prms.dynamicMu, prms.shearK, self._dt, prms.scaling)
+        elif isinstance(prms, HertzMindlinPrms):  # LsmMpiPy::createHertzMindlinIG sets dt (LsmMpiPy.cpp:508-517)
+            s.add_hertz_mindlin_group(prms.name, prms.youngsModulus, prms.poissonsRatio, prms.dynamicMu, self._dt)
         elif isinstance(prms, NRotBondPrms):
             s.add_nrot_bond_group(prms.name, prms.tag, prms.normalK, prms.breakDistance, prms.scaling)
         elif isinstance(prms, NRotElasticWallPrms):

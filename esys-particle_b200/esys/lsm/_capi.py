@@ -33,6 +33,7 @@ SIGNATURES = {
     "dem_add_rot_bond_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 8 + [C.c_int, C.c_int, C.c_double]),
     "dem_add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
     "dem_add_local_damping": (C.c_int, [_P, _S, C.c_int, C.c_double]),
+    "dem_add_hertz_mindlin_group": (C.c_int, [_P, _S] + [C.c_double] * 4),
     "dem_add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
     "dem_add_wall_group": (C.c_int, [_P, _S, _S, C.c_double]),
     "dem_add_gravity": (C.c_int, [_P, _S, _D]),
@@ -176,6 +177,10 @@ class DemSim:
         self._chk(self.lib.dem_add_rot_friction_group(self.h, name.encode(), float(k), float(mu_s), float(mu_d),
                                                       float(k_s), float(dt), int(scaling), int(meanR_scaling)))
         self._dyn_prm[name] = (1, [float(k), float(k_s)])
+
+    def add_hertz_mindlin_group(self, name, E, nu, mu, dt):
+        self._chk(self.lib.dem_add_hertz_mindlin_group(self.h, name.encode(), float(E), float(nu), float(mu), float(dt)))
+        self._dyn_prm[name] = (3, [float(E), float(nu)])
 
     def add_local_damping(self, name, rot, visc):
         self._chk(self.lib.dem_add_local_damping(self.h, name.encode(), int(rot), float(visc)))

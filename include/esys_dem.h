@@ -78,6 +78,13 @@ int dem_add_rot_friction_group(dem_sim* h, const char* name, double k, double mu
  * translation, forces only.  FP64 form; no differentiable window or batched ensemble. */
 int dem_add_nrot_friction_group(dem_sim* h, const char* name, double k, double mu, double ks, double dt, int scaling);
 
+/* TSubLattice::addPairIG, type "HertzMindlin" (HertzMindlinPrms; Parallel/SubLattice.hpp:1324-1339):
+ * CHertzMindlinInteraction (Model/HertzMindlinInteraction.cpp:108-172) with CHertzMindlinIGP's packing
+ * order E, nu, mu, dt: Hertz normal force, Mindlin tangential stiffness, forces only.  Its storage is
+ * PIS_NE: the tangential history restarts at every neighbour rebuild, and checkpoints do not save it.
+ * FP64 form; no device bond hand-off, differentiable window or batched ensemble. */
+int dem_add_hertz_mindlin_group(dem_sim* h, const char* name, double E, double nu, double mu, double dt);
+
 /* TSubLattice::addBondedIG (NRotBondPrms; Parallel/SubLattice.hpp:1791-1831): CBondedInteraction
  * (Model/BondedInteraction.cpp:43-140) between connections of `tag`; rest length r1 + r2, failure
  * when the extension exceeds (r1 + r2) * rbreak; rbreak < 0: unbreakable.  Forces only.  No

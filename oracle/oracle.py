@@ -68,6 +68,7 @@ def _lib(backend: str):
         "move_tagged": (C.c_int, [_P, C.c_int, C.c_int, _D]),
         "add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
         "add_local_damping": (C.c_int, [_P, _S, C.c_int, C.c_double]),
+        "add_hertz_mindlin_group": (C.c_int, [_P, _S] + [C.c_double] * 4),
         "add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
         "save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
         "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
@@ -153,6 +154,12 @@ class OracleSim:
                            meanR_scaling=True, truncated=1.0):
         self._chk(self.f["add_rot_bond_group"](self.h, name.encode(), tag, kr, ks, kt, kb, max_n, max_s, max_t,
                                                max_b, int(scaling), int(meanR_scaling), truncated))
+
+    def add_hertz_mindlin_group(self, name, E, nu, mu, dt):
+        """HertzMindlin (CHertzMindlinInteraction) group (reference backend)."""
+        if "add_hertz_mindlin_group" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no HertzMindlin groups")
+        self._chk(self.f["add_hertz_mindlin_group"](self.h, name.encode(), E, nu, mu, dt))
 
     def add_local_damping(self, name, rot, visc):
         """LocalDamping / RotLocalDamping group (reference backend)."""

@@ -44,6 +44,7 @@
 #include "Model/EWallInteractionGroup.h"
 #include "Model/ElasticInteraction.h"
 #include "Model/FrictionInteraction.h"
+#include "Model/HertzMindlinInteraction.h"
 #include "Model/LocalDamping.h"
 #include "Model/LocalDampingIGP.h"
 #include "Model/RotLocalDamping.h"
@@ -74,6 +75,13 @@ struct BreakEvent { int id1, id2, step; };
 
 /* Read access to CFrictionInteraction's tangential force and flags (protected members), through
  * pointers to members formed in a derived class. */
+/* The same for CHertzMindlinInteraction. */
+struct HMAccess : CHertzMindlinInteraction {
+  static Vec3 CHertzMindlinInteraction::*ffric() { return &HMAccess::m_Ffric; }
+  static bool CHertzMindlinInteraction::*slipping() { return &HMAccess::m_is_slipping; }
+  static bool CHertzMindlinInteraction::*touching() { return &HMAccess::m_is_touching; }
+};
+
 struct FricAccess : CFrictionInteraction {
   static Vec3 CFrictionInteraction::*ffric() { return &FricAccess::m_Ffric; }
   static bool CFrictionInteraction::*slipping() { return &FricAccess::m_is_slipping; }
@@ -96,6 +104,7 @@ struct ASim {
   virtual int add_wall_group(const char* name, const char* wall, double k) = 0;
   virtual int add_nrot_friction(const char* name, double k, double mu, double ks, double dt, int scaling) = 0;
   virtual int add_nrot_bond(const char* name, int tag, double k, double rbreak, int scaling) = 0;
+  virtual int add_hertz_mindlin(const char* name, double E, double nu, double mu, double dt) = 0;
   virtual int add_gravity(const char* name, const double* g) = 0;
   virtual int add_damping(int rot, double visc, int maxiter) = 0;
   virtual int add_local_damping(const char* name, int rot, double visc) = 0;
@@ -137,6 +146,7 @@ struct RefSim : public ASim {
   std::map<std::string, void*> fric, bond;
   std::map<std::string, Exposed<ParallelInteractionStorage_ED<T, CFrictionInteraction>>*> nfric;
   std::map<std::string, Exposed<ParallelInteractionStorage_EB<T, CBondedInteraction>>*> nbond;
+  std::map<std::string, Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinInteraction>>*> hm;
 
   RefSim(double gs, double vd, const double* mn, const double* mx, const int* circ, double dt_)
       : comm(MPI_COMM_WORLD), dt(dt_), nrange(gs), alpha(vd) {
@@ -374,6 +384,14 @@ struct RefSim : public ASim {
     nfric[name] = s;
     return 0;
   }
+  /* TSubLattice::addPairIG, type "HertzMindlin" (Parallel/SubLattice.hpp:1324-1339) */
+  int add_hertz_mindlin(const char* name, double E, double nu, double mu, double dt_) override {
+    CHertzMindlinIGP p(name, E, nu, mu, dt_);
+    auto* s = new Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinInteraction>>(ppa, p);
+    dpis[name] = s;
+    hm[name] = s;
+    return 0;
+  }
   /* TSubLattice::addBondedIG (Parallel/SubLattice.hpp:1791-1831) */
   int add_nrot_bond(const char* name, int tag, double k, double rbreak, int scaling) override {
     CBondedIGP p(name, tag, k, rbreak, scaling != 0);
@@ -502,6 +520,7 @@ struct RefSim : public ASim {
   int num_pairs(const char* group) override {
     if (elastic.count(group)) return (int)elastic[group]->list().size();
     if (nfric.count(group)) return (int)nfric[group]->list().size();
+    if (hm.count(group)) return (int)hm[group]->list().size();
     if (nbond.count(group)) return (int)nbond[group]->list().size();
     if constexpr (kRot) {
       if (fric.count(group))
@@ -525,6 +544,20 @@ struct RefSim : public ASim {
           for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k];
           state[5 * i + 3] = (in.*FricAccess::slipping()) ? 1.0 : 0.0;
           state[5 * i + 4] = (in.*FricAccess::touching()) ? 1.0 : 0.0;
+        }
+        ++i;
+      }
+      return i;
+    }
+    if (hm.count(group)) {  /* HertzMindlin: tangential force (3), slipping, touching */
+      for (auto& in : hm[group]->list()) {
+        auto v = in.getAllID();
+        id1[i] = v[0]; id2[i] = v[1];
+        if (state) {
+          const Vec3 f = in.*HMAccess::ffric();
+          for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k];
+          state[5 * i + 3] = (in.*HMAccess::slipping()) ? 1.0 : 0.0;
+          state[5 * i + 4] = (in.*HMAccess::touching()) ? 1.0 : 0.0;
         }
         ++i;
       }
@@ -621,6 +654,9 @@ int ref_add_rot_bond_group(void* h, const char* name, int tag, double kr, double
   return static_cast<ASim*>(h)->add_rot_bond(name, tag, kr, ks, kt, kb, mn, ms, mt, mb, scaling, meanR, trunc);
 }
 int ref_add_wall_group(void* h, const char* name, const char* wall, double k) { return static_cast<ASim*>(h)->add_wall_group(name, wall, k); }
+int ref_add_hertz_mindlin_group(void* h, const char* name, double E, double nu, double mu, double dt) {
+  return static_cast<ASim*>(h)->add_hertz_mindlin(name, E, nu, mu, dt);
+}
 int ref_add_local_damping(void* h, const char* name, int rot, double visc) {
   return static_cast<ASim*>(h)->add_local_damping(name, rot, visc);
 }

@@ -66,6 +66,29 @@ def nrot_friction_pack(make, rot=False, n_side=5, seed=8, dt=1e-4, vscale=0.5):
     return sim
 
 
+def hertz_mindlin_pack(make, rot=False, n_side=5, seed=10, dt=1e-4, vscale=1.0, skin=0.05):
+    """nrot_friction_pack's lattice with a HertzMindlin group (CHertzMindlinInteraction,
+    E = 1e4, nu = 0.3, mu = 0.5) and a small Verlet skin, so that neighbour rebuilds (which
+    restart the law's tangential history, its storage being PIS_NE) fall inside a short run."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(n_side), np.arange(n_side), np.arange(n_side), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) * 0.95 + rng.uniform(-0.03, 0.03, size=g.shape)
+    rad = rng.uniform(0.46, 0.5, size=len(g))
+    n = len(g)
+    L = n_side * 0.95
+    sim = make("RotSphere" if rot else "NRotSphere", 1.2, skin, (0, 0, 0), (L, L, 2 * L), (0, 0, 0), dt)
+    vel = rng.normal(0, vscale, size=(n, 3))
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=vel)
+    sim.add_hertz_mindlin_group("hm", 1e4, 0.3, 0.5, dt)
+    sim.add_gravity("gravity", (0, 0, -9.81))
+    sim.add_damping(0, 0.01, 100)
+    for name, o, nrm in (("xlo", (0, 0, 0), (1, 0, 0)), ("xhi", (L, 0, 0), (-1, 0, 0)),
+                         ("zlo", (0, 0, 0), (0, 0, 1))):
+        sim.add_wall(name, o, nrm)
+        sim.add_wall_group(name + "_w", name, 1000.0)
+    return sim
+
+
 def nrot_bonded_block(make, nx=5, ny=6, nz=5, seed=9, dt=1e-4, k=1e4, rbreak=0.02, load_rate=0.01):
     """NRotSphere block with NRotBond (CBondedInteraction) between lattice neighbours (gap within
     0.015), failing on extension beyond r0 * rbreak, and an NRotFriction group for the contacts

@@ -133,3 +133,25 @@ def test_local_damping_matches_reference(gpu, ref, name):
     pa, pb = a.particles(), b.particles()
     for k in ("pos", "vel", "angvel"):
         _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
+
+
+@pytest.mark.parametrize("rot", [False, True])
+def test_hertz_mindlin_matches_reference(gpu, ref, rot):
+    """HertzMindlin (CHertzMindlinInteraction) through several neighbour rebuilds, which restart
+    its tangential history (PIS_NE storage) in the reference and here alike."""
+    a, b = S.hertz_mindlin_pack(gpu, rot=rot), S.hertz_mindlin_pack(ref, rot=rot)
+    c0 = a.counters()["rebuilds"]
+    a.step(300)
+    b.step(300)
+    assert a.counters()["rebuilds"] - c0 >= 2
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel"):
+        _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
+    fa, fb = _pairs(a, "hm"), _pairs(b, "hm")
+    assert fa.keys() == fb.keys()
+    keys = sorted(fb)
+    A = np.array([fa[k] for k in keys])
+    B = np.array([fb[k] for k in keys])
+    assert np.array_equal(A[:, 3:], B[:, 3:])
+    assert B[:, 4].sum() > 50 and B[:, 3].sum() > 10
+    _close(A[:, :3], B[:, :3], 1e-8, "history")
