@@ -57,6 +57,7 @@ struct Particles {
   ParticleBuf buf[2];
   double2* inv;          // 1/mass, 1/inertia
   double4* oldpos;       // position at the last neighbour search
+  double* cshift;        // accumulated circular shift in x (CParticle::m_circular_shift)
   double4* force;        // last accumulated force  (w unused)
   double4* moment;       // last accumulated moment (w unused)
   double4* force_eval;   // FP32 forces of an evaluation-only pass (precision check)

@@ -84,9 +84,11 @@ __global__ void k_bin(Grid g, Particles P, int cur, int* cell_count) {
   double4 p = P.buf[cur].pr[i];
   if (g.circx && isfinite(p.x)) {  // circular shift of particles that left through an x face (pp_array.hpp:465-503)
     if (p.x >= g.xmin + g.Lx || p.x < g.xmin) {
+      const double x0 = p.x;
       p.x -= g.Lx * floor((p.x - g.xmin) / g.Lx);
       if (p.x >= g.xmin + g.Lx) p.x -= g.Lx;  // rounding at the upper face
       P.buf[cur].pr[i] = p;
+      P.cshift[i] += p.x - x0;  // CParticle::setCircular moves m_initpos with m_pos (Model/Particle.cpp:335-341)
     }
   }
   int c = cell_of(g, p.x, p.y, p.z);
@@ -757,6 +759,34 @@ __global__ void k_particle_field(Particles P, int cur, int rot, int field, doubl
 }
 void launch_particle_field(const Particles& P, int cur, int rot, int field, double* out, cudaStream_t s) {
   if (P.n) k_particle_field<<<nblk(P.n, 256), 256, 0, s>>>(P, cur, rot, field, out);
+}
+
+// Per-particle vector fields (CParticle::getVectorFieldFunction, Model/Particle.cpp:166-184;
+// CRotParticle's, Model/RotParticle.cpp:459-480): 0 position, 1 velocity, 2 force, 3 ang_velocity
+// (getAngVelNR), 4 displacement (getTotalDisplacement = m_pos - m_initpos, m_initpos carried
+// along by the circular shifts).  initpos: 3 doubles per slot, the position at creation.
+__global__ void k_particle_vector_field(Particles P, int cur, int field, const double* initpos, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  V r = mk(0.0, 0.0, 0.0);
+  switch (field) {
+    case 0: r = xyz(P.buf[cur].pr[i]); break;
+    case 1: r = xyz(P.buf[cur].vm[i]); break;
+    case 2: r = xyz(P.force[i]); break;
+    case 3: r = xyz(P.buf[cur].wi[i]); break;
+    default: {
+      const V x = xyz(P.buf[cur].pr[i]);
+      const V x0 = mk(initpos[3 * i] + P.cshift[i], initpos[3 * i + 1], initpos[3 * i + 2]);
+      r = x - x0;
+    }
+  }
+  out[3 * i] = r.x;
+  out[3 * i + 1] = r.y;
+  out[3 * i + 2] = r.z;
+}
+void launch_particle_vector_field(const Particles& P, int cur, int field, const double* initpos, double* out,
+                                  cudaStream_t s) {
+  if (P.n) k_particle_vector_field<<<nblk(P.n, 256), 256, 0, s>>>(P, cur, field, initpos, out);
 }
 
 // Pair fields of a dynamic group from the state its last force evaluation read (buffer `prev`)

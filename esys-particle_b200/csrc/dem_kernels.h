@@ -44,6 +44,8 @@ void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const
 void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex, int* xbond, cudaStream_t s);
 void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s);
 void launch_particle_field(const Particles& P, int cur, int rot, int field, double* out, cudaStream_t s);
+void launch_particle_vector_field(const Particles& P, int cur, int field, const double* initpos, double* out,
+                                  cudaStream_t s);
 void launch_pair_field(const Grid& g, const Particles& P, int prev, const unsigned long long* keys, int m, int kind,
                        double k, double ks, int scaling, int meanR, const double4* hist, const float4* hist32,
                        int field, double* out, cudaStream_t s);

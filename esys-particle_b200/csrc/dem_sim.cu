@@ -195,7 +195,7 @@ struct DemSim {
     win.release();
     void* ps[] = {P.buf[0].pr, P.buf[0].vm, P.buf[0].wi, P.buf[0].qq, P.buf[1].pr, P.buf[1].vm, P.buf[1].wi,
                   P.buf[1].qq, P.buf[0].vw, P.buf[1].vw, P.inv, P.oldpos, P.force, P.moment, P.force_eval,
-                  P.moment_eval, P.sum_f, P.sum_m, P.pflags, P.flagged, P.id, P.tag, P.cell};
+                  P.moment_eval, P.sum_f, P.sum_m, P.pflags, P.flagged, P.id, P.tag, P.cell, P.cshift};
     for (void* p : ps) if (p) cudaFree(p);
     cell_count.release(); cell_start.release(); cell_cursor.release(); cell_list.release();
     scratch_i.release(); scratch_j.release(); scalars.release(); scan_tmp.release();
@@ -275,7 +275,7 @@ struct DemSim {
     grow_array(P.sum_f, n, nc); grow_array(P.sum_m, n, nc);
     grow_array(P.inv, n, nc); grow_array(P.oldpos, n, nc); grow_array(P.force, n, nc); grow_array(P.moment, n, nc);
     grow_array(P.pflags, n, nc); grow_array(P.flagged, n, nc); grow_array(P.id, n, nc); grow_array(P.tag, n, nc);
-    grow_array(P.cell, n, nc);
+    grow_array(P.cell, n, nc); grow_array(P.cshift, n, nc);
     cap = nc;
   }
 
@@ -329,6 +329,7 @@ struct DemSim {
       DEM_CUDA(cudaMemsetAsync(P.flagged + n, 0, add, s));
       DEM_CUDA(cudaMemsetAsync(P.force + n, 0, sizeof(double4) * add, s));
       DEM_CUDA(cudaMemsetAsync(P.moment + n, 0, sizeof(double4) * add, s));
+      DEM_CUDA(cudaMemsetAsync(P.cshift + n, 0, sizeof(double) * add, s));
       for (int i = 0; i < add; ++i) {
         id2slot[ids[i]] = n + i;
         h_id.push_back(ids[i]);
@@ -1366,6 +1367,7 @@ struct DemSim {
     std::vector<double4> pr(n), vm(n), wi(n), qq(n), op(n), fo(n);
     std::vector<unsigned> pf(n);
     std::vector<int> tg(n);
+    std::vector<double> csh(n);
     if (n) {
       const ParticleBuf& b = P.buf[cur];
       DEM_CUDA(cudaMemcpyAsync(pr.data(), b.pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
@@ -1376,6 +1378,7 @@ struct DemSim {
       if (store_forces) DEM_CUDA(cudaMemcpyAsync(fo.data(), P.force, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
       DEM_CUDA(cudaMemcpyAsync(pf.data(), P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s));
       DEM_CUDA(cudaMemcpyAsync(tg.data(), P.tag, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(csh.data(), P.cshift, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     }
     sync();
     const char d = ' ';
@@ -1387,11 +1390,12 @@ struct DemSim {
     os << alive << "\n";
     for (int i = 0; i < n; ++i) {
       if (!(pf[i] & PF_ALIVE)) continue;
-      // CParticle::saveCheckPointData (Model/Particle.cpp:461-475); one worker: no circular shift
+      // CParticle::saveCheckPointData (Model/Particle.cpp:461-475): the initial position less the
+      // circular shift, and the shift
       os << pr[i].x << d << pr[i].y << d << pr[i].z << d << pr[i].w << d << h_id[i] << d << tg[i] << d << vm[i].w << d
          << h_initpos[3 * (size_t)i] << d << h_initpos[3 * (size_t)i + 1] << d << h_initpos[3 * (size_t)i + 2] << d
          << op[i].x << d << op[i].y << d << op[i].z << d << vm[i].x << d << vm[i].y << d << vm[i].z << d
-         << fo[i].x << d << fo[i].y << d << fo[i].z << d << 0.0 << d << 0.0 << d << 0.0 << d
+         << fo[i].x << d << fo[i].y << d << fo[i].z << d << csh[i] << d << 0.0 << d << 0.0 << d
          << ((pf[i] & PF_DYN) ? 1 : 0);
       if (rot)  // CRotParticle::saveCheckPointData (Model/RotParticle.cpp:510-519)
         os << d << wi[i].w << d << qq[i].x << d << qq[i].y << d << qq[i].z << d << qq[i].w << d << wi[i].x << d
@@ -1543,6 +1547,7 @@ struct DemSim {
     std::vector<double4> pr(n), vm(n), wi(n), qq(n), op(n), fo(n);
     std::vector<unsigned> pf(n);
     std::vector<int> tg(n);
+    std::vector<double> csh(n);
     if (n) {
       const ParticleBuf& b = P.buf[cur];
       DEM_CUDA(cudaMemcpyAsync(pr.data(), b.pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
@@ -1553,6 +1558,7 @@ struct DemSim {
       if (store_forces) DEM_CUDA(cudaMemcpyAsync(fo.data(), P.force, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
       DEM_CUDA(cudaMemcpyAsync(pf.data(), P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s));
       DEM_CUDA(cudaMemcpyAsync(tg.data(), P.tag, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+      DEM_CUDA(cudaMemcpyAsync(csh.data(), P.cshift, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     }
     sync();
     const char d = ' ';
@@ -1564,7 +1570,7 @@ struct DemSim {
       os << pr[i].x << d << pr[i].y << d << pr[i].z << d << pr[i].w << d << h_id[i] << d << tg[i] << d << vm[i].w << d
          << h_initpos[3 * (size_t)i] << d << h_initpos[3 * (size_t)i + 1] << d << h_initpos[3 * (size_t)i + 2] << d
          << op[i].x << d << op[i].y << d << op[i].z << d << vm[i].x << d << vm[i].y << d << vm[i].z << d
-         << fo[i].x << d << fo[i].y << d << fo[i].z << d << 0.0 << d << 0.0 << d << 0.0;
+         << fo[i].x << d << fo[i].y << d << fo[i].z << d << csh[i] << d << 0.0 << d << 0.0;
       if (rot)
         os << d << qq[i].x << d << qq[i].y << d << qq[i].z << d << qq[i].w << d << wi[i].x << d << wi[i].y << d
            << wi[i].z;
@@ -1608,14 +1614,15 @@ struct DemSim {
     if (!is || np < 0) fail("bad particle block header");
     std::vector<int> ids(np), tags(np), flags(np);
     std::vector<double> pos(3 * (size_t)np), rad(np), mass(np), vel(3 * (size_t)np), angvel(3 * (size_t)np),
-        quat(4 * (size_t)np), initpos(3 * (size_t)np);
+        quat(4 * (size_t)np), initpos(3 * (size_t)np), shx(np);
     for (int i = 0; i < np; ++i) {
       double op[3], f[3], sh[3];
       int dynb = 1, rotb = 1;
       is >> pos[3 * i] >> pos[3 * i + 1] >> pos[3 * i + 2] >> rad[i] >> ids[i] >> tags[i] >> mass[i] >> initpos[3 * i]
          >> initpos[3 * i + 1] >> initpos[3 * i + 2] >> op[0] >> op[1] >> op[2] >> vel[3 * i] >> vel[3 * i + 1]
          >> vel[3 * i + 2] >> f[0] >> f[1] >> f[2] >> sh[0] >> sh[1] >> sh[2] >> dynb;
-      for (int k = 0; k < 3; ++k) initpos[3 * i + k] += sh[k];
+      shx[i] = sh[0];  // x: the circular shift, carried on the device
+      for (int k = 1; k < 3; ++k) initpos[3 * i + k] += sh[k];
       quat[4 * i] = 1.0;
       if (rot) {
         double inert;
@@ -1627,11 +1634,14 @@ struct DemSim {
     }
     add_particles(np, ids.data(), tags.data(), pos.data(), rad.data(), mass.data(), vel.data(),
                   rot ? angvel.data() : nullptr, rot ? quat.data() : nullptr, flags.data());
+    std::vector<double> csh(n, 0.0);
     for (int i = 0; i < np; ++i) {
       auto sl = id2slot.find(ids[i]);
-      if (sl != id2slot.end())
-        for (int k = 0; k < 3; ++k) h_initpos[3 * (size_t)sl->second + k] = initpos[3 * i + k];
+      if (sl == id2slot.end()) continue;
+      for (int k = 0; k < 3; ++k) h_initpos[3 * (size_t)sl->second + k] = initpos[3 * i + k];
+      csh[sl->second] = shx[i];
     }
+    if (n) DEM_CUDA(cudaMemcpyAsync(P.cshift, csh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
     std::vector<double4> pr(n);
     if (n) DEM_CUDA(cudaMemcpyAsync(pr.data(), P.buf[cur].pr, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
     sync();
@@ -2938,6 +2948,38 @@ int dem_particle_scalar_field(dem_sim* h, const char* field, double* values) {
     int k = 0;
     for (int i = 0; i < n; ++i)
       if (pf[i] & dem::PF_ALIVE) values[k++] = v[i];
+    return k;
+  });
+}
+
+int dem_particle_vector_field(dem_sim* h, const char* field, double* values) {
+  return guard(h, [&](DemSim& s) {
+    static const char* names[] = {"position", "velocity", "force", "ang_velocity", "displacement"};
+    const std::string f = field ? field : "";
+    int code = -1;
+    for (int k = 0; k < 5; ++k)
+      if (f == names[k]) code = k;
+    if (code < 0 || (code == 3 && !s.rot)) throw std::invalid_argument("unknown particle vector field " + f);
+    if (!values) throw std::invalid_argument("null output");
+    const int n = s.n;
+    s.scratch_d.reserve(std::max(6 * n, 1));
+    if (code == 4 && n)
+      DEM_CUDA(cudaMemcpyAsync(s.scratch_d.p + 3 * (size_t)n, s.h_initpos.data(), sizeof(double) * 3 * n,
+                               cudaMemcpyHostToDevice, s.s));
+    launch_particle_vector_field(s.P, s.cur, code, s.scratch_d.p + 3 * (size_t)n, s.scratch_d.p, s.s);
+    std::vector<double> v(3 * (size_t)n);
+    std::vector<unsigned> pf(n);
+    if (n) {
+      DEM_CUDA(cudaMemcpyAsync(v.data(), s.scratch_d.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s.s));
+      DEM_CUDA(cudaMemcpyAsync(pf.data(), s.P.pflags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s.s));
+    }
+    s.sync();
+    int k = 0;
+    for (int i = 0; i < n; ++i)
+      if (pf[i] & dem::PF_ALIVE) {
+        for (int c = 0; c < 3; ++c) values[3 * k + c] = v[3 * (size_t)i + c];
+        ++k;
+      }
     return k;
   });
 }

@@ -17,13 +17,15 @@ import numpy as np
 from . import _capi
 from .checkpoint import CheckPointer, CheckPointPrms, RestartCheckPointPrms, read_info, walls_in, worker_file
 from .fields import (FieldSaver, InteractionScalarFieldSaverPrms, ParticleScalarFieldSaverPrms,
-                     WallVectorFieldSaverPrms)
+                     ParticleVectorFieldSaverPrms, TaggedParticleScalarFieldSaverPrms,
+                     TaggedParticleVectorFieldSaverPrms, WallVectorFieldSaverPrms)
 from .util import BoundingBox, Vec3
 
 __all__ = [
     "LsmMpi", "NRotSphere", "RotSphere", "Runnable", "NRotElasticPrms", "RotFrictionPrms", "RotBondPrms",
     "NRotElasticWallPrms", "LinDampingPrms", "RotDampingPrms", "GravityPrms", "Vec3", "BoundingBox",
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
+    "ParticleVectorFieldSaverPrms", "TaggedParticleScalarFieldSaverPrms", "TaggedParticleVectorFieldSaverPrms",
     "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms", "LocalDampingPrms",
     "RotLocalDampingPrms", "HertzMindlinPrms",
 ]

@@ -62,6 +62,7 @@ SIGNATURES = {
     "dem_wall_reactions_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dem_set_group_param": (C.c_int, [_P, _S, _S, C.c_double]),
     "dem_particle_scalar_field": (C.c_int, [_P, _S, _D]),
+    "dem_particle_vector_field": (C.c_int, [_P, _S, _D]),
     "dem_interaction_scalar_field": (C.c_int, [_P, _S, _S, _D]),
     "dem_window_num_params": (C.c_int, [_P]),
     "dem_window_forward": (C.c_int, [_P, C.c_int, C.c_int, _D]),
@@ -316,6 +317,19 @@ class DemSim:
         n = self.num_particles()
         v = np.zeros(max(n, 1))
         self._chk(self.lib.dem_particle_scalar_field(self.h, field.encode(), _dp(v)))
+        ids = np.zeros(max(n, 1), np.int32)
+        self._chk(self.lib.dem_get_particles(self.h, _ip(ids), None, None, None, None, None, None))
+        ids, v = ids[:n], v[:n]
+        if sort:
+            o = np.argsort(ids, kind="stable")
+            return ids[o], v[o]
+        return ids, v
+
+    def particle_vector_field(self, field, sort=True):
+        """(ids, values n x 3) of a particle vector field (dem_particle_vector_field), by id when sort."""
+        n = self.num_particles()
+        v = np.zeros((max(n, 1), 3))
+        self._chk(self.lib.dem_particle_vector_field(self.h, field.encode(), _dp(v)))
         ids = np.zeros(max(n, 1), np.int32)
         self._chk(self.lib.dem_get_particles(self.h, _ip(ids), None, None, None, None, None, None))
         ids, v = ids[:n], v[:n]

@@ -240,6 +240,13 @@ int dem_set_option(dem_sim* h, const char* key, double value);
  * "id", "tag".  values[] in dem_get_particles order; returns the count. */
 int dem_particle_scalar_field(dem_sim* h, const char* field, double* values);
 
+/* Per-particle vector field (CParticle::getVectorFieldFunction, Model/Particle.cpp:166-184;
+ * CRotParticle::getVectorFieldFunction, Model/RotParticle.cpp:459-480): "position", "velocity",
+ * "force", "displacement" (getTotalDisplacement: position less the position at creation, which
+ * follows the circular shifts) and, for RotSpheres, "ang_velocity".  values[] is n x 3 in
+ * dem_get_particles order; returns the count. */
+int dem_particle_vector_field(dem_sim* h, const char* field, double* values);
+
 /* Per-interaction scalar field of one group, from the state its last force evaluation read:
  * NRotElastic "count", "potential_energy"; RotFriction "count", "potential_energy", "slipping",
  * "sticking" (Model/RotFricInteraction.cpp:384-452, 486-508); RotBond "count",

@@ -119,3 +119,60 @@ def test_lsm_field_savers_write_reference_formats(dem_lib, tmp_path):
         s += x
     assert ek[-1] == "%g" % s
     sim.exit()
+
+
+def _gas(make, n_side=5, with_particles=True):
+    """NRotSpheres, one per x-row of a 5 x 5 (y, z) lattice, crossing the periodic x faces at
+    5 to 12 per unit time: no contacts, so each one's unwrapped path is x0 + v t."""
+    sim = make("NRotSphere", 1.2, 0.2, (0, 0, 0), (6, 6, 6), (1, 0, 0), 1e-3)
+    sim.add_elastic_group("elastic", 1000.0, True)
+    if with_particles:
+        rng = np.random.default_rng(21)
+        yz = np.stack(np.meshgrid(np.arange(n_side), np.arange(n_side), indexing="ij"), -1).reshape(-1, 2)
+        n = len(yz)
+        pos = np.zeros((n, 3))
+        pos[:, 0] = rng.uniform(0.5, 5.5, n)
+        pos[:, 1:] = yz * 1.2 + 0.6 + rng.uniform(-0.1, 0.1, size=yz.shape)
+        vel = np.zeros((n, 3))
+        vel[:, 0] = rng.uniform(5.0, 12.0, n) * rng.choice([-1.0, 1.0], n)
+        sim.add_particles(np.arange(n), pos, np.full(n, 0.3), np.full(n, 0.1), tag=np.zeros(n, np.int32), vel=vel)
+        sim._x0, sim._v = pos, vel
+    return sim
+
+
+def test_vector_fields_match_particle_state(gpu):
+    s = S.friction_pack(gpu)
+    s.step(30)
+    p = s.particles()
+    for field, key in (("position", "pos"), ("velocity", "vel"), ("force", "force"), ("ang_velocity", "angvel")):
+        ids, v = s.particle_vector_field(field)
+        assert np.array_equal(ids, p["id"]) and np.array_equal(v, p[key]), field
+    with pytest.raises(Exception):
+        _gas(gpu).particle_vector_field("ang_velocity")  # NRotSpheres have no spin field
+
+
+def test_displacement_follows_circular_shifts_and_checkpoints(gpu, tmp_path):
+    """getTotalDisplacement = m_pos - m_initpos, with m_initpos moved by every circular shift
+    (CParticle::setCircular): continuous across the periodic faces, and carried by a restart
+    checkpoint's shift column (CParticle::saveCheckPointData)."""
+    s = _gas(gpu)
+    s.step(300)
+    t = 300 * 1e-3
+    ids, d = s.particle_vector_field("displacement")
+    p = s.particles()
+    want = s._v[ids] * t
+    assert np.abs(d - want).max() < 1e-9
+    wrapped = np.abs((p["pos"] - s._x0[ids])[:, 0] - d[:, 0]) > 1.0
+    assert wrapped.sum() >= 5
+    path = str(tmp_path / "gas_t=300_1.txt")
+    s.save_checkpoint(path, 17)
+    s2 = _gas(gpu, with_particles=False)
+    s2.load_checkpoint(path, 300)
+    _, d2 = s2.particle_vector_field("displacement")
+    assert np.abs(d2 - d).max() < 1e-12
+    s.step(100)
+    s2.step(100)
+    _, d3 = s.particle_vector_field("displacement")
+    _, d4 = s2.particle_vector_field("displacement")
+    assert np.abs(d3 - d4).max() < 1e-12
+    assert np.abs(d3 - s._v[ids] * 0.4).max() < 1e-9
