@@ -95,8 +95,10 @@ struct DynDev {
 };
 
 struct BondDev {
-  int kind;                 // 0 RotBond (ARotBondedInteraction), 1 NRotBond (CBondedInteraction)
+  int kind;                 // 0 RotBond (ARotBondedInteraction), 1 NRotBond (CBondedInteraction),
+                            // 2 BrittleBeamDZC (RotBond forces, BrittleBeamDZCInteraction::broken)
   double knb, rbreak;       // NRotBond: normal stiffness (unscaled), relative breaking distance (< 0: unbreakable)
+  double cohesion, tan_angle, t_cutoff, c_cutoff, beta1, beta2;  // BrittleBeamDZC failure criterion
   double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
   int scaling, meanR;
   const int* adj_start;

@@ -355,6 +355,21 @@ __device__ __forceinline__ bool bond_broken(const BondK& K, const BondOut& o, do
   return (normalStress > truncated) || (shearStress > (1.0 - normalStress));
 }
 
+// BrittleBeamDZCInteraction::broken (Model/BrittleBeamDZC.cpp:122-139) with the effective beam
+// section of its constructor (:99-102): radius half the bond's length at creation (dist0),
+// area pi R^2, second moments pi R^4 / 4 and pi R^4 / 2.
+__device__ __forceinline__ bool dzc_broken(const BondOut& o, double dist0, double cohesion, double tan_angle,
+                                           double t_cutoff, double c_cutoff, double beta1, double beta2) {
+  const double pi = 3.14159265358979323846;  // M_PI
+  const double effR = 0.5 * dist0;
+  const double effA = pi * effR * effR;
+  const double effI = 0.25 * pi * effR * effR * effR * effR;
+  const double effJ = 0.5 * pi * effR * effR * effR * effR;
+  const double shearStress = o.shF / effA + beta2 * o.tM * effR / effJ;
+  const double normalStress = -1. * (o.nF / effA + beta1 * o.bM * effR / effI);
+  return (normalStress < -1. * t_cutoff) || (shearStress > c_cutoff) || (shearStress > (cohesion + normalStress * tan_angle));
+}
+
 // CElasticWallInteraction: ctor scaling (Model/EWallInteraction.hpp:26-36) and
 // calcForces (:42-78).  Returns true when in contact; F is the force on the particle.
 __device__ __forceinline__ bool law_wall(double k, const V& o, const V& n, const V& x, double r, V& F) {

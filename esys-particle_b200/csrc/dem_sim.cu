@@ -94,8 +94,9 @@ struct DynGroup {
 };
 
 struct BondGroup {
-  int kind = 0;                 // 0 RotBond, 1 NRotBond (CBondedInteraction)
+  int kind = 0;                 // 0 RotBond, 1 NRotBond (CBondedInteraction), 2 BrittleBeamDZC
   double knb = 0, rbreak = 0;   // NRotBond: normalK, relative breaking distance (< 0: unbreakable)
+  double cohesion = 0, tan_angle = 0, t_cutoff = 0, c_cutoff = 0, beta1 = 0, beta2 = 0;  // BrittleBeamDZC
   int tag;
   double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
   int scaling, meanR;
@@ -688,7 +689,7 @@ struct DemSim {
 
   bool widened() const {
     for (auto& d : dyn) if (d.second.kind >= 2) return true;
-    for (auto& b : bond) if (b.second.kind == 1) return true;
+    for (auto& b : bond) if (b.second.kind != 0) return true;
     return false;
   }
 
@@ -735,6 +736,8 @@ struct DemSim {
       BondGroup& B = b.second;
       BondDev& D = a.bond[a.nbond++];
       D.kind = B.kind; D.knb = B.knb; D.rbreak = B.rbreak;
+      D.cohesion = B.cohesion; D.tan_angle = B.tan_angle; D.t_cutoff = B.t_cutoff; D.c_cutoff = B.c_cutoff;
+      D.beta1 = B.beta1; D.beta2 = B.beta2;
       D.kr = B.kr; D.ks = B.ks; D.kt = B.kt; D.kb = B.kb; D.mn = B.mn; D.ms = B.ms; D.mt = B.mt; D.mb = B.mb;
       D.truncated = B.truncated; D.scaling = B.scaling; D.meanR = B.meanR;
       D.adj_start = B.adj_start.p; D.adj = B.adj.p; D.D0 = B.D0.p; D.broken_step = B.broken_step.p;
@@ -1363,6 +1366,8 @@ struct DemSim {
   }
 
   void save_checkpoint(std::ostream& os) {
+    for (auto& b : bond)
+      if (b.second.kind == 2) throw std::invalid_argument("restart checkpoints of BrittleBeamDZC groups are not built");
     download_walls();
     std::vector<double4> pr(n), vm(n), wi(n), qq(n), op(n), fo(n);
     std::vector<unsigned> pf(n);
@@ -1605,6 +1610,8 @@ struct DemSim {
   // the groups' parameters).  timestep: the master's step counter (CheckPointInfo).
   void load_checkpoint(std::istream& is, long long timestep) {
     if (n) throw StateError("a checkpoint is loaded into a worker without particles");
+    for (auto& b : bond)
+      if (b.second.kind == 2) throw std::invalid_argument("restart checkpoints of BrittleBeamDZC groups are not built");
     auto fail = [&](const std::string& what) { throw std::invalid_argument("checkpoint: " + what); };
     double bp[3];
     int bi[3];
@@ -2499,6 +2506,27 @@ int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, dou
   });
 }
 
+// TRotSubLattice::addBrittleBeamDZCIG (Parallel/RotSubLattice.hpp:227-267): BrittleBeamDZCIGP from raw
+// stiffnesses, which ARotBondedIGP scales with the bond's half length (scaling on); the failure
+// criterion's friction angle is in degrees, its tangent taken as the interaction's constructor does
+// (Model/BrittleBeamDZC.cpp:90-103).
+int dem_add_brittle_beam_dzc_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                                   double cohesion, double tCutoff, double cCutoff, double fAngle, double beta1,
+                                   double beta2) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.rot) throw std::invalid_argument("BrittleBeamDZC needs RotSphere particles");
+    add_bond_group(s, name, tag, [&](dem::BondGroup& B) {
+      B.kind = 2;
+      B.kr = kr; B.ks = ks; B.kt = kt; B.kb = kb;
+      B.mn = B.ms = B.mt = B.mb = 1.0;  // no force strengths: the criterion is the beam's
+      B.scaling = 1; B.meanR = 1; B.truncated = 1.0;
+      B.cohesion = cohesion; B.tan_angle = std::tan(fAngle / 57.2957795); B.t_cutoff = tCutoff;
+      B.c_cutoff = cCutoff; B.beta1 = beta1; B.beta2 = beta2;
+    });
+    return DEM_OK;
+  });
+}
+
 // TSubLattice::addBondedIG (Parallel/SubLattice.hpp:1791-1831): CBondedIGP (tag, k, rbreak, scaling);
 // rbreak < 0 makes the group unbreakable.
 int dem_add_nrot_bond_group(dem_sim* h, const char* name, int tag, double k, double rbreak, int scaling) {
@@ -3028,6 +3056,8 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto b = s.bond.find(gname);
     if (b == s.bond.end()) throw std::invalid_argument("no such group " + gname);
     if (b->second.kind == 1) throw std::invalid_argument("interaction fields of NRotBond groups are not built");
+    if (b->second.kind == 2 && f == "breaking_criterion")
+      throw std::invalid_argument("BrittleBeamDZC groups have no breaking_criterion field");
     static const char* names[] = {"count", "potential_energy", "e_pot_normal", "e_pot_shear", "e_pot_twist",
                                   "e_pot_bend", "breaking_criterion"};
     int code = -1;

@@ -299,7 +299,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           if (isp1) {
             Fp += o.force;
             Mp += o.moment1;
-            if (!EVAL && bond_broken(K, o, B.truncated)) {
+            const bool brk = B.kind == 2 ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff,
+                                                      B.beta1, B.beta2)
+                                         : bond_broken(K, o, B.truncated);
+            if (!EVAL && brk) {
               B.broken_step[k] = (int)(step + 1);
               a.P.flagged[i] = 1;
               a.P.flagged[j] = 1;
@@ -592,7 +595,9 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
   r[0] = d4(o.force, 0.0);
   r[1] = d4(o.moment1, 0.0);
   r[2] = d4(o.moment2, 0.0);
-  if (!EVAL && bond_broken(K, o, B.truncated)) {
+  const bool brk = B.kind == 2 ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff, B.beta1, B.beta2)
+                               : bond_broken(K, o, B.truncated);
+  if (!EVAL && brk) {
     const int i = e.x, j = e.y;
     B.broken_step[k] = (int)(step + 1);
     a.P.flagged[i] = 1;

@@ -27,7 +27,7 @@ __all__ = [
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
     "ParticleVectorFieldSaverPrms", "TaggedParticleScalarFieldSaverPrms", "TaggedParticleVectorFieldSaverPrms",
     "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms", "LocalDampingPrms",
-    "RotLocalDampingPrms", "HertzMindlinPrms",
+    "RotLocalDampingPrms", "HertzMindlinPrms", "BrittleBeamDZCPrms",
 ]
 
 
@@ -142,6 +142,23 @@ class HertzMindlinPrms:  # InteractionParamsPy.cpp:1350-1380 (CHertzMindlinIGP)
     def __init__(self, name, youngsModulus, poissonsRatio, dynamicMu):
         self.name, self.youngsModulus, self.poissonsRatio = name, float(youngsModulus), float(poissonsRatio)
         self.dynamicMu = float(dynamicMu)
+
+
+class BrittleBeamDZCPrms:  # InteractionParamsPy.cpp:711-727, 1733-1760 (BrittleBeamDZCIGP)
+    """Stiffnesses from the beam's Young's modulus and Poisson's ratio as ARotBondedIGP forms them
+    (Model/ARotBondedInteraction.cpp: kr = kb = pi E, ks = kt = pi E / (2 (1 + nu)))."""
+
+    def __init__(self, name, youngsModulus, poissonsRatio, cohesion, frictionAngle, tensileCutoff, compressCutoff,
+                 beta1, beta2, tag):
+        import math
+
+        self.name, self.tag = name, int(tag)
+        E, nu = float(youngsModulus), float(poissonsRatio)
+        G = E / (2.0 * (1. + nu))
+        self.kr, self.ks, self.kb, self.kt = math.pi * E, math.pi * G, math.pi * E, math.pi * G
+        self.cohesion, self.frictionAngle = float(cohesion), float(frictionAngle)
+        self.tensileCutoff, self.compressCutoff = float(tensileCutoff), float(compressCutoff)
+        self.beta1, self.beta2 = float(beta1), float(beta2)
 
 
 class LocalDampingPrms:  # InteractionParamsPy.cpp:1033-1048 (CLocalDampingIGP "LocalDamping")
@@ -318,6 +335,10 @@ class LsmMpi:
             s.add_nrot_friction_group(prms.name, prms.normalK, prms.dynamicMu, prms.shearK, self._dt, prms.scaling)
         elif isinstance(prms, HertzMindlinPrms):  # LsmMpiPy::createHertzMindlinIG sets dt (LsmMpiPy.cpp:508-517)
             s.add_hertz_mindlin_group(prms.name, prms.youngsModulus, prms.poissonsRatio, prms.dynamicMu, self._dt)
+        elif isinstance(prms, BrittleBeamDZCPrms):  # LsmMpiPy::createBrittleBeamDZCInteractGrp
+            s.add_brittle_beam_dzc_group(prms.name, prms.tag, prms.kr, prms.ks, prms.kt, prms.kb, prms.cohesion,
+                                         prms.tensileCutoff, prms.compressCutoff, prms.frictionAngle, prms.beta1,
+                                         prms.beta2)
         elif isinstance(prms, NRotBondPrms):
             s.add_nrot_bond_group(prms.name, prms.tag, prms.normalK, prms.breakDistance, prms.scaling)
         elif isinstance(prms, NRotElasticWallPrms):

@@ -85,6 +85,17 @@ int dem_add_nrot_friction_group(dem_sim* h, const char* name, double k, double m
  * FP64 form; no device bond hand-off, differentiable window or batched ensemble. */
 int dem_add_hertz_mindlin_group(dem_sim* h, const char* name, double E, double nu, double mu, double dt);
 
+/* TRotSubLattice::addBrittleBeamDZCIG (BrittleBeamDZCPrms; Parallel/RotSubLattice.hpp:227-267):
+ * BrittleBeamDZCInteraction (Model/BrittleBeamDZC.cpp) between the tagged connections, with the
+ * master's packing order kr, ks, kt, kb, cohesion, tCutoff, cCutoff, fAngle (degrees), beta1,
+ * beta2.  Forces and moments are RotBond's (ARotBondedInteraction::calcForces, stiffnesses scaled by
+ * the half bond length); failure when the beam's normal stress falls below -tCutoff, its shear
+ * stress exceeds cCutoff, or exceeds cohesion + normal stress * tan(fAngle).  RotSpheres; no
+ * restart checkpoint, differentiable window or batched ensemble. */
+int dem_add_brittle_beam_dzc_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                                   double cohesion, double tCutoff, double cCutoff, double fAngle, double beta1,
+                                   double beta2);
+
 /* TSubLattice::addBondedIG (NRotBondPrms; Parallel/SubLattice.hpp:1791-1831): CBondedInteraction
  * (Model/BondedInteraction.cpp:43-140) between connections of `tag`; rest length r1 + r2, failure
  * when the extension exceeds (r1 + r2) * rbreak; rbreak < 0: unbreakable.  Forces only.  No

@@ -69,6 +69,7 @@ def _lib(backend: str):
         "add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
         "add_local_damping": (C.c_int, [_P, _S, C.c_int, C.c_double]),
         "add_hertz_mindlin_group": (C.c_int, [_P, _S] + [C.c_double] * 4),
+        "add_brittle_beam_dzc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 10),
         "add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
         "save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
         "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
@@ -160,6 +161,13 @@ class OracleSim:
         if "add_hertz_mindlin_group" not in self.f:
             raise NotImplementedError(f"{self.backend} has no HertzMindlin groups")
         self._chk(self.f["add_hertz_mindlin_group"](self.h, name.encode(), E, nu, mu, dt))
+
+    def add_brittle_beam_dzc_group(self, name, tag, kr, ks, kt, kb, cohesion, tCutoff, cCutoff, fAngle, beta1, beta2):
+        """BrittleBeamDZC (BrittleBeamDZCInteraction) group (reference backend)."""
+        if "add_brittle_beam_dzc_group" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no BrittleBeamDZC groups")
+        self._chk(self.f["add_brittle_beam_dzc_group"](self.h, name.encode(), int(tag), *(float(x) for x in (
+            kr, ks, kt, kb, cohesion, tCutoff, cCutoff, fAngle, beta1, beta2))))
 
     def add_local_damping(self, name, rot, visc):
         """LocalDamping / RotLocalDamping group (reference backend)."""

@@ -161,7 +161,7 @@ def friction_pack(make, nx=6, ny=5, nz=6, seed=2, periodic=False, dt=5e-5, vscal
 
 
 def bonded_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, strength=(0.5, 1.0, 1.0, 0.5), load_rate=0.02,
-                 with_friction=True):
+                 with_friction=True, bonds=True):
     """Small bonded block: jittered cubic RotSpheres, every pair within gap 1e-3
     of touching bonded (cf. Geometry/DistConnections), RotBond with brittle
     failure, RotFriction + exclusion for post-break contacts, platens at y."""
@@ -181,7 +181,8 @@ def bonded_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, strength=(0.5, 1.0, 1.
     sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32))
     sim.add_connections(np.ones(len(i1), np.int32), i1, i2)
     mn, ms, mt, mb = strength
-    sim.add_rot_bond_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, mn, ms, mt, mb, True, True, 1.0)
+    if bonds:
+        sim.add_rot_bond_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, mn, ms, mt, mb, True, True, 1.0)
     if with_friction:
         sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
         sim.add_exclusion("bonds", "friction")
@@ -192,6 +193,18 @@ def bonded_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, strength=(0.5, 1.0, 1.
     sim.add_damping(0, 0.01, 50)
     sim.add_damping(1, 0.01, 50)
     sim._load_rate = load_rate
+    return sim
+
+
+def dzc_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, crit=(3.0, 5.0, 20.0, 30.0, 1.0, 1.0), load_rate=0.02):
+    """bonded_block's specimen with BrittleBeamDZC bonds (BrittleBeamDZCInteraction: RotBond forces,
+    a cut-off Mohr-Coulomb failure of the beam's normal and shear stress) instead of RotBond.
+    crit = (cohesion, tCutoff, cCutoff, fAngle in degrees, beta1, beta2)."""
+    sim = bonded_block(make, nx, ny, nz, seed, dt, load_rate=load_rate, with_friction=False, bonds=False)
+    coh, tcut, ccut, fang, b1, b2 = crit
+    sim.add_brittle_beam_dzc_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, coh, tcut, ccut, fang, b1, b2)
+    sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
+    sim.add_exclusion("bonds", "friction")
     return sim
 
 

@@ -155,3 +155,21 @@ def test_hertz_mindlin_matches_reference(gpu, ref, rot):
     assert np.array_equal(A[:, 3:], B[:, 3:])
     assert B[:, 4].sum() > 50 and B[:, 3].sum() > 10
     _close(A[:, :3], B[:, :3], 1e-8, "history")
+
+
+def test_brittle_beam_dzc_failures_match_reference(gpu, ref):
+    """BrittleBeamDZC (BrittleBeamDZCInteraction): RotBond forces and moments, the beam-stress
+    failure criterion; failure events exact, state within 1e-9 of the reference's own class."""
+    a, b = S.dzc_block(gpu), S.dzc_block(ref)
+    S.run_loaded(a, 400, 2e-4)
+    S.run_loaded(b, 400, 2e-4)
+    ea, eb = ({e for e in zip(*(x.tolist() for x in log)) if e[2] <= 400} for log in (a.breaks(), b.breaks()))
+    assert len(eb) > 20 and len({e[2] for e in eb}) > 10  # failures spread over the run
+    assert ea == eb
+    assert _pairs(a, "bonds").keys() == _pairs(b, "bonds").keys()
+    assert _pairs(a, "friction").keys() == _pairs(b, "friction").keys()
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel", "angvel"):
+        _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
+    with pytest.raises(Exception):
+        a.save_checkpoint("unused_t=1_1.txt", 12)  # restart records of these groups are not built

@@ -162,3 +162,60 @@ def test_lsmmpi_widened_law_prms_match_direct_calls(oracle_libs):
             assert np.array_equal(a[k], b[k]), (law, k)
         st = np.array(d.pairs("c")[2])
         assert st[:, 4].sum() > 5, law  # contacts were touching
+
+
+def test_lsmmpi_brittle_beam_dzc_prms_match_direct_calls(oracle_libs):
+    """BrittleBeamDZCPrms(name, E, nu, cohesion, frictionAngle, tensileCutoff, compressCutoff, beta1,
+    beta2, tag) reaches the group the raw-stiffness call makes (ARotBondedIGP's kr = kb = pi E,
+    ks = kt = pi E / (2 (1 + nu))), and its bonds fail in the reference's own class."""
+    import math
+
+    import pytest
+
+    from esys.lsm import BrittleBeamDZCPrms, LsmMpi, RotSphere, NRotElasticWallPrms
+    from esys.lsm.util import BoundingBox, Vec3
+
+    if not oracle_libs.available("ref"):
+        pytest.skip("reference harness not built")
+    E, nu = 3e4, 0.25
+    crit = dict(cohesion=2.0, frictionAngle=30.0, tensileCutoff=3.0, compressCutoff=10.0, beta1=1.0, beta2=1.0)
+    rng = np.random.default_rng(5)
+    pos = [(0.5 + (i % 3), 0.5 + (i // 3 % 3), 0.5 + (i // 9)) for i in range(18)]
+    pos = [tuple(x + rng.uniform(-0.005, 0.005) for x in p) for p in pos]
+    bonds = [(i, j) for i in range(18) for j in range(i + 1, 18)
+             if abs(np.linalg.norm(np.subtract(pos[i], pos[j])) - 1.0) < 0.02]
+
+    sim = LsmMpi(numWorkerProcesses=1, mpiDimList=[1, 1, 1], _backend=RefBackend)
+    sim.initNeighbourSearch(particleType="RotSphere", gridSpacing=1.25, verletDist=0.2)
+    sim.setNumTimeSteps(150)
+    sim.setTimeStepSize(1e-5)
+    sim.setSpatialDomain(BoundingBox(Vec3(0, 0, 0), Vec3(3, 3, 2)))
+    vel = rng.normal(0, 2.0, size=(18, 3))
+    parts = []
+    for i, p in enumerate(pos):
+        q = RotSphere(i, Vec3(*p), 0.5, float(S.sphere_mass(0.5)))
+        q.setLinearVelocity(Vec3(*vel[i]))
+        parts.append(q)
+    sim.createParticles(parts)
+    sim.createConnections([(1, i, j) for i, j in bonds])
+    sim.createInteractionGroup(BrittleBeamDZCPrms("bb", E, nu, tag=1, **crit))
+    sim.createWall("top", Vec3(0, 3.02, 0), Vec3(0, -1, 0))
+    sim.createInteractionGroup(NRotElasticWallPrms("top_w", "top", 1e5))
+    sim.run()
+
+    d = RefBackend("RotSphere", 1.25, 0.2, (0, 0, 0), (3, 3, 2), (0, 0, 0), 1e-5)
+    d.add_particles(list(range(18)), [list(p) for p in pos], [0.5] * 18, [float(S.sphere_mass(0.5))] * 18,
+                    tag=[0] * 18, vel=vel)
+    d.add_connections([1] * len(bonds), [i for i, _ in bonds], [j for _, j in bonds])
+    G = E / (2.0 * (1. + nu))
+    d.add_brittle_beam_dzc_group("bb", 1, math.pi * E, math.pi * G, math.pi * G, math.pi * E, 2.0, 3.0, 10.0, 30.0,
+                                 1.0, 1.0)
+    d.add_wall("top", (0, 3.02, 0), (0, -1, 0))
+    d.add_wall_group("top_w", "top", 1e5)
+    d.step(150)
+    a, b = sim._sim.particles(), d.particles()
+    for k in ("pos", "vel", "angvel"):
+        assert np.array_equal(a[k], b[k]), k
+    assert len(bonds) > 20 and np.abs(b["angvel"]).max() > 0
+    ba, bb = sim._sim.breaks(), d.breaks()
+    assert all(np.array_equal(x, y) for x, y in zip(ba, bb)) and 0 < len(bb[0]) < len(bonds)
