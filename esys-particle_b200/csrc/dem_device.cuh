@@ -96,9 +96,10 @@ struct DynDev {
 
 struct BondDev {
   int kind;                 // 0 RotBond (ARotBondedInteraction), 1 NRotBond (CBondedInteraction),
-                            // 2 BrittleBeamDZC (RotBond forces, BrittleBeamDZCInteraction::broken)
+                            // 2 BrittleBeamDZC (RotBond forces, BrittleBeamDZCInteraction::broken),
+                            // 3 BrittleBeamSC (RotBond forces, BrittleBeamSCInteraction::broken at the update)
   double knb, rbreak;       // NRotBond: normal stiffness (unscaled), relative breaking distance (< 0: unbreakable)
-  double cohesion, tan_angle, t_cutoff, c_cutoff, beta1, beta2;  // BrittleBeamDZC failure criterion
+  double cohesion, tan_angle, t_cutoff, c_cutoff, beta1, beta2;  // BrittleBeamDZC / SC failure criteria
   double kr, ks, kt, kb, mn, ms, mt, mb, truncated;
   int scaling, meanR;
   const int* adj_start;
@@ -155,6 +156,7 @@ struct StepArgs {
   int* brk_step;
   int stop_skip;            // CTRL_* bits that do not stop the chunk (0: every raised bit stops it)
   int replay;               // recompute of steps already taken: bond failures are not logged again
+  double* sig;              // BrittleBeamSC present: each particle's stress sum of the last step (9 per slot)
   unsigned* pf_log;         // window recompute (else null): the PF_* bits each particle used in this step
   // adjoint recompute pass only (null otherwise): the pair + bond + wall + body force
   // sums before damping, and the damping iterations (lin, rot) of every particle

@@ -689,16 +689,60 @@ void launch_bond_pass_f64(const StepArgs& a, bool eval, cudaStream_t s) {
   else launch_bond_pass<false, false>(a, s);
 }
 
+// PIS_EB::update of BrittleBeamSC groups at the head of a step (BrittleBeamSCInteraction::broken,
+// Model/BrittleBeamSC.cpp:96-150): the positions the step starts from and the stress sums of the step
+// before.  A failure removes the bond before this step's forces and stops the chunk, so that the host's
+// update builds the new pairs first (as updateInteractions does after a bond update); the relaunched
+// step finds the bond gone.  Bonds of group d only; the event's step is the step that opens with it.
+__global__ void k_sc_check(const StepArgs a, int d, int nb) {
+  if (*a.stop) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nb) return;
+  const BondDev& B = a.bond[d];
+  const long long step = *a.step_counter + 1;
+  if (B.broken_step[k] <= step) return;
+  const ParticleBuf in = a.P.buf[a.cur];
+  const int2 e = B.ends[k];
+  const double4 pa = in.pr[e.x], pb = in.pr[e.y];
+  const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+  if (!sc_broken(x1, pa.w, a.sig + 9 * (size_t)e.x, x2, pb.w, a.sig + 9 * (size_t)e.y, B.cohesion, B.tan_angle,
+                 B.t_cutoff))
+    return;
+  B.broken_step[k] = (int)step;
+  a.P.flagged[e.x] = 1;
+  a.P.flagged[e.y] = 1;
+  if (!a.replay) {
+    const int slot = atomicAdd(B.nevents, 1);
+    if (slot < B.cap_events) {
+      B.events[3 * slot] = a.P.id[e.x];
+      B.events[3 * slot + 1] = a.P.id[e.y];
+      B.events[3 * slot + 2] = (int)step;
+    } else {
+      atomicOr(a.ctrl, CTRL_OVERFLOW);
+    }
+    atomicOr(a.ctrl, CTRL_BROKE);
+  }
+  if (a.handoff) a.brk_step[(step - 1) & 1] = (int)(step - 1);
+  else *a.stop = 1;
+}
+
 void launch_step(const StepArgs& a, bool rot, int tpp, bool split, cudaStream_t s) {
   bool el = false, fr = false, widened = false;
   for (int d = 0; d < a.ndyn; ++d) {
     if (a.dyn[d].kind >= 2) widened = true;  // NRotFriction, HertzMindlin
     (a.dyn[d].kind == 0 ? el : fr) = true;
   }
-  for (int d = 0; d < a.nbond; ++d) widened = widened || a.bond[d].kind == 1;
+  for (int d = 0; d < a.nbond; ++d) widened = widened || a.bond[d].kind == 1 || a.bond[d].kind == 3;
   const bool bd = a.nbond > 0;
   const bool gather = bd && a.bond[0].bf;  // bonds evaluated once by the bond pass
+  if (a.sig)
+    for (int d = 0; d < a.nbond; ++d)
+      if (a.bond[d].kind == 3 && a.bond[d].nb_launch > 0)
+        k_sc_check<<<(a.bond[d].nb_launch + kBondPassThreads - 1) / kBondPassThreads, kBondPassThreads, 0, s>>>(
+            a, d, a.bond[d].nb_launch);
   if (gather) launch_bond_pass<false, false>(a, s);
+  if (widened && a.sig && rot)  // BrittleBeamSC: the general instance with the stress sums
+    return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_NFRIC | F_BGATHER | F_STRESS, false, false>(a, tpp, s);
   if (widened) {  // NRotFriction / HertzMindlin / NRotBond groups: one general instance per particle type
     if (!rot) return launch_step_tpp<false, F_ELASTIC | F_NFRIC | F_BGATHER, false, false>(a, tpp, s);
     return launch_step_tpp<true, F_ELASTIC | F_FRIC | F_NFRIC | F_BGATHER, false, false>(a, tpp, s);

@@ -370,6 +370,46 @@ __device__ __forceinline__ bool dzc_broken(const BondOut& o, double dist0, doubl
   return (normalStress < -1. * t_cutoff) || (shearStress > c_cutoff) || (shearStress > (cohesion + normalStress * tan_angle));
 }
 
+// BrittleBeamSCInteraction::broken (Model/BrittleBeamSC.cpp:96-150): the bond axis n = (x2 - x1)/|x2 - x1|
+// with two transverse axes, the symmetric part of the two particles' mean stress (CParticle::sigma:
+// the stress sum over the particle's volume, Model/Particle.cpp:405-408) rotated into that frame, and a
+// truncated Mohr-Coulomb test on its normal and shear components.  S1, S2: the stress sums m_sigma.
+__device__ __forceinline__ bool sc_broken(const V& x1, double r1, const double* S1, const V& x2, double r2,
+                                          const double* S2, double cohesion, double tan_angle, double sigma3) {
+  const double pi = 3.14159265358979323846;  // M_PI
+  const V d = x2 - x1;
+  const V n = d / norm(d);
+  V sx;
+  if (n.x != 1.0 || n.y != 0.0 || n.z != 0.0) {
+    const V c = cross(n, mk(1.0, 0.0, 0.0));
+    sx = c / norm(c);
+  } else {
+    const V c = cross(n, mk(0.0, 1.0, 0.0));
+    sx = c / norm(c);
+  }
+  const V t = cross(n, sx);
+  const double dv1 = 1.0 / (4.0 / 3.0 * pi * r1 * r1 * r1), dv2 = 1.0 / (4.0 / 3.0 * pi * r2 * r2 * r2);
+  double avg[9], sym[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) avg[k] = 0.5 * (S1[k] * dv1 + S2[k] * dv2);
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) sym[3 * p + q] = 0.5 * (avg[3 * p + q] + avg[3 * q + p]);
+  const double nv[3] = {n.x, n.y, n.z}, sv[3] = {sx.x, sx.y, sx.z}, tv[3] = {t.x, t.y, t.z};
+  double sn = 0.0, tx = 0.0, ty = 0.0;  // rows n, s, t of the rotation: n.S.n, n.S.s, n.S.t
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      sn += nv[p] * sym[3 * p + q] * nv[q];
+      tx += nv[p] * sym[3 * p + q] * sv[q];
+      ty += nv[p] * sym[3 * p + q] * tv[q];
+    }
+  const double tau = sqrt(tx * tx + ty * ty);
+  return (sn < -1.0 * sigma3) || (tau > cohesion + sn * tan_angle);
+}
+
 // CElasticWallInteraction: ctor scaling (Model/EWallInteraction.hpp:26-36) and
 // calcForces (:42-78).  Returns true when in contact; F is the force on the particle.
 __device__ __forceinline__ bool law_wall(double k, const V& o, const V& n, const V& x, double r, V& F) {

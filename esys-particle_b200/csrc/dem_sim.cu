@@ -94,7 +94,7 @@ struct DynGroup {
 };
 
 struct BondGroup {
-  int kind = 0;                 // 0 RotBond, 1 NRotBond (CBondedInteraction), 2 BrittleBeamDZC
+  int kind = 0;                 // 0 RotBond, 1 NRotBond (CBondedInteraction), 2 BrittleBeamDZC, 3 BrittleBeamSC
   double knb = 0, rbreak = 0;   // NRotBond: normalK, relative breaking distance (< 0: unbreakable)
   double cohesion = 0, tan_angle = 0, t_cutoff = 0, c_cutoff = 0, beta1 = 0, beta2 = 0;  // BrittleBeamDZC
   int tag;
@@ -176,6 +176,7 @@ struct DemSim {
   std::map<std::string, int> bond_alive; // intact bonds per group at the last update
   DBuf<double> stage;                    // host-state staging (dem_set_particles)
   DBuf<double> scratch_d;                // field-saver values
+  DBuf<double> sig;                      // BrittleBeamSC: per-slot stress sums of the last step (9 each)
   DBuf<int> stage_slot;
 
   DemSim() {
@@ -202,7 +203,7 @@ struct DemSim {
     scratch_i.release(); scratch_j.release(); scalars.release(); scan_tmp.release();
     d_walls.release(); d_wall_vel.release(); d_wall_partial.release(); d_wall_force.release();
     d_block_counter.release(); d_step.release(); d_ctrl.release(); d_stop.release();
-    stage.release(); stage_slot.release(); scratch_d.release();
+    stage.release(); stage_slot.release(); scratch_d.release(); sig.release();
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -359,9 +360,11 @@ struct DemSim {
   void set_precision(int want) {
     want = want ? 1 : 0;
     if (want == fp32) return;
-    if (want)
+    if (want) {
       for (auto& d : dyn)
         if (d.second.kind >= 2) throw std::invalid_argument("NRotFriction and HertzMindlin groups run in the FP64 form only");
+      if (has_sc()) throw std::invalid_argument("BrittleBeamSC groups run in the FP64 form only");
+    }
     for (auto& d : dyn) {
       DynGroup& G = d.second;
       if (G.kind == 0 || G.m == 0) continue;
@@ -704,8 +707,25 @@ struct DemSim {
     return c;
   }
 
+  bool has_sc() const {
+    for (auto& b : bond) if (b.second.kind == 3) return true;
+    return false;
+  }
+  // The stress sums BrittleBeamSC groups read: zero until a step has written them (the particles'
+  // m_sigma starts at zero), kept when the particle storage grows.
+  double* ensure_sig() {
+    const size_t need = 9 * (size_t)std::max(n, 1);
+    if (sig.cap < need) {
+      const size_t old = sig.cap;
+      sig.reserve(need, true, s);
+      DEM_CUDA(cudaMemsetAsync(sig.p + old, 0, sizeof(double) * (sig.cap - old), s));
+    }
+    return sig.p;
+  }
+
   StepArgs make_args(int c) {
     StepArgs a{};
+    if (has_sc()) a.sig = ensure_sig();
     a.g = g;
     a.P = P;
     a.cur = c;
@@ -827,7 +847,11 @@ struct DemSim {
       std::memcpy(&dev_t, h_ctrl, sizeof(long long));
       const int ran = (int)(dev_t - t0);
       pending_ctrl = h_ctrl[2];
-      if (ran < 1 || ran > k) { err = "device step counter out of sequence"; return -3; }
+      // a BrittleBeamSC failure at the head of the chunk's first step stops it before any step
+      if (ran < 0 || ran > k || (ran == 0 && !(pending_ctrl & CTRL_BROKE))) {
+        err = "device step counter out of sequence";
+        return -3;
+      }
       t = dev_t;
       cur = (cur + ran) & 1;
       done += ran;
@@ -1367,7 +1391,7 @@ struct DemSim {
 
   void save_checkpoint(std::ostream& os) {
     for (auto& b : bond)
-      if (b.second.kind == 2) throw std::invalid_argument("restart checkpoints of BrittleBeamDZC groups are not built");
+      if (b.second.kind >= 2) throw std::invalid_argument("restart checkpoints of BrittleBeam groups are not built");
     download_walls();
     std::vector<double4> pr(n), vm(n), wi(n), qq(n), op(n), fo(n);
     std::vector<unsigned> pf(n);
@@ -1611,7 +1635,7 @@ struct DemSim {
   void load_checkpoint(std::istream& is, long long timestep) {
     if (n) throw StateError("a checkpoint is loaded into a worker without particles");
     for (auto& b : bond)
-      if (b.second.kind == 2) throw std::invalid_argument("restart checkpoints of BrittleBeamDZC groups are not built");
+      if (b.second.kind >= 2) throw std::invalid_argument("restart checkpoints of BrittleBeam groups are not built");
     auto fail = [&](const std::string& what) { throw std::invalid_argument("checkpoint: " + what); };
     double bp[3];
     int bi[3];
@@ -2527,6 +2551,25 @@ int dem_add_brittle_beam_dzc_group(dem_sim* h, const char* name, int tag, double
   });
 }
 
+// TRotSubLattice::addBrittleBeamSCIG (Parallel/RotSubLattice.hpp:188-225): BrittleBeamSCIGP from raw
+// stiffnesses (scaled as for BrittleBeamDZC); the failure test reads the particles' stress sums, which
+// the step then accumulates (BrittleBeamSCInteraction ctor and broken, Model/BrittleBeamSC.cpp).
+int dem_add_brittle_beam_sc_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                                  double cohesion, double tCutoff, double fAngle) {
+  return guard(h, [&](DemSim& s) {
+    if (!s.rot) throw std::invalid_argument("BrittleBeamSC needs RotSphere particles");
+    if (s.fp32) throw std::invalid_argument("BrittleBeamSC groups run in the FP64 form only");
+    add_bond_group(s, name, tag, [&](dem::BondGroup& B) {
+      B.kind = 3;
+      B.kr = kr; B.ks = ks; B.kt = kt; B.kb = kb;
+      B.mn = B.ms = B.mt = B.mb = 1.0;
+      B.scaling = 1; B.meanR = 1; B.truncated = 1.0;
+      B.cohesion = cohesion; B.tan_angle = std::tan(fAngle / 57.2957795); B.t_cutoff = tCutoff;
+    });
+    return DEM_OK;
+  });
+}
+
 // TSubLattice::addBondedIG (Parallel/SubLattice.hpp:1791-1831): CBondedIGP (tag, k, rbreak, scaling);
 // rbreak < 0 makes the group unbreakable.
 int dem_add_nrot_bond_group(dem_sim* h, const char* name, int tag, double k, double rbreak, int scaling) {
@@ -3056,8 +3099,8 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto b = s.bond.find(gname);
     if (b == s.bond.end()) throw std::invalid_argument("no such group " + gname);
     if (b->second.kind == 1) throw std::invalid_argument("interaction fields of NRotBond groups are not built");
-    if (b->second.kind == 2 && f == "breaking_criterion")
-      throw std::invalid_argument("BrittleBeamDZC groups have no breaking_criterion field");
+    if (b->second.kind >= 2 && f == "breaking_criterion")
+      throw std::invalid_argument("BrittleBeam groups have no breaking_criterion field");
     static const char* names[] = {"count", "potential_energy", "e_pot_normal", "e_pot_shear", "e_pot_twist",
                                   "e_pot_bend", "breaking_criterion"};
     int code = -1;

@@ -64,7 +64,19 @@ __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
 // F_BGATHER: bonds were evaluated by the bond pass (k_bond_pass, once per bond); the particle
 // gathers their forces and moments in its adjacency order instead of evaluating the law.
 // F_NFRIC: NRotFriction and HertzMindlin groups (FP64 only).
-enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8, F_NFRIC = 16 };
+// F_STRESS: each particle's stress sum (CParticle::m_sigma) is accumulated and stored in a.sig
+// (BrittleBeamSC groups read it in their failure test).
+enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8, F_NFRIC = 16, F_STRESS = 32 };
+
+// CParticle::applyForce's stress update (Model/Particle.cpp:392-401): m_sigma(i,j) -= f[i] * (pos - x)[j].
+__device__ __forceinline__ void stress_add(double* S, const V& f, const V& pos, const V& x) {
+  const V r = pos - x;
+  const double fv[3] = {f.x, f.y, f.z}, rv[3] = {r.x, r.y, r.z};
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) S[3 * p + q] -= fv[p] * rv[q];
+}
 
 // Sum of the pair-group and bond contributions on particle i (all TPP lanes of
 // the particle call this; on return every lane holds the combined sums).  The
@@ -73,7 +85,8 @@ enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8, F_NFRIC = 16 
 template <bool ROT, int TPP, int FEAT, bool FP32, bool EVAL>
 __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& in, int i, int lane, bool alive,
                                           long long step, const double4& p4, const double4& q4, V& Fp, V& Mp,
-                                          double* gross = nullptr) {
+                                          double* gross = nullptr, double* stress = nullptr) {
+  constexpr bool STRESS = !FP32 && (FEAT & F_STRESS) != 0;
   Fp = mk(0.0, 0.0, 0.0);
   Mp = mk(0.0, 0.0, 0.0);
   double Gs = 0.0;  // evaluation pass: sum of the contributions' magnitudes (the particle's force scale)
@@ -141,6 +154,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                 V f;
                 if (law_elastic(elastic_k(G.k, G.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, f)) {
                   if (isp1) Fp += -1.0 * f; else Fp += f;
+                  if constexpr (STRESS) {  // CElasticInteraction::calcForces: at x2 + r2 / (r1 + r2) D
+                    const V pos = x2 + (pb.w / eq_dist) * D;
+                    stress_add(stress, isp1 ? -1.0 * f : f, pos, isp1 ? x1 : x2);
+                  }
                 }
               } else {
                 Vf f;
@@ -169,6 +186,12 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
               } else {  // E in k, nu in ks; the normal force on p1 is +fn: negated for the common form
                 law_hertz_mindlin(G.k, G.ks, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
                 o.fn = -1.0 * o.fn;
+              }
+              if constexpr (STRESS) {
+                const V pos = x2 + (pb.w / eq_dist) * D;
+                const V xs = isp1 ? x1 : x2;
+                stress_add(stress, isp1 ? -1.0 * o.fn : o.fn, pos, xs);
+                stress_add(stress, isp1 ? o.Ffric : -1.0 * o.Ffric, pos, xs);
               }
               if (isp1) {  // p1: -force, then +Ffric; p2: +force, then -Ffric
                 Fp += -1.0 * o.fn;
@@ -201,6 +224,12 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                 FricOut o;
                 law_friction(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, xyz(va), xyz(wa), x2, pb.w, xyz(vb),
                              xyz(wb), mk(h.x, h.y, h.z), (((int)h.w) & 1) != 0, o);
+                if constexpr (STRESS) {  // CRotFrictionInteraction::calcSimpleForces: both forces at the contact
+                  const V pos = x2 + (pb.w / eq_dist) * D;
+                  const V xs = isp1 ? x1 : x2;
+                  stress_add(stress, isp1 ? -1.0 * o.fn : o.fn, pos, xs);
+                  stress_add(stress, isp1 ? o.Ffric : -1.0 * o.Ffric, pos, xs);
+                }
                 if (isp1) {
                   Fp += -1.0 * o.fn;
                   Mp += o.M1;
@@ -269,6 +298,15 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
             Fp += -1.0 * xyz(ldg4(r));
             if (ROT) Mp += xyz(ldg4(r + 2));
           }
+          if constexpr (STRESS) {  // bonds apply their force at x2 + r2 / (r1 + r2) (x1 - x2)
+            const double4 pj = ldg4(in.pr + en.x);
+            const bool isp1 = en.y < 0;
+            const double4 pa = isp1 ? p4 : pj, pb = isp1 ? pj : p4;
+            const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+            const V pos = x2 + (pb.w / (pa.w + pb.w)) * (x1 - x2);
+            const V f1 = xyz(ldg4(r));
+            stress_add(stress, isp1 ? f1 : -1.0 * f1, pos, isp1 ? x1 : x2);
+          }
           if (EVAL) Gs += norm(xyz(ldg4(r)));
         }
       }
@@ -299,9 +337,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           if (isp1) {
             Fp += o.force;
             Mp += o.moment1;
-            const bool brk = B.kind == 2 ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff,
-                                                      B.beta1, B.beta2)
-                                         : bond_broken(K, o, B.truncated);
+            const bool brk = B.kind == 2   ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff,
+                                                        B.beta1, B.beta2)
+                             : B.kind == 3 ? false
+                                           : bond_broken(K, o, B.truncated);
             if (!EVAL && brk) {
               B.broken_step[k] = (int)(step + 1);
               a.P.flagged[i] = 1;
@@ -338,6 +377,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
     Fp = lane_sum<TPP>(Fp);
     Mp = lane_sum<TPP>(Mp);
     if (EVAL) Gs = lane_sum<TPP>(Gs);
+    if constexpr (STRESS) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) stress[c] = lane_sum<TPP>(stress[c]);
+    }
   }
   if (FP32) {
     // FP64-form sums (bonds) are added after the compensated FP32 pair sums
@@ -595,8 +638,10 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
   r[0] = d4(o.force, 0.0);
   r[1] = d4(o.moment1, 0.0);
   r[2] = d4(o.moment2, 0.0);
-  const bool brk = B.kind == 2 ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff, B.beta1, B.beta2)
-                               : bond_broken(K, o, B.truncated);
+  // BrittleBeamSC: tested at the update that opens the step (k_sc_check), not on the forces
+  const bool brk = B.kind == 2   ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff, B.beta1, B.beta2)
+                   : B.kind == 3 ? false
+                                 : bond_broken(K, o, B.truncated);
   if (!EVAL && brk) {
     const int i = e.x, j = e.y;
     B.broken_step[k] = (int)(step + 1);
@@ -664,9 +709,30 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
     const bool alive = valid && (pf & PF_ALIVE);
     V Fp, Mp;
     double gross = 0.0;
-    pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp, &gross);
+    double Sg[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) Sg[c] = 0.0;
+    pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp, &gross, Sg);
     finish_particle<ROT, TPP, FP32, EVAL>(a, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
                                           ROT && (FEAT & F_BOND), Fp, Mp, s_red);
+    if constexpr (!FP32 && !EVAL && (FEAT & F_STRESS) != 0) {
+      if (alive && lane == 0) {
+        const V xi = xyz(p4);
+        for (int w = 0; w < a.nwall; ++w) {  // CElasticWallInteraction: at x - dist n
+          if (!(pf & (1u << (PF_WALL_SHIFT + w)))) continue;
+          const WallDev W = a.walls[w];
+          const V o = mk(W.ox, W.oy, W.oz), nrm = mk(W.nx, W.ny, W.nz);
+          V f;
+          if (law_wall(W.k, o, nrm, xi, p4.w, f)) {
+            const double dist = dot(xi - o, nrm);
+            stress_add(Sg, f, xi - dist * nrm, xi);
+          }
+        }
+        double* out_s = a.sig + 9 * (size_t)i;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) out_s[c] = Sg[c];
+      }
+    }
     // evaluation pass: the particle's contact-force scale beside its force (w of the record)
     if (EVAL && alive && lane == 0) reinterpret_cast<double*>(a.P.force_eval + i)[3] = gross;
   }

@@ -27,7 +27,7 @@ __all__ = [
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
     "ParticleVectorFieldSaverPrms", "TaggedParticleScalarFieldSaverPrms", "TaggedParticleVectorFieldSaverPrms",
     "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms", "LocalDampingPrms",
-    "RotLocalDampingPrms", "HertzMindlinPrms", "BrittleBeamDZCPrms",
+    "RotLocalDampingPrms", "HertzMindlinPrms", "BrittleBeamDZCPrms", "BrittleBeamSCPrms",
 ]
 
 
@@ -159,6 +159,19 @@ class BrittleBeamDZCPrms:  # InteractionParamsPy.cpp:711-727, 1733-1760 (Brittle
         self.cohesion, self.frictionAngle = float(cohesion), float(frictionAngle)
         self.tensileCutoff, self.compressCutoff = float(tensileCutoff), float(compressCutoff)
         self.beta1, self.beta2 = float(beta1), float(beta2)
+
+
+class BrittleBeamSCPrms:  # InteractionParamsPy.cpp:1689-1715 (BrittleBeamSCIGP)
+    """Stiffnesses from E and nu as for BrittleBeamDZCPrms."""
+
+    def __init__(self, name, youngsModulus, poissonsRatio, cohesion, frictionAngle, tensileCutoff, tag):
+        import math
+
+        self.name, self.tag = name, int(tag)
+        E, nu = float(youngsModulus), float(poissonsRatio)
+        G = E / (2.0 * (1. + nu))
+        self.kr, self.ks, self.kb, self.kt = math.pi * E, math.pi * G, math.pi * E, math.pi * G
+        self.cohesion, self.frictionAngle, self.tensileCutoff = float(cohesion), float(frictionAngle), float(tensileCutoff)
 
 
 class LocalDampingPrms:  # InteractionParamsPy.cpp:1033-1048 (CLocalDampingIGP "LocalDamping")
@@ -339,6 +352,9 @@ class LsmMpi:
             s.add_brittle_beam_dzc_group(prms.name, prms.tag, prms.kr, prms.ks, prms.kt, prms.kb, prms.cohesion,
                                          prms.tensileCutoff, prms.compressCutoff, prms.frictionAngle, prms.beta1,
                                          prms.beta2)
+        elif isinstance(prms, BrittleBeamSCPrms):  # LsmMpiPy::createBrittleBeamSCInteractGrp
+            s.add_brittle_beam_sc_group(prms.name, prms.tag, prms.kr, prms.ks, prms.kt, prms.kb, prms.cohesion,
+                                        prms.tensileCutoff, prms.frictionAngle)
         elif isinstance(prms, NRotBondPrms):
             s.add_nrot_bond_group(prms.name, prms.tag, prms.normalK, prms.breakDistance, prms.scaling)
         elif isinstance(prms, NRotElasticWallPrms):

@@ -96,6 +96,16 @@ int dem_add_brittle_beam_dzc_group(dem_sim* h, const char* name, int tag, double
                                    double cohesion, double tCutoff, double cCutoff, double fAngle, double beta1,
                                    double beta2);
 
+/* TRotSubLattice::addBrittleBeamSCIG (BrittleBeamSCPrms; Parallel/RotSubLattice.hpp:188-225):
+ * BrittleBeamSCInteraction (Model/BrittleBeamSC.cpp) with the master's packing order kr, ks, kt, kb,
+ * cohesion, tCutoff, fAngle (degrees).  RotBond forces and moments; the bond fails at the update that
+ * opens a step when the symmetric part of its two particles' mean stress (each particle's sum of
+ * -f (x) (contact point - centre) over the last step's forces, over its volume), in the frame of the bond
+ * axis, has a normal component below -tCutoff or a shear magnitude above cohesion + normal * tan(fAngle).
+ * RotSpheres; FP64 form; no restart checkpoint, differentiable window or batched ensemble. */
+int dem_add_brittle_beam_sc_group(dem_sim* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                                  double cohesion, double tCutoff, double fAngle);
+
 /* TSubLattice::addBondedIG (NRotBondPrms; Parallel/SubLattice.hpp:1791-1831): CBondedInteraction
  * (Model/BondedInteraction.cpp:43-140) between connections of `tag`; rest length r1 + r2, failure
  * when the extension exceeds (r1 + r2) * rbreak; rbreak < 0: unbreakable.  Forces only.  No

@@ -70,6 +70,7 @@ def _lib(backend: str):
         "add_local_damping": (C.c_int, [_P, _S, C.c_int, C.c_double]),
         "add_hertz_mindlin_group": (C.c_int, [_P, _S] + [C.c_double] * 4),
         "add_brittle_beam_dzc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 10),
+        "add_brittle_beam_sc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 7),
         "add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
         "save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
         "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
@@ -168,6 +169,13 @@ class OracleSim:
             raise NotImplementedError(f"{self.backend} has no BrittleBeamDZC groups")
         self._chk(self.f["add_brittle_beam_dzc_group"](self.h, name.encode(), int(tag), *(float(x) for x in (
             kr, ks, kt, kb, cohesion, tCutoff, cCutoff, fAngle, beta1, beta2))))
+
+    def add_brittle_beam_sc_group(self, name, tag, kr, ks, kt, kb, cohesion, tCutoff, fAngle):
+        """BrittleBeamSC (BrittleBeamSCInteraction) group (reference backend)."""
+        if "add_brittle_beam_sc_group" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no BrittleBeamSC groups")
+        self._chk(self.f["add_brittle_beam_sc_group"](self.h, name.encode(), int(tag), *(float(x) for x in (
+            kr, ks, kt, kb, cohesion, tCutoff, fAngle))))
 
     def add_local_damping(self, name, rot, visc):
         """LocalDamping / RotLocalDamping group (reference backend)."""

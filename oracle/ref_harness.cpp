@@ -46,6 +46,7 @@
 #include "Model/FrictionInteraction.h"
 #include "Model/HertzMindlinInteraction.h"
 #include "Model/BrittleBeamDZC.h"
+#include "Model/BrittleBeamSC.h"
 #include "Model/LocalDamping.h"
 #include "Model/LocalDampingIGP.h"
 #include "Model/RotLocalDamping.h"
@@ -108,6 +109,8 @@ struct ASim {
   virtual int add_hertz_mindlin(const char* name, double E, double nu, double mu, double dt) = 0;
   virtual int add_brittle_beam_dzc(const char* name, int tag, double kr, double ks, double kt, double kb, double coh,
                                    double tcut, double ccut, double fang, double b1, double b2) = 0;
+  virtual int add_brittle_beam_sc(const char* name, int tag, double kr, double ks, double kt, double kb, double coh,
+                                  double tcut, double fang) = 0;
   virtual int add_gravity(const char* name, const double* g) = 0;
   virtual int add_damping(int rot, double visc, int maxiter) = 0;
   virtual int add_local_damping(const char* name, int rot, double visc) = 0;
@@ -146,8 +149,9 @@ struct RefSim : public ASim {
   bool first = true;
   /* typed handles for queries */
   std::map<std::string, Exposed<ParallelInteractionStorage_NE<T, CElasticInteraction>>*> elastic;
-  std::map<std::string, void*> fric, bond, dzc;
+  std::map<std::string, void*> fric, bond, dzc, bsc;
   using DzcPis = Exposed<ParallelInteractionStorage_EB<CRotParticle, BrittleBeamDZCInteraction>>;
+  using ScPis = Exposed<ParallelInteractionStorage_EB<CRotParticle, BrittleBeamSCInteraction>>;
   std::map<std::string, Exposed<ParallelInteractionStorage_ED<T, CFrictionInteraction>>*> nfric;
   std::map<std::string, Exposed<ParallelInteractionStorage_EB<T, CBondedInteraction>>*> nbond;
   std::map<std::string, Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinInteraction>>*> hm;
@@ -205,6 +209,8 @@ struct RefSim : public ASim {
           collect_ids(nbond[b.first], s);
         } else if (dzc.count(b.first)) {
           collect_ids(static_cast<DzcPis*>(dzc[b.first]), s);
+        } else if (bsc.count(b.first)) {
+          collect_ids(static_cast<ScPis*>(bsc[b.first]), s);
         } else if constexpr (kRot) {
           collect_ids(static_cast<Exposed<ParallelInteractionStorage_EB<T, CRotBondedInteraction>>*>(bond[b.first]), s);
         }
@@ -398,6 +404,22 @@ struct RefSim : public ASim {
     err = "BrittleBeamDZC needs RotSphere particles";
     return -1;
   }
+  /* TRotSubLattice::addBrittleBeamSCIG (Parallel/RotSubLattice.hpp:188-225) */
+  int add_brittle_beam_sc(const char* name, int tag, double kr, double ks, double kt, double kb, double coh,
+                          double tcut, double fang) override {
+    if constexpr (kRot) {
+      BrittleBeamSCIGP p(name, kr, ks, kt, kb, coh, fang, tcut, tag);
+      auto* st = new ScPis(ppa, p);
+      std::vector<int>& conns = temp_conn[tag];
+      std::vector<int> vi(2, -1);
+      for (size_t i = 0; i + 1 < conns.size(); i += 2) { vi[0] = conns[i]; vi[1] = conns[i + 1]; st->tryInsert(vi); }
+      bpis[name] = st;
+      bsc[name] = st;
+      return 0;
+    }
+    err = "BrittleBeamSC needs RotSphere particles";
+    return -1;
+  }
   /* TSubLattice::addPairIG, type "Friction" (Parallel/SubLattice.hpp:1055-1076) */
   int add_nrot_friction(const char* name, double k, double mu, double ks, double dt_, int scaling) override {
     CFrictionIGP p(name, k, mu, ks, dt_, scaling != 0);
@@ -545,6 +567,7 @@ struct RefSim : public ASim {
     if (hm.count(group)) return (int)hm[group]->list().size();
     if (nbond.count(group)) return (int)nbond[group]->list().size();
     if (dzc.count(group)) return (int)static_cast<DzcPis*>(dzc[group])->list().size();
+    if (bsc.count(group)) return (int)static_cast<ScPis*>(bsc[group])->list().size();
     if constexpr (kRot) {
       if (fric.count(group))
         return (int)static_cast<Exposed<ParallelInteractionStorage_ED<T, CRotFrictionInteraction>>*>(fric[group])->list().size();
@@ -588,6 +611,15 @@ struct RefSim : public ASim {
     }
     if (dzc.count(group)) {  /* BrittleBeamDZC: force on p1 (3), 0, 0 */
       for (auto& in : static_cast<DzcPis*>(dzc[group])->list()) {
+        auto v = in.getAllID();
+        id1[i] = v[0]; id2[i] = v[1];
+        if (state) { Vec3 f = in.getForce(); for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k]; state[5 * i + 3] = 0; state[5 * i + 4] = 0; }
+        ++i;
+      }
+      return i;
+    }
+    if (bsc.count(group)) {  /* BrittleBeamSC: force on p1 (3), 0, 0 */
+      for (auto& in : static_cast<ScPis*>(bsc[group])->list()) {
         auto v = in.getAllID();
         id1[i] = v[0]; id2[i] = v[1];
         if (state) { Vec3 f = in.getForce(); for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k]; state[5 * i + 3] = 0; state[5 * i + 4] = 0; }
@@ -698,6 +730,10 @@ int ref_add_nrot_friction_group(void* h, const char* name, double k, double mu, 
 int ref_add_brittle_beam_dzc_group(void* h, const char* name, int tag, double kr, double ks, double kt, double kb,
                                    double coh, double tcut, double ccut, double fang, double b1, double b2) {
   return static_cast<ASim*>(h)->add_brittle_beam_dzc(name, tag, kr, ks, kt, kb, coh, tcut, ccut, fang, b1, b2);
+}
+int ref_add_brittle_beam_sc_group(void* h, const char* name, int tag, double kr, double ks, double kt, double kb,
+                                  double coh, double tcut, double fang) {
+  return static_cast<ASim*>(h)->add_brittle_beam_sc(name, tag, kr, ks, kt, kb, coh, tcut, fang);
 }
 int ref_add_nrot_bond_group(void* h, const char* name, int tag, double k, double rbreak, int scaling) {
   return static_cast<ASim*>(h)->add_nrot_bond(name, tag, k, rbreak, scaling);

@@ -208,6 +208,18 @@ def dzc_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, crit=(3.0, 5.0, 20.0, 30.
     return sim
 
 
+def sc_block(make, nx=5, ny=6, nz=5, seed=3, dt=1e-5, crit=(50.0, 50.0, 30.0), load_rate=0.02):
+    """bonded_block's specimen with BrittleBeamSC bonds (BrittleBeamSCInteraction: RotBond forces, a
+    truncated Mohr-Coulomb failure of the particles' mean stress across the bond) instead of RotBond.
+    crit = (cohesion, tCutoff, fAngle in degrees)."""
+    sim = bonded_block(make, nx, ny, nz, seed, dt, load_rate=load_rate, with_friction=False, bonds=False)
+    coh, tcut, fang = crit
+    sim.add_brittle_beam_sc_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, coh, tcut, fang)
+    sim.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, dt, True, True)
+    sim.add_exclusion("bonds", "friction")
+    return sim
+
+
 def bonded_block_script(make, nx=5, ny=6, nz=5, dt=1e-5, strength=(0.5, 1.0, 1.0, 0.5), with_friction=True):
     """The restart script of bonded_block: the same domain, groups, walls and damping, and no
     particles or connections (they come from the checkpoint, as with LsmMpi.loadCheckPoint)."""

@@ -173,3 +173,20 @@ def test_brittle_beam_dzc_failures_match_reference(gpu, ref):
         _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
     with pytest.raises(Exception):
         a.save_checkpoint("unused_t=1_1.txt", 12)  # restart records of these groups are not built
+
+
+def test_brittle_beam_sc_failures_match_reference(gpu, ref):
+    """BrittleBeamSC (BrittleBeamSCInteraction): RotBond forces; failure at the update from the
+    particles' stress sums (CParticle::applyForce's m_sigma) of the step before.  Failure events
+    exact, state within 1e-9 of the reference's own class."""
+    a, b = S.sc_block(gpu), S.sc_block(ref)
+    S.run_loaded(a, 400, 2e-4)
+    S.run_loaded(b, 400, 2e-4)
+    ea, eb = ({e for e in zip(*(x.tolist() for x in log))} for log in (a.breaks(), b.breaks()))
+    assert len(eb) > 10 and len({e[2] for e in eb}) > 8
+    assert ea == eb
+    assert _pairs(a, "bonds").keys() == _pairs(b, "bonds").keys()
+    assert _pairs(a, "friction").keys() == _pairs(b, "friction").keys()
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel", "angvel"):
+        _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)

@@ -164,7 +164,11 @@ def test_lsmmpi_widened_law_prms_match_direct_calls(oracle_libs):
         assert st[:, 4].sum() > 5, law  # contacts were touching
 
 
-def test_lsmmpi_brittle_beam_dzc_prms_match_direct_calls(oracle_libs):
+import pytest as _pytest
+
+
+@_pytest.mark.parametrize("law", ["dzc", "sc"])
+def test_lsmmpi_brittle_beam_prms_match_direct_calls(oracle_libs, law):
     """BrittleBeamDZCPrms(name, E, nu, cohesion, frictionAngle, tensileCutoff, compressCutoff, beta1,
     beta2, tag) reaches the group the raw-stiffness call makes (ARotBondedIGP's kr = kb = pi E,
     ks = kt = pi E / (2 (1 + nu))), and its bonds fail in the reference's own class."""
@@ -172,7 +176,7 @@ def test_lsmmpi_brittle_beam_dzc_prms_match_direct_calls(oracle_libs):
 
     import pytest
 
-    from esys.lsm import BrittleBeamDZCPrms, LsmMpi, RotSphere, NRotElasticWallPrms
+    from esys.lsm import BrittleBeamDZCPrms, BrittleBeamSCPrms, LsmMpi, NRotElasticWallPrms, RotSphere
     from esys.lsm.util import BoundingBox, Vec3
 
     if not oracle_libs.available("ref"):
@@ -198,7 +202,11 @@ def test_lsmmpi_brittle_beam_dzc_prms_match_direct_calls(oracle_libs):
         parts.append(q)
     sim.createParticles(parts)
     sim.createConnections([(1, i, j) for i, j in bonds])
-    sim.createInteractionGroup(BrittleBeamDZCPrms("bb", E, nu, tag=1, **crit))
+    if law == "dzc":
+        sim.createInteractionGroup(BrittleBeamDZCPrms("bb", E, nu, tag=1, **crit))
+    else:
+        sim.createInteractionGroup(BrittleBeamSCPrms("bb", E, nu, cohesion=20.0, frictionAngle=30.0,
+                                                     tensileCutoff=20.0, tag=1))
     sim.createWall("top", Vec3(0, 3.02, 0), Vec3(0, -1, 0))
     sim.createInteractionGroup(NRotElasticWallPrms("top_w", "top", 1e5))
     sim.run()
@@ -208,8 +216,11 @@ def test_lsmmpi_brittle_beam_dzc_prms_match_direct_calls(oracle_libs):
                     tag=[0] * 18, vel=vel)
     d.add_connections([1] * len(bonds), [i for i, _ in bonds], [j for _, j in bonds])
     G = E / (2.0 * (1. + nu))
-    d.add_brittle_beam_dzc_group("bb", 1, math.pi * E, math.pi * G, math.pi * G, math.pi * E, 2.0, 3.0, 10.0, 30.0,
-                                 1.0, 1.0)
+    if law == "dzc":
+        d.add_brittle_beam_dzc_group("bb", 1, math.pi * E, math.pi * G, math.pi * G, math.pi * E, 2.0, 3.0, 10.0,
+                                     30.0, 1.0, 1.0)
+    else:
+        d.add_brittle_beam_sc_group("bb", 1, math.pi * E, math.pi * G, math.pi * G, math.pi * E, 20.0, 20.0, 30.0)
     d.add_wall("top", (0, 3.02, 0), (0, -1, 0))
     d.add_wall_group("top_w", "top", 1e5)
     d.step(150)
