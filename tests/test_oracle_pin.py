@@ -37,7 +37,7 @@ def _same_state(a, b, groups):
 
 
 def test_kat_two_sphere_friction(oracle_libs):
-    """Two-sphere RotFriction known answer (values from the reference run)."""
+    """Two-sphere RotFriction known answer (values from a run of the reference's own classes)."""
     m = S.sphere_mass([0.5, 0.5])
     for backend in ("ref", "orc"):
         if backend == "ref" and not oracle_libs.available("ref"):
@@ -53,7 +53,7 @@ def test_kat_two_sphere_friction(oracle_libs):
 
 
 def test_kat_two_sphere_elastic(oracle_libs):
-    """Non-rotational spheres 0.9 apart with k=1000: F0 = (-25, 0, 0)."""
+    """Non-rotational spheres 0.9 apart with k=1000: F0 = (-25, 0, 0), the elastic law by hand."""
     m = S.sphere_mass([0.5, 0.5])
     s = oracle_libs.OracleSim("orc", "NRotSphere", 2.5, 0.2, (-5, -5, -5), (5, 5, 5), dt=1e-4)
     s.add_particles([0, 1], [[0, 0, 0], [0.9, 0, 0]], [0.5, 0.5], m)
@@ -65,7 +65,7 @@ def test_kat_two_sphere_elastic(oracle_libs):
 
 
 def test_kat_two_sphere_bond(oracle_libs):
-    """Bonded pair stretched by 0.001 in x after creation: F0 and M0z."""
+    """Bonded pair stretched by 0.001 in x after creation: F0 and M0z of the reference's own classes."""
     m = S.sphere_mass([0.5, 0.5])
     for backend in ("ref", "orc"):
         if backend == "ref" and not oracle_libs.available("ref"):
