@@ -864,9 +864,17 @@ __global__ void k_pair_field(Grid g, Particles P, int prev, const unsigned long 
     if (field == 0) r = touching ? 1.0 : 0.0;
     else if (field == 2) r = slipping ? 1.0 : 0.0;
     else if (field == 3) r = (touching && !slipping) ? 1.0 : 0.0;
-    else if (field == 1 && touching) {
+    else if (field == 1 && touching && kind == 3) {  // CHertzMindlinInteraction::getPotentialEnergy (:371-375)
+      const double R_ij = 1.0 / (1.0 / pa.w + 1.0 / pb.w);
+      const double dist = sqrt(d2);
+      const double dn = eq - dist;
+      const V fn = (D / norm(D)) * (4.0 / 3.0 * k * sqrt(R_ij) * pow(dn, 1.5));
+      r = dot(0.5 * fn, fn) / k;  // k holds E
+    } else if (field == 1 && touching) {
+      // CRotFrictionInteraction / CFrictionInteraction::getPotentialEnergy (FrictionInteraction.cpp:336-342)
       double ke, kse;
-      friction_k(k, ks, scaling, meanR, pa.w, pb.w, ke, kse);
+      if (kind == 2) nfriction_k(k, ks, scaling, pa.w, pb.w, ke, kse);
+      else friction_k(k, ks, scaling, meanR, pa.w, pb.w, ke, kse);
       const double dist = sqrt(d2);
       const V Fn = D * (ke * (dist - eq) / dist);
       const V Ff = mk((double)h.x, (double)h.y, (double)h.z);

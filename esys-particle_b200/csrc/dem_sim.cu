@@ -3063,7 +3063,6 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto d = s.dyn.find(gname);
     if (d != s.dyn.end()) {
       dem::DynGroup& G = d->second;
-      if (G.kind >= 2) throw std::invalid_argument("interaction fields of NRotFriction and HertzMindlin groups are not built");
       int code = f == "count" ? 0 : f == "potential_energy" ? 1 : -1;
       if (G.kind != 0 && f == "slipping") code = 2;
       if (G.kind != 0 && f == "sticking") code = 3;

@@ -273,7 +273,9 @@ int dem_particle_vector_field(dem_sim* h, const char* field, double* values);
  * "sticking" (Model/RotFricInteraction.cpp:384-452, 486-508); RotBond "count",
  * "potential_energy", "e_pot_normal", "e_pot_shear", "e_pot_twist", "e_pot_bend",
  * "breaking_criterion" (Model/ARotBondedInteraction.cpp:456-485, RotBondedInteraction.cpp:
- * 221-256).  values[] in dem_get_pairs order; returns the count.  NRotElastic's
+ * 221-256); NRotFriction and HertzMindlin "count", "potential_energy", "slipping", "sticking"
+ * (Model/FrictionInteraction.cpp:336-400, HertzMindlinInteraction.cpp:371-400).  BrittleBeam groups
+ * as RotBond without "breaking_criterion".  values[] in dem_get_pairs order; returns the count.  NRotElastic's
  * potential_energy is 0 for a pair not touching at that evaluation (the reference keeps the
  * last contact force of such a pair until the next rebuild). */
 int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* field, double* values);

@@ -176,3 +176,42 @@ def test_displacement_follows_circular_shifts_and_checkpoints(gpu, tmp_path):
     _, d4 = s2.particle_vector_field("displacement")
     assert np.abs(d3 - d4).max() < 1e-12
     assert np.abs(d3 - s._v[ids] * 0.4).max() < 1e-9
+
+
+@pytest.mark.parametrize("law", ["nfric", "hm"])
+def test_nrot_friction_and_hertz_mindlin_fields(gpu, law):
+    """count / slipping / sticking from the flags the step wrote, and potential_energy from the positions
+    the force evaluation read: CFrictionInteraction 0.5 Fn.Fn / k + 0.5 Ff.Ff / ks (scaled k, ks), and
+    CHertzMindlinInteraction 0.5 Fn.Fn / E."""
+    sim = gpu("NRotSphere", 1.2, 0.2, (0, 0, 0), (6, 6, 6), (0, 0, 0), 1e-4)
+    pos = np.array([[2.0, 2.0, 2.0], [2.85, 2.1, 2.0], [4.5, 4.5, 4.5]])
+    rad = np.array([0.5, 0.45, 0.4])
+    sim.add_particles(np.arange(3), pos, rad, np.ones(3), tag=np.zeros(3, np.int32),
+                      vel=[[0.0, 0.3, 0.0], [0.0, -0.3, 0.1], [0.0, 0.0, 0.0]])
+    if law == "nfric":
+        sim.add_nrot_friction_group("c", 1e4, 0.5, 5e3, 1e-4, True)
+    else:
+        sim.add_hertz_mindlin_group("c", 1e4, 0.3, 0.5, 1e-4)
+    sim.step(1)
+    pa, pb, pst = sim.pairs("c")
+    by_key = {(int(x), int(y)): r for x, y, r in zip(pa, pb, pst)}
+    a, b, _ = sim.interaction_scalar_field("c", "count")
+    st = np.array([by_key[(int(x), int(y))] for x, y in zip(a, b)])
+    fields = {f: sim.interaction_scalar_field("c", f)[2] for f in ("count", "potential_energy", "slipping", "sticking")}
+    assert np.array_equal(fields["count"], st[:, 4]) and np.array_equal(fields["slipping"], st[:, 3])
+    assert np.array_equal(fields["sticking"], st[:, 4] * (1 - st[:, 3]))
+    q = [i for i in range(len(a)) if {int(a[i]), int(b[i])} == {0, 1}][0]
+    D = pos[0] - pos[1]
+    dist, eq = np.linalg.norm(D), rad[0] + rad[1]
+    if law == "nfric":
+        f = 0.5 * (rad[0] + rad[1])
+        ke, kse = f * 1e4, f * 5e3
+        Fn = D * (ke * (dist - eq) / dist)
+        Ff = st[q, :3]
+        want = (0.5 * Fn) @ Fn / ke + (0.5 * Ff) @ Ff / kse
+    else:
+        R = 1.0 / (1.0 / rad[0] + 1.0 / rad[1])
+        fn = D / np.linalg.norm(D) * (4.0 / 3.0 * 1e4 * np.sqrt(R) * (eq - dist) ** 1.5)
+        want = (0.5 * fn) @ fn / 1e4
+    assert fields["count"][q] == 1.0
+    assert abs(fields["potential_energy"][q] - want) <= 1e-12 * abs(want)
