@@ -487,6 +487,54 @@ __device__ __forceinline__ void law_hertz_mindlin(double E, double nu, double mu
   }
 }
 
+// CHertzMindlinViscoInteraction::calcForces (Model/HertzMindlinViscoInteraction.cpp:119-200): the Hertz
+// normal force less a normal damping term, and a tangential force recomputed every step (no history)
+// less a tangential damping term, both from the coefficient of restitution (Antypov 2011, as the
+// reference writes it, with its 3.1415926).  fn here is the net normal force on p1 (p2 gets -fn),
+// Ffric the tangential force on p1 (p2 gets -Ffric).
+__device__ __forceinline__ void law_hertz_mindlin_visco(double E, double nu, double mu, double COR, double dt,
+                                                        const V& x1, double r1, double m1, const V& v1, const V& x2,
+                                                        double r2, double m2, const V& v2, FricOut& o) {
+  const V D = x1 - x2;
+  double dist = dot(D, D);
+  const double eq_dist = r1 + r2;
+  o.M1 = o.M2 = mk(0.0, 0.0, 0.0);
+  if (!(dist < (eq_dist * eq_dist))) {
+    o.Ffric = o.fn = mk(0.0, 0.0, 0.0);
+    o.slipping = false;
+    o.touching = false;
+    return;
+  }
+  const double R_ij = 1.0 / (1.0 / r1 + 1.0 / r2);
+  dist = sqrt(dist);
+  const double dn = eq_dist - dist;
+  const V dir = D / norm(D);
+  const double norm_fn = 4.0 / 3.0 * E * sqrt(R_ij) * pow(dn, 1.5);
+  const V fn = dir * norm_fn;
+  const double M_ij = 1.0 / (1.0 / m1 + 1.0 / m2);
+  const V v_rel = v2 - v1;
+  const V v_nor = dot(v_rel, dir) * dir;
+  const double lnCOR = log(COR);
+  const V normal_damping = 2.0 * sqrt(5.0 / 3.0) * lnCOR / sqrt(pow(lnCOR, 2) + pow(3.1415926, 2)) * sqrt(M_ij * E) *
+                           pow(R_ij, 0.25) * pow(dn, 0.25) * v_nor;
+  const V d1 = v1 * dt;
+  const V d2 = v2 * dt;
+  V ds = d2 - d1;
+  ds -= dot(ds, dir) * dir;
+  V Ffric = 2.0 / 3.0 * 8.0 * E / 2.0 / (1.0 + nu) * sqrt(R_ij) * sqrt(dn) * ds;
+  const V v_tan = v_rel - v_nor;
+  const V tange_damping = sqrt(80.0 / 3.0) * lnCOR / sqrt(pow(lnCOR, 2) + pow(3.1415926, 2)) *
+                          sqrt(M_ij * E / 2.0 / (1.0 + nu)) * pow(R_ij, 0.25) * pow(dn, 0.25) * v_tan;
+  Ffric -= tange_damping;
+  const double FfricNorm = norm(Ffric);
+  const double forceNorm = norm(fn);
+  o.slipping = FfricNorm > forceNorm * mu;
+  if (o.slipping) Ffric = Ffric * ((mu * forceNorm) / FfricNorm);
+  o.fn = fn - normal_damping;
+  o.Ffric = Ffric;
+  o.touching = true;
+}
+
 // CLocalDamping::calcForces (Model/LocalDamping.hpp:82-118) and CRotLocalDamping::calcForces
 // (Model/RotLocalDamping.hpp:82-117): each component of the accumulated force (moment) with the
 // sign of the velocity (spin) component, zero where that component is zero, times -visc.

@@ -670,7 +670,7 @@ struct DemSim {
     if (on == (handoff != 0)) return;
     if (on)
       for (auto& d : dyn)
-        if (d.second.kind == 0 || d.second.kind == 3)
+        if (d.second.kind == 0 || d.second.kind >= 3)
           throw std::invalid_argument("the device bond hand-off needs every dynamic group to be RotFriction or NRotFriction");
     handoff = on;
     if (!d_brk.p) {
@@ -688,7 +688,7 @@ struct DemSim {
   // History handling of a dynamic group's list at a rebuild: 0 none (NRotElastic), 1 carried for
   // persistent pairs (PIS_ED groups: RotFriction, NRotFriction), 2 reset (HertzMindlin, whose
   // history lives in a PIS_NE storage that rebuilds its list from scratch).
-  static int hist_mode(const DynGroup& G) { return G.kind == 0 ? 0 : (G.kind == 3 ? 2 : 1); }
+  static int hist_mode(const DynGroup& G) { return G.kind == 0 ? 0 : (G.kind >= 3 ? 2 : 1); }
 
   bool widened() const {
     for (auto& d : dyn) if (d.second.kind >= 2) return true;
@@ -1494,7 +1494,7 @@ struct DemSim {
     os << nsave << "\n";
     for (auto& it : dyn) {
       DynGroup& G = it.second;
-      if (G.kind == 0 || G.kind == 3) continue;  // PIS_NE storages do not save
+      if (G.kind == 0 || G.kind >= 3) continue;  // PIS_NE storages do not save
       std::vector<unsigned long long> keys(G.m);
       std::vector<double4> h(G.m);
       std::vector<int> xb(handoff ? G.m : 0);
@@ -1745,7 +1745,7 @@ struct DemSim {
     if (!is || nsave != want) fail("the number of friction groups differs from the script's");
     for (auto& it : dyn) {
       DynGroup& G = it.second;
-      if (G.kind == 0 || G.kind == 3) continue;
+      if (G.kind == 0 || G.kind >= 3) continue;
       std::string type;
       is >> type;
       const std::string want_type = G.kind == 1 ? "RotFriction" : "Friction";
@@ -2530,6 +2530,21 @@ int dem_add_rot_bond_group(dem_sim* h, const char* name, int tag, double kr, dou
   });
 }
 
+// TSubLattice::addPairIG, type "HertzMindlinVisco" (Parallel/SubLattice.hpp:1340-1356): CHertzMindlinViscoIGP
+// packing order E, nu, mu, COR, dt; PIS_NE storage like HertzMindlin.
+int dem_add_hertz_mindlin_visco_group(dem_sim* h, const char* name, double E, double nu, double mu, double COR,
+                                      double dt) {
+  return guard(h, [&](DemSim& s) {
+    if ((int)s.dyn.size() >= dem::kMaxDyn && !s.dyn.count(name)) throw std::invalid_argument("too many dynamic groups");
+    if (s.fp32) throw std::invalid_argument("HertzMindlinVisco groups run in the FP64 form only");
+    if (s.handoff) throw std::invalid_argument("the device bond hand-off needs RotFriction or NRotFriction groups");
+    dem::DynGroup& G = s.dyn[name];
+    G.kind = 4; G.k = E; G.ks = nu; G.mu_s = mu; G.mu_d = COR; G.dt = dt; G.scaling = 0; G.meanR = 0;
+    s.resize_adjacency();
+    return DEM_OK;
+  });
+}
+
 // TRotSubLattice::addBrittleBeamDZCIG (Parallel/RotSubLattice.hpp:227-267): BrittleBeamDZCIGP from raw
 // stiffnesses, which ARotBondedIGP scales with the bond's half length (scaling on); the failure
 // criterion's friction angle is in degrees, its tangent taken as the interaction's constructor does
@@ -3063,7 +3078,7 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto d = s.dyn.find(gname);
     if (d != s.dyn.end()) {
       dem::DynGroup& G = d->second;
-      int code = f == "count" ? 0 : f == "potential_energy" ? 1 : -1;
+      int code = f == "count" ? 0 : (f == "potential_energy" && G.kind != 4) ? 1 : -1;
       if (G.kind != 0 && f == "slipping") code = 2;
       if (G.kind != 0 && f == "sticking") code = 3;
       if (code < 0) throw std::invalid_argument("unknown interaction scalar field " + f + " of group " + gname);

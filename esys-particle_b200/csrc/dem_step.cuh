@@ -183,8 +183,12 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                 double keff, kseff;
                 nfriction_k(G.k, G.ks, G.scaling, pa.w, pb.w, keff, kseff);
                 law_nfriction(keff, kseff, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
-              } else {  // E in k, nu in ks; the normal force on p1 is +fn: negated for the common form
+              } else if (G.kind == 3) {  // E in k, nu in ks; the normal force on p1 is +fn: negated for the common form
                 law_hertz_mindlin(G.k, G.ks, G.mu_s, G.dt, x1, pa.w, xyz(va), x2, pb.w, xyz(vb), mk(h.x, h.y, h.z), o);
+                o.fn = -1.0 * o.fn;
+              } else {  // HertzMindlinVisco: E, nu, mu, restitution in k, ks, mu_s, mu_d; masses in the w's
+                law_hertz_mindlin_visco(G.k, G.ks, G.mu_s, G.mu_d, G.dt, x1, pa.w, va.w, xyz(va), x2, pb.w, vb.w, xyz(vb),
+                                        o);
                 o.fn = -1.0 * o.fn;
               }
               if constexpr (STRESS) {

@@ -27,7 +27,7 @@ __all__ = [
     "ConnectionFinder", "ParticleScalarFieldSaverPrms", "InteractionScalarFieldSaverPrms", "WallVectorFieldSaverPrms",
     "ParticleVectorFieldSaverPrms", "TaggedParticleScalarFieldSaverPrms", "TaggedParticleVectorFieldSaverPrms",
     "CheckPointPrms", "RestartCheckPointPrms", "NRotFrictionPrms", "NRotBondPrms", "LocalDampingPrms",
-    "RotLocalDampingPrms", "HertzMindlinPrms", "BrittleBeamDZCPrms", "BrittleBeamSCPrms",
+    "RotLocalDampingPrms", "HertzMindlinPrms", "BrittleBeamDZCPrms", "BrittleBeamSCPrms", "HertzMindlinViscoPrms",
 ]
 
 
@@ -172,6 +172,12 @@ class BrittleBeamSCPrms:  # InteractionParamsPy.cpp:1689-1715 (BrittleBeamSCIGP)
         G = E / (2.0 * (1. + nu))
         self.kr, self.ks, self.kb, self.kt = math.pi * E, math.pi * G, math.pi * E, math.pi * G
         self.cohesion, self.frictionAngle, self.tensileCutoff = float(cohesion), float(frictionAngle), float(tensileCutoff)
+
+
+class HertzMindlinViscoPrms:  # InteractionParamsPy.cpp:1390-1420 (CHertzMindlinViscoIGP)
+    def __init__(self, name, youngsModulus, poissonsRatio, dynamicMu, restitution):
+        self.name, self.youngsModulus, self.poissonsRatio = name, float(youngsModulus), float(poissonsRatio)
+        self.dynamicMu, self.restitution = float(dynamicMu), float(restitution)
 
 
 class LocalDampingPrms:  # InteractionParamsPy.cpp:1033-1048 (CLocalDampingIGP "LocalDamping")
@@ -355,6 +361,9 @@ class LsmMpi:
         elif isinstance(prms, BrittleBeamSCPrms):  # LsmMpiPy::createBrittleBeamSCInteractGrp
             s.add_brittle_beam_sc_group(prms.name, prms.tag, prms.kr, prms.ks, prms.kt, prms.kb, prms.cohesion,
                                         prms.tensileCutoff, prms.frictionAngle)
+        elif isinstance(prms, HertzMindlinViscoPrms):  # LsmMpiPy::createHertzMindlinViscoIG sets dt
+            s.add_hertz_mindlin_visco_group(prms.name, prms.youngsModulus, prms.poissonsRatio, prms.dynamicMu,
+                                            prms.restitution, self._dt)
         elif isinstance(prms, NRotBondPrms):
             s.add_nrot_bond_group(prms.name, prms.tag, prms.normalK, prms.breakDistance, prms.scaling)
         elif isinstance(prms, NRotElasticWallPrms):

@@ -34,6 +34,7 @@ SIGNATURES = {
     "dem_add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
     "dem_add_local_damping": (C.c_int, [_P, _S, C.c_int, C.c_double]),
     "dem_add_hertz_mindlin_group": (C.c_int, [_P, _S] + [C.c_double] * 4),
+    "dem_add_hertz_mindlin_visco_group": (C.c_int, [_P, _S] + [C.c_double] * 5),
     "dem_add_brittle_beam_dzc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 10),
     "dem_add_brittle_beam_sc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 7),
     "dem_add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
@@ -192,6 +193,10 @@ class DemSim:
     def add_brittle_beam_sc_group(self, name, tag, kr, ks, kt, kb, cohesion, tCutoff, fAngle):
         self._chk(self.lib.dem_add_brittle_beam_sc_group(self.h, name.encode(), int(tag), *(float(x) for x in (
             kr, ks, kt, kb, cohesion, tCutoff, fAngle))))
+
+    def add_hertz_mindlin_visco_group(self, name, E, nu, mu, COR, dt):
+        self._chk(self.lib.dem_add_hertz_mindlin_visco_group(self.h, name.encode(), float(E), float(nu), float(mu),
+                                                             float(COR), float(dt)))
 
     def add_local_damping(self, name, rot, visc):
         self._chk(self.lib.dem_add_local_damping(self.h, name.encode(), int(rot), float(visc)))

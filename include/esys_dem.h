@@ -85,6 +85,14 @@ int dem_add_nrot_friction_group(dem_sim* h, const char* name, double k, double m
  * FP64 form; no device bond hand-off, differentiable window or batched ensemble. */
 int dem_add_hertz_mindlin_group(dem_sim* h, const char* name, double E, double nu, double mu, double dt);
 
+/* TSubLattice::addPairIG, type "HertzMindlinVisco" (HertzMindlinViscoPrms; Parallel/SubLattice.hpp:
+ * 1340-1356): CHertzMindlinViscoInteraction (Model/HertzMindlinViscoInteraction.cpp:119-200), packing
+ * order E, nu, mu, COR (restitution), dt: HertzMindlin with normal and tangential damping from the
+ * restitution coefficient and a tangential force without history.  PIS_NE; FP64 form; fields "count",
+ * "slipping", "sticking". */
+int dem_add_hertz_mindlin_visco_group(dem_sim* h, const char* name, double E, double nu, double mu, double COR,
+                                      double dt);
+
 /* TRotSubLattice::addBrittleBeamDZCIG (BrittleBeamDZCPrms; Parallel/RotSubLattice.hpp:227-267):
  * BrittleBeamDZCInteraction (Model/BrittleBeamDZC.cpp) between the tagged connections, with the
  * master's packing order kr, ks, kt, kb, cohesion, tCutoff, cCutoff, fAngle (degrees), beta1,

@@ -69,6 +69,7 @@ def _lib(backend: str):
         "add_nrot_friction_group": (C.c_int, [_P, _S] + [C.c_double] * 4 + [C.c_int]),
         "add_local_damping": (C.c_int, [_P, _S, C.c_int, C.c_double]),
         "add_hertz_mindlin_group": (C.c_int, [_P, _S] + [C.c_double] * 4),
+        "add_hertz_mindlin_visco_group": (C.c_int, [_P, _S] + [C.c_double] * 5),
         "add_brittle_beam_dzc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 10),
         "add_brittle_beam_sc_group": (C.c_int, [_P, _S, C.c_int] + [C.c_double] * 7),
         "add_nrot_bond_group": (C.c_int, [_P, _S, C.c_int, C.c_double, C.c_double, C.c_int]),
@@ -176,6 +177,12 @@ class OracleSim:
             raise NotImplementedError(f"{self.backend} has no BrittleBeamSC groups")
         self._chk(self.f["add_brittle_beam_sc_group"](self.h, name.encode(), int(tag), *(float(x) for x in (
             kr, ks, kt, kb, cohesion, tCutoff, fAngle))))
+
+    def add_hertz_mindlin_visco_group(self, name, E, nu, mu, COR, dt):
+        """HertzMindlinVisco (CHertzMindlinViscoInteraction) group (reference backend)."""
+        if "add_hertz_mindlin_visco_group" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no HertzMindlinVisco groups")
+        self._chk(self.f["add_hertz_mindlin_visco_group"](self.h, name.encode(), E, nu, mu, COR, dt))
 
     def add_local_damping(self, name, rot, visc):
         """LocalDamping / RotLocalDamping group (reference backend)."""

@@ -45,6 +45,7 @@
 #include "Model/ElasticInteraction.h"
 #include "Model/FrictionInteraction.h"
 #include "Model/HertzMindlinInteraction.h"
+#include "Model/HertzMindlinViscoInteraction.h"
 #include "Model/BrittleBeamDZC.h"
 #include "Model/BrittleBeamSC.h"
 #include "Model/LocalDamping.h"
@@ -107,6 +108,7 @@ struct ASim {
   virtual int add_nrot_friction(const char* name, double k, double mu, double ks, double dt, int scaling) = 0;
   virtual int add_nrot_bond(const char* name, int tag, double k, double rbreak, int scaling) = 0;
   virtual int add_hertz_mindlin(const char* name, double E, double nu, double mu, double dt) = 0;
+  virtual int add_hertz_mindlin_visco(const char* name, double E, double nu, double mu, double cor, double dt) = 0;
   virtual int add_brittle_beam_dzc(const char* name, int tag, double kr, double ks, double kt, double kb, double coh,
                                    double tcut, double ccut, double fang, double b1, double b2) = 0;
   virtual int add_brittle_beam_sc(const char* name, int tag, double kr, double ks, double kt, double kb, double coh,
@@ -403,6 +405,13 @@ struct RefSim : public ASim {
     }
     err = "BrittleBeamDZC needs RotSphere particles";
     return -1;
+  }
+  /* TSubLattice::addPairIG, type "HertzMindlinVisco" (Parallel/SubLattice.hpp:1340-1356) */
+  int add_hertz_mindlin_visco(const char* name, double E, double nu, double mu, double cor, double dt_) override {
+    CHertzMindlinViscoIGP p(name, E, nu, mu, cor, dt_);
+    auto* st = new Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinViscoInteraction>>(ppa, p);
+    dpis[name] = st;
+    return 0;
   }
   /* TRotSubLattice::addBrittleBeamSCIG (Parallel/RotSubLattice.hpp:188-225) */
   int add_brittle_beam_sc(const char* name, int tag, double kr, double ks, double kt, double kb, double coh,
@@ -734,6 +743,10 @@ int ref_add_brittle_beam_dzc_group(void* h, const char* name, int tag, double kr
 int ref_add_brittle_beam_sc_group(void* h, const char* name, int tag, double kr, double ks, double kt, double kb,
                                   double coh, double tcut, double fang) {
   return static_cast<ASim*>(h)->add_brittle_beam_sc(name, tag, kr, ks, kt, kb, coh, tcut, fang);
+}
+int ref_add_hertz_mindlin_visco_group(void* h, const char* name, double E, double nu, double mu, double cor,
+                                      double dt) {
+  return static_cast<ASim*>(h)->add_hertz_mindlin_visco(name, E, nu, mu, cor, dt);
 }
 int ref_add_nrot_bond_group(void* h, const char* name, int tag, double k, double rbreak, int scaling) {
   return static_cast<ASim*>(h)->add_nrot_bond(name, tag, k, rbreak, scaling);

@@ -66,7 +66,7 @@ def nrot_friction_pack(make, rot=False, n_side=5, seed=8, dt=1e-4, vscale=0.5):
     return sim
 
 
-def hertz_mindlin_pack(make, rot=False, n_side=5, seed=10, dt=1e-4, vscale=1.0, skin=0.05):
+def hertz_mindlin_pack(make, rot=False, n_side=5, seed=10, dt=1e-4, vscale=1.0, skin=0.05, restitution=None):
     """nrot_friction_pack's lattice with a HertzMindlin group (CHertzMindlinInteraction,
     E = 1e4, nu = 0.3, mu = 0.5) and a small Verlet skin, so that neighbour rebuilds (which
     restart the law's tangential history, its storage being PIS_NE) fall inside a short run."""
@@ -79,7 +79,10 @@ def hertz_mindlin_pack(make, rot=False, n_side=5, seed=10, dt=1e-4, vscale=1.0, 
     sim = make("RotSphere" if rot else "NRotSphere", 1.2, skin, (0, 0, 0), (L, L, 2 * L), (0, 0, 0), dt)
     vel = rng.normal(0, vscale, size=(n, 3))
     sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=vel)
-    sim.add_hertz_mindlin_group("hm", 1e4, 0.3, 0.5, dt)
+    if restitution is None:
+        sim.add_hertz_mindlin_group("hm", 1e4, 0.3, 0.5, dt)
+    else:  # HertzMindlinVisco (CHertzMindlinViscoInteraction) with this restitution coefficient
+        sim.add_hertz_mindlin_visco_group("hm", 1e4, 0.3, 0.5, restitution, dt)
     sim.add_gravity("gravity", (0, 0, -9.81))
     sim.add_damping(0, 0.01, 100)
     for name, o, nrm in (("xlo", (0, 0, 0), (1, 0, 0)), ("xhi", (L, 0, 0), (-1, 0, 0)),

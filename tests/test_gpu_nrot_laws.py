@@ -190,3 +190,19 @@ def test_brittle_beam_sc_failures_match_reference(gpu, ref):
     pa, pb = a.particles(), b.particles()
     for k in ("pos", "vel", "angvel"):
         _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
+
+
+@pytest.mark.parametrize("rot", [False, True])
+def test_hertz_mindlin_visco_matches_reference(gpu, ref, rot):
+    """HertzMindlinVisco (CHertzMindlinViscoInteraction): damped Hertz-Mindlin contacts through several
+    neighbour rebuilds, state within 1e-9 of the reference's own class."""
+    a, b = S.hertz_mindlin_pack(gpu, rot=rot, restitution=0.6), S.hertz_mindlin_pack(ref, rot=rot, restitution=0.6)
+    c0 = a.counters()["rebuilds"]
+    a.step(300)
+    b.step(300)
+    assert a.counters()["rebuilds"] - c0 >= 2
+    pa, pb = a.particles(), b.particles()
+    for k in ("pos", "vel"):
+        _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
+    c = a.interaction_scalar_field("hm", "count")[2]
+    assert c.sum() > 20
