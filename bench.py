@@ -520,7 +520,7 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
     t_setup = time.perf_counter() - t0
     make = lambda *a: _capi.DemSim(*a)
     best, table = autotune_ensemble(lambda sp, g, sk: cylinder_sim(make, sp, g, sk), specs, 1.0,
-                                    skins=(0.1, 0.2, 0.35), cell_factors=(1.0,), tpps=(2, 4, 8), sample=24,
+                                    skins=(0.1, 0.2, 0.35), cell_factors=(1.0,), tpps=(2, 4, 8, 16), sample=24,
                                     warmup=30, trial=80)
     sims = [cylinder_sim(make, sp, best["grid_spacing"], best["verlet_dist"]) for sp in specs]
     for s in sims:

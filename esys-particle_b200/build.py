@@ -19,7 +19,7 @@ SOURCES = [("dem_kernels.cu", False), ("dem_sim.cu", False), ("dem_noalloc.cu", 
            ("dem_adjoint.cu", False), ("dem_batch.cu", False), ("dem_batch_fp32.cu", True),
            ("packing.cpp", False)]
 HEADERS = ["dem_device.cuh", "dem_kernels.h", "dem_laws.cuh", "dem_laws_f32.cuh", "dem_math.cuh", "dem_common.cuh",
-           "dem_step.cuh", "dem_adjoint.h", "dem_dual.cuh", "dem_batch.cuh", "dem_bond_vjp.cuh", "dem_pair_vjp.cuh"]
+           "dem_step.cuh", "dem_tiled.cuh", "dem_adjoint.h", "dem_dual.cuh", "dem_batch.cuh", "dem_bond_vjp.cuh", "dem_pair_vjp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -16,6 +16,7 @@
 #pragma once
 #include "dem_kernels.h"
 #include "dem_step.cuh"
+#include "dem_tiled.cuh"
 
 namespace dem {
 
@@ -33,53 +34,8 @@ __device__ __forceinline__ int batch_specimen(const BatchArgs& B, int tile) {
 __device__ __forceinline__ void batch_tile_epilogue(const StepArgs& a, long long step, int ltile, int ntiles,
                                                     int wlane, int warp, double (*s_red)[kMaxWalls][3],
                                                     bool* s_last) {
-  const int nw3 = a.nwall * 3;
-  __syncthreads();
-  if (threadIdx.x < nw3) {
-    const int w = threadIdx.x / 3, c = threadIdx.x % 3;
-    double acc = 0.0;
-    for (int k = 0; k < kStepWarps; ++k) acc += s_red[k][w][c];
-    a.wall_partial[((size_t)ltile * kMaxWalls + w) * 3 + c] = acc;
-    __threadfence();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned prev = atomicInc(a.block_counter, (unsigned)ntiles - 1u);
-    *s_last = (prev == (unsigned)ntiles - 1u);
-  }
-  __syncthreads();
-  if (!*s_last) return;
-  __threadfence();
-  for (int wc = 0; wc < nw3; ++wc) {
-    const int w = wc / 3, c = wc % 3;
-    double acc = 0.0;
-    for (int b = threadIdx.x; b < ntiles; b += blockDim.x)
-      acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    __syncthreads();
-    if (wlane == 0) s_red[warp][0][0] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
-      a.wall_force[3 * w + c] = t;
-      if (a.wall_hist) a.wall_hist[(size_t)(step - a.wall_hist_t0 - 1) * (kMaxWalls * 3) + 3 * w + c] = t;
-    }
-  }
-  if (threadIdx.x == 0) {
-    for (int w = 0; w < a.nwall; ++w) {  // native wall loader: origin += v*dt per step
-      WallDev* W = a.walls + w;
-      if (a.wall_vel[3 * w] != 0.0 || a.wall_vel[3 * w + 1] != 0.0 || a.wall_vel[3 * w + 2] != 0.0) {
-        W->ox += a.wall_vel[3 * w] * a.dt;
-        W->oy += a.wall_vel[3 * w + 1] * a.dt;
-        W->oz += a.wall_vel[3 * w + 2] * a.dt;
-      }
-    }
-    *a.step_counter = step;
-    volatile int* ctrl = a.ctrl;
-    if (*ctrl & ~a.stop_skip) *a.stop = 1;
-  }
+  if (!block_partials(a, ltile, ntiles, a.block_counter, s_red, s_last)) return;
+  launch_tail(a, step, ntiles, wlane, warp);
 }
 
 template <bool ROT, int TPP, int FEAT, bool FP32>
@@ -124,8 +80,49 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F
     const bool alive = valid && (pf & PF_ALIVE);
     V Fp, Mp;
     pair_sums<ROT, TPP, FEAT, FP32, false>(a, in, i, lane, alive, step, p4, q4, Fp, Mp);
-    finish_particle<ROT, TPP, FP32, false>(a, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
+    finish_particle<ROT, TPP, FP32, false>(a, step, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
                                            ROT && (FEAT & F_BOND), Fp, Mp, s_red);
+    batch_tile_epilogue(a, step, ltile, ntiles, wlane, warp, s_red, &s_last);
+  }
+}
+
+// Tiled form of k_step_batch (dem_tiled.cuh): the tile's pair and bond entries are
+// evaluated by the whole block, then each particle adds its entries in adjacency order.
+template <bool ROT, int FEAT, bool FP32>
+__global__ void __launch_bounds__(kTileThreads, FP32 ? kTiledBlocks32 : kTiledBlocks64) k_step_batch_tiled(const BatchArgs B) {
+  __shared__ double s_red[kStepWarps][kMaxWalls][3];
+  __shared__ bool s_last;
+  __shared__ TileSmem<FP32, false> S;
+  const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int tile = blockIdx.x; tile < B.total_tiles; tile += gridDim.x) {
+    const int sp = batch_specimen(B, tile);
+    const StepArgs& a0 = B.args[2 * sp];
+    // The specimen's counter and stop word change only in its own last tile, after every
+    // tile of this launch has read them: the decision below is uniform over its tiles.
+    const long long done = *(volatile long long*)a0.step_counter;
+    if (*(volatile int*)a0.stop || done >= __ldg(B.target + sp)) continue;
+    const int cur = (int)((done - __ldg(B.base_t + sp) + __ldg(B.base_cur + sp)) & 1);
+    const StepArgs& a = B.args[2 * sp + cur];
+    const long long step = done + 1;
+    const int t0 = __ldg(B.tile_start + sp);
+    const int ltile = tile - t0, ntiles = __ldg(B.tile_start + sp + 1) - t0;
+    const ParticleBuf in = a.P.buf[a.cur];
+    const ParticleBuf out = a.P.buf[a.cur ^ 1];
+    __syncthreads();  // the previous tile's epilogue has finished with s_red
+    for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kTileThreads) (&s_red[0][0][0])[k] = 0.0;
+    const int i0 = ltile * kTileThreads;
+    const int np = max(0, min(kTileThreads, a.P.n - i0));
+    const int i = i0 + threadIdx.x;
+    const bool valid = (int)threadIdx.x < np;
+    unsigned pf;
+    double4 p4;
+    tile_own<ROT, FEAT, FP32, false>(a, in, i0, np, pf, p4, S);
+    const bool alive = valid && (pf & PF_ALIVE);
+    V Fp, Mp;
+    double gross;
+    tile_pair_sums<ROT, FEAT, FP32, false>(a, in, i0, np, step, S, Fp, Mp, gross);
+    finish_particle<ROT, 1, FP32, false>(a, step, in, out, i, 0, wlane, warp, pf, alive, p4, make_double4(1, 0, 0, 0), false,
+                                         Fp, Mp, s_red);
     batch_tile_epilogue(a, step, ltile, ntiles, wlane, warp, s_red, &s_last);
   }
 }
@@ -175,7 +172,18 @@ inline void launch_batch_fixed(const BatchArgs& B, cudaStream_t s) {
 }
 
 template <bool R, int FEAT, bool FP32>
+inline void launch_batch_tiled(const BatchArgs& B, cudaStream_t s) {
+  const int wave = one_wave(k_step_batch_tiled<R, FEAT, FP32>, kTileThreads);
+  const int grid = B.total_tiles < wave ? B.total_tiles : wave;
+  if (grid > 0) k_step_batch_tiled<R, FEAT, FP32><<<grid, kTileThreads, 0, s>>>(B);
+}
+
+template <bool R, int FEAT, bool FP32>
 inline void launch_batch_tpp(const BatchArgs& B, int tpp, cudaStream_t s) {
+  if (tpp == kTiled) {
+    if constexpr (TiledSupported<FEAT>::value) return launch_batch_tiled<R, FEAT, FP32>(B, s);
+    tpp = 1;
+  }
   switch (tpp) {
     case 1: launch_batch_fixed<R, 1, FEAT, FP32>(B, s); break;
     case 2: launch_batch_fixed<R, 2, FEAT, FP32>(B, s); break;

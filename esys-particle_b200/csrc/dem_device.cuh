@@ -33,6 +33,11 @@ constexpr int kMaxDyn = 2;
 constexpr int kMaxBond = 2;
 constexpr int kBondAlive = 0x7fffffff;
 constexpr int kBondPassThreads = 128;  // bonds per block of the bond pass
+constexpr int kTiled = 16;             // threads_per_particle setting of the tiled step kernels (dem_tiled.cuh)
+#ifndef DEM_TILE_THREADS
+#define DEM_TILE_THREADS 256
+#endif
+constexpr int kTileThreads = DEM_TILE_THREADS;  // threads (= particles) per tile of the tiled step kernels
 
 struct Grid {
   double p0x, p0y, p0z;  // origin of the global grid (the grown bounding box minimum)
@@ -149,6 +154,7 @@ struct StepArgs {
   int damp_loc, damp_rotloc, loc_before_lin;
   double visc_loc, visc_rotloc;
   int store_forces;
+  long long force_step;     // forces are stored by this step only (-1: by every step)
   // device bond hand-off: a bond failure does not stop the chunk; the pairs it excluded turn
   // into ordinary pairs (DynDev::xbond) and every particle refreshes its wall candidacy at the
   // step after a failure (brk_step: last step with a failure)

@@ -18,7 +18,7 @@
 #include "dem_kernels.h"
 #include "dem_common.cuh"
 #include "dem_laws.cuh"
-#include "dem_step.cuh"
+#include "dem_tiled.cuh"
 
 namespace dem {
 
@@ -426,36 +426,76 @@ __global__ void k_move_tagged(Particles P, int cur, int tag, double dx, double d
 
 // ---------------------------------------------------------------------------
 // CEWallInteractionGroup::applyForce (EWallInteractionGroup.hpp:93-164): servo
-// iteration of one wall against its candidates' elastic contacts.  One block.
+// iteration of one wall against its candidates' elastic contacts.  One block of
+// kServoThreads.  Thread t owns the slots t, t + kServoThreads, ... (a fixed assignment,
+// so the sums are reproducible): it first lists its candidates of wall w, in slot order,
+// in its own segment of idx (offsets from a block scan of the counts), then every
+// iteration visits only that segment instead of rescanning all slots.
 // ---------------------------------------------------------------------------
-__global__ void k_wall_servo(Particles P, int cur, int w, WallDev* walls, double Fx, double Fy, double Fz) {
+constexpr int kServoThreads = 1024;
+
+__global__ void __launch_bounds__(kServoThreads) k_wall_servo(Particles P, int cur, int w, WallDev* walls, double Fx,
+                                                               double Fy, double Fz, int* idx) {
   __shared__ double red[32][4];
-  __shared__ double s_move[3];
+  __shared__ int s_wsum[32];
   __shared__ int s_done;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const unsigned cand = 1u << (PF_WALL_SHIFT + w), inner = 1u << (PF_INNER_SHIFT + w);
+  // this thread's candidates: count, block exclusive scan, then list them
+  int c = 0;
+  for (int i = t; i < P.n; i += kServoThreads) {
+    const unsigned pf = P.pflags[i];
+    c += ((pf & PF_ALIVE) && (pf & cand)) ? 1 : 0;
+  }
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) s_wsum[wid] = incl;
+  if (t == 0) s_done = 0;
+  __syncthreads();
+  if (wid == 0) {
+    int v = s_wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    s_wsum[lane] = v;  // inclusive over warps
+  }
+  __syncthreads();
+  const int off = (wid ? s_wsum[wid - 1] : 0) + incl - c;
+  int e = off;
+  for (int i = t; i < P.n; i += kServoThreads) {
+    const unsigned pf = P.pflags[i];
+    if ((pf & PF_ALIVE) && (pf & cand)) idx[e++] = (pf & inner) ? (i | (int)0x80000000) : i;
+  }
+  // the fixed point (each thread reads back only what it wrote itself)
   const V Fv = mk(Fx, Fy, Fz);
   const double Fn = norm(Fv);
   const V O_f = Fv / Fn;
   WallDev* W = walls + w;
+  const double4* pr = P.buf[cur].pr;
   int it = 0;
-  if (threadIdx.x == 0) s_done = 0;
-  __syncthreads();
   while (!s_done) {
     const V o = mk(W->ox, W->oy, W->oz), n = mk(W->nx, W->ny, W->nz);
+    const double kw = W->k;
     double kl = 0, fx = 0, fy = 0, fz = 0;
-    for (int i = threadIdx.x; i < P.n; i += blockDim.x) {
-      unsigned pf = P.pflags[i];
-      if (!(pf & PF_ALIVE) || !(pf & (1u << (PF_WALL_SHIFT + w)))) continue;
-      const double4 p = P.buf[cur].pr[i];
+    for (int q = off; q < off + c; ++q) {
+      const int code = idx[q];
+      const double4 p = pr[code & 0x7fffffff];
       double f = 1.0;
       f *= 3.141592654 * p.w;
-      const double mk_ = f * W->k;
+      const double mk_ = f * kw;
       double dist = dot(xyz(p) - o, n);
       if (dist < p.w) {
         kl += mk_;  // getStiffness
-        if (pf & (1u << (PF_INNER_SHIFT + w))) {
+        if (code < 0) {
           V fi = -1.0 * (mk_ * (p.w - dist) * n);  // getForce
-          V c = dot(fi, O_f) * O_f;
-          fx += c.x; fy += c.y; fz += c.z;
+          V cc = dot(fi, O_f) * O_f;
+          fx += cc.x; fy += cc.y; fz += cc.z;
         }
       }
     }
@@ -465,11 +505,11 @@ __global__ void k_wall_servo(Particles P, int cur, int w, WallDev* walls, double
       fy += __shfl_down_sync(0xffffffffu, fy, o2);
       fz += __shfl_down_sync(0xffffffffu, fz, o2);
     }
-    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5][0] = kl; red[threadIdx.x >> 5][1] = fx; red[threadIdx.x >> 5][2] = fy; red[threadIdx.x >> 5][3] = fz; }
+    if (lane == 0) { red[wid][0] = kl; red[wid][1] = fx; red[wid][2] = fy; red[wid][3] = fz; }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (t == 0) {
       double K = 0, gx = 0, gy = 0, gz = 0;
-      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { K += red[k][0]; gx += red[k][1]; gy += red[k][2]; gz += red[k][3]; }
+      for (int k = 0; k < kServoThreads / 32; ++k) { K += red[k][0]; gx += red[k][1]; gy += red[k][2]; gz += red[k][3]; }
       double d, ef;
       if (K > 0) {
         const V Fg = mk(gx, gy, gz);
@@ -674,8 +714,8 @@ void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* c
 void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, cudaStream_t s) {
   if (P.n) k_move_tagged<<<nblk(P.n, 256), 256, 0, s>>>(P, cur, tag, d[0], d[1], d[2]);
 }
-void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s) {
-  k_wall_servo<<<1, 1024, 0, s>>>(P, cur, w, walls, F[0], F[1], F[2]);
+void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, int* idx, cudaStream_t s) {
+  k_wall_servo<<<1, kServoThreads, 0, s>>>(P, cur, w, walls, F[0], F[1], F[2], idx);
 }
 
 int step_grid(int n, int tpp) { return step_blocks(n, tpp); }

@@ -40,7 +40,8 @@ void launch_set_state(const Particles& P, int cur, int cnt, const int* slots, co
                       const double* angvel, const double* quat, cudaStream_t s);
 void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* ctrl, cudaStream_t s);
 void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, cudaStream_t s);
-void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, cudaStream_t s);
+// idx: scratch of at least P.n ints (each servo thread's candidate list)
+void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, int* idx, cudaStream_t s);
 void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex, int* xbond, cudaStream_t s);
 void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s);
 void launch_particle_field(const Particles& P, int cur, int rot, int field, double* out, cudaStream_t s);

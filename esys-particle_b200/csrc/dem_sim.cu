@@ -131,6 +131,7 @@ struct DemSim {
   int adj_tangents = 0;  // adjoint RotBond VJP: 0 hand-written reverse, else dual tangents per pass
   int adj_pair_duals = 0;  // adjoint pair-law VJPs: 0 hand-written reverse, 1 forward-mode duals
   DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
+  DBuf<int> d_servo_idx; // wall servo: candidate lists of its threads (n ints)
   // particles
   int n = 0, cap = 0;
   Particles P{};
@@ -203,7 +204,7 @@ struct DemSim {
     scratch_i.release(); scratch_j.release(); scalars.release(); scan_tmp.release();
     d_walls.release(); d_wall_vel.release(); d_wall_partial.release(); d_wall_force.release();
     d_block_counter.release(); d_step.release(); d_ctrl.release(); d_stop.release();
-    stage.release(); stage_slot.release(); scratch_d.release(); sig.release();
+    stage.release(); stage_slot.release(); scratch_d.release(); sig.release(); d_servo_idx.release(); d_brk.release();
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -776,6 +777,7 @@ struct DemSim {
     a.visc_lin = visc_lin; a.visc_rot = visc_rot; a.dt_lin = dt; a.dt_rot = dt;
     a.iter_lin = iter_lin; a.iter_rot = iter_rot;
     a.store_forces = store_forces;
+    a.force_step = -1;
     a.handoff = handoff;
     a.brk_step = d_brk.p;
     a.stop_skip = handoff ? CTRL_BROKE : 0;
@@ -788,8 +790,18 @@ struct DemSim {
     return a;
   }
 
+  // Groups the tiled step kernels cover: the core pair laws, and bonds through the bond pass.
+  bool tiled_ok() const {
+    for (auto& d : dyn) if (d.second.kind >= 2) return false;
+    for (auto& b : bond) if (b.second.kind == 1 || b.second.kind == 3) return false;
+    return bond.empty() || bond_pass || fp32;
+  }
+
+  // Lanes per particle when none is set: from the mean adjacency length.  The tiled kernels
+  // (kTiled) are chosen explicitly or by the ensemble autotuner; on the 250k shear cell and
+  // the 1M bonded block they measured no faster than the lane kernels.
   int pick_tpp() {
-    if (tpp) return tpp;
+    if (tpp) return tpp == kTiled && !tiled_ok() ? 1 : tpp;
     long long e = 0;
     for (auto& d : dyn) e += 2LL * d.second.m;
     for (auto& b : bond) e += 2LL * b.second.nb;
@@ -815,6 +827,8 @@ struct DemSim {
 
   int step(int nsteps) {
     int done = 0;
+    // the forces a caller can observe are the last step's: only that step stores them
+    const long long t_last = t + nsteps;
     while (done < nsteps) {
       if (!prepare()) return -2;
       // launch a chunk of force + integration steps
@@ -834,6 +848,7 @@ struct DemSim {
       const bool two = split == 1;  // automatic = fused: measured faster on the 250k shear cell
       for (int j = 0; j < k; ++j) {
         StepArgs a = make_args((cur + j) & 1);
+        a.force_step = t_last;
         if (fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
         else launch_step(a, rot != 0, t_pp, two, s);
       }
@@ -1989,6 +2004,11 @@ struct Ensemble {
   }
 
   int pick_tpp() const {
+    if (tpp == kTiled) {
+      bool tiled = true;
+      for (DemSim* d : sims) tiled = tiled && d->tiled_ok() && (d->bond.empty() || d->bond_pass);
+      return tiled ? kTiled : 1;
+    }
     if (tpp) return tpp;
     long long e = 0, np = 0;
     for (DemSim* d : sims) {
@@ -2104,6 +2124,7 @@ struct Ensemble {
       h_args[2 * q] = d.make_args(0);
       h_args[2 * q + 1] = d.make_args(1);
       h_args[2 * q].store_forces = h_args[2 * q + 1].store_forces = d.store_forces;
+      h_args[2 * q].force_step = h_args[2 * q + 1].force_step = target[q];
       if (window) {
         for (int c = 0; c < 2; ++c) {
           h_args[2 * q + c].wall_hist = d.win.R.p;
@@ -2731,7 +2752,8 @@ int dem_apply_force_to_wall(dem_sim* h, const char* group, const double* f) {
     auto it = s.wig.find(group);
     if (it == s.wig.end()) throw std::invalid_argument("no such wall group");
     int w = (int)std::distance(s.wig.begin(), it);
-    dem::launch_wall_servo(s.P, s.cur, w, s.d_walls.p, f, s.s);
+    s.d_servo_idx.reserve(std::max(s.n, 1));
+    dem::launch_wall_servo(s.P, s.cur, w, s.d_walls.p, f, s.d_servo_idx.p, s.s);
     s.sync();
     // the servo moves the group's copy of the wall: propagate to groups sharing the wall
     std::vector<dem::WallDev> wd(s.wig.size());
@@ -2979,7 +3001,8 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
     std::string k = key ? key : "";
     if (k == "threads_per_particle") {
       int v = (int)value;
-      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8) throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8");
+      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8 && v != dem::kTiled)
+        throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8 or 16 (tiled)");
       s.tpp = v;
     } else if (k == "chunk") {
       if (value < 1) throw std::invalid_argument("chunk must be >= 1");
@@ -3299,7 +3322,8 @@ int dem_ensemble_set_option(dem_ensemble* h, const char* key, double value) {
     const std::string k = key ? key : "";
     if (k == "threads_per_particle") {
       const int v = (int)value;
-      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8) throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8");
+      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8 && v != dem::kTiled)
+        throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8 or 16 (tiled)");
       e.tpp = v;
     } else if (k == "chunk") {
       if (value < 1) throw std::invalid_argument("chunk must be >= 1");

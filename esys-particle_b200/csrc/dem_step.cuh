@@ -53,7 +53,13 @@ constexpr int kStepWarps = kStepThreads / 32;
 #endif
 constexpr int kFp32Blocks = DEM_FP32_BLOCKS;  // resident blocks per SM targeted by the FP32 pair instances
 
+// Lanes per particle of a threads_per_particle setting, in units of kStepThreads per tile:
+// the tiled kernels (kTiled, dem_tiled.cuh) give each particle one thread of a block of
+// kTileThreads, i.e. a tile of kTileThreads particles.
+__host__ __device__ __forceinline__ int tile_lanes(int tpp) { return tpp == kTiled ? kStepThreads / kTileThreads : tpp; }
+
 __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
+  tpp = tile_lanes(tpp);
   long long t = (long long)(n > 0 ? n : 1) * tpp;
   return (int)((t + kStepThreads - 1) / kStepThreads);
 }
@@ -398,8 +404,9 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
 // (TSubLattice::calcForces group order, then integrate + rescale).  Every thread
 // of the block calls this: the wall reactions are reduced across the block.
 template <bool ROT, int TPP, bool FP32, bool EVAL>
-__device__ __forceinline__ void finish_particle(const StepArgs& a, const ParticleBuf& in, const ParticleBuf& out, int i,
-                                                int lane, int wlane, int warp, unsigned pf, bool alive,
+__device__ __forceinline__ void finish_particle(const StepArgs& a, long long step, const ParticleBuf& in,
+                                                const ParticleBuf& out, int i, int lane, int wlane, int warp,
+                                                unsigned pf, bool alive,
                                                 const double4& p4, double4 q4, bool q_loaded, const V& Fp, const V& Mp,
                                                 double (*s_red)[kMaxWalls][3]) {
   double4 v4 = make_double4(0.0, 0.0, 0.0, 0.0), w4 = v4;
@@ -414,7 +421,6 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
   //    CEWallInteractionGroup::Update does in that step's updateInteractions
   //    (EWallInteractionGroup.hpp:57-82, NeighborTable::getParticlesAtPlane ntable.hpp:674-690)
   if (a.handoff && alive) {
-    const long long step = *a.step_counter + 1;
     if (a.brk_step[(step - 1) & 1] == (int)(step - 1)) {
       pf &= ~(0xffffu << PF_WALL_SHIFT);
       const bool inner = inner_of(a.g, p4.x, p4.y, p4.z);
@@ -522,7 +528,7 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
         out.vw[2 * i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)w.x);
         out.vw[2 * i + 1] = make_float4((float)w.y, (float)w.z, 0.f, 0.f);
       }
-      if (a.store_forces) {
+      if (a.store_forces && (a.force_step < 0 || step == a.force_step)) {
         a.P.force[i] = d4(F, 0.0);
         if (ROT) a.P.moment[i] = d4(M, 0.0);
       }
@@ -534,61 +540,81 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, const Particl
   }
 }
 
-// Per-block wall reactions (fixed order over warps), then the last block of the
-// launch finishes the step: wall totals, native wall loaders, step counter and
-// the stop word.  All threads of the block call this.
-__device__ __forceinline__ void step_epilogue(const StepArgs& a, int wlane, int warp, double (*s_red)[kMaxWalls][3],
-                                              bool* s_last) {
-  const long long step = *a.step_counter + 1;
-  // per-block wall reactions (fixed order over warps), then the last block finishes the step
+// Totals of the wall reactions from the nparts per-block (or per-tile) partials, in
+// the last block of a launch: component wc = 3 w + c is summed by warp wc % (warps of the
+// block), lane l adding partials l, l + 32, ... in order, then a fixed butterfly; all
+// components at once, so the launch's serial tail is one round of loads.
+__device__ __forceinline__ void wall_totals(const StepArgs& a, long long step, int nparts, int wlane, int warp) {
+  const int nw3 = a.nwall * 3;
+  const int nwarps = (int)(blockDim.x >> 5);
+  for (int wc = warp; wc < nw3; wc += nwarps) {
+    const int w = wc / 3, c = wc % 3;
+    double acc = 0.0;
+#pragma unroll 4
+    for (int b = wlane; b < nparts; b += 32) acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (wlane == 0) {
+      a.wall_force[3 * w + c] = acc;
+      if (a.wall_hist) a.wall_hist[(size_t)(step - a.wall_hist_t0 - 1) * (kMaxWalls * 3) + 3 * w + c] = acc;
+    }
+  }
+}
+
+// This block's wall partials (fixed order over warps) into slot `part`, then the
+// last-arriving block of the `nparts` is detected on `counter`.  Returns true in that block.
+// All threads of the block call this.
+__device__ __forceinline__ bool block_partials(const StepArgs& a, int part, int nparts, unsigned* counter,
+                                               double (*s_red)[kMaxWalls][3], bool* s_last) {
   const int nw3 = a.nwall * 3;
   __syncthreads();
   if (threadIdx.x < nw3) {
     const int w = threadIdx.x / 3, c = threadIdx.x % 3;
     double acc = 0.0;
     for (int k = 0; k < kStepWarps; ++k) acc += s_red[k][w][c];
-    a.wall_partial[((size_t)blockIdx.x * kMaxWalls + w) * 3 + c] = acc;
-    __threadfence();
+    a.wall_partial[((size_t)part * kMaxWalls + w) * 3 + c] = acc;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned prev = atomicInc(a.block_counter, gridDim.x - 1);
-    *s_last = (prev == gridDim.x - 1);
+    __threadfence();  // the block's partials and control bits before its arrival
+    const unsigned prev = atomicInc(counter, (unsigned)nparts - 1u);
+    *s_last = (prev == (unsigned)nparts - 1u);
   }
   __syncthreads();
-  if (!*s_last) return;
+  if (!*s_last) return false;
   __threadfence();
-  // wall reactions: thread t sums blocks t, t+256, ... (fixed assignment), then a fixed tree
-  for (int wc = 0; wc < nw3; ++wc) {
-    const int w = wc / 3, c = wc % 3;
-    double acc = 0.0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-      acc += __ldcg(a.wall_partial + ((size_t)b * kMaxWalls + w) * 3 + c);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (wlane == 0) s_red[warp][0][0] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int k = 0; k < kStepWarps; ++k) t += s_red[k][0][0];
-      a.wall_force[3 * w + c] = t;
-      if (a.wall_hist) a.wall_hist[(size_t)(step - a.wall_hist_t0 - 1) * (kMaxWalls * 3) + 3 * w + c] = t;
+  return true;
+}
+
+// The end of a timestep, run by the last block: wall totals, native wall loaders (one
+// thread per wall: origin += v dt, WallLoaderRunnable), the step counter and the stop word.
+// The control word is read first, so its load overlaps the totals'.
+__device__ __forceinline__ void launch_tail(const StepArgs& a, long long step, int nparts, int wlane, int warp) {
+  int ctrl = 0;
+  if (threadIdx.x == 0) ctrl = *(volatile int*)a.ctrl;
+  wall_totals(a, step, nparts, wlane, warp);
+  if ((int)threadIdx.x < a.nwall) {
+    const int w = threadIdx.x;
+    const double vx = a.wall_vel[3 * w], vy = a.wall_vel[3 * w + 1], vz = a.wall_vel[3 * w + 2];
+    if (vx != 0.0 || vy != 0.0 || vz != 0.0) {
+      WallDev* W = a.walls + w;
+      W->ox += vx * a.dt;
+      W->oy += vy * a.dt;
+      W->oz += vz * a.dt;
     }
-    __syncthreads();
   }
   if (threadIdx.x == 0) {
-    for (int w = 0; w < a.nwall; ++w) {  // native wall loader: origin += v*dt per step (WallLoaderRunnable)
-      WallDev* W = a.walls + w;
-      if (a.wall_vel[3 * w] != 0.0 || a.wall_vel[3 * w + 1] != 0.0 || a.wall_vel[3 * w + 2] != 0.0) {
-        W->ox += a.wall_vel[3 * w] * a.dt;
-        W->oy += a.wall_vel[3 * w + 1] * a.dt;
-        W->oz += a.wall_vel[3 * w + 2] * a.dt;
-      }
-    }
     *a.step_counter = step;
-    volatile int* ctrl = a.ctrl;
-    if (*ctrl & ~a.stop_skip) *a.stop = 1;
+    if (ctrl & ~a.stop_skip) *a.stop = 1;
   }
+}
+
+// Per-block wall reactions, then the last block of the launch finishes the step.  All
+// threads of the block call this.
+__device__ __forceinline__ void step_epilogue(const StepArgs& a, long long step, int wlane, int warp,
+                                              double (*s_red)[kMaxWalls][3], bool* s_last) {
+  if (!block_partials(a, blockIdx.x, gridDim.x, a.block_counter, s_red, s_last)) return;
+  launch_tail(a, step, gridDim.x, wlane, warp);
 }
 
 
@@ -717,7 +743,7 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
 #pragma unroll
     for (int c = 0; c < 9; ++c) Sg[c] = 0.0;
     pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp, &gross, Sg);
-    finish_particle<ROT, TPP, FP32, EVAL>(a, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
+    finish_particle<ROT, TPP, FP32, EVAL>(a, step, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
                                           ROT && (FEAT & F_BOND), Fp, Mp, s_red);
     if constexpr (!FP32 && !EVAL && (FEAT & F_STRESS) != 0) {
       if (alive && lane == 0) {
@@ -741,7 +767,7 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
     if (EVAL && alive && lane == 0) reinterpret_cast<double*>(a.P.force_eval + i)[3] = gross;
   }
   if (EVAL) return;
-  step_epilogue(a, wlane, warp, s_red, &s_last);
+  step_epilogue(a, step, wlane, warp, s_red, &s_last);
 }
 
 // Split step, part 1: pair and bond sums of every particle into P.sum_f / P.sum_m
@@ -776,6 +802,7 @@ __global__ void __launch_bounds__(kStepThreads, 3) k_integrate(const StepArgs a)
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;
   if (*a.stop) return;
+  const long long step = *a.step_counter + 1;
   for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kStepThreads) (&s_red[0][0][0])[k] = 0.0;
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -792,12 +819,13 @@ __global__ void __launch_bounds__(kStepThreads, 3) k_integrate(const StepArgs a)
     Fp = xyz(ldg4(a.P.sum_f + i));
     if (ROT) Mp = xyz(ldg4(a.P.sum_m + i));
   }
-  finish_particle<ROT, 1, FP32, false>(a, in, out, i, 0, wlane, warp, pf, alive, p4, make_double4(1, 0, 0, 0), false,
+  finish_particle<ROT, 1, FP32, false>(a, step, in, out, i, 0, wlane, warp, pf, alive, p4, make_double4(1, 0, 0, 0), false,
                                        Fp, Mp, s_red);
-  step_epilogue(a, wlane, warp, s_red, &s_last);
+  step_epilogue(a, step, wlane, warp, s_red, &s_last);
 }
 
 inline int step_blocks(int n, int tpp) {
+  tpp = tile_lanes(tpp);
   long long t = (long long)(n > 0 ? n : 1) * tpp;
   return (int)((t + kStepThreads - 1) / kStepThreads);
 }
@@ -805,7 +833,7 @@ inline int step_blocks(int n, int tpp) {
 // Blocks of one wave of kernel K on the current device, cached per kernel (every
 // instance of k_step shares one function type, so the cache is keyed by address).
 template <class K>
-inline int one_wave(K kernel) {
+inline int one_wave(K kernel, int threads = kStepThreads) {
   static std::mutex mu;
   static std::map<const void*, int> cache;
   std::lock_guard<std::mutex> lock(mu);
@@ -815,7 +843,7 @@ inline int one_wave(K kernel) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStepThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
   const int v = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
   cache[key] = v;
   return v;
@@ -823,6 +851,7 @@ inline int one_wave(K kernel) {
 
 template <bool R, int FEAT, bool FP32>
 inline void launch_split_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
+  tpp = tile_lanes(tpp);
   const int grid = step_blocks(a.P.n, tpp);
   switch (tpp) {
     case 1: k_pairs<R, 1, FEAT, FP32><<<grid, kStepThreads, 0, s>>>(a); break;
@@ -846,16 +875,6 @@ inline void launch_bond_pass(const StepArgs& a, cudaStream_t s) {
     const int nb = a.bond[d].nb_launch;
     if (nb > 0)
       k_bond_pass<EVAL, FP32><<<(nb + kBondPassThreads - 1) / kBondPassThreads, kBondPassThreads, 0, s>>>(a, d, nb);
-  }
-}
-
-template <bool R, int FEAT, bool FP32, bool EVAL>
-inline void launch_step_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
-  switch (tpp) {
-    case 1: launch_fused<R, 1, FEAT, FP32, EVAL>(a, s); break;
-    case 2: launch_fused<R, 2, FEAT, FP32, EVAL>(a, s); break;
-    case 4: launch_fused<R, 4, FEAT, FP32, EVAL>(a, s); break;
-    default: launch_fused<R, 8, FEAT, FP32, EVAL>(a, s); break;
   }
 }
 

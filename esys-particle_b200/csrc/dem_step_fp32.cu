@@ -3,7 +3,7 @@
 // overlap / integration in FP64.  Built with FMA contraction (the FP32 form is
 // checked against FP64 at a stated relative tolerance, not bit for bit).
 #include "dem_kernels.h"
-#include "dem_step.cuh"
+#include "dem_tiled.cuh"
 
 namespace dem {
 

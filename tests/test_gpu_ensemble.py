@@ -54,7 +54,8 @@ def _same(a, b, groups, tol_wall=1e-12):
 
 @pytest.mark.parametrize("kind,groups,steps", [("friction", ["friction"], 300), ("elastic", ["elastic"], 200)])
 @pytest.mark.parametrize("precision", [64, 32])
-def test_ensemble_equals_specimens_alone(gpu, kind, groups, steps, precision):
+@pytest.mark.parametrize("tpp", [2, 16])
+def test_ensemble_equals_specimens_alone(gpu, kind, groups, steps, precision, tpp):
     from esys.lsm import _capi
 
     if kind == "elastic" and precision == 32:
@@ -63,9 +64,9 @@ def test_ensemble_equals_specimens_alone(gpu, kind, groups, steps, precision):
     alone = _specimens(gpu, kind)
     for s in ens_sims + alone:
         s.set_option("precision", precision)
-        s.set_option("threads_per_particle", 2)
+        s.set_option("threads_per_particle", tpp)
     e = _capi.Ensemble(ens_sims)
-    e.set_option("threads_per_particle", 2)
+    e.set_option("threads_per_particle", tpp)
     e.set_option("chunk", 48)
     e.step(steps)
     for s in alone:
@@ -77,7 +78,8 @@ def test_ensemble_equals_specimens_alone(gpu, kind, groups, steps, precision):
     e.close()
 
 
-def test_bonded_ensemble_breaks_like_specimens_alone(gpu):
+@pytest.mark.parametrize("tpp", [4, 16])
+def test_bonded_ensemble_breaks_like_specimens_alone(gpu, tpp):
     """Bond failures (of different strengths, so at different steps), the exclusion hand-off
     to friction and rebuilds happen at different steps in different specimens."""
     from esys.lsm import _capi
@@ -85,9 +87,9 @@ def test_bonded_ensemble_breaks_like_specimens_alone(gpu):
     ens_sims = _specimens(gpu, "bonded")
     alone = _specimens(gpu, "bonded")
     e = _capi.Ensemble(ens_sims)
-    e.set_option("threads_per_particle", 4)
+    e.set_option("threads_per_particle", tpp)
     for s in alone:
-        s.set_option("threads_per_particle", 4)
+        s.set_option("threads_per_particle", tpp)
     _advance_loaded(ens_sims, 60, 0.002, e.step)
     for s in alone:
         S.run_loaded(s, 60, 0.002)

@@ -77,19 +77,29 @@ def _block_sim(gpu, data, precision=64, bond_pass=1):
 STEPS = 60
 
 
+def _same_runs(runs):
+    for r in runs[1:]:
+        assert np.array_equal(r[0], runs[0][0]) and np.array_equal(r[1], runs[0][1])
+        for u, v in zip(r[2], runs[0][2]):
+            assert np.array_equal(u, v)
+
+
 def test_bonded_block_1m_deterministic_and_bond_pass_exact(gpu, block_1m):
+    """Two runs of the default (tiled) step are bit-identical; the bond pass equals the
+    in-line evaluation of the bond law bit for bit when both sum a particle's contributions
+    in the same order (the lane-parallel kernels at four lanes per particle)."""
     runs = []
-    for bp in (1, 1, 0):
+    for bp, tpp in ((1, 0), (1, 0), (1, 4), (0, 4)):
         s = _block_sim(gpu, block_1m, 64, bp)
+        if tpp:
+            s.set_option("threads_per_particle", tpp)
         assert s.num_particles() == 1_000_000
         s.step(STEPS)
         p = s.particles(sort=False)
         runs.append((p["pos"], p["quat"], s.breaks()))
         s.close()
-    for r in runs[1:]:
-        assert np.array_equal(r[0], runs[0][0]) and np.array_equal(r[1], runs[0][1])
-        for u, v in zip(r[2], runs[0][2]):
-            assert np.array_equal(u, v)
+    _same_runs(runs[:2])
+    _same_runs(runs[2:])
 
 
 def test_bonded_block_1m_fp32_break_log_equals_fp64(gpu, block_1m):

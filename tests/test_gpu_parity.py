@@ -56,7 +56,7 @@ def test_gravity_box(gpu, orc, steps):
         assert np.abs(fa - fb).max() <= 1e-8 * max(np.abs(fb).max(), 1.0), w
 
 
-@pytest.mark.parametrize("tpp", [1, 2, 4, 8])
+@pytest.mark.parametrize("tpp", [1, 2, 4, 8, 16])
 def test_friction_pack_threads_per_particle(gpu, orc, tpp):
     a, b = S.friction_pack(gpu), S.friction_pack(orc)
     a.set_option("threads_per_particle", tpp)
@@ -176,6 +176,7 @@ def test_bond_pass_equals_inline_bond_law(gpu, precision):
     b = S.bonded_block(gpu, strength=(0.4, 0.8, 0.8, 0.4))
     for s in (a, b):
         s.set_option("precision", precision)
+        s.set_option("threads_per_particle", 4)  # the lane-parallel kernels carry both forms
     b.set_option("bond_pass", 0)
     S.run_loaded(a, 120, 0.002)
     S.run_loaded(b, 120, 0.002)
