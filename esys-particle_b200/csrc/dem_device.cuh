@@ -115,6 +115,9 @@ struct BondDev {
   int* nevents;
   int cap_events;
   double4* bf;              // bond pass (else null): per bond the force on p1, the moment on p1 and on p2
+  float4* bf32;             // FP32-force form (else null; takes the place of bf): per bond two 32-byte
+                            // records, p1's then p2's, each (Fx, Fy, Fz, Mx), (My, Mz, 0, 0) of the
+                            // force and moment on that particle
   int nb_launch;            // bonds in the group (the bond pass's extent)
   const int2* ends;         // (p1 slot, p2 slot) of each bond, p1 = lower id
 };

@@ -106,10 +106,11 @@ struct BondGroup {
   DBuf<double4> D0;
   DBuf<int> broken_step, adj_start, adj_count, adj_cursor, p1_start, events, nevents;
   DBuf<int2> adj;
+  DBuf<float4> bf32;  // FP32-force form: the bond pass's FP32 records
   DBuf<double4> bf;  // bond pass results (3 records per bond)
   int cap_events = 0;
   void release() {
-    bf.release();
+    bf.release(); bf32.release();
     keys.release(); ends.release(); D0.release(); broken_step.release(); adj_start.release(); adj_count.release();
     adj_cursor.release(); p1_start.release(); events.release(); nevents.release(); adj.release();
   }
@@ -769,6 +770,10 @@ struct DemSim {
       if (bond_pass || fp32 || widened()) {
         B.bf.reserve((size_t)3 * std::max(B.nb, 1));
         D.bf = B.bf.p;
+      }
+      if (fp32) {  // the FP32 form gathers its bonds' forces from FP32 records of the same pass
+        B.bf32.reserve((size_t)4 * std::max(B.nb, 1));
+        D.bf32 = B.bf32.p;
       }
     }
     a.damp_lin = damp_lin; a.damp_rot = damp_rot;

@@ -299,7 +299,14 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
         for (int e = e0 + lane; e < e1; e += TPP) {
           const int2 en = __ldg(B.adj + e);
           const int k = en.y & 0x7fffffff;
-          if (B.broken_step[k] <= step) continue;  // removed by an earlier update
+          // a bond removed by an earlier update carries zero records (bond_pass_one writes them)
+          if constexpr (FP32 && !EVAL) {
+            const float4* rf = B.bf32 + 4 * (size_t)k + (en.y < 0 ? 0 : 2);
+            const float4 a0 = __ldg(rf), a1 = __ldg(rf + 1);
+            Fp += mk((double)a0.x, (double)a0.y, (double)a0.z);
+            if (ROT) Mp += mk((double)a0.w, (double)a1.x, (double)a1.y);
+            continue;
+          }
           const double4* r = B.bf + 3 * (size_t)k;
           if (en.y < 0) {
             Fp += xyz(ldg4(r));
@@ -622,9 +629,29 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a, long long step,
 // particle pass to gather (F_BGATHER); the failure test and its records as the p1 side of
 // the in-line evaluation writes them.  The same law and operation order as in pair_sums,
 // so the gathered values equal what either side would compute.
+// The bond pass's records of bond k: f the force on p1, m1 / m2 the moments on p1 / p2.
+__device__ __forceinline__ void store_bond(const BondDev& B, int k, const V& f, const V& m1, const V& m2) {
+  if (B.bf32) {
+    float4* r = B.bf32 + 4 * (size_t)k;
+    r[0] = make_float4((float)f.x, (float)f.y, (float)f.z, (float)m1.x);
+    r[1] = make_float4((float)m1.y, (float)m1.z, 0.f, 0.f);
+    r[2] = make_float4((float)(-f.x), (float)(-f.y), (float)(-f.z), (float)m2.x);
+    r[3] = make_float4((float)m2.y, (float)m2.z, 0.f, 0.f);
+  } else {
+    double4* r = B.bf + 3 * (size_t)k;
+    r[0] = d4(f, 0.0);
+    r[1] = d4(m1, 0.0);
+    r[2] = d4(m2, 0.0);
+  }
+}
+
 template <bool EVAL>
 __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& B, int k, long long step) {
-  if (B.broken_step[k] <= step) return;
+  if (B.broken_step[k] <= step) {  // removed by an earlier update: zero records, so gathers need no test
+    const V z = mk(0.0, 0.0, 0.0);
+    store_bond(B, k, z, z, z);
+    return;
+  }
   const ParticleBuf in = a.P.buf[a.cur];
   const int2 e = __ldg(B.ends + k);
   if (B.kind == 1) {  // NRotBond: force on p2 F, on p1 -F, no moments
@@ -633,9 +660,8 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
     V F;
     double dist;
     law_nbond(nbond_k(B.knb, B.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, F, dist);
-    double4* r = B.bf + 3 * (size_t)k;
-    r[0] = d4(-1.0 * F, 0.0);
-    r[1] = r[2] = make_double4(0.0, 0.0, 0.0, 0.0);
+    const V z = mk(0.0, 0.0, 0.0);
+    store_bond(B, k, -1.0 * F, z, z);
     if (!EVAL && nbond_broken(dist, pa.w, pb.w, B.rbreak)) {
       B.broken_step[k] = (int)(step + 1);
       a.P.flagged[e.x] = 1;
@@ -664,10 +690,7 @@ __device__ __forceinline__ void bond_pass_one(const StepArgs& a, const BondDev& 
   const BondK K = bond_k(B.kr, B.ks, B.kt, B.kb, B.mn, B.ms, B.mt, B.mb, B.scaling, B.meanR, dist0, pa.w, pb.w);
   BondOut o;
   law_bond(K, mD, x1, pa.w, Qd{qa.x, mk(qa.y, qa.z, qa.w)}, x2, pb.w, Qd{qb.x, mk(qb.y, qb.z, qb.w)}, o);
-  double4* r = B.bf + 3 * (size_t)k;
-  r[0] = d4(o.force, 0.0);
-  r[1] = d4(o.moment1, 0.0);
-  r[2] = d4(o.moment2, 0.0);
+  store_bond(B, k, o.force, o.moment1, o.moment2);
   // BrittleBeamSC: tested at the update that opens the step (k_sc_check), not on the forces
   const bool brk = B.kind == 2   ? dzc_broken(o, dist0, B.cohesion, B.tan_angle, B.t_cutoff, B.c_cutoff, B.beta1, B.beta2)
                    : B.kind == 3 ? false

@@ -257,29 +257,37 @@ __device__ __forceinline__ void tile_eval_pairs(const StepArgs& a, const Particl
 }
 
 // Bond entries [Eb, Eb + m) of group B (bond pass results): the force and moment on the
-// entry's own particle.
+// entry's own particle.  A bond removed by an earlier update carries zero records.
 template <bool ROT, bool FP32, bool EVAL>
 __device__ __forceinline__ void tile_eval_bonds(const BondDev& B, int Eb, int m, long long step,
                                                 TileSmem<FP32, EVAL>& S) {
   for (int u = threadIdx.x; u < m; u += kTileThreads) {
     const int2 en = __ldg(B.adj + Eb + u);
     const int k = en.y & 0x7fffffff;
-    const bool live = S.alive[S.owner[u]] && B.broken_step[k] > step;  // not removed by an earlier update
+    const bool live = S.alive[S.owner[u]];
     if (live) {
-      const double4* r = B.bf + 3 * (size_t)k;
       const bool isp1 = en.y < 0;
-      const double4 f = ldg4(r);
-      const V F = isp1 ? xyz(f) : -1.0 * xyz(f);
+      V F, M = mk(0.0, 0.0, 0.0);
+      if constexpr (FP32 && !EVAL) {
+        const float4* rf = B.bf32 + 4 * (size_t)k + (isp1 ? 0 : 2);
+        const float4 a0 = __ldg(rf), a1 = __ldg(rf + 1);
+        F = mk((double)a0.x, (double)a0.y, (double)a0.z);
+        if (ROT) M = mk((double)a0.w, (double)a1.x, (double)a1.y);
+      } else {
+        const double4* r = B.bf + 3 * (size_t)k;
+        const double4 f = ldg4(r);
+        F = isp1 ? xyz(f) : -1.0 * xyz(f);
+        if (ROT) M = xyz(ldg4(r + (isp1 ? 1 : 2)));
+      }
       S.c.bond.f[0][u] = F.x;
       S.c.bond.f[1][u] = F.y;
       S.c.bond.f[2][u] = F.z;
       if (ROT) {
-        const double4 mm = ldg4(r + (isp1 ? 1 : 2));
-        S.c.bond.m[0][u] = mm.x;
-        S.c.bond.m[1][u] = mm.y;
-        S.c.bond.m[2][u] = mm.z;
+        S.c.bond.m[0][u] = M.x;
+        S.c.bond.m[1][u] = M.y;
+        S.c.bond.m[2][u] = M.z;
       }
-      if constexpr (EVAL) S.g[u] = norm(xyz(f));
+      if constexpr (EVAL) S.g[u] = norm(F);
     }
     S.live[u] = live ? 1 : 0;
   }
