@@ -1,17 +1,20 @@
-"""Benchmark of the B200 DEM step on the rotational frictional shear cell.
+"""Benchmark of the B200 DEM step on the rotational frictional shear cell, with legs for the
+other workloads of the per-timestep hot path.
 
-Workload (the headline configuration): 250,000 RotSpheres, lognormal radii
-(median 0.5, sigma 0.25, clipped to [0.2, 1.0]) packed by seeded random
-sequential insertion into a 100 x 50 x 100 box periodic in x; RotFriction
-kn = ks = 1e4, mu = 0.6; elastic walls (k = 1e4) at y = 0 and y = 50 moving at
--/+0.01 in x with a 1e3 normal-load servo on the top wall; dt = 5e-5.
-Initial velocities and spins are seeded N(0, 0.1) so that contacts form.
+Headline workload: 250,000 RotSpheres, lognormal radii (median 0.5, sigma 0.25, clipped to
+[0.2, 1.0]) packed by seeded random sequential insertion into a 100 x 50 x 100 box periodic
+in x; RotFriction kn = ks = 1e4, mu = 0.6; elastic walls (k = 1e4) at y = 0 and y = 50 moving
+at -/+0.01 in x with a 1e3 normal-load servo on the top wall; dt = 5e-5.  Initial velocities
+and spins are seeded N(0, 0.1) so that contacts form.
 
-One bench "step" = --dem-steps timesteps (runOneStep x S) plus one servo
-call.  `value` is contact-updates/s (Verlet-list pairs + wall candidates
-evaluated per timestep) with the state resident in HBM; `e2e` repeats it
-through the C ABI with the particle state copied host->device before and
-device->host after every bench step.  L2 is flushed between bench steps.
+One bench "step" = --dem-steps timesteps (runOneStep x S) plus one servo call.  `value` is
+contact-updates/s (Verlet-list pairs + wall candidates evaluated per timestep) with the state
+resident in HBM; `e2e` repeats it through the C ABI with the particle state copied
+host->device before and device->host after every bench step.  L2 is flushed between bench
+steps.  Legs: the 8,000-sphere gravity packing (FP64), the 1,000,000-sphere bonded block
+(FP32-force and FP64 forms), the NRotFriction law on the headline packing, the
+differentiable calibration window and the batched ensemble of bonded cylinders, each beside
+the reference's own C++ timed on this host's cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 """
@@ -36,24 +39,25 @@ METRIC = "contact-updates/s at <=1e-5 rel force err vs FP64"
 UNIT = "contact-updates/s"
 
 
-def workload(n=250_000, seed=2):
-    """Seeded C2 packing through the library's RSI packer (esys_geometry.h)."""
-    from esys.lsm import _capi
+def product_rsi(seed, n, bmin, bmax, periodic_x, dist, p0, p1, rmin, rmax, max_attempts):
+    """The seeded RSI packer of the product library (include/esys_geometry.h)."""
+    from esys.lsm import geometry as G
 
-    lib = _capi.load_library()
-    f = lib.lsm_pack_rsi
-    D = C.POINTER(C.c_double)
-    f.argtypes = [C.c_ulonglong, C.c_int, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
-                  C.c_int, D, D]
-    f.restype = C.c_int
-    pos = np.zeros((n, 3))
-    rad = np.zeros(n)
+    kw = {"lognormal": (p0, p1)} if dist == 1 else {"uniform": (p0, p1)}
+    return G.rsi_pack(n, bmin, bmax, seed=seed, periodic_x=bool(periodic_x), rmin=rmin, rmax=rmax,
+                      max_attempts=max_attempts, **kw)
+
+
+def workload(n=250_000, seed=2, packer=None):
+    """Seeded shear-cell packing.  `packer` is the RSI packer to use (the product library's by
+    default; the reference arm passes the same packer linked into the reference library, so it
+    loads no product code): both give the same spheres for the same seed."""
+    packer = packer or product_rsi
     bmin = np.array([0.0, 0.0, 0.0])
     bmax = np.array([100.0, 50.0, 100.0])
-    k = f(seed, n, bmin.ctypes.data_as(D), bmax.ctypes.data_as(D), 1, 1, 0.5, 0.25, 0.2, 1.0, 5000,
-          pos.ctypes.data_as(D), rad.ctypes.data_as(D))
-    if k != n:
-        raise RuntimeError(f"packer placed {k} of {n} spheres")
+    pos, rad = packer(seed, n, bmin, bmax, 1, 1, 0.5, 0.25, 0.2, 1.0, 5000)
+    if len(rad) != n:
+        raise RuntimeError(f"packer placed {len(rad)} of {n} spheres")
     rng = np.random.default_rng(seed + 100)
     vel = rng.normal(0.0, 0.1, size=(n, 3))
     angvel = rng.normal(0.0, 0.1, size=(n, 3))
@@ -62,6 +66,8 @@ def workload(n=250_000, seed=2):
                 ids=np.arange(n, dtype=np.int32))
 
 
+HEADLINE_WORKLOAD = ("rot-friction shear cell: 250,000 RotSpheres, lognormal r (0.5, 0.25) in [0.2,1.0], 100x50x100, "
+                     "kn=ks=1e4 mu=0.6, 2 elastic walls +-0.01 x, 1e3 servo load, dt=5e-5")
 DT = 5e-5
 GRID, SKIN = 2.2, 0.2
 KN = KS = 1e4
@@ -245,15 +251,20 @@ def window_target(R, seed=4):
     return np.abs(R).max() * rng.uniform(0.5, 1.0, size=(1, R.shape[1], 3)) * t * np.sign(R.mean(axis=0) + 1e-300)
 
 
-def adjoint_leg(stream):
-    """Forward window + reverse sweep on the C4-style bonded block; adjoint grads/s vs the
-    central-difference alternative (two forward windows per gradient component)."""
+def adjoint_leg(stream, precision=32):
+    """Forward window + reverse sweep on the C4-style bonded block in the FP32-force form (FP32
+    pair forces in the forward and its recompute, FP64 reverse); adjoint grads/s vs the
+    central-difference alternative (two forward windows per gradient component), and the
+    adjoint gradients of kn, ks, kt, kb, the linear and rotational damping and three initial
+    velocity components against FP64 central differences (h = 1e-6 relative; the best of
+    h = 1e-6, 1e-5, 1e-4 is reported beside it, as a 2,000-step loaded window carries FP64
+    rounding noise in its loss)."""
     from esys.lsm import _capi
 
     w = window_workload()
     sim = window_setup(lambda *a: _capi.DemSim(*a), w)
     sim.set_stream(stream.cuda_stream)
-    sim.set_option("precision", 64)
+    sim.set_option("precision", precision)
     sim.step(1)  # set-up step (first neighbour search), not part of the window
     n = sim.num_particles()
     t0 = time.perf_counter()
@@ -264,40 +275,100 @@ def adjoint_leg(stream):
     g = sim.window_adjoint(gR)
     t2 = time.perf_counter()
     loss0 = float(((R - tgt) ** 2).mean())
-    # a plain forward window (the unit cost of a finite difference)
     sim.window_rewind()
     t3 = time.perf_counter()
-    sim.window_forward(W_STEPS, W_STEPS)
+    sim.window_forward(W_STEPS, W_STEPS)  # a plain forward window: the unit cost of a difference
     t4 = time.perf_counter()
-    # central difference of the loss in normalK at h = 1e-6 relative, beside the adjoint's value
     layout = sim.param_layout()
-    slot = layout.index(("bonds", "normalK"))
-    losses = []
-    for sgn in (1, -1):
-        sim.window_rewind()
-        sim.set_group_param("bonds", "normalK", W_KN * (1 + sgn * 1e-6))
-        r = sim.window_forward(W_STEPS, W_STEPS)
-        losses.append(float(((r - tgt) ** 2).mean()))
-    sim.window_rewind()
-    sim.set_group_param("bonds", "normalK", W_KN)
-    g_fd = (losses[0] - losses[1]) / (2e-6 * W_KN)
+    sim.close()
+
+    # FP64 central differences on a second handle of the same block
+    ref = window_setup(lambda *a: _capi.DemSim(*a), w)
+    ref.set_stream(stream.cuda_stream)
+    ref.set_option("precision", 64)
+    ref.step(1)
+    # the FP64 form's own adjoint of the same window, beside the FP32 form's
+    R64 = ref.window_forward(W_STEPS, W_CKPT)
+    g64 = ref.window_adjoint(2.0 * (R64 - tgt) / R64.size)
+    ref.window_rewind()
+    p0 = ref.particles()
+    base_vals = ref.param_values()
+    loss_base = float(((R64 - tgt) ** 2).mean())
+
+    def mse(r):
+        return float(((r - tgt) ** 2).mean())
+
+    def loss_param(slot, x):
+        group, key = ref.param_layout()[slot]
+        ref.window_rewind()
+        ref.set_group_param(group, key, x)
+        r = ref.window_forward(W_STEPS, W_STEPS)
+        ref.window_rewind()
+        ref.set_group_param(group, key, base_vals[slot])
+        return mse(r)
+
+    def loss_vel(row, c, x):
+        ref.window_rewind()
+        v = p0["vel"].copy()
+        v[row, c] = x
+        ref.set_particles(vel=v, id=p0["id"])
+        r = ref.window_forward(W_STEPS, W_STEPS)
+        ref.window_rewind()
+        ref.set_particles(vel=p0["vel"], id=p0["id"])
+        return mse(r)
+
+    def central(f, base, g_adj, g_adj64):
+        """Central differences at h = 1e-6 ... 1e-2 relative.  The second difference
+        |L(x+h) + L(x-h) - 2 L(x)| bounds the loss's rounding noise at that h (its curvature term
+        is far smaller); a difference is resolved when it exceeds 100x that noise over 2h."""
+        rows = {}
+        for rel in (1e-6, 1e-5, 1e-4, 1e-3, 1e-2):
+            h = rel * max(abs(base), 1e-12)
+            lp, lm = f(base + h), f(base - h)
+            fd = (lp - lm) / (2 * h)
+            noise = abs(lp + lm - 2.0 * loss_base) / (2 * h)
+            rows[rel] = {"fd": fd, "noise": noise, "resolved": abs(fd) > 100.0 * noise,
+                         "rel_err": abs(g_adj - fd) / max(abs(fd), 1e-300),
+                         "rel_err_fp64_adjoint": abs(g_adj64 - fd) / max(abs(fd), 1e-300)}
+        res = [r for r in rows.values() if r["resolved"]] or list(rows.values())
+        best = min(res, key=lambda r: r["rel_err"])
+        return {"adjoint": float(g_adj), "adjoint_fp64": float(g_adj64), "central_difference": rows[1e-6]["fd"],
+                "rel_err": rows[1e-6]["rel_err"], "resolved_at_1e-6": rows[1e-6]["resolved"],
+                "best_rel_err": best["rel_err"], "best_rel_err_fp64_adjoint": min(r["rel_err_fp64_adjoint"] for r in res),
+                "resolved_h_rel": [k for k, r in rows.items() if r["resolved"]]}
+
+    checks = {}
+    for group, key in (("bonds", "normalK"), ("bonds", "shearK"), ("bonds", "torsionK"), ("bonds", "bendingK"),
+                       ("Damping", "viscosity"), ("RotDamping", "viscosity")):
+        slot = layout.index((group, key))
+        checks[f"{group}.{key}"] = central(lambda x, s_=slot: loss_param(s_, x), base_vals[slot], g["params"][slot],
+                                           g64["params"][slot])
+    # the three initial velocity components the loss depends on most (rows sorted by id)
+    gv = g["vel"]
+    for flat in np.argsort(-np.abs(gv).ravel())[:3]:
+        row, c = divmod(int(flat), 3)
+        checks[f"vel[id {int(p0['id'][row])}][{'xyz'[c]}]"] = central(
+            lambda x, r_=row, c_=c: loss_vel(r_, c_, x), p0["vel"][row, c], gv[row, c], g64["vel"][row, c])
+    ref.close()
     grads = len(g["params"]) + 3 * n  # parameters and initial linear velocities (spins come too, uncounted)
     t_adj = t2 - t0
     t_fwd = t4 - t3
     bonds = len(w["i1"])
-    sim.close()
     return {
         "workload": f"bonded block: {n} RotSpheres fitted in 40x80x40 (r in [0.2,1.0]), {bonds} RotBonds "
                     f"(kn=ks=1e5, kt=kb=1e3, elastic regime), 2 elastic platens at 1.0/s, linear+rotational "
                     f"damping 0.05, dt=1e-5, {W_STEPS}-step window, checkpoints every {W_CKPT}",
         "loss": "MSE of the platen reaction histories vs a seeded ramp target", "loss_value": loss0,
-        "dtype": "f64", "gradient_components": grads,
+        "dtype": ("f32-forces/f64-integration forward and recompute, f64 reverse" if precision == 32 else "f64"),
+        "gradient_components": grads,
         "forward_with_checkpoints_s": t1 - t0, "reverse_sweep_s": t2 - t1, "plain_forward_s": t_fwd,
         "adjoint_grads_per_s": grads / t_adj, "fd_grads_per_s": 1.0 / (2.0 * t_fwd),
         "adjoint_vs_fd_speedup": (grads / t_adj) / (1.0 / (2.0 * t_fwd)),
-        "fd_check": {"param": "bonds.normalK", "h_rel": 1e-6, "adjoint": float(g["params"][slot]),
-                     "central_difference": g_fd,
-                     "rel_err": abs(float(g["params"][slot]) - g_fd) / max(abs(g_fd), 1e-300)},
+        "fd_checks": checks,
+        "fd_max_rel_err_resolved_1e-6": max([c["rel_err"] for c in checks.values() if c["resolved_at_1e-6"]],
+                                            default=None),
+        "fd_max_best_rel_err": max(c["best_rel_err"] for c in checks.values()),
+        "fd_max_best_rel_err_fp64_adjoint": max(c["best_rel_err_fp64_adjoint"] for c in checks.values()),
     }
 
 
@@ -425,6 +496,228 @@ def nrot_friction_leg(stream, steps=1000, ref_steps=20):
     }
 
 
+# ---- gravity packing (8,000 NRotSpheres, FP64) --------------------------------------------
+G_DT, G_STEPS = 1e-4, 5000
+
+
+def gravity_world(n_side=20, layers=20, seed=1):
+    """8,000 NRotSpheres on a 20 x 20 x 20 cubic lattice (spacing 1, jitter U(-0.05, 0.05)) in
+    the lower half of a 20 x 20 x 40 box, radii U[0.4, 0.5], density 1."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(n_side), np.arange(n_side), np.arange(layers), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g + 0.5) + rng.uniform(-0.05, 0.05, size=g.shape)
+    rad = rng.uniform(0.4, 0.5, size=len(g))
+    return dict(pos=pos, rad=rad, L=float(n_side), H=2.0 * layers)
+
+
+def gravity_sim(make, w):
+    """NRotElastic k = 1000 (scaled), gravity -9.81 z, linear damping 0.01, six elastic walls
+    k = 1000 on the box faces; gridSpacing 1.2, verletDist 0.2, dt = 1e-4."""
+    L, H = w["L"], w["H"]
+    n = len(w["rad"])
+    sim = make("NRotSphere", 1.2, 0.2, (0, 0, 0), (L, L, H), (0, 0, 0), G_DT)
+    sim.add_particles(np.arange(n, dtype=np.int32), w["pos"], w["rad"], (4.0 / 3.0) * PI_REF * w["rad"] ** 3,
+                      tag=np.zeros(n, np.int32))
+    sim.add_elastic_group("elastic", 1000.0, True)
+    sim.add_gravity("gravity", (0, 0, -9.81))
+    sim.add_damping(0, 0.01, 100)
+    for name, o, nrm in (("xlo", (0, 0, 0), (1, 0, 0)), ("xhi", (L, 0, 0), (-1, 0, 0)),
+                         ("ylo", (0, 0, 0), (0, 1, 0)), ("yhi", (0, L, 0), (0, -1, 0)),
+                         ("zlo", (0, 0, 0), (0, 0, 1)), ("zhi", (0, 0, H), (0, 0, -1))):
+        sim.add_wall(name, o, nrm)
+        sim.add_wall_group(name + "_w", name, 1000.0)
+    return sim
+
+
+def timed_run(sim, stream, steps):
+    """steps timesteps of a library handle on `stream`, timed with CUDA events; returns the
+    device milliseconds and the handle's counters before and after."""
+    import torch
+
+    torch.cuda.synchronize()
+    c0 = sim.counters()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), c0, sim.counters()
+
+
+def cpu_sample(sim, budget_s, max_steps, before=None):
+    """Timesteps of a CPU harness within a time budget (after its first, set-up step);
+    `before` runs ahead of every timestep (a pre-step runnable)."""
+    if before:
+        before()
+    sim.step(1)
+    done, t0 = 0, time.perf_counter()
+    while done < max_steps and time.perf_counter() - t0 < budget_s:
+        if before:
+            before()
+        sim.step(1)
+        done += 1
+    return done, time.perf_counter() - t0
+
+
+def gravity_leg(stream, cpu=True, cpu_budget=20.0):
+    """The plain-FP64 gravity packing over its full 5,000 steps on the GPU, beside the
+    reference's own C++ (one core) on the same spheres."""
+    from esys.lsm import _capi
+
+    w = gravity_world()
+    sim = gravity_sim(lambda *a: _capi.DemSim(*a), w)
+    sim.set_stream(stream.cuda_stream)
+    sim.set_option("profile", 1)
+    sim.set_option("precision", 64)
+    sim.step(1)  # set-up: first neighbour search
+    ms, c0, c1 = timed_run(sim, stream, G_STEPS)
+    n = len(w["rad"])
+    cu = c1["contact_updates"] - c0["contact_updates"]
+    kus = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / max(1, c1["profiled_steps"] - c0["profiled_steps"]) / 1e3
+    m = len(sim.pairs("elastic")[0])
+    touching = int(np.sum(sim.interaction_scalar_field("elastic", "count")[2]))
+    walls = c1["contacts_per_step"] - m
+    alg = n * 136 + m * 8 + walls * 4
+    sim.close()
+    out = {
+        "workload": "gravity packing: 8,000 NRotSpheres (20x20x20 jittered lattice, r in [0.4,0.5]) in a 20x20x40 "
+                    "box, NRotElastic k=1000, gravity -9.81 z, linear damping 0.01, 6 elastic walls k=1000, dt=1e-4",
+        "metric": "contact-updates/s", "value": cu / (ms / 1e3), "dtype": "f64", "timesteps": G_STEPS,
+        "timesteps_per_s": G_STEPS / (ms / 1e3), "ms_total": ms, "kernel_us": kus,
+        "elastic_pairs": m, "wall_candidates": walls, "touching_pairs_end": touching,
+        "roofline": {"bound": "hbm", "achieved_gbs": alg / (kus * 1e-6) / 1e9 if kus > 0 else None,
+                     "algorithmic_bytes_per_timestep": alg,
+                     "note": "8,000 spheres: the step is launch- and latency-bound, far below HBM bandwidth"},
+        "cpu_reference": None,
+    }
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        if oracle.available("ref"):
+            r = gravity_sim(lambda *a: oracle.OracleSim("ref", *a), w)
+            done, dt = cpu_sample(r, cpu_budget, G_STEPS)
+            m_r = r.f["num_pairs"](r.h, b"elastic")
+            out["cpu_reference"] = {"value": (m_r + walls) * done / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": f"{done} of the {G_STEPS} timesteps after set-up"}
+            out["speedup_vs_cpu_reference"] = out["value"] / out["cpu_reference"]["value"]
+    return out
+
+
+# ---- bonded block (1,000,000 RotSpheres) ------------------------------------------------------
+B_DT = 1e-5
+
+
+def block_world(n=1_000_000, seed=3):
+    """The fitting packer's 1M spheres (radii in [0.2, 1.0]) in 66 x 132 x 66 (the 100 x 200 x 100
+    prism of the spec holds 1M spheres only at uniform radii), every pair within a 1e-3 gap bonded."""
+    from esys.lsm import geometry as G
+
+    pos, rad = G.fit_pack(n, (0, 0, 0), (66, 132, 66), 0.2, 1.0, seed=seed, max_failures=300)
+    i1, i2 = G.distance_connections(pos, rad, 1e-3)
+    return dict(pos=pos, rad=rad, i1=i1, i2=i2)
+
+
+def block_sim(make, w, loader=True):
+    """RotBond kn = ks = 1e5, kt = kb = 1e3, brittle strengths 0.5 / 1.0 / 1.0 / 0.5 (normal /
+    shear / torsion / bending); RotFriction (same stiffness, mu 0.6) for post-failure contacts with
+    the bond exclusion; elastic platens (k = 1e5) loading at a strain rate of 1e-4 per 1,000
+    steps split between them; dt = 1e-5."""
+    pos, rad = w["pos"], w["rad"]
+    n = len(rad)
+    s = make("RotSphere", 2.2, 0.2, (0, 0, 0), (66, 132, 66), (0, 0, 0), B_DT)
+    s.add_particles(np.arange(n, dtype=np.int32), pos, rad, (4.0 / 3.0) * PI_REF * rad ** 3,
+                    tag=np.zeros(n, np.int32))
+    s.add_connections(np.ones(len(w["i1"]), np.int32), w["i1"], w["i2"])
+    s.add_rot_bond_group("bonds", 1, 1e5, 1e5, 1e3, 1e3, 0.5, 1.0, 1.0, 0.5, True, True, 1.0)
+    s.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, B_DT, True, True)
+    s.add_exclusion("bonds", "friction")
+    y0, y1 = float((pos[:, 1] - rad).min()), float((pos[:, 1] + rad).max())
+    s.add_wall("bottom", (0, y0, 0), (0, 1, 0))
+    s.add_wall("top", (0, y1, 0), (0, -1, 0))
+    s.add_wall_group("bottom_w", "bottom", 1e5)
+    s.add_wall_group("top_w", "top", 1e5)
+    v = 0.5 * 1e-4 * (y1 - y0) / 1000 / B_DT
+    if loader:  # the library's native wall loader (WallLoaderRunnable)
+        s.set_wall_velocity("bottom", (0, v, 0))
+        s.set_wall_velocity("top", (0, -v, 0))
+    s.platen_step = v * B_DT  # per-step platen displacement, for a harness without a native loader
+    return s
+
+
+def bonded_block_leg(stream, steps=200, warm=20, cpu=True, cpu_budget=15.0):
+    """The 1M-sphere bonded block in both precision forms (device bond hand-off on; the FP32 form
+    on the tiled kernels, which measured fastest on this dense pack), with the reference's own C++
+    (one core) on a bounded sample of the same block."""
+    from esys.lsm import _capi
+
+    t0 = time.perf_counter()
+    w = block_world()
+    t_pack = time.perf_counter() - t0
+    n = len(w["rad"])
+    forms = {}
+    for prec, tpp in ((32, 16), (64, 0)):
+        sim = block_sim(lambda *a: _capi.DemSim(*a), w)
+        sim.set_stream(stream.cuda_stream)
+        sim.set_option("profile", 1)
+        sim.set_option("precision", prec)
+        sim.set_option("bond_handoff", 1)
+        if tpp:
+            sim.set_option("threads_per_particle", tpp)
+        sim.step(warm)
+        ms, c0, c1 = timed_run(sim, stream, steps)
+        cu = c1["contact_updates"] - c0["contact_updates"]
+        kus = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / max(1, c1["profiled_steps"] - c0["profiled_steps"]) / 1e3
+        nb = sim._chk(sim.lib.dem_num_pairs(sim.h, b"bonds"))
+        mf = sim._chk(sim.lib.dem_num_pairs(sim.h, b"friction"))
+        walls = c1["contacts_per_step"] - nb - mf
+        st = sim.pairs("friction")[2]
+        touching = int(st[:, 4].sum()) if len(st) else 0
+        alg = n * 256 + nb * 32 + mf * (36 if prec == 32 else 60) + walls * 4
+        forms[f"fp{prec}"] = {
+            "value": cu / (ms / 1e3), "timesteps_per_s": steps / (ms / 1e3), "ms_per_timestep": ms / steps,
+            "device_us_per_timestep": kus, "threads_per_particle": c1["threads_per_particle"],
+            "intact_bonds": nb, "friction_pairs": mf, "touching_friction_pairs": touching, "wall_candidates": walls,
+            "bond_breaks": int(len(sim.breaks()[0])),
+            "roofline": {"bound": "hbm", "achieved": alg / (kus * 1e-6) / 1e9, "unit": "GB/s",
+                         "algorithmic_bytes_per_timestep": alg,
+                         "kernels": "bond pass + step kernel per timestep (device time between CUDA events)"},
+        }
+        sim.close()
+    peak, _ = peaks()
+    for f in forms.values():
+        f["roofline"]["frac"] = f["roofline"]["achieved"] / peak
+    out = {
+        "workload": f"bonded block: {n} RotSpheres fitted in 66x132x66 (r in [0.2,1.0]), {len(w['i1'])} RotBonds "
+                    f"(kn=ks=1e5, kt=kb=1e3, strengths 0.5/1.0/1.0/0.5), RotFriction + exclusion, platens at "
+                    f"strain rate 1e-4 per 1,000 steps, dt=1e-5, device bond hand-off",
+        "metric": "contact-updates/s", "timed_timesteps": steps, "warmup_timesteps": warm, "pack_s": t_pack,
+        "forms": forms, "fp32_vs_fp64": forms["fp32"]["value"] / forms["fp64"]["value"], "cpu_reference": None,
+    }
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        if oracle.available("ref"):
+            t0 = time.perf_counter()
+            r = block_sim(lambda *a: oracle.OracleSim("ref", *a), w, loader=False)
+            t_set = time.perf_counter() - t0
+            d = r.platen_step
+
+            def load():  # the wall-loader runnable's moveWallBy ahead of each step
+                r.move_wall("bottom", (0, d, 0))
+                r.move_wall("top", (0, -d, 0))
+
+            done, dt = cpu_sample(r, cpu_budget, 50, before=load)
+            m_r = r.f["num_pairs"](r.h, b"friction") + r.f["num_pairs"](r.h, b"bonds")
+            cand = forms["fp64"]["wall_candidates"]
+            out["cpu_reference"] = {"value": (m_r + cand) * done / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": f"{done} timesteps after set-up ({t_set:.0f} s) of the same block"}
+            out["speedup_vs_cpu_reference"] = forms["fp32"]["value"] / out["cpu_reference"]["value"]
+            del r
+    return out
+
+
 def window_bytes(n, m, nb, T, K):
     """Device bytes of one specimen's window: checkpoints every K of T steps (particle records,
     friction histories, wall candidacy) and the reverse pass's recompute of K + 1 states (records,
@@ -499,9 +792,10 @@ def ensemble_window_leg(sims, tpp, nsteps, every):
     }
 
 
-def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window=200, window_every=20):
-    """FP32-force batched ensemble (autotuned, graph-replayed) vs the plain FP64 GPU form
-    (each specimen stepped by itself).  Under torchrun each rank takes a size-balanced share of
+def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window=200, window_every=20,
+                 fp64_batched_steps=200):
+    """FP32-force batched ensemble (autotuned, graph-replayed) vs the FP64 batched ensemble and
+    the plain FP64 GPU form (each specimen stepped by itself), separating precision from batching.  Under torchrun each rank takes a size-balanced share of
     the specimens (no exchange while they run); counts are summed and times maxed at the end."""
     from concurrent.futures import ThreadPoolExecutor
 
@@ -562,6 +856,31 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
             adj = {"failed": str(x)}
     for s in sims:
         s.close()
+    # FP64 batched: the same specimens from their initial state, the ensemble in the FP64 form
+    sims64 = [cylinder_sim(make, sp, best["grid_spacing"], best["verlet_dist"]) for sp in specs]
+    for s in sims64:
+        s.set_option("precision", 64)
+    e64 = _capi.Ensemble(sims64)
+    e64.set_option("threads_per_particle", best["threads_per_particle"])
+    e64.step(100)  # warm-up as above
+    if dist is not None:
+        torch.cuda.synchronize()
+        dist.barrier()
+    b0 = e64.counters()
+    t0 = time.perf_counter()
+    e64.step(fp64_batched_steps)
+    t_b64 = time.perf_counter() - t0
+    c_b64 = float(e64.counters()["contact_updates"] - b0["contact_updates"])
+    e64.close()
+    for s in sims64:
+        s.close()
+    if dist is not None:
+        tt = torch.tensor([t_b64, c_b64], device="cuda", dtype=torch.float64)
+        t_max = tt[:1].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
+        t_b64, c_b64 = float(t_max.item()), float(tt[1].item())
+    batched64 = c_b64 / t_b64
     # plain FP64 GPU form: a size-stratified sample of the specimens, each stepped alone
     nloc = len(specs)
     idx = np.argsort([sp["n"] for sp in specs])[np.linspace(0, nloc - 1, min(max(1, fp64_sample // world), nloc)).astype(int)]
@@ -599,32 +918,58 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
                                                       f"{fp64_steps} steps each, one dem_step per specimen"},
         "scaling": "weak over specimens: each GPU advances its size-balanced share, no exchange" if world > 1
                    else "single GPU",
+        "fp64_batched": {"value": batched64, "steps": fp64_batched_steps,
+                         "sample": "the same specimens from their initial state, batched in the FP64 form"},
         "speedup_vs_plain_fp64": value / plain,
+        "fp32_batched_vs_fp64_batched": value / batched64,
+        "fp64_batched_vs_plain_fp64": batched64 / plain,
         "batched_adjoint": adj,
     }
 
 
 def run_reference_arm(args):
+    """The reference's own C++ (oracle/_ref: ESyS-Particle's hot-path classes compiled from its
+    sources, one worker = one core) on the headline packing, through the same steps and
+    warm-up counts as the GPU arm; one "step" here is one timestep (a bounded sample of the
+    GPU arm's --dem-steps).  The packing comes from the packer linked into the reference
+    library, so this arm maps no product library.  Periodic x needs >= 2 MPI workers in the
+    reference, so it runs the same particles and groups in a non-periodic box."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = workload()
-    res = cpu_reference_sample(w, steps=max(1, args.steps + args.warmup), timeout_s=180.0)
-    if res is None:
-        print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.available("ref"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
         return
+    w = workload(packer=oracle.rsi_pack_ref)
+    sim = setup(lambda *a: oracle.OracleSim("ref", *a), w, periodic=False)
+    sim.step(1)  # first step: neighbour search + interaction set-up (not timed)
+    m = sim.f["num_pairs"](sim.h, b"friction")
+    pos = w["pos"]
+    ncand = int((np.abs(pos[:, 1] - 0.0) < GRID).sum() + (np.abs(pos[:, 1] - 50.0) < GRID).sum())
+    for _ in range(args.warmup):
+        sim.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(1)
+    dt = time.perf_counter() - t0
+    value = (m + ncand) * args.steps / dt
     line = {
-        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": res["steps"],
-        "warmup": 1, "ms_per_step": 1e3 * res["seconds"] / res["steps"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RSI packing)",
         "impl": "reference",
-        "config": {"workload": "rot-friction shear cell, 250k RotSpheres, 100x50x100 (x periodic on the GPU path; "
-                               "the reference needs >=2 MPI workers for periodic x, so it runs non-periodic)",
-                   "dem_steps_per_step": 1},
-        "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": f"{res['steps']} timesteps of the 250k-sphere packing after set-up, "
-                                   f"{res['pairs']} friction pairs + {res['walls']} wall candidates"},
-        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": HEADLINE_WORKLOAD, "particles": len(w["ids"]),
+                   "periodic_x": False,
+                   "reference_note": "the reference needs >= 2 MPI workers for periodic x; one worker runs the "
+                                     "same particles and groups non-periodic",
+                   "timesteps_per_step": 1},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} timesteps after {args.warmup} warm-up timesteps of the "
+                                   f"250k-sphere packing, {m} friction pairs + {ncand} wall candidates"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
@@ -650,6 +995,9 @@ def main():
     ap.add_argument("--ensemble-window-every", type=int, default=20, help="checkpoint interval of that window")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
                     help="step kernels: -1 automatic, 0 fused, 1 pair kernel + integration kernel")
+    ap.add_argument("--no-gravity", action="store_true", help="skip the 8,000-sphere gravity-packing leg")
+    ap.add_argument("--no-block", action="store_true", help="skip the 1M-sphere bonded-block leg")
+    ap.add_argument("--block-steps", type=int, default=200, help="timed timesteps of the bonded-block leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -730,6 +1078,8 @@ def main():
         err = sim.precision_report()
         sim.set_option("precision", 32)
     contacts = c1["contact_updates"] - c0["contact_updates"]
+    fst = sim.pairs("friction")[2]
+    touching = int(fst[:, 4].sum()) if len(fst) else 0  # touching RotFriction pairs after the timed steps
     t_max = ms
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
@@ -751,7 +1101,12 @@ def main():
     alg_bytes = n * 256 + m_fric * (36 if args.precision == 32 else 60) + n_wall_cand * 4
     achieved = alg_bytes / (step_ns * 1e-9) / 1e9
     peak, peak_kind = peaks()
+    tpp_used = c1["threads_per_particle"]
+    kernel_name = (f"k_step<ROT=1, TPP={tpp_used}, FRIC, {'FP32' if args.precision == 32 else 'FP64'}>"
+                   if tpp_used != 16 else f"k_step_tiled<ROT=1, FRIC, {'FP32' if args.precision == 32 else 'FP64'}>")
     traffic = traffic_per_launch()
+    # the ncu capture's traffic counts only for the same kernel instance
+    traffic_bytes = traffic["bytes_per_launch"] if traffic and traffic.get("kernel", "").startswith(kernel_name) else None
 
     # e2e through the C ABI with host buffers (pinned), H2D + D2H inside the timed region
     pin = {k: torch.empty((n, wdt), dtype=torch.float64).pin_memory() for k, wdt in
@@ -790,6 +1145,12 @@ def main():
     nrot = None
     if not args.no_widened and world == 1:
         nrot = nrot_friction_leg(stream)
+    grav = None
+    if not args.no_gravity and world == 1:
+        grav = gravity_leg(stream, cpu=not args.no_cpu_baseline)
+    block = None
+    if not args.no_block and world == 1:
+        block = bonded_block_leg(stream, steps=args.block_steps, cpu=not args.no_cpu_baseline)
     ens = None
     if args.ensemble_specimens > 0:
         ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps, dist=dist, window=args.ensemble_window,
@@ -809,33 +1170,36 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32-forces/f64-integration" if args.precision == 32 else "f64",
             "data": "synthetic (seeded RSI packing)",
-            "config": {"workload": "rot-friction shear cell: 250,000 RotSpheres, lognormal r (0.5, 0.25) in "
-                                   "[0.2,1.0], 100x50x100 periodic-x, kn=ks=1e4 mu=0.6, 2 elastic walls "
-                                   "+-0.01 x, 1e3 servo load, dt=5e-5",
+            "config": {"workload": HEADLINE_WORKLOAD, "periodic_x": True,
                        "dem_steps_per_step": args.dem_steps, "particles": n,
                        "interactions_per_timestep": c1["contacts_per_step"],
+                       "friction_pairs": m_fric, "wall_candidates": n_wall_cand,
+                       "touching_friction_pairs": touching,
                        "threads_per_particle": c1["threads_per_particle"],
-                       "l2": "flushed (256 MB write) between bench steps; working set ~90 MB stays L2-resident "
-                             "within a bench step",
+                       "l2": "flushed (256 MB write) between bench steps; the step's working set (~110 MB) is "
+                             "close to the 126 MB L2, so part of it stays resident between timesteps",
                        "parallelism": "replicas only" if world > 1 else "single GPU",
                        "precision": ("FP32 pair forces (Kahan-compensated), FP64 positions / contact detection / "
                                      "integration" if args.precision == 32 else "FP64 throughout"),
                        "force_error_vs_fp64": err if err is not None else {"max_rel_force_err": 0.0},
                        "fp64_form": fp64},
+            "timesteps_per_s": args.dem_steps * args.steps / (t_max / 1e3),
+            "touching_contact_updates_per_s": value * touching / max(1, c1["contacts_per_step"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (traffic or {}).get("bytes_per_launch"),
-                         "kernel": f"k_step<ROT=1,TPP,FRIC,{'FP32' if args.precision == 32 else 'FP64'}>",
-                         "kernel_us": step_ns / 1e3,
+                         "traffic": traffic_bytes, "traffic_kernel": (traffic or {}).get("kernel"),
+                         "kernel": kernel_name, "kernel_us": step_ns / 1e3,
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": n * (24 + 24 + 24 + 32),
-                    "d2h_bytes_per_step": n * (6 * 32 + 4)},
+                    "d2h_bytes_per_step": n * (4 + 5 * 24 + 32)},
             "gpu_launches": c1["launches"] - c0["launches"],
             "clocks": clk.summary(),
             "adjoint": adj,
             "nrot_friction": nrot,
             "ensemble": ens,
+            "gravity_packing": grav,
+            "bonded_block": block,
         }
         print(json.dumps(line))
     sim.close()

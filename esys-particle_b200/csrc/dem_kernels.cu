@@ -404,6 +404,43 @@ __global__ void k_set_state(Particles P, int cur, int cnt, const int* slots, con
   if (quat) b.qq[i] = make_double4(quat[4 * r], quat[4 * r + 1], quat[4 * r + 2], quat[4 * r + 3]);
 }
 
+// Alive flag of every slot (the rows dem_get_particles returns).
+__global__ void k_alive_flags(Particles P, int* flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P.n) flags[i] = (P.pflags[i] & PF_ALIVE) ? 1 : 0;
+}
+
+// The alive particles' state as host rows (row = rank of the slot among alive slots, or the
+// slot itself when rows is null): id, position, velocity, spin, quaternion, force and moment,
+// each into its own array (null: not wanted).  A non-rotational particle reports zero spin
+// and moment and the identity quaternion.
+__global__ void k_pack_particles(Particles P, int cur, int rot, const int* rows, int* id, double* pos, double* vel,
+                                 double* angvel, double* quat, double* force, double* moment) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n || !(P.pflags[i] & PF_ALIVE)) return;
+  const int r = rows ? rows[i] : i;
+  const ParticleBuf b = P.buf[cur];
+  auto put3 = [&](double* dst, const double4& v, bool zero) {
+    if (!dst) return;
+    dst[3 * (size_t)r] = zero ? 0.0 : v.x;
+    dst[3 * (size_t)r + 1] = zero ? 0.0 : v.y;
+    dst[3 * (size_t)r + 2] = zero ? 0.0 : v.z;
+  };
+  if (id) id[r] = P.id[i];
+  if (pos) put3(pos, b.pr[i], false);
+  if (vel) put3(vel, b.vm[i], false);
+  if (angvel) put3(angvel, b.wi[i], !rot);
+  if (force) put3(force, P.force[i], false);
+  if (moment) put3(moment, P.moment[i], !rot);
+  if (quat) {
+    const double4 q = rot ? b.qq[i] : make_double4(1.0, 0.0, 0.0, 0.0);
+    quat[4 * (size_t)r] = q.x;
+    quat[4 * (size_t)r + 1] = q.y;
+    quat[4 * (size_t)r + 2] = q.z;
+    quat[4 * (size_t)r + 3] = q.w;
+  }
+}
+
 // Displacement check after a host-side move (TSubLattice::checkNeighbors).
 __global__ void k_check_disp(Particles P, int cur, double half_alpha_sq, int* ctrl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -707,6 +744,14 @@ void launch_wall_update(const Grid& g, const Particles& P, int cur, int nwall, c
 void launch_set_state(const Particles& P, int cur, int cnt, const int* slots, const double* pos, const double* vel,
                       const double* angvel, const double* quat, cudaStream_t s) {
   if (cnt) k_set_state<<<nblk(cnt, 256), 256, 0, s>>>(P, cur, cnt, slots, pos, vel, angvel, quat);
+}
+void launch_alive_flags(const Particles& P, int* flags, cudaStream_t s) {
+  if (P.n) k_alive_flags<<<nblk(P.n, 256), 256, 0, s>>>(P, flags);
+}
+void launch_pack_particles(const Particles& P, int cur, int rot, const int* rows, int* id, double* pos, double* vel,
+                           double* angvel, double* quat, double* force, double* moment, cudaStream_t s) {
+  if (P.n)
+    k_pack_particles<<<nblk(P.n, 256), 256, 0, s>>>(P, cur, rot, rows, id, pos, vel, angvel, quat, force, moment);
 }
 void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* ctrl, cudaStream_t s) {
   if (P.n) k_check_disp<<<nblk(P.n, 256), 256, 0, s>>>(P, cur, half_alpha_sq, ctrl);

@@ -133,6 +133,8 @@ struct DemSim {
   int adj_pair_duals = 0;  // adjoint pair-law VJPs: 0 hand-written reverse, 1 forward-mode duals
   DBuf<int> d_brk;       // [2]: last step with a bond failure, by step parity
   DBuf<int> d_servo_idx; // wall servo: candidate lists of its threads (n ints)
+  DBuf<int> rows, pack_id;  // dem_get_particles: row of each alive slot, packed ids
+  DBuf<double> pack;        // dem_get_particles: packed host rows of the wanted fields
   // particles
   int n = 0, cap = 0;
   Particles P{};
@@ -205,7 +207,8 @@ struct DemSim {
     scratch_i.release(); scratch_j.release(); scalars.release(); scan_tmp.release();
     d_walls.release(); d_wall_vel.release(); d_wall_partial.release(); d_wall_force.release();
     d_block_counter.release(); d_step.release(); d_ctrl.release(); d_stop.release();
-    stage.release(); stage_slot.release(); scratch_d.release(); sig.release(); d_servo_idx.release(); d_brk.release();
+    stage.release(); stage_slot.release(); scratch_d.release(); sig.release(); d_servo_idx.release(); d_brk.release(); rows.release(); pack_id.release();
+    pack.release();
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -469,6 +472,41 @@ struct DemSim {
     DEM_CUDA(cudaMemsetAsync(d_ctrl.p, 0, sizeof(int), s));
     c_launches += 2;
     return 0;
+  }
+
+  // The alive particles in slot order into the caller's host arrays (each may be null).  The
+  // rows are packed on the device, then each wanted field is one copy into the caller's array
+  // (direct DMA when the caller's memory is pinned).
+  int get_particles(int* id, double* pos, double* vel, double* angvel, double* quat, double* force, double* moment) {
+    if (!n) return 0;
+    rows.reserve((size_t)n + 1);
+    pack_id.reserve((size_t)n + 1);
+    scan_tmp.reserve(scan_tmp_ints(n + 1));
+    launch_alive_flags(P, pack_id.p, s);  // flags, then the scan's input is free for the ids
+    launch_scan(pack_id.p, rows.p, n, scalars.p + 2, scan_tmp.p, s);
+    const int k = read_int(scalars.p + 2);
+    const int* rp = k == n ? nullptr : rows.p;  // every slot alive: row = slot
+    pack.reserve((size_t)19 * n + 1);
+    double* d = pack.p;
+    const size_t n3 = (size_t)n * 3;
+    double* dpos = pos ? d : nullptr;
+    double* dvel = vel ? d + n3 : nullptr;
+    double* dang = angvel ? d + 2 * n3 : nullptr;
+    double* dfor = force ? d + 3 * n3 : nullptr;
+    double* dmom = moment ? d + 4 * n3 : nullptr;
+    double* dq = quat ? d + 5 * n3 : nullptr;
+    launch_pack_particles(P, cur, rot, rp, id ? pack_id.p : nullptr, dpos, dvel, dang, dq, dfor, dmom, s);
+    const size_t k3 = (size_t)k * 3 * sizeof(double);
+    if (id) DEM_CUDA(cudaMemcpyAsync(id, pack_id.p, sizeof(int) * (size_t)k, cudaMemcpyDeviceToHost, s));
+    if (pos) DEM_CUDA(cudaMemcpyAsync(pos, dpos, k3, cudaMemcpyDeviceToHost, s));
+    if (vel) DEM_CUDA(cudaMemcpyAsync(vel, dvel, k3, cudaMemcpyDeviceToHost, s));
+    if (angvel) DEM_CUDA(cudaMemcpyAsync(angvel, dang, k3, cudaMemcpyDeviceToHost, s));
+    if (quat) DEM_CUDA(cudaMemcpyAsync(quat, dq, (size_t)k * 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (force) DEM_CUDA(cudaMemcpyAsync(force, dfor, k3, cudaMemcpyDeviceToHost, s));
+    if (moment) DEM_CUDA(cudaMemcpyAsync(moment, dmom, k3, cudaMemcpyDeviceToHost, s));
+    sync();
+    c_launches += 3;
+    return k;
   }
 
   // ---- neighbour search (TSubLattice::searchNeighbors, SubLattice.hpp:2395-2408) ----
@@ -2802,41 +2840,7 @@ int dem_num_particles(dem_sim* h) {
 
 int dem_get_particles(dem_sim* h, int* id, double* pos, double* vel, double* angvel, double* quat, double* force,
                       double* moment) {
-  return guard(h, [&](DemSim& s) {
-    const int n = s.n;
-    std::vector<double4> pr(n), vm(n), wi(n), qq(n), f(n), m(n);
-    std::vector<unsigned> pf(n);
-    if (n) {
-      auto dn = [&](void* dst, const void* src, size_t b) { DEM_CUDA(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s.s)); };
-      dn(pr.data(), s.P.buf[s.cur].pr, sizeof(double4) * n);
-      dn(vm.data(), s.P.buf[s.cur].vm, sizeof(double4) * n);
-      dn(wi.data(), s.P.buf[s.cur].wi, sizeof(double4) * n);
-      dn(qq.data(), s.P.buf[s.cur].qq, sizeof(double4) * n);
-      dn(f.data(), s.P.force, sizeof(double4) * n);
-      dn(m.data(), s.P.moment, sizeof(double4) * n);
-      dn(pf.data(), s.P.pflags, sizeof(unsigned) * n);
-    }
-    s.sync();
-    int k = 0;
-    for (int i = 0; i < n; ++i) {
-      if (!(pf[i] & dem::PF_ALIVE)) continue;
-      if (id) id[k] = s.h_id[i];
-      const double4* src[5] = {&pr[i], &vm[i], &wi[i], &f[i], &m[i]};
-      double* dst[5] = {pos, vel, angvel, force, moment};
-      for (int a = 0; a < 5; ++a)
-        if (dst[a]) {
-          double v3[3] = {src[a]->x, src[a]->y, src[a]->z};
-          if ((a == 2 || a == 4) && !s.rot) v3[0] = v3[1] = v3[2] = 0.0;
-          for (int c = 0; c < 3; ++c) dst[a][3 * k + c] = v3[c];
-        }
-      if (quat) {
-        if (s.rot) { quat[4 * k] = qq[i].x; quat[4 * k + 1] = qq[i].y; quat[4 * k + 2] = qq[i].z; quat[4 * k + 3] = qq[i].w; }
-        else { quat[4 * k] = 1.0; quat[4 * k + 1] = quat[4 * k + 2] = quat[4 * k + 3] = 0.0; }
-      }
-      ++k;
-    }
-    return k;
-  });
+  return guard(h, [&](DemSim& s) { return s.get_particles(id, pos, vel, angvel, quat, force, moment); });
 }
 
 int dem_num_pairs(dem_sim* h, const char* group) {

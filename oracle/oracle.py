@@ -6,8 +6,8 @@
 * ``backend="orc"`` loads ``oracle/_build/libesys_oracle.so``: the CPU
   restatement ``oracle/dem_oracle.cpp``, which also covers periodic x.
 
-Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
-use this module; the product path never does.
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline legs and
+reference arm use this module; the product path never does.
 """
 from __future__ import annotations
 
@@ -31,6 +31,26 @@ _S = C.c_char_p
 
 def available(backend: str) -> bool:
     return os.path.exists(_LIBS[backend][0])
+
+
+def rsi_pack_ref(seed, n, bmin, bmax, periodic_x, dist, p0, p1, rmin, rmax, max_attempts):
+    """The benchmarks' seeded RSI packer (``lsm_pack_rsi``, the product's packing.cpp) as
+    linked into the reference library: the same packing without loading the product library.
+    Returns (pos, rad) of the spheres placed."""
+    lib = C.CDLL(_LIBS["ref"][0])
+    f = lib.lsm_pack_rsi
+    f.argtypes = [C.c_ulonglong, C.c_int, _D, _D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.c_int, _D, _D]
+    f.restype = C.c_int
+    pos = np.zeros((n, 3))
+    rad = np.zeros(n)
+    lo = np.ascontiguousarray(bmin, dtype=np.float64)
+    hi = np.ascontiguousarray(bmax, dtype=np.float64)
+    k = f(seed, n, lo.ctypes.data_as(_D), hi.ctypes.data_as(_D), periodic_x, dist, p0, p1, rmin, rmax, max_attempts,
+          pos.ctypes.data_as(_D), rad.ctypes.data_as(_D))
+    if k < 0:
+        raise ValueError("lsm_pack_rsi: bad arguments")
+    return pos[:k], rad[:k]
 
 
 def _lib(backend: str):

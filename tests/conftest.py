@@ -40,8 +40,9 @@ def oracle_libs():
 
     odir = os.path.join(ROOT, "oracle")
     subprocess.run(["make", "-s", "-C", odir, "restate"], check=True)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-j8", "-C", odir, "ref"], check=True)
+    ref = os.environ.get("ESYS_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-j8", "-C", odir, "ref", f"REF={ref}"], check=True)
     import oracle
 
     return oracle

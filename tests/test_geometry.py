@@ -32,3 +32,27 @@ def test_distance_connections_equals_brute_force(dem_lib):
     d = np.linalg.norm(pos[:, None] - pos[None], axis=-1) - rad[:, None] - rad[None]
     bi, bj = np.nonzero(np.triu(d <= 0.3, 1))
     assert np.array_equal(i, bi) and np.array_equal(j, bj)
+
+
+def test_reference_library_packer_equals_product_packer(dem_lib, oracle_libs):
+    """The bench's reference arm builds its packing with the packer linked into the reference
+    library; it must place exactly the product library's spheres."""
+    import ctypes as C
+
+    import pytest
+
+    if not oracle_libs.available("ref"):
+        pytest.skip("reference library not built")
+    D = C.POINTER(C.c_double)
+    f = dem_lib.lsm_pack_rsi
+    f.argtypes = [C.c_ulonglong, C.c_int, D, D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.c_int, D, D]
+    f.restype = C.c_int
+    n = 3000
+    pos, rad = np.zeros((n, 3)), np.zeros(n)
+    lo, hi = np.zeros(3), np.array([30.0, 15.0, 30.0])
+    k = f(7, n, lo.ctypes.data_as(D), hi.ctypes.data_as(D), 1, 1, 0.5, 0.25, 0.2, 1.0, 5000, pos.ctypes.data_as(D),
+          rad.ctypes.data_as(D))
+    pr, rr = oracle_libs.rsi_pack_ref(7, n, lo, hi, 1, 1, 0.5, 0.25, 0.2, 1.0, 5000)
+    assert k == len(rr) > 2000
+    assert np.array_equal(pos[:k], pr) and np.array_equal(rad[:k], rr)
