@@ -84,6 +84,7 @@ struct Particles {
   std::vector<V3> pos, vel, force, oldpos, angvel, moment;
   std::vector<Q> quat;
   std::vector<double> rad, mass, invmass, inert, invinert;
+  std::vector<double> gross_f, gross_m;  /* checker diagnostic: sum of |each force / moment| of the last step */
   std::vector<char> dyn, rot, flag, alive;
   int n() const { return (int)id.size(); }
 };
@@ -290,8 +291,14 @@ static Bond make_bond(const Sim& s, const PairGroup& g, int a, int b) {
 
 /* ---- force laws ------------------------------------------------------------ */
 /* CParticle::applyForce (Model/Particle.cpp:391-400), without the stress tensor */
-static inline void apply_force(Sim& s, int i, const V3& f) { s.P.force[i] += f; }
-static inline void apply_moment(Sim& s, int i, const V3& m) { s.P.moment[i] += m; }
+static inline void apply_force(Sim& s, int i, const V3& f) {
+  s.P.force[i] += f;
+  if (i < (int)s.P.gross_f.size()) s.P.gross_f[i] += norm(f);  /* the checker's force scale, not a force */
+}
+static inline void apply_moment(Sim& s, int i, const V3& m) {
+  s.P.moment[i] += m;
+  if (i < (int)s.P.gross_m.size()) s.P.gross_m[i] += norm(m);
+}
 
 /* CElasticInteraction::calcForces (Model/ElasticInteraction.cpp:54-71) */
 static void calc_elastic(Sim& s, Elastic& e) {
@@ -664,6 +671,8 @@ static void update_interactions(Sim& s) {
 /* TSubLattice::oneStep (SubLattice.hpp:2066-2236): zero, calcForces in group order, integrate, rescale */
 static void one_step(Sim& s) {
   for (int i = 0; i < s.P.n(); ++i) { s.P.force[i] = V3(0, 0, 0); s.P.moment[i] = V3(0, 0, 0); }
+  s.P.gross_f.assign(s.P.n(), 0.0);
+  s.P.gross_m.assign(s.P.n(), 0.0);
   for (auto& w : s.walls) w.second.F = V3(0, 0, 0);
   for (auto& wg : s.wig) { Wall& w = s.walls[wg.second.wall]; for (auto& wi : wg.second.its) calc_wall(s, w, wi); }
   for (auto& g : s.gravity)   /* BodyForceGroup::calcForces (BodyForceGroup.hpp:54-65) */
@@ -992,6 +1001,20 @@ int orc_get_particles(void* h, int* id, double* pos, double* vel, double* angvel
       if (moment) moment[3 * k + c] = s.P.moment[i][c];
     }
     if (quat) { quat[4 * k] = s.P.quat[i].s; for (int c = 0; c < 3; ++c) quat[4 * k + 1 + c] = s.P.quat[i].v[c]; }
+    ++k;
+  }
+  return k;
+}
+/* Checker diagnostic: each alive particle's sum of the magnitudes of the forces and moments
+   applied to it in the last step (the scale its summed force is compared at), in
+   orc_get_particles order. */
+int orc_get_gross(void* h, double* gf, double* gm) {
+  Sim& s = *(Sim*)h;
+  int k = 0;
+  for (int i = 0; i < s.P.n(); ++i) {
+    if (!s.P.alive[i]) continue;
+    if (gf) gf[k] = i < (int)s.P.gross_f.size() ? s.P.gross_f[i] : 0.0;
+    if (gm) gm[k] = i < (int)s.P.gross_m.size() ? s.P.gross_m[i] : 0.0;
     ++k;
   }
   return k;

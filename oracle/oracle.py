@@ -96,6 +96,7 @@ def _lib(backend: str):
         "save_checkpoint": (C.c_int, [_P, _S, C.c_int]),
         "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
         "timestep": (C.c_longlong, [_P]),
+        "get_gross": (C.c_int, [_P, _D, _D]),
     }
     fns = {}
     for name, (res, args) in sig.items():
@@ -297,6 +298,19 @@ class OracleSim:
                                           _dp(out["moment"])))
         order = np.argsort(out["id"], kind="stable")
         return {k: v[order] for k, v in out.items()}
+
+    def gross(self):
+        """Restatement only: each particle's sum of the magnitudes of the forces and of the moments
+        applied to it in the last step (rows sorted by id, like particles()): the scale a summed
+        force is compared at."""
+        if "get_gross" not in self.f:
+            raise NotImplementedError(f"{self.backend} has no contribution sums")
+        n = self._chk(self.f["num_particles"](self.h))
+        ids, gf, gm = np.zeros(n, np.int32), np.zeros(n), np.zeros(n)
+        self._chk(self.f["get_particles"](self.h, _ip(ids), None, None, None, None, None, None))
+        self._chk(self.f["get_gross"](self.h, _dp(gf), _dp(gm)))
+        order = np.argsort(ids, kind="stable")
+        return gf[order], gm[order]
 
     def pairs(self, group):
         n = self._chk(self.f["num_pairs"](self.h, group.encode()))

@@ -396,3 +396,41 @@ def wall_force_history(sim, nsteps, groups=("bottom_w", "top_w"), walls=("bottom
         for k, w in enumerate(walls):
             out[t, k] = sim.wall(w)[1]
     return out
+
+
+def shear_cell(make, n=250_000, periodic=True, seed=2, moving_walls=False):
+    """The headline shear cell: n RotSpheres with lognormal radii (median 0.5, sigma 0.25, in
+    [0.2, 1.0]) packed by the seeded RSI packer into 100 x 50 x 100 (periodic in x), RotFriction
+    kn = ks = 1e4, mu = 0.6, elastic walls (k = 1e4) at y = 0 and y = 50, dt = 5e-5, seeded
+    N(0, 0.1) velocities and spins.  Walls static unless moving_walls (then the caller moves
+    them); gridSpacing 2.2, verletDist 0.2."""
+    from esys.lsm import geometry as G
+
+    pos, rad = G.rsi_pack(n, (0, 0, 0), (100, 50, 100), seed=seed, periodic_x=True, lognormal=(0.5, 0.25),
+                          rmin=0.2, rmax=1.0, max_attempts=5000)
+    assert len(rad) == n
+    rng = np.random.default_rng(seed + 100)
+    vel = rng.normal(0.0, 0.1, size=(n, 3))
+    angvel = rng.normal(0.0, 0.1, size=(n, 3))
+    sim = make("RotSphere", 2.2, 0.2, (0, 0, 0), (100, 50, 100), (1 if periodic else 0, 0, 0), 5e-5)
+    sim.add_particles(np.arange(n, dtype=np.int32), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=vel,
+                      angvel=angvel)
+    sim.add_rot_friction_group("friction", 1e4, 0.6, 0.6, 1e4, 5e-5, True, True)
+    sim.add_wall("bottom", (0, 0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, 50, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e4)
+    sim.add_wall_group("top_w", "top", 1e4)
+    return sim
+
+
+def assert_forces_within_contribution_scale(a, orc_sim, rtol=1e-12):
+    """Per-particle bar of the first force evaluation: |F_gpu - F_oracle| <= rtol times the sum of
+    the magnitudes of the forces summed into F (and likewise for moments), the restatement's
+    contribution sums (rounding of a different summation order is bounded by that sum)."""
+    pa, pb = a.particles(), orc_sim.particles()
+    assert np.array_equal(pa["id"], pb["id"])
+    gf, gm = orc_sim.gross()
+    for k, g in (("force", gf), ("moment", gm)):
+        d = np.linalg.norm(pa[k] - pb[k], axis=1)
+        bad = d > rtol * g + 1e-300
+        assert not bad.any(), (k, int(bad.sum()), float((d / np.maximum(g, 1e-300)).max()))

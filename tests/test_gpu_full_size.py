@@ -1,8 +1,14 @@
-"""The survey's configurations at full size on the GPU, through size-independent checks.
+"""The survey's configurations at full size on the GPU, through size-independent checks and
+against the oracles.
 
-- 8,000-sphere gravity packing (NRotElastic, gravity, damping, six walls): trajectory against
-  the CPU oracle over the first 300 steps.
-- 1,000,000-sphere bonded block (RotBond + RotFriction with exclusion, loaded platens): two
+- 8,000-sphere gravity packing (NRotElastic, gravity, damping, six walls): the full 5,000-step
+  run against the CPU restatement, first-step forces per particle within 1e-12 of their
+  contribution sums.
+- 250,000-sphere shear cell (RotFriction, elastic walls): 30 steps against the reference's own
+  code (non-periodic: the reference reaches periodic x only with >= 2 MPI workers) and, periodic
+  in x, against the restatement with the per-particle first-step bar.
+- 1,000,000-sphere bonded block (RotBond + RotFriction with exclusion, loaded platens): 10 loaded
+  steps against the reference's own code with bond-failure events and pair sets bit-exact; two
   FP64 runs bit-identical (run-to-run determinism), the bond pass bit-identical to the in-line
   law, and the bond-break event log of the FP32-force form against the FP64 form's (the
   FP32 RotFriction contacts that carry load after failures move a few events by a step).  The block
@@ -30,17 +36,77 @@ def orc(oracle_libs):
     return lambda *a: oracle_libs.OracleSim("orc", *a)
 
 
+@pytest.fixture(scope="module")
+def ref(oracle_libs):
+    if not oracle_libs.available("ref"):
+        pytest.skip("reference library not built")
+    return lambda *a: oracle_libs.OracleSim("ref", *a)
+
+
+def _same_state(a, b, groups, rtol_pos=1e-9, rtol_f=1e-8):
+    """Pair sets (and friction flags) exact; state within rtol of each field's largest magnitude."""
+    pa, pb = a.particles(), b.particles()
+    assert np.array_equal(pa["id"], pb["id"])
+    for k, tol in (("pos", rtol_pos), ("vel", rtol_pos), ("angvel", rtol_pos), ("quat", rtol_pos),
+                   ("force", rtol_f), ("moment", rtol_f)):
+        scale = max(np.abs(pb[k]).max(), 1e-300)
+        err = np.abs(pa[k] - pb[k]).max()
+        assert err <= tol * scale, (k, err, scale)
+    for g in groups:
+        x, y = a.pairs(g), b.pairs(g)
+        assert len(x[0]) == len(y[0]), (g, len(x[0]), len(y[0]))
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1]), g
+        if g == "friction":
+            assert np.array_equal(x[2][:, 3:], y[2][:, 3:]), g  # slipping / touching flags
+            sc = max(np.abs(y[2][:, :3]).max(), 1e-300)
+            assert np.abs(x[2][:, :3] - y[2][:, :3]).max() <= rtol_f * sc, g
+
+
 def test_gravity_packing_8000_matches_oracle(gpu, orc):
+    """The full 5,000-step run of the gravity packing: the first step's forces per particle
+    within 1e-12 of its contribution sum, then pair sets exact and state within 1e-9 (forces
+    1e-8) of each field's scale at the end."""
     a = S.gravity_box(gpu, n_side=20, layers=20)
     b = S.gravity_box(orc, n_side=20, layers=20)
     assert a.num_particles() == 8000
-    a.step(300)
-    b.step(300)
-    pa, pb = a.particles(), b.particles()
-    for k in ("pos", "vel"):
-        assert np.abs(pa[k] - pb[k]).max() <= 1e-9 * max(np.abs(pb[k]).max(), 1e-300), k
-    x, y = a.pairs("elastic"), b.pairs("elastic")
-    assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+    a.step(1)
+    b.step(1)
+    S.assert_forces_within_contribution_scale(a, b)
+    a.step(4999)
+    b.step(4999)
+    _same_state(a, b, ["elastic"])
+    for w in ("xlo", "ylo", "zlo", "zhi"):
+        fa, fb = a.wall(w)[1], b.wall(w)[1]
+        assert np.abs(fa - fb).max() <= 1e-8 * max(np.abs(fb).max(), 1.0), w
+
+
+@pytest.fixture(scope="module")
+def shear_cells():
+    """The headline shear cell's construction is the same call on every backend."""
+    return S.shear_cell
+
+
+def test_shear_cell_250k_matches_reference(gpu, ref, shear_cells):
+    """The 250,000-sphere shear cell against the reference's own code (one worker, so not
+    periodic: the reference reaches periodic x only with >= 2 MPI workers), 30 steps."""
+    a = shear_cells(gpu, periodic=False)
+    b = shear_cells(ref, periodic=False)
+    a.step(30)
+    b.step(30)
+    _same_state(a, b, ["friction"])
+
+
+def test_shear_cell_250k_periodic_matches_restatement(gpu, orc, shear_cells):
+    """Periodic in x against the restatement: first-step forces per particle within 1e-12 of
+    their contribution sums, then 30 steps."""
+    a = shear_cells(gpu, periodic=True)
+    b = shear_cells(orc, periodic=True)
+    a.step(1)
+    b.step(1)
+    S.assert_forces_within_contribution_scale(a, b)
+    a.step(29)
+    b.step(29)
+    _same_state(a, b, ["friction"])
 
 
 @pytest.fixture(scope="module")
@@ -52,7 +118,7 @@ def block_1m():
     return pos, rad, i1, i2
 
 
-def _block_sim(gpu, data, precision=64, bond_pass=1):
+def _block_sim(gpu, data, precision=64, bond_pass=1, loader=True):
     pos, rad, i1, i2 = data
     n = len(rad)
     s = gpu("RotSphere", 2.2, 0.2, (0, 0, 0), (66, 132, 66), (0, 0, 0), 1e-5)
@@ -67,6 +133,8 @@ def _block_sim(gpu, data, precision=64, bond_pass=1):
     s.add_wall_group("bottom_w", "bottom", 1e5)
     s.add_wall_group("top_w", "top", 1e5)
     v = 0.5 * 1e-4 * (y1 - y0) / 1000 / 1e-5   # strain rate 1e-4 per 1,000 steps, split between platens
+    if not loader:  # a harness without the native wall loader (the caller moves the platens)
+        return s
     s.set_wall_velocity("bottom", (0, v, 0))
     s.set_wall_velocity("top", (0, -v, 0))
     s.set_option("precision", precision)
@@ -115,3 +183,24 @@ def test_bonded_block_1m_fp32_break_log_equals_fp64(gpu, block_1m):
     # a few failures move by a step (or across the end of the window): measured 20 to 34 of
     # ~11,000 events over 60 steps, i.e. 0.2-0.3 %
     assert diff <= 1e-2 * len(ev[0]), (diff, len(ev[0]))
+
+
+def test_bonded_block_1m_matches_reference(gpu, ref, block_1m):
+    """The 1M-sphere bonded block against the reference's own code over 10 loaded steps (the
+    platens moved before every step, as the reference's wall-loader runnable does): bond-failure
+    events (id1, id2, step) and the bond and friction pair sets bit-exact, state within 1e-9."""
+    a = _block_sim(gpu, block_1m, 64, 1)
+    a.set_wall_velocity("bottom", (0, 0, 0))
+    a.set_wall_velocity("top", (0, 0, 0))
+    b = _block_sim(ref, block_1m, 64, 1, loader=False)
+    pos, rad = block_1m[0], block_1m[1]
+    d = 0.5 * 1e-4 * float((pos[:, 1] + rad).max() - (pos[:, 1] - rad).min()) / 1000
+    for _ in range(10):
+        for s in (a, b):
+            s.move_wall("bottom", (0, d, 0))
+            s.move_wall("top", (0, -d, 0))
+            s.step(1)
+    ea = set(zip(*(x.tolist() for x in a.breaks())))
+    eb = set(zip(*(x.tolist() for x in b.breaks())))
+    assert len(eb) > 100 and ea == eb, (len(ea), len(eb), len(ea ^ eb))
+    _same_state(a, b, ["bonds", "friction"])

@@ -186,3 +186,18 @@ def test_bond_pass_equals_inline_bond_law(gpu, precision):
     for x, y in zip(a.breaks(), b.breaks()):
         assert np.array_equal(x, y)
     assert len(a.breaks()[0]) > 0
+
+
+@pytest.mark.parametrize("name", ["gravity_box", "friction_pack", "bonded_block", "friction_pack_periodic"])
+def test_first_step_forces_within_contribution_scale(gpu, orc, name):
+    """Per particle, the first force evaluation's force and moment differ from the restatement's
+    by at most 1e-12 of the sum of the magnitudes of the contributions summed into them (the
+    only difference is the summation order)."""
+    build = {"gravity_box": lambda m: S.gravity_box(m, 6),
+             "friction_pack": lambda m: S.friction_pack(m),
+             "bonded_block": lambda m: S.bonded_block(m),
+             "friction_pack_periodic": lambda m: S.friction_pack(m, periodic=True)}[name]
+    a, b = build(gpu), build(orc)
+    a.step(1)
+    b.step(1)
+    S.assert_forces_within_contribution_scale(a, b)
