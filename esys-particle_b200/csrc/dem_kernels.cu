@@ -404,6 +404,13 @@ __global__ void k_set_state(Particles P, int cur, int cnt, const int* slots, con
   if (quat) b.qq[i] = make_double4(quat[4 * r], quat[4 * r + 1], quat[4 * r + 2], quat[4 * r + 3]);
 }
 
+// Mark slots alive again (dem_revive_particles); their cells, pairs and wall candidacy come
+// from the neighbour search the host schedules next.
+__global__ void k_set_alive(Particles P, int cnt, const int* slots) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < cnt) P.pflags[slots[r]] |= PF_ALIVE;
+}
+
 // Alive flag of every slot (the rows dem_get_particles returns).
 __global__ void k_alive_flags(Particles P, int* flags) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -744,6 +751,9 @@ void launch_wall_update(const Grid& g, const Particles& P, int cur, int nwall, c
 void launch_set_state(const Particles& P, int cur, int cnt, const int* slots, const double* pos, const double* vel,
                       const double* angvel, const double* quat, cudaStream_t s) {
   if (cnt) k_set_state<<<nblk(cnt, 256), 256, 0, s>>>(P, cur, cnt, slots, pos, vel, angvel, quat);
+}
+void launch_set_alive(const Particles& P, int cnt, const int* slots, cudaStream_t s) {
+  if (cnt) k_set_alive<<<nblk(cnt, 256), 256, 0, s>>>(P, cnt, slots);
 }
 void launch_alive_flags(const Particles& P, int* flags, cudaStream_t s) {
   if (P.n) k_alive_flags<<<nblk(P.n, 256), 256, 0, s>>>(P, flags);

@@ -39,6 +39,7 @@ void launch_wall_update(const Grid& g, const Particles& P, int cur, int nwall, c
 void launch_set_state(const Particles& P, int cur, int cnt, const int* slots, const double* pos, const double* vel,
                       const double* angvel, const double* quat, cudaStream_t s);
 void launch_alive_flags(const Particles& P, int* flags, cudaStream_t s);
+void launch_set_alive(const Particles& P, int cnt, const int* slots, cudaStream_t s);
 void launch_pack_particles(const Particles& P, int cur, int rot, const int* rows, int* id, double* pos, double* vel,
                            double* angvel, double* quat, double* force, double* moment, cudaStream_t s);
 void launch_check_disp(const Particles& P, int cur, double half_alpha_sq, int* ctrl, cudaStream_t s);

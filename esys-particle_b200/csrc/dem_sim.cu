@@ -474,6 +474,21 @@ struct DemSim {
     return 0;
   }
 
+  // Particles deleted when they left the local grid come back alive with the given state
+  // (known ids only; alive ones are only updated).  A neighbour search is scheduled, which
+  // rebuilds their cells, pairs and wall candidacy.
+  int revive_particles(int cnt, const int* id, const double* pos, const double* vel, const double* angvel,
+                       const double* quat) {
+    if (cnt <= 0) return 0;
+    if (!id) throw std::invalid_argument("revive needs particle ids");
+    set_particles(cnt, id, pos, vel, angvel, quat);  // uploads the slots to stage_slot
+    launch_set_alive(P, cnt, stage_slot.p, s);
+    pending_ctrl |= CTRL_REBUILD;
+    sync();
+    c_launches += 1;
+    return 0;
+  }
+
   // The alive particles in slot order into the caller's host arrays (each may be null).  The
   // rows are packed on the device, then each wanted field is one copy into the caller's array
   // (direct DMA when the caller's memory is pinned).
@@ -2858,6 +2873,41 @@ int dem_num_pairs(dem_sim* h, const char* group) {
   });
 }
 
+int dem_set_pair_states(dem_sim* h, const char* group, int n, const int* id1, const int* id2, const double* state) {
+  return guard(h, [&](DemSim& s) {
+    auto d = s.dyn.find(group);
+    if (d == s.dyn.end()) throw std::invalid_argument("no such dynamic group");
+    dem::DynGroup& G = d->second;
+    if (n < 0 || (n && (!id1 || !id2 || !state))) throw std::invalid_argument("null pair arrays");
+    if (G.kind == 0 || !G.m || !n) return 0;  // the elastic law keeps no history
+    std::vector<unsigned long long> keys(G.m);
+    DEM_CUDA(cudaMemcpyAsync(keys.data(), G.keys.p, sizeof(unsigned long long) * G.m, cudaMemcpyDeviceToHost, s.s));
+    s.sync();
+    int done = 0;
+    for (int r = 0; r < n; ++r) {
+      auto ia = s.id2slot.find(std::min(id1[r], id2[r])), ib = s.id2slot.find(std::max(id1[r], id2[r]));
+      if (ia == s.id2slot.end() || ib == s.id2slot.end()) continue;
+      const unsigned long long key = ((unsigned long long)(unsigned)ia->second << 32) | (unsigned)ib->second;
+      auto it = std::lower_bound(keys.begin(), keys.end(), key);
+      if (it == keys.end() || *it != key) continue;
+      const size_t q = (size_t)(it - keys.begin());
+      const double* st = state + 5 * (size_t)r;
+      const double w = (st[3] != 0.0 ? 1.0 : 0.0) + (st[4] != 0.0 ? 2.0 : 0.0);
+      if (s.fp32) {
+        const float4 v = make_float4((float)st[0], (float)st[1], (float)st[2], (float)w);
+        DEM_CUDA(cudaMemcpyAsync(G.hist32[s.cur].p + q, &v, sizeof(float4), cudaMemcpyHostToDevice, s.s));
+        s.sync();
+      } else {
+        const double4 v = make_double4(st[0], st[1], st[2], w);
+        DEM_CUDA(cudaMemcpyAsync(G.hist[s.cur].p + q, &v, sizeof(double4), cudaMemcpyHostToDevice, s.s));
+        s.sync();
+      }
+      ++done;
+    }
+    return done;
+  });
+}
+
 int dem_get_pairs(dem_sim* h, const char* group, int* id1, int* id2, double* state) {
   return guard(h, [&](DemSim& s) {
     auto d = s.dyn.find(group);
@@ -2983,6 +3033,11 @@ int dem_get_counters(dem_sim* h, long long* out, int n) {
 int dem_set_particles(dem_sim* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
                       const double* quat) {
   return guard(h, [&](DemSim& s) { return s.set_particles(n, id, pos, vel, angvel, quat); });
+}
+
+int dem_revive_particles(dem_sim* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
+                         const double* quat) {
+  return guard(h, [&](DemSim& s) { return s.revive_particles(n, id, pos, vel, angvel, quat); });
 }
 
 int dem_precision_check(dem_sim* h, double* out) {

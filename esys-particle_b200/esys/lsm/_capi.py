@@ -58,6 +58,8 @@ SIGNATURES = {
     "dem_timestep": (C.c_longlong, [_P]),
     "dem_set_option": (C.c_int, [_P, _S, C.c_double]),
     "dem_set_particles": (C.c_int, [_P, C.c_int, _I, _D, _D, _D, _D]),
+    "dem_revive_particles": (C.c_int, [_P, C.c_int, _I, _D, _D, _D, _D]),
+    "dem_set_pair_states": (C.c_int, [_P, _S, C.c_int, _I, _I, _D]),
     "dem_set_stream": (C.c_int, [_P, C.c_void_p]),
     "dem_get_counters": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "dem_precision_check": (C.c_int, [_P, C.POINTER(C.c_double)]),
@@ -268,6 +270,21 @@ class DemSim:
         self._chk(self.lib.dem_set_particles(self.h, int(n), ptr(id, _I), ptr(pos, _D), ptr(vel, _D),
                                              ptr(angvel, _D), ptr(quat, _D)))
         del keep
+
+    def revive_particles(self, id, pos=None, vel=None, angvel=None, quat=None):
+        """Particles deleted when they left this worker's grid come back with this state
+        (dem_revive_particles; the ghosts of a slab decomposition)."""
+        id = np.ascontiguousarray(id, dtype=np.int32)
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (pos, vel, angvel, quat)]
+        self._chk(self.lib.dem_revive_particles(self.h, len(id), _ip(id), *(_dp(a) for a in keep)))
+
+    def set_pair_states(self, group, id1, id2, state):
+        """Tangential history of existing pairs of a dynamic group (dem_set_pair_states); returns
+        the pairs written."""
+        a = np.ascontiguousarray(id1, dtype=np.int32)
+        b = np.ascontiguousarray(id2, dtype=np.int32)
+        st = np.ascontiguousarray(np.asarray(state, np.float64).reshape(-1, 5))
+        return self._chk(self.lib.dem_set_pair_states(self.h, group.encode(), len(a), _ip(a), _ip(b), _dp(st)))
 
     def set_stream(self, stream_handle: int):
         self._chk(self.lib.dem_set_stream(self.h, C.c_void_p(int(stream_handle))))

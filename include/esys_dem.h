@@ -211,6 +211,22 @@ long long dem_timestep(dem_sim* h);
 int dem_set_particles(dem_sim* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
                       const double* quat);
 
+/* Ghost particles of a slab decomposition (esys.lsm.slabs): the particles with these ids, deleted
+ * when they left this worker's grid, come back alive with the given state (pos, vel, angvel: 3 per
+ * row; quat: 4 per row; any may be null); alive ones are only updated.  Replaces the reference's
+ * re-sending of the ghost layer at a rebuild (ParallelParticleArray::rebuild, the circular cell
+ * shifts of ppa/src/pp_array.hpp:450-504).  Schedules a neighbour search. */
+int dem_revive_particles(dem_sim* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
+                         const double* quat);
+
+/* Ghost particles of a slab decomposition: the tangential history of pairs of a dynamic group
+ * (rows of dem_get_pairs' state: Fx, Fy, Fz, slipping, touching), written into the pairs of this
+ * worker's current list (pairs not in it are skipped; the elastic law keeps no history).  Returns
+ * the pairs written.  Replaces the interaction records the reference moves with the particles it
+ * moves between workers at a rebuild (ParallelInteractionStorage_ED::update,
+ * pis/pi_storage_ed.hpp:84-161, after pp_array.hpp:450-504). */
+int dem_set_pair_states(dem_sim* h, const char* group, int n, const int* id1, const int* id2, const double* state);
+
 /* Run all device work of this handle on the caller's CUDA stream (a cudaStream_t); the caller
  * keeps ownership.  No reference counterpart (the reference has no device). */
 int dem_set_stream(dem_sim* h, void* stream);

@@ -871,6 +871,61 @@ int orc_step(void* h, int n) {
   }
   return 0;
 }
+/* State of the particles with these ids (rows; any array may be null); a particle deleted when it
+   left the grid comes back alive (the ghost copies of a slab decomposition, which the reference
+   re-sends at every rebuild, pp_array.hpp:450-504); then a neighbour search, as after an insert. */
+int orc_set_particles(void* h, int n, const int* id, const double* pos, const double* vel, const double* angvel,
+                      const double* quat) {
+  Sim& s = *(Sim*)h;
+  std::map<int, int> slot;
+  for (int i = 0; i < s.P.n(); ++i) slot[s.P.id[i]] = i;
+  bool revived = false;
+  for (int r = 0; r < n; ++r) {
+    auto it = slot.find(id[r]);
+    if (it == slot.end()) return -1;
+    const int i = it->second;
+    if (pos) s.P.pos[i] = V3(pos[3 * r], pos[3 * r + 1], pos[3 * r + 2]);
+    if (vel) s.P.vel[i] = V3(vel[3 * r], vel[3 * r + 1], vel[3 * r + 2]);
+    if (angvel && s.rotmode) s.P.angvel[i] = V3(angvel[3 * r], angvel[3 * r + 1], angvel[3 * r + 2]);
+    if (quat && s.rotmode) s.P.quat[i] = Q(quat[4 * r], V3(quat[4 * r + 1], quat[4 * r + 2], quat[4 * r + 3]));
+    if (!s.P.alive[i]) { s.P.alive[i] = 1; revived = true; }
+  }
+  if (revived) search_neighbors(s);
+  return 0;
+}
+/* The neighbour search of the next step, now (force-neutral). */
+int orc_search_neighbors(void* h) {
+  Sim& s = *(Sim*)h;
+  s.first = false;
+  search_neighbors(s);
+  update_interactions(s);
+  return 0;
+}
+/* Neighbour searches so far (the neighbour table's timestamp). */
+int orc_num_rebuilds(void* h) { return ((Sim*)h)->timestamp; }
+/* Tangential history of existing pairs of a RotFriction group (rows Fx, Fy, Fz, slipping,
+   touching); returns the pairs written. */
+int orc_set_pair_states(void* h, const char* group, int n, const int* a, const int* b, const double* st) {
+  Sim& s = *(Sim*)h;
+  auto it = s.dpis.find(group);
+  if (it == s.dpis.end()) return -1;
+  PairGroup& g = *it->second;
+  if (g.kind != 1) return 0;
+  std::map<std::pair<int, int>, int> row;
+  for (int r = 0; r < n; ++r) row[{std::min(a[r], b[r]), std::max(a[r], b[r])}] = r;
+  int done = 0;
+  for (auto& f : g.fr) {
+    const int i1 = s.P.id[f.p1], i2 = s.P.id[f.p2];
+    auto r = row.find({std::min(i1, i2), std::max(i1, i2)});
+    if (r == row.end()) continue;
+    const double* v = st + 5 * r->second;
+    f.Ffric = V3(v[0], v[1], v[2]);
+    f.slipping = v[3] != 0.0;
+    f.touching = v[4] != 0.0;
+    ++done;
+  }
+  return done;
+}
 /* LsmMpi.setInteractionParameter -> forAllInteractionsSet (LatticeMaster.cpp:4290-4301,
  * pi_storage.hpp:277-292), widened to the parameters the differentiable window uses: a group's
  * unscaled parameter is replaced and every existing interaction's scaled constant is recomputed

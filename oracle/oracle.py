@@ -97,6 +97,10 @@ def _lib(backend: str):
         "load_checkpoint": (C.c_int, [_P, _S, C.c_longlong]),
         "timestep": (C.c_longlong, [_P]),
         "get_gross": (C.c_int, [_P, _D, _D]),
+        "set_particles": (C.c_int, [_P, C.c_int, _I, _D, _D, _D, _D]),
+        "search_neighbors": (C.c_int, [_P]),
+        "num_rebuilds": (C.c_int, [_P]),
+        "set_pair_states": (C.c_int, [_P, _S, C.c_int, _I, _I, _D]),
     }
     fns = {}
     for name, (res, args) in sig.items():
@@ -298,6 +302,30 @@ class OracleSim:
                                           _dp(out["moment"])))
         order = np.argsort(out["id"], kind="stable")
         return {k: v[order] for k, v in out.items()}
+
+    def set_particles(self, pos=None, vel=None, angvel=None, quat=None, id=None):
+        """State of the particles with these ids (restatement only); deleted ones come back."""
+        if "set_particles" not in self.f:
+            raise NotImplementedError(f"{self.backend} cannot set particle state")
+        ids = np.ascontiguousarray(id, dtype=np.int32)
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (pos, vel, angvel, quat)]
+        self._chk(self.f["set_particles"](self.h, len(ids), _ip(ids), *(_dp(a) for a in keep)))
+
+    def revive_particles(self, id, pos=None, vel=None, angvel=None, quat=None):
+        self.set_particles(pos=pos, vel=vel, angvel=angvel, quat=quat, id=id)
+
+    def search_neighbors(self):
+        self._chk(self.f["search_neighbors"](self.h))
+
+    def set_pair_states(self, group, id1, id2, state):
+        a = np.ascontiguousarray(id1, dtype=np.int32)
+        b = np.ascontiguousarray(id2, dtype=np.int32)
+        st = np.ascontiguousarray(np.asarray(state, np.float64).reshape(-1, 5))
+        return self._chk(self.f["set_pair_states"](self.h, group.encode(), len(a), _ip(a), _ip(b), _dp(st)))
+
+    def counters(self):
+        """The subset of the GPU handle's counters a restatement has: neighbour searches."""
+        return {"rebuilds": self._chk(self.f["num_rebuilds"](self.h))}
 
     def gross(self):
         """Restatement only: each particle's sum of the magnitudes of the forces and of the moments

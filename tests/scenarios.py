@@ -434,3 +434,81 @@ def assert_forces_within_contribution_scale(a, orc_sim, rtol=1e-12):
         d = np.linalg.norm(pa[k] - pb[k], axis=1)
         bad = d > rtol * g + 1e-300
         assert not bad.any(), (k, int(bad.sum()), float((d / np.maximum(g, 1e-300)).max()))
+
+
+class _Recorder:
+    """Stands in for a simulation and records the calls a scenario builder makes."""
+
+    def __init__(self, *args):
+        self.args, self.calls = args, []
+
+    def __getattr__(self, name):
+        def call(*a, **k):
+            self.calls.append((name, a, k))
+        return call
+
+
+def record(builder, edit=None, **kw):
+    """(particles, connections, configure, creation args) of the scenario `builder(make, **kw)`:
+    its add_particles arrays (after `edit(particles)`), its connections, and a function that makes
+    its other calls (groups, walls) on another simulation."""
+    rec = builder(lambda *a: _Recorder(*a), **kw)
+    add = [c for c in rec.calls if c[0] == "add_particles"]
+    assert len(add) == 1
+    a, k = add[0][1], add[0][2]
+    n = len(a[0])
+    particles = {"id": np.asarray(a[0], np.int32), "pos": np.asarray(a[1], float), "rad": np.asarray(a[2], float),
+                 "mass": np.asarray(a[3], float), "tag": k.get("tag", np.zeros(n, np.int32)), "vel": k.get("vel"),
+                 "angvel": k.get("angvel"), "quat": k.get("quat")}
+    if edit is not None:
+        edit(particles)
+    cc = [c for c in rec.calls if c[0] == "add_connections"]
+    conns = tuple(np.asarray(x) for x in cc[0][1]) if cc else None
+    rest = [c for c in rec.calls if c[0] not in ("add_particles", "add_connections")]
+
+    def configure(sim):
+        for name, a2, k2 in rest:
+            getattr(sim, name)(*a2, **k2)
+
+    return particles, conns, configure, rec.args
+
+
+def split(make, world, builder, history_groups=("friction",), transport=None, edit=None, **kw):
+    """The scenario `builder(make, **kw)` as a slab decomposition (esys.lsm.slabs.SlabDomain) over
+    `world` workers made by `make`; `edit(particles)` may change the particle arrays first (apply
+    the same edit to the one-worker run it is compared with, see replay)."""
+    from esys.lsm.slabs import SlabDomain
+
+    particles, conns, configure, args = record(builder, edit, **kw)
+    return SlabDomain(make, configure, *args, particles, connections=conns, world=world, transport=transport,
+                      history_groups=history_groups)
+
+
+def replay(make, builder, edit=None, **kw):
+    """The scenario on one worker, with the same particle edit as split's."""
+    particles, conns, configure, args = record(builder, edit, **kw)
+    sim = make(*args)
+    p = particles
+    sim.add_particles(p["id"], p["pos"], p["rad"], p["mass"], tag=p["tag"], vel=p["vel"], angvel=p["angvel"],
+                      quat=p["quat"])
+    if conns is not None:
+        sim.add_connections(*conns)
+    configure(sim)
+    return sim
+
+
+def drift_x(v):
+    """Particle edit: a uniform velocity v along x on top of the scenario's own."""
+    def edit(p):
+        vel = np.zeros((len(p["id"]), 3)) if p["vel"] is None else np.array(p["vel"], float)
+        vel[:, 0] += v
+        p["vel"] = vel
+    return edit
+
+
+def wide_friction_pack(make, nx=12, ny=5, nz=6, extra_x=8.0, skin=0.05, **kw):
+    """friction_pack in a box longer in x by extra_x (room to drift) with a small Verlet skin, so
+    that neighbour rebuilds are frequent."""
+    def wider(pt, gs, vd, lo, hi, circ, dt):
+        return make(pt, gs, skin, lo, (hi[0] + extra_x, hi[1], hi[2]), circ, dt)
+    return friction_pack(wider, nx=nx, ny=ny, nz=nz, **kw)
