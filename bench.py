@@ -39,6 +39,15 @@ METRIC = "contact-updates/s at <=1e-5 rel force err vs FP64"
 UNIT = "contact-updates/s"
 
 
+def _jsonable(o):
+    """numpy scalars and arrays in the JSON line as plain numbers and lists."""
+    if isinstance(o, np.generic):
+        return o.item()
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError(f"{type(o).__name__} is not JSON serializable")
+
+
 def product_rsi(seed, n, bmin, bmax, periodic_x, dist, p0, p1, rmin, rmax, max_attempts):
     """The seeded RSI packer of the product library (include/esys_geometry.h)."""
     from esys.lsm import geometry as G
@@ -327,9 +336,9 @@ def adjoint_leg(stream, precision=32):
             lp, lm = f(base + h), f(base - h)
             fd = (lp - lm) / (2 * h)
             noise = abs(lp + lm - 2.0 * loss_base) / (2 * h)
-            rows[rel] = {"fd": fd, "noise": noise, "resolved": abs(fd) > 100.0 * noise,
-                         "rel_err": abs(g_adj - fd) / max(abs(fd), 1e-300),
-                         "rel_err_fp64_adjoint": abs(g_adj64 - fd) / max(abs(fd), 1e-300)}
+            rows[rel] = {"fd": float(fd), "noise": float(noise), "resolved": bool(abs(fd) > 100.0 * noise),
+                         "rel_err": float(abs(g_adj - fd) / max(abs(fd), 1e-300)),
+                         "rel_err_fp64_adjoint": float(abs(g_adj64 - fd) / max(abs(fd), 1e-300))}
         res = [r for r in rows.values() if r["resolved"]] or list(rows.values())
         best = min(res, key=lambda r: r["rel_err"])
         return {"adjoint": float(g_adj), "adjoint_fp64": float(g_adj64), "central_difference": rows[1e-6]["fd"],
@@ -1201,7 +1210,7 @@ def main():
             "gravity_packing": grav,
             "bonded_block": block,
         }
-        print(json.dumps(line))
+        print(json.dumps(line, default=_jsonable))
     sim.close()
     if dist is not None:
         dist.barrier()

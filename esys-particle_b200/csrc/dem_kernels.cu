@@ -959,7 +959,10 @@ __global__ void k_pair_field(Grid g, Particles P, int prev, const unsigned long 
     if (field == 0) r = touching ? 1.0 : 0.0;
     else if (field == 2) r = slipping ? 1.0 : 0.0;
     else if (field == 3) r = (touching && !slipping) ? 1.0 : 0.0;
-    else if (field == 1 && touching && kind == 3) {  // CHertzMindlinInteraction::getPotentialEnergy (:371-375)
+    else if (field == 1 && touching && (kind == 3 || kind == 4)) {
+      // CHertzMindlinInteraction::getPotentialEnergy (HertzMindlinInteraction.cpp:371-375) and
+      // CHertzMindlinViscoInteraction::getPotentialEnergy (HertzMindlinViscoInteraction.cpp:415-419):
+      // the elastic Hertz normal force, the damping left out
       const double R_ij = 1.0 / (1.0 / pa.w + 1.0 / pb.w);
       const double dist = sqrt(d2);
       const double dn = eq - dist;

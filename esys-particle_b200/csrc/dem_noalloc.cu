@@ -3,13 +3,16 @@
 // Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
 // being captured (allocation is not a capturable operation), hosts that give
 // the library only memory from their own pool, and real-time loops that forbid
-// allocation after start-up.  This entry point computes the same per-wall
-// reaction force that the step kernel accumulates for CWall::m_force (the sum
-// over particles of the elastic wall contact forces), but keeps its
-// block-partial sums in a fixed device array instead of memory it allocates.
+// allocation after start-up.  This entry point computes per-wall reaction forces
+// (the sum over the given particles of their elastic wall contact forces) and keeps
+// its block-partial sums in a fixed device array instead of memory it allocates.
+// Every given particle counts, wherever it lies; the step kernel's reaction
+// (CWall::m_force) counts only the wall's candidates (particles within one grid
+// spacing of the plane, in the grid interior), so the two agree when the given
+// particles are those candidates, e.g. all particles of a closed box.
 //
 // The array is a file-scope __device__ object: every GPU that loads the library
-// holds its 111 KiB (113,668 bytes) until the process exits, and every call on that GPU shares
+// holds its 111 KiB (113,672 bytes) until the process exits, and every call on that GPU shares
 // it, so two calls that run at the same time on the same GPU (different
 // streams, overlapping) race and give wrong sums.
 #include <cmath>
@@ -31,6 +34,7 @@ struct NoAllocScratch {
   double partial[kNaMaxBlocks][kNaMaxWalls][3];
   unsigned counter;
 };
+static_assert(sizeof(NoAllocScratch) == 113672, "the documented size of the scratch array");
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
 // Per-particle elastic wall forces (CElasticWallInteraction::calcForces,
@@ -94,6 +98,8 @@ extern "C" int dem_wall_reactions_noalloc(int n, const double* particles, int nw
   if (nwall < 1 || nwall > kNaMaxWalls) return DEM_ERR_ARG;
   if ((n > 0 && !particles) || !walls || !reactions) return DEM_ERR_ARG;
   if (reinterpret_cast<uintptr_t>(particles) % 16 != 0) return DEM_ERR_ARG;  // double4 rows
+  if (reinterpret_cast<uintptr_t>(walls) % 8 != 0 || reinterpret_cast<uintptr_t>(reactions) % 8 != 0)
+    return DEM_ERR_ARG;  // doubles
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DEM_ERR_CUDA;
   NoAllocScratch* scratch = nullptr;

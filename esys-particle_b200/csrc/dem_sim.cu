@@ -3165,7 +3165,7 @@ int dem_interaction_scalar_field(dem_sim* h, const char* group, const char* fiel
     auto d = s.dyn.find(gname);
     if (d != s.dyn.end()) {
       dem::DynGroup& G = d->second;
-      int code = f == "count" ? 0 : (f == "potential_energy" && G.kind != 4) ? 1 : -1;
+      int code = f == "count" ? 0 : f == "potential_energy" ? 1 : -1;
       if (G.kind != 0 && f == "slipping") code = 2;
       if (G.kind != 0 && f == "sticking") code = 3;
       if (code < 0) throw std::invalid_argument("unknown interaction scalar field " + f + " of group " + gname);

@@ -253,13 +253,15 @@ int dem_precision_report(dem_sim* h, double* out, int n);
 /* Allocation-free per-wall reaction forces, for callers that cannot call cudaMalloc: code that
  * runs during CUDA graph capture, hosts that hand the library only memory from their own pool,
  * real-time loops that forbid allocation.  No counterpart in the reference.
- * Computes, for each wall, the sum over the given particles of the elastic wall contact force
- * (the quantity the step accumulates into CWall::m_force, what dem_get_wall reports).
+ * Computes, for each wall, the sum over the given particles of the elastic wall contact force.
+ * Every given particle counts, wherever it lies; the reaction the step accumulates into
+ * CWall::m_force (what dem_get_wall reports) counts only the wall's candidates (within one grid
+ * spacing of the plane, in the grid interior), so pass those particles to get that quantity.
  * particles: device, n rows of 4 doubles (x, y, z, radius), 16-byte aligned; walls: device, nwall
- * rows of 7 doubles (origin xyz, normal xyz, normalK); reactions: device, nwall x 3 doubles;
- * stream: a cudaStream_t (NULL = default stream).  Limits: 1 <= nwall <= 8, 0 <= n <= 16777216;
- * larger sizes return DEM_ERR_ARG.  No memory is allocated: block partial sums live in a fixed
- * 111 KiB (113,668-byte) __device__ array that every GPU loading the library keeps until exit.  The first call on
+ * rows of 7 doubles (origin xyz, normal xyz, normalK), 8-byte aligned; reactions: device, nwall x 3
+ * doubles, 8-byte aligned; stream: a cudaStream_t (NULL = default stream).  Limits:
+ * 1 <= nwall <= 8, 0 <= n <= 16777216; larger sizes or misaligned buffers return DEM_ERR_ARG.  No
+ * memory is allocated: block partial sums live in a fixed 111 KiB (113,672-byte) __device__ array that every GPU loading the library keeps until exit.  The first call on
  * each device looks up that array's address (make it before any stream capture).  All calls on a
  * device share the array, so calls that overlap on the GPU race; the result of each call is
  * written asynchronously on `stream`. */

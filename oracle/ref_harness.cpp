@@ -157,6 +157,7 @@ struct RefSim : public ASim {
   std::map<std::string, Exposed<ParallelInteractionStorage_ED<T, CFrictionInteraction>>*> nfric;
   std::map<std::string, Exposed<ParallelInteractionStorage_EB<T, CBondedInteraction>>*> nbond;
   std::map<std::string, Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinInteraction>>*> hm;
+  std::map<std::string, Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinViscoInteraction>>*> hmv;
 
   RefSim(double gs, double vd, const double* mn, const double* mx, const int* circ, double dt_)
       : comm(MPI_COMM_WORLD), dt(dt_), nrange(gs), alpha(vd) {
@@ -411,6 +412,7 @@ struct RefSim : public ASim {
     CHertzMindlinViscoIGP p(name, E, nu, mu, cor, dt_);
     auto* st = new Exposed<ParallelInteractionStorage_NE<T, CHertzMindlinViscoInteraction>>(ppa, p);
     dpis[name] = st;
+    hmv[name] = st;
     return 0;
   }
   /* TRotSubLattice::addBrittleBeamSCIG (Parallel/RotSubLattice.hpp:188-225) */
@@ -574,6 +576,7 @@ struct RefSim : public ASim {
     if (elastic.count(group)) return (int)elastic[group]->list().size();
     if (nfric.count(group)) return (int)nfric[group]->list().size();
     if (hm.count(group)) return (int)hm[group]->list().size();
+    if (hmv.count(group)) return (int)hmv[group]->list().size();
     if (nbond.count(group)) return (int)nbond[group]->list().size();
     if (dzc.count(group)) return (int)static_cast<DzcPis*>(dzc[group])->list().size();
     if (bsc.count(group)) return (int)static_cast<ScPis*>(bsc[group])->list().size();
@@ -613,6 +616,19 @@ struct RefSim : public ASim {
           for (int k = 0; k < 3; ++k) state[5 * i + k] = f[k];
           state[5 * i + 3] = (in.*HMAccess::slipping()) ? 1.0 : 0.0;
           state[5 * i + 4] = (in.*HMAccess::touching()) ? 1.0 : 0.0;
+        }
+        ++i;
+      }
+      return i;
+    }
+    if (hmv.count(group)) {  /* HertzMindlinVisco: 0 (3), slipping, sticking + slipping (touching) */
+      for (auto& in : hmv[group]->list()) {
+        auto v = in.getAllID();
+        id1[i] = v[0]; id2[i] = v[1];
+        if (state) {
+          for (int k = 0; k < 3; ++k) state[5 * i + k] = 0.0;
+          state[5 * i + 3] = in.getSlipping();
+          state[5 * i + 4] = in.getSlipping() + in.getSticking();
         }
         ++i;
       }

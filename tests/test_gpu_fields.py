@@ -178,11 +178,11 @@ def test_displacement_follows_circular_shifts_and_checkpoints(gpu, tmp_path):
     assert np.abs(d3 - s._v[ids] * 0.4).max() < 1e-9
 
 
-@pytest.mark.parametrize("law", ["nfric", "hm"])
+@pytest.mark.parametrize("law", ["nfric", "hm", "hmv"])
 def test_nrot_friction_and_hertz_mindlin_fields(gpu, law):
     """count / slipping / sticking from the flags the step wrote, and potential_energy from the positions
     the force evaluation read: CFrictionInteraction 0.5 Fn.Fn / k + 0.5 Ff.Ff / ks (scaled k, ks), and
-    CHertzMindlinInteraction 0.5 Fn.Fn / E."""
+    CHertzMindlinInteraction and CHertzMindlinViscoInteraction 0.5 Fn.Fn / E of the elastic Hertz force."""
     sim = gpu("NRotSphere", 1.2, 0.2, (0, 0, 0), (6, 6, 6), (0, 0, 0), 1e-4)
     pos = np.array([[2.0, 2.0, 2.0], [2.85, 2.1, 2.0], [4.5, 4.5, 4.5]])
     rad = np.array([0.5, 0.45, 0.4])
@@ -190,8 +190,10 @@ def test_nrot_friction_and_hertz_mindlin_fields(gpu, law):
                       vel=[[0.0, 0.3, 0.0], [0.0, -0.3, 0.1], [0.0, 0.0, 0.0]])
     if law == "nfric":
         sim.add_nrot_friction_group("c", 1e4, 0.5, 5e3, 1e-4, True)
-    else:
+    elif law == "hm":
         sim.add_hertz_mindlin_group("c", 1e4, 0.3, 0.5, 1e-4)
+    else:
+        sim.add_hertz_mindlin_visco_group("c", 1e4, 0.3, 0.5, 0.8, 1e-4)
     sim.step(1)
     pa, pb, pst = sim.pairs("c")
     by_key = {(int(x), int(y)): r for x, y, r in zip(pa, pb, pst)}

@@ -192,11 +192,13 @@ def test_brittle_beam_sc_failures_match_reference(gpu, ref):
         _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
 
 
-@pytest.mark.parametrize("rot", [False, True])
-def test_hertz_mindlin_visco_matches_reference(gpu, ref, rot):
+@pytest.mark.parametrize("rot,restitution", [(False, 0.6), (True, 0.6), (True, 0.95)])
+def test_hertz_mindlin_visco_matches_reference(gpu, ref, rot, restitution):
     """HertzMindlinVisco (CHertzMindlinViscoInteraction): damped Hertz-Mindlin contacts through several
-    neighbour rebuilds, state within 1e-9 of the reference's own class."""
-    a, b = S.hertz_mindlin_pack(gpu, rot=rot, restitution=0.6), S.hertz_mindlin_pack(ref, rot=rot, restitution=0.6)
+    neighbour rebuilds, state within 1e-9 of the reference's own class, and the slipping / sticking
+    interaction fields equal to its getSlipping / getSticking; restitution 0.95 leaves little damping."""
+    a = S.hertz_mindlin_pack(gpu, rot=rot, restitution=restitution)
+    b = S.hertz_mindlin_pack(ref, rot=rot, restitution=restitution)
     c0 = a.counters()["rebuilds"]
     a.step(300)
     b.step(300)
@@ -206,3 +208,13 @@ def test_hertz_mindlin_visco_matches_reference(gpu, ref, rot):
         _close(_by_id(pa, k), _by_id(pb, k), 1e-9, k)
     c = a.interaction_scalar_field("hm", "count")[2]
     assert c.sum() > 20
+    ia, ib, _ = a.interaction_scalar_field("hm", "slipping")
+    fa = {f: dict(zip(zip(ia.tolist(), ib.tolist()), a.interaction_scalar_field("hm", f)[2]))
+          for f in ("slipping", "sticking")}
+    ra, rb, rst = b.pairs("hm")
+    rb_map = {(int(x), int(y)): r for x, y, r in zip(ra, rb, rst)}
+    common = [k for k in fa["slipping"] if k in rb_map]
+    assert len(common) > 20
+    for k in common:
+        assert fa["slipping"][k] == rb_map[k][3], k
+        assert fa["sticking"][k] == rb_map[k][4] - rb_map[k][3], k

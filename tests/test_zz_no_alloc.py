@@ -60,6 +60,28 @@ def test_noalloc_rejects_sizes_beyond_the_limit(dem_lib):
     fn = dem_lib.dem_wall_reactions_noalloc
     buf = torch.zeros(64, dtype=torch.float64, device="cuda:0")
     p = ctypes.c_void_p(buf.data_ptr())
+    odd = ctypes.c_void_p(buf.data_ptr() + 4)
     assert fn(1, p, 9, p, p, None) == -1            # more than 8 walls
     assert fn(1 << 25, p, 1, p, p, None) == -1      # more than 16777216 particles
     assert fn(-1, p, 1, p, p, None) == -1
+    assert fn(1, p, 1, odd, p, None) == -1           # walls not 8-byte aligned
+    assert fn(1, p, 1, p, odd, None) == -1           # reactions not 8-byte aligned
+
+
+def test_noalloc_counts_every_given_particle(dem_lib):
+    """Unlike the step's reaction, which counts only a wall's candidates, every particle passed in
+    counts: one far behind a wall plane gets the elastic wall force of its overlap,
+    k pi r (r - d) along the normal (CElasticWallInteraction, pi = 3.141592654)."""
+    import torch
+
+    dev = torch.device("cuda:0")
+    r, d, k = 0.5, -3.0, 1000.0
+    parts = torch.tensor([[1.0, d, 2.0, r]], dtype=torch.float64, device=dev)
+    walls = torch.tensor([[0, 0, 0, 0, 1, 0, k]], dtype=torch.float64, device=dev)
+    out = torch.full((1, 3), float("nan"), dtype=torch.float64, device=dev)
+    rc = dem_lib.dem_wall_reactions_noalloc(1, ctypes.c_void_p(parts.data_ptr()), 1, ctypes.c_void_p(walls.data_ptr()),
+                                            ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 0
+    torch.cuda.synchronize(dev)
+    expect = k * 3.141592654 * r * (r - d)
+    assert np.allclose(out.cpu().numpy(), [[0.0, expect, 0.0]], rtol=1e-12, atol=0.0)
