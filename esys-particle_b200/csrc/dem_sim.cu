@@ -11,6 +11,7 @@
 // raises a control flag that makes the remaining launches of the chunk
 // return at once, and the host resumes from there.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -216,6 +217,27 @@ struct DemSim {
   }
 
   void sync() { DEM_CUDA(cudaStreamSynchronize(s)); }
+  // Capacity of a bonded group's failure-event log: every bond can fail once, so the
+  // default never overflows; the "event_capacity" option sets a fixed size instead.
+  int ev_cap = 0;
+  int event_cap(int nb) const { return ev_cap > 0 ? ev_cap : std::max(1024, nb); }
+  void set_event_capacity(int cap) {
+    for (auto& b : bond) {
+      BondGroup& B = b.second;
+      const int c = cap > 0 ? cap : std::max(1024, B.nb);
+      const int ne = read_int(B.nevents.p);
+      if (ne > B.cap_events)  // entries past the old capacity were never written
+        throw std::invalid_argument("the event log of bonded group '" + b.first + "' has overflowed; its capacity is fixed");
+      if (ne > c) throw std::invalid_argument("event_capacity is below the events already logged");
+    }
+    ev_cap = cap;
+    for (auto& b : bond) {
+      BondGroup& B = b.second;
+      B.cap_events = event_cap(B.nb);
+      B.events.reserve(3 * (size_t)B.cap_events, true, s);
+    }
+    sync();
+  }
   int read_int(const int* d) {
     DEM_CUDA(cudaMemcpyAsync(h_ctrl, d, sizeof(int), cudaMemcpyDeviceToHost, s));
     sync();
@@ -878,13 +900,23 @@ struct DemSim {
     if (pending_ctrl & CTRL_REBUILD) search_neighbors();
     if (handoff && (pending_ctrl & CTRL_BROKE) && timestamp == last_ns) refresh_counts();
     else update_interactions((pending_ctrl & CTRL_BROKE) != 0);
-    if (pending_ctrl & CTRL_OVERFLOW) { err = "bond-break event log overflowed"; return false; }
     pending_ctrl = 0;
     return true;
   }
 
+  // A full event log loses entries only: the failures themselves are in each bond's state.
+  // The call in which the log filled reports it; later calls go on.
+  bool take_overflow() {
+    const bool o = (pending_ctrl & CTRL_OVERFLOW) != 0;
+    pending_ctrl &= ~CTRL_OVERFLOW;
+    return o;
+  }
+  static constexpr const char* kOverflowText =
+      "bond-break event log overflowed (failures past its capacity are not logged; the bond states are exact)";
+
   int step(int nsteps) {
     int done = 0;
+    bool overflowed = false;
     // the forces a caller can observe are the last step's: only that step stores them
     const long long t_last = t + nsteps;
     while (done < nsteps) {
@@ -920,6 +952,7 @@ struct DemSim {
       std::memcpy(&dev_t, h_ctrl, sizeof(long long));
       const int ran = (int)(dev_t - t0);
       pending_ctrl = h_ctrl[2];
+      overflowed |= take_overflow();
       // a BrittleBeamSC failure at the head of the chunk's first step stops it before any step
       if (ran < 0 || ran > k || (ran == 0 && !(pending_ctrl & CTRL_BROKE))) {
         err = "device step counter out of sequence";
@@ -937,6 +970,7 @@ struct DemSim {
         prof_steps += ran;
       }
     }
+    if (overflowed) { err = kOverflowText; return -2; }
     return 0;
   }
 
@@ -1789,7 +1823,7 @@ struct DemSim {
       B.nb = (int)rec.size();
       const int nb = std::max(B.nb, 1);
       B.keys.reserve(nb); B.ends.reserve(nb); B.D0.reserve(nb); B.broken_step.reserve(nb);
-      B.cap_events = std::max(1024, B.nb);
+      B.cap_events = event_cap(B.nb);
       B.events.reserve(3 * B.cap_events); B.nevents.reserve(1);
       std::vector<unsigned long long> keys(B.nb);
       std::vector<int2> ends(B.nb);
@@ -2246,6 +2280,7 @@ struct Ensemble {
     for (int k = 0; k < ns; ++k) target[k] = sims[k]->t + nsteps;
     const int t_pp = pick_tpp();
     std::vector<long long> cps;
+    int overflow_at = -1;
     while (true) {
       long long remaining = 0;
       for (int k = 0; k < ns; ++k) remaining = std::max(remaining, target[k] - sims[k]->t);
@@ -2262,12 +2297,17 @@ struct Ensemble {
         d.c_steps += ran;
         d.c_contacts += ran * cps[j];
         d.pending_ctrl = h_ctrl[j];
+        if (d.take_overflow() && overflow_at < 0) overflow_at = j;
         c_steps += ran;
         c_contacts += ran * cps[j];
         ran_total += ran;
         if (h_ctrl[j] & CTRL_REBUILD) ++c_rebuild_calls;
       }
       if (ran_total == 0) { err = "no specimen advanced in a chunk"; return -3; }
+    }
+    if (overflow_at >= 0) {
+      err = "specimen " + std::to_string(overflow_at) + ": " + DemSim::kOverflowText;
+      return DEM_ERR_OVERFLOW;
     }
     return 0;
   }
@@ -2420,6 +2460,47 @@ struct Ensemble {
 using dem::DemSim;
 
 namespace {
+// Text of this thread's last failed dem_create (there is no handle to keep it in).
+thread_local std::string g_create_err;
+
+int create_fail(int rc, const std::string& why) {
+  g_create_err = "dem_create: " + why;
+  return rc;
+}
+
+// The checks of TSubLattice::initNeighborTable and the ParallelParticleArray ctor
+// (Parallel/SubLattice.hpp:455-564, ppa/src/pp_array.hpp:72-88) made before any device
+// work: the reference throws "size doesn't fit range" where the grown domain is not a
+// whole number of cells.  Here the grid is grown the same way (non-periodic sides to
+// whole cells, the range of a periodic x side adjusted to divide it), so what remains
+// is a domain that is empty, not finite, periodic in y or z, or too small or too large
+// for the cell grid.  Returns "" when the domain is usable.
+std::string check_domain(double range, double alpha, const double* mn, const double* mx, const int* circ) {
+  if (!(range > 0) || !std::isfinite(range)) return "grid spacing must be positive";
+  if (!(alpha >= 0) || !std::isfinite(alpha)) return "verlet distance must be non-negative";
+  if (!mn || !mx) return "null bounding box";
+  for (int i = 0; i < 3; ++i) {
+    if (!std::isfinite(mn[i]) || !std::isfinite(mx[i])) return "bounding box is not finite";
+    if (!(mx[i] > mn[i])) return "bounding box max must exceed min in every dimension";
+  }
+  if (circ && (circ[1] || circ[2])) return "only x may be periodic (circDimList y and z must be false)";
+  double cells = 1.0;
+  for (int i = 0; i < 3; ++i) {
+    const double sz = mx[i] - mn[i];
+    double n = std::ceil(sz / range);
+    if (i == 0 && circ && circ[0]) {
+      n = std::floor(sz / range);
+      if (std::fabs(sz / range - std::lrint(sz / range)) <= 1e-6) n = (double)std::lrint(sz / range);
+      if (n < 3) return "periodic x needs at least 3 cells of the grid spacing";
+    } else {
+      n += 2;  // the padding layer on both sides
+    }
+    cells *= n;
+  }
+  if (!(cells < 2147483647.0)) return "the cell grid has more than 2^31 - 1 cells";
+  return "";
+}
+
 template <class F>
 int guard(dem_sim* h, F&& f) {
   DemSim* s = reinterpret_cast<DemSim*>(h);
@@ -2471,7 +2552,7 @@ static void add_bond_group(DemSim& s, const char* name, int tag, F&& set) {
     B.nb = (int)keys.size();
     const int nb = std::max(B.nb, 1);
     B.keys.reserve(nb); B.ends.reserve(nb); B.D0.reserve(nb); B.broken_step.reserve(nb);
-    B.cap_events = std::max(1024, B.nb);
+    B.cap_events = s.event_cap(B.nb);
     B.events.reserve(3 * B.cap_events); B.nevents.reserve(1);
     std::vector<int2> ends(B.nb);
     for (int i = 0; i < B.nb; ++i) ends[i] = make_int2((int)(keys[i] >> 32), (int)(keys[i] & 0xffffffffu));
@@ -2491,21 +2572,29 @@ extern "C" {
 
 int dem_create(dem_sim** out, int particle_type, double grid_spacing, double verlet_dist, const double* bbox_min,
                const double* bbox_max, const int* circ, double dt) {
-  if (!out) return DEM_ERR_ARG;
+  if (!out) return create_fail(DEM_ERR_ARG, "null output handle");
   *out = nullptr;
+  // the domain is checked on the host before any device is touched
+  if (particle_type != 0 && particle_type != 1) return create_fail(DEM_ERR_ARG, "particle type must be 0 or 1");
+  if (!(dt > 0) || !std::isfinite(dt)) return create_fail(DEM_ERR_ARG, "time step must be positive");
+  const std::string bad = check_domain(grid_spacing, verlet_dist, bbox_min, bbox_max, circ);
+  if (!bad.empty()) return create_fail(DEM_ERR_ARG, bad);
   int dev_count = 0;
-  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return DEM_ERR_CUDA;
-  if (!(grid_spacing > 0) || !(verlet_dist >= 0) || !(dt > 0) || !bbox_min || !bbox_max) return DEM_ERR_ARG;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return create_fail(DEM_ERR_CUDA, "no usable GPU");
   DemSim* s = nullptr;
   try {
     s = new DemSim();
     s->rot = particle_type ? 1 : 0;
     s->dt = dt; s->nrange = grid_spacing; s->alpha = verlet_dist;
     s->init_grid(bbox_min, bbox_max, circ);
-  } catch (const std::exception&) {
+  } catch (const dem::CudaError& e) {
     delete s;
-    return DEM_ERR_ARG;
+    return create_fail(DEM_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    delete s;
+    return create_fail(DEM_ERR_ARG, e.what());
   }
+  g_create_err.clear();
   *out = reinterpret_cast<dem_sim*>(s);
   return DEM_OK;
 }
@@ -2515,7 +2604,10 @@ int dem_destroy(dem_sim* h) {
   return DEM_OK;
 }
 
-const char* dem_last_error(dem_sim* h) { return h ? reinterpret_cast<DemSim*>(h)->err.c_str() : "null handle"; }
+const char* dem_last_error(dem_sim* h) {
+  if (h) return reinterpret_cast<DemSim*>(h)->err.c_str();
+  return g_create_err.empty() ? "null handle" : g_create_err.c_str();
+}
 
 int dem_add_particles(dem_sim* h, int n, const int* id, const int* tag, const double* pos, const double* rad,
                       const double* mass, const double* vel, const double* angvel, const double* quat,
@@ -3089,6 +3181,10 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
       s.adj_tangents = v;
     } else if (k == "adjoint_pair_duals") {
       s.adj_pair_duals = value != 0;
+    } else if (k == "event_capacity") {
+      if (!(value >= 0 && value <= 1 << 30) || value != std::floor(value))
+        throw std::invalid_argument("event_capacity must be a whole number in [0, 2^30] (0 = one entry per bond)");
+      s.set_event_capacity((int)value);
     } else if (k == "precision") {
       if (value != 32 && value != 64) throw std::invalid_argument("precision must be 64 or 32");
       s.set_precision(value == 32);

@@ -98,9 +98,10 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
   double Gs = 0.0;  // evaluation pass: sum of the contributions' magnitudes (the particle's force scale)
   // 3. dynamic pair groups (PIS_NE / PIS_ED::calcForces).  Contact is tested first from the
   //    positions alone; the partner's velocity / spin and the pair's history are gathered only
-  //    for touching pairs (a non-touching RotFriction pair just resets its history).  Adjacency
-  //    entries and partner positions are fetched kBatch at a time to keep several gathers in
-  //    flight per thread.
+  //    for touching pairs (a non-touching RotFriction pair just resets its history).  Each lane
+  //    takes one adjacency entry per pass (kBatch = 1); the gathers in flight come from the TPP
+  //    lanes of a particle and the warps resident on the SM, not from batching within a thread.
+  //    kBatch > 1 would fetch that many entries and partner positions per lane before use.
   KSum3 Fk, Mk;                                      // FP32 form
   Fk.zero();
   Mk.zero();

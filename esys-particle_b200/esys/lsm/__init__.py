@@ -12,6 +12,8 @@ raise ``NotImplementedError``.
 """
 from __future__ import annotations
 
+import sys
+
 import numpy as np
 
 from . import _capi
@@ -259,6 +261,7 @@ class LsmMpi:
         self._pending = []  # particles created before setSpatialDomain
         self._walls = {}
         self._wig_of_wall = {}
+        self._bonded, self._dynamic = set(), set()  # group names, for createExclusion
         self._bbox, self._circ = None, (False, False, False)
 
     # -- set-up (LsmMpiPy.cpp:2187-2300) --
@@ -341,31 +344,40 @@ class LsmMpi:
         s = self._require()
         if isinstance(prms, NRotElasticPrms):
             s.add_elastic_group(prms.name, prms.normalK, prms.scaling)
+            self._dynamic.add(prms.name)
         elif isinstance(prms, RotFrictionPrms):
             if prms.rigid:
                 raise NotImplementedError("RotFrictionPrms(rigid=True) is not on the GPU path")
             s.add_rot_friction_group(prms.name, prms.normalK, prms.staticMu, prms.dynamicMu, prms.shearK, self._dt,
                                      prms.scaling, prms.meanR_scaling)
+            self._dynamic.add(prms.name)
         elif isinstance(prms, RotBondPrms):
             s.add_rot_bond_group(prms.name, prms.tag, prms.normalK, prms.shearK, prms.torsionK, prms.bendingK,
                                  prms.normalBrkForce, prms.shearBrkForce, prms.torsionBrkForce, prms.bendingBrkForce,
                                  prms.scaling, prms.meanR_scaling, prms.truncated)
+            self._bonded.add(prms.name)
         elif isinstance(prms, NRotFrictionPrms):  # LsmMpiPy::createNRotFrictionInteractGrp sets dt
             s.add_nrot_friction_group(prms.name, prms.normalK, prms.dynamicMu, prms.shearK, self._dt, prms.scaling)
+            self._dynamic.add(prms.name)
         elif isinstance(prms, HertzMindlinPrms):  # LsmMpiPy::createHertzMindlinIG sets dt (LsmMpiPy.cpp:508-517)
             s.add_hertz_mindlin_group(prms.name, prms.youngsModulus, prms.poissonsRatio, prms.dynamicMu, self._dt)
+            self._dynamic.add(prms.name)
         elif isinstance(prms, BrittleBeamDZCPrms):  # LsmMpiPy::createBrittleBeamDZCInteractGrp
             s.add_brittle_beam_dzc_group(prms.name, prms.tag, prms.kr, prms.ks, prms.kt, prms.kb, prms.cohesion,
                                          prms.tensileCutoff, prms.compressCutoff, prms.frictionAngle, prms.beta1,
                                          prms.beta2)
+            self._bonded.add(prms.name)
         elif isinstance(prms, BrittleBeamSCPrms):  # LsmMpiPy::createBrittleBeamSCInteractGrp
             s.add_brittle_beam_sc_group(prms.name, prms.tag, prms.kr, prms.ks, prms.kt, prms.kb, prms.cohesion,
                                         prms.tensileCutoff, prms.frictionAngle)
+            self._bonded.add(prms.name)
         elif isinstance(prms, HertzMindlinViscoPrms):  # LsmMpiPy::createHertzMindlinViscoIG sets dt
             s.add_hertz_mindlin_visco_group(prms.name, prms.youngsModulus, prms.poissonsRatio, prms.dynamicMu,
                                             prms.restitution, self._dt)
+            self._dynamic.add(prms.name)
         elif isinstance(prms, NRotBondPrms):
             s.add_nrot_bond_group(prms.name, prms.tag, prms.normalK, prms.breakDistance, prms.scaling)
+            self._bonded.add(prms.name)
         elif isinstance(prms, NRotElasticWallPrms):
             s.add_wall_group(prms.name, prms.wallName, prms.normalK)
             self._wig_of_wall[prms.name] = prms.wallName
@@ -391,20 +403,35 @@ class LsmMpi:
     createLocalDamping = createRotLocalDamping = createGravity = createDamping
 
     def createExclusion(self, interactionName1, interactionName2):
-        self._require().add_exclusion(interactionName1, interactionName2)
+        """TSubLattice::setExIG (SubLattice.hpp:1980-2009): a name that names no group is
+        reported on the error console and the run goes on without the exclusion."""
+        s = self._require()
+        if interactionName1 not in self._bonded or interactionName2 not in self._dynamic:
+            print("TSubLattice<T>::setExIG() - nonexisting interaction group", file=sys.stderr)
+            return
+        s.add_exclusion(interactionName1, interactionName2)
 
     # -- walls and particles during the run --
+    # A wall (or wall group) name that names nothing is ignored by the workers, and its
+    # position and force read as zero (TSubLattice::moveWallBy, getWallPos, getWallForce,
+    # applyForceToWall: SubLattice.hpp:2878-2891, 835-860, 897-921, 2935-2948).
     def moveWallBy(self, name, move):
-        self._require().move_wall(name, list(move))
+        if name in self._walls:
+            self._require().move_wall(name, list(move))
 
     def getWallPosition(self, name):
+        if name not in self._walls:
+            return Vec3(0.0, 0.0, 0.0)
         return Vec3(*self._require().wall(name)[0])
 
     def getWallForce(self, name):
+        if name not in self._walls:
+            return Vec3(0.0, 0.0, 0.0)
         return Vec3(*self._require().wall(name)[1])
 
     def applyForceToWall(self, interactionName, force):
-        self._require().apply_force_to_wall(interactionName, list(force))
+        if interactionName in self._wig_of_wall:
+            self._require().apply_force_to_wall(interactionName, list(force))
 
     def moveTaggedParticlesBy(self, tag, displacement):
         self._require().move_tagged(int(tag), list(displacement))

@@ -119,8 +119,16 @@ def _v3(v):
     return np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(3))
 
 
+# Status codes of include/esys_dem.h
+DEM_OK, DEM_ERR_ARG, DEM_ERR_OVERFLOW, DEM_ERR_CUDA, DEM_ERR_INTERNAL, DEM_ERR_STATE = 0, -1, -2, -3, -4, -5
+
+
 class DemError(RuntimeError):
-    pass
+    """A failed library call; ``status`` is its DEM_ERR_* code (None where no call failed)."""
+
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status
 
 
 class DemSim:
@@ -135,7 +143,7 @@ class DemSim:
         rc = self.lib.dem_create(C.byref(self.h), pt, float(grid_spacing), float(verlet_dist), _dp(mn), _dp(mx),
                                  _ip(cc), float(dt))
         if rc != 0:
-            raise DemError(f"dem_create failed ({rc}): no usable GPU or invalid domain")
+            raise DemError(self.lib.dem_last_error(None).decode(), rc)
         self.rot = pt == 1
         self.wall_groups = []  # wall interaction groups, in the library's (name) order
         self._bond_prm = {}    # RotBond group -> [normalK, shearK, torsionK, bendingK]
@@ -144,7 +152,7 @@ class DemSim:
 
     def _chk(self, rc):
         if rc < 0:
-            raise DemError(self.lib.dem_last_error(self.h).decode())
+            raise DemError(self.lib.dem_last_error(self.h).decode(), rc)
         return rc
 
     def close(self):
@@ -507,7 +515,7 @@ class Ensemble:
 
     def _chk(self, rc):
         if rc < 0:
-            raise DemError(self.lib.dem_ensemble_last_error(self.h).decode())
+            raise DemError(self.lib.dem_ensemble_last_error(self.h).decode(), rc)
         return rc
 
     def step(self, n=1):

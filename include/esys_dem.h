@@ -40,7 +40,12 @@ enum {
  * (Parallel/LatticeMaster.cpp:528-553, 574-583, 613-693) -> TSubLattice ctor and
  * initNeighborTable(min, max[, circ]) (Parallel/SubLattice.hpp:455-564).
  * grid_spacing / verlet_dist are initNeighbourSearch's gridSpacing and
- * verletDist; circ[0] != 0 makes x periodic (circDimList). */
+ * verletDist; circ[0] != 0 makes x periodic (circDimList).  The domain is checked on the host
+ * before any device is touched, so a bad one returns DEM_ERR_ARG with or without a GPU:
+ * bbox_max <= bbox_min or a non-finite corner, grid_spacing <= 0, verlet_dist < 0, dt <= 0,
+ * circ[1] or circ[2] set, a periodic x side shorter than 3 grid spacings, more than 2^31 - 1
+ * cells.  Without a usable GPU a valid domain returns DEM_ERR_CUDA.  Failing, *out is NULL and
+ * dem_last_error(NULL) gives this thread's last dem_create failure. */
 int dem_create(dem_sim** out, int particle_type, double grid_spacing, double verlet_dist, const double* bbox_min,
                const double* bbox_max, const int* circ, double dt);
 int dem_destroy(dem_sim* h);
@@ -268,7 +273,8 @@ int dem_precision_report(dem_sim* h, double* out, int n);
 int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const double* walls, double* reactions,
                                void* stream);
 
-/* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic, 1, 2, 4, 8),
+/* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic, 1, 2, 4, 8,
+ * 16 = block-cooperative tiles),
  * "chunk" (steps launched per host round trip), "store_forces" (keep per-particle F/M),
  * "profile" (time the force/integration kernels with CUDA events), "precision" (64 = FP64 form,
  * 32 = FP32 pair forces with Kahan-compensated accumulation, FP64 positions / contact detection /
@@ -276,7 +282,12 @@ int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const 
  * evaluated once per step and gathered), "bond_handoff" (1: bond failures handed to the friction
  * lists on the device), "adjoint_bond_tangents" (0: hand-written RotBond reverse; 3, 6, 9, 18:
  * forward-mode dual tangents per pass), "adjoint_pair_duals" (0: hand-written pair-law
- * reverses; 1: forward-mode duals). */
+ * reverses; 1: forward-mode duals), "event_capacity" (entries of each bonded group's failure-event
+ * log, existing groups and later ones; 0 = one per bond, the default, which cannot overflow; a
+ * smaller log that fills makes the dem_step or dem_ensemble_step call in which it filled return
+ * DEM_ERR_OVERFLOW after running all its steps; the bond states stay exact, dem_get_breaks holds
+ * the events logged before it filled, later calls go on, and the capacity of a group whose log
+ * overflowed can no longer change). */
 int dem_set_option(dem_sim* h, const char* key, double value);
 
 /* ---- Field savers ----------------------------------------------------------------------- */

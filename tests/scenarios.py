@@ -512,3 +512,42 @@ def wide_friction_pack(make, nx=12, ny=5, nz=6, extra_x=8.0, skin=0.05, **kw):
     def wider(pt, gs, vd, lo, hi, circ, dt):
         return make(pt, gs, skin, lo, (hi[0] + extra_x, hi[1], hi[2]), circ, dt)
     return friction_pack(wider, nx=nx, ny=ny, nz=nz, **kw)
+
+
+def damped_cloud(make, rot=True, n_side=4, seed=5, dt=1e-3, visc=100.0, max_iter=3, vdecades=(-6.0, 1.0)):
+    """Isolated spheres (no contacts) under gravity with linear (and rotational) damping of
+    viscosity * dt = 0.1, speeds spread over decades: the damping fixed point converges in
+    a few iterations for slow particles and in more for fast ones, so a small maxIterations
+    splits them into damped particles and particles left undamped (v_rel = 0)."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(*[np.arange(n_side)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    n = len(g)
+    pos = (g + 0.5) * 3.0
+    rad = np.full(n, 0.4)
+
+    def spread():
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        return d * 10.0 ** rng.uniform(*vdecades, size=(n, 1))
+
+    L = 3.0 * n_side
+    sim = make("RotSphere" if rot else "NRotSphere", 1.2, 0.2, (0, 0, 0), (L, L, L), (0, 0, 0), dt)
+    sim.add_particles(np.arange(n), pos, rad, sphere_mass(rad), tag=np.zeros(n, np.int32), vel=spread(),
+                      angvel=spread() if rot else None)
+    sim.add_elastic_group("elastic", 1000.0, True)
+    sim.add_gravity("gravity", (0, 0, -9.81))
+    sim.add_damping(0, visc, max_iter)
+    if rot:
+        sim.add_damping(1, visc, max_iter)
+    return sim
+
+
+def damping_iterations(v, f, inv_mass, mass, visc, dt, max_iter):
+    """Iteration count of CDamping<T>::calcForces (Model/Damping.hpp:99-124) for one particle."""
+    v_rel, error, count = np.zeros(3), 1.0, 0
+    while error * error > 1e-12 and count < max_iter:
+        count += 1
+        old = v_rel
+        v_rel = v + inv_mass * dt * (f - v_rel * visc * mass)
+        error = float(np.dot(v_rel - old, v_rel - old))
+    return count

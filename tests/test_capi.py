@@ -1,7 +1,6 @@
 """The C-ABI library builds, loads and exports every symbol include/esys_dem.h
 declares (no compute: runs without a GPU); without a GPU dem_create fails
 with a status instead of falling back to the CPU."""
-import ctypes
 import os
 import re
 
@@ -37,8 +36,3 @@ def test_create_without_gpu_fails_loudly(dem_lib):
 
     with pytest.raises(_capi.DemError):
         _capi.DemSim("NRotSphere", 1.2, 0.2, (0, 0, 0), (5, 5, 5))
-
-
-def test_null_handle_error_text(dem_lib):
-    dem_lib.dem_last_error.restype = ctypes.c_char_p
-    assert dem_lib.dem_last_error(None) == b"null handle"
