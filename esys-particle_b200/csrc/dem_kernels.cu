@@ -892,7 +892,8 @@ __global__ void k_particle_field(Particles P, int cur, int rot, int field, doubl
     case 3: r = norm(v); break;                                                     // v_abs
     case 4: r = p.w; break;                                                         // radius
     case 5: r = (double)P.id[i]; break;                                             // id
-    default: r = (double)P.tag[i]; break;                                           // tag
+    case 6: r = (double)P.tag[i]; break;                                            // tag
+    default: r = vm.w; break;                                                       // mass
   }
   out[i] = r;
 }

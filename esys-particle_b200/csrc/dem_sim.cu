@@ -3115,10 +3115,12 @@ int dem_set_stream(dem_sim* h, void* stream) {
 
 int dem_get_counters(dem_sim* h, long long* out, int n) {
   return guard(h, [&](DemSim& s) {
-    long long v[8] = {s.c_steps, s.c_contacts, s.c_rebuilds, s.c_launches,
-                      (long long)(s.prof_ms * 1e6), s.prof_steps, s.contacts_per_step(), (long long)s.pick_tpp()};
-    for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
-    return std::min(n, 8);
+    const long long search_due = (s.first || (s.pending_ctrl & dem::CTRL_REBUILD)) ? 1 : 0;
+    long long v[9] = {s.c_steps, s.c_contacts, s.c_rebuilds, s.c_launches,
+                      (long long)(s.prof_ms * 1e6), s.prof_steps, s.contacts_per_step(), (long long)s.pick_tpp(),
+                      search_due};
+    for (int i = 0; i < n && i < 9; ++i) out[i] = v[i];
+    return std::min(n, 9);
   });
 }
 
@@ -3197,10 +3199,10 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
 
 int dem_particle_scalar_field(dem_sim* h, const char* field, double* values) {
   return guard(h, [&](DemSim& s) {
-    static const char* names[] = {"e_kin", "e_kin_linear", "e_kin_rot", "v_abs", "radius", "id", "tag"};
+    static const char* names[] = {"e_kin", "e_kin_linear", "e_kin_rot", "v_abs", "radius", "id", "tag", "mass"};
     const std::string f = field ? field : "";
     int code = -1;
-    for (int k = 0; k < 7; ++k)
+    for (int k = 0; k < 8; ++k)
       if (f == names[k]) code = k;
     if (code < 0) throw std::invalid_argument("unknown particle scalar field " + f);
     if (!values) throw std::invalid_argument("null output");

@@ -298,10 +298,10 @@ class DemSim:
         self._chk(self.lib.dem_set_stream(self.h, C.c_void_p(int(stream_handle))))
 
     def counters(self):
-        out = (C.c_longlong * 8)()
-        self._chk(self.lib.dem_get_counters(self.h, out, 8))
+        out = (C.c_longlong * 9)()
+        self._chk(self.lib.dem_get_counters(self.h, out, 9))
         keys = ("steps", "contact_updates", "rebuilds", "launches", "step_kernel_ns", "profiled_steps",
-                "contacts_per_step", "threads_per_particle")
+                "contacts_per_step", "threads_per_particle", "search_due")
         return dict(zip(keys, list(out)))
 
     def get_particles_raw(self, id_ptr, pos_ptr, vel_ptr, angvel_ptr, quat_ptr, force_ptr, moment_ptr):

@@ -240,7 +240,10 @@ int dem_set_stream(dem_sim* h, void* stream);
  * phases instead): out[0] steps, [1] interactions evaluated (Verlet pairs + intact bonds + wall
  * candidates, summed over steps), [2] neighbour searches, [3] kernel launches, [4] device time of
  * the force/integration kernels in ns (with option "profile"), [5] steps timed by [4],
- * [6] interactions evaluated per step now, [7] threads per particle in use.  Returns entries written. */
+ * [6] interactions evaluated per step now, [7] threads per particle in use, [8] 1 when a neighbour
+ * search is due at the head of the next step (a particle moved more than verletDist/2 since the
+ * last search, dem_search_neighbors was called, or no step has run yet: what
+ * TSubLattice::checkNeighbors reports, Parallel/SubLattice.hpp:2473-2520).  Returns entries written. */
 int dem_get_counters(dem_sim* h, long long* out, int n);
 
 /* Precision check of the FP32-force form, no reference counterpart: from the FP64 form, evaluates
@@ -295,7 +298,8 @@ int dem_set_option(dem_sim* h, const char* key, double value);
 /* Per-particle scalar field, computed on the device in the reference's accessor arithmetic
  * (CParticle / CRotParticle::getScalarFieldFunction, Model/Particle.cpp:140-160,
  * Model/RotParticle.cpp:422-456): "e_kin", "e_kin_linear", "e_kin_rot", "v_abs", "radius",
- * "id", "tag".  values[] in dem_get_particles order; returns the count. */
+ * "id", "tag", and "mass" (no reference field: CParticle::getMass).  values[] in
+ * dem_get_particles order; returns the count. */
 int dem_particle_scalar_field(dem_sim* h, const char* field, double* values);
 
 /* Per-particle vector field (CParticle::getVectorFieldFunction, Model/Particle.cpp:166-184;

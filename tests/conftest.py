@@ -46,3 +46,20 @@ def oracle_libs():
     import oracle
 
     return oracle
+
+
+@pytest.fixture(scope="session")
+def binding_lib(dem_lib):
+    """The ASubLattice binding's test build (tests/binding): rebuilt when the reference tree is
+    present, else the prebuilt library; skipped when neither exists."""
+    import ctypes
+    import subprocess
+
+    bdir = os.path.join(ROOT, "tests", "binding")
+    ref = os.environ.get("ESYS_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-j8", "-C", bdir, f"REF={ref}"], check=True)
+    path = os.path.join(bdir, "_build", "libsublattice_binding.so")
+    if not os.path.exists(path):
+        pytest.skip("binding test build absent (needs the reference tree to build)")
+    return ctypes.CDLL(path)
