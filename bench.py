@@ -1053,6 +1053,29 @@ def main():
         sim.step(args.dem_steps)
         sim.apply_force_to_wall("top_w", (0.0, -NORMAL_LOAD, 0.0))
 
+    sweeps = {}
+
+    def pick_lanes(sim, label):
+        """Lanes per particle measured on this workload before the timed steps: one lane, two
+        lanes, and the warp-cooperative pair sums (32); the fastest is kept."""
+        if args.tpp:
+            return
+        table = {}
+        for t in (1, 2, 32):
+            sim.set_option("threads_per_particle", t)
+            bench_step(sim)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(2):
+                bench_step(sim)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            table[t] = e0.elapsed_time(e1) / 2
+        best = min(table, key=table.get)
+        sim.set_option("threads_per_particle", best)
+        sweeps[label] = {"chosen": best, "ms_per_bench_step": {str(k): round(v, 4) for k, v in table.items()}}
+
     def timed(sim, clk=None):
         for _ in range(args.warmup):
             bench_step(sim)
@@ -1072,12 +1095,14 @@ def main():
     fp64 = None
     if args.precision == 32 and not args.no_fp64_compare:
         s64 = make_sim(64)
+        pick_lanes(s64, "fp64")
         a0, a1, ms64 = timed(s64)
         ns64 = (a1["step_kernel_ns"] - a0["step_kernel_ns"]) / max(1, a1["profiled_steps"] - a0["profiled_steps"])
         fp64 = {"value": (a1["contact_updates"] - a0["contact_updates"]) / (ms64 / 1e3), "kernel_us": ns64 / 1e3,
                 "ms_per_step": ms64 / args.steps}
         s64.close()
     sim = make_sim(args.precision)
+    pick_lanes(sim, "fp32" if args.precision == 32 else "fp64")
     with Clocks(local) as clk:
         c0, c1, ms = timed(sim)
     err = None
@@ -1185,6 +1210,7 @@ def main():
                        "friction_pairs": m_fric, "wall_candidates": n_wall_cand,
                        "touching_friction_pairs": touching,
                        "threads_per_particle": c1["threads_per_particle"],
+                       "lanes_sweep": sweeps,
                        "l2": "flushed (256 MB write) between bench steps; the step's working set (~110 MB) is "
                              "close to the 126 MB L2, so part of it stays resident between timesteps",
                        "parallelism": "replicas only" if world > 1 else "single GPU",

@@ -34,6 +34,7 @@ constexpr int kMaxBond = 2;
 constexpr int kBondAlive = 0x7fffffff;
 constexpr int kBondPassThreads = 128;  // bonds per block of the bond pass
 constexpr int kTiled = 16;             // threads_per_particle setting of the tiled step kernels (dem_tiled.cuh)
+constexpr int kWarpCoop = 32;          // threads_per_particle setting of the warp-cooperative pair sums (dem_step.cuh)
 #ifndef DEM_TILE_THREADS
 #define DEM_TILE_THREADS 256
 #endif
@@ -158,6 +159,8 @@ struct StepArgs {
   double visc_loc, visc_rotloc;
   int store_forces;
   long long force_step;     // forces are stored by this step only (-1: by every step)
+  bool skip_vw;             // FP32 form: do not keep the FP32 velocity shadow (vw) up to date; set only
+                            // where no kernel of the chunk reads it (the lane kernels read vm / wi)
   // device bond hand-off: a bond failure does not stop the chunk; the pairs it excluded turn
   // into ordinary pairs (DynDev::xbond) and every particle refreshes its wall candidacy at the
   // step after a failure (brk_step: last step with a failure)

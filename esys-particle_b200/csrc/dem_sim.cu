@@ -939,6 +939,7 @@ struct DemSim {
       for (int j = 0; j < k; ++j) {
         StepArgs a = make_args((cur + j) & 1);
         a.force_step = t_last;
+        a.skip_vw = t_pp != kTiled;  // only the tiled kernels read the FP32 velocity shadow
         if (fp32) launch_step_fp32(a, rot != 0, t_pp, false, two, s);
         else launch_step(a, rot != 0, t_pp, two, s);
       }
@@ -3159,8 +3160,8 @@ int dem_set_option(dem_sim* h, const char* key, double value) {
     std::string k = key ? key : "";
     if (k == "threads_per_particle") {
       int v = (int)value;
-      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8 && v != dem::kTiled)
-        throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8 or 16 (tiled)");
+      if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8 && v != dem::kTiled && v != dem::kWarpCoop)
+        throw std::invalid_argument("threads_per_particle must be 0,1,2,4,8, 16 (tiled) or 32 (warp-cooperative)");
       s.tpp = v;
     } else if (k == "chunk") {
       if (value < 1) throw std::invalid_argument("chunk must be >= 1");

@@ -52,11 +52,22 @@ constexpr int kStepWarps = kStepThreads / 32;
 #define DEM_FP32_BLOCKS 3
 #endif
 constexpr int kFp32Blocks = DEM_FP32_BLOCKS;  // resident blocks per SM targeted by the FP32 pair instances
+// Adjacency entries each lane of the pair loop fetches before using them.
+#ifndef DEM_KBATCH
+#define DEM_KBATCH 1
+#endif
+// 1: the fused step runs one persistent wave of blocks striding over the particle tiles;
+// 0: one block per tile, the hardware scheduler balancing blocks across the SMs.
+#ifndef DEM_STEP_PERSISTENT
+#define DEM_STEP_PERSISTENT 1
+#endif
 
 // Lanes per particle of a threads_per_particle setting, in units of kStepThreads per tile:
 // the tiled kernels (kTiled, dem_tiled.cuh) give each particle one thread of a block of
 // kTileThreads, i.e. a tile of kTileThreads particles.
-__host__ __device__ __forceinline__ int tile_lanes(int tpp) { return tpp == kTiled ? kStepThreads / kTileThreads : tpp; }
+__host__ __device__ __forceinline__ int tile_lanes(int tpp) {
+  return tpp == kTiled ? kStepThreads / kTileThreads : (tpp == kWarpCoop ? 1 : tpp);
+}
 
 __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
   tpp = tile_lanes(tpp);
@@ -73,6 +84,14 @@ __host__ __device__ __forceinline__ int step_tiles(int n, int tpp) {
 // F_STRESS: each particle's stress sum (CParticle::m_sigma) is accumulated and stored in a.sig
 // (BrittleBeamSC groups read it in their failure test).
 enum : int { F_ELASTIC = 1, F_FRIC = 2, F_BOND = 4, F_BGATHER = 8, F_NFRIC = 16, F_STRESS = 32 };
+
+// Instances the warp-cooperative pair sums cover: the dynamic groups' contact laws (Elastic,
+// RotFriction) with gathered bond records; the widened laws, in-line bonds and stress sums keep
+// the lane loop.
+template <int FEAT>
+struct WarpCoopSupported {
+  static constexpr bool value = (FEAT & (F_NFRIC | F_BOND | F_STRESS)) == 0;
+};
 
 // CParticle::applyForce's stress update (Model/Particle.cpp:392-401): m_sigma(i,j) -= f[i] * (pos - x)[j].
 __device__ __forceinline__ void stress_add(double* S, const V& f, const V& pos, const V& x) {
@@ -106,13 +125,15 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
   Fk.zero();
   Mk.zero();
   if ((FEAT & (F_ELASTIC | F_FRIC | F_NFRIC)) && alive) {
-    constexpr int kBatch = 1;
+    constexpr int kBatch = DEM_KBATCH;
     Vf vself = mk(0.f, 0.f, 0.f), wself = vself;
     double4 v4 = make_double4(0.0, 0.0, 0.0, 0.0), w4 = v4;
     if (FP32) {
-      const float4 r0 = __ldg(in.vw + 2 * i), r1 = __ldg(in.vw + 2 * i + 1);
-      vself = mk(r0.x, r0.y, r0.z);
-      wself = mk(r0.w, r1.x, r1.y);
+      if (ROT && (FEAT & F_FRIC)) {  // the FP32 form's velocity and spin: the FP64 records rounded
+        const double4 a0 = ldg4(in.vm + i), a1 = ldg4(in.wi + i);
+        vself = mk((float)a0.x, (float)a0.y, (float)a0.z);
+        wself = mk((float)a1.x, (float)a1.y, (float)a1.z);
+      }
     } else if (FEAT & (F_FRIC | F_NFRIC)) {
       v4 = ldg4(in.vm + i);
       if (ROT) w4 = ldg4(in.wi + i);
@@ -253,8 +274,8 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
                   Fp += -1.0 * o.Ffric;
                 }
               } else {
-                const float4 r0 = __ldg(in.vw + 2 * j), r1 = __ldg(in.vw + 2 * j + 1);
-                const Vf vj = mk(r0.x, r0.y, r0.z), wj = mk(r0.w, r1.x, r1.y);
+                const double4 b0 = ldg4(in.vm + j), b1 = ldg4(in.wi + j);
+                const Vf vj = mk((float)b0.x, (float)b0.y, (float)b0.z), wj = mk((float)b1.x, (float)b1.y, (float)b1.z);
                 Vf hF;
                 bool hs;
                 if (EVAL) {  // evaluation pass of an FP64 run: its FP64 history
@@ -408,6 +429,259 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
   if (EVAL && gross) *gross = Gs;
 }
 
+// Warp-cooperative pair sums (threads_per_particle = kWarpCoop), for the particle layout of
+// TPP = 1: one thread per particle, 32 consecutive particle slots per warp.  The warp's
+// adjacency entries of a group are one contiguous range of the CSR (the particles' ranges in
+// lane order); the warp takes them 32 at a time, one entry per lane, so the adjacency reads
+// are coalesced and each lane has one partner gather in flight per batch however the entries
+// are spread over the particles (a lane of the one-lane loop walks its own particle's entries
+// one dependent gather after another, and its warp waits for the longest list).  The owner of
+// an entry is the last lane whose range starts at or before it.  A touching entry's
+// contributions go to the owner's lane in entry order (lanes in order within a batch, batches
+// in order), so every particle adds the contributions the one-lane loop adds, in the same
+// order: the sums are those of TPP = 1.
+template <bool ROT, int FEAT, bool FP32, bool EVAL>
+__device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const ParticleBuf& in, int i, bool valid, bool alive,
+                                               long long step, const double4& p4, V& Fp, V& Mp, double* gross) {
+  static_assert(WarpCoopSupported<FEAT>::value, "instance outside the warp-cooperative pair sums");
+  constexpr unsigned kFull = 0xffffffffu;
+  const int wl = threadIdx.x & 31;
+  Fp = mk(0.0, 0.0, 0.0);
+  Mp = mk(0.0, 0.0, 0.0);
+  double Gs = 0.0;
+  KSum3 Fk, Mk;
+  Fk.zero();
+  Mk.zero();
+  if constexpr ((FEAT & (F_ELASTIC | F_FRIC)) != 0) {
+    // the owner-side records the friction law reads (as the one-lane loop loads them)
+    Vf vself = mk(0.f, 0.f, 0.f), wself = vself;
+    double4 v4 = make_double4(0.0, 0.0, 0.0, 0.0), w4 = v4;
+    if (ROT && (FEAT & F_FRIC) && alive) {
+      v4 = ldg4(in.vm + i);
+      w4 = ldg4(in.wi + i);
+      if (FP32) {  // the FP32 form's velocity and spin: the FP64 records rounded
+        vself = mk((float)v4.x, (float)v4.y, (float)v4.z);
+        wself = mk((float)w4.x, (float)w4.y, (float)w4.z);
+      }
+    }
+    for (int d = 0; d < a.ndyn; ++d) {
+      const DynDev& G = a.dyn[d];
+      int s0 = valid ? __ldg(G.adj_start + i) : 0;
+      const int s1 = valid ? __ldg(G.adj_start + i + 1) : 0;
+      const int w1 = __reduce_max_sync(kFull, s1);
+      if (!valid) s0 = w1;  // lanes past the last particle: empty ranges at the warp's end
+      const int w0 = __reduce_min_sync(kFull, s0);
+      for (int base = w0; base < w1; base += 32) {
+        const int e = base + wl;
+        const bool has = e < w1;
+        int o = 0;  // owner lane: the last lane whose range starts at or before e
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const int sv = __shfl_sync(kFull, s0, o + st);
+          if (sv <= e) o += st;
+        }
+        const int oi = __shfl_sync(kFull, i, o);
+        const bool oalive = __shfl_sync(kFull, (int)alive, o) != 0;
+        const double4 po = make_double4(__shfl_sync(kFull, p4.x, o), __shfl_sync(kFull, p4.y, o),
+                                        __shfl_sync(kFull, p4.z, o), __shfl_sync(kFull, p4.w, o));
+        const bool act = has && oalive;
+        const int2 en = act ? __ldg(G.adj + e) : make_int2(-1, 0);
+        const double4 pj = act ? ldg4(in.pr + en.x) : make_double4(0.0, 0.0, 0.0, 0.0);
+        const int j = en.x;
+        const bool isp1 = en.y < 0;
+        const int k = en.y & 0x7fffffff;
+        bool live = act;
+        if (act && G.xbond) {  // device bond hand-off: skipped while the bond that excluded it holds
+          const int xb = __ldg(G.xbond + k);
+          if (xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step) {
+            if (isp1 && !EVAL) {
+              if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+              else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+            live = false;
+          }
+        }
+        // canonical orientation: p1 = lower id
+        const double4 pa = isp1 ? po : pj, pb = isp1 ? pj : po;
+        const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
+        const V D = x1 - x2;
+        const double eq_dist = pa.w + pb.w;
+        const bool touching = live && dot(D, D) < (eq_dist * eq_dist);  // the laws' contact test
+        if (live && !touching && G.kind == 1 && isp1 && !EVAL) {  // CRotFrictionInteraction: no-contact branch
+          if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+          else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+        if (!__any_sync(kFull, touching)) continue;
+        // the owner's velocity and spin for the friction law
+        Vf vo = vself, wo = wself;
+        double4 vo4 = v4, wo4 = w4;
+        if (ROT && (FEAT & F_FRIC)) {
+          if (FP32) {
+            vo = mk(__shfl_sync(kFull, vself.x, o), __shfl_sync(kFull, vself.y, o), __shfl_sync(kFull, vself.z, o));
+            wo = mk(__shfl_sync(kFull, wself.x, o), __shfl_sync(kFull, wself.y, o), __shfl_sync(kFull, wself.z, o));
+          } else {
+            vo4 = make_double4(__shfl_sync(kFull, v4.x, o), __shfl_sync(kFull, v4.y, o), __shfl_sync(kFull, v4.z, o), 0.0);
+            wo4 = make_double4(__shfl_sync(kFull, w4.x, o), __shfl_sync(kFull, w4.y, o), __shfl_sync(kFull, w4.z, o), 0.0);
+          }
+        }
+        // this entry's contributions to its owner, in the order the one-lane loop adds them:
+        // forces c0 then c1 (c1 only for friction), moment cm
+        int nf = 0;
+        bool hm = false;
+        V c0 = mk(0.0, 0.0, 0.0), c1 = c0, cm = c0;
+        Vf f0 = mk(0.f, 0.f, 0.f), f1 = f0, fm = f0;
+        double g = 0.0;
+        if (touching) {
+          if (G.kind == 0) {
+            if constexpr ((FEAT & F_ELASTIC) != 0) {
+              if constexpr (!FP32) {
+                V f;
+                if (law_elastic(elastic_k(G.k, G.scaling, pa.w, pb.w), x1, pa.w, x2, pb.w, f)) {
+                  c0 = isp1 ? -1.0 * f : f;
+                  nf = 1;
+                }
+              } else {
+                Vf f;
+                if (law_elastic_f32(elastic_k(G.k, G.scaling, pa.w, pb.w), D, pa.w, pb.w, f)) {
+                  f0 = isp1 ? -f : f;
+                  nf = 1;
+                  if (EVAL) g = (double)norm(f);
+                }
+              }
+            }
+          } else {
+            if constexpr (ROT && (FEAT & F_FRIC) != 0) {
+              double keff, kseff;
+              friction_k(G.k, G.ks, G.scaling, G.meanR, pa.w, pb.w, keff, kseff);
+              if constexpr (!FP32) {
+                const double4 vj = ldg4(in.vm + j), wj = ldg4(in.wi + j);
+                const double4 va = isp1 ? vo4 : vj, vb = isp1 ? vj : vo4;
+                const double4 wa = isp1 ? wo4 : wj, wb = isp1 ? wj : wo4;
+                const double4 h = ldg4(G.hist_in + k);
+                FricOut fo;
+                law_friction(keff, kseff, G.mu_s, G.mu_d, G.dt, x1, pa.w, xyz(va), xyz(wa), x2, pb.w, xyz(vb),
+                             xyz(wb), mk(h.x, h.y, h.z), (((int)h.w) & 1) != 0, fo);
+                if (isp1) {
+                  c0 = -1.0 * fo.fn;
+                  c1 = fo.Ffric;
+                  cm = fo.M1;
+                  if (!EVAL)
+                    G.hist_out[k] = make_double4(fo.Ffric.x, fo.Ffric.y, fo.Ffric.z,
+                                                 (fo.slipping ? 1.0 : 0.0) + (fo.touching ? 2.0 : 0.0));
+                } else {
+                  c0 = fo.fn;
+                  c1 = -1.0 * fo.Ffric;
+                  cm = fo.M2;
+                }
+                nf = 2;
+                hm = true;
+              } else {
+                const double4 b0 = ldg4(in.vm + j), b1 = ldg4(in.wi + j);
+                const Vf vj = mk((float)b0.x, (float)b0.y, (float)b0.z), wj = mk((float)b1.x, (float)b1.y, (float)b1.z);
+                Vf hF;
+                bool hs;
+                if (EVAL) {  // evaluation pass of an FP64 run: its FP64 history
+                  const double4 h = ldg4(G.hist_in + k);
+                  hF = mk((float)h.x, (float)h.y, (float)h.z);
+                  hs = (((int)h.w) & 1) != 0;
+                } else {
+                  const float4 h = __ldg(G.hist32_in + k);
+                  hF = mk(h.x, h.y, h.z);
+                  hs = (((int)h.w) & 1) != 0;
+                }
+                FricOutF fo;
+                law_friction_f32(keff, kseff, G.mu_s, G.mu_d, (float)G.dt, D, pa.w, pb.w, isp1 ? vo : vj,
+                                 isp1 ? wo : wj, isp1 ? vj : vo, isp1 ? wj : wo, hF, hs, fo);
+                if (isp1) {
+                  f0 = -fo.fn;
+                  f1 = fo.Ffric;
+                  fm = fo.M1;
+                  if (!EVAL)
+                    G.hist32_out[k] = make_float4(fo.Ffric.x, fo.Ffric.y, fo.Ffric.z,
+                                                  (fo.slipping ? 1.f : 0.f) + (fo.touching ? 2.f : 0.f));
+                } else {
+                  f0 = fo.fn;
+                  f1 = -fo.Ffric;
+                  fm = fo.M2;
+                }
+                nf = 2;
+                hm = true;
+                if (EVAL) g = (double)norm(fo.fn) + (double)norm(fo.Ffric);
+              }
+            }
+          }
+        }
+        // deliver, source lanes in order
+        unsigned m = __ballot_sync(kFull, nf > 0);
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          const int dst = __shfl_sync(kFull, o, src);
+          const int snf = __shfl_sync(kFull, nf, src);
+          const bool shm = __shfl_sync(kFull, (int)hm, src) != 0;
+          if constexpr (FP32) {
+            const Vf a0 = mk(__shfl_sync(kFull, f0.x, src), __shfl_sync(kFull, f0.y, src), __shfl_sync(kFull, f0.z, src));
+            const Vf a1 = mk(__shfl_sync(kFull, f1.x, src), __shfl_sync(kFull, f1.y, src), __shfl_sync(kFull, f1.z, src));
+            const Vf am = mk(__shfl_sync(kFull, fm.x, src), __shfl_sync(kFull, fm.y, src), __shfl_sync(kFull, fm.z, src));
+            const double ag = EVAL ? __shfl_sync(kFull, g, src) : 0.0;
+            if (wl == dst) {
+              Fk.add(a0);
+              if (snf > 1) Fk.add(a1);
+              if (shm) Mk.add(am);
+              if (EVAL) Gs += ag;
+            }
+          } else {
+            const V a0 = mk(__shfl_sync(kFull, c0.x, src), __shfl_sync(kFull, c0.y, src), __shfl_sync(kFull, c0.z, src));
+            const V a1 = mk(__shfl_sync(kFull, c1.x, src), __shfl_sync(kFull, c1.y, src), __shfl_sync(kFull, c1.z, src));
+            const V am = mk(__shfl_sync(kFull, cm.x, src), __shfl_sync(kFull, cm.y, src), __shfl_sync(kFull, cm.z, src));
+            if (wl == dst) {
+              Fp += a0;
+              if (shm) Mp += am;
+              if (snf > 1) Fp += a1;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // bonds evaluated by the bond pass: their records gathered in adjacency order
+  if constexpr ((FEAT & F_BGATHER) != 0) {
+    if (alive) {
+      for (int d = 0; d < a.nbond; ++d) {
+        const BondDev& B = a.bond[d];
+        const int e0 = __ldg(B.adj_start + i), e1 = __ldg(B.adj_start + i + 1);
+        for (int e = e0; e < e1; ++e) {
+          const int2 en = __ldg(B.adj + e);
+          const int k = en.y & 0x7fffffff;
+          if constexpr (FP32 && !EVAL) {
+            const float4* rf = B.bf32 + 4 * (size_t)k + (en.y < 0 ? 0 : 2);
+            const float4 a0 = __ldg(rf), a1 = __ldg(rf + 1);
+            Fp += mk((double)a0.x, (double)a0.y, (double)a0.z);
+            if (ROT) Mp += mk((double)a0.w, (double)a1.x, (double)a1.y);
+            continue;
+          }
+          const double4* r = B.bf + 3 * (size_t)k;
+          if (en.y < 0) {
+            Fp += xyz(ldg4(r));
+            if (ROT) Mp += xyz(ldg4(r + 1));
+          } else {
+            Fp += -1.0 * xyz(ldg4(r));
+            if (ROT) Mp += xyz(ldg4(r + 2));
+          }
+          if (EVAL) Gs += norm(xyz(ldg4(r)));
+        }
+      }
+    }
+  }
+  if (FP32) {
+    // FP64-form sums (bonds) are added after the compensated FP32 pair sums
+    Fp = Fk.value() + Fp;
+    Mp = Mk.value() + Mp;
+  }
+  if (EVAL && gross) *gross = Gs;
+}
+
 // Walls, body force, the pair sums, damping and the integration of particle i
 // (TSubLattice::calcForces group order, then integrate + rescale).  Every thread
 // of the block calls this: the wall reactions are reduced across the block.
@@ -532,7 +806,7 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, long long ste
       }
       out.pr[i] = d4(x, p4.w);
       out.vm[i] = d4(v, v4.w);
-      if (FP32) {
+      if (FP32 && !a.skip_vw) {
         out.vw[2 * i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)w.x);
         out.vw[2 * i + 1] = make_float4((float)w.y, (float)w.z, 0.f, 0.f);
       }
@@ -733,16 +1007,17 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
   __shared__ bool s_last;
   if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
   const long long step = *a.step_counter + 1;
-  const int lane = threadIdx.x % TPP;
+  constexpr int LT = TPP == kWarpCoop ? 1 : TPP;  // lanes per particle of the particle's own work
+  const int lane = threadIdx.x % LT;
   const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const ParticleBuf in = a.P.buf[a.cur];
   const ParticleBuf out = a.P.buf[a.cur ^ 1];
   for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kStepThreads) (&s_red[0][0][0])[k] = 0.0;
   __syncthreads();
-  // Persistent grid: one wave of blocks strides over tiles of kStepThreads / TPP particles.
+  // Persistent grid: one wave of blocks strides over tiles of kStepThreads / LT particles.
   const int ntiles = step_tiles(a.P.n, TPP);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int i = (tile * kStepThreads + threadIdx.x) / TPP;
+    const int i = (tile * kStepThreads + threadIdx.x) / LT;
     const bool valid = i < a.P.n;
     // All of the particle's own loads are issued at once: the flags and position into
     // registers, the records needed after the pair loop into L1.
@@ -755,7 +1030,6 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
         prefetch_l1(in.vm + i);
         if (ROT) { prefetch_l1(in.wi + i); prefetch_l1(in.qq + i); }
         prefetch_l1(a.P.oldpos + i);
-        if (FP32 && ROT) prefetch_l1(in.vw + 2 * i);
         for (int d = 0; d < a.ndyn; ++d) prefetch_l1(a.dyn[d].adj_start + i);
       }
       if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);
@@ -766,9 +1040,12 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
     double Sg[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) Sg[c] = 0.0;
-    pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp, &gross, Sg);
-    finish_particle<ROT, TPP, FP32, EVAL>(a, step, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
-                                          ROT && (FEAT & F_BOND), Fp, Mp, s_red);
+    if constexpr (TPP == kWarpCoop)
+      pair_sums_warp<ROT, FEAT, FP32, EVAL>(a, in, i, valid, alive, step, p4, Fp, Mp, &gross);
+    else
+      pair_sums<ROT, TPP, FEAT, FP32, EVAL>(a, in, i, lane, alive, step, p4, q4, Fp, Mp, &gross, Sg);
+    finish_particle<ROT, LT, FP32, EVAL>(a, step, in, out, i, lane, wlane, warp, pf, alive, p4, q4,
+                                         ROT && (FEAT & F_BOND), Fp, Mp, s_red);
     if constexpr (!FP32 && !EVAL && (FEAT & F_STRESS) != 0) {
       if (alive && lane == 0) {
         const V xi = xyz(p4);
@@ -889,8 +1166,12 @@ inline void launch_split_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
 template <bool R, int T, int FEAT, bool FP32, bool EVAL>
 inline void launch_fused(const StepArgs& a, cudaStream_t s) {
   const int tiles = step_blocks(a.P.n, T);
+#if DEM_STEP_PERSISTENT
   const int wave = one_wave(k_step<R, T, FEAT, FP32, EVAL>);
   k_step<R, T, FEAT, FP32, EVAL><<<tiles < wave ? tiles : wave, kStepThreads, 0, s>>>(a);
+#else
+  k_step<R, T, FEAT, FP32, EVAL><<<tiles, kStepThreads, 0, s>>>(a);
+#endif
 }
 
 template <bool EVAL, bool FP32>

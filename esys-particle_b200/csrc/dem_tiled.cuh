@@ -456,6 +456,10 @@ inline void launch_step_tpp(const StepArgs& a, int tpp, cudaStream_t s) {
     if constexpr (TiledSupported<FEAT>::value) return launch_tiled<R, FEAT, FP32, EVAL>(a, s);
     tpp = 1;
   }
+  if (tpp == kWarpCoop) {
+    if constexpr (WarpCoopSupported<FEAT>::value) return launch_fused<R, kWarpCoop, FEAT, FP32, EVAL>(a, s);
+    tpp = 1;
+  }
   switch (tpp) {
     case 1: launch_fused<R, 1, FEAT, FP32, EVAL>(a, s); break;
     case 2: launch_fused<R, 2, FEAT, FP32, EVAL>(a, s); break;

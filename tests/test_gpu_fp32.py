@@ -28,7 +28,7 @@ def _check(sim):
     return list(out)
 
 
-@pytest.mark.parametrize("tpp", [1, 2, 4, 16])
+@pytest.mark.parametrize("tpp", [1, 2, 4, 16, 32])
 def test_fp32_force_error_friction(gpu, tpp):
     s = S.friction_pack(gpu)
     s.set_option("threads_per_particle", tpp)

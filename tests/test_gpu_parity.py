@@ -56,7 +56,7 @@ def test_gravity_box(gpu, orc, steps):
         assert np.abs(fa - fb).max() <= 1e-8 * max(np.abs(fb).max(), 1.0), w
 
 
-@pytest.mark.parametrize("tpp", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("tpp", [1, 2, 4, 8, 16, 32])
 def test_friction_pack_threads_per_particle(gpu, orc, tpp):
     a, b = S.friction_pack(gpu), S.friction_pack(orc)
     a.set_option("threads_per_particle", tpp)
