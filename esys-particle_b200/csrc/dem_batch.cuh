@@ -72,7 +72,6 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1 : ((FEAT & F
       if (lane == 0) {
         prefetch_l1(in.vm + i);
         if (ROT) { prefetch_l1(in.wi + i); prefetch_l1(in.qq + i); }
-        prefetch_l1(a.P.oldpos + i);
         if (FP32 && ROT) prefetch_l1(in.vw + 2 * i);
       }
       if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);

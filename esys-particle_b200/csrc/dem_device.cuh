@@ -63,6 +63,8 @@ struct Particles {
   ParticleBuf buf[2];
   double2* inv;          // 1/mass, 1/inertia
   double4* oldpos;       // position at the last neighbour search
+  float* dbound;         // upper bound of |position - oldpos| (FP32, rounded up): the step displacements
+                         // summed since the last search, or the exact distance after a host-side move
   double* cshift;        // accumulated circular shift in x (CParticle::m_circular_shift)
   double4* force;        // last accumulated force  (w unused)
   double4* moment;       // last accumulated moment (w unused)

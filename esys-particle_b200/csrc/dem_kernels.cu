@@ -99,6 +99,7 @@ __global__ void k_bin(Grid g, Particles P, int cur, int* cell_count) {
   }
   P.cell[i] = c;
   P.oldpos[i] = make_double4(p.x, p.y, p.z, 0.0);
+  P.dbound[i] = 0.f;
   atomicAdd(&cell_count[c], 1);
 }
 
@@ -456,6 +457,9 @@ __global__ void k_check_disp(Particles P, int cur, double half_alpha_sq, int* ct
   double4 p = P.buf[cur].pr[i], o = P.oldpos[i];
   V d = mk(p.x - o.x, p.y - o.y, p.z - o.z);
   if (dot(d, d) > half_alpha_sq) atomicOr(ctrl, CTRL_REBUILD);
+  // the bound the step kernels extend restarts from this distance (the subtraction's rounding
+  // of positions up to ~1e3 is covered by the absolute margin)
+  P.dbound[i] = __fadd_ru(__fmul_ru(__double2float_ru(sqrt(dot(d, d))), 1.0000005f), 1e-9f);
 }
 
 // moveTaggedParticlesBy (SubLattice.hpp:2577-2587): exact tag match.

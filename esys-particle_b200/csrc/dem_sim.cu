@@ -201,7 +201,7 @@ struct DemSim {
     for (auto& b : bond) b.second.release();
     win.release();
     void* ps[] = {P.buf[0].pr, P.buf[0].vm, P.buf[0].wi, P.buf[0].qq, P.buf[1].pr, P.buf[1].vm, P.buf[1].wi,
-                  P.buf[1].qq, P.buf[0].vw, P.buf[1].vw, P.inv, P.oldpos, P.force, P.moment, P.force_eval,
+                  P.buf[1].qq, P.buf[0].vw, P.buf[1].vw, P.inv, P.oldpos, P.dbound, P.force, P.moment, P.force_eval,
                   P.moment_eval, P.sum_f, P.sum_m, P.pflags, P.flagged, P.id, P.tag, P.cell, P.cshift};
     for (void* p : ps) if (p) cudaFree(p);
     cell_count.release(); cell_start.release(); cell_cursor.release(); cell_list.release();
@@ -302,7 +302,7 @@ struct DemSim {
       grow_array(P.buf[b].vw, 2 * n, 2 * nc);
     }
     grow_array(P.sum_f, n, nc); grow_array(P.sum_m, n, nc);
-    grow_array(P.inv, n, nc); grow_array(P.oldpos, n, nc); grow_array(P.force, n, nc); grow_array(P.moment, n, nc);
+    grow_array(P.inv, n, nc); grow_array(P.oldpos, n, nc); grow_array(P.dbound, n, nc); grow_array(P.force, n, nc); grow_array(P.moment, n, nc);
     grow_array(P.pflags, n, nc); grow_array(P.flagged, n, nc); grow_array(P.id, n, nc); grow_array(P.tag, n, nc);
     grow_array(P.cell, n, nc); grow_array(P.cshift, n, nc);
     cap = nc;

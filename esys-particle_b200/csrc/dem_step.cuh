@@ -814,10 +814,19 @@ __device__ __forceinline__ void finish_particle(const StepArgs& a, long long ste
         a.P.force[i] = d4(F, 0.0);
         if (ROT) a.P.moment[i] = d4(M, 0.0);
       }
-      // 7. displacement check for the next step (TSubLattice::checkNeighbors)
-      const double4 op = ldg4(a.P.oldpos + i);
-      const V dd = mk(x.x - op.x, x.y - op.y, x.z - op.z);
-      if (dot(dd, dd) > a.half_alpha_sq) atomicOr(a.ctrl, CTRL_REBUILD);
+      // 7. displacement check for the next step (TSubLattice::checkNeighbors): |x - oldpos| >
+      //    verletDist/2, evaluated exactly whenever the running bound of it (this step's
+      //    displacement added to the bound, in FP32 rounded up) does not already rule it out.
+      //    The difference of a position before and after one step is exact (the two are close),
+      //    so the bound only has to cover the norm's rounding.
+      const V sd = mk(x.x - xi.x, x.y - xi.y, x.z - xi.z);
+      const float b = __fadd_ru(a.P.dbound[i], __fmul_ru(__double2float_ru(sqrt(dot(sd, sd))), 1.0000005f));
+      a.P.dbound[i] = b;
+      if ((double)b * (double)b >= a.half_alpha_sq * 0.999999) {
+        const double4 op = ldg4(a.P.oldpos + i);
+        const V dd = mk(x.x - op.x, x.y - op.y, x.z - op.z);
+        if (dot(dd, dd) > a.half_alpha_sq) atomicOr(a.ctrl, CTRL_REBUILD);
+      }
     }
   }
 }
@@ -1029,7 +1038,6 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
       if (lane == 0) {
         prefetch_l1(in.vm + i);
         if (ROT) { prefetch_l1(in.wi + i); prefetch_l1(in.qq + i); }
-        prefetch_l1(a.P.oldpos + i);
         for (int d = 0; d < a.ndyn; ++d) prefetch_l1(a.dyn[d].adj_start + i);
       }
       if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);

@@ -396,7 +396,6 @@ __device__ __forceinline__ void tile_own(const StepArgs& a, const ParticleBuf& i
     if (DEM_TILED_PREFETCH) {
       prefetch_l1(in.vm + i);
       if (ROT) { prefetch_l1(in.wi + i); prefetch_l1(in.qq + i); }
-      prefetch_l1(a.P.oldpos + i);
       if (FP32 && ROT) prefetch_l1(in.vw + 2 * i);
     }
   }
