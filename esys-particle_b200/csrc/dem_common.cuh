@@ -82,6 +82,7 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
 
 // Bring a line into L1 without holding registers (records a kernel reads later).
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 __device__ __forceinline__ unsigned long long pair_key(int a, int b) {
   return ((unsigned long long)(unsigned)a << 32) | (unsigned)b;

@@ -934,7 +934,7 @@ struct DemSim {
         if (!ev0) { DEM_CUDA(cudaEventCreate(&ev0)); DEM_CUDA(cudaEventCreate(&ev1)); }
         DEM_CUDA(cudaEventRecord(ev0, s));
       }
-      if (fp32) launch_sync_vw(P, cur, s);
+      if (fp32 && t_pp == kTiled) launch_sync_vw(P, cur, s);  // only the tiled kernels read the shadow
       const bool two = split == 1;  // automatic = fused: measured faster on the 250k shear cell
       for (int j = 0; j < k; ++j) {
         StepArgs a = make_args((cur + j) & 1);

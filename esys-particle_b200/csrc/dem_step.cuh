@@ -61,6 +61,10 @@ constexpr int kFp32Blocks = DEM_FP32_BLOCKS;  // resident blocks per SM targeted
 #ifndef DEM_STEP_PERSISTENT
 #define DEM_STEP_PERSISTENT 1
 #endif
+// 1: while a tile is processed, the records of the block's next tile are prefetched into L2.
+#ifndef DEM_STEP_PREFETCH_NEXT
+#define DEM_STEP_PREFETCH_NEXT 0
+#endif
 
 // Lanes per particle of a threads_per_particle setting, in units of kStepThreads per tile:
 // the tiled kernels (kTiled, dem_tiled.cuh) give each particle one thread of a block of
@@ -1042,6 +1046,21 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
       }
       if (ROT && (FEAT & F_BOND)) q4 = ldg4(in.qq + i);
     }
+#if DEM_STEP_PREFETCH_NEXT
+    {  // the records of this thread's particle in the block's next tile, into L2
+      const int inext = ((tile + gridDim.x) * kStepThreads + threadIdx.x) / LT;
+      if (lane == 0 && inext < a.P.n) {
+        if (DEM_STEP_PREFETCH_NEXT == 2) prefetch_l1(in.pr + inext);
+        else prefetch_l2(in.pr + inext);
+        prefetch_l2(in.vm + inext);
+        if (ROT) { prefetch_l2(in.wi + inext); prefetch_l2(in.qq + inext); }
+        for (int d = 0; d < a.ndyn; ++d) {
+          if (DEM_STEP_PREFETCH_NEXT == 2) prefetch_l1(a.dyn[d].adj_start + inext);
+          else prefetch_l2(a.dyn[d].adj_start + inext);
+        }
+      }
+    }
+#endif
     const bool alive = valid && (pf & PF_ALIVE);
     V Fp, Mp;
     double gross = 0.0;
