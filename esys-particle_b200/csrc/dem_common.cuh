@@ -83,6 +83,11 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
 // Bring a line into L1 without holding registers (records a kernel reads later).
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+// Programmatic dependent launch (sm_90+): wait for the prerequisite grid's completion and memory
+// (returns at once for a grid launched without a programmatic dependency), and allow the
+// dependent grid to launch.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned long long pair_key(int a, int b) {
   return ((unsigned long long)(unsigned)a << 32) | (unsigned)b;

@@ -61,6 +61,10 @@ constexpr int kFp32Blocks = DEM_FP32_BLOCKS;  // resident blocks per SM targeted
 #ifndef DEM_STEP_PERSISTENT
 #define DEM_STEP_PERSISTENT 1
 #endif
+// 1: the fused step is launched as a programmatic dependent of the stream's previous kernel.
+#ifndef DEM_STEP_PDL
+#define DEM_STEP_PDL 1
+#endif
 // 1: while a tile is processed, the records of the block's next tile are prefetched into L2.
 #ifndef DEM_STEP_PREFETCH_NEXT
 #define DEM_STEP_PREFETCH_NEXT 0
@@ -1018,15 +1022,18 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
     k_step(const StepArgs a) {
   __shared__ double s_red[kStepWarps][kMaxWalls][3];
   __shared__ bool s_last;
-  if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
-  const long long step = *a.step_counter + 1;
   constexpr int LT = TPP == kWarpCoop ? 1 : TPP;  // lanes per particle of the particle's own work
   const int lane = threadIdx.x % LT;
   const int wlane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const ParticleBuf in = a.P.buf[a.cur];
   const ParticleBuf out = a.P.buf[a.cur ^ 1];
   for (int k = threadIdx.x; k < kStepWarps * kMaxWalls * 3; k += kStepThreads) (&s_red[0][0][0])[k] = 0.0;
+  // Launched as a programmatic dependent of the previous step (launch_fused): everything the
+  // previous step wrote is read after this wait, which returns once that grid has completed.
+  grid_dependency_wait();
   __syncthreads();
+  if (!EVAL && *a.stop) return;  // an earlier step of this chunk asked the host to intervene
+  const long long step = *a.step_counter + 1;
   // Persistent grid: one wave of blocks strides over tiles of kStepThreads / LT particles.
   const int ntiles = step_tiles(a.P.n, TPP);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -1094,6 +1101,9 @@ __global__ void __launch_bounds__(kStepThreads, (FEAT & F_BOND) ? 1
     // evaluation pass: the particle's contact-force scale beside its force (w of the record)
     if (EVAL && alive && lane == 0) reinterpret_cast<double*>(a.P.force_eval + i)[3] = gross;
   }
+  // the next step may start launching once every block is past its tiles (it waits for this
+  // grid's completion before reading anything)
+  grid_dependents_launch();
   if (EVAL) return;
   step_epilogue(a, step, wlane, warp, s_red, &s_last);
 }
@@ -1195,9 +1205,26 @@ inline void launch_fused(const StepArgs& a, cudaStream_t s) {
   const int tiles = step_blocks(a.P.n, T);
 #if DEM_STEP_PERSISTENT
   const int wave = one_wave(k_step<R, T, FEAT, FP32, EVAL>);
-  k_step<R, T, FEAT, FP32, EVAL><<<tiles < wave ? tiles : wave, kStepThreads, 0, s>>>(a);
+  const int grid = tiles < wave ? tiles : wave;
 #else
-  k_step<R, T, FEAT, FP32, EVAL><<<tiles, kStepThreads, 0, s>>>(a);
+  const int grid = tiles;
+#endif
+#if DEM_STEP_PDL
+  // programmatic dependent launch: the step's blocks are scheduled while the previous kernel
+  // of the stream finishes (its last block's epilogue), and wait in grid_dependency_wait
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kStepThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_step<R, T, FEAT, FP32, EVAL>, a);
+#else
+  k_step<R, T, FEAT, FP32, EVAL><<<grid, kStepThreads, 0, s>>>(a);
 #endif
 }
 
