@@ -551,3 +551,30 @@ def damping_iterations(v, f, inv_mass, mass, visc, dt, max_iter):
         v_rel = v + inv_mass * dt * (f - v_rel * visc * mass)
         error = float(np.dot(v_rel - old, v_rel - old))
     return count
+
+
+def fitted_window_block(make, n=2000, L=10.0, seed=4, kt=1e3, kb=1e3, visc=0.05, dt=1e-5):
+    """The differentiable-window benchmark's block at a small size: n spheres of radii in
+    [0.2, 1.0] fitted by the packer into L x 2L x L, every pair within a 1e-3 gap bonded, seeded
+    small initial velocities and spins, platens closing at 1.0, linear and rotational damping."""
+    from esys.lsm import geometry as G
+
+    pos, rad = G.fit_pack(n, (0, 0, 0), (L, 2 * L, L), 0.2, 1.0, seed=seed, max_failures=2000)
+    i1, i2 = G.distance_connections(pos, rad, 1e-3)
+    rng = np.random.default_rng(seed + 100)
+    m = len(rad)
+    sim = make("RotSphere", 2.2, 0.2, (0, 0, 0), (L, 2 * L, L), (0, 0, 0), dt)
+    sim.add_particles(np.arange(m), pos, rad, sphere_mass(rad), tag=np.zeros(m, np.int32),
+                      vel=rng.normal(0, 0.01, size=(m, 3)), angvel=rng.normal(0, 0.01, size=(m, 3)))
+    sim.add_connections(np.ones(len(i1), np.int32), i1, i2)
+    sim.add_rot_bond_group("bonds", 1, 1e5, 1e5, kt, kb, 1e6, 1e6, 1e6, 1e6, True, True, 1.0)
+    y0, y1 = float((pos[:, 1] - rad).min()), float((pos[:, 1] + rad).max())
+    sim.add_wall("bottom", (0, y0, 0), (0, 1, 0))
+    sim.add_wall("top", (0, y1, 0), (0, -1, 0))
+    sim.add_wall_group("bottom_w", "bottom", 1e5)
+    sim.add_wall_group("top_w", "top", 1e5)
+    sim.add_damping(0, visc, 100)
+    sim.add_damping(1, visc, 100)
+    sim.set_wall_velocity("bottom", (0, 1.0, 0))
+    sim.set_wall_velocity("top", (0, -1.0, 0))
+    return sim
