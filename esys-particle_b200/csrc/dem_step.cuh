@@ -157,24 +157,32 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           const int eb = e + b * TPP;
           en[b] = eb < e1 ? __ldg(G.adj + eb) : make_int2(-1, 0);
         }
+        // device bond hand-off: a pair is skipped while the bond that excluded it holds, and its
+        // partner record is not fetched
+        bool held[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+          held[b] = false;
+          if (G.xbond && en[b].x >= 0) {
+            const int xb = __ldg(G.xbond + (en[b].y & 0x7fffffff));
+            held[b] = xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step;
+          }
+        }
 #pragma unroll
         for (int b = 0; b < kBatch; ++b)
-          pjs[b] = en[b].x >= 0 ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
+          pjs[b] = (en[b].x >= 0 && !held[b]) ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
           if (en[b].x < 0) continue;
           const int j = en[b].x;
           const bool isp1 = en[b].y < 0;
           const int k = en[b].y & 0x7fffffff;
-          if (G.xbond) {  // device bond hand-off: skipped while the bond that excluded it holds
-            const int xb = __ldg(G.xbond + k);
-            if (xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step) {
-              if (isp1 && !EVAL) {
-                if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
-              }
-              continue;
+          if (held[b]) {
+            if (isp1 && !EVAL) {
+              if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+              else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
             }
+            continue;
           }
           const double4 pj = pjs[b];
           // canonical orientation: p1 = lower id
@@ -494,7 +502,6 @@ __device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const Particle
                                         __shfl_sync(kFull, p4.z, o), __shfl_sync(kFull, p4.w, o));
         const bool act = has && oalive;
         const int2 en = act ? __ldg(G.adj + e) : make_int2(-1, 0);
-        const double4 pj = act ? ldg4(in.pr + en.x) : make_double4(0.0, 0.0, 0.0, 0.0);
         const int j = en.x;
         const bool isp1 = en.y < 0;
         const int k = en.y & 0x7fffffff;
@@ -509,6 +516,7 @@ __device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const Particle
             live = false;
           }
         }
+        const double4 pj = live ? ldg4(in.pr + j) : make_double4(0.0, 0.0, 0.0, 0.0);
         // canonical orientation: p1 = lower id
         const double4 pa = isp1 ? po : pj, pb = isp1 ? pj : po;
         const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));

@@ -233,9 +233,20 @@ __device__ __forceinline__ void tile_eval_pairs(const StepArgs& a, const Particl
       const int u = u0 + b * kTileThreads;
       en[b] = u < m ? __ldg(G.adj + Eb + u) : make_int2(-1, 0);
     }
+    // under the device bond hand-off a pair is skipped while its excluding bond holds: its partner
+    // record is not needed (in a bonded specimen that is most of the friction list)
+    bool held[kB];
+#pragma unroll
+    for (int b = 0; b < kB; ++b) {
+      held[b] = false;
+      if (G.xbond && en[b].x >= 0) {
+        const int xb = __ldg(G.xbond + (en[b].y & 0x7fffffff));
+        held[b] = xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step;
+      }
+    }
 #pragma unroll
     for (int b = 0; b < kB; ++b)
-      pj[b] = en[b].x >= 0 ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
+      pj[b] = (en[b].x >= 0 && !held[b]) ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
     unsigned todo = 0u;
 #pragma unroll
     for (int b = 0; b < kB; ++b) {
