@@ -408,7 +408,7 @@ __device__ __forceinline__ void adj_post_one(const AdjArgs& A, int i) {
     const AdjDyn& G = A.dyn[d];
     for (int e = G.adj_start[i]; e < G.adj_start[i + 1]; ++e) {
       const int2 en = G.adj[e];
-      const int k = en.y & 0x7fffffff;
+      const int k = en.y & kAdjIndex;
       if (!G.gact[k]) continue;
       const double4* r = G.gpair + 3 * (size_t)k;
       const double4 r0 = r[0];

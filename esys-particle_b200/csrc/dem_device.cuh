@@ -32,6 +32,11 @@ constexpr int kMaxGrav = 4;
 constexpr int kMaxDyn = 2;
 constexpr int kMaxBond = 2;
 constexpr int kBondAlive = 0x7fffffff;
+// Dynamic-group adjacency entry .y: the pair index in the low 30 bits, bit 30 set under the
+// device bond hand-off when an intact bond excluded the pair as the list was built, bit 31
+// set when the entry's own particle is the pair's p1.
+constexpr int kAdjIndex = 0x3fffffff;
+constexpr int kAdjHeld = 0x40000000;
 constexpr int kBondPassThreads = 128;  // bonds per block of the bond pass
 constexpr int kTiled = 16;             // threads_per_particle setting of the tiled step kernels (dem_tiled.cuh)
 constexpr int kWarpCoop = 32;          // threads_per_particle setting of the warp-cooperative pair sums (dem_step.cuh)
@@ -91,14 +96,15 @@ struct DynDev {
   double k, ks, mu_s, mu_d, dt;
   int scaling, meanR;
   const int* adj_start; // n+1
-  const int2* adj;      // (partner slot, pair index | 0x80000000 when this particle is p1)
+  const int2* adj;      // (partner slot, pair index | kAdjHeld | 0x80000000 when this particle is p1)
   const double4* hist_in;   // RotFriction: Ffric xyz, w = slipping + 2*touching
   double4* hist_out;
   const float4* hist32_in;  // the same in the FP32 form
   float4* hist32_out;
   // device bond hand-off only (else null): per pair, the bond that excluded it when the list
   // was built, (bond group << 28) | bond index, or -1.  Such a pair is skipped while that
-  // bond is intact and becomes an ordinary pair at the step after the bond fails.
+  // bond is intact and becomes an ordinary pair at the step after the bond fails.  Its
+  // adjacency entries carry kAdjHeld.
   const int* xbond;
 };
 

@@ -208,6 +208,19 @@ void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex
   if (m > 0) k_pairs_xbond<<<(m + 255) / 256, 256, 0, s>>>(keys, m, ex, xbond);
 }
 
+// Device bond hand-off: kAdjHeld on the adjacency entries of the pairs with an excluding bond,
+// so the step tests a bit of the entry it already holds instead of loading xbond.
+__global__ void k_adj_mark_held(int ne, const int* xbond, int2* adj) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  int2 en = adj[e];
+  en.y = (en.y & ~kAdjHeld) | (xbond[en.y & kAdjIndex] >= 0 ? kAdjHeld : 0);
+  adj[e] = en;
+}
+void launch_adj_mark_held(int ne, const int* xbond, int2* adj, cudaStream_t s) {
+  if (ne > 0) k_adj_mark_held<<<(ne + 255) / 256, 256, 0, s>>>(ne, xbond, adj);
+}
+
 // Wall candidates counted from the particles' flags; intact bonds counted from the break log.
 __global__ void k_count_candidates(int n, const unsigned* pflags, int* ncand) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

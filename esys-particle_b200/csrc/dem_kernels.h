@@ -47,6 +47,7 @@ void launch_move_tagged(const Particles& P, int cur, int tag, const double* d, c
 // idx: scratch of at least P.n ints (each servo thread's candidate list)
 void launch_wall_servo(const Particles& P, int cur, int w, WallDev* walls, const double* F, int* idx, cudaStream_t s);
 void launch_pairs_xbond(const unsigned long long* keys, int m, const ExclDev& ex, int* xbond, cudaStream_t s);
+void launch_adj_mark_held(int ne, const int* xbond, int2* adj, cudaStream_t s);
 void launch_count_candidates(int n, const unsigned* pflags, int* ncand, cudaStream_t s);
 void launch_particle_field(const Particles& P, int cur, int rot, int field, double* out, cudaStream_t s);
 void launch_particle_vector_field(const Particles& P, int cur, int field, const double* initpos, double* out,

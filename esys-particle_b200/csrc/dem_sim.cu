@@ -376,8 +376,11 @@ struct DemSim {
   // Per-particle adjacency arrays are sized by the particle count: re-derive them
   // whenever particles are added or a group is created.
   void resize_adjacency() {
-    for (auto& d : dyn) build_adjacency(d.second.keys, d.second.m, d.second.adj_start, d.second.adj_count,
-                                        d.second.adj_cursor, d.second.p1_start, d.second.adj);
+    for (auto& d : dyn) {
+      build_adjacency(d.second.keys, d.second.m, d.second.adj_start, d.second.adj_count, d.second.adj_cursor,
+                      d.second.p1_start, d.second.adj);
+      if (handoff) mark_handoff(d.second);
+    }
     for (auto& b : bond) build_adjacency(b.second.keys, b.second.nb, b.second.adj_start, b.second.adj_count,
                                          b.second.adj_cursor, b.second.p1_start, b.second.adj);
     sync();
@@ -588,15 +591,15 @@ struct DemSim {
   // PIS_NE::update / PIS_ED::update after a rebuild: the full pair list with history carried
   // for persistent RotFriction interactions (pi_storage_ne.hpp:49-80, pi_storage_ed.hpp:84-129).
   void dyn_full_update(DynGroup& G) {
-    const ExclDev ex_bonds = excl_of(G);
-    // with the device hand-off the list keeps the bond-excluded pairs (marked in xbond)
-    const ExclDev ex = handoff ? ExclDev{} : ex_bonds;
+    // with the device hand-off the list keeps the bond-excluded pairs (marked by mark_handoff)
+    const ExclDev ex = handoff ? ExclDev{} : excl_of(G);
     scratch_i.reserve(n + 1); scratch_j.reserve(n + 1);
     launch_pairs_count(g, P, cur, cell_start.p, cell_list.p, ex, scratch_i.p, s);
     scan_tmp.reserve(scan_tmp_ints(n + 2));
     launch_scan(scratch_i.p, scratch_j.p, n, scalars.p, scan_tmp.p, s);
     const int m = read_int(scalars.p);
     c_launches += 3;
+    check_list_size(m);
     G.keys_spare.reserve(std::max(m, 1));
     if (G.kind != 0) G.hist_spare.reserve(std::max(m, 1));
     if (fp32) {
@@ -618,11 +621,23 @@ struct DemSim {
       }
     }
     G.m = m;
-    if (handoff) {
-      G.xbond.reserve(std::max(m, 1));
-      launch_pairs_xbond(G.keys.p, m, ex_bonds, G.xbond.p, s);
-    }
     build_adjacency(G.keys, m, G.adj_start, G.adj_count, G.adj_cursor, G.p1_start, G.adj);
+    if (handoff) mark_handoff(G);
+  }
+
+  // A dynamic group's adjacency entries hold the pair index in 30 bits (kAdjIndex).
+  static void check_list_size(long long m) {
+    if (m > (long long)kAdjIndex + 1) throw StateError("a dynamic interaction group would hold more than 2^30 pairs");
+  }
+
+  // Device bond hand-off: per pair of the list the intact bond that excludes it (xbond) and
+  // kAdjHeld on the pair's two adjacency entries.  Run after every build of the group's
+  // adjacency while the hand-off is on.
+  void mark_handoff(DynGroup& G) {
+    G.xbond.reserve(std::max(G.m, 1));
+    launch_pairs_xbond(G.keys.p, G.m, excl_of(G), G.xbond.p, s);
+    launch_adj_mark_held(2 * G.m, G.xbond.p, G.adj.p, s);
+    c_launches += 2;
   }
 
   // PIS_NE / PIS_ED::update without a rebuild: append the "new list" of flagged pairs
@@ -640,6 +655,7 @@ struct DemSim {
       c_launches += 2;
       G.cand.reserve(nb);
       launch_newlist_write(g, P, cell_start.p, cell_list.p, ex, G.keys.p, G.m, check_in, scratch_j.p, G.cand.p, s);
+      check_list_size((long long)G.m + nb);
       const int m2 = G.m + nb;
       G.keys_spare.reserve(m2);
       if (fp32) {
@@ -2830,7 +2846,10 @@ int dem_add_exclusion(dem_sim* h, const char* bonded, const char* dynamic) {
       throw std::invalid_argument("nonexisting interaction group");
     dem::DynGroup& G = dy->second;
     G.excl.push_back(bonded);
-    if (G.m > 0) {  // clean out pairs that are now excluded, keeping the others' history
+    if (G.m > 0 && s.handoff) {  // the hand-off keeps excluded pairs in the list, marked
+      s.mark_handoff(G);
+      s.sync();
+    } else if (G.m > 0) {  // clean out pairs that are now excluded, keeping the others' history
       dem::BondGroup& B = s.bond[bonded];
       std::vector<unsigned long long> keys(G.m), bk(B.nb);
       std::vector<double4> hist(G.kind != 0 ? G.m : 0);

@@ -101,6 +101,25 @@ struct WarpCoopSupported {
   static constexpr bool value = (FEAT & (F_NFRIC | F_BOND | F_STRESS)) == 0;
 };
 
+// Device bond hand-off: whether adjacency entry .y = ey of group G is skipped at this step
+// because the intact bond that excluded its pair when the list was built still holds.  Only
+// bond failures set Particles::flagged, and under the hand-off nothing clears it while a list
+// stands, so a particle whose flag is clear still has every bond the list's exclusions name and
+// only a flagged one reads the bond's failure step.  A failure in the current step keeps its
+// pair held until the next step whether or not its flag is seen set.
+__device__ __forceinline__ bool handoff_held(const StepArgs& a, const DynDev& G, int ey, bool self_flagged,
+                                             long long step) {
+  if (!G.xbond || !(ey & kAdjHeld)) return false;
+  if (!self_flagged) return true;
+  const int xb = __ldg(G.xbond + (ey & kAdjIndex));
+  return a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step;
+}
+
+// The flag that handoff_held takes for particle i (read only under the hand-off).
+__device__ __forceinline__ bool handoff_flag(const StepArgs& a, int i) {
+  return a.handoff && a.P.flagged[i] != 0;
+}
+
 // CParticle::applyForce's stress update (Model/Particle.cpp:392-401): m_sigma(i,j) -= f[i] * (pos - x)[j].
 __device__ __forceinline__ void stress_add(double* S, const V& f, const V& pos, const V& x) {
   const V r = pos - x;
@@ -146,6 +165,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
       v4 = ldg4(in.vm + i);
       if (ROT) w4 = ldg4(in.wi + i);
     }
+    const bool flg = handoff_flag(a, i);
     for (int d = 0; d < a.ndyn; ++d) {
       const DynDev& G = a.dyn[d];
       const int e0 = __ldg(G.adj_start + i), e1 = __ldg(G.adj_start + i + 1);
@@ -161,13 +181,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
         // partner record is not fetched
         bool held[kBatch];
 #pragma unroll
-        for (int b = 0; b < kBatch; ++b) {
-          held[b] = false;
-          if (G.xbond && en[b].x >= 0) {
-            const int xb = __ldg(G.xbond + (en[b].y & 0x7fffffff));
-            held[b] = xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step;
-          }
-        }
+        for (int b = 0; b < kBatch; ++b) held[b] = en[b].x >= 0 && handoff_held(a, G, en[b].y, flg, step);
 #pragma unroll
         for (int b = 0; b < kBatch; ++b)
           pjs[b] = (en[b].x >= 0 && !held[b]) ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
@@ -176,7 +190,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
           if (en[b].x < 0) continue;
           const int j = en[b].x;
           const bool isp1 = en[b].y < 0;
-          const int k = en[b].y & 0x7fffffff;
+          const int k = en[b].y & kAdjIndex;
           if (held[b]) {
             if (isp1 && !EVAL) {
               if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -480,6 +494,7 @@ __device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const Particle
         wself = mk((float)w4.x, (float)w4.y, (float)w4.z);
       }
     }
+    const int flg = valid && alive && handoff_flag(a, i) ? 1 : 0;
     for (int d = 0; d < a.ndyn; ++d) {
       const DynDev& G = a.dyn[d];
       int s0 = valid ? __ldg(G.adj_start + i) : 0;
@@ -498,23 +513,21 @@ __device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const Particle
         }
         const int oi = __shfl_sync(kFull, i, o);
         const bool oalive = __shfl_sync(kFull, (int)alive, o) != 0;
+        const bool oflg = __shfl_sync(kFull, flg, o) != 0;
         const double4 po = make_double4(__shfl_sync(kFull, p4.x, o), __shfl_sync(kFull, p4.y, o),
                                         __shfl_sync(kFull, p4.z, o), __shfl_sync(kFull, p4.w, o));
         const bool act = has && oalive;
         const int2 en = act ? __ldg(G.adj + e) : make_int2(-1, 0);
         const int j = en.x;
         const bool isp1 = en.y < 0;
-        const int k = en.y & 0x7fffffff;
+        const int k = en.y & kAdjIndex;
         bool live = act;
-        if (act && G.xbond) {  // device bond hand-off: skipped while the bond that excluded it holds
-          const int xb = __ldg(G.xbond + k);
-          if (xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step) {
-            if (isp1 && !EVAL) {
-              if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-              else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
-            }
-            live = false;
+        if (act && handoff_held(a, G, en.y, oflg, step)) {  // device bond hand-off
+          if (isp1 && !EVAL) {
+            if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);
           }
+          live = false;
         }
         const double4 pj = live ? ldg4(in.pr + j) : make_double4(0.0, 0.0, 0.0, 0.0);
         // canonical orientation: p1 = lower id

@@ -63,7 +63,7 @@ struct TileSmem {
   int start[kTileThreads + 1];     // the tile's adjacency starts
   int owner[kChunkMax];            // local particle of each entry of the chunk
   unsigned char live[kChunkMax];   // entry contributes (touching pair / intact bond)
-  unsigned char alive[kTileThreads];
+  unsigned char alive[kTileThreads];  // bit 0 alive; bit 1 its hand-off flag
   double4 p[kTileThreads];         // the tile's positions and radii
   union {
     struct { T f[3][kPairChunk]; T m[3][kPairChunk]; } pair;
@@ -87,13 +87,10 @@ __device__ __forceinline__ bool tile_pair_test(const StepArgs& a, const DynDev& 
   const int o = S.owner[u];
   if (!S.alive[o]) return false;
   const bool isp1 = en.y < 0;
-  const int k = en.y & 0x7fffffff;
+  const int k = en.y & kAdjIndex;
   bool clear = false, eval = false;
-  bool held = false;
-  if (G.xbond) {  // device bond hand-off: skipped while the bond that excluded it holds
-    const int xb = __ldg(G.xbond + k);
-    held = xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step;
-  }
+  // device bond hand-off: skipped while the bond that excluded it holds
+  const bool held = handoff_held(a, G, en.y, (S.alive[o] & 2) != 0, step);
   if (held) {
     clear = true;
   } else {
@@ -126,7 +123,7 @@ __device__ __forceinline__ bool tile_pair_law(const StepArgs& a, const ParticleB
   const int o = S.owner[u];
   const int j = en.x;
   const bool isp1 = en.y < 0;
-  const int k = en.y & 0x7fffffff;
+  const int k = en.y & kAdjIndex;
   const double4 ps = S.p[o];
   const double4 pa = isp1 ? ps : pj, pb = isp1 ? pj : ps;
   const V x1 = xyz(pa), x2 = image_of(a.g, x1, xyz(pb));
@@ -238,11 +235,8 @@ __device__ __forceinline__ void tile_eval_pairs(const StepArgs& a, const Particl
     bool held[kB];
 #pragma unroll
     for (int b = 0; b < kB; ++b) {
-      held[b] = false;
-      if (G.xbond && en[b].x >= 0) {
-        const int xb = __ldg(G.xbond + (en[b].y & 0x7fffffff));
-        held[b] = xb >= 0 && a.bond[xb >> 28].broken_step[xb & 0x0fffffff] > step;
-      }
+      const int u = u0 + b * kTileThreads;
+      held[b] = en[b].x >= 0 && handoff_held(a, G, en[b].y, (S.alive[S.owner[u]] & 2) != 0, step);
     }
 #pragma unroll
     for (int b = 0; b < kB; ++b)
@@ -413,7 +407,8 @@ __device__ __forceinline__ void tile_own(const StepArgs& a, const ParticleBuf& i
   if (starts && t == 0) st_end = __ldg(a.dyn[0].adj_start + i0 + np);
   __syncthreads();  // the previous tile's pair phase has finished with S.p / S.alive / S.start
   S.p[t] = p4;
-  S.alive[t] = (valid && (pf & PF_ALIVE)) ? 1 : 0;
+  // bit 0 alive, bit 1 the hand-off flag of a live particle (handoff_held)
+  S.alive[t] = (valid && (pf & PF_ALIVE)) ? (handoff_flag(a, i) ? 3 : 1) : 0;
   if (starts) {
     if (valid) S.start[t] = st;
     if (t == 0) S.start[np] = st_end;

@@ -53,6 +53,35 @@ def test_handoff_equals_host_handoff(gpu, precision):
     assert np.array_equal(host.wall("top")[1], dev.wall("top")[1])
 
 
+@pytest.mark.parametrize("precision,tpp", [(64, 1), (32, 1), (64, 16), (32, 16), (64, 32), (32, 32)])
+def test_handoff_equals_host_handoff_in_each_step_form(gpu, precision, tpp):
+    """Lane, tiled (16) and warp-cooperative (32) step forms with the bond pass.  A held pair is
+    recognised from a bit of its adjacency entry; only a particle that a failure has flagged reads
+    its bond's failure step, so the block has both kinds, and pairs of broken bonds that touch."""
+    host = S.bonded_block(gpu, nx=6, ny=8, nz=6, strength=(0.3, 0.6, 0.6, 0.3))
+    dev = S.bonded_block(gpu, nx=6, ny=8, nz=6, strength=(0.3, 0.6, 0.6, 0.3))
+    for s in (host, dev):
+        s.set_option("precision", precision)
+        s.set_option("bond_pass", 1)
+        s.set_option("threads_per_particle", tpp)
+    dev.set_option("bond_handoff", 1)
+    S.run_loaded(host, 200, 0.002)
+    S.run_loaded(dev, 200, 0.002)
+    ph, pd = host.particles(), dev.particles()
+    for k in ("id", "pos", "vel", "angvel", "quat", "force", "moment"):
+        assert np.array_equal(ph[k], pd[k]), k
+    bh, bd = host.breaks(), dev.breaks()
+    for u, v in zip(bh, bd):
+        assert np.array_equal(u, v)
+    flagged = np.unique(np.concatenate([bh[0], bh[1]]))
+    assert 0 < len(flagged) < len(ph["id"])
+    hp, dp = _pairs(host), _pairs(dev)
+    broken = {(int(min(a, b)), int(max(a, b))) for a, b in zip(bh[0], bh[1])}
+    assert any(dp[k][4] != 0.0 for k in broken if k in dp)  # pairs of broken bonds in contact
+    for k in dp:
+        assert hp[k] == dp[k], k
+
+
 def test_handoff_does_not_stop_chunks(gpu):
     host = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
     dev = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
