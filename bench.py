@@ -619,12 +619,15 @@ B_DT = 1e-5
 
 def block_world(n=1_000_000, seed=3):
     """The fitting packer's 1M spheres (radii in [0.2, 1.0]) in 66 x 132 x 66 (the 100 x 200 x 100
-    prism of the spec holds 1M spheres only at uniform radii), every pair within a 1e-3 gap bonded."""
+    prism of the spec holds 1M spheres only at uniform radii), every pair within a 1e-3 gap bonded.
+    Another n scales the box by (n / 1M)^(1/3) at the same packing density."""
     from esys.lsm import geometry as G
 
-    pos, rad = G.fit_pack(n, (0, 0, 0), (66, 132, 66), 0.2, 1.0, seed=seed, max_failures=300)
+    f = (n / 1e6) ** (1.0 / 3.0)
+    box = (66 * f, 132 * f, 66 * f)
+    pos, rad = G.fit_pack(n, (0, 0, 0), box, 0.2, 1.0, seed=seed, max_failures=300)
     i1, i2 = G.distance_connections(pos, rad, 1e-3)
-    return dict(pos=pos, rad=rad, i1=i1, i2=i2)
+    return dict(pos=pos, rad=rad, i1=i1, i2=i2, box=box)
 
 
 def block_sim(make, w, loader=True):
@@ -634,7 +637,7 @@ def block_sim(make, w, loader=True):
     steps split between them; dt = 1e-5."""
     pos, rad = w["pos"], w["rad"]
     n = len(rad)
-    s = make("RotSphere", 2.2, 0.2, (0, 0, 0), (66, 132, 66), (0, 0, 0), B_DT)
+    s = make("RotSphere", 2.2, 0.2, (0, 0, 0), w["box"], (0, 0, 0), B_DT)
     s.add_particles(np.arange(n, dtype=np.int32), pos, rad, (4.0 / 3.0) * PI_REF * rad ** 3,
                     tag=np.zeros(n, np.int32))
     s.add_connections(np.ones(len(w["i1"]), np.int32), w["i1"], w["i2"])
@@ -654,25 +657,31 @@ def block_sim(make, w, loader=True):
     return s
 
 
-def bonded_block_leg(stream, steps=200, warm=20, cpu=True, cpu_budget=15.0):
-    """The 1M-sphere bonded block in both precision forms (device bond hand-off on; the FP32 form
-    on the tiled kernels, which measured fastest on this dense pack), with the reference's own C++
-    (one core) on a bounded sample of the same block."""
+def bonded_block_leg(stream, steps=200, warm=20, cpu=True, cpu_budget=15.0, sweep_steps=10, n=1_000_000, tpp=0):
+    """The 1M-sphere bonded block in both precision forms (device bond hand-off on), each on the
+    step form (one lane, eight lanes or the tiled kernels) that measured fastest on a short run of
+    the same block (or on `tpp` lanes when set), with the reference's own C++ (one core) on a
+    bounded sample of the block."""
     from esys.lsm import _capi
 
     t0 = time.perf_counter()
-    w = block_world()
+    w = block_world(n)
     t_pack = time.perf_counter() - t0
     n = len(w["rad"])
     forms = {}
-    for prec, tpp in ((32, 16), (64, 0)):
+    for prec in (32, 64):
         sim = block_sim(lambda *a: _capi.DemSim(*a), w)
         sim.set_stream(stream.cuda_stream)
         sim.set_option("profile", 1)
         sim.set_option("precision", prec)
         sim.set_option("bond_handoff", 1)
-        if tpp:
-            sim.set_option("threads_per_particle", tpp)
+        table = {}
+        for t in ((tpp,) if tpp else (16, 8, 1)):
+            sim.set_option("threads_per_particle", t)
+            sim.step(2)
+            table[t] = timed_run(sim, stream, sweep_steps)[0] / sweep_steps
+        best = min(table, key=table.get)
+        sim.set_option("threads_per_particle", best)
         sim.step(warm)
         ms, c0, c1 = timed_run(sim, stream, steps)
         cu = c1["contact_updates"] - c0["contact_updates"]
@@ -688,6 +697,8 @@ def bonded_block_leg(stream, steps=200, warm=20, cpu=True, cpu_budget=15.0):
             "device_us_per_timestep": kus, "threads_per_particle": c1["threads_per_particle"],
             "intact_bonds": nb, "friction_pairs": mf, "touching_friction_pairs": touching, "wall_candidates": walls,
             "bond_breaks": int(len(sim.breaks()[0])),
+            "lanes_sweep": {"chosen": best, "ms_per_timestep": {str(k): round(v, 4) for k, v in table.items()},
+                            "timesteps_each": sweep_steps},
             "roofline": {"bound": "hbm", "achieved": alg / (kus * 1e-6) / 1e9, "unit": "GB/s",
                          "algorithmic_bytes_per_timestep": alg,
                          "kernels": "bond pass + step kernel per timestep (device time between CUDA events)"},
@@ -697,7 +708,8 @@ def bonded_block_leg(stream, steps=200, warm=20, cpu=True, cpu_budget=15.0):
     for f in forms.values():
         f["roofline"]["frac"] = f["roofline"]["achieved"] / peak
     out = {
-        "workload": f"bonded block: {n} RotSpheres fitted in 66x132x66 (r in [0.2,1.0]), {len(w['i1'])} RotBonds "
+        "workload": f"bonded block: {n} RotSpheres fitted in {'x'.join(f'{b:g}' for b in w['box'])} (r in [0.2,1.0]), "
+                    f"{len(w['i1'])} RotBonds "
                     f"(kn=ks=1e5, kt=kb=1e3, strengths 0.5/1.0/1.0/0.5), RotFriction + exclusion, platens at "
                     f"strain rate 1e-4 per 1,000 steps, dt=1e-5, device bond hand-off",
         "metric": "contact-updates/s", "timed_timesteps": steps, "warmup_timesteps": warm, "pack_s": t_pack,
@@ -1007,6 +1019,8 @@ def main():
     ap.add_argument("--no-gravity", action="store_true", help="skip the 8,000-sphere gravity-packing leg")
     ap.add_argument("--no-block", action="store_true", help="skip the 1M-sphere bonded-block leg")
     ap.add_argument("--block-steps", type=int, default=200, help="timed timesteps of the bonded-block leg")
+    ap.add_argument("--block-particles", type=int, default=1_000_000, help="spheres of the bonded block")
+    ap.add_argument("--block-tpp", type=int, default=0, help="lanes per particle of the bonded block (0: measured)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -1184,7 +1198,8 @@ def main():
         grav = gravity_leg(stream, cpu=not args.no_cpu_baseline)
     block = None
     if not args.no_block and world == 1:
-        block = bonded_block_leg(stream, steps=args.block_steps, cpu=not args.no_cpu_baseline)
+        block = bonded_block_leg(stream, steps=args.block_steps, cpu=not args.no_cpu_baseline, n=args.block_particles,
+                                 tpp=args.block_tpp)
     ens = None
     if args.ensemble_specimens > 0:
         ens = ensemble_leg(args.ensemble_specimens, args.ensemble_steps, dist=dist, window=args.ensemble_window,

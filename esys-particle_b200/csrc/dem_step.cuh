@@ -107,8 +107,11 @@ struct WarpCoopSupported {
 // stands, so a particle whose flag is clear still has every bond the list's exclusions name and
 // only a flagged one reads the bond's failure step.  A failure in the current step keeps its
 // pair held until the next step whether or not its flag is seen set.
+// Instances without bond groups (FEAT without F_BOND / F_BGATHER) hold no pair and carry none of this.
+template <int FEAT>
 __device__ __forceinline__ bool handoff_held(const StepArgs& a, const DynDev& G, int ey, bool self_flagged,
                                              long long step) {
+  if constexpr ((FEAT & (F_BOND | F_BGATHER)) == 0) return false;
   if (!G.xbond || !(ey & kAdjHeld)) return false;
   if (!self_flagged) return true;
   const int xb = __ldg(G.xbond + (ey & kAdjIndex));
@@ -116,7 +119,9 @@ __device__ __forceinline__ bool handoff_held(const StepArgs& a, const DynDev& G,
 }
 
 // The flag that handoff_held takes for particle i (read only under the hand-off).
+template <int FEAT>
 __device__ __forceinline__ bool handoff_flag(const StepArgs& a, int i) {
+  if constexpr ((FEAT & (F_BOND | F_BGATHER)) == 0) return false;
   return a.handoff && a.P.flagged[i] != 0;
 }
 
@@ -165,7 +170,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
       v4 = ldg4(in.vm + i);
       if (ROT) w4 = ldg4(in.wi + i);
     }
-    const bool flg = handoff_flag(a, i);
+    const bool flg = handoff_flag<FEAT>(a, i);
     for (int d = 0; d < a.ndyn; ++d) {
       const DynDev& G = a.dyn[d];
       const int e0 = __ldg(G.adj_start + i), e1 = __ldg(G.adj_start + i + 1);
@@ -181,7 +186,7 @@ __device__ __forceinline__ void pair_sums(const StepArgs& a, const ParticleBuf& 
         // partner record is not fetched
         bool held[kBatch];
 #pragma unroll
-        for (int b = 0; b < kBatch; ++b) held[b] = en[b].x >= 0 && handoff_held(a, G, en[b].y, flg, step);
+        for (int b = 0; b < kBatch; ++b) held[b] = en[b].x >= 0 && handoff_held<FEAT>(a, G, en[b].y, flg, step);
 #pragma unroll
         for (int b = 0; b < kBatch; ++b)
           pjs[b] = (en[b].x >= 0 && !held[b]) ? ldg4(in.pr + en[b].x) : make_double4(0.0, 0.0, 0.0, 0.0);
@@ -494,7 +499,7 @@ __device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const Particle
         wself = mk((float)w4.x, (float)w4.y, (float)w4.z);
       }
     }
-    const int flg = valid && alive && handoff_flag(a, i) ? 1 : 0;
+    const int flg = valid && alive && handoff_flag<FEAT>(a, i) ? 1 : 0;
     for (int d = 0; d < a.ndyn; ++d) {
       const DynDev& G = a.dyn[d];
       int s0 = valid ? __ldg(G.adj_start + i) : 0;
@@ -522,7 +527,7 @@ __device__ __forceinline__ void pair_sums_warp(const StepArgs& a, const Particle
         const bool isp1 = en.y < 0;
         const int k = en.y & kAdjIndex;
         bool live = act;
-        if (act && handoff_held(a, G, en.y, oflg, step)) {  // device bond hand-off
+        if (act && handoff_held<FEAT>(a, G, en.y, oflg, step)) {  // device bond hand-off
           if (isp1 && !EVAL) {
             if (FP32) G.hist32_out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
             else G.hist_out[k] = make_double4(0.0, 0.0, 0.0, 0.0);

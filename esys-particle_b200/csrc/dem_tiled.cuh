@@ -90,7 +90,7 @@ __device__ __forceinline__ bool tile_pair_test(const StepArgs& a, const DynDev& 
   const int k = en.y & kAdjIndex;
   bool clear = false, eval = false;
   // device bond hand-off: skipped while the bond that excluded it holds
-  const bool held = handoff_held(a, G, en.y, (S.alive[o] & 2) != 0, step);
+  const bool held = handoff_held<FEAT>(a, G, en.y, (S.alive[o] & 2) != 0, step);
   if (held) {
     clear = true;
   } else {
@@ -236,7 +236,7 @@ __device__ __forceinline__ void tile_eval_pairs(const StepArgs& a, const Particl
 #pragma unroll
     for (int b = 0; b < kB; ++b) {
       const int u = u0 + b * kTileThreads;
-      held[b] = en[b].x >= 0 && handoff_held(a, G, en[b].y, (S.alive[S.owner[u]] & 2) != 0, step);
+      held[b] = en[b].x >= 0 && handoff_held<FEAT>(a, G, en[b].y, (S.alive[S.owner[u]] & 2) != 0, step);
     }
 #pragma unroll
     for (int b = 0; b < kB; ++b)
@@ -408,7 +408,7 @@ __device__ __forceinline__ void tile_own(const StepArgs& a, const ParticleBuf& i
   __syncthreads();  // the previous tile's pair phase has finished with S.p / S.alive / S.start
   S.p[t] = p4;
   // bit 0 alive, bit 1 the hand-off flag of a live particle (handoff_held)
-  S.alive[t] = (valid && (pf & PF_ALIVE)) ? (handoff_flag(a, i) ? 3 : 1) : 0;
+  S.alive[t] = (valid && (pf & PF_ALIVE)) ? (handoff_flag<FEAT>(a, i) ? 3 : 1) : 0;
   if (starts) {
     if (valid) S.start[t] = st;
     if (t == 0) S.start[np] = st_end;
