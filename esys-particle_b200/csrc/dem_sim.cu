@@ -893,11 +893,20 @@ struct DemSim {
     return bond.empty() || bond_pass || fp32;
   }
 
-  // Lanes per particle when none is set: from the mean adjacency length.  The tiled kernels
-  // (kTiled) are chosen explicitly or by the ensemble autotuner; on the 250k shear cell and
-  // the 1M bonded block they measured no faster than the lane kernels.
+  // Lanes per particle when none is set.  A specimen with at least as many particles as the
+  // GPU keeps step threads resident (3 blocks of 256 per SM) already fills it at one lane per
+  // particle, which measured fastest on the 250k shear cell and the 1M bonded block; a smaller
+  // one spreads each particle's adjacency over lanes by its mean length.  The tiled kernels
+  // (kTiled) are chosen explicitly or by the ensemble autotuner.
   int pick_tpp() {
     if (tpp) return tpp == kTiled && !tiled_ok() ? 1 : tpp;
+    static const long long resident = [] {
+      int dev = 0, sms = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      return 768LL * (sms > 0 ? sms : 148);
+    }();
+    if (n >= resident) return 1;
     long long e = 0;
     for (auto& d : dyn) e += 2LL * d.second.m;
     for (auto& b : bond) e += 2LL * b.second.nb;

@@ -276,8 +276,9 @@ int dem_precision_report(dem_sim* h, double* out, int n);
 int dem_wall_reactions_noalloc(int n, const double* particles, int nwall, const double* walls, double* reactions,
                                void* stream);
 
-/* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic, 1, 2, 4, 8,
- * 16 = block-cooperative tiles),
+/* Tuning knobs with no reference counterpart: "threads_per_particle" (0 = automatic: one lane for
+ * a specimen with at least 768 particles per SM, else by the mean adjacency length; 1, 2, 4, 8;
+ * 16 = block-cooperative tiles; 32 = warp-cooperative pair sums),
  * "chunk" (steps launched per host round trip), "store_forces" (keep per-particle F/M),
  * "profile" (time the force/integration kernels with CUDA events), "precision" (64 = FP64 form,
  * 32 = FP32 pair forces with Kahan-compensated accumulation, FP64 positions / contact detection /

@@ -82,6 +82,32 @@ def test_handoff_equals_host_handoff_in_each_step_form(gpu, precision, tpp):
         assert hp[k] == dp[k], k
 
 
+@pytest.mark.parametrize("tpp", [1, 32])
+def test_exclusion_added_while_running_under_handoff(gpu, tpp):
+    """TSubLattice::setExIG on lists that already hold bonded pairs (SubLattice.hpp:1980-2009): the
+    host path removes them, the hand-off keeps and marks them held; the runs stay bit-identical.
+    The lanes are fixed: with several lanes per particle the entries a lane sums depend on the
+    list's length, which differs between the two paths (held pairs stay in the hand-off's list)."""
+    host = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3), with_friction=False)
+    dev = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3), with_friction=False)
+    for s in (host, dev):
+        s.add_rot_friction_group("friction", 1e5, 0.6, 0.6, 1e5, 1e-5, True, True)
+        s.set_option("bond_pass", 1)
+        s.set_option("threads_per_particle", tpp)
+    dev.set_option("bond_handoff", 1)
+    for s in (host, dev):
+        S.run_loaded(s, 5, 0.002)
+        s.add_exclusion("bonds", "friction")
+        S.run_loaded(s, 150, 0.002)
+    ph, pd = host.particles(), dev.particles()
+    for k in ("pos", "vel", "angvel", "quat", "force", "moment"):
+        assert np.array_equal(ph[k], pd[k]), k
+    bh, bd = host.breaks(), dev.breaks()
+    assert len(bh[0]) > 0
+    for u, v in zip(bh, bd):
+        assert np.array_equal(u, v)
+
+
 def test_handoff_does_not_stop_chunks(gpu):
     host = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
     dev = S.bonded_block(gpu, strength=(0.3, 0.6, 0.6, 0.3))
