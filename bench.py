@@ -824,7 +824,7 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
 
     from esys.lsm import _capi
     from esys.lsm.autotune import autotune_ensemble
-    from esys.lsm.parallel import partition_specimens
+    from esys.lsm.parallel import partition_specimens, sharded_totals
 
     world = dist.get_world_size() if dist is not None else 1
     rank = dist.get_rank() if dist is not None else 0
@@ -853,12 +853,7 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
     dt = time.perf_counter() - t0
     c1 = e.counters()
     contacts = float(c1["contact_updates"] - c0["contact_updates"])
-    if dist is not None:
-        tt = torch.tensor([dt, contacts], device="cuda", dtype=torch.float64)
-        t_max = tt[:1].clone()
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
-        dt, contacts = float(t_max.item()), float(tt[1].item())
+    dt, contacts = sharded_totals(dt, contacts, dist, device="cuda")
     value = contacts / dt
     kern_ms = (c1["step_kernel_ns"] - c0["step_kernel_ns"]) / 1e6
     # FP32 force error vs FP64 on the developed states of a few specimens
@@ -895,12 +890,7 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
     e64.close()
     for s in sims64:
         s.close()
-    if dist is not None:
-        tt = torch.tensor([t_b64, c_b64], device="cuda", dtype=torch.float64)
-        t_max = tt[:1].clone()
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
-        t_b64, c_b64 = float(t_max.item()), float(tt[1].item())
+    t_b64, c_b64 = sharded_totals(t_b64, c_b64, dist, device="cuda")
     batched64 = c_b64 / t_b64
     # plain FP64 GPU form: a size-stratified sample of the specimens, each stepped alone
     nloc = len(specs)
@@ -917,12 +907,8 @@ def ensemble_leg(nspec, steps, fp64_sample=32, fp64_steps=100, dist=None, window
         t64 += time.perf_counter() - t0
         c64 += s.counters()["contact_updates"] - a["contact_updates"]
         s.close()
-    if dist is not None:  # every GPU runs its own sample: aggregate rate = sum of counts / max time
-        tt = torch.tensor([t64, float(c64)], device="cuda", dtype=torch.float64)
-        t_max = tt[:1].clone()
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
-        t64, c64 = float(t_max.item()), float(tt[1].item())
+    # every GPU runs its own sample: aggregate rate = sum of counts / max time
+    t64, c64 = sharded_totals(t64, c64, dist, device="cuda")
     plain = c64 / t64
     return {
         "workload": f"{nspec} bonded cylinders (height 4R), particle counts log-uniform in [2,000, 40,000] "
