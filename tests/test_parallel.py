@@ -71,6 +71,18 @@ def test_partition_by_work_per_particle():
     assert sorted(map(sorted, parts)) == [[0, 1], [2]]
 
 
+def test_partition_edges():
+    """More ranks than specimens leaves the extra ranks empty; no specimens gives empty shares;
+    a world below one is refused; without a process group the helpers act on the one process."""
+    assert partition_specimens([7, 3], 4) == [[0], [1], [], []]
+    assert partition_specimens([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        partition_specimens([1], 0)
+    merged, mine = run_share([4, 2], lambda k: 10 * k, lambda sims: {k: v + 1 for k, v in sims.items()})
+    assert merged == {0: 1, 1: 11} and mine == [0, 1]
+    assert sharded_totals(2.5, 7) == (2.5, 7.0)
+
+
 # Specimen k of the stepped test: a small bonded block (seed and height from k) under platen loading.
 _SPEC_STEPS = 40
 
