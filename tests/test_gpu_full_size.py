@@ -1,4 +1,4 @@
-"""The survey's configurations at full size on the GPU, through size-independent checks and
+"""The benchmark configurations at full size on the GPU, through size-independent checks and
 against the oracles.
 
 - 8,000-sphere gravity packing (NRotElastic, gravity, damping, six walls): the full 5,000-step
